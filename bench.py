@@ -1,0 +1,363 @@
+"""Benchmark: cells/s of PCA50 + exact kNN15 at 1M cells on one B200.
+
+Workload (``config.workload``): 1,000,000 cells x 2,000 genes, f32 log1p CSR with about
+600 stored values per cell (negative-binomial counts, log-normal gene means, 50 planted
+cell types, normalize_total(1e4) + log1p), seeded synthetic data of the benchmark's
+shape; then kyto's PCA (50 components, seed 0, 11 passes) and exact Euclidean kNN
+(n_neighbors 15 = 14 stored neighbours per cell, kyto's semantics).
+
+One step = the whole path over the whole dataset: push the CSR to the PCA session
+(held in HBM), run all passes, search the embedding's exact neighbours.
+- ``value``: inputs already resident in HBM when the timed region starts (device CSR).
+- ``e2e``: the same through the public API from pinned host CSR, host->device copy of
+  the input and device->host copy of the graph inside every step.
+Inputs (4.8 GB) are larger than L2 (126 MB), so no flush is needed between steps.
+
+``--impl reference``: kyto's CPU algorithms (the C++ restatement in oracle/, all host
+threads) timed on a bounded sample of the same workload: the PCA over a subset of the
+cells (all 11 passes) and the exact search of a subset of query cells against every
+cell; cells/s = 1 / (PCA seconds per cell + kNN seconds per query cell).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "cells/s PCA50+kNN15 at 1M cells"
+WORKLOAD = "1M cells x 2,000 genes f32 log1p CSR (~600 nnz/cell, 50 planted types) -> PCA 50 (11 passes, seed 0) -> exact kNN n_neighbors 15"
+
+
+def parse() -> argparse.Namespace:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cells", type=int, default=1_000_000)
+    ap.add_argument("--genes", type=int, default=2000)
+    ap.add_argument("--nnz", type=float, default=600.0)
+    ap.add_argument("--types", type=int, default=50)
+    ap.add_argument("--components", type=int, default=50)
+    ap.add_argument("--neighbors", type=int, default=15)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-pca-cells", type=int, default=40_000)
+    ap.add_argument("--cpu-knn-queries", type=int, default=1024)
+    return ap.parse_args()
+
+
+def peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "bf16_tflops": d["bf16_tflops"],
+                "bf16_tflops_sustained": d.get("bf16_tflops_sustained"), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+            "source": "fallback"}
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"kyto_clocks_{os.getpid()}.csv"
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        self.path.unlink(missing_ok=True)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_data(args, rank: int):
+    """The workload's CSR on the host (numpy) and the device (torch)."""
+    import torch
+
+    import kyto_b200 as K
+    from kyto_b200 import synthetic
+
+    x = synthetic.counts_csr(args.cells, args.genes, args.nnz, args.types, 200, mu=0.0,
+                             sigma=1.5, dispersion=0.3, seed=rank, device="cuda")
+    ctx = K.default_context()
+    dev_indptr = torch.from_numpy(x.indptr.view(np.int64)).cuda()
+    dev_idx = torch.from_numpy(x.indices.view(np.int32)).cuda()
+    dev_counts = torch.from_numpy(x.values.view(np.int32)).cuda()
+    dev_vals = torch.empty(x.nnz, dtype=torch.float32, device="cuda")
+    # normalize_total(1e4) + log1p with the library's own map kernel (data preparation).
+    K._check(K.library().kg_normalize_log1p(
+        ctx.handle, K._ptr(dev_indptr), K._ptr(dev_counts), K.KG_U32, x.n_cells, 1e4, 1,
+        K._ptr(dev_vals)))
+    del dev_counts
+    vals = dev_vals.cpu().numpy()
+    torch.cuda.synchronize()
+    return x, vals, dev_indptr, dev_idx, dev_vals
+
+
+def run_step(args, ctx, indptr, idx, vals, out, host: bool):
+    """One step through the public API: PCA session + exact kNN."""
+    import kyto_b200 as K
+
+    sess = K.PcaSession(args.components, args.genes, seed=0, ctx=ctx)
+    sess.push(indptr, idx, vals)
+    sess.run()
+    n = args.cells
+    emb_ptr = sess.embedding_device_ptr()
+    stats = K.KnnStats()
+    L = K.library()
+    K._check(L.kg_knn_exact(ctx.handle, emb_ptr, n, args.components, 0, args.neighbors,
+                            K._ptr(out[0]), K._ptr(out[1]), K._ptr(out[2]),
+                            K.ctypes.byref(stats)))
+    sess.close()
+    return stats
+
+
+def cpu_baseline(args, x, vals, embedding) -> dict:
+    """kyto's CPU path (the oracle's C++ restatement) on a bounded sample."""
+    from oracle import oracle as O
+
+    threads = O.max_threads()
+    s = min(args.cpu_pca_cells, args.cells)
+    e = int(x.indptr[s])
+    sub = O.Csr(x.indptr[: s + 1], x.indices[:e], vals[:e], args.genes)
+    t0 = time.perf_counter()
+    O.pca(sub, args.components, 0)
+    t_pca = time.perf_counter() - t0
+    q = min(args.cpu_knn_queries, args.cells)
+    t0 = time.perf_counter()
+    O.knn_exact_sample(embedding, args.neighbors, 0, q)
+    t_knn = time.perf_counter() - t0
+    per_cell = t_pca / s + t_knn / q
+    return {
+        "value": 1.0 / per_cell, "unit": "cells/s", "cores": threads, "kind": "port",
+        "sample": (f"kyto's CPU PCA (C++ restatement, {threads} threads) over the first {s:,} "
+                   f"cells, all 11 passes ({t_pca:.2f} s), and its filtered exact kNN for "
+                   f"{q:,} query cells against all {args.cells:,} ({t_knn:.2f} s); "
+                   f"cells/s = 1/(PCA s per cell + kNN s per query)"),
+        "pca_s_per_cell": t_pca / s, "knn_s_per_query": t_knn / q,
+    }
+
+
+def main() -> int:
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return reference_arm(args, rank, world)
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    import kyto_b200 as K
+
+    ctx = K.Context(local)
+    K._default = ctx
+    x, vals, d_indptr, d_idx, d_vals = make_data(args, rank)
+    n, k = args.cells, args.neighbors - 1
+    out_dev = (torch.empty(n + 1, dtype=torch.int64, device="cuda"),
+               torch.empty(n * k, dtype=torch.int32, device="cuda"),
+               torch.empty(n * k, dtype=torch.float32, device="cuda"))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(args.warmup):
+        run_step(args, ctx, d_indptr, d_idx, d_vals, out_dev, host=False)
+    clocks = Clocks(local)
+    launches0 = K.kernel_launches()
+    barrier()
+    clocks.start()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    filter_ms = []
+    for _ in range(args.steps):
+        st = run_step(args, ctx, d_indptr, d_idx, d_vals, out_dev, host=False)
+        filter_ms.append(st.filter_ms)
+    stop.record()
+    barrier()
+    clk = clocks.stop()
+    launches = K.kernel_launches() - launches0
+    ms = max_over_ranks(start.elapsed_time(stop) / args.steps)
+    value = world * n / (ms / 1e3)
+
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda a: torch.from_numpy(a).pin_memory()  # noqa: E731
+        h_indptr = pin(x.indptr.view(np.int64))
+        h_idx = pin(x.indices.view(np.int32))
+        h_vals = pin(vals)
+        out_host = (torch.empty(n + 1, dtype=torch.int64).pin_memory(),
+                    torch.empty(n * k, dtype=torch.int32).pin_memory(),
+                    torch.empty(n * k, dtype=torch.float32).pin_memory())
+        run_step(args, ctx, h_indptr, h_idx, h_vals, out_host, host=True)
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            run_step(args, ctx, h_indptr, h_idx, h_vals, out_host, host=True)
+        e1.record()
+        barrier()
+        ems = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+        h2d = x.indptr.nbytes + x.indices.nbytes + vals.nbytes
+        d2h = sum(t.numel() * t.element_size() for t in out_host)
+        e2e = {"value": world * n / (ems / 1e3), "unit": "cells/s", "ms_per_step": ems,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    pk = peaks()
+    d = args.components
+    fl = 2.0 * n * n * d
+    f_ms = statistics.median(filter_ms)
+    achieved = fl / (f_ms / 1e3) / 1e12
+    roofline = {
+        "kernel": "kNN candidate filter (distance GEMM + selection)",
+        "bound": "tensor", "achieved": achieved, "peak": pk["bf16_tflops"], "unit": "TFLOP/s",
+        "frac": achieved / pk["bf16_tflops"], "traffic": None,
+        "peak_source": f"{pk['source']} (bf16 burst)", "launch_ms": f_ms,
+        "algorithmic": f"2*n^2*d = {fl:.3e} flop per launch (n={n}, d={d})",
+    }
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        emb = np.empty((n, d), dtype=np.float32)
+        sess = K.PcaSession(args.components, args.genes, seed=0, ctx=ctx)
+        sess.push(d_indptr, d_idx, d_vals)
+        sess.run()
+        emb = sess.results().embedding
+        sess.close()
+        cpu = cpu_baseline(args, x, vals, emb)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 values; f64 dense steps and exact keys", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "cells": n, "genes": args.genes,
+                       "nnz": x.nnz, "n_components": d, "n_neighbors": args.neighbors,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs (>4 GB) larger than L2; no flush"},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "clocks": clk, "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def reference_arm(args, rank: int, world: int) -> int:
+    """kyto's CPU path (oracle restatement) on the box's host cores; rank 0 only."""
+    if rank != 0:
+        return 0
+    from kyto_b200 import synthetic
+    from oracle import oracle as O
+
+    threads = O.max_threads()
+    s = min(args.cpu_pca_cells, args.cells)
+    # The sample's own data: the first s cells of the same generator, and a kNN sample
+    # over the full embedding's shape (points from a Gaussian mixture of 50 types in 50
+    # dimensions stand in for the PCA embedding, which needs the full PCA to exist).
+    x = synthetic.counts_csr(s, args.genes, args.nnz, args.types, 200, seed=0, device="cpu")
+    sub = O.normalize_log1p(O.Csr(x.indptr, x.indices, x.values, args.genes))
+    pts, _ = synthetic.gaussian_mixture(args.cells, args.components, args.types, seed=0,
+                                        device="cpu")
+    q = min(args.cpu_knn_queries, args.cells)
+
+    def step():
+        t0 = time.perf_counter()
+        O.pca(sub, args.components, 0)
+        t1 = time.perf_counter()
+        O.knn_exact_sample(pts, args.neighbors, 0, q)
+        t2 = time.perf_counter()
+        return t1 - t0, t2 - t1
+
+    for _ in range(args.warmup):
+        step()
+    times = [step() for _ in range(args.steps)]
+    t_pca = statistics.median(t[0] for t in times)
+    t_knn = statistics.median(t[1] for t in times)
+    value = 1.0 / (t_pca / s + t_knn / q)
+    cpu = {"value": value, "unit": "cells/s", "cores": threads, "kind": "port",
+           "sample": (f"PCA over {s:,} cells (11 passes) {t_pca:.2f} s + exact kNN of {q:,} "
+                      f"queries against {args.cells:,} points {t_knn:.2f} s per step")}
+    line = {"metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * (t_pca + t_knn), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32 (CPU)",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "cells": args.cells, "genes": args.genes,
+                       "n_components": args.components, "n_neighbors": args.neighbors},
+            "cpu_baseline": cpu,
+            "e2e": {"value": value, "unit": "cells/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,189 @@
+/*
+ * kyto_gpu.h - the C ABI of libkyto_gpu.so, a B200 (sm_100a) backend for kyto's
+ * PCA -> exact-kNN hot path.
+ *
+ * It replaces, for this path, the Rust type `kyto_gpu::DeviceKernels` of datavil/kyto
+ * (crates/kyto-gpu/src/launch.rs:42-93, launch_matrix.rs:183-287) with coarser,
+ * device-resident calls: a whole PCA (all 11 Krylov passes, the input held in HBM) or a
+ * whole exact-kNN search per call instead of one host round trip per fold.
+ *
+ * Conventions (all entry points):
+ *  - Plain pointers and sizes only. Array arguments may be host or device (CUDA)
+ *    pointers unless a comment says otherwise; host arrays are only read or written
+ *    during the call.
+ *  - Every call returns a kg_status; no C++ exception crosses the ABI. After an error
+ *    kg_last_error() gives the message (kyto's KytoError text goes there).
+ *  - Status -> kyto error code: KG_ERR_INVALID -> KY-E215, KG_ERR_DEVICE / KG_ERR_OOM /
+ *    KG_ERR_TIMEOUT / KG_ERR_STATE -> KY-E505, KG_CANCELLED -> KY-E503
+ *    (kyto errors.toml:635,790,826,839).
+ *  - A kg_ctx may be used from several threads for distinct sessions (each session
+ *    has its own CUDA stream); one session is used from one thread at a time.
+ *  - Results are the same bits run to run (no floating-point atomics on any path).
+ */
+#ifndef KYTO_GPU_H
+#define KYTO_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define KG_API __attribute__((visibility("default")))
+#else
+#define KG_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum kg_status {
+  KG_OK = 0,
+  KG_ERR_INVALID = 1,   /* input outside the contract (kyto: KY-E215) */
+  KG_ERR_DEVICE = 2,    /* a CUDA call failed (kyto: KY-E505) */
+  KG_ERR_OOM = 3,       /* device memory exhausted (KY-E505, "lower memory_limit") */
+  KG_CANCELLED = 4,     /* the cancel flag was set (kyto: KY-E503) */
+  KG_ERR_TIMEOUT = 5,   /* a bounded wait on the device ran out (KY-E505) */
+  KG_ERR_STATE = 6      /* calls out of order, e.g. results before run (KY-E505) */
+} kg_status;
+
+/* Value type of a CSR block: kyto's CellValues::{U32, F32}
+ * (crates/kyto-store/src/cell_block.rs). */
+typedef enum kg_dtype { KG_U32 = 0, KG_F32 = 1 } kg_dtype;
+
+typedef struct kg_ctx kg_ctx;
+typedef struct kg_pca kg_pca;
+
+/* ---------------------------------------------------------------- context --------- */
+
+/* Open device `device` (a CUDA ordinal). Replaces DeviceKernels::open
+ * (crates/kyto-gpu/src/launch.rs:81-93). */
+KG_API kg_status kg_open(int device, kg_ctx** out);
+KG_API void kg_close(kg_ctx* ctx);
+
+/* The last error's message, NUL-terminated into buf (truncated to len); returns the
+ * message length. Thread-local per context. */
+KG_API size_t kg_last_error(const kg_ctx* ctx, char* buf, size_t len);
+
+/* A flag polled between passes and query tiles; nonzero cancels the running call
+ * with KG_CANCELLED. Replaces RunControl::check (crates/kyto-exec/src/run_control.rs,
+ * called at neighbors_gpu.rs:95). NULL clears it. */
+KG_API kg_status kg_set_cancel_flag(kg_ctx* ctx, const volatile int32_t* flag);
+
+/* Work done / total of the running or last call, in cells (all passes counted), as
+ * RunControl::progress. */
+KG_API kg_status kg_progress(const kg_ctx* ctx, uint64_t* done, uint64_t* total);
+
+/* ---------------------------------------------------------------- maps ------------ */
+
+/* normalize_total(target_sum) then log1p of one CSR block, into out (nnz f32):
+ * total = the row's values summed in f64 (8 lanes, kyto's fixed tree), divisor =
+ * f32(total) / f32(target_sum) (0 -> 1), value = f32(v) / divisor (IEEE f32
+ * division), log1p = f32(log1p(f64(v))). target_sum NaN skips normalize_total;
+ * log1p 0 skips log1p. Replaces DeviceKernels::{row_sums, divide_rows, log1p}
+ * (crates/kyto-gpu/src/launch.rs:106-173) as kyto-exec/src/elementwise.rs:205-235
+ * calls them. */
+KG_API kg_status kg_normalize_log1p(kg_ctx* ctx, const uint64_t* indptr, const void* values,
+                             kg_dtype dtype, uint64_t n_rows, double target_sum,
+                             int32_t log1p, float* out);
+
+/* The seurat statistics pass of highly_variable_genes over one CSR block, with
+ * normalize_total/log1p (as kg_normalize_log1p) fused in: per gene sum of
+ * t = f32(expm1(f64(x))), sum of f32(t*t) (both f64) and the cells with x > 0.
+ * Replaces HvgAccumulator::fold_rows (crates/kyto-exec/src/hvg_pass.rs:157-219).
+ * Each gene's sums add its cells in cell order (the bits of one kyto leaf). */
+KG_API kg_status kg_hvg_moments(kg_ctx* ctx, const uint64_t* indptr, const uint32_t* indices,
+                         const void* values, kg_dtype dtype, uint64_t n_rows,
+                         uint32_t n_genes, double target_sum, int32_t log1p,
+                         double* sums, double* sums_of_squares, uint64_t* positives);
+
+/* seurat flags from the moments (host arithmetic on n_genes values, as kyto runs it on
+ * the host): crates/kyto-exec/src/hvg.rs:284-361,393-437,501-580. n_top_genes < 0
+ * uses scanpy's mean/dispersion cutoffs. Outputs are host arrays of n_genes. */
+KG_API kg_status kg_hvg_seurat(const double* sums, const double* sums_of_squares,
+                        const uint64_t* positives, uint64_t n_cells, uint32_t n_genes,
+                        int64_t n_top_genes, double* means, double* dispersions,
+                        double* dispersions_norm, uint8_t* highly_variable);
+
+/* ---------------------------------------------------------------- PCA ------------- */
+
+typedef struct kg_pca_params {
+  uint32_t n_components;     /* k (kyto: pca(n_components=...)) */
+  uint32_t n_genes;          /* genes of the pushed blocks (the stream's genes) */
+  uint64_t seed;             /* kyto: pca(seed=...), drives Omega (pca.rs:936-950) */
+  const uint32_t* gene_map;  /* NULL: every gene; else n_genes entries, the gene's
+                                position among the PCA's genes or 0xFFFFFFFF to skip
+                                it (pca.rs:352-372: pca(genes=...) / HVG selection) */
+  double target_sum;         /* normalize_total before the PCA; NaN: none */
+  int32_t log1p;             /* nonzero: log1p after normalize_total */
+  uint32_t reserved;
+} kg_pca_params;
+
+/* Start a PCA session (kyto's PcaAccumulator::new, pca.rs:343-403). */
+KG_API kg_status kg_pca_begin(kg_ctx* ctx, const kg_pca_params* params, kg_pca** out);
+
+/* Push the next block of cells in stream order (kyto's store cell blocks). The block
+ * is copied to the device, normalized/log1p'd/gene-selected there in one kernel and
+ * held in HBM for every pass (kyto's held input, held_input.rs). cells: each row's
+ * table position (Omega's seed input); NULL numbers the rows on from the last
+ * block. */
+KG_API kg_status kg_pca_push_block(kg_pca* pca, const uint64_t* indptr, const uint32_t* indices,
+                            const void* values, kg_dtype dtype, uint64_t n_rows,
+                            const uint64_t* cells);
+
+/* Run all passes on the device (pass 0 sketch, 9 Krylov products, the embedding pass)
+ * with the FP64 orthonormalisation and Rayleigh-Ritz steps between them. Replaces
+ * the folds of pca/gpu.rs:149-219 and PcaAccumulator::end_pass (pca.rs:699-801). */
+KG_API kg_status kg_pca_run(kg_pca* pca);
+
+/* Results (kyto's PcaStatistics, pca.rs:804-845): embedding n_cells x k f32 (row-major,
+ * cell order), loadings n_genes x k f32 (zeros outside the gene set), variance and
+ * variance_ratio k f64, means (one per PCA gene) f64. Any pointer may be NULL. */
+KG_API kg_status kg_pca_results(kg_pca* pca, float* embedding, float* loadings, double* variance,
+                         double* variance_ratio, double* means);
+
+/* Sizes after run: cells pushed, PCA genes, passes run (fewer than 11 when the basis
+ * spans the data early). */
+KG_API kg_status kg_pca_info(const kg_pca* pca, uint64_t* n_cells, uint32_t* n_pca_genes,
+                      uint32_t* passes_run);
+
+/* The device address of the f32 embedding (n_cells x k) after run, valid until
+ * kg_pca_free: lets kg_knn_exact search it without a host round trip. */
+KG_API kg_status kg_pca_embedding_device(const kg_pca* pca, const float** out);
+
+KG_API void kg_pca_free(kg_pca* pca);
+
+/* ---------------------------------------------------------------- exact kNN ------- */
+
+typedef struct kg_knn_stats {
+  uint64_t candidates;     /* approximate candidates ranked by their exact keys */
+  uint64_t rows_full;      /* rows searched against every row (filter could not prove
+                              its candidates complete) */
+  double filter_ms;        /* device time of the candidate filter */
+  double rank_ms;          /* device time of the exact re-rank (and full rows) */
+} kg_knn_stats;
+
+/* Each row's n_neighbors - 1 nearest other rows of `embedding` (n_rows x width f32,
+ * row-major; the first n_components used, 0 = all) by kyto's exact key (the f64 sum of
+ * squared f64 differences in kyto's 8-lane order), ties to the lower row, the row
+ * itself excluded by position. Output: kyto's NeighborGraph CSR (neighbors.rs:412-435):
+ * indptr n_rows+1 (u64), indices and distances n_rows*(n_neighbors-1), each row's
+ * columns increasing, distance f32(sqrt(key)). The same graph as kyto's CPU exact
+ * search (neighbors_exact.rs:50-356) bit for bit. Replaces neighbors_gpu::exact +
+ * DeviceKernels::nearest_keys (neighbors_gpu.rs:70-127, launch_matrix.rs:253-287). */
+KG_API kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t n_rows,
+                       uint32_t width, uint32_t n_components, uint32_t n_neighbors,
+                       uint64_t* indptr, uint32_t* indices, float* distances,
+                       kg_knn_stats* stats);
+
+/* ---------------------------------------------------------------- diagnostics ----- */
+
+/* Kernels of this library launched since it was loaded (library calls such as cuBLAS
+ * not counted): lets a benchmark state how many of its own kernels a timed region ran.
+ * No counterpart in kyto (diagnostics only). */
+KG_API kg_status kg_diag_kernel_launches(uint64_t* count);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KYTO_GPU_H */

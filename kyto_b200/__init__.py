@@ -1,0 +1,378 @@
+"""kyto_b200: kyto's PCA -> exact-kNN hot path on a B200, behind a C ABI.
+
+The compute lives in ``libkyto_gpu.so`` (CUDA for sm_100a, C ABI in
+``include/kyto_gpu.h``). This module is the host-side mirror of kyto's operator
+interface for the path (kyto's ``Atlas.pca`` / ``Atlas.neighbors``, crates/kyto-py/src/
+atlas.rs:823-966, over ``kyto_gpu::DeviceKernels``): the same argument names and
+meanings, errors raised with kyto's codes. There is no CPU fallback: without the built
+library or a CUDA device every call raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libkyto_gpu.so"
+
+KG_OK, KG_ERR_INVALID, KG_ERR_DEVICE, KG_ERR_OOM, KG_CANCELLED, KG_ERR_TIMEOUT, KG_ERR_STATE = range(7)
+KG_U32, KG_F32 = 0, 1
+NO_GENE = 0xFFFFFFFF
+
+# kyto's error registry (errors.toml): the status a call returns -> kyto's code.
+KYTO_CODE = {
+    KG_ERR_INVALID: "KY-E215",
+    KG_ERR_DEVICE: "KY-E505",
+    KG_ERR_OOM: "KY-E505",
+    KG_CANCELLED: "KY-E503",
+    KG_ERR_TIMEOUT: "KY-E505",
+    KG_ERR_STATE: "KY-E505",
+}
+
+# Every entry point of include/kyto_gpu.h.
+EXPORTS = (
+    "kg_open", "kg_close", "kg_last_error", "kg_set_cancel_flag", "kg_progress",
+    "kg_normalize_log1p", "kg_hvg_moments", "kg_hvg_seurat",
+    "kg_pca_begin", "kg_pca_push_block", "kg_pca_run", "kg_pca_results", "kg_pca_info",
+    "kg_pca_embedding_device", "kg_pca_free", "kg_knn_exact", "kg_diag_kernel_launches",
+)
+
+
+class KytoError(RuntimeError):
+    """A failed call: ``code`` is kyto's error code, ``status`` the C ABI's."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        self.code = KYTO_CODE.get(status, "KY-E505")
+        super().__init__(f"{self.code}: {message}")
+
+
+class _PcaParams(ctypes.Structure):
+    _fields_ = [
+        ("n_components", ctypes.c_uint32),
+        ("n_genes", ctypes.c_uint32),
+        ("seed", ctypes.c_uint64),
+        ("gene_map", ctypes.c_void_p),
+        ("target_sum", ctypes.c_double),
+        ("log1p", ctypes.c_int32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
+class KnnStats(ctypes.Structure):
+    _fields_ = [
+        ("candidates", ctypes.c_uint64),
+        ("rows_full", ctypes.c_uint64),
+        ("filter_ms", ctypes.c_double),
+        ("rank_ms", ctypes.c_double),
+    ]
+
+
+_lib = None
+
+
+def library() -> ctypes.CDLL:
+    """The loaded ``libkyto_gpu.so``; raises if it was not built."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise KytoError(KG_ERR_DEVICE, f"{LIB_PATH} is missing: run `python -m kyto_b200.build`")
+        lib = ctypes.CDLL(str(LIB_PATH))
+        P, U64, U32, I32 = ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int32
+        sig = {
+            "kg_open": [ctypes.c_int, ctypes.POINTER(P)],
+            "kg_last_error": [P, ctypes.c_char_p, ctypes.c_size_t],
+            "kg_set_cancel_flag": [P, P],
+            "kg_progress": [P, P, P],
+            "kg_normalize_log1p": [P, P, P, ctypes.c_int, U64, ctypes.c_double, I32, P],
+            "kg_hvg_moments": [P, P, P, P, ctypes.c_int, U64, U32, ctypes.c_double, I32, P, P, P],
+            "kg_hvg_seurat": [P, P, P, U64, U32, ctypes.c_int64, P, P, P, P],
+            "kg_pca_begin": [P, ctypes.POINTER(_PcaParams), ctypes.POINTER(P)],
+            "kg_pca_push_block": [P, P, P, P, ctypes.c_int, U64, P],
+            "kg_pca_run": [P],
+            "kg_pca_results": [P, P, P, P, P, P],
+            "kg_pca_info": [P, P, P, P],
+            "kg_pca_embedding_device": [P, ctypes.POINTER(P)],
+            "kg_knn_exact": [P, P, U64, U32, U32, U32, P, P, P, ctypes.POINTER(KnnStats)],
+            "kg_diag_kernel_launches": [P],
+        }
+        for name, args in sig.items():
+            fn = getattr(lib, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        lib.kg_close.argtypes = [P]
+        lib.kg_close.restype = None
+        lib.kg_pca_free.argtypes = [P]
+        lib.kg_pca_free.restype = None
+        lib.kg_last_error.restype = ctypes.c_size_t
+        _lib = lib
+    return _lib
+
+
+def _check(status: int) -> None:
+    if status != KG_OK:
+        buf = ctypes.create_string_buffer(4096)
+        library().kg_last_error(None, buf, len(buf))
+        raise KytoError(status, buf.value.decode(errors="replace"))
+
+
+def _ptr(a):
+    """A numpy array's data pointer, a torch tensor's (host or CUDA), or None."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data_as(ctypes.c_void_p)
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    raise TypeError(f"not an array: {type(a)}")
+
+
+class Context:
+    """An open device (kg_open); closes itself when collected or on ``close()``."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        _check(library().kg_open(int(device), ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            library().kg_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_cancel_flag(self, flag: np.ndarray | None) -> None:
+        _check(library().kg_set_cancel_flag(self._h, _ptr(flag)))
+
+    def progress(self) -> tuple[int, int]:
+        done, total = ctypes.c_uint64(), ctypes.c_uint64()
+        _check(library().kg_progress(self._h, ctypes.byref(done), ctypes.byref(total)))
+        return done.value, total.value
+
+
+_default: Context | None = None
+
+
+def default_context() -> Context:
+    global _default
+    if _default is None:
+        _default = Context(0)
+    return _default
+
+
+def _dtype_code(values) -> int:
+    dt = values.dtype if isinstance(values, np.ndarray) else values.dtype
+    name = str(dt)
+    if name in ("uint32", "torch.uint32", "torch.int32", "int32"):
+        return KG_U32
+    if name in ("float32", "torch.float32"):
+        return KG_F32
+    raise TypeError(f"values must be uint32 counts or float32 values, not {name}")
+
+
+def _u64(a):
+    return np.ascontiguousarray(a, dtype=np.uint64) if isinstance(a, np.ndarray) else a
+
+
+def _u32(a):
+    return np.ascontiguousarray(a, dtype=np.uint32) if isinstance(a, np.ndarray) else a
+
+
+def kernel_launches() -> int:
+    """Kernels this library has launched since it was loaded."""
+    c = ctypes.c_uint64()
+    _check(library().kg_diag_kernel_launches(ctypes.byref(c)))
+    return c.value
+
+
+# ------------------------------------------------------------------ maps -------------
+def normalize_log1p(indptr, values, target_sum: float | None = 1e4, log1p: bool = True,
+                    ctx: Context | None = None) -> np.ndarray:
+    """normalize_total(target_sum) then log1p of a CSR block's values (f32, one per
+    stored value). ``target_sum=None`` skips normalize_total."""
+    ctx = ctx or default_context()
+    indptr = _u64(indptr)
+    n_rows = len(indptr) - 1
+    out = np.empty(int(indptr[-1]), dtype=np.float32)
+    _check(library().kg_normalize_log1p(
+        ctx.handle, _ptr(indptr), _ptr(values), _dtype_code(values), n_rows,
+        math.nan if target_sum is None else float(target_sum), int(bool(log1p)), _ptr(out)))
+    return out
+
+
+@dataclass
+class HvgResult:
+    means: np.ndarray
+    dispersions: np.ndarray
+    dispersions_norm: np.ndarray
+    highly_variable: np.ndarray
+
+
+def highly_variable_genes(indptr, indices, values, n_genes: int, n_top_genes: int | None = 2000,
+                          target_sum: float | None = 1e4, log1p: bool = True,
+                          ctx: Context | None = None) -> HvgResult:
+    """kyto's ``highly_variable_genes(flavor="seurat")`` on the log1p of normalized
+    counts: the statistics pass on the device, the flags on the host."""
+    ctx = ctx or default_context()
+    indptr, indices = _u64(indptr), _u32(indices)
+    n_rows = len(indptr) - 1
+    sums = np.empty(n_genes)
+    squares = np.empty(n_genes)
+    positives = np.empty(n_genes, dtype=np.uint64)
+    L = library()
+    _check(L.kg_hvg_moments(
+        ctx.handle, _ptr(indptr), _ptr(indices), _ptr(values), _dtype_code(values), n_rows,
+        int(n_genes), math.nan if target_sum is None else float(target_sum), int(bool(log1p)),
+        _ptr(sums), _ptr(squares), _ptr(positives)))
+    means, disp, norm = np.empty(n_genes), np.empty(n_genes), np.empty(n_genes)
+    flags = np.empty(n_genes, dtype=np.uint8)
+    _check(L.kg_hvg_seurat(
+        _ptr(sums), _ptr(squares), _ptr(positives), n_rows, int(n_genes),
+        -1 if n_top_genes is None else int(n_top_genes), _ptr(means), _ptr(disp), _ptr(norm),
+        _ptr(flags)))
+    return HvgResult(means, disp, norm, flags.astype(bool))
+
+
+# ------------------------------------------------------------------ PCA --------------
+@dataclass
+class PcaResult:
+    """kyto's PcaStatistics (crates/kyto-exec/src/pca.rs:51-120)."""
+
+    embedding: np.ndarray
+    loadings: np.ndarray
+    variance: np.ndarray
+    variance_ratio: np.ndarray
+    means: np.ndarray
+    passes_run: int
+
+
+class PcaSession:
+    """One ``pca`` node: push the blocks in stream order, run, read the results."""
+
+    def __init__(self, n_components: int, n_genes: int, seed: int = 0,
+                 gene_set: np.ndarray | None = None, target_sum: float | None = None,
+                 log1p: bool = False, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self._map = None
+        if gene_set is not None:
+            flags = np.asarray(gene_set, dtype=bool)
+            if flags.shape != (n_genes,):
+                raise KytoError(KG_ERR_INVALID, "gene_set must flag every gene")
+            self._map = np.full(n_genes, NO_GENE, dtype=np.uint32)
+            self._map[flags] = np.arange(int(flags.sum()), dtype=np.uint32)
+        p = _PcaParams(int(n_components), int(n_genes), int(seed),
+                       None if self._map is None else self._map.ctypes.data,
+                       math.nan if target_sum is None else float(target_sum),
+                       int(bool(log1p)), 0)
+        h = ctypes.c_void_p()
+        _check(library().kg_pca_begin(self.ctx.handle, ctypes.byref(p), ctypes.byref(h)))
+        self._h = h
+        self.n_components = int(n_components)
+        self.n_genes = int(n_genes)
+
+    def push(self, indptr, indices, values, cells=None) -> None:
+        indptr, indices = _u64(indptr), _u32(indices)
+        n_rows = (len(indptr) if isinstance(indptr, np.ndarray) else indptr.shape[0]) - 1
+        _check(library().kg_pca_push_block(
+            self._h, _ptr(indptr), _ptr(indices), _ptr(values), _dtype_code(values), n_rows,
+            _ptr(_u64(cells) if cells is not None else None)))
+
+    def run(self) -> None:
+        _check(library().kg_pca_run(self._h))
+
+    def info(self) -> tuple[int, int, int]:
+        n, g, p = ctypes.c_uint64(), ctypes.c_uint32(), ctypes.c_uint32()
+        _check(library().kg_pca_info(self._h, ctypes.byref(n), ctypes.byref(g), ctypes.byref(p)))
+        return n.value, g.value, p.value
+
+    def embedding_device_ptr(self) -> int:
+        out = ctypes.c_void_p()
+        _check(library().kg_pca_embedding_device(self._h, ctypes.byref(out)))
+        return out.value
+
+    def results(self) -> PcaResult:
+        n, g, passes = self.info()
+        k = self.n_components
+        emb = np.empty((n, k), dtype=np.float32)
+        load = np.empty((self.n_genes, k), dtype=np.float32)
+        var, ratio, means = np.empty(k), np.empty(k), np.empty(g)
+        _check(library().kg_pca_results(self._h, _ptr(emb), _ptr(load), _ptr(var),
+                                        _ptr(ratio), _ptr(means)))
+        return PcaResult(emb, load, var, ratio, means, passes)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            library().kg_pca_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def pca(indptr, indices, values, n_genes: int, n_components: int = 50, seed: int = 0,
+        gene_set: np.ndarray | None = None, target_sum: float | None = None,
+        log1p: bool = False, block_cells: int | None = None,
+        ctx: Context | None = None) -> PcaResult:
+    """kyto's ``pca(n_components, seed, genes=...)`` on a CSR matrix (optionally after
+    normalize_total/log1p), pushed in blocks of ``block_cells`` cells."""
+    sess = PcaSession(n_components, n_genes, seed, gene_set, target_sum, log1p, ctx)
+    indptr = np.ascontiguousarray(indptr, dtype=np.uint64)
+    n = len(indptr) - 1
+    step = n if not block_cells else int(block_cells)
+    for a in range(0, n, max(step, 1)):
+        b = min(n, a + step)
+        s, e = int(indptr[a]), int(indptr[b])
+        sess.push(indptr[a:b + 1] - np.uint64(s), indices[s:e], values[s:e],
+                  np.arange(a, b, dtype=np.uint64))
+    sess.run()
+    res = sess.results()
+    sess.close()
+    return res
+
+
+# ------------------------------------------------------------------ neighbors --------
+@dataclass
+class Graph:
+    """kyto's NeighborGraph: k = n_neighbors - 1 entries a row, columns increasing
+    within a row, f32 distances."""
+
+    indptr: np.ndarray
+    indices: np.ndarray
+    distances: np.ndarray
+    stats: KnnStats | None = None
+
+
+def neighbors(embedding, n_neighbors: int = 15, n_components: int | None = None,
+              ctx: Context | None = None) -> Graph:
+    """kyto's exact ``neighbors(n_neighbors, n_components, metric="euclidean")``."""
+    ctx = ctx or default_context()
+    if isinstance(embedding, np.ndarray):
+        embedding = np.ascontiguousarray(embedding, dtype=np.float32)
+    n, width = embedding.shape
+    k = int(n_neighbors) - 1
+    indptr = np.empty(n + 1, dtype=np.uint64)
+    indices = np.empty(max(n * k, 0), dtype=np.uint32)
+    dist = np.empty(max(n * k, 0), dtype=np.float32)
+    stats = KnnStats()
+    _check(library().kg_knn_exact(ctx.handle, _ptr(embedding), n, width,
+                                  0 if n_components is None else int(n_components),
+                                  int(n_neighbors), _ptr(indptr), _ptr(indices), _ptr(dist),
+                                  ctypes.byref(stats)))
+    return Graph(indptr, indices, dist, stats)

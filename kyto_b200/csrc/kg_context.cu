@@ -1,0 +1,95 @@
+// The context entry points of the C ABI: open/close, errors, cancel flag, progress.
+#include "kg_internal.cuh"
+
+namespace kg {
+std::atomic<uint64_t> g_launches{0};
+
+std::string& last_error() {
+  thread_local std::string message;
+  return message;
+}
+}  // namespace kg
+
+extern "C" {
+
+kg_status kg_open(int device, kg_ctx** out) {
+  return kg::guarded([&] {
+    if (!out) kg::fail(KG_ERR_INVALID, "kg_open: out is NULL");
+    *out = nullptr;
+    int n = 0;
+    KG_CUDA(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n)
+      kg::fail(KG_ERR_INVALID, "kg_open: device " + std::to_string(device) +
+                                   " does not exist (" + std::to_string(n) + " found)");
+    KG_CUDA(cudaSetDevice(device));
+    cudaDeviceProp prop{};
+    KG_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major < 10)
+      kg::fail(KG_ERR_INVALID, std::string("kg_open: ") + prop.name +
+                                   " is not a Blackwell (sm_100a) device");
+    auto* ctx = new kg_ctx();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    try {
+      KG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+      KG_CUBLAS(cublasCreate(&ctx->cublas));
+      KG_CUSOLVER(cusolverDnCreate(&ctx->cusolver));
+      // Pool memory stays with the pool between calls (no release to the OS).
+      cudaMemPool_t pool;
+      KG_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+      uint64_t threshold = UINT64_MAX;
+      KG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    } catch (...) {
+      if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
+      if (ctx->cublas) cublasDestroy(ctx->cublas);
+      if (ctx->stream) cudaStreamDestroy(ctx->stream);
+      delete ctx;
+      throw;
+    }
+    *out = ctx;
+  });
+}
+
+void kg_close(kg_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
+  if (ctx->cublas) cublasDestroy(ctx->cublas);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+size_t kg_last_error(const kg_ctx*, char* buf, size_t len) {
+  const std::string& m = kg::last_error();
+  if (buf && len) {
+    size_t n = m.size() < len - 1 ? m.size() : len - 1;
+    std::memcpy(buf, m.data(), n);
+    buf[n] = '\0';
+  }
+  return m.size();
+}
+
+kg_status kg_set_cancel_flag(kg_ctx* ctx, const volatile int32_t* flag) {
+  return kg::guarded([&] {
+    if (!ctx) kg::fail(KG_ERR_INVALID, "kg_set_cancel_flag: ctx is NULL");
+    ctx->cancel = flag;
+  });
+}
+
+kg_status kg_progress(const kg_ctx* ctx, uint64_t* done, uint64_t* total) {
+  return kg::guarded([&] {
+    if (!ctx) kg::fail(KG_ERR_INVALID, "kg_progress: ctx is NULL");
+    if (done) *done = ctx->done.load();
+    if (total) *total = ctx->total.load();
+  });
+}
+
+kg_status kg_diag_kernel_launches(uint64_t* count) {
+  return kg::guarded([&] {
+    if (!count) kg::fail(KG_ERR_INVALID, "kg_diag_kernel_launches: count is NULL");
+    *count = kg::g_launches.load();
+  });
+}
+
+}  // extern "C"

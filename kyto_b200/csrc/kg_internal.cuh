@@ -1,0 +1,221 @@
+// Internal helpers of libkyto_gpu.so: errors, the context, device buffers, bounded
+// waits. Nothing here crosses the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cublas_v2.h>
+#include <cusolverDn.h>
+
+#include <atomic>
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <utility>
+
+#include "kyto_gpu.h"
+
+namespace kg {
+
+// An error inside the library: the status the entry point returns, and its message.
+struct Error {
+  kg_status status;
+  std::string message;
+};
+
+[[noreturn]] inline void fail(kg_status status, std::string message) {
+  throw Error{status, std::move(message)};
+}
+
+[[noreturn]] inline void fail_cuda(cudaError_t e, const char* what, const char* file,
+                                   int line) {
+  kg_status s = (e == cudaErrorMemoryAllocation) ? KG_ERR_OOM : KG_ERR_DEVICE;
+  std::string msg = std::string("CUDA error ") + cudaGetErrorName(e) + " (" +
+                    cudaGetErrorString(e) + ") in " + what + " at " + file + ":" +
+                    std::to_string(line);
+  if (s == KG_ERR_OOM) msg += "; the device ran out of memory: lower memory_limit";
+  fail(s, msg);
+}
+
+#define KG_CUDA(call)                                                   \
+  do {                                                                  \
+    cudaError_t kg_e_ = (call);                                         \
+    if (kg_e_ != cudaSuccess) ::kg::fail_cuda(kg_e_, #call, __FILE__, __LINE__); \
+  } while (0)
+
+#define KG_CUBLAS(call)                                                            \
+  do {                                                                             \
+    cublasStatus_t kg_s_ = (call);                                                 \
+    if (kg_s_ != CUBLAS_STATUS_SUCCESS)                                            \
+      ::kg::fail(KG_ERR_DEVICE, std::string("cuBLAS status ") +                    \
+                                    std::to_string((int)kg_s_) + " in " #call);    \
+  } while (0)
+
+#define KG_CUSOLVER(call)                                                          \
+  do {                                                                             \
+    cusolverStatus_t kg_s_ = (call);                                               \
+    if (kg_s_ != CUSOLVER_STATUS_SUCCESS)                                          \
+      ::kg::fail(KG_ERR_DEVICE, std::string("cuSOLVER status ") +                  \
+                                    std::to_string((int)kg_s_) + " in " #call);    \
+  } while (0)
+
+// Kernels of this library launched so far (kg_diag_kernel_launches); every launch
+// site is followed by KG_LAUNCH_CHECK.
+extern std::atomic<uint64_t> g_launches;
+
+#define KG_LAUNCH_CHECK()                        \
+  do {                                           \
+    ::kg::g_launches.fetch_add(1, std::memory_order_relaxed); \
+    KG_CUDA(cudaGetLastError());                 \
+  } while (0)
+
+// The calling thread's last error message (kg_last_error).
+std::string& last_error();
+
+// A device allocation, stream-ordered (cudaMallocAsync / cudaFreeAsync).
+template <class T>
+struct DeviceBuffer {
+  T* ptr = nullptr;
+  size_t count = 0;
+  cudaStream_t stream = nullptr;
+
+  DeviceBuffer() = default;
+  DeviceBuffer(size_t n, cudaStream_t s) { alloc(n, s); }
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  DeviceBuffer(DeviceBuffer&& o) noexcept { swap(o); }
+  DeviceBuffer& operator=(DeviceBuffer&& o) noexcept {
+    reset();
+    swap(o);
+    return *this;
+  }
+  ~DeviceBuffer() { reset(); }
+
+  void swap(DeviceBuffer& o) noexcept {
+    std::swap(ptr, o.ptr);
+    std::swap(count, o.count);
+    std::swap(stream, o.stream);
+  }
+  void alloc(size_t n, cudaStream_t s) {
+    reset();
+    stream = s;
+    count = n;
+    if (n) KG_CUDA(cudaMallocAsync((void**)&ptr, n * sizeof(T), s));
+  }
+  void reset() noexcept {
+    if (ptr) cudaFreeAsync(ptr, stream);
+    ptr = nullptr;
+    count = 0;
+  }
+  void zero() {
+    if (count) KG_CUDA(cudaMemsetAsync(ptr, 0, count * sizeof(T), stream));
+  }
+  T* get() const { return ptr; }
+  size_t bytes() const { return count * sizeof(T); }
+};
+
+// Whether p is memory the device can read directly (device or managed).
+inline bool is_device_pointer(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a{};
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// `count` elements at `src` (host or device) as a device pointer: src itself when the
+// device can read it, else a copy in `holder`.
+template <class T>
+const T* device_view(const T* src, size_t count, DeviceBuffer<T>& holder,
+                     cudaStream_t stream) {
+  if (is_device_pointer(src)) return src;
+  holder.alloc(count, stream);
+  if (count)
+    KG_CUDA(cudaMemcpyAsync(holder.ptr, src, count * sizeof(T), cudaMemcpyHostToDevice,
+                            stream));
+  return holder.ptr;
+}
+
+}  // namespace kg
+
+// The context behind the C ABI's kg_ctx.
+struct kg_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cublasHandle_t cublas = nullptr;
+  cusolverDnHandle_t cusolver = nullptr;
+  std::mutex handles;  // cuBLAS/cuSOLVER handles are bound to one stream at a time
+  const volatile int32_t* cancel = nullptr;
+  std::atomic<uint64_t> done{0}, total{0};
+  int sm_count = 0;
+  // Seconds a bounded wait gives the device before KG_ERR_TIMEOUT.
+  double wait_limit_s = 900.0;
+};
+
+namespace kg {
+
+// Make ctx's device current for this thread.
+inline void use_device(kg_ctx* ctx) { KG_CUDA(cudaSetDevice(ctx->device)); }
+
+inline void check_cancel(const kg_ctx* ctx) {
+  if (ctx->cancel && *ctx->cancel) fail(KG_CANCELLED, "the run was cancelled");
+}
+
+// Wait for `stream` with a deadline: polls an event instead of blocking forever, so a
+// stuck device surfaces as KG_ERR_TIMEOUT, and the cancel flag is honoured meanwhile
+// (the work already queued still runs to its end before the call returns).
+inline void wait_stream(kg_ctx* ctx, cudaStream_t stream) {
+  cudaEvent_t ev;
+  KG_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  KG_CUDA(cudaEventRecord(ev, stream));
+  auto start = std::chrono::steady_clock::now();
+  int spins = 0;
+  for (;;) {
+    cudaError_t e = cudaEventQuery(ev);
+    if (e == cudaSuccess) break;
+    if (e != cudaErrorNotReady) {
+      cudaEventDestroy(ev);
+      fail_cuda(e, "cudaEventQuery (a kernel failed)", __FILE__, __LINE__);
+    }
+    double waited =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+    if (waited > ctx->wait_limit_s) {
+      cudaEventDestroy(ev);
+      fail(KG_ERR_TIMEOUT, "the device did not finish within the wait limit");
+    }
+    if (++spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(50));
+  }
+  cudaEventDestroy(ev);
+}
+
+template <class F>
+kg_status guarded(F&& body) {
+  try {
+    body();
+    return KG_OK;
+  } catch (const Error& e) {
+    last_error() = e.message;
+    return e.status;
+  } catch (const std::bad_alloc&) {
+    last_error() = "host memory exhausted";
+    return KG_ERR_OOM;
+  } catch (const std::exception& e) {
+    last_error() = e.what();
+    return KG_ERR_DEVICE;
+  } catch (...) {
+    last_error() = "unknown error";
+    return KG_ERR_DEVICE;
+  }
+}
+
+inline unsigned blocks_for(uint64_t n, unsigned per_block) {
+  uint64_t b = (n + per_block - 1) / per_block;
+  return (unsigned)(b ? b : 1);
+}
+
+}  // namespace kg

@@ -1,0 +1,550 @@
+// Exact Euclidean kNN (kyto's neighbors.rs + neighbors_exact.rs) on the device.
+//
+// Three steps, each one kernel family:
+//  1. filter: every query against every point by an approximate key with a proven
+//     error bound; each query keeps its k smallest approximate keys and every point
+//     whose approximate key is at most the k-th plus twice its slack (kyto's
+//     neighbors_exact.rs:50-356 algorithm, one query per thread, the point tile in
+//     shared memory);
+//  2. rank: the candidates' exact keys (f64, kyto's 8-lane order, no FMA: the same bits
+//     as the CPU) ranked by (key, row); a row whose candidates are not proven complete
+//     (too many, or an approximate key outside its slack) is flagged;
+//  3. full rows: flagged rows searched against every row with exact keys.
+// So every row is the CPU's brute-force row, bit for bit.
+#include <cub/device/device_segmented_radix_sort.cuh>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <vector>
+
+#include "kg_internal.cuh"
+#include "kg_knn.cuh"
+
+namespace kg {
+
+// ------------------------------------------------------------------ prepare --------
+
+__global__ void finite_check_kernel(const float* x, uint64_t n, uint32_t width, uint32_t d,
+                                    unsigned long long* first_bad) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n * d;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t r = i / d, j = i % d;
+    if (!isfinite(x[r * width + j])) atomicMin(first_bad, (unsigned long long)(r * width + j));
+  }
+}
+
+// Column means in f64, columns summed in row order by one thread each (fixed order).
+__global__ void column_mean_kernel(const float* x, uint64_t n, uint32_t width, uint32_t d,
+                                   double* mean) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= d) return;
+  double s = 0.0;
+  for (uint64_t r = 0; r < n; ++r) s = __dadd_rn(s, (double)x[r * width + j]);
+  mean[j] = s / (double)n;
+}
+
+// Centred f32 rows padded to kDim (zeros), their f32 squared norms and f64 squares.
+__global__ void centre_kernel(const float* x, uint64_t n, uint32_t width, uint32_t d,
+                              const double* mean, float* rows, float* offsets,
+                              double* squares) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double s = 0.0;
+  for (uint32_t j = 0; j < kDim; ++j) {
+    float c = 0.0f;
+    if (j < d) c = (float)__dadd_rn((double)x[r * width + j], -mean[j]);
+    rows[r * kDim + j] = c;
+    s = __dadd_rn(s, __dmul_rn((double)c, (double)c));
+  }
+  squares[r] = s;
+  offsets[r] = (float)s;
+}
+
+__global__ void max_kernel(const double* v, uint64_t n, double* out) {
+  __shared__ double red[256];
+  double m = 0.0;
+  for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, v[i]);
+  red[threadIdx.x] = m;
+  __syncthreads();
+  for (unsigned s = blockDim.x / 2; s; s >>= 1) {
+    if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *out = red[0];
+}
+
+// kyto's slack E_q = 2 (w + 8) u (|a_q| + max |a|)^2 + 4 (w + 8) FLT_MIN
+// (neighbors_exact.rs:80-95, 114-136).
+__global__ void slack_kernel(const double* squares, uint64_t n, uint32_t d,
+                             const double* largest_sq, double* slack) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double u = 1.0 / 16777216.0;
+  double factor = 2.0 * ((double)d + 8.0) * u;
+  double underflow = 4.0 * ((double)d + 8.0) * (double)FLT_MIN;
+  double a = sqrt(squares[r]) + sqrt(*largest_sq);
+  slack[r] = factor * a * a + underflow;
+}
+
+// ------------------------------------------------------------------ filter ---------
+
+__device__ __forceinline__ float round_up_f32(double v) {
+  float r = (float)v;
+  if ((double)r < v) r = nextafterf(r, INFINITY);
+  return r;
+}
+
+// One thread per query: its centred row in registers, point tiles of kTile rows
+// staged in shared memory. Each query's k smallest approximate keys live in local
+// memory; candidates go to its own slice of the candidate buffer (kyto's Query::offer,
+// neighbors_exact.rs:216-255), compacted against the falling threshold when full.
+__global__ void __launch_bounds__(kFilterThreads)
+filter_kernel(const float* __restrict__ rows, const float* __restrict__ offsets,
+              const double* __restrict__ slack, uint64_t n, uint64_t q_begin,
+              uint64_t q_end, uint32_t k, uint32_t cap, float* cand_key, uint32_t* cand_row,
+              uint32_t* cand_count, float* threshold_out) {
+  __shared__ float tile[kTile * kDim];
+  __shared__ float tile_off[kTile];
+  uint64_t q = q_begin + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  bool active = q < q_end;
+  float qv[kDim];
+#pragma unroll
+  for (int j = 0; j < kDim; ++j) qv[j] = active ? rows[q * kDim + j] : 0.0f;
+  float off_q = active ? offsets[q] : 0.0f;
+  double sl = active ? slack[q] : 0.0;
+  float smallest[kMaxK];
+  uint32_t n_small = 0;
+  float threshold = INFINITY;
+  uint64_t slot = (q - q_begin) * (uint64_t)cap;
+  uint32_t count = 0, compact_at = 64;
+  bool overflowed = false;
+  for (uint64_t p0 = 0; p0 < n; p0 += kTile) {
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < kTile * kDim; i += blockDim.x) {
+      uint64_t p = p0 + i / kDim;
+      tile[i] = p < n ? rows[p0 * kDim + i] : 0.0f;
+    }
+    for (uint32_t i = threadIdx.x; i < kTile; i += blockDim.x)
+      tile_off[i] = p0 + i < n ? offsets[p0 + i] : INFINITY;
+    __syncthreads();
+    if (!active || overflowed) continue;
+    uint32_t span = (uint32_t)((n - p0) < kTile ? (n - p0) : kTile);
+    for (uint32_t c = 0; c < span; ++c) {
+      const float* pv = &tile[c * kDim];
+      float dot = 0.0f;
+#pragma unroll
+      for (int j = 0; j < kDim; ++j) dot = fmaf(qv[j], pv[j], dot);
+      float key = __fsub_rn(__fadd_rn(off_q, tile_off[c]), 2.0f * dot);
+      uint64_t p = p0 + c;
+      if (!(key <= threshold) || p == q) continue;
+      if (n_small < k || key < smallest[k - 1]) {
+        if (n_small < k) ++n_small;
+        uint32_t at = n_small - 1;
+        while (at > 0 && smallest[at - 1] > key) {
+          smallest[at] = smallest[at - 1];
+          --at;
+        }
+        smallest[at] = key;
+        if (n_small == k) threshold = round_up_f32((double)smallest[k - 1] + 2.0 * sl);
+      }
+      if (key <= threshold) {
+        if (count == cap) {
+          overflowed = true;
+          break;
+        }
+        cand_key[slot + count] = key;
+        cand_row[slot + count] = (uint32_t)p;
+        ++count;
+        if (count >= compact_at) {
+          uint32_t kept = 0;
+          for (uint32_t i = 0; i < count; ++i) {
+            float ck = cand_key[slot + i];
+            if (ck <= threshold) {
+              cand_key[slot + kept] = ck;
+              cand_row[slot + kept] = cand_row[slot + i];
+              ++kept;
+            }
+          }
+          count = kept;
+          if (count > kCandidateLimit) {
+            overflowed = true;
+            break;
+          }
+          compact_at = min(max(2 * count, 64u), cap);
+        }
+      }
+    }
+  }
+  if (active) {
+    cand_count[q - q_begin] = overflowed ? kOverflow : count;
+    threshold_out[q - q_begin] = threshold;
+  }
+}
+
+// ------------------------------------------------------------------ exact keys -----
+
+// kyto's exact key (kernels.rs:420-448): component j's difference and square in f64
+// into lane j % 8 (no FMA), the lanes combined by the fixed tree.
+__device__ __forceinline__ double exact_key(const float* a, const float* b, uint32_t d) {
+  double lanes[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (uint32_t j = 0; j < d; ++j) {
+    double diff = __dsub_rn((double)a[j], (double)b[j]);
+    lanes[j & 7] = __dadd_rn(lanes[j & 7], __dmul_rn(diff, diff));
+  }
+  double h0 = __dadd_rn(lanes[0], lanes[4]);
+  double h1 = __dadd_rn(lanes[1], lanes[5]);
+  double h2 = __dadd_rn(lanes[2], lanes[6]);
+  double h3 = __dadd_rn(lanes[3], lanes[7]);
+  return __dadd_rn(__dadd_rn(h0, h2), __dadd_rn(h1, h3));
+}
+
+__device__ __forceinline__ bool before(double ka, uint32_t ia, double kb, uint32_t ib) {
+  return ka < kb || (ka == kb && ia < ib);
+}
+
+// Offer (key, row) to a ranked list of at most k entries (kyto's Nearest::offer).
+__device__ __forceinline__ void offer(double* keys, uint32_t* idx, uint32_t& len, uint32_t k,
+                                      double key, uint32_t row) {
+  if (len == k) {
+    if (before(keys[k - 1], idx[k - 1], key, row)) return;
+    --len;
+  }
+  uint32_t at = len;
+  while (at > 0 && before(key, row, keys[at - 1], idx[at - 1])) {
+    keys[at] = keys[at - 1];
+    idx[at] = idx[at - 1];
+    --at;
+  }
+  keys[at] = key;
+  idx[at] = row;
+  ++len;
+}
+
+// Merge the warp's per-lane ranked lists into the first k of all: k rounds of a warp
+// arg-min over the lanes' heads.
+__device__ void warp_merge(const double* keys, const uint32_t* idx, uint32_t len, uint32_t k,
+                           double* out_key, uint32_t* out_row, uint32_t* out_len) {
+  unsigned lane = threadIdx.x & 31u;
+  uint32_t head = 0;
+  uint32_t produced = 0;
+  for (uint32_t r = 0; r < k; ++r) {
+    double hk = head < len ? keys[head] : INFINITY;
+    uint32_t hi = head < len ? idx[head] : 0xFFFFFFFFu;
+    bool has = head < len;
+    double bk = hk;
+    uint32_t bi = hi;
+    unsigned bl = has ? lane : 32u;
+    for (int o = 16; o; o >>= 1) {
+      double ok = __shfl_xor_sync(0xFFFFFFFFu, bk, o);
+      uint32_t oi = __shfl_xor_sync(0xFFFFFFFFu, bi, o);
+      unsigned ol = __shfl_xor_sync(0xFFFFFFFFu, bl, o);
+      bool take = (ol < 32u) && (bl == 32u || before(ok, oi, bk, bi));
+      if (take) {
+        bk = ok;
+        bi = oi;
+        bl = ol;
+      }
+    }
+    if (bl == 32u) break;
+    if (lane == bl) ++head;
+    if (lane == 0) {
+      out_key[r] = bk;
+      out_row[r] = bi;
+    }
+    ++produced;
+  }
+  if (lane == 0) *out_len = produced;
+}
+
+// One warp per query: exact keys of its candidates, the k best by (key, row). A row
+// that overflowed, holds fewer than k candidates or has a candidate outside its slack
+// is flagged for a full search (kyto's rank, neighbors_exact.rs:318-340).
+__global__ void rank_kernel(const float* __restrict__ x, uint32_t width, uint32_t d,
+                            uint64_t q_begin, uint64_t q_end, uint32_t k, uint32_t cap,
+                            const float* cand_key, const uint32_t* cand_row,
+                            const uint32_t* cand_count, const float* threshold,
+                            const double* slack, double* out_key, uint32_t* out_row,
+                            uint32_t* full_flag, unsigned long long* n_candidates) {
+  uint64_t qi = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  unsigned lane = threadIdx.x & 31u;
+  uint64_t q = q_begin + qi;
+  if (q >= q_end) return;
+  uint32_t count = cand_count[qi];
+  if (count == kOverflow) {
+    if (lane == 0) full_flag[q] = 1;
+    return;
+  }
+  float th = threshold[qi];
+  double sl = slack[q];
+  const float* qrow = x + q * width;
+  double keys[kMaxK];
+  uint32_t idx[kMaxK];
+  uint32_t len = 0;
+  bool bad = false;
+  uint32_t used = 0;
+  for (uint32_t c = lane; c < count; c += 32) {
+    float ak = cand_key[qi * (uint64_t)cap + c];
+    if (ak > th) continue;
+    uint32_t p = cand_row[qi * (uint64_t)cap + c];
+    double e = exact_key(qrow, x + (uint64_t)p * width, d);
+    if (fabs(e - (double)ak) > sl) bad = true;
+    offer(keys, idx, len, k, e, p);
+    ++used;
+  }
+  for (int o = 16; o; o >>= 1) used += __shfl_xor_sync(0xFFFFFFFFu, used, o);
+  bool any_bad = __any_sync(0xFFFFFFFFu, bad);
+  __shared__ uint32_t merged_len[kRankWarps];
+  unsigned w = threadIdx.x >> 5;
+  double* ok = out_key + q * (uint64_t)k;
+  uint32_t* orow = out_row + q * (uint64_t)k;
+  warp_merge(keys, idx, len, k, ok, orow, &merged_len[w]);
+  __syncwarp();
+  if (lane == 0) {
+    atomicAdd(n_candidates, (unsigned long long)used);
+    full_flag[q] = (any_bad || merged_len[w] != k) ? 1u : 0u;
+  }
+}
+
+// One CTA per flagged row: every other row's exact key, the k best by (key, row).
+__global__ void full_rows_kernel(const float* __restrict__ x, uint64_t n, uint32_t width,
+                                 uint32_t d, uint32_t k, const uint32_t* rows_list,
+                                 double* out_key, uint32_t* out_row) {
+  uint64_t q = rows_list[blockIdx.x];
+  const float* qrow = x + q * width;
+  double keys[kMaxK];
+  uint32_t idx[kMaxK];
+  uint32_t len = 0;
+  for (uint64_t p = threadIdx.x; p < n; p += blockDim.x) {
+    if (p == q) continue;
+    offer(keys, idx, len, k, exact_key(qrow, x + p * width, d), (uint32_t)p);
+  }
+  // Each warp merges its lanes; warp 0 then merges the warps' lists.
+  __shared__ double wkeys[kFullWarps][kMaxK];
+  __shared__ uint32_t wrow[kFullWarps][kMaxK];
+  __shared__ uint32_t wlen[kFullWarps];
+  unsigned w = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  warp_merge(keys, idx, len, k, wkeys[w], wrow[w], &wlen[w]);
+  __syncthreads();
+  if (w == 0) {
+    uint32_t l2 = 0;
+    if (lane < kFullWarps) {
+      for (uint32_t i = 0; i < wlen[lane]; ++i) {
+        keys[i] = wkeys[lane][i];
+        idx[i] = wrow[lane][i];
+      }
+      l2 = wlen[lane];
+    }
+    __shared__ uint32_t final_len;
+    warp_merge(keys, idx, l2, k, out_key + q * (uint64_t)k, out_row + q * (uint64_t)k,
+               &final_len);
+  }
+}
+
+// Each row's ranked entries sorted by row index, distances f32(sqrt(key))
+// (neighbors.rs:412-435).
+__global__ void graph_kernel(const double* keys, const uint32_t* rows, uint64_t n,
+                             uint32_t k, uint64_t* indptr, uint32_t* indices,
+                             float* distances) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r == 0) indptr[0] = 0;
+  if (r >= n) return;
+  indptr[r + 1] = (r + 1) * (uint64_t)k;
+  const double* kr = keys + r * k;
+  const uint32_t* rr = rows + r * k;
+  uint32_t* oi = indices + r * k;
+  float* od = distances + r * k;
+  // Insertion by row index (k is small; rows are distinct).
+  for (uint32_t i = 0; i < k; ++i) {
+    uint32_t row = rr[i];
+    float dist = (float)sqrt(kr[i]);
+    uint32_t at = i;
+    while (at > 0 && oi[at - 1] > row) {
+      oi[at] = oi[at - 1];
+      od[at] = od[at - 1];
+      --at;
+    }
+    oi[at] = row;
+    od[at] = dist;
+  }
+}
+
+__global__ void compact_flags_kernel(const uint32_t* flag, uint64_t n, uint32_t* list,
+                                     unsigned int* count) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r < n && flag[r]) list[atomicAdd(count, 1u)] = (uint32_t)r;
+}
+
+}  // namespace kg
+
+using namespace kg;
+
+namespace {
+
+struct Timer {
+  cudaEvent_t a, b;
+  cudaStream_t s;
+  explicit Timer(cudaStream_t st) : s(st) {
+    KG_CUDA(cudaEventCreate(&a));
+    KG_CUDA(cudaEventCreate(&b));
+    KG_CUDA(cudaEventRecord(a, s));
+  }
+  double stop_ms() {
+    KG_CUDA(cudaEventRecord(b, s));
+    KG_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    KG_CUDA(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms;
+  }
+};
+
+}  // namespace
+
+extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t n,
+                                  uint32_t width, uint32_t n_components,
+                                  uint32_t n_neighbors, uint64_t* indptr, uint32_t* indices,
+                                  float* distances, kg_knn_stats* stats) {
+  return guarded([&] {
+    if (!ctx || !embedding || !indptr || !indices || !distances)
+      fail(KG_ERR_INVALID, "kg_knn_exact: NULL argument");
+    if (width == 0) fail(KG_ERR_INVALID, "neighbors: an embedding of 0 components");
+    uint32_t d = n_components ? n_components : width;
+    if (d > width)
+      fail(KG_ERR_INVALID, "neighbors: n_components " + std::to_string(n_components) +
+                               " is more than the embedding's " + std::to_string(width));
+    if (d > (uint32_t)kDim)
+      fail(KG_ERR_INVALID, "neighbors: more than " + std::to_string(kDim) + " components");
+    if (n_neighbors < 2 || n_neighbors > n)
+      fail(KG_ERR_INVALID, "neighbors: n_neighbors " + std::to_string(n_neighbors) +
+                               " (it counts the cell itself; " + std::to_string(n) +
+                               " cells): an int from 2 to " + std::to_string(std::max<uint64_t>(n, 2)));
+    if (n - 1 >= (1ull << 32)) fail(KG_ERR_INVALID, "neighbors: at most 2^32 cells");
+    uint32_t k = n_neighbors - 1;
+    if (k > (uint32_t)kMaxK)
+      fail(KG_ERR_INVALID, "neighbors: n_neighbors above " + std::to_string(kMaxK + 1));
+    use_device(ctx);
+    cudaStream_t s = ctx->stream;
+    ctx->total = n;
+    ctx->done = 0;
+    DeviceBuffer<float> hold;
+    const float* x = device_view(embedding, n * width, hold, s);
+    // Finite values only (neighbors.rs:279-291).
+    {
+      DeviceBuffer<unsigned long long> bad(1, s);
+      unsigned long long init = ~0ull;
+      KG_CUDA(cudaMemcpyAsync(bad.ptr, &init, 8, cudaMemcpyHostToDevice, s));
+      finite_check_kernel<<<std::min<unsigned>(blocks_for(n * d, 256), 8192), 256, 0, s>>>(
+          x, n, width, d, bad.ptr);
+      KG_LAUNCH_CHECK();
+      unsigned long long first = 0;
+      KG_CUDA(cudaMemcpyAsync(&first, bad.ptr, 8, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaStreamSynchronize(s));
+      if (first != ~0ull)
+        fail(KG_ERR_INVALID, "neighbors: row " + std::to_string(first / width) +
+                                 ", component " + std::to_string(first % width) +
+                                 " is not finite");
+    }
+    DeviceBuffer<double> mean(d, s), squares(n, s), slack(n, s), largest(1, s);
+    DeviceBuffer<float> rows(n * kDim, s), offsets(n, s);
+    column_mean_kernel<<<blocks_for(d, 64), 64, 0, s>>>(x, n, width, d, mean.ptr);
+    centre_kernel<<<blocks_for(n, 128), 128, 0, s>>>(x, n, width, d, mean.ptr, rows.ptr,
+                                                     offsets.ptr, squares.ptr);
+    max_kernel<<<1, 256, 0, s>>>(squares.ptr, n, largest.ptr);
+    slack_kernel<<<blocks_for(n, 256), 256, 0, s>>>(squares.ptr, n, d, largest.ptr, slack.ptr);
+    KG_LAUNCH_CHECK();
+    double h_largest = 0;
+    KG_CUDA(cudaMemcpyAsync(&h_largest, largest.ptr, 8, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+    bool brute = !std::isfinite(h_largest) || std::sqrt(h_largest) > 1e15;
+
+    DeviceBuffer<double> out_key(n * k, s);
+    DeviceBuffer<uint32_t> out_row(n * k, s), full_flag(n, s);
+    DeviceBuffer<unsigned long long> n_cand(1, s);
+    n_cand.zero();
+    double filter_ms = 0, rank_ms = 0;
+    if (brute) {
+      uint32_t one = 1;
+      std::vector<uint32_t> all(n, one);
+      KG_CUDA(cudaMemcpyAsync(full_flag.ptr, all.data(), n * 4, cudaMemcpyHostToDevice, s));
+    } else {
+      const uint32_t cap = kCandidateCap;
+      uint64_t chunk = std::min<uint64_t>(n, kQueryChunk);
+      DeviceBuffer<float> cand_key(chunk * cap, s), thr(chunk, s);
+      DeviceBuffer<uint32_t> cand_row(chunk * cap, s), cand_count(chunk, s);
+      for (uint64_t q0 = 0; q0 < n; q0 += chunk) {
+        check_cancel(ctx);
+        uint64_t q1 = std::min(n, q0 + chunk);
+        Timer tf(s);
+        filter_kernel<<<blocks_for(q1 - q0, kFilterThreads), kFilterThreads, 0, s>>>(
+            rows.ptr, offsets.ptr, slack.ptr, n, q0, q1, k, cap, cand_key.ptr, cand_row.ptr,
+            cand_count.ptr, thr.ptr);
+        KG_LAUNCH_CHECK();
+        filter_ms += tf.stop_ms();
+        Timer tr(s);
+        rank_kernel<<<blocks_for((q1 - q0) * 32, kRankWarps * 32), kRankWarps * 32, 0, s>>>(
+            x, width, d, q0, q1, k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
+            slack.ptr, out_key.ptr, out_row.ptr, full_flag.ptr, n_cand.ptr);
+        KG_LAUNCH_CHECK();
+        rank_ms += tr.stop_ms();
+        ctx->done = q1;
+      }
+    }
+    // Rows that need a full search.
+    DeviceBuffer<uint32_t> list(n, s);
+    DeviceBuffer<unsigned int> n_full(1, s);
+    n_full.zero();
+    compact_flags_kernel<<<blocks_for(n, 256), 256, 0, s>>>(full_flag.ptr, n, list.ptr,
+                                                            n_full.ptr);
+    KG_LAUNCH_CHECK();
+    unsigned int h_full = 0;
+    KG_CUDA(cudaMemcpyAsync(&h_full, n_full.ptr, 4, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+    if (h_full) {
+      // The list's order does not matter: each CTA writes its own row.
+      Timer tr(s);
+      for (uint64_t a = 0; a < h_full; a += 65535) {
+        check_cancel(ctx);
+        unsigned blocks = (unsigned)std::min<uint64_t>(65535, h_full - a);
+        full_rows_kernel<<<blocks, kFullWarps * 32, 0, s>>>(x, n, width, d, k, list.ptr + a,
+                                                            out_key.ptr, out_row.ptr);
+        KG_LAUNCH_CHECK();
+      }
+      rank_ms += tr.stop_ms();
+    }
+    // The CSR graph.
+    DeviceBuffer<uint64_t> g_indptr;
+    DeviceBuffer<uint32_t> g_idx;
+    DeviceBuffer<float> g_dist;
+    bool dev_out = is_device_pointer(indptr);
+    uint64_t* gi = indptr;
+    uint32_t* gx = indices;
+    float* gd = distances;
+    if (!dev_out) {
+      g_indptr.alloc(n + 1, s);
+      g_idx.alloc(n * k, s);
+      g_dist.alloc(n * k, s);
+      gi = g_indptr.ptr;
+      gx = g_idx.ptr;
+      gd = g_dist.ptr;
+    }
+    graph_kernel<<<blocks_for(n, 128), 128, 0, s>>>(out_key.ptr, out_row.ptr, n, k, gi, gx, gd);
+    KG_LAUNCH_CHECK();
+    if (!dev_out) {
+      KG_CUDA(cudaMemcpyAsync(indptr, gi, (n + 1) * 8, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaMemcpyAsync(indices, gx, n * k * 4, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaMemcpyAsync(distances, gd, n * k * 4, cudaMemcpyDeviceToHost, s));
+    }
+    unsigned long long h_cand = 0;
+    KG_CUDA(cudaMemcpyAsync(&h_cand, n_cand.ptr, 8, cudaMemcpyDeviceToHost, s));
+    wait_stream(ctx, s);
+    ctx->done = n;
+    if (stats) {
+      stats->candidates = h_cand;
+      stats->rows_full = h_full;
+      stats->filter_ms = filter_ms;
+      stats->rank_ms = rank_ms;
+    }
+  });
+}

@@ -1,0 +1,859 @@
+// The PCA session: kyto's streamed randomized block Krylov PCA
+// (crates/kyto-exec/src/pca.rs, pca_dense.rs) with the input held in HBM.
+//
+// Layout in HBM: the held input is a CSR (u64 row pointers, u32 PCA-gene positions,
+// f32 values after normalize/log1p) plus, built once per run, its gene-major twin
+// (CSC: u32 rows, f32 values) cut into fixed segments so that X^T D runs as
+// independent, deterministic per-segment sums. Dense g x w matrices (the basis, the
+// products, the blocks) are f64 column-major for cuBLAS/cuSOLVER; per-cell matrices
+// (Omega, W, the embedding rows) are row-major n x w.
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "kg_internal.cuh"
+#include "kg_maps.cuh"
+#include "kg_spmm.cuh"
+
+namespace kg {
+
+// Declared in kg_maps.cu.
+void map_block(const uint64_t* d_indptr, const void* d_values, kg_dtype dtype,
+               uint64_t n_rows, uint64_t nnz, double target_sum, int do_log1p,
+               float* d_out, cudaStream_t stream);
+template <class P>
+void sort_by_gene(const uint32_t* genes, const P* payload, uint64_t nnz, uint32_t n_genes,
+                  DeviceBuffer<uint32_t>& genes_out, DeviceBuffer<P>& payload_out,
+                  cudaStream_t stream);
+void column_starts(const uint32_t* sorted_genes, uint64_t nnz, uint32_t n_genes,
+                   uint64_t* colptr, cudaStream_t stream);
+void check_indices(const uint32_t* d_idx, uint64_t nnz, uint32_t n_genes, cudaStream_t s);
+
+constexpr uint32_t kNoGene = 0xFFFFFFFFu;
+constexpr int kPasses = 11;            // 2 + PCA_POWER_ITERATIONS (pca.rs:123)
+constexpr uint32_t kOversamples = 10;  // PCA_OVERSAMPLES (estimate.rs:153)
+constexpr double kDropTolerance = 1e-10;  // pca_dense.rs:30
+
+// ----------------------------------------------------------------- pack kernels ----
+
+// Kept entries per row (genes mapped into the PCA's set), one warp per row.
+__global__ void count_kept_kernel(const uint64_t* indptr, const uint32_t* idx,
+                                  uint64_t n_rows, const uint32_t* gene_map,
+                                  uint64_t* kept) {
+  uint64_t row = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  unsigned lane = threadIdx.x & 31u;
+  if (row >= n_rows) return;
+  uint64_t s = indptr[row], e = indptr[row + 1];
+  uint64_t count = 0;
+  for (uint64_t i = s + lane; i < e; i += 32)
+    count += (gene_map == nullptr || gene_map[idx[i]] != kNoGene);
+  for (int o = 16; o; o >>= 1) count += __shfl_down_sync(0xFFFFFFFFu, count, o);
+  if (lane == 0) kept[row] = count;
+}
+
+// Writes each row's kept entries in order at out_ptr[row] (warp per row, ballot
+// compaction keeps the row's gene order).
+__global__ void write_kept_kernel(const uint64_t* indptr, const uint32_t* idx,
+                                  const float* mapped, uint64_t n_rows,
+                                  const uint32_t* gene_map, const uint64_t* out_ptr,
+                                  uint32_t* col, float* val) {
+  uint64_t row = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  unsigned lane = threadIdx.x & 31u;
+  if (row >= n_rows) return;
+  uint64_t s = indptr[row], e = indptr[row + 1];
+  uint64_t base = out_ptr[row];
+  for (uint64_t i0 = s; i0 < e; i0 += 32) {
+    uint64_t i = i0 + lane;
+    bool in = i < e;
+    uint32_t p = kNoGene;
+    if (in) p = gene_map ? gene_map[idx[i]] : idx[i];
+    bool keep = in && p != kNoGene;
+    unsigned ballot = __ballot_sync(0xFFFFFFFFu, keep);
+    if (keep) {
+      uint64_t at = base + __popc(ballot & ((1u << lane) - 1u));
+      col[at] = p;
+      val[at] = mapped[i];
+    }
+    base += __popc(ballot);
+  }
+}
+
+// The row of each held entry (for the gene-major twin).
+__global__ void row_of_kernel(const uint64_t* indptr, uint64_t n_rows, uint32_t* row_of) {
+  uint64_t row = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  unsigned lane = threadIdx.x & 31u;
+  if (row >= n_rows) return;
+  for (uint64_t i = indptr[row] + lane; i < indptr[row + 1]; i += 32) row_of[i] = (uint32_t)row;
+}
+
+__global__ void gather_csc_kernel(const uint32_t* perm, const uint32_t* row_of,
+                                  const float* val, uint64_t nnz, uint32_t* csc_row,
+                                  float* csc_val) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nnz;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t e = perm[i];
+    csc_row[i] = row_of[e];
+    csc_val[i] = val[e];
+  }
+}
+
+__global__ void add_offset_kernel(uint64_t* p, uint64_t n, uint64_t offset) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) p[i] += offset;
+}
+
+// --------------------------------------------------------------- small kernels -----
+
+// Omega's rows (pca.rs:936-950) beside a column of ones (the gene sums' column):
+// out is n x (width + 1) row-major.
+__device__ __forceinline__ uint64_t splitmix_mix(uint64_t v) {
+  v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ull;
+  v = (v ^ (v >> 27)) * 0x94D049BB133111EBull;
+  return v ^ (v >> 31);
+}
+
+__global__ void omega_kernel(const uint64_t* cells, uint64_t n, uint32_t width,
+                             uint64_t seed, double* out) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  uint64_t state = splitmix_mix(seed ^ splitmix_mix(cells[r] + 0x9E3779B97F4A7C15ull));
+  double* row = out + r * (uint64_t)(width + 1);
+  for (uint32_t j = 0; j < width; ++j) {
+    state += 0x9E3779B97F4A7C15ull;
+    row[j] = __dadd_rn((double)(splitmix_mix(state) >> 11) * 0x1p-52, -1.0);
+  }
+  row[width] = 1.0;
+}
+
+// Column sums of an n x w row-major matrix, stage 1: block b sums rows
+// [b*rows_per, ...) in row order per column.
+__global__ void colsum_partial_kernel(const double* m, uint64_t n, uint32_t w,
+                                      uint32_t ld, uint64_t rows_per, double* partial) {
+  uint64_t r0 = blockIdx.x * rows_per;
+  uint64_t r1 = min(n, r0 + rows_per);
+  for (uint32_t j = threadIdx.x; j < w; j += blockDim.x) {
+    double acc = 0.0;
+    for (uint64_t r = r0; r < r1; ++r) acc = __dadd_rn(acc, m[r * ld + j]);
+    partial[blockIdx.x * (uint64_t)w + j] = acc;
+  }
+}
+
+__global__ void colsum_final_kernel(const double* partial, uint32_t nb, uint32_t w,
+                                    double* out) {
+  for (uint32_t j = threadIdx.x; j < w; j += blockDim.x) {
+    double acc = 0.0;
+    for (uint32_t b = 0; b < nb; ++b) acc = __dadd_rn(acc, partial[b * (uint64_t)w + j]);
+    out[j] = acc;
+  }
+}
+
+// m[:, j] -= means * sums[j]  (g x w column-major).
+__global__ void subtract_outer_kernel(double* m, const double* means, const double* sums,
+                                      uint32_t g, uint32_t w) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= (uint64_t)g * w) return;
+  uint32_t j = (uint32_t)(i / g), r = (uint32_t)(i % g);
+  m[i] = __dadd_rn(m[i], -__dmul_rn(means[r], sums[j]));
+}
+
+// out[j] = sum_g means[g] * m[g, j], genes in order (set_block / finish_basis).
+__global__ void mean_dot_kernel(const double* m, const double* means, uint32_t g,
+                                uint32_t w, double* out) {
+  uint32_t j = blockIdx.x;
+  if (j >= w) return;
+  __shared__ double part[256];
+  double acc = 0.0;
+  uint32_t chunk = (g + blockDim.x - 1) / blockDim.x;
+  uint32_t a = threadIdx.x * chunk, b = min(g, a + chunk);
+  for (uint32_t r = a; r < b; ++r) acc = __dadd_rn(acc, __dmul_rn(means[r], m[(uint64_t)j * g + r]));
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (unsigned t = 0; t < blockDim.x; ++t) s = __dadd_rn(s, part[t]);
+    out[j] = s;
+  }
+}
+
+// Column-major g x w -> row-major g x w.
+__global__ void to_row_major_kernel(const double* cm, uint32_t g, uint32_t w, double* rm) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= (uint64_t)g * w) return;
+  uint32_t r = (uint32_t)(i / w), j = (uint32_t)(i % w);
+  rm[i] = cm[(uint64_t)j * g + r];
+}
+
+// sym = (B + B^T) / 2.
+__global__ void symmetrize_kernel(const double* b, uint32_t m, double* sym) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= (uint64_t)m * m) return;
+  uint32_t r = (uint32_t)(i % m), c = (uint32_t)(i / m);
+  sym[i] = 0.5 * __dadd_rn(b[i], b[(uint64_t)r * m + c]);
+}
+
+// chosen[:, c] = vectors[:, m - 1 - c] (largest eigenvalue first).
+__global__ void pick_columns_kernel(const double* vectors, uint32_t m, uint32_t taken,
+                                    double* chosen) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= (uint64_t)m * taken) return;
+  uint32_t r = (uint32_t)(i % m), c = (uint32_t)(i / m);
+  chosen[i] = vectors[(uint64_t)(m - 1 - c) * m + r];
+}
+
+// pca_dense.rs:225-253 (complement): `count` unit vectors of the least-covered genes
+// (first on ties), projected off the columns twice, appended after column `have`.
+// One CTA; l is g x k column-major with columns [0, have) filled.
+__global__ void complement_kernel(double* l, uint32_t g, uint32_t have, uint32_t k,
+                                  double* coeff, double* vec) {
+  __shared__ double red[256];
+  __shared__ uint32_t red_i[256];
+  for (uint32_t col = have; col < k; ++col) {
+    // The least covered gene.
+    double best = INFINITY;
+    uint32_t best_i = 0;
+    for (uint32_t r = threadIdx.x; r < g; r += blockDim.x) {
+      double c = 0.0;
+      for (uint32_t j = 0; j < col; ++j) {
+        double v = l[(uint64_t)j * g + r];
+        c += v * v;
+      }
+      if (c < best || (c == best && r < best_i)) {
+        best = c;
+        best_i = r;
+      }
+    }
+    red[threadIdx.x] = best;
+    red_i[threadIdx.x] = best_i;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (unsigned t = 1; t < blockDim.x; ++t)
+        if (red[t] < red[0] || (red[t] == red[0] && red_i[t] < red_i[0])) {
+          red[0] = red[t];
+          red_i[0] = red_i[t];
+        }
+    }
+    __syncthreads();
+    uint32_t gene = red_i[0];
+    for (uint32_t r = threadIdx.x; r < g; r += blockDim.x) vec[r] = (r == gene) ? 1.0 : 0.0;
+    __syncthreads();
+    for (int pass = 0; pass < 2; ++pass) {
+      for (uint32_t j = threadIdx.x; j < col; j += blockDim.x) {
+        double s = 0.0;
+        for (uint32_t r = 0; r < g; ++r) s += l[(uint64_t)j * g + r] * vec[r];
+        coeff[j] = s;
+      }
+      __syncthreads();
+      for (uint32_t r = threadIdx.x; r < g; r += blockDim.x) {
+        double s = 0.0;
+        for (uint32_t j = 0; j < col; ++j) s += l[(uint64_t)j * g + r] * coeff[j];
+        vec[r] -= s;
+      }
+      __syncthreads();
+    }
+    double part = 0.0;
+    for (uint32_t r = threadIdx.x; r < g; r += blockDim.x) part += vec[r] * vec[r];
+    red[threadIdx.x] = part;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (unsigned t = 0; t < blockDim.x; ++t) s += red[t];
+      red[0] = sqrt(s);
+    }
+    __syncthreads();
+    double norm = red[0];
+    for (uint32_t r = threadIdx.x; r < g; r += blockDim.x) l[(uint64_t)col * g + r] = vec[r] / norm;
+    __syncthreads();
+  }
+}
+
+// pca_dense.rs:257-275 (flip_signs): one CTA per column; the first largest |v| made
+// positive.
+__global__ void flip_signs_kernel(double* l, uint32_t g) {
+  uint32_t j = blockIdx.x;
+  __shared__ double best_v[256];
+  __shared__ uint32_t best_i[256];
+  double bv = 0.0;
+  uint32_t bi = 0xFFFFFFFFu;
+  double sign = 1.0;
+  for (uint32_t r = threadIdx.x; r < g; r += blockDim.x) {
+    double v = l[(uint64_t)j * g + r];
+    if (fabs(v) > bv) {
+      bv = fabs(v);
+      bi = r;
+    }
+  }
+  best_v[threadIdx.x] = bv;
+  best_i[threadIdx.x] = bi;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (unsigned t = 1; t < blockDim.x; ++t)
+      if (best_v[t] > best_v[0] || (best_v[t] == best_v[0] && best_i[t] < best_i[0])) {
+        best_v[0] = best_v[t];
+        best_i[0] = best_i[t];
+      }
+    if (best_i[0] != 0xFFFFFFFFu && l[(uint64_t)j * g + best_i[0]] < 0.0) sign = -1.0;
+    best_v[0] = sign;
+  }
+  __syncthreads();
+  if (best_v[0] < 0.0)
+    for (uint32_t r = threadIdx.x; r < g; r += blockDim.x) l[(uint64_t)j * g + r] = -l[(uint64_t)j * g + r];
+}
+
+// Loadings over the stream's genes (zeros outside the set), f32, row-major.
+__global__ void scatter_loadings_kernel(const double* l, uint32_t g, uint32_t k,
+                                        const uint32_t* set_genes, uint32_t stream_genes,
+                                        float* out) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= (uint64_t)g * k) return;
+  uint32_t r = (uint32_t)(i / k), c = (uint32_t)(i % k);
+  uint32_t sg = set_genes ? set_genes[r] : r;
+  out[(uint64_t)sg * k + c] = (float)l[(uint64_t)c * g + r];
+}
+
+__global__ void to_f32_kernel(const double* in, uint64_t n, float* out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+
+__global__ void divide_kernel(const double* in, uint32_t n, double d, double* out) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = in[i] / d;
+}
+
+}  // namespace kg
+
+using namespace kg;
+
+struct kg_pca {
+  kg_ctx* ctx = nullptr;
+  cudaStream_t stream = nullptr;
+  cublasHandle_t cublas = nullptr;
+  cusolverDnHandle_t cusolver = nullptr;
+  uint32_t k = 0, stream_genes = 0, n_genes = 0, width = 0;
+  uint64_t seed = 0;
+  double target_sum = NAN;
+  int log1p = 0;
+  DeviceBuffer<uint32_t> gene_map, set_genes;
+  // Held input (CSR over the PCA's genes).
+  DeviceBuffer<uint64_t> indptr;
+  DeviceBuffer<uint32_t> col;
+  DeviceBuffer<float> val;
+  DeviceBuffer<uint64_t> cells;
+  uint64_t n_cells = 0, nnz = 0, next_cell = 0;
+  // Results.
+  bool ran = false;
+  uint32_t passes_run = 0;
+  DeviceBuffer<float> embedding, loadings;
+  DeviceBuffer<double> means;
+  std::vector<double> variance, variance_ratio;
+
+  ~kg_pca() {
+    if (stream) cudaStreamSynchronize(stream);
+    if (cusolver) cusolverDnDestroy(cusolver);
+    if (cublas) cublasDestroy(cublas);
+    gene_map.reset();
+    set_genes.reset();
+    indptr.reset();
+    col.reset();
+    val.reset();
+    cells.reset();
+    embedding.reset();
+    loadings.reset();
+    means.reset();
+    if (stream) {
+      cudaStreamSynchronize(stream);
+      cudaStreamDestroy(stream);
+    }
+  }
+
+  template <class T>
+  void grow(DeviceBuffer<T>& buf, size_t used, size_t need) {
+    if (need <= buf.count) return;
+    size_t cap = std::max(need, buf.count + buf.count / 2);
+    DeviceBuffer<T> bigger(cap, stream);
+    if (used) KG_CUDA(cudaMemcpyAsync(bigger.ptr, buf.ptr, used * sizeof(T),
+                                      cudaMemcpyDeviceToDevice, stream));
+    buf = std::move(bigger);
+  }
+
+  void push(const uint64_t* h_indptr, const uint32_t* h_idx, const void* h_values,
+            kg_dtype dtype, uint64_t n_rows, const uint64_t* h_cells);
+  void run();
+};
+
+void kg_pca::push(const uint64_t* in_indptr, const uint32_t* in_idx, const void* in_values,
+                  kg_dtype dtype, uint64_t n_rows, const uint64_t* in_cells) {
+  if (ran) fail(KG_ERR_STATE, "kg_pca_push_block after kg_pca_run");
+  if (dtype != KG_U32 && dtype != KG_F32) fail(KG_ERR_INVALID, "unknown dtype");
+  if (n_rows == 0) return;
+  cudaStream_t s = stream;
+  DeviceBuffer<uint64_t> hp, hc;
+  const uint64_t* d_indptr = device_view(in_indptr, n_rows + 1, hp, s);
+  uint64_t ends[2];
+  KG_CUDA(cudaMemcpyAsync(&ends[0], d_indptr, 8, cudaMemcpyDefault, s));
+  KG_CUDA(cudaMemcpyAsync(&ends[1], d_indptr + n_rows, 8, cudaMemcpyDefault, s));
+  KG_CUDA(cudaStreamSynchronize(s));
+  if (ends[0] != 0) fail(KG_ERR_INVALID, "a block's indptr must start at 0");
+  uint64_t bnnz = ends[1];
+  DeviceBuffer<uint32_t> hi, hv;
+  const uint32_t* d_idx = device_view(in_idx, bnnz, hi, s);
+  const void* d_values = device_view((const uint32_t*)in_values, bnnz, hv, s);
+  check_indices(d_idx, bnnz, stream_genes, s);
+  DeviceBuffer<float> mapped(bnnz, s);
+  map_block(d_indptr, d_values, dtype, n_rows, bnnz, target_sum, log1p, mapped.ptr, s);
+  // Kept entries per row, then their offsets after the held entries.
+  DeviceBuffer<uint64_t> kept(n_rows + 1, s);
+  kept.zero();
+  unsigned threads = 256;
+  count_kept_kernel<<<blocks_for(n_rows * 32, threads), threads, 0, s>>>(
+      d_indptr, d_idx, n_rows, gene_map.ptr, kept.ptr);
+  KG_LAUNCH_CHECK();
+  size_t temp = 0;
+  KG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, kept.ptr, kept.ptr, n_rows + 1, s));
+  DeviceBuffer<unsigned char> scratch(temp, s);
+  KG_CUDA(cub::DeviceScan::ExclusiveSum(scratch.ptr, temp, kept.ptr, kept.ptr, n_rows + 1, s));
+  uint64_t added = 0;
+  KG_CUDA(cudaMemcpyAsync(&added, kept.ptr + n_rows, 8, cudaMemcpyDeviceToHost, s));
+  KG_CUDA(cudaStreamSynchronize(s));
+  add_offset_kernel<<<blocks_for(n_rows + 1, 256), 256, 0, s>>>(kept.ptr, n_rows + 1, nnz);
+  KG_LAUNCH_CHECK();
+  grow(indptr, n_cells + 1, n_cells + n_rows + 1);
+  grow(col, nnz, nnz + added);
+  grow(val, nnz, nnz + added);
+  grow(cells, n_cells, n_cells + n_rows);
+  KG_CUDA(cudaMemcpyAsync(indptr.ptr + n_cells, kept.ptr, (n_rows + 1) * 8,
+                          cudaMemcpyDeviceToDevice, s));
+  write_kept_kernel<<<blocks_for(n_rows * 32, threads), threads, 0, s>>>(
+      d_indptr, d_idx, mapped.ptr, n_rows, gene_map.ptr, kept.ptr, col.ptr, val.ptr);
+  KG_LAUNCH_CHECK();
+  if (in_cells) {
+    const uint64_t* d_cells = device_view(in_cells, n_rows, hc, s);
+    KG_CUDA(cudaMemcpyAsync(cells.ptr + n_cells, d_cells, n_rows * 8, cudaMemcpyDeviceToDevice, s));
+    std::vector<uint64_t> last(1);
+    KG_CUDA(cudaMemcpyAsync(last.data(), d_cells + n_rows - 1, 8, cudaMemcpyDefault, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+    next_cell = last[0] + 1;
+  } else {
+    std::vector<uint64_t> pos(n_rows);
+    for (uint64_t r = 0; r < n_rows; ++r) pos[r] = next_cell + r;
+    KG_CUDA(cudaMemcpyAsync(cells.ptr + n_cells, pos.data(), n_rows * 8, cudaMemcpyHostToDevice, s));
+    next_cell += n_rows;
+    KG_CUDA(cudaStreamSynchronize(s));
+  }
+  n_cells += n_rows;
+  nnz += added;
+  KG_CUDA(cudaStreamSynchronize(s));
+}
+
+namespace {
+
+// Dense FP64 helpers over one session (column-major g x w matrices).
+struct Dense {
+  kg_pca* p;
+  cudaStream_t s;
+  uint32_t g;
+
+  double fro_norm(const double* m, uint64_t count) {
+    double out = 0.0;
+    KG_CUBLAS(cublasDnrm2(p->cublas, (int)count, m, 1, &out));
+    return out;
+  }
+
+  // pca_dense.rs:105-129: the directions `block` (g x w) adds to `basis` (g x m):
+  // CGS twice, thin SVD, keep sigma > 1e-10 |block|_F. Returns the new block.
+  DeviceBuffer<double> extend_basis(const double* basis, uint32_t m, const double* block,
+                                    uint32_t w, uint32_t* keep_out) {
+    *keep_out = 0;
+    DeviceBuffer<double> none;
+    if (w == 0) return none;
+    double scale = fro_norm(block, (uint64_t)g * w);
+    if (!(scale > 0.0)) {
+      if (std::isnan(scale)) fail(KG_ERR_INVALID, "pca: the Krylov block is not finite");
+      return none;
+    }
+    DeviceBuffer<double> rest((uint64_t)g * w, s);
+    KG_CUDA(cudaMemcpyAsync(rest.ptr, block, rest.bytes(), cudaMemcpyDeviceToDevice, s));
+    if (m > 0) {
+      DeviceBuffer<double> proj((uint64_t)m * w, s);
+      const double one = 1.0, zero = 0.0, minus = -1.0;
+      for (int pass = 0; pass < 2; ++pass) {
+        KG_CUBLAS(cublasDgemm(p->cublas, CUBLAS_OP_T, CUBLAS_OP_N, m, w, g, &one, basis, g,
+                              rest.ptr, g, &zero, proj.ptr, m));
+        KG_CUBLAS(cublasDgemm(p->cublas, CUBLAS_OP_N, CUBLAS_OP_N, g, w, m, &minus, basis, g,
+                              proj.ptr, m, &one, rest.ptr, g));
+      }
+    }
+    int lwork = 0;
+    KG_CUSOLVER(cusolverDnDgesvd_bufferSize(p->cusolver, g, w, &lwork));
+    DeviceBuffer<double> work(std::max(lwork, 1), s), sv(w, s), u((uint64_t)g * w, s),
+        vt(1, s), rwork(w, s);
+    DeviceBuffer<int> info(1, s);
+    KG_CUSOLVER(cusolverDnDgesvd(p->cusolver, 'S', 'N', g, w, rest.ptr, g, sv.ptr, u.ptr, g,
+                                 vt.ptr, 1, work.ptr, lwork, rwork.ptr, info.ptr));
+    std::vector<double> h_sv(w);
+    int h_info = 0;
+    KG_CUDA(cudaMemcpyAsync(h_sv.data(), sv.ptr, w * 8ull, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaMemcpyAsync(&h_info, info.ptr, 4, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+    if (h_info != 0)
+      fail(KG_ERR_INVALID, "pca: orthonormalising a Krylov block did not converge");
+    uint32_t keep = 0;
+    while (keep < w && h_sv[keep] > kDropTolerance * scale) ++keep;
+    *keep_out = keep;
+    if (keep == 0) return none;
+    DeviceBuffer<double> out((uint64_t)g * keep, s);
+    KG_CUDA(cudaMemcpyAsync(out.ptr, u.ptr, out.bytes(), cudaMemcpyDeviceToDevice, s));
+    return out;
+  }
+
+  void mean_dot(const double* m, const double* means, uint32_t w, double* out) {
+    if (w == 0) return;
+    mean_dot_kernel<<<w, 256, 0, s>>>(m, means, g, w, out);
+    KG_LAUNCH_CHECK();
+  }
+};
+
+}  // namespace
+
+void kg_pca::run() {
+  if (ran) fail(KG_ERR_STATE, "kg_pca_run called twice");
+  kg_ctx* c = ctx;
+  cudaStream_t s = stream;
+  const uint64_t n = n_cells;
+  const uint32_t g = n_genes;
+  if (n < 2)
+    fail(KG_ERR_INVALID, std::to_string(n) + " cells reach pca (it needs at least 2)");
+  if (g == 0) fail(KG_ERR_INVALID, "pca: the gene set holds no gene");
+  if (k > std::min<uint64_t>(n, g))
+    fail(KG_ERR_INVALID, "pca: n_components " + std::to_string(k) + " is more than " +
+                             std::to_string(std::min<uint64_t>(n, g)) +
+                             " (the cells and genes reaching pca)");
+  if (nnz >= (1ull << 32)) fail(KG_ERR_INVALID, "pca: more than 2^32 stored values");
+  if (n >= (1ull << 32)) fail(KG_ERR_INVALID, "pca: more than 2^32 cells");
+  const uint32_t l = width;
+  c->total = n * kPasses;
+  c->done = 0;
+
+  // The gene-major twin of the held input, cut into segments.
+  DeviceBuffer<uint32_t> row_of(nnz, s), iota(nnz, s);
+  row_of_kernel<<<blocks_for(n * 32, 256), 256, 0, s>>>(indptr.ptr, n, row_of.ptr);
+  KG_LAUNCH_CHECK();
+  GeneMajor gm;
+  {
+    iota_fill(iota.ptr, nnz, s);
+    DeviceBuffer<uint32_t> genes_sorted, perm;
+    sort_by_gene<uint32_t>(col.ptr, iota.ptr, nnz, g, genes_sorted, perm, s);
+    iota.reset();
+    gm.colptr.alloc((uint64_t)g + 1, s);
+    column_starts(genes_sorted.ptr, nnz, g, gm.colptr.ptr, s);
+    genes_sorted.reset();
+    gm.row.alloc(nnz, s);
+    gm.val.alloc(nnz, s);
+    if (nnz) {
+      gather_csc_kernel<<<std::min<unsigned>(blocks_for(nnz, 256), 16384), 256, 0, s>>>(
+          perm.ptr, row_of.ptr, val.ptr, nnz, gm.row.ptr, gm.val.ptr);
+      KG_LAUNCH_CHECK();
+    }
+    gm.build_segments(g, nnz, s);
+  }
+  row_of.reset();
+
+  Dense dense{this, s, g};
+  auto colsums = [&](const double* m, uint32_t w, uint32_t ld, double* out) {
+    uint64_t rows_per = 2048;
+    uint32_t nb = (uint32_t)((n + rows_per - 1) / rows_per);
+    DeviceBuffer<double> part((uint64_t)nb * w, s);
+    colsum_partial_kernel<<<nb, 64, 0, s>>>(m, n, w, ld, rows_per, part.ptr);
+    KG_LAUNCH_CHECK();
+    colsum_final_kernel<<<1, 64, 0, s>>>(part.ptr, nb, w, out);
+    KG_LAUNCH_CHECK();
+  };
+
+  // ---- pass 0: sketch X^T [Omega 1] (pca.rs:588-622, end_pass pca.rs:707-749) ----
+  means.alloc(g, s);
+  DeviceBuffer<double> omega_sums(l, s), sketch1((uint64_t)g * (l + 1), s);
+  {
+    DeviceBuffer<double> omega(n * (l + 1), s);
+    omega_kernel<<<blocks_for(n, 128), 128, 0, s>>>(cells.ptr, n, l, seed, omega.ptr);
+    KG_LAUNCH_CHECK();
+    colsums(omega.ptr, l, l + 1, omega_sums.ptr);
+    gm.transposed_product(omega.ptr, l + 1, g, sketch1.ptr, s);
+  }
+  divide_kernel<<<blocks_for(g, 256), 256, 0, s>>>(sketch1.ptr + (uint64_t)l * g, g,
+                                                     (double)n, means.ptr);
+  KG_LAUNCH_CHECK();
+  {
+    std::vector<double> h_means(g);
+    KG_CUDA(cudaMemcpyAsync(h_means.data(), means.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+    for (uint32_t i = 0; i < g; ++i)
+      if (!std::isfinite(h_means[i]))
+        fail(KG_ERR_INVALID, "pca: gene " + std::to_string(i) +
+                                 " holds a value that is not finite (NaN or infinity)");
+  }
+  subtract_outer_kernel<<<blocks_for((uint64_t)g * l, 256), 256, 0, s>>>(
+      sketch1.ptr, means.ptr, omega_sums.ptr, g, l);
+  KG_LAUNCH_CHECK();
+  c->done += n;
+  check_cancel(c);
+
+  const uint32_t max_basis = (kPasses - 2) * l;
+  DeviceBuffer<double> basis((uint64_t)g * max_basis, s), products((uint64_t)g * max_basis, s);
+  uint32_t m = 0;  // basis columns
+  uint32_t w = 0;
+  DeviceBuffer<double> block = dense.extend_basis(basis.ptr, 0, sketch1.ptr, l, &w);
+  sketch1.reset();
+  bool finished = false;
+  std::vector<double> eigen;
+  DeviceBuffer<double> loadings64, mean_projection;
+  passes_run = 1;
+
+  auto finish_basis = [&]() {
+    // pca_dense.rs:141-174 (rayleigh_ritz) and pca.rs:848-862 (finish_basis).
+    loadings64.alloc((uint64_t)g * k, s);
+    uint32_t taken = std::min(k, m);
+    eigen.assign(k, 0.0);
+    if (m > 0) {
+      DeviceBuffer<double> b((uint64_t)m * m, s), sym((uint64_t)m * m, s), evals(m, s);
+      const double one = 1.0, zero = 0.0;
+      KG_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_T, CUBLAS_OP_N, m, m, g, &one, basis.ptr, g,
+                            products.ptr, g, &zero, b.ptr, m));
+      symmetrize_kernel<<<blocks_for((uint64_t)m * m, 256), 256, 0, s>>>(b.ptr, m, sym.ptr);
+      KG_LAUNCH_CHECK();
+      int lwork = 0;
+      KG_CUSOLVER(cusolverDnDsyevd_bufferSize(cusolver, CUSOLVER_EIG_MODE_VECTOR,
+                                              CUBLAS_FILL_MODE_LOWER, m, sym.ptr, m,
+                                              evals.ptr, &lwork));
+      DeviceBuffer<double> work(std::max(lwork, 1), s);
+      DeviceBuffer<int> info(1, s);
+      KG_CUSOLVER(cusolverDnDsyevd(cusolver, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER,
+                                   m, sym.ptr, m, evals.ptr, work.ptr, lwork, info.ptr));
+      std::vector<double> h_evals(m);
+      int h_info = 0;
+      KG_CUDA(cudaMemcpyAsync(h_evals.data(), evals.ptr, m * 8ull, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaMemcpyAsync(&h_info, info.ptr, 4, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaStreamSynchronize(s));
+      if (h_info != 0)
+        fail(KG_ERR_INVALID, "pca: the Rayleigh-Ritz eigendecomposition did not converge");
+      for (uint32_t i = 0; i < taken; ++i) eigen[i] = std::max(h_evals[m - 1 - i], 0.0);
+      DeviceBuffer<double> chosen((uint64_t)m * taken, s);
+      pick_columns_kernel<<<blocks_for((uint64_t)m * taken, 256), 256, 0, s>>>(
+          sym.ptr, m, taken, chosen.ptr);
+      KG_LAUNCH_CHECK();
+      KG_CUBLAS(cublasDgemm(cublas, CUBLAS_OP_N, CUBLAS_OP_N, g, taken, m, &one, basis.ptr, g,
+                            chosen.ptr, m, &zero, loadings64.ptr, g));
+    }
+    if (taken < k) {
+      DeviceBuffer<double> coeff(k, s), vec(g, s);
+      complement_kernel<<<1, 256, 0, s>>>(loadings64.ptr, g, taken, k, coeff.ptr, vec.ptr);
+      KG_LAUNCH_CHECK();
+    }
+    flip_signs_kernel<<<k, 256, 0, s>>>(loadings64.ptr, g);
+    KG_LAUNCH_CHECK();
+    mean_projection.alloc(k, s);
+    dense.mean_dot(loadings64.ptr, means.ptr, k, mean_projection.ptr);
+    finished = true;
+  };
+
+  if (w == 0) finish_basis();
+  for (int pass = 1; pass < kPasses - 1 && !finished; ++pass) {
+    check_cancel(c);
+    // w = x Q - mu^T Q per row (pca.rs:623-645); C Q = X^T W - mu (sum w) (pca.rs:750-775).
+    DeviceBuffer<double> block_means(w, s), block_rm((uint64_t)g * w, s), wrows(n * w, s),
+        wsums(w, s);
+    dense.mean_dot(block.ptr, means.ptr, w, block_means.ptr);
+    to_row_major_kernel<<<blocks_for((uint64_t)g * w, 256), 256, 0, s>>>(block.ptr, g, w,
+                                                                          block_rm.ptr);
+    KG_LAUNCH_CHECK();
+    row_product(indptr.ptr, col.ptr, val.ptr, n, block_rm.ptr, block_means.ptr, w, wrows.ptr, s);
+    colsums(wrows.ptr, w, w, wsums.ptr);
+    double* product = products.ptr + (uint64_t)m * g;
+    gm.transposed_product(wrows.ptr, w, g, product, s);
+    subtract_outer_kernel<<<blocks_for((uint64_t)g * w, 256), 256, 0, s>>>(
+        product, means.ptr, wsums.ptr, g, w);
+    KG_LAUNCH_CHECK();
+    KG_CUDA(cudaMemcpyAsync(basis.ptr + (uint64_t)m * g, block.ptr, (uint64_t)g * w * 8,
+                            cudaMemcpyDeviceToDevice, s));
+    m += w;
+    ++passes_run;
+    c->done += n;
+    if (pass == kPasses - 2) {
+      finish_basis();
+    } else {
+      block = dense.extend_basis(basis.ptr, m, product, w, &w);
+      if (w == 0) finish_basis();
+    }
+  }
+  check_cancel(c);
+
+  // ---- last pass: rows (x - mu) V and the centred squares (pca.rs:649-677, 779-797) ----
+  {
+    DeviceBuffer<double> l_rm((uint64_t)g * k, s), rows(n * k, s);
+    to_row_major_kernel<<<blocks_for((uint64_t)g * k, 256), 256, 0, s>>>(loadings64.ptr, g, k,
+                                                                          l_rm.ptr);
+    KG_LAUNCH_CHECK();
+    row_product(indptr.ptr, col.ptr, val.ptr, n, l_rm.ptr, mean_projection.ptr, k, rows.ptr, s);
+    embedding.alloc(n * k, s);
+    to_f32_kernel<<<std::min<unsigned>(blocks_for(n * k, 256), 16384), 256, 0, s>>>(
+        rows.ptr, n * k, embedding.ptr);
+    KG_LAUNCH_CHECK();
+  }
+  std::vector<double> squares(g);
+  std::vector<uint64_t> colptr(g + 1);
+  {
+    DeviceBuffer<double> sq(g, s);
+    gm.centred_squares(means.ptr, g, sq.ptr, s);
+    KG_CUDA(cudaMemcpyAsync(squares.data(), sq.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaMemcpyAsync(colptr.data(), gm.colptr.ptr, (g + 1) * 8ull, cudaMemcpyDeviceToHost, s));
+  }
+  std::vector<double> h_means(g);
+  KG_CUDA(cudaMemcpyAsync(h_means.data(), means.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
+  loadings.alloc((uint64_t)stream_genes * k, s);
+  loadings.zero();
+  scatter_loadings_kernel<<<blocks_for((uint64_t)g * k, 256), 256, 0, s>>>(
+      loadings64.ptr, g, k, set_genes.ptr, stream_genes, loadings.ptr);
+  KG_LAUNCH_CHECK();
+  wait_stream(c, s);
+  ++passes_run;
+  c->done += n;
+  double total = 0.0;
+  for (uint32_t i = 0; i < g; ++i) {
+    uint64_t stored = colptr[i + 1] - colptr[i];
+    total += squares[i] + (double)(n - stored) * h_means[i] * h_means[i];
+  }
+  double total_variance = total / ((double)n - 1.0);
+  bool constant = total_variance == 0.0;
+  variance.assign(k, 0.0);
+  variance_ratio.assign(k, 0.0);
+  for (uint32_t i = 0; i < k; ++i) {
+    variance[i] = constant ? 0.0 : eigen[i] / ((double)n - 1.0);
+    variance_ratio[i] = variance[i] / total_variance;
+  }
+  ran = true;
+}
+
+extern "C" {
+
+kg_status kg_pca_begin(kg_ctx* ctx, const kg_pca_params* params, kg_pca** out) {
+  return guarded([&] {
+    if (!ctx || !params || !out) fail(KG_ERR_INVALID, "kg_pca_begin: NULL argument");
+    *out = nullptr;
+    if (params->n_components == 0) fail(KG_ERR_INVALID, "pca: n_components must be at least 1");
+    if (params->n_genes == 0) fail(KG_ERR_INVALID, "pca: blocks of 0 genes");
+    use_device(ctx);
+    auto* p = new kg_pca();
+    try {
+      p->ctx = ctx;
+      KG_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+      KG_CUBLAS(cublasCreate(&p->cublas));
+      KG_CUBLAS(cublasSetStream(p->cublas, p->stream));
+      KG_CUSOLVER(cusolverDnCreate(&p->cusolver));
+      KG_CUSOLVER(cusolverDnSetStream(p->cusolver, p->stream));
+      p->k = params->n_components;
+      p->stream_genes = params->n_genes;
+      p->seed = params->seed;
+      p->target_sum = params->target_sum;
+      p->log1p = params->log1p;
+      if (params->gene_map) {
+        std::vector<uint32_t> map(params->n_genes), set;
+        KG_CUDA(cudaMemcpy(map.data(), params->gene_map, params->n_genes * 4ull,
+                           cudaMemcpyDefault));
+        uint32_t next = 0;
+        for (uint32_t i = 0; i < params->n_genes; ++i) {
+          if (map[i] == kNoGene) continue;
+          if (map[i] != next)
+            fail(KG_ERR_INVALID, "pca: gene_map must number the kept genes 0, 1, ... in order");
+          set.push_back(i);
+          ++next;
+        }
+        p->n_genes = next;
+        p->gene_map.alloc(params->n_genes, p->stream);
+        KG_CUDA(cudaMemcpyAsync(p->gene_map.ptr, map.data(), map.size() * 4, cudaMemcpyHostToDevice,
+                                p->stream));
+        p->set_genes.alloc(set.size(), p->stream);
+        if (!set.empty())
+          KG_CUDA(cudaMemcpyAsync(p->set_genes.ptr, set.data(), set.size() * 4,
+                                  cudaMemcpyHostToDevice, p->stream));
+        KG_CUDA(cudaStreamSynchronize(p->stream));
+      } else {
+        p->n_genes = params->n_genes;
+      }
+      p->width = std::min<uint32_t>(p->k + kOversamples, p->n_genes);
+      p->indptr.alloc(1, p->stream);
+      p->indptr.zero();
+    } catch (...) {
+      delete p;
+      throw;
+    }
+    *out = p;
+  });
+}
+
+kg_status kg_pca_push_block(kg_pca* pca, const uint64_t* indptr, const uint32_t* indices,
+                            const void* values, kg_dtype dtype, uint64_t n_rows,
+                            const uint64_t* cells) {
+  return guarded([&] {
+    if (!pca || (n_rows && (!indptr || !indices || !values)))
+      fail(KG_ERR_INVALID, "kg_pca_push_block: NULL argument");
+    use_device(pca->ctx);
+    pca->push(indptr, indices, values, dtype, n_rows, cells);
+  });
+}
+
+kg_status kg_pca_run(kg_pca* pca) {
+  return guarded([&] {
+    if (!pca) fail(KG_ERR_INVALID, "kg_pca_run: NULL argument");
+    use_device(pca->ctx);
+    pca->run();
+  });
+}
+
+kg_status kg_pca_results(kg_pca* pca, float* embedding, float* loadings, double* variance,
+                         double* variance_ratio, double* means) {
+  return guarded([&] {
+    if (!pca) fail(KG_ERR_INVALID, "kg_pca_results: NULL argument");
+    if (!pca->ran) fail(KG_ERR_STATE, "kg_pca_results before kg_pca_run");
+    use_device(pca->ctx);
+    cudaStream_t s = pca->stream;
+    if (embedding)
+      KG_CUDA(cudaMemcpyAsync(embedding, pca->embedding.ptr, pca->embedding.bytes(),
+                              cudaMemcpyDefault, s));
+    if (loadings)
+      KG_CUDA(cudaMemcpyAsync(loadings, pca->loadings.ptr, pca->loadings.bytes(),
+                              cudaMemcpyDefault, s));
+    if (means)
+      KG_CUDA(cudaMemcpyAsync(means, pca->means.ptr, pca->means.bytes(), cudaMemcpyDefault, s));
+    wait_stream(pca->ctx, s);
+    if (variance) std::memcpy(variance, pca->variance.data(), pca->k * 8ull);
+    if (variance_ratio) std::memcpy(variance_ratio, pca->variance_ratio.data(), pca->k * 8ull);
+  });
+}
+
+kg_status kg_pca_info(const kg_pca* pca, uint64_t* n_cells, uint32_t* n_pca_genes,
+                      uint32_t* passes_run) {
+  return guarded([&] {
+    if (!pca) fail(KG_ERR_INVALID, "kg_pca_info: NULL argument");
+    if (n_cells) *n_cells = pca->n_cells;
+    if (n_pca_genes) *n_pca_genes = pca->n_genes;
+    if (passes_run) *passes_run = pca->passes_run;
+  });
+}
+
+kg_status kg_pca_embedding_device(const kg_pca* pca, const float** out) {
+  return guarded([&] {
+    if (!pca || !out) fail(KG_ERR_INVALID, "kg_pca_embedding_device: NULL argument");
+    if (!pca->ran) fail(KG_ERR_STATE, "kg_pca_embedding_device before kg_pca_run");
+    *out = pca->embedding.ptr;
+  });
+}
+
+void kg_pca_free(kg_pca* pca) {
+  if (!pca) return;
+  cudaSetDevice(pca->ctx->device);
+  delete pca;
+}
+
+}  // extern "C"

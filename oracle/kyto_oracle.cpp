@@ -305,8 +305,20 @@ double ko_key(const float* points, uint32_t width, uint64_t q, uint64_t p) {
 // f32 matrix-product filter with a proven slack, candidates re-ranked by f64 keys, rows
 // that break an assumption searched against every row). Same result as ko_knn_brute.
 // Timed as the CPU baseline. Returns the number of rows that fell back to a full search.
+uint64_t ko_knn_exact_range(const float* points, uint64_t n, uint32_t width, uint32_t k,
+                            uint64_t query_begin, uint64_t query_end, double* keys_out,
+                            uint32_t* rows_out);
+
 uint64_t ko_knn_exact(const float* points, uint64_t n, uint32_t width, uint32_t k,
                       double* keys_out, uint32_t* rows_out) {
+  return ko_knn_exact_range(points, n, width, k, 0, n, keys_out, rows_out);
+}
+
+// Queries [query_begin, query_end) only (a timed sample of the CPU path); outputs are
+// indexed from query_begin.
+uint64_t ko_knn_exact_range(const float* points, uint64_t n, uint32_t width, uint32_t k,
+                            uint64_t query_begin, uint64_t query_end, double* keys_out,
+                            uint32_t* rows_out) {
   constexpr uint64_t kQueryRows = 128, kPointRows = 1024, kCandidateLimit = 4096;
   const double u = 1.0 / 16777216.0;
   const double factor = 2.0 * ((double)width + 8.0) * u;
@@ -331,6 +343,7 @@ uint64_t ko_knn_exact(const float* points, uint64_t n, uint32_t width, uint32_t 
   }
   largest = std::sqrt(largest);
   if (!std::isfinite(largest) || largest > 1e15) {
+    if (query_begin != 0 || query_end != n) return (uint64_t)-1;
     ko_knn_brute(points, n, width, k, keys_out, rows_out);
     return n;
   }
@@ -351,7 +364,8 @@ uint64_t ko_knn_exact(const float* points, uint64_t n, uint32_t width, uint32_t 
       tiles[(t * width + j) * kPointRows + c] = rows[p * width + j];
   }
   uint64_t fallbacks = 0;
-  uint64_t n_blocks = (n + kQueryRows - 1) / kQueryRows;
+  uint64_t n_queries = query_end - query_begin;
+  uint64_t n_blocks = (n_queries + kQueryRows - 1) / kQueryRows;
 #pragma omp parallel reduction(+ : fallbacks)
   {
     std::vector<float> keys(kQueryRows * kPointRows);
@@ -365,7 +379,8 @@ uint64_t ko_knn_exact(const float* points, uint64_t n, uint32_t width, uint32_t 
     std::vector<Query> states(kQueryRows);
 #pragma omp for schedule(dynamic, 1)
     for (int64_t b = 0; b < (int64_t)n_blocks; ++b) {
-      uint64_t q0 = (uint64_t)b * kQueryRows, q1 = std::min(n, q0 + kQueryRows);
+      uint64_t q0 = query_begin + (uint64_t)b * kQueryRows;
+      uint64_t q1 = std::min(query_end, q0 + kQueryRows);
       for (uint64_t qi = 0; qi < q1 - q0; ++qi) {
         states[qi] = Query();
         states[qi].smallest.reserve(k + 1);
@@ -450,8 +465,8 @@ uint64_t ko_knn_exact(const float* points, uint64_t n, uint32_t width, uint32_t 
             if (p != query) found.offer(ko_key(points, width, query, p), (uint32_t)p);
         }
         for (uint32_t i = 0; i < k; ++i) {
-          keys_out[query * k + i] = found.entries[i].first;
-          rows_out[query * k + i] = found.entries[i].second;
+          keys_out[(query - query_begin) * k + i] = found.entries[i].first;
+          rows_out[(query - query_begin) * k + i] = found.entries[i].second;
         }
       }
     }

@@ -55,6 +55,7 @@ def lib() -> ctypes.CDLL:
             build()
         _lib = ctypes.CDLL(str(LIB_PATH))
         _lib.ko_knn_exact.restype = ctypes.c_uint64
+        _lib.ko_knn_exact_range.restype = ctypes.c_uint64
         _lib.ko_key.restype = ctypes.c_double
         _lib.ko_key.argtypes = [_P, _U32, _U64, _U64]
         _lib.ko_max_threads.restype = ctypes.c_int
@@ -452,6 +453,19 @@ def knn_ranked(points: np.ndarray, n_neighbors: int, method: str = "brute"):
         fallbacks = lib().ko_knn_exact(_ptr(points), _U64(n), _U32(width), _U32(k),
                                        _ptr(keys), _ptr(rows))
     return keys, rows, int(fallbacks)
+
+
+def knn_exact_sample(points: np.ndarray, n_neighbors: int, q_begin: int, q_end: int):
+    """kyto's CPU exact search (the filtered path) for queries [q_begin, q_end) against
+    every row: the CPU baseline's timed sample."""
+    points = np.ascontiguousarray(points, dtype=np.float32)
+    n, width = points.shape
+    k = int(n_neighbors) - 1
+    keys = np.empty((q_end - q_begin, k))
+    rows = np.empty((q_end - q_begin, k), dtype=np.uint32)
+    fb = lib().ko_knn_exact_range(_ptr(points), _U64(n), _U32(width), _U32(k), _U64(q_begin),
+                                  _U64(q_end), _ptr(keys), _ptr(rows))
+    return keys, rows, int(fb)
 
 
 def neighbors(points: np.ndarray, n_neighbors: int = 15, method: str = "brute") -> Graph:

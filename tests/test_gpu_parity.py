@@ -1,0 +1,202 @@
+"""Parity of the CUDA path (through the C ABI) with the oracle and kyto's goldens.
+
+Bars: normalize/log1p, HVG moments and flags, and every kNN row (indices and f32
+distances) bit for bit; PCA within kyto's own GPU-vs-CPU agreement bar, tightened:
+singular values (variances) 1e-6 relative to the FP64 oracle (the product path
+accumulates in f64), loadings/embedding columns 1e-5 of their largest value.
+"""
+
+import numpy as np
+import pytest
+
+import kyto_b200 as K
+from kyto_b200 import synthetic
+from oracle import oracle as O
+from tests.conftest import load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return K.Context(0)
+
+
+@pytest.fixture(scope="module")
+def counts():
+    g = load_golden("synthetic_counts")
+    return O.Csr(g["indptr"], g["indices"], g["counts"], int(g["n_genes"][0]))
+
+
+def test_normalize_log1p_bits(ctx, counts):
+    gold = load_golden("synthetic_normalize_log1p")
+    norm = K.normalize_log1p(counts.indptr, counts.values, 1e4, False, ctx=ctx)
+    assert np.array_equal(norm.view(np.uint32), gold["normalized"].view(np.uint32))
+    gpu = K.normalize_log1p(counts.indptr, counts.values, 1e4, True, ctx=ctx)
+    cpu = O.normalize_log1p(counts, 1e4, True).values
+    assert np.array_equal(gpu.view(np.uint32), cpu.view(np.uint32))
+
+
+def test_normalize_f32_values_and_empty_rows(ctx):
+    rng = np.random.default_rng(3)
+    x = synthetic.counts_csr(300, 500, 40, 3, 20, seed=3, device="cpu")
+    vals = (x.values.astype(np.float32) * rng.uniform(0.1, 3.0, x.nnz).astype(np.float32))
+    # Empty rows (no counts) keep divisor 1.
+    indptr = x.indptr.copy()
+    gpu = K.normalize_log1p(indptr, vals, 1e4, True, ctx=ctx)
+    cpu = O.normalize_log1p(O.Csr(indptr, x.indices, vals, x.n_genes), 1e4, True).values
+    assert np.array_equal(gpu.view(np.uint32), cpu.view(np.uint32))
+
+
+def test_hvg_moments_and_flags(ctx, counts):
+    gold = load_golden("synthetic_hvg")
+    res = K.highly_variable_genes(counts.indptr, counts.indices, counts.values, counts.n_genes,
+                                  n_top_genes=100, ctx=ctx)
+    assert np.array_equal(res.highly_variable, gold["highly_variable"])
+    log1p = O.normalize_log1p(counts)
+    s, q, p = O.hvg_moments(log1p)
+    om, od, on, of = O.hvg_seurat(s, q, p, counts.n_rows, 100)
+    assert np.array_equal(res.means, om)
+    fin = np.isfinite(on)
+    assert np.array_equal(res.dispersions_norm[fin], on[fin])
+
+
+def _col_diff(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+def test_pca_synthetic_golden(ctx, counts):
+    hv = load_golden("synthetic_hvg")["highly_variable"]
+    gold = load_golden("synthetic_pca")
+    res = K.pca(counts.indptr, counts.indices, counts.values, counts.n_genes, 20, seed=0,
+                gene_set=hv, target_sum=1e4, log1p=True, ctx=ctx)
+    assert np.max(np.abs(res.variance - gold["variance"]) / gold["variance"]) <= 1e-3
+    ref = O.pca(O.normalize_log1p(counts), 20, 0, gene_set=hv)
+    assert np.max(np.abs(res.variance - ref.variance) / ref.variance) <= 1e-6
+    for c in range(20):
+        assert _col_diff(res.loadings[:, c], ref.loadings[:, c]) <= 1e-5
+        assert _col_diff(res.embedding[:, c], ref.embedding[:, c]) <= 1e-5
+    assert res.passes_run == ref.passes_run
+
+
+@pytest.fixture(scope="module")
+def planted():
+    x = synthetic.counts_csr(6000, 3000, 300, 12, 100, seed=1, dispersion=0.3)
+    return x
+
+
+def test_pca_planted_with_hvg_matches_oracle(ctx, planted):
+    x = planted
+    hv = K.highly_variable_genes(x.indptr, x.indices, x.values, x.n_genes, 1000, ctx=ctx)
+    logx = O.normalize_log1p(O.Csr(x.indptr, x.indices, x.values, x.n_genes))
+    s, q, p = O.hvg_moments(logx)
+    assert np.array_equal(hv.highly_variable, O.hvg_seurat(s, q, p, x.n_cells, 1000)[3])
+    res = K.pca(x.indptr, x.indices, x.values, x.n_genes, 50, seed=0,
+                gene_set=hv.highly_variable, target_sum=1e4, log1p=True, ctx=ctx)
+    ref = O.pca(logx, 50, 0, gene_set=hv.highly_variable)
+    rel = np.abs(res.variance - ref.variance) / ref.variance
+    assert rel.max() <= 1e-6, rel.max()
+    assert np.allclose(res.variance_ratio, ref.variance_ratio, rtol=1e-6)
+    for c in range(10):
+        assert _col_diff(res.embedding[:, c], ref.embedding[:, c]) <= 1e-5
+
+
+def test_pca_blocks_give_the_same_bits(ctx, planted):
+    x = planted
+    one = K.pca(x.indptr, x.indices, x.values, x.n_genes, 20, target_sum=1e4, log1p=True, ctx=ctx)
+    blocks = K.pca(x.indptr, x.indices, x.values, x.n_genes, 20, target_sum=1e4, log1p=True,
+                   block_cells=37, ctx=ctx)
+    again = K.pca(x.indptr, x.indices, x.values, x.n_genes, 20, target_sum=1e4, log1p=True, ctx=ctx)
+    assert np.array_equal(one.embedding, blocks.embedding)
+    assert np.array_equal(one.embedding, again.embedding)
+    assert np.array_equal(one.variance, again.variance)
+
+
+def test_pca_refusals(ctx):
+    indptr = np.array([0, 1], dtype=np.uint64)
+    with pytest.raises(K.KytoError) as e:
+        K.pca(indptr, np.array([0], np.uint32), np.array([1.0], np.float32), 3, 1, ctx=ctx)
+    assert e.value.code == "KY-E215"
+    indptr = np.array([0, 1, 2], dtype=np.uint64)
+    with pytest.raises(K.KytoError):
+        K.pca(indptr, np.array([0, 1], np.uint32), np.array([1.0, 2.0], np.float32), 3, 3, ctx=ctx)
+    with pytest.raises(K.KytoError):
+        K.pca(indptr, np.array([0, 1], np.uint32), np.array([1.0, np.nan], np.float32), 3, 1,
+              ctx=ctx)
+
+
+def test_pca_rank_deficient_completes_loadings(ctx):
+    # Two distinct cells: one direction of variance; kyto completes the loadings with
+    # orthonormal zero-variance directions (pca_dense.rs complement).
+    indptr = np.array([0, 2, 4, 6], dtype=np.uint64)
+    idx = np.array([0, 1, 0, 1, 0, 1], dtype=np.uint32)
+    val = np.array([1, 2, 1, 2, 3, 1], dtype=np.float32)
+    res = K.pca(indptr, idx, val, 4, 3, ctx=ctx)
+    ref = O.pca(O.Csr(indptr, idx, val, 4), 3)
+    np.testing.assert_allclose(res.variance, ref.variance, rtol=1e-9, atol=1e-12)
+    l = res.loadings.astype(np.float64)
+    np.testing.assert_allclose(l.T @ l, np.eye(3), atol=1e-6)
+
+
+def _graph_equal(gpu: K.Graph, cpu: O.Graph):
+    assert np.array_equal(gpu.indptr, cpu.indptr)
+    assert np.array_equal(gpu.indices, cpu.indices)
+    assert np.array_equal(gpu.distances.view(np.uint32), cpu.distances.view(np.uint32))
+
+
+def test_knn_pbmc3k_bits_and_scanpy(ctx):
+    g = load_golden("pbmc3k_neighbors")
+    gpu = K.neighbors(g["embedding"], 15, ctx=ctx)
+    _graph_equal(gpu, O.neighbors(g["embedding"], 15))
+    assert np.array_equal(gpu.indices.astype(np.int64), g["indices"])
+
+
+def test_knn_synthetic_duplicates(ctx):
+    emb = load_golden("synthetic_pca")["embedding"]
+    _graph_equal(K.neighbors(emb, 15, ctx=ctx), O.neighbors(emb, 15))
+
+
+def test_knn_clusters_ties_and_duplicates(ctx):
+    pts, _ = synthetic.gaussian_mixture(6000, 50, 40, seed=5, device="cpu")
+    pts[100:140] = pts[7]  # a block of exact duplicates (ties past the candidates)
+    pts[200:230] = np.round(pts[200:230])
+    _graph_equal(K.neighbors(pts, 31, ctx=ctx), O.neighbors(pts, 31))
+
+
+@pytest.mark.parametrize("n_neighbors,n_components", [(2, None), (16, 7), (64, 1)])
+def test_knn_edges(ctx, n_neighbors, n_components):
+    pts, _ = synthetic.gaussian_mixture(1500, 50, 10, seed=9, device="cpu")
+    ref_pts = pts if n_components is None else pts[:, :n_components]
+    gpu = K.neighbors(pts, n_neighbors, n_components, ctx=ctx)
+    _graph_equal(gpu, O.neighbors(ref_pts, n_neighbors))
+
+
+def test_knn_every_row_a_neighbour(ctx):
+    pts, _ = synthetic.gaussian_mixture(97, 20, 3, seed=2, device="cpu")
+    _graph_equal(K.neighbors(pts, 97, ctx=ctx), O.neighbors(pts, 97))
+
+
+def test_knn_line_known_answer(ctx):
+    g = K.neighbors(np.array([[0.0], [1.0], [3.0], [7.0]], np.float32), 3, ctx=ctx)
+    assert g.indices.tolist() == [1, 2, 0, 2, 0, 1, 1, 2]
+    assert g.distances.tolist() == [1.0, 3.0, 1.0, 2.0, 3.0, 2.0, 6.0, 4.0]
+
+
+def test_knn_refusals(ctx):
+    pts = np.zeros((5, 3), np.float32)
+    for bad in (1, 6):
+        with pytest.raises(K.KytoError) as e:
+            K.neighbors(pts, bad, ctx=ctx)
+        assert e.value.code == "KY-E215"
+    pts[2, 1] = np.nan
+    with pytest.raises(K.KytoError) as e:
+        K.neighbors(pts, 2, ctx=ctx)
+    assert "row 2, component 1" in str(e.value)
+
+
+def test_knn_huge_norms_search_every_row(ctx):
+    pts, _ = synthetic.gaussian_mixture(300, 8, 3, seed=4, device="cpu")
+    pts[5] = 1e18
+    gpu = K.neighbors(pts, 5, ctx=ctx)
+    _graph_equal(gpu, O.neighbors(pts, 5))
+    assert gpu.stats.rows_full == 300
