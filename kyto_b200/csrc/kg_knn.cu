@@ -18,8 +18,12 @@
 #include <cmath>
 #include <vector>
 
+#include <cstdlib>
+#include <string>
+
 #include "kg_internal.cuh"
 #include "kg_knn.cuh"
+#include "kg_knn_tc.cuh"
 
 namespace kg {
 
@@ -72,6 +76,11 @@ __global__ void max_kernel(const double* v, uint64_t n, double* out) {
     __syncthreads();
   }
   if (threadIdx.x == 0) *out = red[0];
+}
+
+void max_kernel_launch(const double* v, uint64_t n, double* out, cudaStream_t s) {
+  max_kernel<<<1, 256, 0, s>>>(v, n, out);
+  KG_LAUNCH_CHECK();
 }
 
 // kyto's slack E_q = 2 (w + 8) u (|a_q| + max |a|)^2 + 4 (w + 8) FLT_MIN
@@ -260,11 +269,15 @@ __device__ void warp_merge(const double* keys, const uint32_t* idx, uint32_t len
 // One warp per query: exact keys of its candidates, the k best by (key, row). A row
 // that overflowed, holds fewer than k candidates or has a candidate outside its slack
 // is flagged for a full search (kyto's rank, neighbors_exact.rs:318-340).
+// An approximate key a stands for the squared distance a * inv_s2 + qn2[q] (the
+// tensor-core filter's keys are scaled and shifted by the query's norm; the SIMT
+// filter's are distances already: inv_s2 = 1, qn2 = NULL).
 __global__ void rank_kernel(const float* __restrict__ x, uint32_t width, uint32_t d,
                             uint64_t q_begin, uint64_t q_end, uint32_t k, uint32_t cap,
                             const float* cand_key, const uint32_t* cand_row,
                             const uint32_t* cand_count, const float* threshold,
-                            const double* slack, double* out_key, uint32_t* out_row,
+                            const double* slack, double inv_s2, const double* qn2,
+                            double* out_key, uint32_t* out_row,
                             uint32_t* full_flag, unsigned long long* n_candidates) {
   uint64_t qi = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   unsigned lane = threadIdx.x & 31u;
@@ -277,6 +290,7 @@ __global__ void rank_kernel(const float* __restrict__ x, uint32_t width, uint32_
   }
   float th = threshold[qi];
   double sl = slack[q];
+  double shift = qn2 ? qn2[q] : 0.0;
   const float* qrow = x + q * width;
   double keys[kMaxK];
   uint32_t idx[kMaxK];
@@ -288,7 +302,7 @@ __global__ void rank_kernel(const float* __restrict__ x, uint32_t width, uint32_
     if (ak > th) continue;
     uint32_t p = cand_row[qi * (uint64_t)cap + c];
     double e = exact_key(qrow, x + (uint64_t)p * width, d);
-    if (fabs(e - (double)ak) > sl) bad = true;
+    if (fabs(e - ((double)ak * inv_s2 + shift)) > sl) bad = true;
     offer(keys, idx, len, k, e, p);
     ++used;
   }
@@ -464,10 +478,36 @@ extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t 
     DeviceBuffer<unsigned long long> n_cand(1, s);
     n_cand.zero();
     double filter_ms = 0, rank_ms = 0;
+    // The filter: the tensor-core GEMM (fp16, or bf16 on request) when the components
+    // and the three norm columns fit one 64-wide operand row; the SIMT filter otherwise
+    // or on request (KYTO_GPU_KNN_FILTER=simt|fp16|bf16). All give the same graph.
+    const char* choice = std::getenv("KYTO_GPU_KNN_FILTER");
+    std::string filter = choice ? choice : "fp16";
+    bool tc = !brute && d + 3 <= 64 && (filter == "fp16" || filter == "bf16");
     if (brute) {
       uint32_t one = 1;
       std::vector<uint32_t> all(n, one);
       KG_CUDA(cudaMemcpyAsync(full_flag.ptr, all.data(), n * 4, cudaMemcpyHostToDevice, s));
+    } else if (tc) {
+      check_cancel(ctx);
+      const uint32_t cap = kTcCap;
+      DeviceBuffer<float> cand_key(n * cap, s), thr(n, s);
+      DeviceBuffer<uint32_t> cand_row(n * cap, s), cand_count(n, s);
+      DeviceBuffer<double> qn2(n, s), slack_d(n, s);
+      double scale = 1.0;
+      Timer tf(s);
+      tc_filter(ctx, s, x, n, width, d, mean.ptr, filter == "bf16", k, cap, cand_key.ptr,
+                cand_row.ptr, cand_count.ptr, thr.ptr, qn2.ptr, slack_d.ptr, &scale);
+      filter_ms += tf.stop_ms();
+      check_cancel(ctx);
+      Timer tr(s);
+      rank_kernel<<<blocks_for(n * 32, kRankWarps * 32), kRankWarps * 32, 0, s>>>(
+          x, width, d, 0, n, k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
+          slack_d.ptr, 1.0 / (scale * scale), qn2.ptr, out_key.ptr, out_row.ptr,
+          full_flag.ptr, n_cand.ptr);
+      KG_LAUNCH_CHECK();
+      rank_ms += tr.stop_ms();
+      ctx->done = n;
     } else {
       const uint32_t cap = kCandidateCap;
       uint64_t chunk = std::min<uint64_t>(n, kQueryChunk);
@@ -485,7 +525,7 @@ extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t 
         Timer tr(s);
         rank_kernel<<<blocks_for((q1 - q0) * 32, kRankWarps * 32), kRankWarps * 32, 0, s>>>(
             x, width, d, q0, q1, k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
-            slack.ptr, out_key.ptr, out_row.ptr, full_flag.ptr, n_cand.ptr);
+            slack.ptr, 1.0, nullptr, out_key.ptr, out_row.ptr, full_flag.ptr, n_cand.ptr);
         KG_LAUNCH_CHECK();
         rank_ms += tr.stop_ms();
         ctx->done = q1;

@@ -1,0 +1,443 @@
+// The exact-kNN candidate filter on the 5th-generation tensor cores (tcgen05, TMEM,
+// TMA). It computes, for every (query, point) pair, an approximate key
+//     A = |p|^2 - 2 q.p      (rows centred on the mean and scaled by a power of two)
+// as ONE fp16 (or bf16) GEMM with f32 accumulation: the query operand is
+// [-2 q, 1, 1, 1, 0...] and the point operand [p, h1, h2, h3, 0...] with h1+h2+h3 the
+// point's squared norm split into three fp16 parts, so the norm is added by the tensor
+// core and the epilogue reads finished keys straight from TMEM. The epilogue keeps
+// kyto's filter state per query (neighbors_exact.rs:216-255): its k smallest keys and
+// every point within twice the proven slack of the k-th, appended to the query's
+// candidate slice. Candidates are then ranked by exact f64 keys (kg_knn.cu).
+//
+// CTA layout (one persistent CTA per SM, 320 threads):
+//   warps 0-7  epilogue: thread t owns query t of the CTA's 256-query block (TMEM lane
+//              32*(warp%4)+lane of accumulator warp/4);
+//   warp 8     TMA producer: the block's two 128-query operand tiles, then 128-point
+//              tiles through a ring of kStages shared-memory stages;
+//   warp 9     MMA issuer: per point tile, two M=128 N=128 K=64 products (one per
+//              128-query half) into one of two TMEM accumulator buffers.
+// TMEM: 2 buffers x (2 halves x 128 columns) = 512 columns, f32.
+#include <cudaTypedefs.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "kg_internal.cuh"
+#include "kg_knn.cuh"
+#include "kg_knn_tc.cuh"
+#include "kg_sm100.cuh"
+
+namespace kg {
+
+using namespace sm100;
+
+constexpr int kTcQueries = 256;
+constexpr int kTcPoints = 128;
+constexpr int kTcK = 64;  // operand width (fp16 elements, one 128-byte swizzle row)
+constexpr int kStages = 6;
+constexpr uint32_t kTileBytes = 128u * 128u;  // 128 rows x 64 fp16
+constexpr int kEpiWarps = 8;
+constexpr int kTcThreads = (kEpiWarps + 2) * 32;
+constexpr uint32_t kTmemCols = 512;
+
+struct TcSmem {
+  uint8_t a[2][kTileBytes];          // the query block's two operand tiles
+  uint8_t b[kStages][kTileBytes];    // point tiles
+  float scratch[kEpiWarps * 32][33]; // a thread's 32 keys when some may pass
+  uint64_t full[kStages], empty[kStages];
+  uint64_t tmem_full[2], tmem_empty[2];
+  uint64_t a_full, a_empty, drained;
+  uint32_t tmem_base;
+  int abort;
+};
+constexpr size_t kTcSmemBytes = sizeof(TcSmem) + 1024;  // + alignment slack
+
+__device__ __forceinline__ float round_up_f32d(double v) {
+  float r = (float)v;
+  if ((double)r < v) r = nextafterf(r, INFINITY);
+  return r;
+}
+
+// Per-query filter state (kyto's Query, neighbors_exact.rs:196-255).
+struct QueryState {
+  float th;
+  uint32_t n_small, count, compact_at;
+  bool overflowed;
+};
+
+// Offer approximate key `key` of point `p` (already <= st.th) to the query's state.
+__device__ __noinline__ void tc_offer(QueryState& st, float* smallest, uint32_t k,
+                                      double slack2, float key, uint32_t p, float* ck,
+                                      uint32_t* cr, uint32_t cap) {
+  if (st.n_small < k || key < smallest[k - 1]) {
+    if (st.n_small < k) ++st.n_small;
+    uint32_t at = st.n_small - 1;
+    while (at > 0 && smallest[at - 1] > key) {
+      smallest[at] = smallest[at - 1];
+      --at;
+    }
+    smallest[at] = key;
+    if (st.n_small == k) st.th = round_up_f32d((double)smallest[k - 1] + slack2);
+  }
+  if (!(key <= st.th)) return;
+  if (st.count == cap) {
+    st.overflowed = true;
+    return;
+  }
+  ck[st.count] = key;
+  cr[st.count] = p;
+  ++st.count;
+  if (st.count >= st.compact_at) {
+    uint32_t kept = 0;
+    for (uint32_t i = 0; i < st.count; ++i) {
+      float v = ck[i];
+      if (v <= st.th) {
+        ck[kept] = v;
+        cr[kept] = cr[i];
+        ++kept;
+      }
+    }
+    st.count = kept;
+    if (st.count > kTcCandidateLimit) st.overflowed = true;
+    st.compact_at = min(max(2 * st.count, 64u), cap);
+  }
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
+                     const __grid_constant__ CUtensorMap tmap_p, uint64_t n, uint32_t k,
+                     const float* __restrict__ slack2, uint32_t idesc, uint32_t cap,
+                     float* cand_key, uint32_t* cand_row, uint32_t* cand_count,
+                     float* threshold_out, int* error) {
+  extern __shared__ uint8_t smem_raw[];
+  TcSmem& sm = *reinterpret_cast<TcSmem*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const uint64_t n_qblocks = (n + kTcQueries - 1) / kTcQueries;
+  const uint32_t n_tiles = (uint32_t)((n + kTcPoints - 1) / kTcPoints);
+  volatile int* abort = &sm.abort;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < kStages; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&sm.tmem_full[b], 1);
+      mbar_init(&sm.tmem_empty[b], kEpiWarps);
+    }
+    mbar_init(&sm.a_full, 1);
+    mbar_init(&sm.a_empty, 1);
+    mbar_init(&sm.drained, 1);
+    sm.abort = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0) tmem_alloc(&sm.tmem_base, kTmemCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sm.tmem_base;
+
+  if (warp == kEpiWarps) {
+    // ------------------------------------------------------------ TMA producer ----
+    if (lane == 0) {
+      prefetch_tmap(&tmap_q);
+      prefetch_tmap(&tmap_p);
+      uint64_t it = 0;
+      uint32_t bi = 0;
+      int issued_phase[kStages];
+      for (int s = 0; s < kStages; ++s) issued_phase[s] = -1;
+      bool ok = true;
+      for (uint64_t qb = blockIdx.x; qb < n_qblocks && ok; qb += gridDim.x, ++bi) {
+        if (!mbar_wait(&sm.a_empty, (bi & 1) ^ 1, abort)) break;
+        mbar_arrive_expect_tx(&sm.a_full, 2 * kTileBytes);
+        tma_load_2d(sm.a[0], &tmap_q, &sm.a_full, 0, (int32_t)(qb * kTcQueries));
+        tma_load_2d(sm.a[1], &tmap_q, &sm.a_full, 0, (int32_t)(qb * kTcQueries + 128));
+        for (uint32_t t = 0; t < n_tiles; ++t, ++it) {
+          int s = (int)(it % kStages);
+          uint32_t ph = (uint32_t)((it / kStages) & 1);
+          if (!mbar_wait(&sm.empty[s], ph ^ 1, abort)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&sm.full[s], kTileBytes);
+          tma_load_2d(sm.b[s], &tmap_p, &sm.full[s], 0, (int32_t)(t * kTcPoints));
+          issued_phase[s] = (int)ph;
+        }
+      }
+      // Every load issued has landed before the CTA may leave (bounded, own loop).
+      for (int s = 0; s < kStages; ++s) {
+        if (issued_phase[s] < 0) continue;
+        for (uint32_t i = 0; i < kWaitPolls && !mbar_try_wait(&sm.full[s], issued_phase[s]); ++i)
+          __nanosleep(64);
+      }
+    }
+  } else if (warp == kEpiWarps + 1) {
+    // ------------------------------------------------------------ MMA issuer ------
+    if (lane == 0) {
+      uint64_t it = 0;
+      uint32_t bi = 0;
+      bool ok = true;
+      const uint32_t a0 = smem_addr(sm.a[0]), a1 = smem_addr(sm.a[1]);
+      for (uint64_t qb = blockIdx.x; qb < n_qblocks && ok; qb += gridDim.x, ++bi) {
+        if (!mbar_wait(&sm.a_full, bi & 1, abort)) break;
+        tc_fence_after();
+        for (uint32_t t = 0; t < n_tiles; ++t, ++it) {
+          int s = (int)(it % kStages);
+          uint32_t ph = (uint32_t)((it / kStages) & 1);
+          uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
+          if (!mbar_wait(&sm.tmem_empty[ab], aph ^ 1, abort) ||
+              !mbar_wait(&sm.full[s], ph, abort)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t bsm = smem_addr(sm.b[s]);
+          const uint32_t d0 = tmem + ab * 256u, d1 = d0 + 128u;
+#pragma unroll
+          for (int kk = 0; kk < kTcK / 16; ++kk) {
+            const uint64_t bd = desc_k_sw128(bsm + kk * 32);
+            mma_f16(d0, desc_k_sw128(a0 + kk * 32), bd, idesc, kk > 0);
+            mma_f16(d1, desc_k_sw128(a1 + kk * 32), bd, idesc, kk > 0);
+          }
+          mma_commit(&sm.empty[s]);
+          mma_commit(&sm.tmem_full[ab]);
+        }
+        if (ok) mma_commit(&sm.a_empty);
+      }
+      // No product may still be running when TMEM is released.
+      mma_commit(&sm.drained);
+      for (uint32_t i = 0; i < kWaitPolls && !mbar_try_wait(&sm.drained, 0); ++i) __nanosleep(64);
+    }
+  } else {
+    // ------------------------------------------------------------ epilogue --------
+    const uint32_t half = (uint32_t)warp >> 2, quad = (uint32_t)warp & 3;
+    float* my = sm.scratch[threadIdx.x];
+    float smallest[kMaxK];
+    uint64_t it = 0;
+    bool ok = true;
+    for (uint64_t qb = blockIdx.x; qb < n_qblocks && ok; qb += gridDim.x) {
+      const uint64_t q = qb * kTcQueries + half * 128 + quad * 32 + lane;
+      const bool active = q < n;
+      QueryState st{INFINITY, 0, 0, 64, false};
+      const double sl2 = active ? (double)slack2[q] : 0.0;
+      float* ck = cand_key + (active ? q : 0) * (uint64_t)cap;
+      uint32_t* cr = cand_row + (active ? q : 0) * (uint64_t)cap;
+      for (uint32_t t = 0; t < n_tiles; ++t, ++it) {
+        uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
+        if (!mbar_wait(&sm.tmem_full[ab], aph, abort)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+#pragma unroll 1
+        for (int c = 0; c < kTcPoints / 32; ++c) {
+          __syncwarp();
+          float v[32];
+          tmem_load_32(tmem + ((quad * 32u) << 16) + ab * 256u + half * 128u + c * 32u, v);
+          if (active && !st.overflowed) {
+            float m = v[0];
+#pragma unroll
+            for (int j = 1; j < 32; ++j) m = fminf(m, v[j]);
+            if (m <= st.th) {
+#pragma unroll
+              for (int j = 0; j < 32; ++j) my[j] = v[j];
+              const uint64_t p0 = (uint64_t)t * kTcPoints + c * 32;
+              for (int j = 0; j < 32; ++j) {
+                float key = my[j];
+                uint64_t p = p0 + j;
+                if (key <= st.th && p < n && p != q && !st.overflowed)
+                  tc_offer(st, smallest, k, sl2, key, (uint32_t)p, ck, cr, cap);
+              }
+            }
+          }
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.tmem_empty[ab]);
+      }
+      if (active && ok) {
+        cand_count[q] = st.overflowed ? kOverflow : st.count;
+        threshold_out[q] = st.th;
+      }
+    }
+  }
+  __syncwarp();
+  __syncthreads();
+  if (sm.abort && threadIdx.x == 0) atomicExch(error, 1);
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, kTmemCols);
+  }
+}
+
+// ------------------------------------------------------------------ operands -------
+
+// Rows centred (f64) and scaled by 2^e: the query operand [-2 q, 1, 1, 1, 0...] and the
+// point operand [p, h1, h2, h3, 0...] (fp16 or bf16), each row's centred squared norm
+// (unscaled, f64) and the row's doubled slack in scaled units.
+template <class H>
+__global__ void tc_operands_kernel(const float* x, uint64_t n, uint32_t width, uint32_t d,
+                                   const double* mean, double scale, double u, double eta,
+                                   const double* max_sq, H* aq, H* bp, double* qn2,
+                                   float* slack2, double* slack_d) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double n2 = 0.0, n2s = 0.0;
+  for (uint32_t j = 0; j < kTcK; ++j) {
+    H a = H(0.0f), b = H(0.0f);
+    if (j < d) {
+      double c = (double)x[r * width + j] - mean[j];
+      double cs = c * scale;
+      n2 += c * c;
+      n2s += cs * cs;
+      b = H((float)cs);
+      a = H(-2.0f * (float)b);  // exact: a power-of-two multiple of a 16-bit value
+    }
+    aq[r * kTcK + j] = a;
+    bp[r * kTcK + j] = b;
+  }
+  // The squared norm in three parts (each rounded from what the previous left).
+  double r1 = n2s;
+  H h1 = H((float)r1);
+  double r2 = r1 - (double)(float)h1;
+  H h2 = H((float)r2);
+  double r3 = r2 - (double)(float)h2;
+  H h3 = H((float)r3);
+  bp[r * kTcK + d] = h1;
+  bp[r * kTcK + d + 1] = h2;
+  bp[r * kTcK + d + 2] = h3;
+  aq[r * kTcK + d] = H(1.0f);
+  aq[r * kTcK + d + 1] = H(1.0f);
+  aq[r * kTcK + d + 2] = H(1.0f);
+  qn2[r] = n2;
+  // The bound of |A - s^2 (D - |q|^2)| (scaled units), D the exact squared distance:
+  // quantisation 2(2u + u^2)|q||p| + 2 eta sqrt(d)(|q| + |p|) + 2 d eta^2, the norm's
+  // three parts u^3 |p|^2 + 2 eta, the f32 accumulation gamma (2|q||p| + |p|^2) with
+  // gamma = 2^-17 (64 terms, truncating adds), and f64 rounding of the exact key; |p|
+  // bounded by the largest row norm R. Doubled, as kyto doubles its own.
+  const double gamma = 0x1p-17, tiny = 0x1p-40;
+  double qs = sqrt(n2s), rs = sqrt(*max_sq) * scale;
+  double e = 2.0 * (2.0 * u + u * u) * qs * rs + 2.0 * eta * sqrt((double)d) * (qs + rs) +
+             2.0 * d * eta * eta + 2.0 * u * u * u * rs * rs + 2.0 * eta +
+             gamma * (2.02 * qs * rs + 1.02 * rs * rs) + tiny * (qs + rs) * (qs + rs);
+  e *= 2.0;
+  slack_d[r] = e / (scale * scale);
+  slack2[r] = round_up_f32d(2.0 * e);
+}
+
+// The largest centred squared norm, f64.
+__global__ void centred_norm_kernel(const float* x, uint64_t n, uint32_t width, uint32_t d,
+                                    const double* mean, double* sq) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  double s = 0.0;
+  for (uint32_t j = 0; j < d; ++j) {
+    double c = (double)x[r * width + j] - mean[j];
+    s += c * c;
+  }
+  sq[r] = s;
+}
+
+// ------------------------------------------------------------------ host -----------
+
+namespace {
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault,
+                                         &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  if (!fn) fail(KG_ERR_DEVICE, "cuTensorMapEncodeTiled is not available from the driver");
+  return fn;
+}
+
+// A [rows x 64] 16-bit row-major matrix, boxes of 128 rows x 64 (one 128-byte swizzle
+// row each), zero fill past the last row.
+CUtensorMap tile_map(const void* base, uint64_t rows, bool bf16) {
+  CUtensorMap m;
+  std::memset(&m, 0, sizeof(m));
+  cuuint64_t dims[2] = {(cuuint64_t)kTcK, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)kTcK * 2};
+  cuuint32_t box[2] = {(cuuint32_t)kTcK, 128};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = encode_fn()(&m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
+                           2, const_cast<void*>(base), dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) fail(KG_ERR_DEVICE, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+  return m;
+}
+
+}  // namespace
+
+void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint64_t n, uint32_t width,
+               uint32_t d, const double* mean, bool bf16, uint32_t k, uint32_t cap,
+               float* cand_key, uint32_t* cand_row, uint32_t* cand_count, float* threshold,
+               double* qn2, double* slack_d, double* out_scale) {
+  if (d + 3 > (uint32_t)kTcK) fail(KG_ERR_INVALID, "tensor-core filter: more than 61 components");
+  DeviceBuffer<double> sq(n, s), max_sq(1, s);
+  centred_norm_kernel<<<blocks_for(n, 256), 256, 0, s>>>(x, n, width, d, mean, sq.ptr);
+  KG_LAUNCH_CHECK();
+  max_kernel_launch(sq.ptr, n, max_sq.ptr, s);
+  double h_max = 0.0;
+  KG_CUDA(cudaMemcpyAsync(&h_max, max_sq.ptr, 8, cudaMemcpyDeviceToHost, s));
+  KG_CUDA(cudaStreamSynchronize(s));
+  // Scale so that the largest centred row norm is at most 2^7: squared norms stay below
+  // 2^14 (fp16's range) and -2q below 2^8.
+  double scale = 1.0;
+  if (h_max > 0.0 && std::isfinite(h_max)) {
+    int e = 0;
+    std::frexp(std::sqrt(h_max), &e);  // sqrt(h_max) < 2^e
+    int shift = std::max(-1000, std::min(1000, 7 - e));
+    scale = std::ldexp(1.0, shift);
+  }
+  *out_scale = scale;
+  const double u = bf16 ? 0x1p-8 : 0x1p-11;
+  const double eta = bf16 ? 0x1p-134 : 0x1p-25;
+  DeviceBuffer<uint16_t> aq(n * kTcK, s), bp(n * kTcK, s);
+  DeviceBuffer<float> slack2(n, s);
+  if (bf16)
+    tc_operands_kernel<__nv_bfloat16><<<blocks_for(n, 128), 128, 0, s>>>(
+        x, n, width, d, mean, scale, u, eta, max_sq.ptr, (__nv_bfloat16*)aq.ptr,
+        (__nv_bfloat16*)bp.ptr, qn2, slack2.ptr, slack_d);
+  else
+    tc_operands_kernel<__half><<<blocks_for(n, 128), 128, 0, s>>>(
+        x, n, width, d, mean, scale, u, eta, max_sq.ptr, (__half*)aq.ptr, (__half*)bp.ptr,
+        qn2, slack2.ptr, slack_d);
+  KG_LAUNCH_CHECK();
+  CUtensorMap mq = tile_map(aq.ptr, n, bf16), mp = tile_map(bp.ptr, n, bf16);
+  static std::once_flag attr;
+  std::call_once(attr, [] {
+    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kTcSmemBytes));
+  });
+  DeviceBuffer<int> err(1, s);
+  err.zero();
+  uint64_t n_qblocks = (n + kTcQueries - 1) / kTcQueries;
+  unsigned grid = (unsigned)std::min<uint64_t>(n_qblocks, (uint64_t)ctx->sm_count);
+  uint32_t idesc = idesc_f32acc(bf16 ? 1u : 0u, 128, kTcPoints);
+  knn_filter_tc_kernel<<<grid, kTcThreads, kTcSmemBytes, s>>>(
+      mq, mp, n, k, slack2.ptr, idesc, cap, cand_key, cand_row, cand_count, threshold, err.ptr);
+  KG_LAUNCH_CHECK();
+  int h_err = 0;
+  KG_CUDA(cudaMemcpyAsync(&h_err, err.ptr, 4, cudaMemcpyDeviceToHost, s));
+  wait_stream(ctx, s);
+  if (h_err) fail(KG_ERR_TIMEOUT, "the tensor-core kNN filter gave up waiting on its pipeline");
+}
+
+}  // namespace kg

@@ -173,6 +173,25 @@ def test_knn_clusters_ties_and_duplicates(ctx):
     _graph_equal(K.neighbors(pts, 31, ctx=ctx), O.neighbors(pts, 31))
 
 
+@pytest.mark.parametrize("candidate_filter", ["fp16", "bf16", "simt"])
+def test_knn_every_filter_gives_the_exact_graph(ctx, monkeypatch, candidate_filter):
+    # The tensor-core filter in fp16 or bf16 (wider slack, more candidates) and the
+    # SIMT f32 filter all end in the same exact ranking.
+    monkeypatch.setenv("KYTO_GPU_KNN_FILTER", candidate_filter)
+    pts, _ = synthetic.gaussian_mixture(5000, 50, 30, seed=11, device="cpu")
+    pts[40:60] = pts[3]
+    gpu = K.neighbors(pts, 16, ctx=ctx)
+    _graph_equal(gpu, O.neighbors(pts, 16))
+    assert gpu.stats.candidates >= 5000 * 15
+
+
+def test_knn_tensor_core_tiles_past_the_end(ctx):
+    # n not a multiple of the 128-point tile or the 256-query block; one CTA per SM
+    # walks several query blocks (more blocks than SMs).
+    pts, _ = synthetic.gaussian_mixture(148 * 256 + 77, 12, 25, seed=12, device="cpu")
+    _graph_equal(K.neighbors(pts, 10, ctx=ctx), O.neighbors(pts, 10))
+
+
 @pytest.mark.parametrize("n_neighbors,n_components", [(2, None), (16, 7), (64, 1)])
 def test_knn_edges(ctx, n_neighbors, n_components):
     pts, _ = synthetic.gaussian_mixture(1500, 50, 10, seed=9, device="cpu")
