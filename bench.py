@@ -238,7 +238,10 @@ def main() -> int:
     start.record()
     filter_ms = []
     for _ in range(args.steps):
+        # The range names the timed steps for a profiler's launch list (ncu --nvtx).
+        torch.cuda.nvtx.range_push("kyto_step")
         st = run_step(args, ctx, d_indptr, d_idx, d_vals, out_dev, host=False)
+        torch.cuda.nvtx.range_pop()
         filter_ms.append(st.filter_ms)
     stop.record()
     barrier()

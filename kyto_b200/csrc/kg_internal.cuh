@@ -9,7 +9,10 @@
 #include <atomic>
 #include <chrono>
 #include <cstdint>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <vector>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -192,6 +195,52 @@ inline void wait_stream(kg_ctx* ctx, cudaStream_t stream) {
   }
   cudaEventDestroy(ev);
 }
+
+// Phase timings of a call, on its stream, printed to stderr when KYTO_GPU_TRACE is set
+// (one line per call: phase name, count, total ms). Costs nothing when unset.
+struct Trace {
+  bool on = false;
+  cudaStream_t s = nullptr;
+  std::string what;
+  std::vector<std::pair<std::string, cudaEvent_t>> marks;
+  Trace(cudaStream_t st, const char* call) : s(st), what(call) {
+    on = std::getenv("KYTO_GPU_TRACE") != nullptr;
+    mark("start");
+  }
+  void mark(const char* name) {
+    if (!on) return;
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return;
+    cudaEventRecord(e, s);
+    marks.emplace_back(name, e);
+  }
+  ~Trace() {
+    if (!on || marks.empty()) return;
+    cudaEventSynchronize(marks.back().second);
+    std::vector<std::pair<std::string, std::pair<int, double>>> acc;
+    for (size_t i = 1; i < marks.size(); ++i) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, marks[i - 1].second, marks[i].second);
+      bool found = false;
+      for (auto& a : acc)
+        if (a.first == marks[i].first) {
+          a.second.first += 1;
+          a.second.second += ms;
+          found = true;
+        }
+      if (!found) acc.push_back({marks[i].first, {1, ms}});
+    }
+    std::string line = "[kyto_gpu trace] " + what + ":";
+    for (auto& a : acc) {
+      char buf[128];
+      std::snprintf(buf, sizeof buf, " %s x%d %.3f ms;", a.first.c_str(), a.second.first,
+                    a.second.second);
+      line += buf;
+    }
+    std::fprintf(stderr, "%s\n", line.c_str());
+    for (auto& m : marks) cudaEventDestroy(m.second);
+  }
+};
 
 template <class F>
 kg_status guarded(F&& body) {

@@ -460,6 +460,7 @@ extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t 
                                  ", component " + std::to_string(first % width) +
                                  " is not finite");
     }
+    Trace trace(s, "knn_exact");
     DeviceBuffer<double> mean(d, s), squares(n, s), slack(n, s), largest(1, s);
     DeviceBuffer<float> rows(n * kDim, s), offsets(n, s);
     column_mean_kernel<<<blocks_for(d, 64), 64, 0, s>>>(x, n, width, d, mean.ptr);
@@ -531,6 +532,7 @@ extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t 
         ctx->done = q1;
       }
     }
+    trace.mark("filter + rank");
     // Rows that need a full search.
     DeviceBuffer<uint32_t> list(n, s);
     DeviceBuffer<unsigned int> n_full(1, s);
@@ -553,6 +555,7 @@ extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t 
       }
       rank_ms += tr.stop_ms();
     }
+    trace.mark("full rows");
     // The CSR graph.
     DeviceBuffer<uint64_t> g_indptr;
     DeviceBuffer<uint32_t> g_idx;
@@ -576,6 +579,7 @@ extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t 
       KG_CUDA(cudaMemcpyAsync(indices, gx, n * k * 4, cudaMemcpyDeviceToHost, s));
       KG_CUDA(cudaMemcpyAsync(distances, gd, n * k * 4, cudaMemcpyDeviceToHost, s));
     }
+    trace.mark("graph");
     unsigned long long h_cand = 0;
     KG_CUDA(cudaMemcpyAsync(&h_cand, n_cand.ptr, 8, cudaMemcpyDeviceToHost, s));
     wait_stream(ctx, s);

@@ -168,6 +168,9 @@ void sort_by_gene(const uint32_t* genes, const P* payload, uint64_t nnz, uint32_
 template void sort_by_gene<uint32_t>(const uint32_t*, const uint32_t*, uint64_t, uint32_t,
                                      DeviceBuffer<uint32_t>&, DeviceBuffer<uint32_t>&,
                                      cudaStream_t);
+template void sort_by_gene<uint64_t>(const uint32_t*, const uint64_t*, uint64_t, uint32_t,
+                                     DeviceBuffer<uint32_t>&, DeviceBuffer<uint64_t>&,
+                                     cudaStream_t);
 
 void column_starts(const uint32_t* sorted_genes, uint64_t nnz, uint32_t n_genes,
                    uint64_t* colptr, cudaStream_t stream) {

@@ -9,6 +9,9 @@
 // (Omega, W, the embedding rows) are row-major n x w.
 #include <cub/device/device_scan.cuh>
 
+#include <cstdlib>
+#include <string>
+
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -16,6 +19,7 @@
 #include "kg_internal.cuh"
 #include "kg_maps.cuh"
 #include "kg_spmm.cuh"
+#include "kg_spmm_tc.cuh"
 
 namespace kg {
 
@@ -323,6 +327,260 @@ __global__ void divide_kernel(const double* in, uint32_t n, double d, double* ou
   if (i < n) out[i] = in[i] / d;
 }
 
+// ------------------------------------------------ tensor-core product support -------
+
+__device__ __forceinline__ float tf32_rna(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// D^T in two tf32 parts from a g x w column-major f64 matrix: t[j][r] for j < 64,
+// r < ld (zero past w columns and g rows).
+__global__ void split_t_kernel(const double* cm, uint32_t g, uint32_t w, uint64_t ld,
+                               float* t_hi, float* t_lo) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= 64 * ld) return;
+  uint32_t j = (uint32_t)(i / ld);
+  uint64_t r = i % ld;
+  double v = (j < w && r < g) ? cm[(uint64_t)j * g + r] : 0.0;
+  float hi = tf32_rna((float)v);
+  t_hi[i] = hi;
+  t_lo[i] = tf32_rna((float)(v - (double)hi));
+}
+
+// Omega^T beside a row of ones (the gene sums), two tf32 parts, 64 x ld; and each
+// block's Omega column sums (of the parts, f64, a fixed tree) for the centring.
+__global__ void omega_t_kernel(const uint64_t* cells, uint64_t n, uint32_t width,
+                               uint64_t seed, uint64_t ld, float* t_hi, float* t_lo,
+                               double* block_sums) {
+  __shared__ double red[8][64];
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  bool live = r < n;
+  uint64_t state = live ? splitmix_mix(seed ^ splitmix_mix(cells[r] + 0x9E3779B97F4A7C15ull)) : 0;
+  const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  for (uint32_t j = 0; j < 64; ++j) {
+    float hi = 0.0f, lo = 0.0f;
+    if (live && j < width) {
+      state += 0x9E3779B97F4A7C15ull;
+      double om = __dadd_rn((double)(splitmix_mix(state) >> 11) * 0x1p-52, -1.0);
+      hi = tf32_rna((float)om);
+      lo = tf32_rna((float)(om - (double)hi));
+    } else if (live && j == width) {
+      hi = 1.0f;
+    }
+    if (r < ld) {
+      t_hi[(uint64_t)j * ld + r] = hi;
+      t_lo[(uint64_t)j * ld + r] = lo;
+    }
+    if (j < width) {
+      double sv = (double)hi + (double)lo;
+      for (int o = 16; o; o >>= 1) sv += __shfl_xor_sync(0xFFFFFFFFu, sv, o);
+      if (lane == 0) red[warp][j] = sv;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < width) {
+    double t = 0.0;
+    for (unsigned w8 = 0; w8 < blockDim.x / 32; ++w8) t += red[w8][threadIdx.x];
+    block_sums[blockIdx.x * (uint64_t)64 + threadIdx.x] = t;
+  }
+}
+
+// out[j] = sum over blocks (in order) of partial[b][j], j < w.
+__global__ void sum_blocks_kernel(const double* partial, uint64_t nb, uint32_t w, double* out) {
+  uint32_t j = threadIdx.x;
+  if (j >= w) return;
+  double t = 0.0;
+  for (uint64_t b = 0; b < nb; ++b) t += partial[b * 64 + j];
+  out[j] = t;
+}
+
+// out (g x w column-major) = sum over segments (in order) of partial[seg][gene][j].
+__global__ void reduce_segments_kernel(const double* partial, uint32_t segs, uint32_t g,
+                                       uint32_t w, double* out) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= (uint64_t)g * w) return;
+  uint32_t gene = (uint32_t)(i / w), j = (uint32_t)(i % w);
+  double t = 0.0;
+  for (uint32_t sg = 0; sg < segs; ++sg) t += partial[((uint64_t)sg * g + gene) * 64 + j];
+  out[(uint64_t)j * g + gene] = t;
+}
+
+// Each gene's sum of (x - mean)^2 over its stored values: a warp per gene, lanes over
+// the gene's entries in order, then a fixed shuffle tree.
+__global__ void gene_squares_kernel(const uint64_t* ptr, const float* val, const double* means,
+                                    uint32_t g, double* out) {
+  uint64_t gene = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  unsigned lane = threadIdx.x & 31u;
+  if (gene >= g) return;
+  double mu = means[gene], acc = 0.0;
+  for (uint64_t i = ptr[gene] + lane; i < ptr[gene + 1]; i += 32) {
+    double c = (double)val[i] - mu;
+    acc = fma(c, c, acc);
+  }
+  for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+  if (lane == 0) out[gene] = acc;
+}
+
+__global__ void to_u16_kernel(const uint32_t* in, uint64_t n, uint16_t* out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = (uint16_t)in[i];
+}
+
+// (row << 32) | value bits, for the gene-major sort.
+__global__ void pack_rows_kernel(const uint64_t* indptr, const float* val, uint64_t n_rows,
+                                 uint64_t* packed) {
+  uint64_t row = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  unsigned lane = threadIdx.x & 31u;
+  if (row >= n_rows) return;
+  for (uint64_t i = indptr[row] + lane; i < indptr[row + 1]; i += 32)
+    packed[i] = (row << 32) | (uint64_t)__float_as_uint(val[i]);
+}
+
+__global__ void unpack_rows_kernel(const uint64_t* packed, uint64_t n, uint32_t* row,
+                                   float* val) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t p = packed[i];
+    row[i] = (uint32_t)(p >> 32);
+    val[i] = __uint_as_float((uint32_t)p);
+  }
+}
+
+// The held input for the tensor-core products: X with 16-bit gene indices, its
+// gene-major twin X^T (32-bit cell indices), and the D^T buffers the passes fill.
+struct TcHeld {
+  static constexpr uint64_t kSegCells = 16384;  // K per X^T work item (cells)
+  uint64_t n = 0, g = 0, n_ld = 0, g_ld = 0;
+  const uint64_t* x_ptr = nullptr;
+  const float* x_val = nullptr;
+  DeviceBuffer<uint16_t> x_col;
+  DeviceBuffer<uint64_t> t_ptr;
+  DeviceBuffer<uint32_t> t_col;
+  DeviceBuffer<float> t_val;
+  DeviceBuffer<float> dt_hi, dt_lo;    // 64 x n_ld: Omega^T or W^T
+  DeviceBuffer<float> qt_hi, qt_lo;    // 64 x g_ld: Q^T or V^T
+  int sm = 148;
+
+  void build(const uint64_t* indptr, const uint32_t* col, const float* val, uint64_t n_rows,
+             uint32_t n_genes, uint64_t nnz, int sm_count, cudaStream_t s) {
+    n = n_rows;
+    g = n_genes;
+    n_ld = (n + 3) & ~3ull;
+    g_ld = (g + 3) & ~3ull;
+    x_ptr = indptr;
+    x_val = val;
+    sm = sm_count;
+    x_col.alloc(nnz, s);
+    if (nnz) {
+      to_u16_kernel<<<std::min<unsigned>(blocks_for(nnz, 256), 16384), 256, 0, s>>>(col, nnz, x_col.ptr);
+      KG_LAUNCH_CHECK();
+    }
+    DeviceBuffer<uint64_t> packed(nnz, s);
+    pack_rows_kernel<<<blocks_for(n * 32, 256), 256, 0, s>>>(indptr, val, n, packed.ptr);
+    KG_LAUNCH_CHECK();
+    DeviceBuffer<uint32_t> genes_sorted;
+    DeviceBuffer<uint64_t> packed_sorted;
+    sort_by_gene<uint64_t>(col, packed.ptr, nnz, (uint32_t)g, genes_sorted, packed_sorted, s);
+    packed.reset();
+    t_ptr.alloc(g + 1, s);
+    column_starts(genes_sorted.ptr, nnz, (uint32_t)g, t_ptr.ptr, s);
+    genes_sorted.reset();
+    t_col.alloc(nnz, s);
+    t_val.alloc(nnz, s);
+    if (nnz) {
+      unpack_rows_kernel<<<std::min<unsigned>(blocks_for(nnz, 256), 16384), 256, 0, s>>>(
+          packed_sorted.ptr, nnz, t_col.ptr, t_val.ptr);
+      KG_LAUNCH_CHECK();
+    }
+    dt_hi.alloc(64 * n_ld, s);
+    dt_lo.alloc(64 * n_ld, s);
+    qt_hi.alloc(64 * g_ld, s);
+    qt_lo.alloc(64 * g_ld, s);
+  }
+
+  // out (g x (width + 1) column-major) = X^T [Omega 1]; omega_sums (width).
+  void sketch(const uint64_t* cells, uint32_t width, uint64_t seed, double* out,
+              double* omega_sums, cudaStream_t s) {
+    unsigned nb = blocks_for(n_ld, 256);
+    DeviceBuffer<double> bsum((uint64_t)nb * 64, s);
+    omega_t_kernel<<<nb, 256, 0, s>>>(cells, n, width, seed, n_ld, dt_hi.ptr, dt_lo.ptr, bsum.ptr);
+    KG_LAUNCH_CHECK();
+    sum_blocks_kernel<<<1, 64, 0, s>>>(bsum.ptr, nb, width, omega_sums);
+    KG_LAUNCH_CHECK();
+    transposed(width + 1, out, s);
+  }
+
+  // out (g x w column-major) = X^T W with W^T in dt.
+  void transposed(uint32_t w, double* out, cudaStream_t s) {
+    uint64_t segs = (n + kSegCells - 1) / kSegCells;
+    DeviceBuffer<double> partial(segs * g * 64, s);
+    SpmmArgs a;
+    a.ptr = t_ptr.ptr;
+    a.col32 = t_col.ptr;
+    a.val = t_val.ptr;
+    a.rows = g;
+    a.K = n;
+    a.seg_len = kSegCells;
+    a.dt_hi = dt_hi.ptr;
+    a.dt_lo = dt_lo.ptr;
+    a.ld_t = n_ld;
+    a.out.mode = kOutPartial;
+    a.out.partial = partial.ptr;
+    a.sm_count = sm;
+    spmm_tc(a, s);
+    reduce_segments_kernel<<<blocks_for(g * w, 256), 256, 0, s>>>(partial.ptr, (uint32_t)segs,
+                                                                  (uint32_t)g, w, out);
+    KG_LAUNCH_CHECK();
+  }
+
+  // Rows of X M - offsets for M = m (g x w column-major): as W^T into dt (with the
+  // column sums into wsums) or as f32 rows into rows_f32.
+  void rows(const double* m, uint32_t w, const double* offsets, double* wsums, float* rows_f32,
+            cudaStream_t s) {
+    split_t_kernel<<<blocks_for(64 * g_ld, 256), 256, 0, s>>>(m, (uint32_t)g, w, g_ld,
+                                                              qt_hi.ptr, qt_lo.ptr);
+    KG_LAUNCH_CHECK();
+    uint64_t tiles = (n + 127) / 128;
+    DeviceBuffer<double> colsum;
+    SpmmArgs a;
+    a.ptr = x_ptr;
+    a.col16 = x_col.ptr;
+    a.val = x_val;
+    a.rows = n;
+    a.K = g;
+    a.seg_len = (g + 31) & ~31ull;
+    a.dt_hi = qt_hi.ptr;
+    a.dt_lo = qt_lo.ptr;
+    a.ld_t = g_ld;
+    a.out.mode = kOutRows;
+    a.out.width = w;
+    a.out.offsets = offsets;
+    if (wsums) {
+      colsum.alloc(tiles * 64, s);
+      a.out.t_hi = dt_hi.ptr;
+      a.out.t_lo = dt_lo.ptr;
+      a.out.ld_t = n_ld;
+      a.out.colsum_partial = colsum.ptr;
+    }
+    a.out.rows_f32 = rows_f32;
+    a.sm_count = sm;
+    spmm_tc(a, s);
+    if (wsums) {
+      sum_blocks_kernel<<<1, 64, 0, s>>>(colsum.ptr, tiles, w, wsums);
+      KG_LAUNCH_CHECK();
+    }
+  }
+
+  void squares(const double* means, double* out, cudaStream_t s) {
+    gene_squares_kernel<<<blocks_for(g * 32, 256), 256, 0, s>>>(t_ptr.ptr, t_val.ptr, means,
+                                                                (uint32_t)g, out);
+    KG_LAUNCH_CHECK();
+  }
+};
+
 }  // namespace kg
 
 using namespace kg;
@@ -537,11 +795,21 @@ void kg_pca::run() {
   c->total = n * kPasses;
   c->done = 0;
 
+  // The products run on the tensor cores (tf32 parts, f64 sums) when the genes fit
+  // 16-bit indices and the widths one 64-column tile; else on the SIMT pipes (f64).
+  const char* pchoice = std::getenv("KYTO_GPU_PCA_PRODUCTS");
+  const bool tc = g <= 65535 && l <= 64 && k <= 64 &&
+                  !(pchoice && std::string(pchoice) == "simt");
+  Trace trace(s, tc ? "pca (tensor-core products)" : "pca (SIMT products)");
+  GeneMajor gm;
+  TcHeld th;
+  if (tc) {
+    th.build(indptr.ptr, col.ptr, val.ptr, n, g, nnz, c->sm_count, s);
+  } else {
   // The gene-major twin of the held input, cut into segments.
   DeviceBuffer<uint32_t> row_of(nnz, s), iota(nnz, s);
   row_of_kernel<<<blocks_for(n * 32, 256), 256, 0, s>>>(indptr.ptr, n, row_of.ptr);
   KG_LAUNCH_CHECK();
-  GeneMajor gm;
   {
     iota_fill(iota.ptr, nnz, s);
     DeviceBuffer<uint32_t> genes_sorted, perm;
@@ -559,8 +827,9 @@ void kg_pca::run() {
     }
     gm.build_segments(g, nnz, s);
   }
-  row_of.reset();
+  }
 
+  trace.mark("gene-major twin");
   Dense dense{this, s, g};
   auto colsums = [&](const double* m, uint32_t w, uint32_t ld, double* out) {
     uint64_t rows_per = 2048;
@@ -575,7 +844,9 @@ void kg_pca::run() {
   // ---- pass 0: sketch X^T [Omega 1] (pca.rs:588-622, end_pass pca.rs:707-749) ----
   means.alloc(g, s);
   DeviceBuffer<double> omega_sums(l, s), sketch1((uint64_t)g * (l + 1), s);
-  {
+  if (tc) {
+    th.sketch(cells.ptr, l, seed, sketch1.ptr, omega_sums.ptr, s);
+  } else {
     DeviceBuffer<double> omega(n * (l + 1), s);
     omega_kernel<<<blocks_for(n, 128), 128, 0, s>>>(cells.ptr, n, l, seed, omega.ptr);
     KG_LAUNCH_CHECK();
@@ -604,7 +875,9 @@ void kg_pca::run() {
   DeviceBuffer<double> basis((uint64_t)g * max_basis, s), products((uint64_t)g * max_basis, s);
   uint32_t m = 0;  // basis columns
   uint32_t w = 0;
+  trace.mark("sketch pass");
   DeviceBuffer<double> block = dense.extend_basis(basis.ptr, 0, sketch1.ptr, l, &w);
+  trace.mark("extend basis");
   sketch1.reset();
   bool finished = false;
   std::vector<double> eigen;
@@ -656,22 +929,29 @@ void kg_pca::run() {
     mean_projection.alloc(k, s);
     dense.mean_dot(loadings64.ptr, means.ptr, k, mean_projection.ptr);
     finished = true;
+    trace.mark("rayleigh-ritz");
   };
 
   if (w == 0) finish_basis();
   for (int pass = 1; pass < kPasses - 1 && !finished; ++pass) {
     check_cancel(c);
     // w = x Q - mu^T Q per row (pca.rs:623-645); C Q = X^T W - mu (sum w) (pca.rs:750-775).
-    DeviceBuffer<double> block_means(w, s), block_rm((uint64_t)g * w, s), wrows(n * w, s),
-        wsums(w, s);
+    DeviceBuffer<double> block_means(w, s), wsums(w, s);
     dense.mean_dot(block.ptr, means.ptr, w, block_means.ptr);
-    to_row_major_kernel<<<blocks_for((uint64_t)g * w, 256), 256, 0, s>>>(block.ptr, g, w,
-                                                                          block_rm.ptr);
-    KG_LAUNCH_CHECK();
-    row_product(indptr.ptr, col.ptr, val.ptr, n, block_rm.ptr, block_means.ptr, w, wrows.ptr, s);
-    colsums(wrows.ptr, w, w, wsums.ptr);
     double* product = products.ptr + (uint64_t)m * g;
-    gm.transposed_product(wrows.ptr, w, g, product, s);
+    if (tc) {
+      th.rows(block.ptr, w, block_means.ptr, wsums.ptr, nullptr, s);
+      th.transposed(w, product, s);
+    } else {
+      DeviceBuffer<double> block_rm((uint64_t)g * w, s), wrows(n * w, s);
+      to_row_major_kernel<<<blocks_for((uint64_t)g * w, 256), 256, 0, s>>>(block.ptr, g, w,
+                                                                            block_rm.ptr);
+      KG_LAUNCH_CHECK();
+      row_product(indptr.ptr, col.ptr, val.ptr, n, block_rm.ptr, block_means.ptr, w, wrows.ptr, s);
+      colsums(wrows.ptr, w, w, wsums.ptr);
+      gm.transposed_product(wrows.ptr, w, g, product, s);
+    }
+    trace.mark("product pass");
     subtract_outer_kernel<<<blocks_for((uint64_t)g * w, 256), 256, 0, s>>>(
         product, means.ptr, wsums.ptr, g, w);
     KG_LAUNCH_CHECK();
@@ -683,20 +963,25 @@ void kg_pca::run() {
     if (pass == kPasses - 2) {
       finish_basis();
     } else {
+      trace.mark("basis bookkeeping");
       block = dense.extend_basis(basis.ptr, m, product, w, &w);
+      trace.mark("extend basis");
       if (w == 0) finish_basis();
     }
   }
   check_cancel(c);
 
   // ---- last pass: rows (x - mu) V and the centred squares (pca.rs:649-677, 779-797) ----
-  {
+  trace.mark("basis bookkeeping");
+  embedding.alloc(n * k, s);
+  if (tc) {
+    th.rows(loadings64.ptr, k, mean_projection.ptr, nullptr, embedding.ptr, s);
+  } else {
     DeviceBuffer<double> l_rm((uint64_t)g * k, s), rows(n * k, s);
     to_row_major_kernel<<<blocks_for((uint64_t)g * k, 256), 256, 0, s>>>(loadings64.ptr, g, k,
                                                                           l_rm.ptr);
     KG_LAUNCH_CHECK();
     row_product(indptr.ptr, col.ptr, val.ptr, n, l_rm.ptr, mean_projection.ptr, k, rows.ptr, s);
-    embedding.alloc(n * k, s);
     to_f32_kernel<<<std::min<unsigned>(blocks_for(n * k, 256), 16384), 256, 0, s>>>(
         rows.ptr, n * k, embedding.ptr);
     KG_LAUNCH_CHECK();
@@ -705,10 +990,15 @@ void kg_pca::run() {
   std::vector<uint64_t> colptr(g + 1);
   {
     DeviceBuffer<double> sq(g, s);
-    gm.centred_squares(means.ptr, g, sq.ptr, s);
+    if (tc)
+      th.squares(means.ptr, sq.ptr, s);
+    else
+      gm.centred_squares(means.ptr, g, sq.ptr, s);
     KG_CUDA(cudaMemcpyAsync(squares.data(), sq.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
-    KG_CUDA(cudaMemcpyAsync(colptr.data(), gm.colptr.ptr, (g + 1) * 8ull, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaMemcpyAsync(colptr.data(), tc ? th.t_ptr.ptr : gm.colptr.ptr, (g + 1) * 8ull,
+                            cudaMemcpyDeviceToHost, s));
   }
+  trace.mark("embedding pass");
   std::vector<double> h_means(g);
   KG_CUDA(cudaMemcpyAsync(h_means.data(), means.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
   loadings.alloc((uint64_t)stream_genes * k, s);

@@ -75,17 +75,37 @@ def _col_diff(a, b):
     return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
 
 
-def test_pca_synthetic_golden(ctx, counts):
+# The two product engines: tensor cores (tf32 parts, f32 sums of at most 512 terms
+# flushed into f64) and the SIMT pipes (f64 throughout). Bars against the FP64 oracle:
+# variances (singular values squared) and loadings/embedding columns.
+PRODUCTS = {"tc": (2e-5, 2e-4), "simt": (1e-6, 1e-5)}
+
+
+@pytest.fixture(params=sorted(PRODUCTS))
+def products(request, monkeypatch):
+    monkeypatch.setenv("KYTO_GPU_PCA_PRODUCTS", request.param)
+    return PRODUCTS[request.param]
+
+
+def _angle(a, b):
+    qa, _ = np.linalg.qr(a.astype(np.float64))
+    qb, _ = np.linalg.qr(b.astype(np.float64))
+    s = np.linalg.svd(qa.T @ qb, compute_uv=False)
+    return float(np.arccos(np.clip(s.min(), -1.0, 1.0)))
+
+
+def test_pca_synthetic_golden(ctx, counts, products):
+    var_tol, col_tol = products
     hv = load_golden("synthetic_hvg")["highly_variable"]
     gold = load_golden("synthetic_pca")
     res = K.pca(counts.indptr, counts.indices, counts.values, counts.n_genes, 20, seed=0,
                 gene_set=hv, target_sum=1e4, log1p=True, ctx=ctx)
     assert np.max(np.abs(res.variance - gold["variance"]) / gold["variance"]) <= 1e-3
     ref = O.pca(O.normalize_log1p(counts), 20, 0, gene_set=hv)
-    assert np.max(np.abs(res.variance - ref.variance) / ref.variance) <= 1e-6
+    assert np.max(np.abs(res.variance - ref.variance) / ref.variance) <= var_tol
     for c in range(20):
-        assert _col_diff(res.loadings[:, c], ref.loadings[:, c]) <= 1e-5
-        assert _col_diff(res.embedding[:, c], ref.embedding[:, c]) <= 1e-5
+        assert _col_diff(res.loadings[:, c], ref.loadings[:, c]) <= col_tol
+        assert _col_diff(res.embedding[:, c], ref.embedding[:, c]) <= col_tol
     assert res.passes_run == ref.passes_run
 
 
@@ -95,7 +115,8 @@ def planted():
     return x
 
 
-def test_pca_planted_with_hvg_matches_oracle(ctx, planted):
+def test_pca_planted_with_hvg_matches_oracle(ctx, planted, products):
+    var_tol, col_tol = products
     x = planted
     hv = K.highly_variable_genes(x.indptr, x.indices, x.values, x.n_genes, 1000, ctx=ctx)
     logx = O.normalize_log1p(O.Csr(x.indptr, x.indices, x.values, x.n_genes))
@@ -105,10 +126,12 @@ def test_pca_planted_with_hvg_matches_oracle(ctx, planted):
                 gene_set=hv.highly_variable, target_sum=1e4, log1p=True, ctx=ctx)
     ref = O.pca(logx, 50, 0, gene_set=hv.highly_variable)
     rel = np.abs(res.variance - ref.variance) / ref.variance
-    assert rel.max() <= 1e-6, rel.max()
-    assert np.allclose(res.variance_ratio, ref.variance_ratio, rtol=1e-6)
+    assert rel.max() <= var_tol, rel.max()
+    assert np.allclose(res.variance_ratio, ref.variance_ratio, rtol=var_tol)
     for c in range(10):
-        assert _col_diff(res.embedding[:, c], ref.embedding[:, c]) <= 1e-5
+        assert _col_diff(res.embedding[:, c], ref.embedding[:, c]) <= col_tol
+    assert _angle(res.loadings[hv.highly_variable][:, :10],
+                  ref.loadings[hv.highly_variable][:, :10]) <= 1e-3
 
 
 def test_pca_blocks_give_the_same_bits(ctx, planted):
