@@ -237,18 +237,26 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           break;
         }
         tc_fence_after();
-#pragma unroll 1
-        for (int c = 0; c < kTcPoints / 32; ++c) {
-          __syncwarp();
-          float v[32];
-          tmem_load_32(tmem + ((quad * 32u) << 16) + ab * 256u + half * 128u + c * 32u, v);
-          if (active && !st.overflowed) {
-            float m = v[0];
+        // All 128 keys of the tile into registers with one wait, then the accumulator
+        // goes straight back to the MMA warp; the keys are scanned meanwhile.
+        __syncwarp();
+        uint32_t r[kTcPoints / 32][32];
+        const uint32_t base = tmem + ((quad * 32u) << 16) + ab * 256u + half * 128u;
 #pragma unroll
-            for (int j = 1; j < 32; ++j) m = fminf(m, v[j]);
+        for (int c = 0; c < kTcPoints / 32; ++c) tmem_ld_32(base + c * 32u, r[c]);
+        tmem_wait_ld();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.tmem_empty[ab]);
+        if (active && !st.overflowed) {
+#pragma unroll
+          for (int c = 0; c < kTcPoints / 32; ++c) {
+            float m = __uint_as_float(r[c][0]);
+#pragma unroll
+            for (int j = 1; j < 32; ++j) m = fminf(m, __uint_as_float(r[c][j]));
             if (m <= st.th) {
 #pragma unroll
-              for (int j = 0; j < 32; ++j) my[j] = v[j];
+              for (int j = 0; j < 32; ++j) my[j] = __uint_as_float(r[c][j]);
               const uint64_t p0 = (uint64_t)t * kTcPoints + c * 32;
               for (int j = 0; j < 32; ++j) {
                 float key = my[j];
@@ -259,9 +267,6 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
             }
           }
         }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&sm.tmem_empty[ab]);
       }
       if (active && ok) {
         cand_count[q] = st.overflowed ? kOverflow : st.count;

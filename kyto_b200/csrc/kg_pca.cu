@@ -327,6 +327,110 @@ __global__ void divide_kernel(const double* in, uint32_t n, double d, double* ou
   if (i < n) out[i] = in[i] / d;
 }
 
+// ------------------------------------------------ thin SVD (one-sided Jacobi) -------
+
+constexpr uint32_t kJacobiMaxCols = 256;
+
+// Hestenes' one-sided Jacobi SVD of the g x w column-major f64 matrix `a` (w <= 256),
+// one CTA of 32 warps: columns are rotated pairwise (round-robin tournament, one warp
+// per pair, dot products by a fixed shuffle tree) until every pair is orthogonal to
+// 1e-15 of its norms. Then a = U diag(sigma) column by column; sigma[c] is the c-th
+// largest column norm and order[c] its column (ties to the lower column). Relative
+// accuracy for small singular values, as the drop rule (1e-10 of the block's norm)
+// needs. status: 0, or 1 if 60 sweeps did not converge.
+__global__ void __launch_bounds__(1024)
+jacobi_svd_kernel(double* a, uint32_t g, uint32_t w, double* sigma, uint32_t* order,
+                  int* status) {
+  __shared__ int rotated;
+  __shared__ double norms[kJacobiMaxCols];
+  const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const unsigned warps = blockDim.x >> 5;
+  const uint32_t players = (w + 1) & ~1u;
+  int sweep = 0;
+  for (; sweep < 60; ++sweep) {
+    if (threadIdx.x == 0) rotated = 0;
+    __syncthreads();
+    for (uint32_t r = 0; r + 1 < players; ++r) {
+      for (uint32_t pr = warp; pr < players / 2; pr += warps) {
+        auto at = [&](uint32_t pos) {
+          return pos == 0 ? 0u : ((pos - 1 + r) % (players - 1)) + 1;
+        };
+        uint32_t i = at(pr), j = at(players - 1 - pr);
+        if (i > j) {
+          uint32_t t = i;
+          i = j;
+          j = t;
+        }
+        if (j >= w) continue;
+        double* ai = a + (uint64_t)i * g;
+        double* aj = a + (uint64_t)j * g;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (uint32_t x = lane; x < g; x += 32) {
+          double u = ai[x], v = aj[x];
+          al = fma(u, u, al);
+          be = fma(v, v, be);
+          ga = fma(u, v, ga);
+        }
+        for (int o = 16; o; o >>= 1) {
+          al += __shfl_xor_sync(0xFFFFFFFFu, al, o);
+          be += __shfl_xor_sync(0xFFFFFFFFu, be, o);
+          ga += __shfl_xor_sync(0xFFFFFFFFu, ga, o);
+        }
+        if (!(al > 0.0) || !(be > 0.0) || !(fabs(ga) > 1e-15 * sqrt(al) * sqrt(be))) continue;
+        double zeta = (be - al) / (2.0 * ga);
+        double t = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + hypot(1.0, zeta));
+        double c = 1.0 / sqrt(1.0 + t * t), sn = c * t;
+        for (uint32_t x = lane; x < g; x += 32) {
+          double u = ai[x], v = aj[x];
+          ai[x] = c * u - sn * v;
+          aj[x] = sn * u + c * v;
+        }
+        if (lane == 0) rotated = 1;
+      }
+      __syncthreads();
+    }
+    bool again = rotated != 0;
+    __syncthreads();
+    if (!again) break;
+  }
+  // Column norms, then the order by norm (descending, ties to the lower column).
+  for (uint32_t col = warp; col < w; col += warps) {
+    const double* ac = a + (uint64_t)col * g;
+    double ss = 0.0;
+    for (uint32_t x = lane; x < g; x += 32) ss = fma(ac[x], ac[x], ss);
+    for (int o = 16; o; o >>= 1) ss += __shfl_xor_sync(0xFFFFFFFFu, ss, o);
+    if (lane == 0) norms[col] = sqrt(ss);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t idx[kJacobiMaxCols];
+    for (uint32_t c = 0; c < w; ++c) idx[c] = c;
+    for (uint32_t c = 1; c < w; ++c) {
+      uint32_t v = idx[c], at = c;
+      while (at > 0 && norms[idx[at - 1]] < norms[v]) {
+        idx[at] = idx[at - 1];
+        --at;
+      }
+      idx[at] = v;
+    }
+    for (uint32_t c = 0; c < w; ++c) {
+      order[c] = idx[c];
+      sigma[c] = norms[idx[c]];
+    }
+    *status = sweep >= 60 ? 1 : 0;
+  }
+}
+
+// out[:, c] = a[:, order[c]] / sigma[c] (the left singular vectors kept).
+__global__ void gather_unit_columns_kernel(const double* a, uint32_t g, uint32_t keep,
+                                           const double* sigma, const uint32_t* order,
+                                           double* out) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= (uint64_t)g * keep) return;
+  uint32_t c = (uint32_t)(i / g), r = (uint32_t)(i % g);
+  out[i] = a[(uint64_t)order[c] * g + r] / sigma[c];
+}
+
 // ------------------------------------------------ tensor-core product support -------
 
 __device__ __forceinline__ float tf32_rna(float x) {
@@ -744,13 +848,13 @@ struct Dense {
                               proj.ptr, m, &one, rest.ptr, g));
       }
     }
-    int lwork = 0;
-    KG_CUSOLVER(cusolverDnDgesvd_bufferSize(p->cusolver, g, w, &lwork));
-    DeviceBuffer<double> work(std::max(lwork, 1), s), sv(w, s), u((uint64_t)g * w, s),
-        vt(1, s), rwork(w, s);
+    // Thin SVD by one-sided Jacobi in one kernel (the block is at most 64 columns).
+    if (w > kJacobiMaxCols) fail(KG_ERR_INVALID, "pca: a Krylov block wider than 256 columns");
+    DeviceBuffer<double> sv(w, s);
+    DeviceBuffer<uint32_t> order(w, s);
     DeviceBuffer<int> info(1, s);
-    KG_CUSOLVER(cusolverDnDgesvd(p->cusolver, 'S', 'N', g, w, rest.ptr, g, sv.ptr, u.ptr, g,
-                                 vt.ptr, 1, work.ptr, lwork, rwork.ptr, info.ptr));
+    jacobi_svd_kernel<<<1, 1024, 0, s>>>(rest.ptr, g, w, sv.ptr, order.ptr, info.ptr);
+    KG_LAUNCH_CHECK();
     std::vector<double> h_sv(w);
     int h_info = 0;
     KG_CUDA(cudaMemcpyAsync(h_sv.data(), sv.ptr, w * 8ull, cudaMemcpyDeviceToHost, s));
@@ -763,7 +867,9 @@ struct Dense {
     *keep_out = keep;
     if (keep == 0) return none;
     DeviceBuffer<double> out((uint64_t)g * keep, s);
-    KG_CUDA(cudaMemcpyAsync(out.ptr, u.ptr, out.bytes(), cudaMemcpyDeviceToDevice, s));
+    gather_unit_columns_kernel<<<blocks_for((uint64_t)g * keep, 256), 256, 0, s>>>(
+        rest.ptr, g, keep, sv.ptr, order.ptr, out.ptr);
+    KG_LAUNCH_CHECK();
     return out;
   }
 
@@ -798,7 +904,7 @@ void kg_pca::run() {
   // The products run on the tensor cores (tf32 parts, f64 sums) when the genes fit
   // 16-bit indices and the widths one 64-column tile; else on the SIMT pipes (f64).
   const char* pchoice = std::getenv("KYTO_GPU_PCA_PRODUCTS");
-  const bool tc = g <= 65535 && l <= 64 && k <= 64 &&
+  const bool tc = g <= 65535 && l + 1 <= 64 && k <= 64 &&
                   !(pchoice && std::string(pchoice) == "simt");
   Trace trace(s, tc ? "pca (tensor-core products)" : "pca (SIMT products)");
   GeneMajor gm;
