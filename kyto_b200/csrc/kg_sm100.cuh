@@ -54,8 +54,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Polls before a wait gives up (try_wait itself suspends for a while per poll; with the
-// back-off below this is seconds, far above any legitimate wait in these kernels).
+// Polls before a wait gives up. try_wait suspends the thread in hardware until the
+// phase completes or a short time limit passes, so a poll is cheap and wakes at once;
+// a sleep is added only after 2^20 polls, when something is already wrong. The bound
+// is seconds, far above any legitimate wait in these kernels.
 constexpr uint32_t kWaitPolls = 1u << 24;
 
 // Wait for phase `parity` of `bar`; false (and *abort set) if it never completes or
@@ -65,7 +67,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity,
   for (uint32_t i = 0; i < kWaitPolls; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
     if (*abort) return false;
-    if (i > 64) __nanosleep(128);
+    if (i > (1u << 20)) __nanosleep(256);
   }
   *abort = 1;
   return false;
