@@ -243,6 +243,9 @@ def main() -> int:
         st = run_step(args, ctx, d_indptr, d_idx, d_vals, out_dev, host=False)
         torch.cuda.nvtx.range_pop()
         filter_ms.append(st.filter_ms)
+        knn_stats = {"candidates_per_row": st.candidates / args.cells,
+                     "rows_searched_in_full": st.rows_full,
+                     "filter_ms": st.filter_ms, "rank_ms": st.rank_ms}
     stop.record()
     barrier()
     clk = clocks.stop()
@@ -305,7 +308,7 @@ def main() -> int:
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs (>4 GB) larger than L2; no flush"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
-            "clocks": clk, "gpu_launches": launches,
+            "clocks": clk, "gpu_launches": launches, "knn": knn_stats,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -255,13 +255,23 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
 #pragma unroll
             for (int j = 1; j < 32; ++j) m = fminf(m, __uint_as_float(r[c][j]));
             if (m <= st.th) {
+              // Only the keys at or under the threshold, in column order (the threshold
+              // only falls while they are offered).
+              uint32_t mask = 0;
+              const float th0 = st.th;
 #pragma unroll
-              for (int j = 0; j < 32; ++j) my[j] = __uint_as_float(r[c][j]);
-              const uint64_t p0 = (uint64_t)t * kTcPoints + c * 32;
               for (int j = 0; j < 32; ++j) {
-                float key = my[j];
-                uint64_t p = p0 + j;
-                if (key <= st.th && p < n && p != q && !st.overflowed)
+                const float key = __uint_as_float(r[c][j]);
+                my[j] = key;
+                mask |= (key <= th0 ? 1u : 0u) << j;
+              }
+              const uint64_t p0 = (uint64_t)t * kTcPoints + c * 32;
+              while (mask && !st.overflowed) {
+                const int j = __ffs(mask) - 1;
+                mask &= mask - 1;
+                const float key = my[j];
+                const uint64_t p = p0 + j;
+                if (key <= st.th && p < n && p != q)
                   tc_offer(st, smallest, k, sl2, key, (uint32_t)p, ck, cr, cap);
               }
             }

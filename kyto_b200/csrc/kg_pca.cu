@@ -110,8 +110,7 @@ __global__ void add_offset_kernel(uint64_t* p, uint64_t n, uint64_t offset) {
 
 // --------------------------------------------------------------- small kernels -----
 
-// Omega's rows (pca.rs:936-950) beside a column of ones (the gene sums' column):
-// out is n x (width + 1) row-major.
+// Omega's rows (pca.rs:936-950): out is n x width row-major.
 __device__ __forceinline__ uint64_t splitmix_mix(uint64_t v) {
   v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ull;
   v = (v ^ (v >> 27)) * 0x94D049BB133111EBull;
@@ -123,12 +122,16 @@ __global__ void omega_kernel(const uint64_t* cells, uint64_t n, uint32_t width,
   uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (r >= n) return;
   uint64_t state = splitmix_mix(seed ^ splitmix_mix(cells[r] + 0x9E3779B97F4A7C15ull));
-  double* row = out + r * (uint64_t)(width + 1);
+  double* row = out + r * (uint64_t)width;
   for (uint32_t j = 0; j < width; ++j) {
     state += 0x9E3779B97F4A7C15ull;
     row[j] = __dadd_rn((double)(splitmix_mix(state) >> 11) * 0x1p-52, -1.0);
   }
-  row[width] = 1.0;
+}
+
+__global__ void fill_kernel(double* p, uint64_t n, double v) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
 }
 
 // Column sums of an n x w row-major matrix, stage 1: block b sums rows
@@ -453,8 +456,8 @@ __global__ void split_t_kernel(const double* cm, uint32_t g, uint32_t w, uint64_
   t_lo[i] = tf32_rna((float)(v - (double)hi));
 }
 
-// Omega^T beside a row of ones (the gene sums), two tf32 parts, 64 x ld; and each
-// block's Omega column sums (of the parts, f64, a fixed tree) for the centring.
+// Omega^T in two tf32 parts, 64 x ld (rows past width zero); and each block's Omega
+// column sums (of the parts, f64, a fixed tree) for the centring.
 __global__ void omega_t_kernel(const uint64_t* cells, uint64_t n, uint32_t width,
                                uint64_t seed, uint64_t ld, float* t_hi, float* t_lo,
                                double* block_sums) {
@@ -470,8 +473,6 @@ __global__ void omega_t_kernel(const uint64_t* cells, uint64_t n, uint32_t width
       double om = __dadd_rn((double)(splitmix_mix(state) >> 11) * 0x1p-52, -1.0);
       hi = tf32_rna((float)om);
       lo = tf32_rna((float)(om - (double)hi));
-    } else if (live && j == width) {
-      hi = 1.0f;
     }
     if (r < ld) {
       t_hi[(uint64_t)j * ld + r] = hi;
@@ -553,17 +554,12 @@ __global__ void unpack_rows_kernel(const uint64_t* packed, uint64_t n, uint32_t*
   }
 }
 
-// The held input for the tensor-core products: X with 16-bit gene indices, its
-// gene-major twin X^T (32-bit cell indices), and the D^T buffers the passes fill.
+// The held input for the tensor-core products: X and X^T in the blocked layout
+// (kg_spmm_tc.cuh), and the D^T buffers the passes fill.
 struct TcHeld {
-  static constexpr uint64_t kSegCells = 16384;  // K per X^T work item (cells)
+  static constexpr uint64_t kSegChunks = 512;  // K-chunks (16,384 cells) per X^T work item
   uint64_t n = 0, g = 0, n_ld = 0, g_ld = 0;
-  const uint64_t* x_ptr = nullptr;
-  const float* x_val = nullptr;
-  DeviceBuffer<uint16_t> x_col;
-  DeviceBuffer<uint64_t> t_ptr;
-  DeviceBuffer<uint32_t> t_col;
-  DeviceBuffer<float> t_val;
+  Blocked bx, bxt;
   DeviceBuffer<float> dt_hi, dt_lo;    // 64 x n_ld: Omega^T or W^T
   DeviceBuffer<float> qt_hi, qt_lo;    // 64 x g_ld: Q^T or V^T
   int sm = 148;
@@ -574,38 +570,16 @@ struct TcHeld {
     g = n_genes;
     n_ld = (n + 3) & ~3ull;
     g_ld = (g + 3) & ~3ull;
-    x_ptr = indptr;
-    x_val = val;
     sm = sm_count;
-    x_col.alloc(nnz, s);
-    if (nnz) {
-      to_u16_kernel<<<std::min<unsigned>(blocks_for(nnz, 256), 16384), 256, 0, s>>>(col, nnz, x_col.ptr);
-      KG_LAUNCH_CHECK();
-    }
-    DeviceBuffer<uint64_t> packed(nnz, s);
-    pack_rows_kernel<<<blocks_for(n * 32, 256), 256, 0, s>>>(indptr, val, n, packed.ptr);
-    KG_LAUNCH_CHECK();
-    DeviceBuffer<uint32_t> genes_sorted;
-    DeviceBuffer<uint64_t> packed_sorted;
-    sort_by_gene<uint64_t>(col, packed.ptr, nnz, (uint32_t)g, genes_sorted, packed_sorted, s);
-    packed.reset();
-    t_ptr.alloc(g + 1, s);
-    column_starts(genes_sorted.ptr, nnz, (uint32_t)g, t_ptr.ptr, s);
-    genes_sorted.reset();
-    t_col.alloc(nnz, s);
-    t_val.alloc(nnz, s);
-    if (nnz) {
-      unpack_rows_kernel<<<std::min<unsigned>(blocks_for(nnz, 256), 16384), 256, 0, s>>>(
-          packed_sorted.ptr, nnz, t_col.ptr, t_val.ptr);
-      KG_LAUNCH_CHECK();
-    }
+    build_blocked(indptr, col, val, n, g, nnz, false, bx, s);
+    build_blocked(indptr, col, val, n, g, nnz, true, bxt, s);
     dt_hi.alloc(64 * n_ld, s);
     dt_lo.alloc(64 * n_ld, s);
     qt_hi.alloc(64 * g_ld, s);
     qt_lo.alloc(64 * g_ld, s);
   }
 
-  // out (g x (width + 1) column-major) = X^T [Omega 1]; omega_sums (width).
+  // out (g x width column-major) = X^T Omega; omega_sums (width).
   void sketch(const uint64_t* cells, uint32_t width, uint64_t seed, double* out,
               double* omega_sums, cudaStream_t s) {
     unsigned nb = blocks_for(n_ld, 256);
@@ -614,20 +588,16 @@ struct TcHeld {
     KG_LAUNCH_CHECK();
     sum_blocks_kernel<<<1, 64, 0, s>>>(bsum.ptr, nb, width, omega_sums);
     KG_LAUNCH_CHECK();
-    transposed(width + 1, out, s);
+    transposed(width, out, s);
   }
 
   // out (g x w column-major) = X^T W with W^T in dt.
   void transposed(uint32_t w, double* out, cudaStream_t s) {
-    uint64_t segs = (n + kSegCells - 1) / kSegCells;
+    uint64_t segs = (bxt.n_chunks + kSegChunks - 1) / kSegChunks;
     DeviceBuffer<double> partial(segs * g * 64, s);
     SpmmArgs a;
-    a.ptr = t_ptr.ptr;
-    a.col32 = t_col.ptr;
-    a.val = t_val.ptr;
-    a.rows = g;
-    a.K = n;
-    a.seg_len = kSegCells;
+    a.s = &bxt;
+    a.seg_chunks = kSegChunks;
     a.dt_hi = dt_hi.ptr;
     a.dt_lo = dt_lo.ptr;
     a.ld_t = n_ld;
@@ -650,12 +620,8 @@ struct TcHeld {
     uint64_t tiles = (n + 127) / 128;
     DeviceBuffer<double> colsum;
     SpmmArgs a;
-    a.ptr = x_ptr;
-    a.col16 = x_col.ptr;
-    a.val = x_val;
-    a.rows = n;
-    a.K = g;
-    a.seg_len = (g + 31) & ~31ull;
+    a.s = &bx;
+    a.seg_chunks = bx.n_chunks;
     a.dt_hi = qt_hi.ptr;
     a.dt_lo = qt_lo.ptr;
     a.ld_t = g_ld;
@@ -676,12 +642,6 @@ struct TcHeld {
       sum_blocks_kernel<<<1, 64, 0, s>>>(colsum.ptr, tiles, w, wsums);
       KG_LAUNCH_CHECK();
     }
-  }
-
-  void squares(const double* means, double* out, cudaStream_t s) {
-    gene_squares_kernel<<<blocks_for(g * 32, 256), 256, 0, s>>>(t_ptr.ptr, t_val.ptr, means,
-                                                                (uint32_t)g, out);
-    KG_LAUNCH_CHECK();
   }
 };
 
@@ -711,6 +671,7 @@ struct kg_pca {
   DeviceBuffer<float> embedding, loadings;
   DeviceBuffer<double> means;
   std::vector<double> variance, variance_ratio;
+  const char* products_engine = "";
 
   ~kg_pca() {
     if (stream) cudaStreamSynchronize(stream);
@@ -901,22 +862,14 @@ void kg_pca::run() {
   c->total = n * kPasses;
   c->done = 0;
 
-  // The products run on the tensor cores (tf32 parts, f64 sums) when the genes fit
-  // 16-bit indices and the widths one 64-column tile; else on the SIMT pipes (f64).
-  const char* pchoice = std::getenv("KYTO_GPU_PCA_PRODUCTS");
-  const bool tc = g <= 65535 && l + 1 <= 64 && k <= 64 &&
-                  !(pchoice && std::string(pchoice) == "simt");
-  Trace trace(s, tc ? "pca (tensor-core products)" : "pca (SIMT products)");
+  Trace trace(s, "pca");
+  // The gene-major twin of the held input (each gene's values in cell order), cut into
+  // segments: the genes' exact f64 statistics, and the SIMT products' operand.
   GeneMajor gm;
-  TcHeld th;
-  if (tc) {
-    th.build(indptr.ptr, col.ptr, val.ptr, n, g, nnz, c->sm_count, s);
-  } else {
-  // The gene-major twin of the held input, cut into segments.
-  DeviceBuffer<uint32_t> row_of(nnz, s), iota(nnz, s);
-  row_of_kernel<<<blocks_for(n * 32, 256), 256, 0, s>>>(indptr.ptr, n, row_of.ptr);
-  KG_LAUNCH_CHECK();
   {
+    DeviceBuffer<uint32_t> row_of(nnz, s), iota(nnz, s);
+    row_of_kernel<<<blocks_for(n * 32, 256), 256, 0, s>>>(indptr.ptr, n, row_of.ptr);
+    KG_LAUNCH_CHECK();
     iota_fill(iota.ptr, nnz, s);
     DeviceBuffer<uint32_t> genes_sorted, perm;
     sort_by_gene<uint32_t>(col.ptr, iota.ptr, nnz, g, genes_sorted, perm, s);
@@ -933,9 +886,51 @@ void kg_pca::run() {
     }
     gm.build_segments(g, nnz, s);
   }
-  }
-
   trace.mark("gene-major twin");
+
+  // Gene means (pass 0's sums, pca.rs:707-717) and centred sums of squares over the
+  // stored values (the last pass's, pca.rs:664-676), in f64 in a fixed order.
+  means.alloc(g, s);
+  std::vector<double> squares(g), h_means(g);
+  std::vector<uint64_t> colptr(g + 1);
+  {
+    DeviceBuffer<double> ones(n, s), sums(g, s), sq(g, s);
+    fill_kernel<<<blocks_for(n, 256), 256, 0, s>>>(ones.ptr, n, 1.0);
+    KG_LAUNCH_CHECK();
+    gm.transposed_product(ones.ptr, 1, g, sums.ptr, s);
+    divide_kernel<<<blocks_for(g, 256), 256, 0, s>>>(sums.ptr, g, (double)n, means.ptr);
+    KG_LAUNCH_CHECK();
+    gm.centred_squares(means.ptr, g, sq.ptr, s);
+    KG_CUDA(cudaMemcpyAsync(h_means.data(), means.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaMemcpyAsync(squares.data(), sq.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaMemcpyAsync(colptr.data(), gm.colptr.ptr, (g + 1) * 8ull, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+  }
+  for (uint32_t i = 0; i < g; ++i)
+    if (!std::isfinite(h_means[i]))
+      fail(KG_ERR_INVALID, "pca: gene " + std::to_string(i) +
+                               " holds a value that is not finite (NaN or infinity)");
+  trace.mark("gene statistics");
+
+  // The products run on the tensor cores (tf32 parts, f32 sums of at most 512 terms
+  // flushed into f64) when the genes fit 16-bit positions, the block one 64-column tile,
+  // and no gene's mean dwarfs its spread (the rows are centred after the product, so
+  // the products' relative error is scaled by |mean| / sd: at most 64, about 2^-15);
+  // else on the SIMT pipes in f64 (kyto's arithmetic, any data).
+  double worst_ratio = 0.0;
+  for (uint32_t i = 0; i < g; ++i) {
+    uint64_t stored = colptr[i + 1] - colptr[i];
+    double var = (squares[i] + (double)(n - stored) * h_means[i] * h_means[i]) / (double)n;
+    if (var > 0.0) worst_ratio = std::max(worst_ratio, h_means[i] * h_means[i] / var);
+  }
+  const char* pchoice = std::getenv("KYTO_GPU_PCA_PRODUCTS");
+  const bool tc = g <= 65535 && l <= 64 && k <= 64 && worst_ratio <= 4096.0 &&
+                  !(pchoice && std::string(pchoice) == "simt");
+  products_engine = tc ? "tensor-core" : "simt";
+  TcHeld th;
+  if (tc) th.build(indptr.ptr, col.ptr, val.ptr, n, g, nnz, c->sm_count, s);
+  trace.mark(tc ? "blocked layouts" : "no blocked layouts");
+
   Dense dense{this, s, g};
   auto colsums = [&](const double* m, uint32_t w, uint32_t ld, double* out) {
     uint64_t rows_per = 2048;
@@ -947,29 +942,16 @@ void kg_pca::run() {
     KG_LAUNCH_CHECK();
   };
 
-  // ---- pass 0: sketch X^T [Omega 1] (pca.rs:588-622, end_pass pca.rs:707-749) ----
-  means.alloc(g, s);
-  DeviceBuffer<double> omega_sums(l, s), sketch1((uint64_t)g * (l + 1), s);
+  // ---- pass 0: sketch X^T Omega (pca.rs:588-622, end_pass pca.rs:707-749) ----
+  DeviceBuffer<double> omega_sums(l, s), sketch1((uint64_t)g * l, s);
   if (tc) {
     th.sketch(cells.ptr, l, seed, sketch1.ptr, omega_sums.ptr, s);
   } else {
-    DeviceBuffer<double> omega(n * (l + 1), s);
+    DeviceBuffer<double> omega(n * l, s);
     omega_kernel<<<blocks_for(n, 128), 128, 0, s>>>(cells.ptr, n, l, seed, omega.ptr);
     KG_LAUNCH_CHECK();
-    colsums(omega.ptr, l, l + 1, omega_sums.ptr);
-    gm.transposed_product(omega.ptr, l + 1, g, sketch1.ptr, s);
-  }
-  divide_kernel<<<blocks_for(g, 256), 256, 0, s>>>(sketch1.ptr + (uint64_t)l * g, g,
-                                                     (double)n, means.ptr);
-  KG_LAUNCH_CHECK();
-  {
-    std::vector<double> h_means(g);
-    KG_CUDA(cudaMemcpyAsync(h_means.data(), means.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
-    KG_CUDA(cudaStreamSynchronize(s));
-    for (uint32_t i = 0; i < g; ++i)
-      if (!std::isfinite(h_means[i]))
-        fail(KG_ERR_INVALID, "pca: gene " + std::to_string(i) +
-                                 " holds a value that is not finite (NaN or infinity)");
+    colsums(omega.ptr, l, l, omega_sums.ptr);
+    gm.transposed_product(omega.ptr, l, g, sketch1.ptr, s);
   }
   subtract_outer_kernel<<<blocks_for((uint64_t)g * l, 256), 256, 0, s>>>(
       sketch1.ptr, means.ptr, omega_sums.ptr, g, l);
@@ -1092,21 +1074,7 @@ void kg_pca::run() {
         rows.ptr, n * k, embedding.ptr);
     KG_LAUNCH_CHECK();
   }
-  std::vector<double> squares(g);
-  std::vector<uint64_t> colptr(g + 1);
-  {
-    DeviceBuffer<double> sq(g, s);
-    if (tc)
-      th.squares(means.ptr, sq.ptr, s);
-    else
-      gm.centred_squares(means.ptr, g, sq.ptr, s);
-    KG_CUDA(cudaMemcpyAsync(squares.data(), sq.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
-    KG_CUDA(cudaMemcpyAsync(colptr.data(), tc ? th.t_ptr.ptr : gm.colptr.ptr, (g + 1) * 8ull,
-                            cudaMemcpyDeviceToHost, s));
-  }
   trace.mark("embedding pass");
-  std::vector<double> h_means(g);
-  KG_CUDA(cudaMemcpyAsync(h_means.data(), means.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
   loadings.alloc((uint64_t)stream_genes * k, s);
   loadings.zero();
   scatter_loadings_kernel<<<blocks_for((uint64_t)g * k, 256), 256, 0, s>>>(

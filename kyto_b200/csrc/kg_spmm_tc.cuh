@@ -1,4 +1,5 @@
-// The tensor-core sparse x dense product of the PCA (kg_spmm_tc.cu).
+// The tensor-core sparse x dense product of the PCA (kg_spmm_tc.cu) and the blocked
+// sparse layout it reads.
 #pragma once
 
 #include <cstdint>
@@ -7,7 +8,29 @@
 
 namespace kg {
 
+// A sparse matrix (rows x K) cut into blocks of 128 rows x 32 columns: block
+// (tile, chunk) holds its entries contiguously at [off[b], off[b+1]) with
+// b = tile * n_chunks + chunk, each entry a 16-bit (row_in_tile << 5 | col_in_chunk) and
+// an f32 value. Every block's length is a multiple of 8 (padding entries are 0xFFFF),
+// so each block starts 16-byte aligned in both arrays and one bulk copy fetches it.
+// The order of the entries inside a block is free: each lands on its own cell of the
+// densified tile, so the products do not depend on it.
+struct Blocked {
+  uint64_t rows = 0, K = 0;
+  uint32_t n_tiles = 0, n_chunks = 0;
+  uint64_t nnz_padded = 0;
+  DeviceBuffer<uint64_t> off;
+  DeviceBuffer<uint16_t> idx;
+  DeviceBuffer<float> val;
+};
+
+// The blocked layout of a CSR matrix (n_rows x n_cols, u32 column indices, each row's
+// columns strictly increasing), or of its transpose (rows = the CSR's columns).
+void build_blocked(const uint64_t* ptr, const uint32_t* col, const float* val, uint64_t n_rows,
+                   uint64_t n_cols, uint64_t nnz, bool transpose, Blocked& out, cudaStream_t s);
+
 enum : int { kOutRows = 0, kOutPartial = 1 };
+enum : int { kValuePlain = 0, kValueCentredSquare = 1 };
 
 // Where C = S D goes.
 struct SpmmOut {
@@ -26,12 +49,10 @@ struct SpmmOut {
 };
 
 struct SpmmArgs {
-  const uint64_t* ptr = nullptr;   // CSR row pointers (rows + 1)
-  const uint16_t* col16 = nullptr; // column indices, 16-bit ...
-  const uint32_t* col32 = nullptr; // ... or 32-bit
-  const float* val = nullptr;
-  uint64_t rows = 0, K = 0;
-  uint64_t seg_len = 0;            // K per work item (a multiple of 32)
+  const Blocked* s = nullptr;      // the sparse operand
+  int value_mode = kValuePlain;    // kValueCentredSquare: (v - row_means[row])^2
+  const double* row_means = nullptr;
+  uint64_t seg_chunks = 0;         // K-chunks (32 columns) per work item
   const float* dt_hi = nullptr;    // D^T, 64 x K, tf32 parts, row stride ld_t floats
   const float* dt_lo = nullptr;
   uint64_t ld_t = 0;
