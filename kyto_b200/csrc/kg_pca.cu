@@ -129,6 +129,14 @@ __global__ void omega_kernel(const uint64_t* cells, uint64_t n, uint32_t width,
   }
 }
 
+// D^T = [1 ... 1; 0 ...] (row 0 ones over the n cells, everything else zero).
+__global__ void fill_rows_kernel(float* hi, float* lo, uint64_t n, uint64_t ld) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= 64 * ld) return;
+  hi[i] = (i < n) ? 1.0f : 0.0f;
+  lo[i] = 0.0f;
+}
+
 __global__ void fill_kernel(double* p, uint64_t n, double v) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i < n) p[i] = v;
@@ -424,6 +432,166 @@ jacobi_svd_kernel(double* a, uint32_t g, uint32_t w, double* sigma, uint32_t* or
   }
 }
 
+constexpr uint32_t kQrMaxCols = 64;
+
+// The thin SVD's left singular vectors of the g x w column-major block `b` (w <= 64,
+// overwritten), one CTA of 32 warps: Householder QR in place (b = Q R, the reflectors
+// below the diagonal, LAPACK's dlarfg convention v_j = 1), then Hestenes' one-sided
+// Jacobi on R in shared memory (R V = U_R diag(sigma); pairs orthogonal to 1e-15 of
+// their norms), then U = Q [U_R; 0] by applying the reflectors backwards. QR is
+// backward stable, so sigma carries an absolute error of about 1e-16 |b|: the drop rule
+// (sigma > 1e-10 |b|_F) sees rank deficiency as an SVD of b would.
+// Outputs: sigma (w, descending; ties to the lower column), u (g x w: column c the
+// unit vector of sigma[c]). status: 0, or 1 if 60 sweeps did not converge.
+__global__ void __launch_bounds__(1024)
+qr_svd_kernel(double* b, uint32_t g, uint32_t w, double* sigma, double* u, int* status) {
+  __shared__ double rs[kQrMaxCols][kQrMaxCols + 1];  // R, then U_R diag(sigma), by column
+  __shared__ double tau[kQrMaxCols];
+  __shared__ double norms[kQrMaxCols];
+  __shared__ uint32_t order[kQrMaxCols];
+  __shared__ int rotated;
+  const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const unsigned warps = blockDim.x >> 5;
+  auto colp = [&](uint32_t c) { return b + (uint64_t)c * g; };
+
+  // Householder QR.
+  for (uint32_t j = 0; j < w; ++j) {
+    if (warp == 0) {
+      const double* bj = colp(j);
+      double ss = 0.0;
+      for (uint32_t i = j + 1 + lane; i < g; i += 32) ss = fma(bj[i], bj[i], ss);
+      for (int o = 16; o; o >>= 1) ss += __shfl_xor_sync(0xFFFFFFFFu, ss, o);
+      if (lane == 0) {
+        double alpha = bj[j];
+        double normx = sqrt(fma(alpha, alpha, ss));
+        if (ss == 0.0) {
+          tau[j] = 0.0;  // already upper triangular in this column
+        } else {
+          double beta = alpha >= 0.0 ? -normx : normx;
+          tau[j] = (beta - alpha) / beta;
+          norms[j] = 1.0 / (alpha - beta);  // scale of v below the diagonal
+          colp(j)[j] = beta;
+        }
+      }
+    }
+    __syncthreads();
+    const double t = tau[j];
+    if (t != 0.0) {
+      double* bj = colp(j);
+      const double sc = norms[j];
+      for (uint32_t i = j + 1 + threadIdx.x; i < g; i += blockDim.x) bj[i] *= sc;
+      __syncthreads();
+      for (uint32_t c = j + 1 + warp; c < w; c += warps) {
+        double* bc = colp(c);
+        double d = (lane == 0) ? bc[j] : 0.0;
+        for (uint32_t i = j + 1 + lane; i < g; i += 32) d = fma(bj[i], bc[i], d);
+        for (int o = 16; o; o >>= 1) d += __shfl_xor_sync(0xFFFFFFFFu, d, o);
+        const double f = t * d;
+        if (lane == 0) bc[j] -= f;
+        for (uint32_t i = j + 1 + lane; i < g; i += 32) bc[i] = fma(-f, bj[i], bc[i]);
+      }
+    }
+    __syncthreads();
+  }
+  // R into shared memory.
+  for (uint32_t x = threadIdx.x; x < w * w; x += blockDim.x) {
+    uint32_t c = x / w, r = x % w;
+    rs[c][r] = r <= c ? colp(c)[r] : 0.0;
+  }
+  __syncthreads();
+  // One-sided Jacobi on R's columns (round-robin tournament, one warp per pair).
+  const uint32_t players = (w + 1) & ~1u;
+  int sweep = 0;
+  for (; sweep < 60; ++sweep) {
+    if (threadIdx.x == 0) rotated = 0;
+    __syncthreads();
+    for (uint32_t r = 0; r + 1 < players; ++r) {
+      for (uint32_t pr = warp; pr < players / 2; pr += warps) {
+        auto at = [&](uint32_t pos) {
+          return pos == 0 ? 0u : ((pos - 1 + r) % (players - 1)) + 1;
+        };
+        uint32_t i = at(pr), j2 = at(players - 1 - pr);
+        if (i > j2) {
+          uint32_t tt = i;
+          i = j2;
+          j2 = tt;
+        }
+        if (j2 >= w) continue;
+        double al = 0.0, be = 0.0, ga = 0.0;
+        for (uint32_t x = lane; x < w; x += 32) {
+          double p = rs[i][x], q = rs[j2][x];
+          al = fma(p, p, al);
+          be = fma(q, q, be);
+          ga = fma(p, q, ga);
+        }
+        for (int o = 16; o; o >>= 1) {
+          al += __shfl_xor_sync(0xFFFFFFFFu, al, o);
+          be += __shfl_xor_sync(0xFFFFFFFFu, be, o);
+          ga += __shfl_xor_sync(0xFFFFFFFFu, ga, o);
+        }
+        if (!(al > 0.0) || !(be > 0.0) || !(fabs(ga) > 1e-15 * sqrt(al) * sqrt(be))) continue;
+        double zeta = (be - al) / (2.0 * ga);
+        double tn = (zeta >= 0.0 ? 1.0 : -1.0) / (fabs(zeta) + hypot(1.0, zeta));
+        double cs = 1.0 / sqrt(1.0 + tn * tn), sn = cs * tn;
+        for (uint32_t x = lane; x < w; x += 32) {
+          double p = rs[i][x], q = rs[j2][x];
+          rs[i][x] = cs * p - sn * q;
+          rs[j2][x] = sn * p + cs * q;
+        }
+        if (lane == 0) rotated = 1;
+      }
+      __syncthreads();
+    }
+    bool again = rotated != 0;
+    __syncthreads();
+    if (!again) break;
+  }
+  // Column norms = singular values; the order (descending, ties to the lower column).
+  for (uint32_t c = warp; c < w; c += warps) {
+    double ss = 0.0;
+    for (uint32_t x = lane; x < w; x += 32) ss = fma(rs[c][x], rs[c][x], ss);
+    for (int o = 16; o; o >>= 1) ss += __shfl_xor_sync(0xFFFFFFFFu, ss, o);
+    if (lane == 0) norms[c] = sqrt(ss);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (uint32_t c = 0; c < w; ++c) order[c] = c;
+    for (uint32_t c = 1; c < w; ++c) {
+      uint32_t v = order[c], pos = c;
+      while (pos > 0 && norms[order[pos - 1]] < norms[v]) {
+        order[pos] = order[pos - 1];
+        --pos;
+      }
+      order[pos] = v;
+    }
+    for (uint32_t c = 0; c < w; ++c) sigma[c] = norms[order[c]];
+    *status = sweep >= 60 ? 1 : 0;
+  }
+  __syncthreads();
+  // U = Q [U_R; 0]: start from U_R's unit columns, apply H_{w-1}, ..., H_0.
+  for (uint64_t x = threadIdx.x; x < (uint64_t)g * w; x += blockDim.x) {
+    uint32_t c = (uint32_t)(x / g), r = (uint32_t)(x % g);
+    double nv = norms[order[c]];
+    u[x] = (r < w && nv > 0.0) ? rs[order[c]][r] / nv : 0.0;
+  }
+  __syncthreads();
+  for (int j = (int)w - 1; j >= 0; --j) {
+    const double t = tau[j];
+    if (t == 0.0) continue;
+    const double* v = colp(j);
+    for (uint32_t c = warp; c < w; c += warps) {
+      double* uc = u + (uint64_t)c * g;
+      double d = (lane == 0) ? uc[j] : 0.0;
+      for (uint32_t i = j + 1 + lane; i < g; i += 32) d = fma(v[i], uc[i], d);
+      for (int o = 16; o; o >>= 1) d += __shfl_xor_sync(0xFFFFFFFFu, d, o);
+      const double f = t * d;
+      if (lane == 0) uc[j] -= f;
+      for (uint32_t i = j + 1 + lane; i < g; i += 32) uc[i] = fma(-f, v[i], uc[i]);
+    }
+    __syncthreads();
+  }
+}
+
 // out[:, c] = a[:, order[c]] / sigma[c] (the left singular vectors kept).
 __global__ void gather_unit_columns_kernel(const double* a, uint32_t g, uint32_t keep,
                                            const double* sigma, const uint32_t* order,
@@ -591,11 +759,21 @@ struct TcHeld {
     transposed(width, out, s);
   }
 
-  // out (g x w column-major) = X^T W with W^T in dt.
-  void transposed(uint32_t w, double* out, cudaStream_t s) {
+  // D^T = a row of ones (the stored values' gene sums, counts, squares).
+  void ones_column() {
+    fill_rows_kernel<<<blocks_for(64 * n_ld, 256), 256, 0, dt_hi.stream>>>(dt_hi.ptr, dt_lo.ptr, n, n_ld);
+    KG_LAUNCH_CHECK();
+  }
+
+  // out (g x w column-major) = X^T W with W^T in dt (the stored values mapped by
+  // value_mode first).
+  void transposed(uint32_t w, double* out, cudaStream_t s, int value_mode = kValuePlain,
+                  const double* row_means = nullptr) {
     uint64_t segs = (bxt.n_chunks + kSegChunks - 1) / kSegChunks;
     DeviceBuffer<double> partial(segs * g * 64, s);
     SpmmArgs a;
+    a.value_mode = value_mode;
+    a.row_means = row_means;
     a.s = &bxt;
     a.seg_chunks = kSegChunks;
     a.dt_hi = dt_hi.ptr;
@@ -809,12 +987,20 @@ struct Dense {
                               proj.ptr, m, &one, rest.ptr, g));
       }
     }
-    // Thin SVD by one-sided Jacobi in one kernel (the block is at most 64 columns).
+    // Thin SVD in one kernel: QR + Jacobi on R for blocks of up to 64 columns (and
+    // g >= w, always true here), one-sided Jacobi on the whole block beyond that.
     if (w > kJacobiMaxCols) fail(KG_ERR_INVALID, "pca: a Krylov block wider than 256 columns");
     DeviceBuffer<double> sv(w, s);
     DeviceBuffer<uint32_t> order(w, s);
     DeviceBuffer<int> info(1, s);
-    jacobi_svd_kernel<<<1, 1024, 0, s>>>(rest.ptr, g, w, sv.ptr, order.ptr, info.ptr);
+    DeviceBuffer<double> u;
+    const bool qr = w <= kQrMaxCols;
+    if (qr) {
+      u.alloc((uint64_t)g * w, s);
+      qr_svd_kernel<<<1, 1024, 0, s>>>(rest.ptr, g, w, sv.ptr, u.ptr, info.ptr);
+    } else {
+      jacobi_svd_kernel<<<1, 1024, 0, s>>>(rest.ptr, g, w, sv.ptr, order.ptr, info.ptr);
+    }
     KG_LAUNCH_CHECK();
     std::vector<double> h_sv(w);
     int h_info = 0;
@@ -828,9 +1014,13 @@ struct Dense {
     *keep_out = keep;
     if (keep == 0) return none;
     DeviceBuffer<double> out((uint64_t)g * keep, s);
-    gather_unit_columns_kernel<<<blocks_for((uint64_t)g * keep, 256), 256, 0, s>>>(
-        rest.ptr, g, keep, sv.ptr, order.ptr, out.ptr);
-    KG_LAUNCH_CHECK();
+    if (qr) {
+      KG_CUDA(cudaMemcpyAsync(out.ptr, u.ptr, out.bytes(), cudaMemcpyDeviceToDevice, s));
+    } else {
+      gather_unit_columns_kernel<<<blocks_for((uint64_t)g * keep, 256), 256, 0, s>>>(
+          rest.ptr, g, keep, sv.ptr, order.ptr, out.ptr);
+      KG_LAUNCH_CHECK();
+    }
     return out;
   }
 
@@ -863,10 +1053,60 @@ void kg_pca::run() {
   c->done = 0;
 
   Trace trace(s, "pca");
-  // The gene-major twin of the held input (each gene's values in cell order), cut into
-  // segments: the genes' exact f64 statistics, and the SIMT products' operand.
+  // The products run on the tensor cores (tf32 parts, f32 sums of at most 512 terms
+  // flushed into f64) when the genes fit 16-bit positions, the block one 64-column tile,
+  // and no gene's mean dwarfs its spread (the rows are centred after the product, so
+  // the products' relative error is scaled by |mean| / sd: at most 64, about 2^-15);
+  // else on the SIMT pipes in f64 (kyto's arithmetic, any data).
+  const char* pchoice = std::getenv("KYTO_GPU_PCA_PRODUCTS");
+  bool tc = g <= 65535 && l <= 64 && k <= 64 && !(pchoice && std::string(pchoice) == "simt");
+  means.alloc(g, s);
+  std::vector<double> squares(g), h_means(g);
+  std::vector<uint64_t> colptr(g + 1);
+  TcHeld th;
   GeneMajor gm;
-  {
+  auto check_means = [&]() {
+    for (uint32_t i = 0; i < g; ++i)
+      if (!std::isfinite(h_means[i]))
+        fail(KG_ERR_INVALID, "pca: gene " + std::to_string(i) +
+                                 " holds a value that is not finite (NaN or infinity)");
+  };
+  if (tc) {
+    // Gene means (pass 0's sums, pca.rs:707-717), stored counts and centred sums of
+    // squares over the stored values (the last pass's, pca.rs:664-676), as products
+    // with a column of ones.
+    th.build(indptr.ptr, col.ptr, val.ptr, n, g, nnz, c->sm_count, s);
+    trace.mark("blocked layouts");
+    DeviceBuffer<double> sums(g, s), cnt(g, s), sq(g, s);
+    th.ones_column();
+    th.transposed(1, sums.ptr, s, kValuePlain, nullptr);
+    divide_kernel<<<blocks_for(g, 256), 256, 0, s>>>(sums.ptr, g, (double)n, means.ptr);
+    KG_LAUNCH_CHECK();
+    th.transposed(1, cnt.ptr, s, kValueOne, nullptr);
+    th.transposed(1, sq.ptr, s, kValueCentredSquare, means.ptr);
+    std::vector<double> h_cnt(g);
+    KG_CUDA(cudaMemcpyAsync(h_means.data(), means.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaMemcpyAsync(squares.data(), sq.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaMemcpyAsync(h_cnt.data(), cnt.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+    check_means();
+    colptr[0] = 0;
+    for (uint32_t i = 0; i < g; ++i) colptr[i + 1] = colptr[i] + (uint64_t)std::llround(h_cnt[i]);
+    double worst_ratio = 0.0;
+    for (uint32_t i = 0; i < g; ++i) {
+      uint64_t stored = colptr[i + 1] - colptr[i];
+      double var = (squares[i] + (double)(n - stored) * h_means[i] * h_means[i]) / (double)n;
+      if (var > 0.0) worst_ratio = std::max(worst_ratio, h_means[i] * h_means[i] / var);
+    }
+    if (worst_ratio > 4096.0) {
+      tc = false;
+      th = TcHeld();
+    }
+    trace.mark("gene statistics");
+  }
+  if (!tc) {
+    // The gene-major twin of the held input (each gene's values in cell order), cut into
+    // segments: the genes' exact f64 statistics and the SIMT products' operand.
     DeviceBuffer<uint32_t> row_of(nnz, s), iota(nnz, s);
     row_of_kernel<<<blocks_for(n * 32, 256), 256, 0, s>>>(indptr.ptr, n, row_of.ptr);
     KG_LAUNCH_CHECK();
@@ -885,15 +1125,7 @@ void kg_pca::run() {
       KG_LAUNCH_CHECK();
     }
     gm.build_segments(g, nnz, s);
-  }
-  trace.mark("gene-major twin");
-
-  // Gene means (pass 0's sums, pca.rs:707-717) and centred sums of squares over the
-  // stored values (the last pass's, pca.rs:664-676), in f64 in a fixed order.
-  means.alloc(g, s);
-  std::vector<double> squares(g), h_means(g);
-  std::vector<uint64_t> colptr(g + 1);
-  {
+    trace.mark("gene-major twin");
     DeviceBuffer<double> ones(n, s), sums(g, s), sq(g, s);
     fill_kernel<<<blocks_for(n, 256), 256, 0, s>>>(ones.ptr, n, 1.0);
     KG_LAUNCH_CHECK();
@@ -905,31 +1137,10 @@ void kg_pca::run() {
     KG_CUDA(cudaMemcpyAsync(squares.data(), sq.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
     KG_CUDA(cudaMemcpyAsync(colptr.data(), gm.colptr.ptr, (g + 1) * 8ull, cudaMemcpyDeviceToHost, s));
     KG_CUDA(cudaStreamSynchronize(s));
+    check_means();
+    trace.mark("gene statistics");
   }
-  for (uint32_t i = 0; i < g; ++i)
-    if (!std::isfinite(h_means[i]))
-      fail(KG_ERR_INVALID, "pca: gene " + std::to_string(i) +
-                               " holds a value that is not finite (NaN or infinity)");
-  trace.mark("gene statistics");
-
-  // The products run on the tensor cores (tf32 parts, f32 sums of at most 512 terms
-  // flushed into f64) when the genes fit 16-bit positions, the block one 64-column tile,
-  // and no gene's mean dwarfs its spread (the rows are centred after the product, so
-  // the products' relative error is scaled by |mean| / sd: at most 64, about 2^-15);
-  // else on the SIMT pipes in f64 (kyto's arithmetic, any data).
-  double worst_ratio = 0.0;
-  for (uint32_t i = 0; i < g; ++i) {
-    uint64_t stored = colptr[i + 1] - colptr[i];
-    double var = (squares[i] + (double)(n - stored) * h_means[i] * h_means[i]) / (double)n;
-    if (var > 0.0) worst_ratio = std::max(worst_ratio, h_means[i] * h_means[i] / var);
-  }
-  const char* pchoice = std::getenv("KYTO_GPU_PCA_PRODUCTS");
-  const bool tc = g <= 65535 && l <= 64 && k <= 64 && worst_ratio <= 4096.0 &&
-                  !(pchoice && std::string(pchoice) == "simt");
   products_engine = tc ? "tensor-core" : "simt";
-  TcHeld th;
-  if (tc) th.build(indptr.ptr, col.ptr, val.ptr, n, g, nnz, c->sm_count, s);
-  trace.mark(tc ? "blocked layouts" : "no blocked layouts");
 
   Dense dense{this, s, g};
   auto colsums = [&](const double* m, uint32_t w, uint32_t ld, double* out) {

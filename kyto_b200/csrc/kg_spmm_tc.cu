@@ -191,6 +191,8 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
           if (value_mode == kValueCentredSquare) {
             float d = v - (float)row_means[(uint64_t)tile * kRows + r];
             v = d * d;
+          } else if (value_mode == kValueOne) {
+            v = 1.0f;
           }
           const float h = tf32_round(v);
           const uint32_t o = sw128_offset(r, kk);

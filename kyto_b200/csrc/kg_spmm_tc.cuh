@@ -30,7 +30,7 @@ void build_blocked(const uint64_t* ptr, const uint32_t* col, const float* val, u
                    uint64_t n_cols, uint64_t nnz, bool transpose, Blocked& out, cudaStream_t s);
 
 enum : int { kOutRows = 0, kOutPartial = 1 };
-enum : int { kValuePlain = 0, kValueCentredSquare = 1 };
+enum : int { kValuePlain = 0, kValueCentredSquare = 1, kValueOne = 2 };
 
 // Where C = S D goes.
 struct SpmmOut {
@@ -50,7 +50,8 @@ struct SpmmOut {
 
 struct SpmmArgs {
   const Blocked* s = nullptr;      // the sparse operand
-  int value_mode = kValuePlain;    // kValueCentredSquare: (v - row_means[row])^2
+  int value_mode = kValuePlain;    // kValueCentredSquare: (v - row_means[row])^2;
+                                   // kValueOne: 1 for every stored value
   const double* row_means = nullptr;
   uint64_t seg_chunks = 0;         // K-chunks (32 columns) per work item
   const float* dt_hi = nullptr;    // D^T, 64 x K, tf32 parts, row stride ld_t floats
