@@ -11,6 +11,7 @@
 //     (too many, or an approximate key outside its slack) is flagged;
 //  3. full rows: flagged rows searched against every row with exact keys.
 // So every row is the CPU's brute-force row, bit for bit.
+#include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_segmented_radix_sort.cuh>
 
 #include <algorithm>
@@ -76,6 +77,81 @@ __global__ void max_kernel(const double* v, uint64_t n, double* out) {
     __syncthreads();
   }
   if (threadIdx.x == 0) *out = red[0];
+}
+
+// Each component's range over the rows (first three components).
+__global__ void range_kernel(const float* x, uint64_t n, uint32_t width, uint32_t dims,
+                             const double* mean, float* lo_hi) {
+  __shared__ float lo[3][256], hi[3][256];
+  float l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (uint64_t r = threadIdx.x; r < n; r += blockDim.x)
+    for (uint32_t j = 0; j < dims; ++j) {
+      float v = (float)((double)x[r * width + j] - mean[j]);
+      l[j] = fminf(l[j], v);
+      h[j] = fmaxf(h[j], v);
+    }
+  for (uint32_t j = 0; j < 3; ++j) {
+    lo[j][threadIdx.x] = l[j];
+    hi[j][threadIdx.x] = h[j];
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    float a = INFINITY, b = -INFINITY;
+    for (unsigned t = 0; t < blockDim.x; ++t) {
+      a = fminf(a, lo[threadIdx.x][t]);
+      b = fmaxf(b, hi[threadIdx.x][t]);
+    }
+    lo_hi[2 * threadIdx.x] = a;
+    lo_hi[2 * threadIdx.x + 1] = b;
+  }
+}
+
+__device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 10 bits -> every third bit
+  v &= 0x3FFu;
+  v = (v | (v << 16)) & 0x030000FFu;
+  v = (v | (v << 8)) & 0x0300F00Fu;
+  v = (v | (v << 4)) & 0x030C30C3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__global__ void morton_kernel(const float* x, uint64_t n, uint32_t width, uint32_t dims,
+                              const double* mean, const float* lo_hi, uint32_t* key,
+                              uint32_t* row) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  uint32_t code = 0;
+  for (uint32_t j = 0; j < dims; ++j) {
+    float v = (float)((double)x[r * width + j] - mean[j]);
+    float span = lo_hi[2 * j + 1] - lo_hi[2 * j];
+    float t = span > 0.0f ? (v - lo_hi[2 * j]) / span : 0.0f;
+    uint32_t q = (uint32_t)fminf(fmaxf(t * 1023.0f, 0.0f), 1023.0f);
+    code |= spread3(q) << j;
+  }
+  key[r] = code;
+  row[r] = (uint32_t)r;
+}
+
+// The rows in Morton order of their first (up to) three centred components: nearby rows
+// end up in nearby tiles. Any order gives the same graph; this one makes the filter's
+// threshold tight early.
+void spatial_order(const float* x, uint64_t n, uint32_t width, uint32_t d, const double* mean,
+                   DeviceBuffer<uint32_t>& perm, cudaStream_t s) {
+  uint32_t dims = d < 3 ? d : 3;
+  DeviceBuffer<float> lo_hi(6, s);
+  range_kernel<<<1, 256, 0, s>>>(x, n, width, dims, mean, lo_hi.ptr);
+  KG_LAUNCH_CHECK();
+  DeviceBuffer<uint32_t> key(n, s), key_sorted(n, s), rows(n, s);
+  morton_kernel<<<blocks_for(n, 256), 256, 0, s>>>(x, n, width, dims, mean, lo_hi.ptr, key.ptr,
+                                                   rows.ptr);
+  KG_LAUNCH_CHECK();
+  perm.alloc(n, s);
+  size_t temp = 0;
+  KG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, key.ptr, key_sorted.ptr, rows.ptr,
+                                          perm.ptr, (int)n, 0, 30, s));
+  DeviceBuffer<unsigned char> scratch(temp, s);
+  KG_CUDA(cub::DeviceRadixSort::SortPairs(scratch.ptr, temp, key.ptr, key_sorted.ptr, rows.ptr,
+                                          perm.ptr, (int)n, 0, 30, s));
 }
 
 void max_kernel_launch(const double* v, uint64_t n, double* out, cudaStream_t s) {
@@ -272,25 +348,28 @@ __device__ void warp_merge(const double* keys, const uint32_t* idx, uint32_t len
 // An approximate key a stands for the squared distance a * inv_s2 + qn2[q] (the
 // tensor-core filter's keys are scaled and shifted by the query's norm; the SIMT
 // filter's are distances already: inv_s2 = 1, qn2 = NULL).
+// With `perm`, the filter ran on the rows in scan order: its query position qp and its
+// candidates' rows are positions there, row perm[.] of x (ranks and outputs use x's).
 __global__ void rank_kernel(const float* __restrict__ x, uint32_t width, uint32_t d,
                             uint64_t q_begin, uint64_t q_end, uint32_t k, uint32_t cap,
                             const float* cand_key, const uint32_t* cand_row,
                             const uint32_t* cand_count, const float* threshold,
                             const double* slack, double inv_s2, const double* qn2,
-                            double* out_key, uint32_t* out_row,
+                            const uint32_t* perm, double* out_key, uint32_t* out_row,
                             uint32_t* full_flag, unsigned long long* n_candidates) {
   uint64_t qi = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   unsigned lane = threadIdx.x & 31u;
-  uint64_t q = q_begin + qi;
-  if (q >= q_end) return;
+  uint64_t qp = q_begin + qi;
+  if (qp >= q_end) return;
+  uint64_t q = perm ? perm[qp] : qp;
   uint32_t count = cand_count[qi];
   if (count == kOverflow) {
     if (lane == 0) full_flag[q] = 1;
     return;
   }
   float th = threshold[qi];
-  double sl = slack[q];
-  double shift = qn2 ? qn2[q] : 0.0;
+  double sl = slack[qp];
+  double shift = qn2 ? qn2[qp] : 0.0;
   const float* qrow = x + q * width;
   double keys[kMaxK];
   uint32_t idx[kMaxK];
@@ -301,6 +380,7 @@ __global__ void rank_kernel(const float* __restrict__ x, uint32_t width, uint32_
     float ak = cand_key[qi * (uint64_t)cap + c];
     if (ak > th) continue;
     uint32_t p = cand_row[qi * (uint64_t)cap + c];
+    if (perm) p = perm[p];
     double e = exact_key(qrow, x + (uint64_t)p * width, d);
     if (fabs(e - ((double)ak * inv_s2 + shift)) > sl) bad = true;
     offer(keys, idx, len, k, e, p);
@@ -497,14 +577,19 @@ extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t 
       DeviceBuffer<double> qn2(n, s), slack_d(n, s);
       double scale = 1.0;
       Timer tf(s);
-      tc_filter(ctx, s, x, n, width, d, mean.ptr, filter == "bf16", k, cap, cand_key.ptr,
-                cand_row.ptr, cand_count.ptr, thr.ptr, qn2.ptr, slack_d.ptr, &scale);
+      // Scan order: the rows sorted by a Morton code of their first three centred
+      // components, so a query block's own tiles hold its nearest points.
+      DeviceBuffer<uint32_t> perm;
+      spatial_order(x, n, width, d, mean.ptr, perm, s);
+      tc_filter(ctx, s, x, n, width, d, perm.ptr, mean.ptr, filter == "bf16", k, cap,
+                cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr, qn2.ptr, slack_d.ptr,
+                &scale);
       filter_ms += tf.stop_ms();
       check_cancel(ctx);
       Timer tr(s);
       rank_kernel<<<blocks_for(n * 32, kRankWarps * 32), kRankWarps * 32, 0, s>>>(
           x, width, d, 0, n, k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
-          slack_d.ptr, 1.0 / (scale * scale), qn2.ptr, out_key.ptr, out_row.ptr,
+          slack_d.ptr, 1.0 / (scale * scale), qn2.ptr, perm.ptr, out_key.ptr, out_row.ptr,
           full_flag.ptr, n_cand.ptr);
       KG_LAUNCH_CHECK();
       rank_ms += tr.stop_ms();
@@ -526,7 +611,8 @@ extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t 
         Timer tr(s);
         rank_kernel<<<blocks_for((q1 - q0) * 32, kRankWarps * 32), kRankWarps * 32, 0, s>>>(
             x, width, d, q0, q1, k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
-            slack.ptr, 1.0, nullptr, out_key.ptr, out_row.ptr, full_flag.ptr, n_cand.ptr);
+            slack.ptr, 1.0, nullptr, nullptr, out_key.ptr, out_row.ptr, full_flag.ptr,
+            n_cand.ptr);
         KG_LAUNCH_CHECK();
         rank_ms += tr.stop_ms();
         ctx->done = q1;

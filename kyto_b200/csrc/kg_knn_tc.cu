@@ -71,21 +71,10 @@ struct QueryState {
   bool overflowed;
 };
 
-// Offer approximate key `key` of point `p` (already <= st.th) to the query's state.
-__device__ __noinline__ void tc_offer(QueryState& st, float* smallest, uint32_t k,
-                                      double slack2, float key, uint32_t p, float* ck,
-                                      uint32_t* cr, uint32_t cap) {
-  if (st.n_small < k || key < smallest[k - 1]) {
-    if (st.n_small < k) ++st.n_small;
-    uint32_t at = st.n_small - 1;
-    while (at > 0 && smallest[at - 1] > key) {
-      smallest[at] = smallest[at - 1];
-      --at;
-    }
-    smallest[at] = key;
-    if (st.n_small == k) st.th = round_up_f32d((double)smallest[k - 1] + slack2);
-  }
-  if (!(key <= st.th)) return;
+// Append candidate (key, p) (already <= st.th) to the query's slice, compacting it
+// against the threshold when it reaches compact_at (neighbors_exact.rs:236-252).
+__device__ __noinline__ void tc_append(QueryState& st, float key, uint32_t p, float* ck,
+                                       uint32_t* cr, uint32_t cap) {
   if (st.count == cap) {
     st.overflowed = true;
     return;
@@ -109,6 +98,53 @@ __device__ __noinline__ void tc_offer(QueryState& st, float* smallest, uint32_t 
   }
 }
 
+// Offer approximate key `key` of point `p` (already <= st.th) to the query's state: its
+// k smallest keys in local memory (any k up to kMaxK).
+__device__ __noinline__ void tc_offer(QueryState& st, float* smallest, uint32_t k,
+                                      double slack2, float key, uint32_t p, float* ck,
+                                      uint32_t* cr, uint32_t cap) {
+  if (st.n_small < k || key < smallest[k - 1]) {
+    if (st.n_small < k) ++st.n_small;
+    uint32_t at = st.n_small - 1;
+    while (at > 0 && smallest[at - 1] > key) {
+      smallest[at] = smallest[at - 1];
+      --at;
+    }
+    smallest[at] = key;
+    if (st.n_small == k) st.th = round_up_f32d((double)smallest[k - 1] + slack2);
+  }
+  if (key <= st.th) tc_append(st, key, p, ck, cr, cap);
+}
+
+// The k smallest keys (k <= KR) in registers, ascending, +inf past those seen: one
+// insertion is 2 KR min/max with no branch and no memory (v[i] = max(v[i-1], min(v[i],
+// key)), all on the old values).
+template <int KR>
+struct RegTopK {
+  float v[KR];
+  __device__ __forceinline__ void init() {
+#pragma unroll
+    for (int i = 0; i < KR; ++i) v[i] = INFINITY;
+  }
+  // Insert key; returns the new k-th smallest.
+  __device__ __forceinline__ float insert(float key, uint32_t k) {
+    float prev = v[0];
+    v[0] = fminf(v[0], key);
+#pragma unroll
+    for (int i = 1; i < KR; ++i) {
+      const float cur = v[i];
+      v[i] = fmaxf(prev, fminf(cur, key));
+      prev = cur;
+    }
+    float kth = v[0];
+#pragma unroll
+    for (int i = 1; i < KR; ++i) kth = (i == (int)k - 1) ? v[i] : kth;
+    return kth;
+  }
+};
+
+// KR > 0: the k smallest keys live in registers (k <= KR); KR == 0: in local memory.
+template <int KR>
 __global__ void __launch_bounds__(kTcThreads, 1)
 knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
                      const __grid_constant__ CUtensorMap tmap_p, uint64_t n, uint32_t k,
@@ -168,7 +204,10 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
             break;
           }
           mbar_arrive_expect_tx(&sm.full[s], kTileBytes);
-          tma_load_2d(sm.b[s], &tmap_p, &sm.full[s], 0, (int32_t)(t * kTcPoints));
+          // The scan starts at the query block's own tiles: with the rows in a spatial
+          // order the nearest points come first and the threshold falls at once.
+          const uint32_t pt = (uint32_t)((t + qb * (kTcQueries / kTcPoints)) % n_tiles);
+          tma_load_2d(sm.b[s], &tmap_p, &sm.full[s], 0, (int32_t)(pt * kTcPoints));
           issued_phase[s] = (int)ph;
         }
       }
@@ -220,13 +259,16 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
     // ------------------------------------------------------------ epilogue --------
     const uint32_t half = (uint32_t)warp >> 2, quad = (uint32_t)warp & 3;
     float* my = sm.scratch[threadIdx.x];
-    float smallest[kMaxK];
+    float smallest[KR == 0 ? kMaxK : 1];
+    RegTopK<KR == 0 ? 1 : KR> topk;
     uint64_t it = 0;
     bool ok = true;
     for (uint64_t qb = blockIdx.x; qb < n_qblocks && ok; qb += gridDim.x) {
       const uint64_t q = qb * kTcQueries + half * 128 + quad * 32 + lane;
       const bool active = q < n;
       QueryState st{INFINITY, 0, 0, 64, false};
+      topk.init();
+      float kth = INFINITY;
       const double sl2 = active ? (double)slack2[q] : 0.0;
       float* ck = cand_key + (active ? q : 0) * (uint64_t)cap;
       uint32_t* cr = cand_row + (active ? q : 0) * (uint64_t)cap;
@@ -265,14 +307,24 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
                 my[j] = key;
                 mask |= (key <= th0 ? 1u : 0u) << j;
               }
-              const uint64_t p0 = (uint64_t)t * kTcPoints + c * 32;
+              const uint32_t pt = (uint32_t)((t + qb * (kTcQueries / kTcPoints)) % n_tiles);
+              const uint64_t p0 = (uint64_t)pt * kTcPoints + c * 32;
               while (mask && !st.overflowed) {
                 const int j = __ffs(mask) - 1;
                 mask &= mask - 1;
                 const float key = my[j];
                 const uint64_t p = p0 + j;
-                if (key <= st.th && p < n && p != q)
-                  tc_offer(st, smallest, k, sl2, key, (uint32_t)p, ck, cr, cap);
+                if (key <= st.th && p < n && p != q) {
+                  if constexpr (KR > 0) {
+                    if (key < kth) {
+                      kth = topk.insert(key, k);
+                      if (kth < INFINITY) st.th = round_up_f32d((double)kth + sl2);
+                    }
+                    if (key <= st.th) tc_append(st, key, (uint32_t)p, ck, cr, cap);
+                  } else {
+                    tc_offer(st, smallest, k, sl2, key, (uint32_t)p, ck, cr, cap);
+                  }
+                }
               }
             }
           }
@@ -300,16 +352,17 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
 // (unscaled, f64) and the row's doubled slack in scaled units.
 template <class H>
 __global__ void tc_operands_kernel(const float* x, uint64_t n, uint32_t width, uint32_t d,
-                                   const double* mean, double scale, double u, double eta,
-                                   const double* max_sq, H* aq, H* bp, double* qn2,
-                                   float* slack2, double* slack_d) {
+                                   const uint32_t* perm, const double* mean, double scale,
+                                   double u, double eta, const double* max_sq, H* aq, H* bp,
+                                   double* qn2, float* slack2, double* slack_d) {
   uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (r >= n) return;
+  const float* xr = x + (uint64_t)(perm ? perm[r] : r) * width;
   double n2 = 0.0, n2s = 0.0;
   for (uint32_t j = 0; j < kTcK; ++j) {
     H a = H(0.0f), b = H(0.0f);
     if (j < d) {
-      double c = (double)x[r * width + j] - mean[j];
+      double c = (double)xr[j] - mean[j];
       double cs = c * scale;
       n2 += c * c;
       n2s += cs * cs;
@@ -401,7 +454,8 @@ CUtensorMap tile_map(const void* base, uint64_t rows, bool bf16) {
 }  // namespace
 
 void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint64_t n, uint32_t width,
-               uint32_t d, const double* mean, bool bf16, uint32_t k, uint32_t cap,
+               uint32_t d, const uint32_t* perm, const double* mean, bool bf16, uint32_t k,
+               uint32_t cap,
                float* cand_key, uint32_t* cand_row, uint32_t* cand_count, float* threshold,
                double* qn2, double* slack_d, double* out_scale) {
   if (d + 3 > (uint32_t)kTcK) fail(KG_ERR_INVALID, "tensor-core filter: more than 61 components");
@@ -428,26 +482,32 @@ void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint64_t n, uint32_t
   DeviceBuffer<float> slack2(n, s);
   if (bf16)
     tc_operands_kernel<__nv_bfloat16><<<blocks_for(n, 128), 128, 0, s>>>(
-        x, n, width, d, mean, scale, u, eta, max_sq.ptr, (__nv_bfloat16*)aq.ptr,
+        x, n, width, d, perm, mean, scale, u, eta, max_sq.ptr, (__nv_bfloat16*)aq.ptr,
         (__nv_bfloat16*)bp.ptr, qn2, slack2.ptr, slack_d);
   else
     tc_operands_kernel<__half><<<blocks_for(n, 128), 128, 0, s>>>(
-        x, n, width, d, mean, scale, u, eta, max_sq.ptr, (__half*)aq.ptr, (__half*)bp.ptr,
+        x, n, width, d, perm, mean, scale, u, eta, max_sq.ptr, (__half*)aq.ptr, (__half*)bp.ptr,
         qn2, slack2.ptr, slack_d);
   KG_LAUNCH_CHECK();
   CUtensorMap mq = tile_map(aq.ptr, n, bf16), mp = tile_map(bp.ptr, n, bf16);
   static std::once_flag attr;
   std::call_once(attr, [] {
-    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kTcSmemBytes));
+    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<16>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes));
+    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<32>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes));
+    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<0>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes));
   });
   DeviceBuffer<int> err(1, s);
   err.zero();
   uint64_t n_qblocks = (n + kTcQueries - 1) / kTcQueries;
   unsigned grid = (unsigned)std::min<uint64_t>(n_qblocks, (uint64_t)ctx->sm_count);
   uint32_t idesc = idesc_f32acc(bf16 ? 1u : 0u, 128, kTcPoints);
-  knn_filter_tc_kernel<<<grid, kTcThreads, kTcSmemBytes, s>>>(
-      mq, mp, n, k, slack2.ptr, idesc, cap, cand_key, cand_row, cand_count, threshold, err.ptr);
+  auto kernel = k <= 16 ? knn_filter_tc_kernel<16>
+                : k <= 32 ? knn_filter_tc_kernel<32> : knn_filter_tc_kernel<0>;
+  kernel<<<grid, kTcThreads, kTcSmemBytes, s>>>(mq, mp, n, k, slack2.ptr, idesc, cap, cand_key,
+                                                cand_row, cand_count, threshold, err.ptr);
   KG_LAUNCH_CHECK();
   int h_err = 0;
   KG_CUDA(cudaMemcpyAsync(&h_err, err.ptr, 4, cudaMemcpyDeviceToHost, s));

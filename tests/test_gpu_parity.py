@@ -158,6 +158,25 @@ def test_pca_refusals(ctx):
               ctx=ctx)
 
 
+@pytest.mark.parametrize("offset", [1e6, 1e7])
+def test_pca_large_means_are_centred_row_by_row(ctx, offset):
+    # kyto's tests/it/pca.rs:486-506: values * 8 + offset, a rank-3 spread. The
+    # tensor-core products cannot resolve the spread under such means, so the session
+    # takes the f64 products; the result must still match the f64 oracle.
+    rng = np.random.default_rng(int(offset) % 97)
+    basis = rng.normal(size=(3, 12))
+    dense = (rng.normal(size=(200, 3)) @ basis + 0.01 * rng.normal(size=(200, 12))) * 8 + offset
+    dense = dense.astype(np.float32)
+    indptr = np.arange(0, 201 * 12, 12, dtype=np.uint64)
+    idx = np.tile(np.arange(12, dtype=np.uint32), 200)
+    vals = dense.reshape(-1)
+    res = K.pca(indptr, idx, vals, 12, 3, ctx=ctx)
+    ref = O.pca(O.Csr(indptr, idx, vals, 12), 3)
+    assert np.max(np.abs(res.variance - ref.variance) / ref.variance) <= 1e-6
+    for c in range(3):
+        assert _col_diff(res.embedding[:, c], ref.embedding[:, c]) <= 1e-5
+
+
 def test_pca_rank_deficient_completes_loadings(ctx, products):
     # Two distinct cells: one direction of variance; kyto completes the loadings with
     # orthonormal zero-variance directions (pca_dense.rs complement).
