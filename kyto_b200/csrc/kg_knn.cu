@@ -39,14 +39,71 @@ __global__ void finite_check_kernel(const float* x, uint64_t n, uint32_t width, 
   }
 }
 
-// Column means in f64, columns summed in row order by one thread each (fixed order).
-__global__ void column_mean_kernel(const float* x, uint64_t n, uint32_t width, uint32_t d,
-                                   double* mean) {
-  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+// Column sums, minima and maxima of the leading d components, per chunk of kMeanRows
+// rows (4 row classes of 64 column threads, combined in a fixed order), then over the
+// chunks in order (column_finish_kernel): the same bits on every run.
+constexpr uint32_t kMeanRows = 2048;
+
+__global__ void __launch_bounds__(256)
+column_partial_kernel(const float* x, uint64_t n, uint32_t width, uint32_t d, double* part_sum,
+                      float* part_lo, float* part_hi) {
+  __shared__ double ss[4][64];
+  __shared__ float sl[4][64], sh[4][64];
+  const uint32_t j = threadIdx.x & 63u, g = threadIdx.x >> 6;
+  const uint64_t r0 = blockIdx.x * (uint64_t)kMeanRows;
+  const uint64_t r1 = r0 + kMeanRows < n ? r0 + kMeanRows : n;
+  double sum = 0.0;
+  float lo = INFINITY, hi = -INFINITY;
+  if (j < d)
+    for (uint64_t r = r0 + g; r < r1; r += 4) {
+      const float v = x[r * width + j];
+      sum = __dadd_rn(sum, (double)v);
+      lo = fminf(lo, v);
+      hi = fmaxf(hi, v);
+    }
+  ss[g][j] = sum;
+  sl[g][j] = lo;
+  sh[g][j] = hi;
+  __syncthreads();
+  if (g == 0 && j < d) {
+    part_sum[blockIdx.x * 64ull + j] =
+        __dadd_rn(__dadd_rn(ss[0][j], ss[1][j]), __dadd_rn(ss[2][j], ss[3][j]));
+    part_lo[blockIdx.x * 64ull + j] = fminf(fminf(sl[0][j], sl[1][j]), fminf(sl[2][j], sl[3][j]));
+    part_hi[blockIdx.x * 64ull + j] = fmaxf(fmaxf(sh[0][j], sh[1][j]), fmaxf(sh[2][j], sh[3][j]));
+  }
+}
+
+// mean[j] (f64) and, for the first three components, the range of the centred values
+// f32(x - mean) (that map is monotonic, so the range is the centred raw range).
+__global__ void column_finish_kernel(const double* part_sum, const float* part_lo,
+                                     const float* part_hi, uint32_t n_parts, uint64_t n,
+                                     uint32_t d, double* mean, float* lo_hi) {
+  const uint32_t j = threadIdx.x;
   if (j >= d) return;
-  double s = 0.0;
-  for (uint64_t r = 0; r < n; ++r) s = __dadd_rn(s, (double)x[r * width + j]);
-  mean[j] = s / (double)n;
+  double sum = 0.0;
+  float lo = INFINITY, hi = -INFINITY;
+  for (uint32_t b = 0; b < n_parts; ++b) {
+    sum = __dadd_rn(sum, part_sum[b * 64ull + j]);
+    lo = fminf(lo, part_lo[b * 64ull + j]);
+    hi = fmaxf(hi, part_hi[b * 64ull + j]);
+  }
+  const double m = sum / (double)n;
+  mean[j] = m;
+  if (j < 3) {
+    lo_hi[2 * j] = (float)((double)lo - m);
+    lo_hi[2 * j + 1] = (float)((double)hi - m);
+  }
+}
+
+void column_stats(const float* x, uint64_t n, uint32_t width, uint32_t d, double* mean,
+                  float* lo_hi, cudaStream_t s) {
+  const uint32_t parts = (uint32_t)((n + kMeanRows - 1) / kMeanRows);
+  DeviceBuffer<double> sum(parts * 64ull, s);
+  DeviceBuffer<float> lo(parts * 64ull, s), hi(parts * 64ull, s);
+  column_partial_kernel<<<parts, 256, 0, s>>>(x, n, width, d, sum.ptr, lo.ptr, hi.ptr);
+  KG_LAUNCH_CHECK();
+  column_finish_kernel<<<1, 64, 0, s>>>(sum.ptr, lo.ptr, hi.ptr, parts, n, d, mean, lo_hi);
+  KG_LAUNCH_CHECK();
 }
 
 // Centred f32 rows padded to kDim (zeros), their f32 squared norms and f64 squares.
@@ -79,33 +136,6 @@ __global__ void max_kernel(const double* v, uint64_t n, double* out) {
   if (threadIdx.x == 0) *out = red[0];
 }
 
-// Each component's range over the rows (first three components).
-__global__ void range_kernel(const float* x, uint64_t n, uint32_t width, uint32_t dims,
-                             const double* mean, float* lo_hi) {
-  __shared__ float lo[3][256], hi[3][256];
-  float l[3] = {INFINITY, INFINITY, INFINITY}, h[3] = {-INFINITY, -INFINITY, -INFINITY};
-  for (uint64_t r = threadIdx.x; r < n; r += blockDim.x)
-    for (uint32_t j = 0; j < dims; ++j) {
-      float v = (float)((double)x[r * width + j] - mean[j]);
-      l[j] = fminf(l[j], v);
-      h[j] = fmaxf(h[j], v);
-    }
-  for (uint32_t j = 0; j < 3; ++j) {
-    lo[j][threadIdx.x] = l[j];
-    hi[j][threadIdx.x] = h[j];
-  }
-  __syncthreads();
-  if (threadIdx.x < 3) {
-    float a = INFINITY, b = -INFINITY;
-    for (unsigned t = 0; t < blockDim.x; ++t) {
-      a = fminf(a, lo[threadIdx.x][t]);
-      b = fmaxf(b, hi[threadIdx.x][t]);
-    }
-    lo_hi[2 * threadIdx.x] = a;
-    lo_hi[2 * threadIdx.x + 1] = b;
-  }
-}
-
 __device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 10 bits -> every third bit
   v &= 0x3FFu;
   v = (v | (v << 16)) & 0x030000FFu;
@@ -136,13 +166,10 @@ __global__ void morton_kernel(const float* x, uint64_t n, uint32_t width, uint32
 // end up in nearby tiles. Any order gives the same graph; this one makes the filter's
 // threshold tight early.
 void spatial_order(const float* x, uint64_t n, uint32_t width, uint32_t d, const double* mean,
-                   DeviceBuffer<uint32_t>& perm, cudaStream_t s) {
+                   const float* lo_hi, DeviceBuffer<uint32_t>& perm, cudaStream_t s) {
   uint32_t dims = d < 3 ? d : 3;
-  DeviceBuffer<float> lo_hi(6, s);
-  range_kernel<<<1, 256, 0, s>>>(x, n, width, dims, mean, lo_hi.ptr);
-  KG_LAUNCH_CHECK();
   DeviceBuffer<uint32_t> key(n, s), key_sorted(n, s), rows(n, s);
-  morton_kernel<<<blocks_for(n, 256), 256, 0, s>>>(x, n, width, dims, mean, lo_hi.ptr, key.ptr,
+  morton_kernel<<<blocks_for(n, 256), 256, 0, s>>>(x, n, width, dims, mean, lo_hi, key.ptr,
                                                    rows.ptr);
   KG_LAUNCH_CHECK();
   perm.alloc(n, s);
@@ -542,8 +569,8 @@ extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t 
     }
     Trace trace(s, "knn_exact");
     DeviceBuffer<double> mean(d, s), squares(n, s), slack(n, s), largest(1, s);
-    DeviceBuffer<float> rows(n * kDim, s), offsets(n, s);
-    column_mean_kernel<<<blocks_for(d, 64), 64, 0, s>>>(x, n, width, d, mean.ptr);
+    DeviceBuffer<float> rows(n * kDim, s), offsets(n, s), lo_hi(6, s);
+    column_stats(x, n, width, d, mean.ptr, lo_hi.ptr, s);
     centre_kernel<<<blocks_for(n, 128), 128, 0, s>>>(x, n, width, d, mean.ptr, rows.ptr,
                                                      offsets.ptr, squares.ptr);
     max_kernel<<<1, 256, 0, s>>>(squares.ptr, n, largest.ptr);
@@ -580,7 +607,7 @@ extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t 
       // Scan order: the rows sorted by a Morton code of their first three centred
       // components, so a query block's own tiles hold its nearest points.
       DeviceBuffer<uint32_t> perm;
-      spatial_order(x, n, width, d, mean.ptr, perm, s);
+      spatial_order(x, n, width, d, mean.ptr, lo_hi.ptr, perm, s);
       tc_filter(ctx, s, x, n, width, d, perm.ptr, mean.ptr, filter == "bf16", k, cap,
                 cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr, qn2.ptr, slack_d.ptr,
                 &scale);
