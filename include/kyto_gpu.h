@@ -96,6 +96,29 @@ KG_API kg_status kg_hvg_moments(kg_ctx* ctx, const uint64_t* indptr, const uint3
                          uint32_t n_genes, double target_sum, int32_t log1p,
                          double* sums, double* sums_of_squares, uint64_t* positives);
 
+/* kg_hvg_moments without any allocation. No counterpart in the reference: kyto's
+ * fold_rows allocates freely; this variant is for callers that cannot, such as a
+ * process whose device memory is already held by another allocator's pool (a PyTorch
+ * caching allocator, a fixed arena), where a fresh cudaMallocAsync can fail with
+ * out-of-memory while the pool still has room, or a per-block fold deep in a long
+ * streaming pass that must not fail late for lack of memory.
+ * Same arguments and results as kg_hvg_moments, with these limits:
+ * - indptr, indices and values must be device memory (staging host inputs would
+ *   allocate); the outputs may be host or device memory;
+ * - at most 1,048,576 stored values per block and 65,536 genes; larger inputs return
+ *   KG_ERR_INVALID before any launch.
+ * Its scratch is one fixed 22.1 MB array of static device memory per device. The first
+ * call on a device sets it up (cudaGetSymbolAddress, which loads the code module there),
+ * so make that call before any stream capture. Every call on a device shares the
+ * array: calls that overlap in time (two contexts on one device from two threads, or a
+ * call made while the kernels of a call that returned KG_CANCELLED or KG_ERR_TIMEOUT
+ * still run) race on it and give wrong results. */
+KG_API kg_status kg_hvg_moments_noalloc(kg_ctx* ctx, const uint64_t* indptr,
+                                        const uint32_t* indices, const void* values,
+                                        kg_dtype dtype, uint64_t n_rows, uint32_t n_genes,
+                                        double target_sum, int32_t log1p, double* sums,
+                                        double* sums_of_squares, uint64_t* positives);
+
 /* seurat flags from the moments (host arithmetic on n_genes values, as kyto runs it on
  * the host): crates/kyto-exec/src/hvg.rs:284-361,393-437,501-580. n_top_genes < 0
  * uses scanpy's mean/dispersion cutoffs. Outputs are host arrays of n_genes. */

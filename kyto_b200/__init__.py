@@ -37,7 +37,7 @@ KYTO_CODE = {
 # Every entry point of include/kyto_gpu.h.
 EXPORTS = (
     "kg_open", "kg_close", "kg_last_error", "kg_set_cancel_flag", "kg_progress",
-    "kg_normalize_log1p", "kg_hvg_moments", "kg_hvg_seurat",
+    "kg_normalize_log1p", "kg_hvg_moments", "kg_hvg_moments_noalloc", "kg_hvg_seurat",
     "kg_pca_begin", "kg_pca_push_block", "kg_pca_run", "kg_pca_results", "kg_pca_info",
     "kg_pca_embedding_device", "kg_pca_free", "kg_knn_exact", "kg_diag_kernel_launches",
 )
@@ -91,6 +91,8 @@ def library() -> ctypes.CDLL:
             "kg_progress": [P, P, P],
             "kg_normalize_log1p": [P, P, P, ctypes.c_int, U64, ctypes.c_double, I32, P],
             "kg_hvg_moments": [P, P, P, P, ctypes.c_int, U64, U32, ctypes.c_double, I32, P, P, P],
+            "kg_hvg_moments_noalloc": [P, P, P, P, ctypes.c_int, U64, U32, ctypes.c_double, I32,
+                                       P, P, P],
             "kg_hvg_seurat": [P, P, P, U64, U32, ctypes.c_int64, P, P, P, P],
             "kg_pca_begin": [P, ctypes.POINTER(_PcaParams), ctypes.POINTER(P)],
             "kg_pca_push_block": [P, P, P, P, ctypes.c_int, U64, P],

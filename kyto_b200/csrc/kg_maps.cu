@@ -394,3 +394,151 @@ kg_status kg_hvg_seurat(const double* sums, const double* sums_of_squares,
 }
 
 }  // extern "C"
+
+// ------------------------------------------ seurat moments in fixed scratch ----------
+
+namespace kg {
+
+constexpr size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// The limits of kg_hvg_moments_noalloc and the layout of its scratch (byte offsets):
+// two flags, the sort's key and payload double buffers, the per-gene arrays, the radix
+// sort's temporary storage. 22.1 MB in all.
+constexpr uint64_t kNoAllocMaxValues = 1ull << 20;  // stored values of one block
+constexpr uint32_t kNoAllocMaxGenes = 1u << 16;
+constexpr size_t kNoAllocValues = align256(kNoAllocMaxValues * 4);
+constexpr size_t kNoAllocGenes = align256(((size_t)kNoAllocMaxGenes + 1) * 8);
+constexpr size_t kNoAllocKeys0 = 256;
+constexpr size_t kNoAllocKeys1 = kNoAllocKeys0 + kNoAllocValues;
+constexpr size_t kNoAllocVals0 = kNoAllocKeys1 + kNoAllocValues;
+constexpr size_t kNoAllocVals1 = kNoAllocVals0 + kNoAllocValues;
+constexpr size_t kNoAllocColptr = kNoAllocVals1 + kNoAllocValues;
+constexpr size_t kNoAllocSums = kNoAllocColptr + kNoAllocGenes;
+constexpr size_t kNoAllocSquares = kNoAllocSums + kNoAllocGenes;
+constexpr size_t kNoAllocPositives = kNoAllocSquares + kNoAllocGenes;
+constexpr size_t kNoAllocSort = kNoAllocPositives + kNoAllocGenes;
+constexpr size_t kNoAllocSortBytes = 4u << 20;
+constexpr size_t kNoAllocBytes = kNoAllocSort + kNoAllocSortBytes;
+
+// One array per device (this module's static device memory), shared by every call on
+// that device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocDevices = 64;
+
+// The scratch's device address on `device` (which must be current). The first call on
+// a device resolves it with cudaGetSymbolAddress, which loads this module there, and
+// checks that the radix sort's storage for the largest block fits its slot.
+unsigned char* noalloc_scratch(int device) {
+  static std::mutex mu;
+  static unsigned char* resolved[kNoAllocDevices] = {};
+  if (device < 0 || device >= kNoAllocDevices)
+    fail(KG_ERR_INVALID, "kg_hvg_moments_noalloc: device ordinal above 63");
+  std::lock_guard<std::mutex> lock(mu);
+  if (resolved[device]) return resolved[device];
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) fail_cuda(e, "cudaGetSymbolAddress (fixed scratch)", __FILE__, __LINE__);
+  size_t temp = 0;
+  cub::DoubleBuffer<uint32_t> keys(nullptr, nullptr), vals(nullptr, nullptr);
+  KG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, keys, vals, (int)kNoAllocMaxValues, 0,
+                                          bits_for(kNoAllocMaxGenes + 1)));
+  if (temp > kNoAllocSortBytes)
+    fail(KG_ERR_DEVICE, "kg_hvg_moments_noalloc: the radix sort wants " +
+                            std::to_string(temp) + " bytes, above its fixed slot");
+  resolved[device] = (unsigned char*)p;
+  return resolved[device];
+}
+
+}  // namespace kg
+
+extern "C" {
+
+kg_status kg_hvg_moments_noalloc(kg_ctx* ctx, const uint64_t* indptr, const uint32_t* indices,
+                                 const void* values, kg_dtype dtype, uint64_t n_rows,
+                                 uint32_t n_genes, double target_sum, int32_t log1p,
+                                 double* sums, double* sums_of_squares, uint64_t* positives) {
+  return guarded([&] {
+    if (!ctx || !indptr || !sums || !sums_of_squares || !positives)
+      fail(KG_ERR_INVALID, "kg_hvg_moments_noalloc: NULL argument");
+    if (dtype != KG_U32 && dtype != KG_F32) fail(KG_ERR_INVALID, "unknown dtype");
+    if (n_genes > kNoAllocMaxGenes)
+      fail(KG_ERR_INVALID, "kg_hvg_moments_noalloc: " + std::to_string(n_genes) +
+                               " genes, above its limit of " +
+                               std::to_string(kNoAllocMaxGenes) + " (use kg_hvg_moments)");
+    use_device(ctx);
+    if (!is_device_pointer(indptr))
+      fail(KG_ERR_INVALID, "kg_hvg_moments_noalloc: indptr must be device memory");
+    unsigned char* base = noalloc_scratch(ctx->device);
+    cudaStream_t s = ctx->stream;
+    uint64_t nnz = 0;
+    KG_CUDA(cudaMemcpyAsync(&nnz, indptr + n_rows, 8, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+    if (nnz > kNoAllocMaxValues)
+      fail(KG_ERR_INVALID, "kg_hvg_moments_noalloc: a block of " + std::to_string(nnz) +
+                               " stored values, above its limit of " +
+                               std::to_string(kNoAllocMaxValues) + " (use kg_hvg_moments)");
+    if (nnz && (!is_device_pointer(indices) || !is_device_pointer(values)))
+      fail(KG_ERR_INVALID, "kg_hvg_moments_noalloc: indices and values must be device memory");
+    int* inexact = (int*)base;
+    unsigned int* max_index = (unsigned int*)(base + 4);
+    uint32_t* keys0 = (uint32_t*)(base + kNoAllocKeys0);
+    uint32_t* keys1 = (uint32_t*)(base + kNoAllocKeys1);
+    float* vals0 = (float*)(base + kNoAllocVals0);
+    float* vals1 = (float*)(base + kNoAllocVals1);
+    uint64_t* colptr = (uint64_t*)(base + kNoAllocColptr);
+    double* dsum = (double*)(base + kNoAllocSums);
+    double* dsq = (double*)(base + kNoAllocSquares);
+    uint64_t* dpos = (uint64_t*)(base + kNoAllocPositives);
+    KG_CUDA(cudaMemsetAsync(base, 0, 8, s));  // both flags start at zero
+    cub::DoubleBuffer<uint32_t> keys(keys0, keys1), vals((uint32_t*)vals0, (uint32_t*)vals1);
+    if (nnz) {
+      unsigned blocks = std::min<unsigned>(blocks_for(nnz, 256), 4096);
+      max_index_kernel<<<blocks, 256, 0, s>>>(indices, nnz, max_index);
+      KG_LAUNCH_CHECK();
+      unsigned int h = 0;
+      KG_CUDA(cudaMemcpyAsync(&h, max_index, 4, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaStreamSynchronize(s));
+      if (h >= n_genes)
+        fail(KG_ERR_INVALID, "a block holds gene index " + std::to_string(h) + " but has " +
+                                 std::to_string(n_genes) + " genes");
+      const int* flag = nullptr;
+      if (dtype == KG_U32 && !std::isnan(target_sum)) {
+        inexact_counts_kernel<<<blocks, 256, 0, s>>>((const uint32_t*)values, nnz, inexact);
+        KG_LAUNCH_CHECK();
+        flag = inexact;
+      }
+      if (dtype == KG_U32)
+        launch_normalize<uint32_t>(indptr, values, n_rows, target_sum, log1p, flag, vals0, s);
+      else
+        launch_normalize<float>(indptr, values, n_rows, target_sum, log1p, flag, vals0, s);
+      expm1_kernel<<<std::min<unsigned>(blocks_for(nnz, 256), 8192), 256, 0, s>>>(vals0, nnz,
+                                                                                 vals0);
+      KG_LAUNCH_CHECK();
+      // The sort may write either half of each double buffer: the keys start as a copy.
+      KG_CUDA(cudaMemcpyAsync(keys0, indices, nnz * 4, cudaMemcpyDeviceToDevice, s));
+      size_t temp = 0;
+      int end_bit = bits_for(n_genes + 1);
+      KG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, keys, vals, (int)nnz, 0, end_bit,
+                                              s));
+      if (temp > kNoAllocSortBytes)
+        fail(KG_ERR_DEVICE, "kg_hvg_moments_noalloc: the radix sort wants " +
+                                std::to_string(temp) + " bytes, above its fixed slot");
+      temp = kNoAllocSortBytes;
+      KG_CUDA(cub::DeviceRadixSort::SortPairs(base + kNoAllocSort, temp, keys, vals, (int)nnz,
+                                              0, end_bit, s));
+    }
+    if (n_genes) {
+      column_starts(keys.Current(), nnz, n_genes, colptr, s);
+      gene_moments_kernel<<<blocks_for(n_genes, 128), 128, 0, s>>>(
+          colptr, (const float*)vals.Current(), n_genes, dsum, dsq, dpos);
+      KG_LAUNCH_CHECK();
+      KG_CUDA(cudaMemcpyAsync(sums, dsum, n_genes * 8ull, cudaMemcpyDefault, s));
+      KG_CUDA(cudaMemcpyAsync(sums_of_squares, dsq, n_genes * 8ull, cudaMemcpyDefault, s));
+      KG_CUDA(cudaMemcpyAsync(positives, dpos, n_genes * 8ull, cudaMemcpyDefault, s));
+    }
+    wait_stream(ctx, s);
+  });
+}
+
+}  // extern "C"
