@@ -64,6 +64,25 @@ __device__ __forceinline__ float round_up_f32d(double v) {
   return r;
 }
 
+// The smallest of 32 keys held as f32 bits, by three-input minima (a tree, for
+// independent instructions).
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ float min_of_32(const uint32_t (&r)[32]) {
+  float m[11];
+#pragma unroll
+  for (int i = 0; i < 10; ++i)
+    m[i] = min3f(__uint_as_float(r[3 * i]), __uint_as_float(r[3 * i + 1]),
+                 __uint_as_float(r[3 * i + 2]));
+  m[10] = fminf(__uint_as_float(r[30]), __uint_as_float(r[31]));
+  const float a = min3f(m[0], m[1], m[2]), b = min3f(m[3], m[4], m[5]);
+  const float c = min3f(m[6], m[7], m[8]), d = fminf(m[9], m[10]);
+  return fminf(min3f(a, b, c), d);
+}
+
 // Per-query filter state (kyto's Query, neighbors_exact.rs:196-255).
 struct QueryState {
   float th;
@@ -116,35 +135,22 @@ __device__ __noinline__ void tc_offer(QueryState& st, float* smallest, uint32_t 
   if (key <= st.th) tc_append(st, key, p, ck, cr, cap);
 }
 
-// The k smallest keys (k <= KR) in registers, ascending, +inf past those seen: one
-// insertion is 2 KR min/max with no branch and no memory (v[i] = max(v[i-1], min(v[i],
-// key)), all on the old values).
-template <int KR>
-struct RegTopK {
-  float v[KR];
-  __device__ __forceinline__ void init() {
-#pragma unroll
-    for (int i = 0; i < KR; ++i) v[i] = INFINITY;
+// Offer the keys of one 32-point chunk selected by `mask` (bit j: point p0 + j, key
+// keys[j]), in column order, to the query's state. Out of line: the filter's hot loop
+// keeps only the threshold in registers and spends nothing on this rare path's state.
+__device__ __noinline__ void tc_offer_chunk(QueryState& st, float* smallest, uint32_t k,
+                                            double slack2, const float* keys, uint32_t mask,
+                                            uint64_t p0, uint64_t q, uint64_t n, float* ck,
+                                            uint32_t* cr, uint32_t cap) {
+  while (mask && !st.overflowed) {
+    const int j = __ffs(mask) - 1;
+    mask &= mask - 1;
+    const float key = keys[j];
+    const uint64_t p = p0 + j;
+    if (key <= st.th && p < n && p != q) tc_offer(st, smallest, k, slack2, key, (uint32_t)p, ck, cr, cap);
   }
-  // Insert key; returns the new k-th smallest.
-  __device__ __forceinline__ float insert(float key, uint32_t k) {
-    float prev = v[0];
-    v[0] = fminf(v[0], key);
-#pragma unroll
-    for (int i = 1; i < KR; ++i) {
-      const float cur = v[i];
-      v[i] = fmaxf(prev, fminf(cur, key));
-      prev = cur;
-    }
-    float kth = v[0];
-#pragma unroll
-    for (int i = 1; i < KR; ++i) kth = (i == (int)k - 1) ? v[i] : kth;
-    return kth;
-  }
-};
+}
 
-// KR > 0: the k smallest keys live in registers (k <= KR); KR == 0: in local memory.
-template <int KR>
 __global__ void __launch_bounds__(kTcThreads, 1)
 knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
                      const __grid_constant__ CUtensorMap tmap_p, uint64_t n, uint32_t k,
@@ -257,18 +263,23 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
     }
   } else {
     // ------------------------------------------------------------ epilogue --------
+    // Per tile: the 128 keys come out of TMEM 64 columns at a time and only their
+    // minimum per 32-column chunk is kept (few registers: no spills in the hot loop).
+    // A chunk whose minimum reaches the threshold (rare once it has fallen) is read
+    // again by the whole warp (tcgen05.ld is warp-wide) and its passing keys offered.
+    // The threshold and overflow flag stay in registers; the rest of the state is
+    // touched only on offers.
     const uint32_t half = (uint32_t)warp >> 2, quad = (uint32_t)warp & 3;
     float* my = sm.scratch[threadIdx.x];
-    float smallest[KR == 0 ? kMaxK : 1];
-    RegTopK<KR == 0 ? 1 : KR> topk;
+    float smallest[kMaxK];
     uint64_t it = 0;
     bool ok = true;
     for (uint64_t qb = blockIdx.x; qb < n_qblocks && ok; qb += gridDim.x) {
       const uint64_t q = qb * kTcQueries + half * 128 + quad * 32 + lane;
       const bool active = q < n;
       QueryState st{INFINITY, 0, 0, 64, false};
-      topk.init();
-      float kth = INFINITY;
+      float th = INFINITY;
+      bool live = active;  // not overflowed
       const double sl2 = active ? (double)slack2[q] : 0.0;
       float* ck = cand_key + (active ? q : 0) * (uint64_t)cap;
       uint32_t* cr = cand_row + (active ? q : 0) * (uint64_t)cap;
@@ -279,60 +290,52 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           break;
         }
         tc_fence_after();
-        // All 128 keys of the tile into registers with one wait, then the accumulator
-        // goes straight back to the MMA warp; the keys are scanned meanwhile.
         __syncwarp();
-        uint32_t r[kTcPoints / 32][32];
         const uint32_t base = tmem + ((quad * 32u) << 16) + ab * 256u + half * 128u;
+        float mins[kTcPoints / 32];
 #pragma unroll
-        for (int c = 0; c < kTcPoints / 32; ++c) tmem_ld_32(base + c * 32u, r[c]);
-        tmem_wait_ld();
+        for (int hf = 0; hf < kTcPoints / 64; ++hf) {
+          uint32_t r0[32], r1[32];
+          tmem_ld_32(base + hf * 64u, r0);
+          tmem_ld_32(base + hf * 64u + 32u, r1);
+          tmem_wait_ld();
+          mins[2 * hf] = min_of_32(r0);
+          mins[2 * hf + 1] = min_of_32(r1);
+        }
+        uint32_t hits = 0;
+#pragma unroll
+        for (int c = 0; c < kTcPoints / 32; ++c) hits |= (live && mins[c] <= th ? 1u : 0u) << c;
+        uint32_t any = __reduce_or_sync(0xFFFFFFFFu, hits);
+#pragma unroll 1
+        while (any) {
+          const int c = __ffs(any) - 1;
+          any &= any - 1;
+          uint32_t r[32];
+          tmem_ld_32(base + c * 32u, r);
+          tmem_wait_ld();
+          if (!((hits >> c) & 1u) || !live) continue;
+          // Only the keys at or under the threshold, in column order (the threshold
+          // only falls while they are offered).
+          uint32_t mask = 0;
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const float key = __uint_as_float(r[j]);
+            my[j] = key;
+            mask |= (key <= th ? 1u : 0u) << j;
+          }
+          const uint32_t pt = (uint32_t)((t + qb * (kTcQueries / kTcPoints)) % n_tiles);
+          const uint64_t p0 = (uint64_t)pt * kTcPoints + c * 32;
+          tc_offer_chunk(st, smallest, k, sl2, my, mask, p0, q, n, ck, cr, cap);
+          th = st.th;
+          live = !st.overflowed;
+        }
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.tmem_empty[ab]);
-        if (active && !st.overflowed) {
-#pragma unroll
-          for (int c = 0; c < kTcPoints / 32; ++c) {
-            float m = __uint_as_float(r[c][0]);
-#pragma unroll
-            for (int j = 1; j < 32; ++j) m = fminf(m, __uint_as_float(r[c][j]));
-            if (m <= st.th) {
-              // Only the keys at or under the threshold, in column order (the threshold
-              // only falls while they are offered).
-              uint32_t mask = 0;
-              const float th0 = st.th;
-#pragma unroll
-              for (int j = 0; j < 32; ++j) {
-                const float key = __uint_as_float(r[c][j]);
-                my[j] = key;
-                mask |= (key <= th0 ? 1u : 0u) << j;
-              }
-              const uint32_t pt = (uint32_t)((t + qb * (kTcQueries / kTcPoints)) % n_tiles);
-              const uint64_t p0 = (uint64_t)pt * kTcPoints + c * 32;
-              while (mask && !st.overflowed) {
-                const int j = __ffs(mask) - 1;
-                mask &= mask - 1;
-                const float key = my[j];
-                const uint64_t p = p0 + j;
-                if (key <= st.th && p < n && p != q) {
-                  if constexpr (KR > 0) {
-                    if (key < kth) {
-                      kth = topk.insert(key, k);
-                      if (kth < INFINITY) st.th = round_up_f32d((double)kth + sl2);
-                    }
-                    if (key <= st.th) tc_append(st, key, (uint32_t)p, ck, cr, cap);
-                  } else {
-                    tc_offer(st, smallest, k, sl2, key, (uint32_t)p, ck, cr, cap);
-                  }
-                }
-              }
-            }
-          }
-        }
       }
       if (active && ok) {
         cand_count[q] = st.overflowed ? kOverflow : st.count;
-        threshold_out[q] = st.th;
+        threshold_out[q] = th;
       }
     }
   }
@@ -492,21 +495,15 @@ void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint64_t n, uint32_t
   CUtensorMap mq = tile_map(aq.ptr, n, bf16), mp = tile_map(bp.ptr, n, bf16);
   static std::once_flag attr;
   std::call_once(attr, [] {
-    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<16>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes));
-    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<32>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes));
-    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<0>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes));
+    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kTcSmemBytes));
   });
   DeviceBuffer<int> err(1, s);
   err.zero();
   uint64_t n_qblocks = (n + kTcQueries - 1) / kTcQueries;
   unsigned grid = (unsigned)std::min<uint64_t>(n_qblocks, (uint64_t)ctx->sm_count);
   uint32_t idesc = idesc_f32acc(bf16 ? 1u : 0u, 128, kTcPoints);
-  auto kernel = k <= 16 ? knn_filter_tc_kernel<16>
-                : k <= 32 ? knn_filter_tc_kernel<32> : knn_filter_tc_kernel<0>;
-  kernel<<<grid, kTcThreads, kTcSmemBytes, s>>>(mq, mp, n, k, slack2.ptr, idesc, cap, cand_key,
+  knn_filter_tc_kernel<<<grid, kTcThreads, kTcSmemBytes, s>>>(mq, mp, n, k, slack2.ptr, idesc, cap, cand_key,
                                                 cand_row, cand_count, threshold, err.ptr);
   KG_LAUNCH_CHECK();
   int h_err = 0;

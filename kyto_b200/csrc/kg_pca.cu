@@ -434,72 +434,16 @@ jacobi_svd_kernel(double* a, uint32_t g, uint32_t w, double* sigma, uint32_t* or
 
 constexpr uint32_t kQrMaxCols = 64;
 
-// The thin SVD's left singular vectors of the g x w column-major block `b` (w <= 64,
-// overwritten), one CTA of 32 warps: Householder QR in place (b = Q R, the reflectors
-// below the diagonal, LAPACK's dlarfg convention v_j = 1), then Hestenes' one-sided
-// Jacobi on R in shared memory (R V = U_R diag(sigma); pairs orthogonal to 1e-15 of
-// their norms), then U = Q [U_R; 0] by applying the reflectors backwards. QR is
-// backward stable, so sigma carries an absolute error of about 1e-16 |b|: the drop rule
-// (sigma > 1e-10 |b|_F) sees rank deficiency as an SVD of b would.
-// Outputs: sigma (w, descending; ties to the lower column), u (g x w: column c the
-// unit vector of sigma[c]). status: 0, or 1 if 60 sweeps did not converge.
-__global__ void __launch_bounds__(1024)
-qr_svd_kernel(double* b, uint32_t g, uint32_t w, double* sigma, double* u, int* status) {
-  __shared__ double rs[kQrMaxCols][kQrMaxCols + 1];  // R, then U_R diag(sigma), by column
-  __shared__ double tau[kQrMaxCols];
-  __shared__ double norms[kQrMaxCols];
-  __shared__ uint32_t order[kQrMaxCols];
-  __shared__ int rotated;
+// Hestenes' one-sided Jacobi on the w columns of the w x w matrix in shared memory `rs`
+// (by column; round-robin tournament, one warp per pair, pairs orthogonal to 1e-15 of
+// their norms): rs becomes U_R diag(sigma). Then norms[c] = sigma of column c, order =
+// the columns by descending sigma (ties to the lower column), sigma[] (global) in that
+// order and *status = 0, or 1 if 60 sweeps did not converge. All threads call it.
+__device__ void jacobi_square(double (*rs)[kQrMaxCols + 1], uint32_t w, double* norms,
+                              uint32_t* order, int* rotated_flag, double* sigma, int* status) {
   const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   const unsigned warps = blockDim.x >> 5;
-  auto colp = [&](uint32_t c) { return b + (uint64_t)c * g; };
-
-  // Householder QR.
-  for (uint32_t j = 0; j < w; ++j) {
-    if (warp == 0) {
-      const double* bj = colp(j);
-      double ss = 0.0;
-      for (uint32_t i = j + 1 + lane; i < g; i += 32) ss = fma(bj[i], bj[i], ss);
-      for (int o = 16; o; o >>= 1) ss += __shfl_xor_sync(0xFFFFFFFFu, ss, o);
-      if (lane == 0) {
-        double alpha = bj[j];
-        double normx = sqrt(fma(alpha, alpha, ss));
-        if (ss == 0.0) {
-          tau[j] = 0.0;  // already upper triangular in this column
-        } else {
-          double beta = alpha >= 0.0 ? -normx : normx;
-          tau[j] = (beta - alpha) / beta;
-          norms[j] = 1.0 / (alpha - beta);  // scale of v below the diagonal
-          colp(j)[j] = beta;
-        }
-      }
-    }
-    __syncthreads();
-    const double t = tau[j];
-    if (t != 0.0) {
-      double* bj = colp(j);
-      const double sc = norms[j];
-      for (uint32_t i = j + 1 + threadIdx.x; i < g; i += blockDim.x) bj[i] *= sc;
-      __syncthreads();
-      for (uint32_t c = j + 1 + warp; c < w; c += warps) {
-        double* bc = colp(c);
-        double d = (lane == 0) ? bc[j] : 0.0;
-        for (uint32_t i = j + 1 + lane; i < g; i += 32) d = fma(bj[i], bc[i], d);
-        for (int o = 16; o; o >>= 1) d += __shfl_xor_sync(0xFFFFFFFFu, d, o);
-        const double f = t * d;
-        if (lane == 0) bc[j] -= f;
-        for (uint32_t i = j + 1 + lane; i < g; i += 32) bc[i] = fma(-f, bj[i], bc[i]);
-      }
-    }
-    __syncthreads();
-  }
-  // R into shared memory.
-  for (uint32_t x = threadIdx.x; x < w * w; x += blockDim.x) {
-    uint32_t c = x / w, r = x % w;
-    rs[c][r] = r <= c ? colp(c)[r] : 0.0;
-  }
-  __syncthreads();
-  // One-sided Jacobi on R's columns (round-robin tournament, one warp per pair).
+  int& rotated = *rotated_flag;
   const uint32_t players = (w + 1) & ~1u;
   int sweep = 0;
   for (; sweep < 60; ++sweep) {
@@ -568,6 +512,74 @@ qr_svd_kernel(double* b, uint32_t g, uint32_t w, double* sigma, double* u, int* 
     *status = sweep >= 60 ? 1 : 0;
   }
   __syncthreads();
+}
+
+// The thin SVD's left singular vectors of the g x w column-major block `b` (w <= 64,
+// overwritten), one CTA of 32 warps: Householder QR in place (b = Q R, the reflectors
+// below the diagonal, LAPACK's dlarfg convention v_j = 1), then Hestenes' one-sided
+// Jacobi on R in shared memory (R V = U_R diag(sigma); pairs orthogonal to 1e-15 of
+// their norms), then U = Q [U_R; 0] by applying the reflectors backwards. QR is
+// backward stable, so sigma carries an absolute error of about 1e-16 |b|: the drop rule
+// (sigma > 1e-10 |b|_F) sees rank deficiency as an SVD of b would.
+// Outputs: sigma (w, descending; ties to the lower column), u (g x w: column c the
+// unit vector of sigma[c]). status: 0, or 1 if 60 sweeps did not converge.
+__global__ void __launch_bounds__(1024)
+qr_svd_kernel(double* b, uint32_t g, uint32_t w, double* sigma, double* u, int* status) {
+  __shared__ double rs[kQrMaxCols][kQrMaxCols + 1];  // R, then U_R diag(sigma), by column
+  __shared__ double tau[kQrMaxCols];
+  __shared__ double norms[kQrMaxCols];
+  __shared__ uint32_t order[kQrMaxCols];
+  __shared__ int rotated;
+  const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const unsigned warps = blockDim.x >> 5;
+  auto colp = [&](uint32_t c) { return b + (uint64_t)c * g; };
+
+  // Householder QR.
+  for (uint32_t j = 0; j < w; ++j) {
+    if (warp == 0) {
+      const double* bj = colp(j);
+      double ss = 0.0;
+      for (uint32_t i = j + 1 + lane; i < g; i += 32) ss = fma(bj[i], bj[i], ss);
+      for (int o = 16; o; o >>= 1) ss += __shfl_xor_sync(0xFFFFFFFFu, ss, o);
+      if (lane == 0) {
+        double alpha = bj[j];
+        double normx = sqrt(fma(alpha, alpha, ss));
+        if (ss == 0.0) {
+          tau[j] = 0.0;  // already upper triangular in this column
+        } else {
+          double beta = alpha >= 0.0 ? -normx : normx;
+          tau[j] = (beta - alpha) / beta;
+          norms[j] = 1.0 / (alpha - beta);  // scale of v below the diagonal
+          colp(j)[j] = beta;
+        }
+      }
+    }
+    __syncthreads();
+    const double t = tau[j];
+    if (t != 0.0) {
+      double* bj = colp(j);
+      const double sc = norms[j];
+      for (uint32_t i = j + 1 + threadIdx.x; i < g; i += blockDim.x) bj[i] *= sc;
+      __syncthreads();
+      for (uint32_t c = j + 1 + warp; c < w; c += warps) {
+        double* bc = colp(c);
+        double d = (lane == 0) ? bc[j] : 0.0;
+        for (uint32_t i = j + 1 + lane; i < g; i += 32) d = fma(bj[i], bc[i], d);
+        for (int o = 16; o; o >>= 1) d += __shfl_xor_sync(0xFFFFFFFFu, d, o);
+        const double f = t * d;
+        if (lane == 0) bc[j] -= f;
+        for (uint32_t i = j + 1 + lane; i < g; i += 32) bc[i] = fma(-f, bj[i], bc[i]);
+      }
+    }
+    __syncthreads();
+  }
+  // R into shared memory.
+  for (uint32_t x = threadIdx.x; x < w * w; x += blockDim.x) {
+    uint32_t c = x / w, r = x % w;
+    rs[c][r] = r <= c ? colp(c)[r] : 0.0;
+  }
+  __syncthreads();
+  jacobi_square(rs, w, norms, order, &rotated, sigma, status);
   // U = Q [U_R; 0]: start from U_R's unit columns, apply H_{w-1}, ..., H_0.
   for (uint64_t x = threadIdx.x; x < (uint64_t)g * w; x += blockDim.x) {
     uint32_t c = (uint32_t)(x / g), r = (uint32_t)(x % g);
@@ -590,6 +602,99 @@ qr_svd_kernel(double* b, uint32_t g, uint32_t w, double* sigma, double* u, int* 
     }
     __syncthreads();
   }
+}
+
+// One step of shifted CholeskyQR3 (Fukaya, Kannan, Nakatsukasa, Yamamoto and Yanagisawa,
+// "Shifted Cholesky QR for computing the QR factorization of ill-conditioned
+// matrices", SIAM J. Sci. Comput. 2020), one CTA, w <= 64: the upper Cholesky factor R
+// of the Gram matrix G (w x w, column-major) plus shift * trace(G) on the diagonal
+// (trace(G) = |A|_F^2 >= |A|_2^2), into r (w x w column-major, zeros below), and the
+// running product r_total = R r_total (R itself when first). *status = 1 if a pivot is
+// not positive (the caller then uses Householder QR).
+__global__ void __launch_bounds__(1024)
+cholesky_step_kernel(const double* gram, uint32_t w, double shift, int first, double* r,
+                     double* r_total, int* status) {
+  __shared__ double a[kQrMaxCols][kQrMaxCols + 1];  // a[row][col]
+  __shared__ double trace;
+  __shared__ int bad;
+  for (uint32_t x = threadIdx.x; x < w * w; x += blockDim.x) a[x % w][x / w] = gram[x];
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tr = 0.0;
+    for (uint32_t j = 0; j < w; ++j) tr += a[j][j];
+    trace = tr;
+  }
+  __syncthreads();
+  if (threadIdx.x < w) a[threadIdx.x][threadIdx.x] += shift * trace;
+  __syncthreads();
+  for (uint32_t j = 0; j < w; ++j) {
+    const double d = a[j][j];
+    if (!(d > 0.0)) {
+      if (threadIdx.x == 0) bad = 1;
+      break;  // every thread reads the same d and leaves together
+    }
+    const double piv = sqrt(d);
+    __syncthreads();
+    // Row j of R: a[j][c] / piv for c > j (the diagonal written after the reads).
+    for (uint32_t c = j + 1 + threadIdx.x; c < w; c += blockDim.x) a[j][c] /= piv;
+    __syncthreads();
+    if (threadIdx.x == 0) a[j][j] = piv;
+    // Trailing update: a[i][c] -= R[j][i] R[j][c] for j < i <= c.
+    const uint32_t m = w - j - 1;
+    for (uint32_t x = threadIdx.x; x < m * m; x += blockDim.x) {
+      uint32_t i = j + 1 + x / m, c = j + 1 + x % m;
+      if (i <= c) a[i][c] -= a[j][i] * a[j][c];
+    }
+    __syncthreads();
+  }
+  __syncthreads();
+  if (bad) {
+    if (threadIdx.x == 0) *status = 1;
+    return;
+  }
+  for (uint32_t x = threadIdx.x; x < w * w; x += blockDim.x) {
+    uint32_t c = x / w, i = x % w;
+    r[x] = i <= c ? a[i][c] : 0.0;
+  }
+  // r_total = R r_total (both upper triangular): every thread computes its (at most 4,
+  // w <= 64 with 1024 threads) entries from the old r_total before any is written.
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (uint32_t x = threadIdx.x, e = 0; x < w * w; x += blockDim.x, ++e) {
+    uint32_t c = x / w, i = x % w;
+    if (i > c) continue;
+    if (first) {
+      v[e] = a[i][c];
+    } else {
+      double acc = 0.0;
+      for (uint32_t q = i; q <= c; ++q) acc = fma(a[i][q], r_total[(uint64_t)c * w + q], acc);
+      v[e] = acc;
+    }
+  }
+  __syncthreads();
+  for (uint32_t x = threadIdx.x, e = 0; x < w * w; x += blockDim.x, ++e) r_total[x] = v[e];
+}
+
+// The SVD of the w x w upper-triangular r (column-major, w <= 64): sigma (descending,
+// ties to the lower column) and u_r (w x w: column c the unit left singular vector of
+// sigma[c]; zero for sigma 0). *status |= 1 if Jacobi did not converge.
+__global__ void __launch_bounds__(1024)
+small_svd_kernel(const double* r, uint32_t w, double* sigma, double* u_r, int* status) {
+  __shared__ double rs[kQrMaxCols][kQrMaxCols + 1];
+  __shared__ double norms[kQrMaxCols];
+  __shared__ uint32_t order[kQrMaxCols];
+  __shared__ int rotated;
+  __shared__ int jstatus;
+  for (uint32_t x = threadIdx.x; x < w * w; x += blockDim.x) rs[x / w][x % w] = r[x];
+  __syncthreads();
+  jacobi_square(rs, w, norms, order, &rotated, sigma, &jstatus);
+  __syncthreads();
+  for (uint32_t x = threadIdx.x; x < w * w; x += blockDim.x) {
+    uint32_t c = x / w, i = x % w;
+    double nv = norms[order[c]];
+    u_r[x] = nv > 0.0 ? rs[order[c]][i] / nv : 0.0;
+  }
+  if (threadIdx.x == 0 && jstatus) *status = 1;
 }
 
 // out[:, c] = a[:, order[c]] / sigma[c] (the left singular vectors kept).
@@ -995,18 +1100,50 @@ struct Dense {
     DeviceBuffer<int> info(1, s);
     DeviceBuffer<double> u;
     const bool qr = w <= kQrMaxCols;
-    if (qr) {
-      u.alloc((uint64_t)g * w, s);
-      qr_svd_kernel<<<1, 1024, 0, s>>>(rest.ptr, g, w, sv.ptr, u.ptr, info.ptr);
-    } else {
-      jacobi_svd_kernel<<<1, 1024, 0, s>>>(rest.ptr, g, w, sv.ptr, order.ptr, info.ptr);
-    }
-    KG_LAUNCH_CHECK();
     std::vector<double> h_sv(w);
     int h_info = 0;
-    KG_CUDA(cudaMemcpyAsync(h_sv.data(), sv.ptr, w * 8ull, cudaMemcpyDeviceToHost, s));
-    KG_CUDA(cudaMemcpyAsync(&h_info, info.ptr, 4, cudaMemcpyDeviceToHost, s));
-    KG_CUDA(cudaStreamSynchronize(s));
+    auto read_back = [&]() {
+      KG_CUDA(cudaMemcpyAsync(h_sv.data(), sv.ptr, w * 8ull, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaMemcpyAsync(&h_info, info.ptr, 4, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaStreamSynchronize(s));
+    };
+    if (qr) {
+      // Shifted CholeskyQR3 (rest = Q R: three Gram/Cholesky/triangular-solve rounds
+      // across the GPU), the SVD of R in one CTA, U = Q U_R; Householder QR in one CTA
+      // if a Cholesky pivot fails (a numerically rank-deficient block).
+      u.alloc((uint64_t)g * w, s);
+      DeviceBuffer<double> saved((uint64_t)g * w, s), gram((uint64_t)w * w, s),
+          rt((uint64_t)w * w, s), rtot((uint64_t)w * w, s), ur((uint64_t)w * w, s);
+      KG_CUDA(cudaMemcpyAsync(saved.ptr, rest.ptr, rest.bytes(), cudaMemcpyDeviceToDevice, s));
+      info.zero();
+      const double one = 1.0, zero = 0.0;
+      const double shift = 11.0 * ((double)g * w + (double)w * (w + 1)) * 0x1p-53;
+      for (int round = 0; round < 3; ++round) {
+        KG_CUBLAS(cublasDgemm(p->cublas, CUBLAS_OP_T, CUBLAS_OP_N, w, w, g, &one, rest.ptr, g,
+                              rest.ptr, g, &zero, gram.ptr, w));
+        cholesky_step_kernel<<<1, 1024, 0, s>>>(gram.ptr, w, round == 0 ? shift : 0.0,
+                                                round == 0, rt.ptr, rtot.ptr, info.ptr);
+        KG_LAUNCH_CHECK();
+        KG_CUBLAS(cublasDtrsm(p->cublas, CUBLAS_SIDE_RIGHT, CUBLAS_FILL_MODE_UPPER, CUBLAS_OP_N,
+                              CUBLAS_DIAG_NON_UNIT, g, w, &one, rt.ptr, w, rest.ptr, g));
+      }
+      small_svd_kernel<<<1, 1024, 0, s>>>(rtot.ptr, w, sv.ptr, ur.ptr, info.ptr);
+      KG_LAUNCH_CHECK();
+      KG_CUBLAS(cublasDgemm(p->cublas, CUBLAS_OP_N, CUBLAS_OP_N, g, w, w, &one, rest.ptr, g,
+                            ur.ptr, w, &zero, u.ptr, g));
+      read_back();
+      if (h_info != 0) {
+        KG_CUDA(cudaMemcpyAsync(rest.ptr, saved.ptr, rest.bytes(), cudaMemcpyDeviceToDevice, s));
+        info.zero();
+        qr_svd_kernel<<<1, 1024, 0, s>>>(rest.ptr, g, w, sv.ptr, u.ptr, info.ptr);
+        KG_LAUNCH_CHECK();
+        read_back();
+      }
+    } else {
+      jacobi_svd_kernel<<<1, 1024, 0, s>>>(rest.ptr, g, w, sv.ptr, order.ptr, info.ptr);
+      KG_LAUNCH_CHECK();
+      read_back();
+    }
     if (h_info != 0)
       fail(KG_ERR_INVALID, "pca: orthonormalising a Krylov block did not converge");
     uint32_t keep = 0;
