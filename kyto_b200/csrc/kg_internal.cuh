@@ -197,12 +197,19 @@ inline void wait_stream(kg_ctx* ctx, cudaStream_t stream) {
 }
 
 // Phase timings of a call, on its stream, printed to stderr when KYTO_GPU_TRACE is set
-// (one line per call: phase name, count, total ms). Costs nothing when unset.
+// (one line per call: phase name, count, device ms between the stream's marks, and the
+// host's wall ms between the same marks; a host figure far above the device one means
+// the stream sat idle while the host worked or waited). Costs nothing when unset.
 struct Trace {
   bool on = false;
   cudaStream_t s = nullptr;
   std::string what;
-  std::vector<std::pair<std::string, cudaEvent_t>> marks;
+  struct Mark {
+    std::string name;
+    cudaEvent_t ev;
+    std::chrono::steady_clock::time_point host;
+  };
+  std::vector<Mark> marks;
   Trace(cudaStream_t st, const char* call) : s(st), what(call) {
     on = std::getenv("KYTO_GPU_TRACE") != nullptr;
     mark("start");
@@ -212,33 +219,41 @@ struct Trace {
     cudaEvent_t e;
     if (cudaEventCreate(&e) != cudaSuccess) return;
     cudaEventRecord(e, s);
-    marks.emplace_back(name, e);
+    marks.push_back({name, e, std::chrono::steady_clock::now()});
   }
   ~Trace() {
     if (!on || marks.empty()) return;
-    cudaEventSynchronize(marks.back().second);
-    std::vector<std::pair<std::string, std::pair<int, double>>> acc;
+    cudaEventSynchronize(marks.back().ev);
+    struct Acc {
+      std::string name;
+      int n;
+      double dev, host;
+    };
+    std::vector<Acc> acc;
     for (size_t i = 1; i < marks.size(); ++i) {
       float ms = 0;
-      cudaEventElapsedTime(&ms, marks[i - 1].second, marks[i].second);
+      cudaEventElapsedTime(&ms, marks[i - 1].ev, marks[i].ev);
+      double host =
+          std::chrono::duration<double, std::milli>(marks[i].host - marks[i - 1].host).count();
       bool found = false;
       for (auto& a : acc)
-        if (a.first == marks[i].first) {
-          a.second.first += 1;
-          a.second.second += ms;
+        if (a.name == marks[i].name) {
+          a.n += 1;
+          a.dev += ms;
+          a.host += host;
           found = true;
         }
-      if (!found) acc.push_back({marks[i].first, {1, ms}});
+      if (!found) acc.push_back({marks[i].name, 1, ms, host});
     }
     std::string line = "[kyto_gpu trace] " + what + ":";
     for (auto& a : acc) {
-      char buf[128];
-      std::snprintf(buf, sizeof buf, " %s x%d %.3f ms;", a.first.c_str(), a.second.first,
-                    a.second.second);
+      char buf[160];
+      std::snprintf(buf, sizeof buf, " %s x%d %.3f ms (host %.3f);", a.name.c_str(), a.n, a.dev,
+                    a.host);
       line += buf;
     }
     std::fprintf(stderr, "%s\n", line.c_str());
-    for (auto& m : marks) cudaEventDestroy(m.second);
+    for (auto& m : marks) cudaEventDestroy(m.ev);
   }
 };
 

@@ -123,17 +123,20 @@ __global__ void centre_kernel(const float* x, uint64_t n, uint32_t width, uint32
   offsets[r] = (float)s;
 }
 
-__global__ void max_kernel(const double* v, uint64_t n, double* out) {
-  __shared__ double red[256];
-  double m = 0.0;
-  for (uint64_t i = threadIdx.x; i < n; i += blockDim.x) m = fmax(m, v[i]);
-  red[threadIdx.x] = m;
-  __syncthreads();
-  for (unsigned s = blockDim.x / 2; s; s >>= 1) {
-    if (threadIdx.x < s) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + s]);
-    __syncthreads();
+// *out = max(*out, max of v): v >= 0 (squared norms), so the f64 bit patterns order as
+// the values do and one atomicMax per warp combines the blocks (*out starts at 0).
+__global__ void max_kernel(const double* v, uint64_t n, unsigned long long* out) {
+  unsigned long long m = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(v[i]);
+    m = b > m ? b : m;
   }
-  if (threadIdx.x == 0) *out = red[0];
+  for (int o = 16; o; o >>= 1) {
+    const unsigned long long t = __shfl_xor_sync(0xFFFFFFFFu, m, o);
+    m = t > m ? t : m;
+  }
+  if ((threadIdx.x & 31u) == 0) atomicMax(out, m);
 }
 
 __device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 10 bits -> every third bit
@@ -181,8 +184,11 @@ void spatial_order(const float* x, uint64_t n, uint32_t width, uint32_t d, const
                                           perm.ptr, (int)n, 0, 30, s));
 }
 
+// *out = the largest of v[0..n) (all >= 0), on the stream.
 void max_kernel_launch(const double* v, uint64_t n, double* out, cudaStream_t s) {
-  max_kernel<<<1, 256, 0, s>>>(v, n, out);
+  KG_CUDA(cudaMemsetAsync(out, 0, sizeof(double), s));
+  unsigned blocks = std::min<unsigned>(blocks_for(n, 256), 1184);
+  max_kernel<<<blocks, 256, 0, s>>>(v, n, reinterpret_cast<unsigned long long*>(out));
   KG_LAUNCH_CHECK();
 }
 
@@ -573,7 +579,7 @@ extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t 
     column_stats(x, n, width, d, mean.ptr, lo_hi.ptr, s);
     centre_kernel<<<blocks_for(n, 128), 128, 0, s>>>(x, n, width, d, mean.ptr, rows.ptr,
                                                      offsets.ptr, squares.ptr);
-    max_kernel<<<1, 256, 0, s>>>(squares.ptr, n, largest.ptr);
+    max_kernel_launch(squares.ptr, n, largest.ptr, s);
     slack_kernel<<<blocks_for(n, 256), 256, 0, s>>>(squares.ptr, n, d, largest.ptr, slack.ptr);
     KG_LAUNCH_CHECK();
     double h_largest = 0;

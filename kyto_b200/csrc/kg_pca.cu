@@ -766,12 +766,22 @@ __global__ void omega_t_kernel(const uint64_t* cells, uint64_t n, uint32_t width
 }
 
 // out[j] = sum over blocks (in order) of partial[b][j], j < w.
-__global__ void sum_blocks_kernel(const double* partial, uint64_t nb, uint32_t w, double* out) {
-  uint32_t j = threadIdx.x;
-  if (j >= w) return;
+// out[j] = the sum over b of partial[b * 64 + j] (j < w): one CTA of 1024 threads, 16
+// row classes per column summed in order, then the classes in order (a fixed tree).
+__global__ void __launch_bounds__(1024)
+sum_blocks_kernel(const double* partial, uint64_t nb, uint32_t w, double* out) {
+  __shared__ double part[16][64];
+  const uint32_t j = threadIdx.x & 63u, cls = threadIdx.x >> 6;
   double t = 0.0;
-  for (uint64_t b = 0; b < nb; ++b) t += partial[b * 64 + j];
-  out[j] = t;
+  if (j < w)
+    for (uint64_t b = cls; b < nb; b += 16) t += partial[b * 64 + j];
+  part[cls][j] = t;
+  __syncthreads();
+  if (cls == 0 && j < w) {
+    double u = 0.0;
+    for (int c = 0; c < 16; ++c) u += part[c][j];
+    out[j] = u;
+  }
 }
 
 // out (g x w column-major) = sum over segments (in order) of partial[seg][gene][j].
@@ -838,14 +848,16 @@ struct TcHeld {
   int sm = 148;
 
   void build(const uint64_t* indptr, const uint32_t* col, const float* val, uint64_t n_rows,
-             uint32_t n_genes, uint64_t nnz, int sm_count, cudaStream_t s) {
+             uint32_t n_genes, uint64_t nnz, int sm_count, cudaStream_t s, Trace& trace) {
     n = n_rows;
     g = n_genes;
     n_ld = (n + 3) & ~3ull;
     g_ld = (g + 3) & ~3ull;
     sm = sm_count;
     build_blocked(indptr, col, val, n, g, nnz, false, bx, s);
+    trace.mark("blocked X");
     build_blocked(indptr, col, val, n, g, nnz, true, bxt, s);
+    trace.mark("blocked X^T");
     dt_hi.alloc(64 * n_ld, s);
     dt_lo.alloc(64 * n_ld, s);
     qt_hi.alloc(64 * g_ld, s);
@@ -859,7 +871,7 @@ struct TcHeld {
     DeviceBuffer<double> bsum((uint64_t)nb * 64, s);
     omega_t_kernel<<<nb, 256, 0, s>>>(cells, n, width, seed, n_ld, dt_hi.ptr, dt_lo.ptr, bsum.ptr);
     KG_LAUNCH_CHECK();
-    sum_blocks_kernel<<<1, 64, 0, s>>>(bsum.ptr, nb, width, omega_sums);
+    sum_blocks_kernel<<<1, 1024, 0, s>>>(bsum.ptr, nb, width, omega_sums);
     KG_LAUNCH_CHECK();
     transposed(width, out, s);
   }
@@ -922,7 +934,7 @@ struct TcHeld {
     a.sm_count = sm;
     spmm_tc(a, s);
     if (wsums) {
-      sum_blocks_kernel<<<1, 64, 0, s>>>(colsum.ptr, tiles, w, wsums);
+      sum_blocks_kernel<<<1, 1024, 0, s>>>(colsum.ptr, tiles, w, wsums);
       KG_LAUNCH_CHECK();
     }
   }
@@ -1212,8 +1224,8 @@ void kg_pca::run() {
     // Gene means (pass 0's sums, pca.rs:707-717), stored counts and centred sums of
     // squares over the stored values (the last pass's, pca.rs:664-676), as products
     // with a column of ones.
-    th.build(indptr.ptr, col.ptr, val.ptr, n, g, nnz, c->sm_count, s);
-    trace.mark("blocked layouts");
+    th.build(indptr.ptr, col.ptr, val.ptr, n, g, nnz, c->sm_count, s, trace);
+    trace.mark("operand buffers");
     DeviceBuffer<double> sums(g, s), cnt(g, s), sq(g, s);
     th.ones_column();
     th.transposed(1, sums.ptr, s, kValuePlain, nullptr);

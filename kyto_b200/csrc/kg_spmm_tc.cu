@@ -3,30 +3,36 @@
 //   C (rows x 64) = S (rows x K, sparse, f32 values) . D (K x 64)
 //
 // S is the held input X (rows = cells, K = genes) for X Q and the embedding pass, or X^T
-// (rows = genes, K = cells) for X^T W, the sketch and the centred squares; both are kept
-// in the blocked layout of kg_spmm_tc.cuh (128 rows x 32 columns per block). D comes as
-// D^T (64 x K) in two tf32 parts (hi + lo), K-major f32. Each 128 x 32 tile of S is
-// densified in shared memory and multiplied by three TF32 MMAs (hi.hi + hi.lo + lo.hi:
-// the f32 operands to about 2^-21), accumulated in TMEM over at most kFlushChunks
-// chunks and then added into f64 registers (no f32 sum runs over more than 512 terms).
+// (rows = genes, K = cells) for X^T W, the sketch and the gene statistics; both are kept
+// in the bitmask block layout of kg_spmm_tc.cuh (128 rows x 32 columns per block). D
+// comes as D^T (64 x K) in two tf32 parts (hi + lo), K-major f32. Each 128 x 32 block of
+// S is expanded straight into tensor memory (one thread per row: its mask word and
+// values become the row's 32 hi and 32 lo tf32 parts, stored into its TMEM lane) and
+// multiplied by three TF32 MMAs that read A from TMEM and D^T from shared memory
+// (hi.hi + hi.lo + lo.hi: the f32 operands to about 2^-21), accumulated in TMEM over at
+// most kFlushChunks chunks and then added into f64 registers (no f32 sum runs over more
+// than 512 terms). Shared memory carries only the loads (D^T tiles and blocks), so the
+// MMAs' operand reads do not compete with the expansion for it.
 //
 // Per CTA (persistent, 320 threads) and per K-chunk of a work item (tile, K segment):
-//   warp 8      TMA: the chunk's D^T tiles (64 x 32, two parts) and the block's entries
-//               (one bulk copy of its indices, one of its values) into a stage;
-//   warps 0-3   densify: zero the stage's 128 x 32 A tiles, then scatter the block's
-//               entries into them (128-byte-swizzled K-major, the layout the MMA reads);
-//   warp 9      MMA: 12 tcgen05.mma (kind::tf32, M=128 N=64 K=8) into one of two TMEM
-//               accumulators;
+//   warp 8      loads: the chunk's D^T tiles (64 x 32, two parts, TMA) and the block (one
+//               bulk copy) into one of kLoadStages stages; the next 32 blocks are
+//               prefetched into L2 ahead of their copies;
+//   warps 0-3   expand: thread r writes row r of the chunk's A tile (hi and lo parts)
+//               into TMEM lane r of one of two A buffers;
+//   warp 9      MMA: 12 tcgen05.mma (kind::tf32, A from TMEM, M=128 N=64 K=8) into one
+//               of two TMEM accumulators;
 //   warps 4-7   drain: TMEM -> f64 registers per flush group; at the end of the item the
 //               rows (C - offsets, as tf32 parts of C^T, f32 rows and column sums) or the
 //               segment's f64 partial.
-// HBM sees each entry once per product (6 bytes) and D^T once per CTA pass (L2 serves
-// the other tiles of a segment).
+// HBM sees each block once per product (its mask and values: 512 + 4 nnz bytes) and
+// D^T about once per pass over it (L2 serves the other tiles of a segment).
 #include <cudaTypedefs.h>
 #include <cub/device/device_scan.cuh>
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <mutex>
 
@@ -43,50 +49,47 @@ namespace {
 constexpr int kRows = 128;              // rows per tile (M)
 constexpr int kChunk = 32;              // K per chunk (one 128-byte swizzle row of f32)
 constexpr int kN = 64;                  // output columns (N)
-constexpr int kStagesS = 3;
+constexpr int kLoadStages = 6;
 constexpr int kFlushChunks = 16;        // K-chunks summed in f32 before the f64 flush
-constexpr uint32_t kABytes = kRows * 128;  // 16 KB: 128 rows x 32 f32
-constexpr uint32_t kBBytes = kN * 128;     // 8 KB: 64 rows x 32 f32
-constexpr uint32_t kMaxEntries = kRows * kChunk;  // a full block (a multiple of 8)
+constexpr uint32_t kBBytes = kN * 128;  // 8 KB: 64 rows x 32 f32
+constexpr uint32_t kMaskBytes = kRows * 4;
+constexpr uint32_t kBlockMaxBytes = kMaskBytes + kRows * kChunk * 4;
 constexpr int kProducerWarps = 4;
 constexpr int kEpilogueWarps = 4;
 constexpr int kSpThreads = (kProducerWarps + kEpilogueWarps + 2) * 32;
-constexpr uint32_t kTmemColsS = 128;   // two 64-column f32 accumulators
-constexpr uint16_t kPad = 0xFFFF;
+// TMEM columns: two 64-column f32 accumulators (0..127), then two A buffers of 64
+// columns (hi parts in the first 32, lo parts in the next 32; lane = row of the tile).
+constexpr uint32_t kTmemColsS = 256;
+constexpr uint32_t kAccCols = 64, kABase = 128, kACols = 64;
 
-struct Stage {
-  uint8_t a_hi[kABytes];
-  uint8_t a_lo[kABytes];
+struct LoadStage {
   uint8_t b_hi[kBBytes];
   uint8_t b_lo[kBBytes];
-  float e_val[kMaxEntries];
-  uint16_t e_idx[kMaxEntries];
+  uint8_t blk[(kBlockMaxBytes + 1023) / 1024 * 1024];  // mask words, then the values
 };
+// Swizzled tiles (TMA destinations, MMA operands) start on 1024-byte boundaries.
+static_assert(sizeof(LoadStage) % 1024 == 0, "load stage size");
 
 struct SpSmem {
-  Stage st[kStagesS];
+  LoadStage st[kLoadStages];
   double colsum[2][kEpilogueWarps][kN];
-  uint64_t load_full[kStagesS], a_ready[kStagesS], empty[kStagesS], zeroed[kStagesS];
+  uint64_t ld_full[kLoadStages], ld_empty[kLoadStages];
+  uint64_t a_full[2], a_empty[2];
   uint64_t cs_ready;
   uint64_t acc_full[2], acc_empty[2];
   uint64_t drained;
-  uint32_t count[kStagesS];
+  uint32_t present[kLoadStages];
   uint32_t tmem_base;
   int abort;
 };
 constexpr size_t kSpSmemBytes = sizeof(SpSmem) + 1024;
+static_assert(kSpSmemBytes <= 227 * 1024, "SpMM shared memory");
+static_assert(offsetof(SpSmem, st) % 1024 == 0, "tile alignment");
 
 __device__ __forceinline__ float tf32_round(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return __uint_as_float(r);
-}
-
-// Byte offset of element kk (0..31) of row i in a 128-byte-swizzled K-major tile
-// (8-row atoms of 1024 bytes; 16-byte chunk c of row i stored at chunk c ^ (i % 8)).
-__device__ __forceinline__ uint32_t sw128_offset(uint32_t i, uint32_t kk) {
-  return (i >> 3) * 1024u + (i & 7u) * 128u + ((((kk >> 2) ^ (i & 7u)) & 7u) << 4) +
-         (kk & 3u) * 4u;
 }
 
 // A 1D bulk copy global -> shared, counted in bytes on `bar` (16-byte aligned, size a
@@ -98,6 +101,13 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
           "r"(smem_addr(dst)),
       "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_addr(bar))
       : "memory");
+}
+
+// Prefetch [src, src + bytes) into L2 (16-byte aligned, size a multiple of 16).
+__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reinterpret_cast<uint64_t>(src)),
+               "r"(bytes)
+               : "memory");
 }
 
 struct Geometry {
@@ -112,34 +122,37 @@ struct Geometry {
     uint32_t c0 = seg * seg_chunks;
     return min(seg_chunks, n_chunks - c0);
   }
+  __device__ __forceinline__ uint64_t first_block(uint32_t tile, uint32_t seg) const {
+    return (uint64_t)tile * n_chunks + (uint64_t)seg * seg_chunks;
+  }
 };
 
 __global__ void __launch_bounds__(kSpThreads, 1)
 spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
                const __grid_constant__ CUtensorMap tmap_lo, const uint64_t* __restrict__ off,
-               const uint16_t* __restrict__ eidx, const float* __restrict__ evals,
-               uint64_t rows, Geometry geo, int value_mode, const double* __restrict__ row_means,
-               SpmmOut out, int* error) {
+               const uint8_t* __restrict__ data, uint64_t rows, Geometry geo, int value_mode,
+               const double* __restrict__ row_means, SpmmOut out, int* error) {
   extern __shared__ uint8_t smem_raw[];
-  SpSmem& sm = *reinterpret_cast<SpSmem*>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  // Aligned to 1024 bytes by an offset into the __shared__ array itself, so the compiler
+  // keeps every access in the shared state space (no generic loads and stores).
+  SpSmem& sm = *reinterpret_cast<SpSmem*>(smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u));
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const uint64_t n_items = geo.items();
   volatile int* abort = &sm.abort;
 
   if (threadIdx.x == 0) {
-    for (int s = 0; s < kStagesS; ++s) {
-      mbar_init(&sm.load_full[s], 1);
-      mbar_init(&sm.a_ready[s], kProducerWarps);
-      mbar_init(&sm.empty[s], 1);
-      mbar_init(&sm.zeroed[s], kProducerWarps);
+    for (int s = 0; s < kLoadStages; ++s) {
+      mbar_init(&sm.ld_full[s], 1);
+      mbar_init(&sm.ld_empty[s], kProducerWarps + 1);  // the expanders and the MMA commit
     }
-    mbar_init(&sm.cs_ready, kEpilogueWarps);
     for (int b = 0; b < 2; ++b) {
+      mbar_init(&sm.a_full[b], kProducerWarps);
+      mbar_init(&sm.a_empty[b], 1);
       mbar_init(&sm.acc_full[b], 1);
       mbar_init(&sm.acc_empty[b], kEpilogueWarps);
     }
+    mbar_init(&sm.cs_ready, kEpilogueWarps);
     mbar_init(&sm.drained, 1);
     sm.abort = 0;
     fence_mbar_init();
@@ -151,57 +164,88 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
   const uint32_t tmem = sm.tmem_base;
 
   if (warp < kProducerWarps) {
-    // ----------------------------------------------------------- densify ------------
-    const uint32_t t = threadIdx.x;  // 0..127
+    // ----------------------------------------------------------- expand -------------
+    const uint32_t r = threadIdx.x;  // the row of the tile this thread writes (0..127)
     uint64_t it = 0;
     bool ok = true;
     for (uint64_t w = blockIdx.x; w < n_items && ok; w += gridDim.x) {
       uint32_t tile, seg;
       geo.item(w, tile, seg);
       const uint32_t nc = geo.chunks(seg);
+      float mean_r = 0.0f;
+      if (value_mode == kValueCentredSquare) {
+        const uint64_t row = (uint64_t)tile * kRows + r;
+        mean_r = row < rows ? (float)row_means[row] : 0.0f;
+      }
       for (uint32_t c = 0; c < nc; ++c, ++it) {
-        const int s = (int)(it % kStagesS);
-        const uint32_t ph = (uint32_t)((it / kStagesS) & 1);
-        if (!mbar_wait(&sm.empty[s], ph ^ 1, abort)) {
+        const int ls = (int)(it % kLoadStages);
+        const uint32_t lph = (uint32_t)((it / kLoadStages) & 1);
+        const uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
+        if (!mbar_wait(&sm.ld_full[ls], lph, abort) || !mbar_wait(&sm.a_empty[ab], aph ^ 1, abort)) {
           ok = false;
           break;
         }
-        Stage& st = sm.st[s];
-        // Zero the two A tiles: 32 KB, 16 stores of 16 bytes a thread.
-        const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+        tc_fence_after();
+        const LoadStage& st = sm.st[ls];
+        const bool present = sm.present[ls] != 0;
+        const uint32_t* masks = reinterpret_cast<const uint32_t*>(st.blk);
+        const float* vals = reinterpret_cast<const float*>(st.blk + kMaskBytes);
+        // The row's first value: the stored values of the rows before it (the earlier
+        // warps' rows summed by every warp, then a scan inside the warp).
+        uint32_t mword = 0, base = 0;
+        if (present) {
+          mword = masks[r];
+          uint32_t before = 0;
+          for (int q = 0; q < warp; ++q) before += __popc(masks[q * 32 + lane]);
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          reinterpret_cast<float4*>(st.a_hi)[q * 128 + t] = z;
-          reinterpret_cast<float4*>(st.a_lo)[q * 128 + t] = z;
-        }
-        // Every producer warp's zeros land before any entry is scattered (bounded waits,
-        // not a named barrier, so an aborted pipeline cannot strand a warp).
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&sm.zeroed[s]);
-        if (!mbar_wait(&sm.zeroed[s], ph, abort) || !mbar_wait(&sm.load_full[s], ph, abort)) {
-          ok = false;
-          break;
-        }
-        const uint32_t cnt = sm.count[s];
-        for (uint32_t e = t; e < cnt; e += kProducerWarps * 32) {
-          const uint16_t p = st.e_idx[e];
-          if (p == kPad) continue;
-          const uint32_t r = p >> 5, kk = p & 31u;
-          float v = st.e_val[e];
-          if (value_mode == kValueCentredSquare) {
-            float d = v - (float)row_means[(uint64_t)tile * kRows + r];
-            v = d * d;
-          } else if (value_mode == kValueOne) {
-            v = 1.0f;
+          for (int o = 16; o; o >>= 1) before += __shfl_xor_sync(0xFFFFFFFFu, before, o);
+          uint32_t incl = __popc(mword);
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += v;
           }
-          const float h = tf32_round(v);
-          const uint32_t o = sw128_offset(r, kk);
-          *reinterpret_cast<float*>(st.a_hi + o) = h;
-          *reinterpret_cast<float*>(st.a_lo + o) = v - h;
+          base = before + incl - __popc(mword);
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        // Branch-free: every column's value is loaded from its would-be rank (the rank
+        // of the next stored value for an empty cell: still inside the stage buffer,
+        // which holds 4,224 values) and kept only where the mask bit is set, so all 32
+        // loads issue back to back.
+        float v[kChunk];
+#pragma unroll
+        for (int col = 0; col < kChunk; ++col) {
+          const uint32_t below = col ? __popc(mword & ((1u << col) - 1u)) : 0u;
+          const float x = vals[base + below];
+          v[col] = ((mword >> col) & 1u) ? x : 0.0f;
+        }
+        if (value_mode == kValueCentredSquare) {
+#pragma unroll
+          for (int col = 0; col < kChunk; ++col) {
+            const float d = v[col] - mean_r;
+            v[col] = ((mword >> col) & 1u) ? d * d : 0.0f;
+          }
+        } else if (value_mode == kValueOne) {
+#pragma unroll
+          for (int col = 0; col < kChunk; ++col) v[col] = ((mword >> col) & 1u) ? 1.0f : 0.0f;
+        }
+        // Row r of the A tile (tf32 hi and lo parts) into TMEM lane r, where the MMA reads it.
+        uint32_t hi[kChunk], lo[kChunk];
+#pragma unroll
+        for (int col = 0; col < kChunk; ++col) {
+          const float h = tf32_round(v[col]);
+          hi[col] = __float_as_uint(h);
+          lo[col] = __float_as_uint(v[col] - h);
+        }
+        const uint32_t arow = tmem + (((uint32_t)warp * 32u) << 16) + kABase + ab * kACols;
+        tmem_st_32(arow, hi);
+        tmem_st_32(arow + 32u, lo);
+        tmem_wait_st();
+        tc_fence_before();
         __syncwarp();
-        if (lane == 0) mbar_arrive(&sm.a_ready[s]);
+        if (lane == 0) {
+          mbar_arrive(&sm.a_full[ab]);
+          mbar_arrive(&sm.ld_empty[ls]);
+        }
       }
     }
   } else if (warp < kProducerWarps + kEpilogueWarps) {
@@ -227,18 +271,18 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
         }
         tc_fence_after();
         __syncwarp();
-        uint32_t r0[32], r1[32];
-        tmem_ld_32(tmem + ((quad * 32u) << 16) + b * 64u, r0);
-        tmem_ld_32(tmem + ((quad * 32u) << 16) + b * 64u + 32u, r1);
-        tmem_wait_ld();
+        // One 32-column half at a time (fewer live registers beside the f64 sums).
+#pragma unroll
+        for (int hf = 0; hf < 2; ++hf) {
+          uint32_t rr[32];
+          tmem_ld_32(tmem + ((quad * 32u) << 16) + b * kAccCols + hf * 32u, rr);
+          tmem_wait_ld();
+#pragma unroll
+          for (int j = 0; j < 32; ++j) acc[hf * 32 + j] += (double)__uint_as_float(rr[j]);
+        }
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.acc_empty[b]);
-#pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          acc[j] += (double)__uint_as_float(r0[j]);
-          acc[32 + j] += (double)__uint_as_float(r1[j]);
-        }
       }
       if (!ok) break;
       if (out.mode == kOutRows) {
@@ -283,44 +327,78 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
       }
     }
   } else if (warp == kProducerWarps + kEpilogueWarps) {
-    // ----------------------------------------------------------- TMA ----------------
+    // ----------------------------------------------------------- loads --------------
+    // Lane 0 issues; the warp reads the item's block offsets 32 at a time ahead of it,
+    // and each window's successor (or the next item's first window) is prefetched into
+    // L2 while this one is copied.
     if (lane == 0) {
       prefetch_tmap(&tmap_hi);
       prefetch_tmap(&tmap_lo);
-      uint64_t it = 0;
-      int issued_phase[kStagesS];
-      for (int s = 0; s < kStagesS; ++s) issued_phase[s] = -1;
-      bool ok = true;
-      for (uint64_t w = blockIdx.x; w < n_items && ok; w += gridDim.x) {
-        uint32_t tile, seg;
-        geo.item(w, tile, seg);
-        const uint32_t nc = geo.chunks(seg);
-        for (uint32_t c = 0; c < nc; ++c, ++it) {
-          const int s = (int)(it % kStagesS);
-          const uint32_t ph = (uint32_t)((it / kStagesS) & 1);
-          if (!mbar_wait(&sm.empty[s], ph ^ 1, abort)) {
-            ok = false;
-            break;
+    }
+    uint64_t it = 0;
+    int issued_phase[kLoadStages];
+    for (int s = 0; s < kLoadStages; ++s) issued_phase[s] = -1;
+    bool ok = true;
+    for (uint64_t w = blockIdx.x; w < n_items && ok; w += gridDim.x) {
+      uint32_t tile, seg;
+      geo.item(w, tile, seg);
+      const uint32_t nc = geo.chunks(seg);
+      const uint64_t b0 = geo.first_block(tile, seg);
+      uint64_t win = 0, win_end = 0;
+      for (uint32_t c = 0; c < nc; ++c, ++it) {
+        const uint32_t at = c & 31u;
+        if (at == 0) {
+          // off[b0 + c + lane] and, in lane 0, off[b0 + c + 32] (indices <= nc: the
+          // offsets array holds one entry past every block).
+          win = c + lane <= nc ? off[b0 + c + lane] : 0;
+          win_end = lane == 0 && c + 32 <= nc ? off[b0 + c + 32] : 0;
+          if (lane == 0) {
+            uint64_t p0 = 0, p1 = 0;
+            if (c + 32 < nc) {
+              p0 = win_end;
+              p1 = off[b0 + min(c + 64, nc)];
+            } else if (w + gridDim.x < n_items) {
+              uint32_t t2, s2;
+              geo.item(w + gridDim.x, t2, s2);
+              const uint64_t nb0 = geo.first_block(t2, s2);
+              p0 = off[nb0];
+              p1 = off[nb0 + min(32u, geo.chunks(s2))];
+            }
+            for (uint64_t u = p0; u < p1; u += 4096) {  // 64 KB per prefetch
+              const uint64_t units = p1 - u < 4096 ? p1 - u : 4096;
+              bulk_prefetch_l2(data + u * 16, (uint32_t)(units * 16));
+            }
           }
-          const uint32_t chunk = seg * geo.seg_chunks + c;
-          const uint64_t b = (uint64_t)tile * geo.n_chunks + chunk;
-          const uint64_t e0 = off[b];
-          const uint32_t cnt = (uint32_t)(off[b + 1] - e0);
-          sm.count[s] = cnt;
-          mbar_arrive_expect_tx(&sm.load_full[s], 2 * kBBytes + cnt * 6u);
-          const int32_t x = (int32_t)(chunk * kChunk);
-          tma_load_2d(sm.st[s].b_hi, &tmap_hi, &sm.load_full[s], x, 0);
-          tma_load_2d(sm.st[s].b_lo, &tmap_lo, &sm.load_full[s], x, 0);
-          if (cnt) {
-            bulk_load(sm.st[s].e_idx, eidx + e0, cnt * 2u, &sm.load_full[s]);
-            bulk_load(sm.st[s].e_val, evals + e0, cnt * 4u, &sm.load_full[s]);
-          }
-          issued_phase[s] = (int)ph;
         }
+        const uint64_t e0 = __shfl_sync(0xFFFFFFFFu, win, at);
+        const uint64_t e1n = __shfl_sync(0xFFFFFFFFu, win, (at + 1) & 31u);
+        const uint64_t e1w = __shfl_sync(0xFFFFFFFFu, win_end, 0);
+        const uint64_t e1 = at == 31 ? e1w : e1n;
+        if (lane == 0) {
+          const int s = (int)(it % kLoadStages);
+          const uint32_t ph = (uint32_t)((it / kLoadStages) & 1);
+          if (!mbar_wait(&sm.ld_empty[s], ph ^ 1, abort)) {
+            ok = false;
+          } else {
+            const uint32_t chunk = seg * geo.seg_chunks + c;
+            const uint32_t bytes = (uint32_t)((e1 - e0) * 16);
+            sm.present[s] = bytes ? 1u : 0u;
+            mbar_arrive_expect_tx(&sm.ld_full[s], 2 * kBBytes + bytes);
+            const int32_t x = (int32_t)(chunk * kChunk);
+            tma_load_2d(sm.st[s].b_hi, &tmap_hi, &sm.ld_full[s], x, 0);
+            tma_load_2d(sm.st[s].b_lo, &tmap_lo, &sm.ld_full[s], x, 0);
+            if (bytes) bulk_load(sm.st[s].blk, data + e0 * 16, bytes, &sm.ld_full[s]);
+            issued_phase[s] = (int)ph;
+          }
+        }
+        ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
+        if (!ok) break;
       }
-      for (int s = 0; s < kStagesS; ++s) {
+    }
+    if (lane == 0) {
+      for (int s = 0; s < kLoadStages; ++s) {
         if (issued_phase[s] < 0) continue;
-        for (uint32_t q = 0; q < kWaitPolls && !mbar_try_wait(&sm.load_full[s], issued_phase[s]); ++q)
+        for (uint32_t q = 0; q < kWaitPolls && !mbar_try_wait(&sm.ld_full[s], issued_phase[s]); ++q)
           ;
       }
     }
@@ -341,24 +419,26 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
             ok = false;
             break;
           }
-          const int s = (int)(it % kStagesS);
-          const uint32_t ph = (uint32_t)((it / kStagesS) & 1);
-          if (!mbar_wait(&sm.load_full[s], ph, abort) || !mbar_wait(&sm.a_ready[s], ph, abort)) {
+          const int ls = (int)(it % kLoadStages);
+          const uint32_t lph = (uint32_t)((it / kLoadStages) & 1);
+          const uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
+          if (!mbar_wait(&sm.ld_full[ls], lph, abort) || !mbar_wait(&sm.a_full[ab], aph, abort)) {
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t d = tmem + b * 64u;
-          const uint32_t ah = smem_addr(sm.st[s].a_hi), al = smem_addr(sm.st[s].a_lo);
-          const uint32_t bh = smem_addr(sm.st[s].b_hi), bl = smem_addr(sm.st[s].b_lo);
+          const uint32_t d = tmem + b * kAccCols;
+          const uint32_t ah = tmem + kABase + ab * kACols, al = ah + 32u;
+          const uint32_t bh = smem_addr(sm.st[ls].b_hi), bl = smem_addr(sm.st[ls].b_lo);
 #pragma unroll
           for (int kk = 0; kk < kChunk / 8; ++kk) {
-            const uint32_t o = kk * 32;
-            mma_tf32(d, desc_k_sw128(ah + o), desc_k_sw128(bh + o), idesc, (in_group | kk) != 0);
-            mma_tf32(d, desc_k_sw128(ah + o), desc_k_sw128(bl + o), idesc, 1);
-            mma_tf32(d, desc_k_sw128(al + o), desc_k_sw128(bh + o), idesc, 1);
+            const uint32_t o = kk * 32;  // 8 tf32 of K: 32 bytes of a B row, 8 A columns
+            mma_tf32_ts(d, ah + kk * 8, desc_k_sw128(bh + o), idesc, (in_group | kk) != 0);
+            mma_tf32_ts(d, ah + kk * 8, desc_k_sw128(bl + o), idesc, 1);
+            mma_tf32_ts(d, al + kk * 8, desc_k_sw128(bh + o), idesc, 1);
           }
-          mma_commit(&sm.empty[s]);
+          mma_commit(&sm.ld_empty[ls]);
+          mma_commit(&sm.a_empty[ab]);
           if (in_group == kFlushChunks - 1 || c == nc - 1) {
             mma_commit(&sm.acc_full[b]);
             ++fg;
@@ -381,16 +461,17 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
 
 // ------------------------------------------------------------------ builders -------
 
-// The block of each stored value, and its packed (row_in_tile << 5 | col_in_chunk).
+// The block of a stored value, and its row (in the tile) and column (in the chunk).
 __device__ __forceinline__ void locate(uint64_t r, uint32_t c, bool transpose, uint32_t n_chunks,
-                                       uint64_t& block, uint16_t& packed) {
+                                       uint64_t& block, uint32_t& br, uint32_t& bc) {
   uint64_t orow = transpose ? c : r;  // row of the output layout
   uint64_t ocol = transpose ? r : c;
   block = (orow / kRows) * n_chunks + ocol / kChunk;
-  packed = (uint16_t)(((orow % kRows) << 5) | (ocol % kChunk));
+  br = (uint32_t)(orow % kRows);
+  bc = (uint32_t)(ocol % kChunk);
 }
 
-// Entries per block (warp per CSR row; lanes whose entries share a block add once).
+// Stored values per block (warp per CSR row; lanes whose values share a block add once).
 __global__ void blocked_count_kernel(const uint64_t* ptr, const uint32_t* col, uint64_t n_rows,
                                      bool transpose, uint32_t n_chunks, uint32_t* counts) {
   uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -402,24 +483,26 @@ __global__ void blocked_count_kernel(const uint64_t* ptr, const uint32_t* col, u
     unsigned active = __ballot_sync(0xFFFFFFFFu, in);
     if (!in) continue;
     uint64_t block;
-    uint16_t packed;
-    uint32_t c = col[i];
-    locate(r, c, transpose, n_chunks, block, packed);
+    uint32_t br, bc;
+    locate(r, col[i], transpose, n_chunks, block, br, bc);
     unsigned same = __match_any_sync(active, block);
     if ((unsigned)__ffs(same) - 1 == lane) atomicAdd(&counts[block], (uint32_t)__popc(same));
   }
 }
 
-__global__ void pad_counts_kernel(const uint32_t* counts, uint64_t n, uint64_t* padded) {
+// A block's size in 16-byte units: 128 mask words and its values padded to 4 (none for
+// an empty block).
+__global__ void block_units_kernel(const uint32_t* counts, uint64_t n, uint64_t* units) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (i < n) padded[i] = ((uint64_t)counts[i] + 7) & ~7ull;
-  if (i == n) padded[i] = 0;
+  if (i < n) units[i] = counts[i] ? kMaskBytes / 16 + ((uint64_t)counts[i] + 3) / 4 : 0;
+  if (i == n) units[i] = 0;
 }
 
-__global__ void blocked_fill_kernel(const uint64_t* ptr, const uint32_t* col, const float* val,
-                                    uint64_t n_rows, bool transpose, uint32_t n_chunks,
-                                    const uint64_t* off, uint32_t* cursor, uint16_t* out_idx,
-                                    float* out_val) {
+// Mask bits: bit c of word r of a block marks the value at (row r, column c). Lanes that
+// hit the same word OR their bits together first.
+__global__ void blocked_mask_kernel(const uint64_t* ptr, const uint32_t* col, uint64_t n_rows,
+                                    bool transpose, uint32_t n_chunks, const uint64_t* off,
+                                    uint8_t* data) {
   uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   unsigned lane = threadIdx.x & 31u;
   if (r >= n_rows) return;
@@ -429,23 +512,52 @@ __global__ void blocked_fill_kernel(const uint64_t* ptr, const uint32_t* col, co
     unsigned active = __ballot_sync(0xFFFFFFFFu, in);
     if (!in) continue;
     uint64_t block;
-    uint16_t packed;
-    locate(r, col[i], transpose, n_chunks, block, packed);
-    unsigned same = __match_any_sync(active, block);
-    unsigned leader = (unsigned)__ffs(same) - 1;
-    uint32_t base = 0;
-    if (lane == leader) base = atomicAdd(&cursor[block], (uint32_t)__popc(same));
-    base = __shfl_sync(same, base, leader);
-    uint64_t at = off[block] + base + __popc(same & ((1u << lane) - 1u));
-    out_idx[at] = packed;
-    out_val[at] = val[i];
+    uint32_t br, bc;
+    locate(r, col[i], transpose, n_chunks, block, br, bc);
+    uint32_t* word = reinterpret_cast<uint32_t*>(data + off[block] * 16) + br;
+    unsigned same = __match_any_sync(active, reinterpret_cast<uint64_t>(word));
+    uint32_t bits = __reduce_or_sync(same, 1u << bc);
+    if ((unsigned)__ffs(same) - 1 == lane) atomicOr(word, bits);
   }
 }
 
-__global__ void fill_u16_kernel(uint16_t* p, uint64_t n, uint16_t v) {
-  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-       i += (uint64_t)gridDim.x * blockDim.x)
-    p[i] = v;
+// prefix[b * 128 + row]: the values of block b in the rows before `row` (warp per block).
+__global__ void row_prefix_kernel(const uint64_t* off, const uint8_t* data, uint64_t n_blocks,
+                                  uint16_t* prefix) {
+  uint64_t b = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  unsigned lane = threadIdx.x & 31u;
+  if (b >= n_blocks || off[b + 1] == off[b]) return;
+  const uint32_t* masks = reinterpret_cast<const uint32_t*>(data + off[b] * 16);
+  uint32_t carry = 0;
+  for (int q = 0; q < kRows / 32; ++q) {
+    uint32_t v = __popc(masks[q * 32 + lane]);
+    uint32_t incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    prefix[b * kRows + q * 32 + lane] = (uint16_t)(carry + incl - v);
+    carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
+  }
+}
+
+// Each value at its rank in its block (rows in order, columns in order inside a row).
+__global__ void blocked_values_kernel(const uint64_t* ptr, const uint32_t* col, const float* val,
+                                      uint64_t n_rows, bool transpose, uint32_t n_chunks,
+                                      const uint64_t* off, const uint16_t* prefix,
+                                      uint8_t* data) {
+  uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  unsigned lane = threadIdx.x & 31u;
+  if (r >= n_rows) return;
+  for (uint64_t i = ptr[r] + lane; i < ptr[r + 1]; i += 32) {
+    uint64_t block;
+    uint32_t br, bc;
+    locate(r, col[i], transpose, n_chunks, block, br, bc);
+    uint8_t* blk = data + off[block] * 16;
+    const uint32_t word = reinterpret_cast<const uint32_t*>(blk)[br];
+    const uint32_t rank = prefix[block * kRows + br] + __popc(word & ((1u << bc) - 1u));
+    reinterpret_cast<float*>(blk + kMaskBytes)[rank] = val[i];
+  }
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode() {
@@ -497,25 +609,29 @@ void build_blocked(const uint64_t* ptr, const uint32_t* col, const float* val, u
     KG_LAUNCH_CHECK();
   }
   out.off.alloc(nb + 1, s);
-  pad_counts_kernel<<<blocks_for(nb + 1, 256), 256, 0, s>>>(counts.ptr, nb, out.off.ptr);
+  block_units_kernel<<<blocks_for(nb + 1, 256), 256, 0, s>>>(counts.ptr, nb, out.off.ptr);
   KG_LAUNCH_CHECK();
+  counts.reset();
   size_t temp = 0;
   KG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, out.off.ptr, out.off.ptr, nb + 1, s));
   DeviceBuffer<unsigned char> scratch(temp, s);
   KG_CUDA(cub::DeviceScan::ExclusiveSum(scratch.ptr, temp, out.off.ptr, out.off.ptr, nb + 1, s));
-  KG_CUDA(cudaMemcpyAsync(&out.nnz_padded, out.off.ptr + nb, 8, cudaMemcpyDeviceToHost, s));
+  uint64_t units = 0;
+  KG_CUDA(cudaMemcpyAsync(&units, out.off.ptr + nb, 8, cudaMemcpyDeviceToHost, s));
   KG_CUDA(cudaStreamSynchronize(s));
-  out.idx.alloc(std::max<uint64_t>(out.nnz_padded, 8), s);
-  out.val.alloc(std::max<uint64_t>(out.nnz_padded, 8), s);
-  fill_u16_kernel<<<std::min<unsigned>(blocks_for(out.idx.count, 256), 16384), 256, 0, s>>>(
-      out.idx.ptr, out.idx.count, kPad);
-  KG_LAUNCH_CHECK();
-  out.val.zero();
+  out.bytes = units * 16;
+  out.data.alloc(std::max<uint64_t>(out.bytes, 16), s);
+  out.data.zero();
   if (nnz) {
-    counts.zero();  // reused as the per-block cursor
-    blocked_fill_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(
-        ptr, col, val, n_rows, transpose, out.n_chunks, out.off.ptr, counts.ptr, out.idx.ptr,
-        out.val.ptr);
+    blocked_mask_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(
+        ptr, col, n_rows, transpose, out.n_chunks, out.off.ptr, out.data.ptr);
+    KG_LAUNCH_CHECK();
+    DeviceBuffer<uint16_t> prefix(nb * kRows, s);
+    row_prefix_kernel<<<blocks_for(nb * 32, 256), 256, 0, s>>>(out.off.ptr, out.data.ptr, nb,
+                                                               prefix.ptr);
+    KG_LAUNCH_CHECK();
+    blocked_values_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(
+        ptr, col, val, n_rows, transpose, out.n_chunks, out.off.ptr, prefix.ptr, out.data.ptr);
     KG_LAUNCH_CHECK();
   }
 }
@@ -541,9 +657,9 @@ void spmm_tc(const SpmmArgs& a, cudaStream_t s) {
   err.zero();
   uint64_t items = (uint64_t)geo.n_tiles * geo.n_segs;
   unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)a.sm_count));
-  spmm_tc_kernel<<<grid, kSpThreads, kSpSmemBytes, s>>>(mh, ml, b.off.ptr, b.idx.ptr, b.val.ptr,
-                                                        b.rows, geo, a.value_mode, a.row_means,
-                                                        a.out, err.ptr);
+  spmm_tc_kernel<<<grid, kSpThreads, kSpSmemBytes, s>>>(mh, ml, b.off.ptr, b.data.ptr, b.rows,
+                                                        geo, a.value_mode, a.row_means, a.out,
+                                                        err.ptr);
   KG_LAUNCH_CHECK();
   int h = 0;
   KG_CUDA(cudaMemcpyAsync(&h, err.ptr, 4, cudaMemcpyDeviceToHost, s));

@@ -8,20 +8,19 @@
 
 namespace kg {
 
-// A sparse matrix (rows x K) cut into blocks of 128 rows x 32 columns: block
-// (tile, chunk) holds its entries contiguously at [off[b], off[b+1]) with
-// b = tile * n_chunks + chunk, each entry a 16-bit (row_in_tile << 5 | col_in_chunk) and
-// an f32 value. Every block's length is a multiple of 8 (padding entries are 0xFFFF),
-// so each block starts 16-byte aligned in both arrays and one bulk copy fetches it.
-// The order of the entries inside a block is free: each lands on its own cell of the
-// densified tile, so the products do not depend on it.
+// A sparse matrix (rows x K) cut into blocks of 128 rows x 32 columns. Block
+// b = tile * n_chunks + chunk starts at byte 16 * off[b] of `data` and is empty
+// (off[b + 1] == off[b]) or holds 128 mask words (bit c of word r: a value at row r,
+// column c of the block) followed by its values, rows in order and columns in order
+// inside a row, padded to a multiple of 4 floats: 16-byte aligned, one bulk copy each.
+// At the benchmark's 30% density that is 512 + 4 nnz bytes a block, against 6 nnz for
+// 16-bit positions beside the values.
 struct Blocked {
   uint64_t rows = 0, K = 0;
   uint32_t n_tiles = 0, n_chunks = 0;
-  uint64_t nnz_padded = 0;
-  DeviceBuffer<uint64_t> off;
-  DeviceBuffer<uint16_t> idx;
-  DeviceBuffer<float> val;
+  uint64_t bytes = 0;
+  DeviceBuffer<uint64_t> off;   // n_tiles * n_chunks + 1 offsets, 16-byte units
+  DeviceBuffer<uint8_t> data;
 };
 
 // The blocked layout of a CSR matrix (n_rows x n_cols, u32 column indices, each row's
