@@ -200,6 +200,63 @@ KG_API kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t n_ro
 
 /* ---------------------------------------------------------------- diagnostics ----- */
 
+/* ------------------------------------------------------- learned-partition kNN ---- */
+
+/* No counterpart in kyto: the north star's learned form. A BF16 MLP (n_components ->
+ * hidden -> hidden -> n_parts, ReLU) is trained on the device on the exact kNN graph of
+ * train_cells evenly strided rows (targets: the k-means parts of a row and of its
+ * n_neighbors - 1 neighbours; soft-target cross-entropy, Adam, `epochs` seeded
+ * shuffles of `batch` rows); every row then gets its n_probe most probable parts, lives
+ * in the most probable one, and is searched exactly (kg_knn_exact's filter and re-rank)
+ * among the rows of the parts its block of 256 query rows probes, or against every row
+ * when the probed parts' summed probability is below `confidence`. */
+typedef struct kg_learned_params {
+  uint32_t n_parts;        /* partitions (>= 2) */
+  uint32_t hidden;         /* hidden width */
+  uint32_t n_probe;        /* parts searched per row (1..64) */
+  float confidence;        /* below: the row is searched against every row */
+  uint64_t train_cells;    /* sampled rows whose exact graph trains the network (0: all) */
+  uint32_t epochs;         /* passes over the sample */
+  uint32_t batch;          /* rows per training step */
+  float learning_rate;     /* Adam's */
+  uint32_t reserved;
+  uint64_t seed;
+} kg_learned_params;
+
+typedef struct kg_learned_stats {
+  uint64_t fallback_rows;  /* rows searched against every row (low confidence) */
+  uint64_t scanned_tiles;  /* point tiles (128 rows) the query blocks scanned, in all */
+  uint64_t candidates;     /* approximate candidates ranked by their exact keys */
+  uint64_t rows_full;      /* rows searched in full by the exact re-rank's own checks */
+  double train_ms;         /* sample graph, parts and training (host wall time) */
+  double index_ms;         /* every row's parts */
+  double search_ms;        /* the restricted exact search and the graph */
+  float final_loss;        /* mean cross-entropy of the last training batch */
+  float reserved;
+} kg_learned_stats;
+
+/* The graph (as kg_knn_exact's: CSR, rows sorted by column, f32 distances) of each
+ * row's n_neighbors - 1 nearest rows among those the learned partitions propose. */
+KG_API kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n_rows,
+                                uint32_t width, uint32_t n_components, uint32_t n_neighbors,
+                                const kg_learned_params* params, uint64_t* indptr,
+                                uint32_t* indices, float* distances, kg_learned_stats* stats);
+
+/* Offsets (floats) of W1, b1, W2, b2, W3, b3 in the network's packed f32 parameters
+ * (W row-major out x in) and their total. */
+KG_API kg_status kg_learned_layout(uint32_t din, uint32_t hidden, uint32_t parts,
+                                   uint64_t* offsets /* 6 */, uint64_t* total);
+
+/* One forward and backward pass of the network on `rows` rows of x (rows x din f32):
+ * the gradients of the mean soft-target cross-entropy (targets: each row's n_labels
+ * part labels, equally weighted) with respect to the packed parameters, each row's loss
+ * and (if not NULL) the logits (rows x parts). For checking the device kernels. */
+KG_API kg_status kg_learned_gradients(kg_ctx* ctx, uint32_t din, uint32_t hidden,
+                                      uint32_t parts, const float* params, const float* x,
+                                      uint32_t rows, const uint32_t* labels,
+                                      uint32_t n_labels, float* grads, float* row_loss,
+                                      float* logits);
+
 /* Kernels of this library launched since it was loaded (library calls such as cuBLAS
  * not counted): lets a benchmark state how many of its own kernels a timed region ran.
  * No counterpart in kyto (diagnostics only). */

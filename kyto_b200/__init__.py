@@ -39,7 +39,8 @@ EXPORTS = (
     "kg_open", "kg_close", "kg_last_error", "kg_set_cancel_flag", "kg_progress",
     "kg_normalize_log1p", "kg_hvg_moments", "kg_hvg_moments_noalloc", "kg_hvg_seurat",
     "kg_pca_begin", "kg_pca_push_block", "kg_pca_run", "kg_pca_results", "kg_pca_info",
-    "kg_pca_embedding_device", "kg_pca_free", "kg_knn_exact", "kg_diag_kernel_launches",
+    "kg_pca_embedding_device", "kg_pca_free", "kg_knn_exact", "kg_knn_learned",
+    "kg_learned_layout", "kg_learned_gradients", "kg_diag_kernel_launches",
 )
 
 
@@ -61,6 +62,43 @@ class _PcaParams(ctypes.Structure):
         ("target_sum", ctypes.c_double),
         ("log1p", ctypes.c_int32),
         ("reserved", ctypes.c_uint32),
+    ]
+
+
+class LearnedParams(ctypes.Structure):
+    """kg_learned_params: the learned-partition kNN's settings (defaults: 1,024 parts,
+    256 hidden, top-8 probes, confidence 0.9, 200,000 training rows)."""
+
+    _fields_ = [
+        ("n_parts", ctypes.c_uint32),
+        ("hidden", ctypes.c_uint32),
+        ("n_probe", ctypes.c_uint32),
+        ("confidence", ctypes.c_float),
+        ("train_cells", ctypes.c_uint64),
+        ("epochs", ctypes.c_uint32),
+        ("batch", ctypes.c_uint32),
+        ("learning_rate", ctypes.c_float),
+        ("reserved", ctypes.c_uint32),
+        ("seed", ctypes.c_uint64),
+    ]
+
+    def __init__(self, n_parts=1024, hidden=256, n_probe=8, confidence=0.9,
+                 train_cells=200_000, epochs=6, batch=4096, learning_rate=1e-3, seed=0):
+        super().__init__(n_parts, hidden, n_probe, confidence, train_cells, epochs, batch,
+                         learning_rate, 0, seed)
+
+
+class LearnedStats(ctypes.Structure):
+    _fields_ = [
+        ("fallback_rows", ctypes.c_uint64),
+        ("scanned_tiles", ctypes.c_uint64),
+        ("candidates", ctypes.c_uint64),
+        ("rows_full", ctypes.c_uint64),
+        ("train_ms", ctypes.c_double),
+        ("index_ms", ctypes.c_double),
+        ("search_ms", ctypes.c_double),
+        ("final_loss", ctypes.c_float),
+        ("reserved", ctypes.c_float),
     ]
 
 
@@ -101,6 +139,10 @@ def library() -> ctypes.CDLL:
             "kg_pca_info": [P, P, P, P],
             "kg_pca_embedding_device": [P, ctypes.POINTER(P)],
             "kg_knn_exact": [P, P, U64, U32, U32, U32, P, P, P, ctypes.POINTER(KnnStats)],
+            "kg_knn_learned": [P, P, U64, U32, U32, U32, ctypes.POINTER(LearnedParams), P, P, P,
+                               ctypes.POINTER(LearnedStats)],
+            "kg_learned_layout": [U32, U32, U32, P, P],
+            "kg_learned_gradients": [P, U32, U32, U32, P, P, U32, P, U32, P, P, P],
             "kg_diag_kernel_launches": [P],
         }
         for name, args in sig.items():
@@ -378,3 +420,50 @@ def neighbors(embedding, n_neighbors: int = 15, n_components: int | None = None,
                                   int(n_neighbors), _ptr(indptr), _ptr(indices), _ptr(dist),
                                   ctypes.byref(stats)))
     return Graph(indptr, indices, dist, stats)
+
+
+def neighbors_learned(embedding, n_neighbors: int = 15, n_components: int | None = None,
+                      params: LearnedParams | None = None,
+                      ctx: Context | None = None) -> tuple[Graph, LearnedStats]:
+    """The learned-partition kNN (kg_knn_learned): the graph of each row's n_neighbors - 1
+    nearest rows among those its learned partitions propose, and the run's counters."""
+    ctx = ctx or default_context()
+    if isinstance(embedding, np.ndarray):
+        embedding = np.ascontiguousarray(embedding, dtype=np.float32)
+    n, width = embedding.shape
+    k = int(n_neighbors) - 1
+    indptr = np.empty(n + 1, dtype=np.uint64)
+    indices = np.empty(max(n * k, 0), dtype=np.uint32)
+    dist = np.empty(max(n * k, 0), dtype=np.float32)
+    stats = LearnedStats()
+    params = params or LearnedParams()
+    _check(library().kg_knn_learned(ctx.handle, _ptr(embedding), n, width,
+                                    0 if n_components is None else int(n_components),
+                                    int(n_neighbors), ctypes.byref(params), _ptr(indptr),
+                                    _ptr(indices), _ptr(dist), ctypes.byref(stats)))
+    return Graph(indptr, indices, dist), stats
+
+
+def learned_layout(din: int, hidden: int, parts: int) -> tuple[list[int], int]:
+    """Offsets of W1, b1, W2, b2, W3, b3 in the network's packed parameters, and the total."""
+    off = np.zeros(6, dtype=np.uint64)
+    total = ctypes.c_uint64()
+    _check(library().kg_learned_layout(din, hidden, parts, _ptr(off), ctypes.byref(total)))
+    return [int(v) for v in off], total.value
+
+
+def learned_gradients(params: np.ndarray, x: np.ndarray, labels: np.ndarray, hidden: int,
+                      parts: int, ctx: Context | None = None):
+    """One forward/backward pass of the partitioner network on the device: (gradients of
+    the packed parameters, per-row losses, logits)."""
+    ctx = ctx or default_context()
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    labels = np.ascontiguousarray(labels, dtype=np.uint32)
+    rows, din = x.shape
+    grads = np.empty(params.shape, dtype=np.float32)
+    loss = np.empty(rows, dtype=np.float32)
+    logits = np.empty((rows, parts), dtype=np.float32)
+    _check(library().kg_learned_gradients(
+        ctx.handle, din, hidden, parts, _ptr(np.ascontiguousarray(params, dtype=np.float32)),
+        _ptr(x), rows, _ptr(labels), labels.shape[1], _ptr(grads), _ptr(loss), _ptr(logits)))
+    return grads, loss, logits

@@ -388,13 +388,14 @@ __global__ void rank_kernel(const float* __restrict__ x, uint32_t width, uint32_
                             const float* cand_key, const uint32_t* cand_row,
                             const uint32_t* cand_count, const float* threshold,
                             const double* slack, double inv_s2, const double* qn2,
-                            const uint32_t* perm, double* out_key, uint32_t* out_row,
-                            uint32_t* full_flag, unsigned long long* n_candidates) {
+                            const uint32_t* qperm, const uint32_t* pperm, double* out_key,
+                            uint32_t* out_row, uint32_t* full_flag,
+                            unsigned long long* n_candidates) {
   uint64_t qi = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   unsigned lane = threadIdx.x & 31u;
   uint64_t qp = q_begin + qi;
   if (qp >= q_end) return;
-  uint64_t q = perm ? perm[qp] : qp;
+  uint64_t q = qperm ? qperm[qp] : qp;
   uint32_t count = cand_count[qi];
   if (count == kOverflow) {
     if (lane == 0) full_flag[q] = 1;
@@ -413,7 +414,7 @@ __global__ void rank_kernel(const float* __restrict__ x, uint32_t width, uint32_
     float ak = cand_key[qi * (uint64_t)cap + c];
     if (ak > th) continue;
     uint32_t p = cand_row[qi * (uint64_t)cap + c];
-    if (perm) p = perm[p];
+    if (pperm) p = pperm[p];
     double e = exact_key(qrow, x + (uint64_t)p * width, d);
     if (fabs(e - ((double)ak * inv_s2 + shift)) > sl) bad = true;
     offer(keys, idx, len, k, e, p);
@@ -502,10 +503,6 @@ __global__ void compact_flags_kernel(const uint32_t* flag, uint64_t n, uint32_t*
   if (r < n && flag[r]) list[atomicAdd(count, 1u)] = (uint32_t)r;
 }
 
-}  // namespace kg
-
-using namespace kg;
-
 namespace {
 
 struct Timer {
@@ -529,6 +526,206 @@ struct Timer {
 
 }  // namespace
 
+// The exact search on device rows: every row's k nearest other rows by (kyto key, row)
+// into out.key / out.row (n x k). `plan` chooses the tensor-core filter's scan (NULL:
+// the rows in a spatial order, each query block scanning every tile from its own).
+void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t d, uint32_t k,
+              const PlanBuilder* plan, KnnResult& out, Trace& trace) {
+  cudaStream_t s = ctx->stream;
+  DeviceBuffer<double> mean(d, s), squares(n, s), slack(n, s), largest(1, s);
+  DeviceBuffer<float> rows(n * kDim, s), offsets(n, s), lo_hi(6, s);
+  column_stats(x, n, width, d, mean.ptr, lo_hi.ptr, s);
+  centre_kernel<<<blocks_for(n, 128), 128, 0, s>>>(x, n, width, d, mean.ptr, rows.ptr,
+                                                   offsets.ptr, squares.ptr);
+  max_kernel_launch(squares.ptr, n, largest.ptr, s);
+  slack_kernel<<<blocks_for(n, 256), 256, 0, s>>>(squares.ptr, n, d, largest.ptr, slack.ptr);
+  KG_LAUNCH_CHECK();
+  double h_largest = 0;
+  KG_CUDA(cudaMemcpyAsync(&h_largest, largest.ptr, 8, cudaMemcpyDeviceToHost, s));
+  KG_CUDA(cudaStreamSynchronize(s));
+  bool brute = !std::isfinite(h_largest) || std::sqrt(h_largest) > 1e15;
+
+  out.key.alloc(n * k, s);
+  out.row.alloc(n * k, s);
+  DeviceBuffer<uint32_t> full_flag(n, s);
+  DeviceBuffer<unsigned long long> n_cand(1, s);
+  n_cand.zero();
+  double filter_ms = 0, rank_ms = 0;
+  // The filter: the tensor-core GEMM (fp16, or bf16 on request) when the components
+  // and the three norm columns fit one 64-wide operand row; the SIMT filter otherwise
+  // or on request (KYTO_GPU_KNN_FILTER=simt|fp16|bf16). All give the same graph.
+  const char* choice = std::getenv("KYTO_GPU_KNN_FILTER");
+  std::string filter = choice ? choice : "fp16";
+  bool tc = !brute && d + 3 <= 64 && (filter == "fp16" || filter == "bf16");
+  if (brute) {
+    uint32_t one = 1;
+    std::vector<uint32_t> all(n, one);
+    KG_CUDA(cudaMemcpyAsync(full_flag.ptr, all.data(), n * 4, cudaMemcpyHostToDevice, s));
+  } else if (tc) {
+    check_cancel(ctx);
+    const uint32_t cap = kTcCap;
+    DeviceBuffer<float> cand_key(n * cap, s), thr(n, s);
+    DeviceBuffer<uint32_t> cand_row(n * cap, s), cand_count(n, s);
+    DeviceBuffer<double> qn2(n, s), slack_d(n, s), max_sq(1, s);
+    Timer tf(s);
+    const double scale = tc_scale(x, n, width, d, mean.ptr, max_sq.ptr, s);
+    ScanPlan sp;
+    if (plan) {
+      (*plan)(x, n, width, d, scale, sp, trace);
+    } else {
+      // The rows sorted by a Morton code of their first three centred components, so
+      // a query block's own tiles hold its nearest points and the scan starts there.
+      spatial_order(x, n, width, d, mean.ptr, lo_hi.ptr, sp.qrows, s);
+      trace.mark("scan order");
+    }
+    FilterScan scan;
+    scan.n_q = n;
+    scan.n_p = n;
+    scan.q_point = sp.q_point.ptr;
+    scan.list_tiles = sp.list_tiles.ptr;
+    scan.list_lb2 = sp.list_lb2.ptr;
+    scan.list_off = sp.list_off.ptr;
+    scan.list_stride = sp.list_stride;
+    const uint32_t* prows = sp.prows.ptr ? sp.prows.ptr : sp.qrows.ptr;
+    tc_filter(ctx, s, x, width, d, sp.qrows.ptr, prows, scan, mean.ptr, scale, max_sq.ptr,
+              filter == "bf16", k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
+              qn2.ptr, slack_d.ptr, &trace);
+    filter_ms += tf.stop_ms();
+    check_cancel(ctx);
+    Timer tr(s);
+    rank_kernel<<<blocks_for(n * 32, kRankWarps * 32), kRankWarps * 32, 0, s>>>(
+        x, width, d, 0, n, k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
+        slack_d.ptr, 1.0 / (scale * scale), qn2.ptr, sp.qrows.ptr, prows, out.key.ptr,
+        out.row.ptr, full_flag.ptr, n_cand.ptr);
+    KG_LAUNCH_CHECK();
+    rank_ms += tr.stop_ms();
+    ctx->done = n;
+  } else {
+    const uint32_t cap = kCandidateCap;
+    uint64_t chunk = std::min<uint64_t>(n, kQueryChunk);
+    DeviceBuffer<float> cand_key(chunk * cap, s), thr(chunk, s);
+    DeviceBuffer<uint32_t> cand_row(chunk * cap, s), cand_count(chunk, s);
+    for (uint64_t q0 = 0; q0 < n; q0 += chunk) {
+      check_cancel(ctx);
+      uint64_t q1 = std::min(n, q0 + chunk);
+      Timer tf(s);
+      filter_kernel<<<blocks_for(q1 - q0, kFilterThreads), kFilterThreads, 0, s>>>(
+          rows.ptr, offsets.ptr, slack.ptr, n, q0, q1, k, cap, cand_key.ptr, cand_row.ptr,
+          cand_count.ptr, thr.ptr);
+      KG_LAUNCH_CHECK();
+      filter_ms += tf.stop_ms();
+      Timer tr(s);
+      rank_kernel<<<blocks_for((q1 - q0) * 32, kRankWarps * 32), kRankWarps * 32, 0, s>>>(
+          x, width, d, q0, q1, k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
+          slack.ptr, 1.0, nullptr, nullptr, nullptr, out.key.ptr, out.row.ptr, full_flag.ptr,
+          n_cand.ptr);
+      KG_LAUNCH_CHECK();
+      rank_ms += tr.stop_ms();
+      ctx->done = q1;
+    }
+  }
+  trace.mark("rank");
+  // Rows that need a full search.
+  DeviceBuffer<uint32_t> list(n, s);
+  DeviceBuffer<unsigned int> n_full(1, s);
+  n_full.zero();
+  compact_flags_kernel<<<blocks_for(n, 256), 256, 0, s>>>(full_flag.ptr, n, list.ptr,
+                                                          n_full.ptr);
+  KG_LAUNCH_CHECK();
+  unsigned int h_full = 0;
+  KG_CUDA(cudaMemcpyAsync(&h_full, n_full.ptr, 4, cudaMemcpyDeviceToHost, s));
+  KG_CUDA(cudaStreamSynchronize(s));
+  if (h_full) {
+    // The list's order does not matter: each CTA writes its own row.
+    Timer tr(s);
+    for (uint64_t a = 0; a < h_full; a += 65535) {
+      check_cancel(ctx);
+      unsigned blocks = (unsigned)std::min<uint64_t>(65535, h_full - a);
+      full_rows_kernel<<<blocks, kFullWarps * 32, 0, s>>>(x, n, width, d, k, list.ptr + a,
+                                                          out.key.ptr, out.row.ptr);
+      KG_LAUNCH_CHECK();
+    }
+    rank_ms += tr.stop_ms();
+  }
+  trace.mark("full rows");
+  unsigned long long h_cand = 0;
+  KG_CUDA(cudaMemcpyAsync(&h_cand, n_cand.ptr, 8, cudaMemcpyDeviceToHost, s));
+  KG_CUDA(cudaStreamSynchronize(s));
+  out.candidates = h_cand;
+  out.rows_full = h_full;
+  out.filter_ms = filter_ms;
+  out.rank_ms = rank_ms;
+}
+
+// n_neighbors and n_components checked as neighbors::search does (neighbors.rs:226-312);
+// returns k and d.
+void check_search_args(uint64_t n, uint32_t width, uint32_t n_components, uint32_t n_neighbors,
+                       uint32_t& k, uint32_t& d) {
+  if (width == 0) fail(KG_ERR_INVALID, "neighbors: an embedding of 0 components");
+  d = n_components ? n_components : width;
+  if (d > width)
+    fail(KG_ERR_INVALID, "neighbors: n_components " + std::to_string(n_components) +
+                             " is more than the embedding's " + std::to_string(width));
+  if (d > (uint32_t)kDim)
+    fail(KG_ERR_INVALID, "neighbors: more than " + std::to_string(kDim) + " components");
+  if (n_neighbors < 2 || n_neighbors > n)
+    fail(KG_ERR_INVALID, "neighbors: n_neighbors " + std::to_string(n_neighbors) +
+                             " (it counts the cell itself; " + std::to_string(n) +
+                             " cells): an int from 2 to " + std::to_string(std::max<uint64_t>(n, 2)));
+  if (n - 1 >= (1ull << 32)) fail(KG_ERR_INVALID, "neighbors: at most 2^32 cells");
+  k = n_neighbors - 1;
+  if (k > (uint32_t)kMaxK)
+    fail(KG_ERR_INVALID, "neighbors: n_neighbors above " + std::to_string(kMaxK + 1));
+}
+
+// Finite values only (neighbors.rs:279-291).
+void check_finite(const float* x, uint64_t n, uint32_t width, uint32_t d, cudaStream_t s) {
+  DeviceBuffer<unsigned long long> bad(1, s);
+  unsigned long long init = ~0ull;
+  KG_CUDA(cudaMemcpyAsync(bad.ptr, &init, 8, cudaMemcpyHostToDevice, s));
+  finite_check_kernel<<<std::min<unsigned>(blocks_for(n * d, 256), 8192), 256, 0, s>>>(
+      x, n, width, d, bad.ptr);
+  KG_LAUNCH_CHECK();
+  unsigned long long first = 0;
+  KG_CUDA(cudaMemcpyAsync(&first, bad.ptr, 8, cudaMemcpyDeviceToHost, s));
+  KG_CUDA(cudaStreamSynchronize(s));
+  if (first != ~0ull)
+    fail(KG_ERR_INVALID, "neighbors: row " + std::to_string(first / width) + ", component " +
+                             std::to_string(first % width) + " is not finite");
+}
+
+// The CSR graph (rows sorted by column, f32 sqrt of the key) into host or device memory.
+void write_graph(const KnnResult& r, uint64_t n, uint32_t k, uint64_t* indptr, uint32_t* indices,
+                 float* distances, cudaStream_t s) {
+  DeviceBuffer<uint64_t> g_indptr;
+  DeviceBuffer<uint32_t> g_idx;
+  DeviceBuffer<float> g_dist;
+  bool dev_out = is_device_pointer(indptr);
+  uint64_t* gi = indptr;
+  uint32_t* gx = indices;
+  float* gd = distances;
+  if (!dev_out) {
+    g_indptr.alloc(n + 1, s);
+    g_idx.alloc(n * k, s);
+    g_dist.alloc(n * k, s);
+    gi = g_indptr.ptr;
+    gx = g_idx.ptr;
+    gd = g_dist.ptr;
+  }
+  graph_kernel<<<blocks_for(n, 128), 128, 0, s>>>(r.key.ptr, r.row.ptr, n, k, gi, gx, gd);
+  KG_LAUNCH_CHECK();
+  if (!dev_out) {
+    KG_CUDA(cudaMemcpyAsync(indptr, gi, (n + 1) * 8, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaMemcpyAsync(indices, gx, n * k * 4, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaMemcpyAsync(distances, gd, n * k * 4, cudaMemcpyDeviceToHost, s));
+  }
+  KG_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace kg
+
+using namespace kg;
+
 extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t n,
                                   uint32_t width, uint32_t n_components,
                                   uint32_t n_neighbors, uint64_t* indptr, uint32_t* indices,
@@ -536,178 +733,27 @@ extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t 
   return guarded([&] {
     if (!ctx || !embedding || !indptr || !indices || !distances)
       fail(KG_ERR_INVALID, "kg_knn_exact: NULL argument");
-    if (width == 0) fail(KG_ERR_INVALID, "neighbors: an embedding of 0 components");
-    uint32_t d = n_components ? n_components : width;
-    if (d > width)
-      fail(KG_ERR_INVALID, "neighbors: n_components " + std::to_string(n_components) +
-                               " is more than the embedding's " + std::to_string(width));
-    if (d > (uint32_t)kDim)
-      fail(KG_ERR_INVALID, "neighbors: more than " + std::to_string(kDim) + " components");
-    if (n_neighbors < 2 || n_neighbors > n)
-      fail(KG_ERR_INVALID, "neighbors: n_neighbors " + std::to_string(n_neighbors) +
-                               " (it counts the cell itself; " + std::to_string(n) +
-                               " cells): an int from 2 to " + std::to_string(std::max<uint64_t>(n, 2)));
-    if (n - 1 >= (1ull << 32)) fail(KG_ERR_INVALID, "neighbors: at most 2^32 cells");
-    uint32_t k = n_neighbors - 1;
-    if (k > (uint32_t)kMaxK)
-      fail(KG_ERR_INVALID, "neighbors: n_neighbors above " + std::to_string(kMaxK + 1));
+    uint32_t k = 0, d = 0;
+    check_search_args(n, width, n_components, n_neighbors, k, d);
     use_device(ctx);
     cudaStream_t s = ctx->stream;
     ctx->total = n;
     ctx->done = 0;
     DeviceBuffer<float> hold;
     const float* x = device_view(embedding, n * width, hold, s);
-    // Finite values only (neighbors.rs:279-291).
-    {
-      DeviceBuffer<unsigned long long> bad(1, s);
-      unsigned long long init = ~0ull;
-      KG_CUDA(cudaMemcpyAsync(bad.ptr, &init, 8, cudaMemcpyHostToDevice, s));
-      finite_check_kernel<<<std::min<unsigned>(blocks_for(n * d, 256), 8192), 256, 0, s>>>(
-          x, n, width, d, bad.ptr);
-      KG_LAUNCH_CHECK();
-      unsigned long long first = 0;
-      KG_CUDA(cudaMemcpyAsync(&first, bad.ptr, 8, cudaMemcpyDeviceToHost, s));
-      KG_CUDA(cudaStreamSynchronize(s));
-      if (first != ~0ull)
-        fail(KG_ERR_INVALID, "neighbors: row " + std::to_string(first / width) +
-                                 ", component " + std::to_string(first % width) +
-                                 " is not finite");
-    }
+    check_finite(x, n, width, d, s);
     Trace trace(s, "knn_exact");
-    DeviceBuffer<double> mean(d, s), squares(n, s), slack(n, s), largest(1, s);
-    DeviceBuffer<float> rows(n * kDim, s), offsets(n, s), lo_hi(6, s);
-    column_stats(x, n, width, d, mean.ptr, lo_hi.ptr, s);
-    centre_kernel<<<blocks_for(n, 128), 128, 0, s>>>(x, n, width, d, mean.ptr, rows.ptr,
-                                                     offsets.ptr, squares.ptr);
-    max_kernel_launch(squares.ptr, n, largest.ptr, s);
-    slack_kernel<<<blocks_for(n, 256), 256, 0, s>>>(squares.ptr, n, d, largest.ptr, slack.ptr);
-    KG_LAUNCH_CHECK();
-    double h_largest = 0;
-    KG_CUDA(cudaMemcpyAsync(&h_largest, largest.ptr, 8, cudaMemcpyDeviceToHost, s));
-    KG_CUDA(cudaStreamSynchronize(s));
-    bool brute = !std::isfinite(h_largest) || std::sqrt(h_largest) > 1e15;
-
-    DeviceBuffer<double> out_key(n * k, s);
-    DeviceBuffer<uint32_t> out_row(n * k, s), full_flag(n, s);
-    DeviceBuffer<unsigned long long> n_cand(1, s);
-    n_cand.zero();
-    double filter_ms = 0, rank_ms = 0;
-    // The filter: the tensor-core GEMM (fp16, or bf16 on request) when the components
-    // and the three norm columns fit one 64-wide operand row; the SIMT filter otherwise
-    // or on request (KYTO_GPU_KNN_FILTER=simt|fp16|bf16). All give the same graph.
-    const char* choice = std::getenv("KYTO_GPU_KNN_FILTER");
-    std::string filter = choice ? choice : "fp16";
-    bool tc = !brute && d + 3 <= 64 && (filter == "fp16" || filter == "bf16");
-    if (brute) {
-      uint32_t one = 1;
-      std::vector<uint32_t> all(n, one);
-      KG_CUDA(cudaMemcpyAsync(full_flag.ptr, all.data(), n * 4, cudaMemcpyHostToDevice, s));
-    } else if (tc) {
-      check_cancel(ctx);
-      const uint32_t cap = kTcCap;
-      DeviceBuffer<float> cand_key(n * cap, s), thr(n, s);
-      DeviceBuffer<uint32_t> cand_row(n * cap, s), cand_count(n, s);
-      DeviceBuffer<double> qn2(n, s), slack_d(n, s);
-      double scale = 1.0;
-      Timer tf(s);
-      // Scan order: the rows sorted by a Morton code of their first three centred
-      // components, so a query block's own tiles hold its nearest points.
-      DeviceBuffer<uint32_t> perm;
-      spatial_order(x, n, width, d, mean.ptr, lo_hi.ptr, perm, s);
-      tc_filter(ctx, s, x, n, width, d, perm.ptr, mean.ptr, filter == "bf16", k, cap,
-                cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr, qn2.ptr, slack_d.ptr,
-                &scale);
-      filter_ms += tf.stop_ms();
-      check_cancel(ctx);
-      Timer tr(s);
-      rank_kernel<<<blocks_for(n * 32, kRankWarps * 32), kRankWarps * 32, 0, s>>>(
-          x, width, d, 0, n, k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
-          slack_d.ptr, 1.0 / (scale * scale), qn2.ptr, perm.ptr, out_key.ptr, out_row.ptr,
-          full_flag.ptr, n_cand.ptr);
-      KG_LAUNCH_CHECK();
-      rank_ms += tr.stop_ms();
-      ctx->done = n;
-    } else {
-      const uint32_t cap = kCandidateCap;
-      uint64_t chunk = std::min<uint64_t>(n, kQueryChunk);
-      DeviceBuffer<float> cand_key(chunk * cap, s), thr(chunk, s);
-      DeviceBuffer<uint32_t> cand_row(chunk * cap, s), cand_count(chunk, s);
-      for (uint64_t q0 = 0; q0 < n; q0 += chunk) {
-        check_cancel(ctx);
-        uint64_t q1 = std::min(n, q0 + chunk);
-        Timer tf(s);
-        filter_kernel<<<blocks_for(q1 - q0, kFilterThreads), kFilterThreads, 0, s>>>(
-            rows.ptr, offsets.ptr, slack.ptr, n, q0, q1, k, cap, cand_key.ptr, cand_row.ptr,
-            cand_count.ptr, thr.ptr);
-        KG_LAUNCH_CHECK();
-        filter_ms += tf.stop_ms();
-        Timer tr(s);
-        rank_kernel<<<blocks_for((q1 - q0) * 32, kRankWarps * 32), kRankWarps * 32, 0, s>>>(
-            x, width, d, q0, q1, k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
-            slack.ptr, 1.0, nullptr, nullptr, out_key.ptr, out_row.ptr, full_flag.ptr,
-            n_cand.ptr);
-        KG_LAUNCH_CHECK();
-        rank_ms += tr.stop_ms();
-        ctx->done = q1;
-      }
-    }
-    trace.mark("filter + rank");
-    // Rows that need a full search.
-    DeviceBuffer<uint32_t> list(n, s);
-    DeviceBuffer<unsigned int> n_full(1, s);
-    n_full.zero();
-    compact_flags_kernel<<<blocks_for(n, 256), 256, 0, s>>>(full_flag.ptr, n, list.ptr,
-                                                            n_full.ptr);
-    KG_LAUNCH_CHECK();
-    unsigned int h_full = 0;
-    KG_CUDA(cudaMemcpyAsync(&h_full, n_full.ptr, 4, cudaMemcpyDeviceToHost, s));
-    KG_CUDA(cudaStreamSynchronize(s));
-    if (h_full) {
-      // The list's order does not matter: each CTA writes its own row.
-      Timer tr(s);
-      for (uint64_t a = 0; a < h_full; a += 65535) {
-        check_cancel(ctx);
-        unsigned blocks = (unsigned)std::min<uint64_t>(65535, h_full - a);
-        full_rows_kernel<<<blocks, kFullWarps * 32, 0, s>>>(x, n, width, d, k, list.ptr + a,
-                                                            out_key.ptr, out_row.ptr);
-        KG_LAUNCH_CHECK();
-      }
-      rank_ms += tr.stop_ms();
-    }
-    trace.mark("full rows");
-    // The CSR graph.
-    DeviceBuffer<uint64_t> g_indptr;
-    DeviceBuffer<uint32_t> g_idx;
-    DeviceBuffer<float> g_dist;
-    bool dev_out = is_device_pointer(indptr);
-    uint64_t* gi = indptr;
-    uint32_t* gx = indices;
-    float* gd = distances;
-    if (!dev_out) {
-      g_indptr.alloc(n + 1, s);
-      g_idx.alloc(n * k, s);
-      g_dist.alloc(n * k, s);
-      gi = g_indptr.ptr;
-      gx = g_idx.ptr;
-      gd = g_dist.ptr;
-    }
-    graph_kernel<<<blocks_for(n, 128), 128, 0, s>>>(out_key.ptr, out_row.ptr, n, k, gi, gx, gd);
-    KG_LAUNCH_CHECK();
-    if (!dev_out) {
-      KG_CUDA(cudaMemcpyAsync(indptr, gi, (n + 1) * 8, cudaMemcpyDeviceToHost, s));
-      KG_CUDA(cudaMemcpyAsync(indices, gx, n * k * 4, cudaMemcpyDeviceToHost, s));
-      KG_CUDA(cudaMemcpyAsync(distances, gd, n * k * 4, cudaMemcpyDeviceToHost, s));
-    }
+    KnnResult r;
+    knn_core(ctx, x, n, width, d, k, nullptr, r, trace);
+    write_graph(r, n, k, indptr, indices, distances, s);
     trace.mark("graph");
-    unsigned long long h_cand = 0;
-    KG_CUDA(cudaMemcpyAsync(&h_cand, n_cand.ptr, 8, cudaMemcpyDeviceToHost, s));
     wait_stream(ctx, s);
     ctx->done = n;
     if (stats) {
-      stats->candidates = h_cand;
-      stats->rows_full = h_full;
-      stats->filter_ms = filter_ms;
-      stats->rank_ms = rank_ms;
+      stats->candidates = r.candidates;
+      stats->rows_full = r.rows_full;
+      stats->filter_ms = r.filter_ms;
+      stats->rank_ms = r.rank_ms;
     }
   });
 }

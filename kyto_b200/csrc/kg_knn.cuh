@@ -2,6 +2,9 @@
 #pragma once
 
 #include <cstdint>
+#include <functional>
+
+#include "kg_internal.cuh"
 
 namespace kg {
 
@@ -15,5 +18,36 @@ constexpr uint32_t kOverflow = 0xFFFFFFFFu;
 constexpr uint64_t kQueryChunk = 1ull << 18;  // queries per filter launch
 constexpr int kRankWarps = 4;
 constexpr int kFullWarps = 8;
+
+// Every row's k nearest other rows (device), with the search's counters.
+struct KnnResult {
+  DeviceBuffer<double> key;    // n x k, ascending by (key, row)
+  DeviceBuffer<uint32_t> row;
+  uint64_t candidates = 0, rows_full = 0;
+  double filter_ms = 0, rank_ms = 0;
+};
+
+// The tensor-core filter's scan: query slot q is row qrows[q], point slot p row prows[p]
+// (prows empty: qrows), q_point (or empty) maps a query slot to the point slot of the
+// same row; each block of 256 query slots scans its list of point tiles (list_off CSR, or
+// list_stride entries a block; no list: every tile from the block's own), skipping
+// tiles on their list_lb2 bounds when given.
+struct ScanPlan {
+  DeviceBuffer<uint32_t> qrows, prows, q_point;
+  DeviceBuffer<uint32_t> list_tiles;
+  DeviceBuffer<float> list_lb2;
+  DeviceBuffer<uint64_t> list_off;
+  uint64_t list_stride = 0;
+};
+using PlanBuilder = std::function<void(const float* x, uint64_t n, uint32_t width, uint32_t d,
+                                       double scale, ScanPlan& plan, Trace& trace)>;
+
+void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t d, uint32_t k,
+              const PlanBuilder* plan, KnnResult& out, Trace& trace);
+void check_search_args(uint64_t n, uint32_t width, uint32_t n_components, uint32_t n_neighbors,
+                       uint32_t& k, uint32_t& d);
+void check_finite(const float* x, uint64_t n, uint32_t width, uint32_t d, cudaStream_t s);
+void write_graph(const KnnResult& r, uint64_t n, uint32_t k, uint64_t* indptr, uint32_t* indices,
+                 float* distances, cudaStream_t s);
 
 }  // namespace kg

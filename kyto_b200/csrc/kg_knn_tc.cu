@@ -37,7 +37,7 @@ namespace kg {
 
 using namespace sm100;
 
-constexpr int kTcQueries = 256;
+constexpr int kTcQueries = (int)kTcQueryBlock;
 constexpr int kTcPoints = 128;
 constexpr int kTcK = 64;  // operand width (fp16 elements, one 128-byte swizzle row)
 constexpr int kStages = 6;
@@ -45,14 +45,20 @@ constexpr uint32_t kTileBytes = 128u * 128u;  // 128 rows x 64 fp16
 constexpr int kEpiWarps = 8;
 constexpr int kTcThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemCols = 512;
+constexpr uint32_t kEndOfBlock = 0xFFFFFFFFu;
 
 struct TcSmem {
   uint8_t a[2][kTileBytes];          // the query block's two operand tiles
   uint8_t b[kStages][kTileBytes];    // point tiles
   float scratch[kEpiWarps * 32][33]; // a thread's 32 keys when some may pass
+  float topk[kEpiWarps * 32][33];    // a thread's k smallest keys (k <= 32)
   uint64_t full[kStages], empty[kStages];
   uint64_t tmem_full[2], tmem_empty[2];
   uint64_t a_full, a_empty, drained;
+  uint32_t stage_tile[kStages];      // the point tile in a stage, or kEndOfBlock
+  uint32_t acc_tile[2];              // the point tile in an accumulator, or kEndOfBlock
+  float u_max[2][kEpiWarps];         // per block parity and epilogue warp: the largest
+                                     // threshold + s^2 |q|^2 of its queries
   uint32_t tmem_base;
   int abort;
 };
@@ -90,10 +96,27 @@ struct QueryState {
   bool overflowed;
 };
 
+// Compact the query's slice against its threshold (neighbors_exact.rs:236-252): out of
+// line, it runs once per doubling of the slice.
+__device__ __noinline__ void tc_compact(QueryState& st, float* ck, uint32_t* cr, uint32_t cap) {
+  uint32_t kept = 0;
+  for (uint32_t i = 0; i < st.count; ++i) {
+    float v = ck[i];
+    if (v <= st.th) {
+      ck[kept] = v;
+      cr[kept] = cr[i];
+      ++kept;
+    }
+  }
+  st.count = kept;
+  if (st.count > kTcCandidateLimit) st.overflowed = true;
+  st.compact_at = min(max(2 * st.count, 64u), cap);
+}
+
 // Append candidate (key, p) (already <= st.th) to the query's slice, compacting it
-// against the threshold when it reaches compact_at (neighbors_exact.rs:236-252).
-__device__ __noinline__ void tc_append(QueryState& st, float key, uint32_t p, float* ck,
-                                       uint32_t* cr, uint32_t cap) {
+// against the threshold when it reaches compact_at.
+__device__ __forceinline__ void tc_append(QueryState& st, float key, uint32_t p, float* ck,
+                                          uint32_t* cr, uint32_t cap) {
   if (st.count == cap) {
     st.overflowed = true;
     return;
@@ -101,20 +124,7 @@ __device__ __noinline__ void tc_append(QueryState& st, float key, uint32_t p, fl
   ck[st.count] = key;
   cr[st.count] = p;
   ++st.count;
-  if (st.count >= st.compact_at) {
-    uint32_t kept = 0;
-    for (uint32_t i = 0; i < st.count; ++i) {
-      float v = ck[i];
-      if (v <= st.th) {
-        ck[kept] = v;
-        cr[kept] = cr[i];
-        ++kept;
-      }
-    }
-    st.count = kept;
-    if (st.count > kTcCandidateLimit) st.overflowed = true;
-    st.compact_at = min(max(2 * st.count, 64u), cap);
-  }
+  if (st.count >= st.compact_at) tc_compact(st, ck, cr, cap);
 }
 
 // Offer approximate key `key` of point `p` (already <= st.th) to the query's state: its
@@ -136,34 +146,80 @@ __device__ __noinline__ void tc_offer(QueryState& st, float* smallest, uint32_t 
 }
 
 // Offer the keys of one 32-point chunk selected by `mask` (bit j: point p0 + j, key
-// keys[j]), in column order, to the query's state. Out of line: the filter's hot loop
-// keeps only the threshold in registers and spends nothing on this rare path's state.
-__device__ __noinline__ void tc_offer_chunk(QueryState& st, float* smallest, uint32_t k,
-                                            double slack2, const float* keys, uint32_t mask,
-                                            uint64_t p0, uint64_t q, uint64_t n, float* ck,
-                                            uint32_t* cr, uint32_t cap) {
-  while (mask && !st.overflowed) {
-    const int j = __ffs(mask) - 1;
-    mask &= mask - 1;
-    const float key = keys[j];
-    const uint64_t p = p0 + j;
-    if (key <= st.th && p < n && p != q) tc_offer(st, smallest, k, slack2, key, (uint32_t)p, ck, cr, cap);
+// keys[j]), in column order, to the query's state. For k <= KR the query's k smallest
+// keys (smallest[0..KR) in the thread's shared-memory slice, ascending, +inf past those
+// seen) move into registers for the chunk: an insertion is 2 KR branch-free min/max
+// (v[i] = max(v[i-1], min(v[i], key)) on the old values), no dependent memory access.
+// Inline: a call here would save and restore the epilogue's live registers each time.
+template <int KR>
+__device__ __forceinline__ void tc_offer_chunk(QueryState& st, float* smallest, uint32_t k,
+                                               double slack2, const float* keys, uint32_t mask,
+                                               uint64_t p0, uint64_t q, uint64_t n, float* ck,
+                                               uint32_t* cr, uint32_t cap) {
+  if constexpr (KR == 0) {
+    while (mask && !st.overflowed) {
+      const int j = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const float key = keys[j];
+      const uint64_t p = p0 + j;
+      if (key <= st.th && p < n && p != q)
+        tc_offer(st, smallest, k, slack2, key, (uint32_t)p, ck, cr, cap);
+    }
+  } else {
+    float v[KR];
+#pragma unroll
+    for (int i = 0; i < KR; ++i) v[i] = smallest[i];
+    float kth = v[0];
+#pragma unroll
+    for (int i = 1; i < KR; ++i) kth = (i == (int)k - 1) ? v[i] : kth;
+    bool changed = false;
+    while (mask && !st.overflowed) {
+      const int j = __ffs(mask) - 1;
+      mask &= mask - 1;
+      const float key = keys[j];
+      const uint64_t p = p0 + j;
+      if (!(key <= st.th) || p >= n || p == q) continue;
+      if (key < kth) {
+        float prev = v[0];
+        v[0] = fminf(v[0], key);
+#pragma unroll
+        for (int i = 1; i < KR; ++i) {
+          const float cur = v[i];
+          v[i] = fmaxf(prev, fminf(cur, key));
+          prev = cur;
+        }
+        kth = v[0];
+#pragma unroll
+        for (int i = 1; i < KR; ++i) kth = (i == (int)k - 1) ? v[i] : kth;
+        if (kth < INFINITY) st.th = round_up_f32d((double)kth + slack2);
+        changed = true;
+      }
+      if (key <= st.th) tc_append(st, key, (uint32_t)p, ck, cr, cap);
+    }
+    if (changed) {
+#pragma unroll
+      for (int i = 0; i < KR; ++i) smallest[i] = v[i];
+    }
   }
 }
 
+// KR: the register top-k width used on offers (k <= KR), or 0 for any k.
+template <int KR>
 __global__ void __launch_bounds__(kTcThreads, 1)
 knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
-                     const __grid_constant__ CUtensorMap tmap_p, uint64_t n, uint32_t k,
+                     const __grid_constant__ CUtensorMap tmap_p, FilterScan scan, uint32_t k,
                      const float* __restrict__ slack2, uint32_t idesc, uint32_t cap,
                      float* cand_key, uint32_t* cand_row, uint32_t* cand_count,
                      float* threshold_out, int* error) {
   extern __shared__ uint8_t smem_raw[];
-  TcSmem& sm = *reinterpret_cast<TcSmem*>(
-      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  // Aligned to 1024 bytes by an offset into the __shared__ array itself, so the compiler
+  // keeps every access in the shared state space (no generic loads and stores).
+  TcSmem& sm = *reinterpret_cast<TcSmem*>(smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u));
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  const uint64_t n_qblocks = (n + kTcQueries - 1) / kTcQueries;
-  const uint32_t n_tiles = (uint32_t)((n + kTcPoints - 1) / kTcPoints);
+  const uint64_t n_q = scan.n_q, n_p = scan.n_p;
+  const uint64_t n_qblocks = (n_q + kTcQueries - 1) / kTcQueries;
+  const uint32_t n_tiles = (uint32_t)((n_p + kTcPoints - 1) / kTcPoints);
   volatile int* abort = &sm.abort;
 
   if (threadIdx.x == 0) {
@@ -172,7 +228,8 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
       mbar_init(&sm.empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
-      mbar_init(&sm.tmem_full[b], 1);
+      // Two arrivals: the MMA thread's own (releasing acc_tile) and the MMAs' commit.
+      mbar_init(&sm.tmem_full[b], 2);
       mbar_init(&sm.tmem_empty[b], kEpiWarps);
     }
     mbar_init(&sm.a_full, 1);
@@ -186,38 +243,88 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = sm.tmem_base;
+  volatile float* u_max = &sm.u_max[0][0];
 
   if (warp == kEpiWarps) {
     // ------------------------------------------------------------ TMA producer ----
+    // Per query block: the two query tiles, then the block's point tiles in list order
+    // (or every tile, from the block's own), then an end marker. With bounds, a tile
+    // whose bound exceeds every query's threshold + s^2 |q|^2 is skipped (it holds no
+    // neighbour: the thresholds only fall). Lane 0 issues; the warp reads the list 32
+    // entries at a time ahead of it.
     if (lane == 0) {
       prefetch_tmap(&tmap_q);
       prefetch_tmap(&tmap_p);
-      uint64_t it = 0;
-      uint32_t bi = 0;
-      int issued_phase[kStages];
-      for (int s = 0; s < kStages; ++s) issued_phase[s] = -1;
-      bool ok = true;
-      for (uint64_t qb = blockIdx.x; qb < n_qblocks && ok; qb += gridDim.x, ++bi) {
-        if (!mbar_wait(&sm.a_empty, (bi & 1) ^ 1, abort)) break;
-        mbar_arrive_expect_tx(&sm.a_full, 2 * kTileBytes);
-        tma_load_2d(sm.a[0], &tmap_q, &sm.a_full, 0, (int32_t)(qb * kTcQueries));
-        tma_load_2d(sm.a[1], &tmap_q, &sm.a_full, 0, (int32_t)(qb * kTcQueries + 128));
-        for (uint32_t t = 0; t < n_tiles; ++t, ++it) {
-          int s = (int)(it % kStages);
-          uint32_t ph = (uint32_t)((it / kStages) & 1);
-          if (!mbar_wait(&sm.empty[s], ph ^ 1, abort)) {
-            ok = false;
-            break;
-          }
-          mbar_arrive_expect_tx(&sm.full[s], kTileBytes);
-          // The scan starts at the query block's own tiles: with the rows in a spatial
-          // order the nearest points come first and the threshold falls at once.
-          const uint32_t pt = (uint32_t)((t + qb * (kTcQueries / kTcPoints)) % n_tiles);
-          tma_load_2d(sm.b[s], &tmap_p, &sm.full[s], 0, (int32_t)(pt * kTcPoints));
-          issued_phase[s] = (int)ph;
+    }
+    uint64_t it = 0;
+    uint32_t bi = 0;
+    int issued_phase[kStages];
+    for (int s = 0; s < kStages; ++s) issued_phase[s] = -1;
+    bool ok = true;
+    for (uint64_t qb = blockIdx.x; qb < n_qblocks && ok; qb += gridDim.x, ++bi) {
+      if (lane == 0) {
+        ok = mbar_wait(&sm.a_empty, (bi & 1) ^ 1, abort);
+        if (ok) {
+          for (int w = 0; w < kEpiWarps; ++w) u_max[(bi & 1) * kEpiWarps + w] = INFINITY;
+          mbar_arrive_expect_tx(&sm.a_full, 2 * kTileBytes);
+          tma_load_2d(sm.a[0], &tmap_q, &sm.a_full, 0, (int32_t)(qb * kTcQueries));
+          tma_load_2d(sm.a[1], &tmap_q, &sm.a_full, 0, (int32_t)(qb * kTcQueries + 128));
         }
       }
-      // Every load issued has landed before the CTA may leave (bounded, own loop).
+      ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
+      if (!ok) break;
+      const uint64_t l0 = scan.list_off ? scan.list_off[qb] : qb * scan.list_stride;
+      const uint64_t len = !scan.list_tiles ? n_tiles
+                           : scan.list_off  ? scan.list_off[qb + 1] - l0
+                                            : scan.list_stride;
+      uint32_t win_tile = 0;
+      float win_lb2 = 0.0f;
+      for (uint64_t i = 0;; ++i) {
+        const uint32_t at = (uint32_t)(i & 31);
+        if (at == 0 && scan.list_tiles) {
+          win_tile = i + lane < len ? scan.list_tiles[l0 + i + lane] : 0u;
+          win_lb2 = (scan.list_lb2 && i + lane < len) ? scan.list_lb2[l0 + i + lane] : 0.0f;
+        }
+        const uint32_t lt = __shfl_sync(0xFFFFFFFFu, win_tile, at);
+        const float lb2 = __shfl_sync(0xFFFFFFFFu, win_lb2, at);
+        if (i < len && scan.list_lb2) {
+          float u = u_max[(bi & 1) * kEpiWarps];
+          for (int w = 1; w < kEpiWarps; ++w) u = fmaxf(u, u_max[(bi & 1) * kEpiWarps + w]);
+          if (lb2 > u) continue;
+        }
+        bool end = false;
+        if (lane == 0) {
+          const int s = (int)(it % kStages);
+          const uint32_t ph = (uint32_t)((it / kStages) & 1);
+          if (!mbar_wait(&sm.empty[s], ph ^ 1, abort)) {
+            ok = false;
+          } else {
+            end = i >= len;
+            if (end) {
+              sm.stage_tile[s] = kEndOfBlock;
+              mbar_arrive(&sm.full[s]);
+              issued_phase[s] = (int)ph;  // the stage's last phase: complete at once
+            } else {
+              // Without a list the scan starts at the query block's own tiles: with the
+              // rows in a spatial order the nearest points come first.
+              const uint32_t pt = scan.list_tiles
+                                      ? lt
+                                      : (uint32_t)((i + qb * (kTcQueries / kTcPoints)) % n_tiles);
+              sm.stage_tile[s] = pt;
+              mbar_arrive_expect_tx(&sm.full[s], kTileBytes);
+              tma_load_2d(sm.b[s], &tmap_p, &sm.full[s], 0, (int32_t)(pt * kTcPoints));
+              issued_phase[s] = (int)ph;
+            }
+          }
+        }
+        ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
+        end = __shfl_sync(0xFFFFFFFFu, end, 0);
+        ++it;
+        if (!ok || end) break;
+      }
+    }
+    // Every load issued has landed before the CTA may leave (bounded, own loop).
+    if (lane == 0) {
       for (int s = 0; s < kStages; ++s) {
         if (issued_phase[s] < 0) continue;
         for (uint32_t i = 0; i < kWaitPolls && !mbar_try_wait(&sm.full[s], issued_phase[s]); ++i)
@@ -234,16 +341,25 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
       for (uint64_t qb = blockIdx.x; qb < n_qblocks && ok; qb += gridDim.x, ++bi) {
         if (!mbar_wait(&sm.a_full, bi & 1, abort)) break;
         tc_fence_after();
-        for (uint32_t t = 0; t < n_tiles; ++t, ++it) {
-          int s = (int)(it % kStages);
-          uint32_t ph = (uint32_t)((it / kStages) & 1);
-          uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
+        for (;; ++it) {
+          const int s = (int)(it % kStages);
+          const uint32_t ph = (uint32_t)((it / kStages) & 1);
+          const uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
           if (!mbar_wait(&sm.tmem_empty[ab], aph ^ 1, abort) ||
               !mbar_wait(&sm.full[s], ph, abort)) {
             ok = false;
             break;
           }
           tc_fence_after();
+          const uint32_t pt = sm.stage_tile[s];
+          sm.acc_tile[ab] = pt;
+          if (pt == kEndOfBlock) {
+            mbar_arrive(&sm.empty[s]);
+            mbar_arrive(&sm.tmem_full[ab]);
+            mbar_arrive(&sm.tmem_full[ab]);
+            ++it;
+            break;
+          }
           const uint32_t bsm = smem_addr(sm.b[s]);
           const uint32_t d0 = tmem + ab * 256u, d1 = d0 + 128u;
 #pragma unroll
@@ -253,6 +369,7 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
             mma_f16(d1, desc_k_sw128(a1 + kk * 32), bd, idesc, kk > 0);
           }
           mma_commit(&sm.empty[s]);
+          mbar_arrive(&sm.tmem_full[ab]);
           mma_commit(&sm.tmem_full[ab]);
         }
         if (ok) mma_commit(&sm.a_empty);
@@ -267,30 +384,43 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
     // minimum per 32-column chunk is kept (few registers: no spills in the hot loop).
     // A chunk whose minimum reaches the threshold (rare once it has fallen) is read
     // again by the whole warp (tcgen05.ld is warp-wide) and its passing keys offered.
-    // The threshold and overflow flag stay in registers; the rest of the state is
-    // touched only on offers.
+    // The threshold and overflow flag stay in registers; after offers the warp
+    // publishes its largest threshold + s^2 |q|^2 for the producer's bound checks.
     const uint32_t half = (uint32_t)warp >> 2, quad = (uint32_t)warp & 3;
     float* my = sm.scratch[threadIdx.x];
-    float smallest[kMaxK];
+    float local_smallest[KR == 0 ? kMaxK : 1];
+    float* smallest = KR == 0 ? local_smallest : sm.topk[threadIdx.x];
     uint64_t it = 0;
+    uint32_t bi = 0;
     bool ok = true;
-    for (uint64_t qb = blockIdx.x; qb < n_qblocks && ok; qb += gridDim.x) {
+    for (uint64_t qb = blockIdx.x; qb < n_qblocks && ok; qb += gridDim.x, ++bi) {
       const uint64_t q = qb * kTcQueries + half * 128 + quad * 32 + lane;
-      const bool active = q < n;
+      const bool active = q < n_q;
+      const uint64_t self = active ? (scan.q_point ? scan.q_point[q] : q) : ~0ull;
+      const double s2qn2 = active && scan.qn2 ? scan.s2 * scan.qn2[q] : 0.0;
       QueryState st{INFINITY, 0, 0, 64, false};
+      if (KR > 0)
+        for (int i = 0; i < KR; ++i) smallest[i] = INFINITY;
       float th = INFINITY;
       bool live = active;  // not overflowed
       const double sl2 = active ? (double)slack2[q] : 0.0;
       float* ck = cand_key + (active ? q : 0) * (uint64_t)cap;
       uint32_t* cr = cand_row + (active ? q : 0) * (uint64_t)cap;
-      for (uint32_t t = 0; t < n_tiles; ++t, ++it) {
-        uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
+      for (;; ++it) {
+        const uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
         if (!mbar_wait(&sm.tmem_full[ab], aph, abort)) {
           ok = false;
           break;
         }
         tc_fence_after();
         __syncwarp();
+        const uint32_t pt = sm.acc_tile[ab];
+        if (pt == kEndOfBlock) {
+          __syncwarp();
+          if (lane == 0) mbar_arrive(&sm.tmem_empty[ab]);
+          ++it;
+          break;
+        }
         const uint32_t base = tmem + ((quad * 32u) << 16) + ab * 256u + half * 128u;
         float mins[kTcPoints / 32];
 #pragma unroll
@@ -306,6 +436,7 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
 #pragma unroll
         for (int c = 0; c < kTcPoints / 32; ++c) hits |= (live && mins[c] <= th ? 1u : 0u) << c;
         uint32_t any = __reduce_or_sync(0xFFFFFFFFu, hits);
+        const bool offered = any != 0;
 #pragma unroll 1
         while (any) {
           const int c = __ffs(any) - 1;
@@ -323,15 +454,22 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
             my[j] = key;
             mask |= (key <= th ? 1u : 0u) << j;
           }
-          const uint32_t pt = (uint32_t)((t + qb * (kTcQueries / kTcPoints)) % n_tiles);
           const uint64_t p0 = (uint64_t)pt * kTcPoints + c * 32;
-          tc_offer_chunk(st, smallest, k, sl2, my, mask, p0, q, n, ck, cr, cap);
+          st.th = th;
+          tc_offer_chunk<KR>(st, smallest, k, sl2, my, mask, p0, self, n_p, ck, cr, cap);
           th = st.th;
           live = !st.overflowed;
         }
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.tmem_empty[ab]);
+        if (offered && scan.list_lb2) {
+          // An overflowed query is searched in full later: it no longer bounds the scan.
+          const float u = active && live ? round_up_f32d((double)th + s2qn2) : -INFINITY;
+          float um = u;
+          for (int o = 16; o; o >>= 1) um = fmaxf(um, __shfl_xor_sync(0xFFFFFFFFu, um, o));
+          if (lane == 0) u_max[(bi & 1) * kEpiWarps + warp] = um;
+        }
       }
       if (active && ok) {
         cand_count[q] = st.overflowed ? kOverflow : st.count;
@@ -350,44 +488,47 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
 
 // ------------------------------------------------------------------ operands -------
 
-// Rows centred (f64) and scaled by 2^e: the query operand [-2 q, 1, 1, 1, 0...] and the
-// point operand [p, h1, h2, h3, 0...] (fp16 or bf16), each row's centred squared norm
-// (unscaled, f64) and the row's doubled slack in scaled units.
+// Rows centred (f64) and scaled by 2^e: the query operand [-2 q, 1, 1, 1, 0...] (with
+// each query's centred squared norm, unscaled, f64, and its doubled slack in scaled
+// units) or the point operand [p, h1, h2, h3, 0...] (fp16 or bf16). Slot r of the
+// operand is row rows[r] of x (or row r).
 template <class H>
 __global__ void tc_operands_kernel(const float* x, uint64_t n, uint32_t width, uint32_t d,
-                                   const uint32_t* perm, const double* mean, double scale,
-                                   double u, double eta, const double* max_sq, H* aq, H* bp,
-                                   double* qn2, float* slack2, double* slack_d) {
+                                   const uint32_t* rows, const double* mean, double scale,
+                                   double u, double eta, const double* max_sq, bool query,
+                                   H* out, double* qn2, float* slack2, double* slack_d) {
   uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (r >= n) return;
-  const float* xr = x + (uint64_t)(perm ? perm[r] : r) * width;
+  const float* xr = x + (uint64_t)(rows ? rows[r] : r) * width;
   double n2 = 0.0, n2s = 0.0;
   for (uint32_t j = 0; j < kTcK; ++j) {
-    H a = H(0.0f), b = H(0.0f);
+    H v = H(0.0f);
     if (j < d) {
       double c = (double)xr[j] - mean[j];
       double cs = c * scale;
       n2 += c * c;
       n2s += cs * cs;
-      b = H((float)cs);
-      a = H(-2.0f * (float)b);  // exact: a power-of-two multiple of a 16-bit value
+      const H b = H((float)cs);
+      v = query ? H(-2.0f * (float)b) : b;  // -2b: exact, a power-of-two multiple
     }
-    aq[r * kTcK + j] = a;
-    bp[r * kTcK + j] = b;
+    out[r * kTcK + j] = v;
   }
-  // The squared norm in three parts (each rounded from what the previous left).
-  double r1 = n2s;
-  H h1 = H((float)r1);
-  double r2 = r1 - (double)(float)h1;
-  H h2 = H((float)r2);
-  double r3 = r2 - (double)(float)h2;
-  H h3 = H((float)r3);
-  bp[r * kTcK + d] = h1;
-  bp[r * kTcK + d + 1] = h2;
-  bp[r * kTcK + d + 2] = h3;
-  aq[r * kTcK + d] = H(1.0f);
-  aq[r * kTcK + d + 1] = H(1.0f);
-  aq[r * kTcK + d + 2] = H(1.0f);
+  if (!query) {
+    // The squared norm in three parts (each rounded from what the previous left).
+    double r1 = n2s;
+    H h1 = H((float)r1);
+    double r2 = r1 - (double)(float)h1;
+    H h2 = H((float)r2);
+    double r3 = r2 - (double)(float)h2;
+    H h3 = H((float)r3);
+    out[r * kTcK + d] = h1;
+    out[r * kTcK + d + 1] = h2;
+    out[r * kTcK + d + 2] = h3;
+    return;
+  }
+  out[r * kTcK + d] = H(1.0f);
+  out[r * kTcK + d + 1] = H(1.0f);
+  out[r * kTcK + d + 2] = H(1.0f);
   qn2[r] = n2;
   // The bound of |A - s^2 (D - |q|^2)| (scaled units), D the exact squared distance:
   // quantisation 2(2u + u^2)|q||p| + 2 eta sqrt(d)(|q| + |p|) + 2 d eta^2, the norm's
@@ -456,18 +597,15 @@ CUtensorMap tile_map(const void* base, uint64_t rows, bool bf16) {
 
 }  // namespace
 
-void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint64_t n, uint32_t width,
-               uint32_t d, const uint32_t* perm, const double* mean, bool bf16, uint32_t k,
-               uint32_t cap,
-               float* cand_key, uint32_t* cand_row, uint32_t* cand_count, float* threshold,
-               double* qn2, double* slack_d, double* out_scale) {
+double tc_scale(const float* x, uint64_t n, uint32_t width, uint32_t d, const double* mean,
+                double* max_sq, cudaStream_t s) {
   if (d + 3 > (uint32_t)kTcK) fail(KG_ERR_INVALID, "tensor-core filter: more than 61 components");
-  DeviceBuffer<double> sq(n, s), max_sq(1, s);
+  DeviceBuffer<double> sq(n, s);
   centred_norm_kernel<<<blocks_for(n, 256), 256, 0, s>>>(x, n, width, d, mean, sq.ptr);
   KG_LAUNCH_CHECK();
-  max_kernel_launch(sq.ptr, n, max_sq.ptr, s);
+  max_kernel_launch(sq.ptr, n, max_sq, s);
   double h_max = 0.0;
-  KG_CUDA(cudaMemcpyAsync(&h_max, max_sq.ptr, 8, cudaMemcpyDeviceToHost, s));
+  KG_CUDA(cudaMemcpyAsync(&h_max, max_sq, 8, cudaMemcpyDeviceToHost, s));
   KG_CUDA(cudaStreamSynchronize(s));
   // Scale so that the largest centred row norm is at most 2^7: squared norms stay below
   // 2^14 (fp16's range) and -2q below 2^8.
@@ -478,34 +616,60 @@ void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint64_t n, uint32_t
     int shift = std::max(-1000, std::min(1000, 7 - e));
     scale = std::ldexp(1.0, shift);
   }
-  *out_scale = scale;
+  return scale;
+}
+
+void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint32_t width, uint32_t d,
+               const uint32_t* qrows, const uint32_t* prows, FilterScan scan,
+               const double* mean, double scale, const double* max_sq, bool bf16, uint32_t k,
+               uint32_t cap, float* cand_key, uint32_t* cand_row, uint32_t* cand_count,
+               float* threshold, double* qn2, double* slack_d, Trace* trace) {
+  if (d + 3 > (uint32_t)kTcK) fail(KG_ERR_INVALID, "tensor-core filter: more than 61 components");
+  const uint64_t n_q = scan.n_q, n_p = scan.n_p;
   const double u = bf16 ? 0x1p-8 : 0x1p-11;
   const double eta = bf16 ? 0x1p-134 : 0x1p-25;
-  DeviceBuffer<uint16_t> aq(n * kTcK, s), bp(n * kTcK, s);
-  DeviceBuffer<float> slack2(n, s);
-  if (bf16)
-    tc_operands_kernel<__nv_bfloat16><<<blocks_for(n, 128), 128, 0, s>>>(
-        x, n, width, d, perm, mean, scale, u, eta, max_sq.ptr, (__nv_bfloat16*)aq.ptr,
-        (__nv_bfloat16*)bp.ptr, qn2, slack2.ptr, slack_d);
-  else
-    tc_operands_kernel<__half><<<blocks_for(n, 128), 128, 0, s>>>(
-        x, n, width, d, perm, mean, scale, u, eta, max_sq.ptr, (__half*)aq.ptr, (__half*)bp.ptr,
-        qn2, slack2.ptr, slack_d);
+  DeviceBuffer<uint16_t> aq(n_q * kTcK, s), bp(n_p * kTcK, s);
+  DeviceBuffer<float> slack2(n_q, s);
+  if (bf16) {
+    tc_operands_kernel<__nv_bfloat16><<<blocks_for(n_q, 128), 128, 0, s>>>(
+        x, n_q, width, d, qrows, mean, scale, u, eta, max_sq, true, (__nv_bfloat16*)aq.ptr, qn2,
+        slack2.ptr, slack_d);
+    tc_operands_kernel<__nv_bfloat16><<<blocks_for(n_p, 128), 128, 0, s>>>(
+        x, n_p, width, d, prows, mean, scale, u, eta, max_sq, false, (__nv_bfloat16*)bp.ptr,
+        nullptr, nullptr, nullptr);
+  } else {
+    tc_operands_kernel<__half><<<blocks_for(n_q, 128), 128, 0, s>>>(
+        x, n_q, width, d, qrows, mean, scale, u, eta, max_sq, true, (__half*)aq.ptr, qn2,
+        slack2.ptr, slack_d);
+    tc_operands_kernel<__half><<<blocks_for(n_p, 128), 128, 0, s>>>(
+        x, n_p, width, d, prows, mean, scale, u, eta, max_sq, false, (__half*)bp.ptr, nullptr,
+        nullptr, nullptr);
+  }
   KG_LAUNCH_CHECK();
-  CUtensorMap mq = tile_map(aq.ptr, n, bf16), mp = tile_map(bp.ptr, n, bf16);
+  if (trace) trace->mark("filter operands");
+  CUtensorMap mq = tile_map(aq.ptr, n_q, bf16), mp = tile_map(bp.ptr, n_p, bf16);
   static std::once_flag attr;
   std::call_once(attr, [] {
-    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)kTcSmemBytes));
+    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<16>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes));
+    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<32>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes));
+    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<0>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes));
   });
   DeviceBuffer<int> err(1, s);
   err.zero();
-  uint64_t n_qblocks = (n + kTcQueries - 1) / kTcQueries;
+  scan.qn2 = qn2;
+  scan.s2 = scale * scale;
+  uint64_t n_qblocks = (n_q + kTcQueries - 1) / kTcQueries;
   unsigned grid = (unsigned)std::min<uint64_t>(n_qblocks, (uint64_t)ctx->sm_count);
   uint32_t idesc = idesc_f32acc(bf16 ? 1u : 0u, 128, kTcPoints);
-  knn_filter_tc_kernel<<<grid, kTcThreads, kTcSmemBytes, s>>>(mq, mp, n, k, slack2.ptr, idesc, cap, cand_key,
+  auto kernel = k <= 16 ? knn_filter_tc_kernel<16>
+                : k <= 32 ? knn_filter_tc_kernel<32> : knn_filter_tc_kernel<0>;
+  kernel<<<grid, kTcThreads, kTcSmemBytes, s>>>(mq, mp, scan, k, slack2.ptr, idesc, cap, cand_key,
                                                 cand_row, cand_count, threshold, err.ptr);
   KG_LAUNCH_CHECK();
+  if (trace) trace->mark("filter kernel");
   int h_err = 0;
   KG_CUDA(cudaMemcpyAsync(&h_err, err.ptr, 4, cudaMemcpyDeviceToHost, s));
   wait_stream(ctx, s);

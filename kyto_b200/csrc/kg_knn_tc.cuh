@@ -9,17 +9,40 @@ namespace kg {
 
 constexpr uint32_t kTcCap = 512;             // candidate slots per query
 constexpr uint32_t kTcCandidateLimit = 256;  // candidates kept after a compaction, at most
+constexpr uint32_t kTcQueryBlock = 256;      // query slots per block of the filter
 
-// Fills cand_key/cand_row (n x cap), cand_count and threshold (n) for every query, and
-// per row qn2 (the centred squared norm) and slack_d (the bound of |approximate -
-// exact| key in squared-distance units). Keys are in units scaled by out_scale^2:
-// the approximate squared distance is key / out_scale^2 + qn2.
-// perm: the rows in scan order (row i of the operands is row perm[i] of x), or NULL.
-void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint64_t n, uint32_t width,
-               uint32_t d, const uint32_t* perm, const double* mean, bool bf16, uint32_t k,
-               uint32_t cap,
-               float* cand_key, uint32_t* cand_row, uint32_t* cand_count, float* threshold,
-               double* qn2, double* slack_d, double* out_scale);
+// What one filter launch scans. Query slot q is row qrows[q] of x, point slot p row
+// prows[p]; each block of 256 query slots scans its list of point tiles (128 slots) in
+// order, or every tile from its own when list_tiles is NULL, skipping a listed tile whose
+// bound (list_lb2, scaled squared distance) exceeds every query's threshold + s^2 |q|^2.
+struct FilterScan {
+  uint64_t n_q = 0, n_p = 0;
+  const uint32_t* q_point = nullptr;     // query slot -> point slot of the same row (NULL:
+                                         // the same slot)
+  const uint32_t* list_tiles = nullptr;  // the blocks' tile lists
+  const float* list_lb2 = nullptr;       // their bounds (or NULL: none skipped)
+  const uint64_t* list_off = nullptr;    // block qb's entries start at list_off[qb] and end
+                                         // at list_off[qb + 1] (or NULL: qb * list_stride,
+                                         // list_stride entries each)
+  uint64_t list_stride = 0;
+  const double* qn2 = nullptr;           // per query slot |q - mean|^2 (set by tc_filter)
+  double s2 = 1.0;                       // scale^2 (set by tc_filter)
+};
+
+// The power-of-two scale of the filter's operands (the largest centred row norm of x's
+// n rows scaled to at most 2^7), and that largest squared norm on the device (max_sq).
+double tc_scale(const float* x, uint64_t n, uint32_t width, uint32_t d, const double* mean,
+                double* max_sq, cudaStream_t s);
+
+// Fills cand_key/cand_row (n_q x cap), cand_count and threshold (n_q) for every query
+// slot, and per query slot qn2 (the centred squared norm) and slack_d (the bound of
+// |approximate - exact| key in squared-distance units). Keys are in units scaled by
+// scale^2: the approximate squared distance is key / scale^2 + qn2.
+void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint32_t width, uint32_t d,
+               const uint32_t* qrows, const uint32_t* prows, FilterScan scan,
+               const double* mean, double scale, const double* max_sq, bool bf16, uint32_t k,
+               uint32_t cap, float* cand_key, uint32_t* cand_row, uint32_t* cand_count,
+               float* threshold, double* qn2, double* slack_d, Trace* trace = nullptr);
 
 void max_kernel_launch(const double* v, uint64_t n, double* out, cudaStream_t s);
 

@@ -1,0 +1,471 @@
+// Learned-partition kNN: a BF16 MLP (kg_mlp.cuh) trained on the exact kNN graph of a
+// sample of the rows proposes, for every row, the partitions to search; the search is
+// the exact kNN's tensor-core filter and exact re-rank restricted to those partitions'
+// points, and every row whose proposal is not confident enough is searched against
+// every row. kyto has no learned partitioner: this is the north star's learned form.
+//
+//   1. sample: m evenly strided rows; their exact graph (the exact search itself);
+//   2. partitions: k-means of the sample into P parts (kg_cluster.cuh);
+//   3. training: soft targets = the parts of a row and of its k neighbours, soft-target
+//      cross-entropy, Adam, `epochs` passes of seeded shuffles;
+//   4. index: the network's top-`probe` parts for every row (their summed softmax is the
+//      confidence), each row stored in its top part;
+//   5. search: query slots sorted by (fallback, top part); each block of 256 query slots
+//      scans the tiles of the union of its queries' probed parts (every tile if one of
+//      them falls back), then the exact re-rank.
+#include <cuda_bf16.h>
+#include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <vector>
+
+#include "kg_cluster.cuh"
+#include "kg_internal.cuh"
+#include "kg_knn.cuh"
+#include "kg_knn_tc.cuh"
+#include "kg_mlp.cuh"
+
+namespace kg {
+
+namespace {
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void strided_rows_kernel(const float* x, uint64_t n, uint32_t width, uint32_t d,
+                                    uint64_t m, float* out) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= m * d) return;
+  const uint64_t r = i / d, j = i % d;
+  const uint64_t row = r * n / m;
+  out[r * d + j] = x[row * width + j];
+}
+
+// labels[i * L + 0] = part of row i, then the parts of its k neighbours (L = k + 1).
+__global__ void target_labels_kernel(const uint32_t* part, const uint32_t* nbr, uint64_t m,
+                                     uint32_t k, uint32_t* labels) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const uint32_t L = k + 1;
+  labels[i * L] = part[i];
+  for (uint32_t j = 0; j < k; ++j) labels[i * L + 1 + j] = part[nbr[i * k + j]];
+}
+
+__global__ void shuffle_keys_kernel(uint64_t m, uint64_t seed, uint32_t epoch,
+                                    unsigned long long* key, uint32_t* idx) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  key[i] = mix64(seed * 0x9E3779B97F4A7C15ull + ((uint64_t)epoch << 40) + i);
+  idx[i] = (uint32_t)i;
+}
+
+// The batch: rows order[b0 + r] of the sample and their labels.
+__global__ void gather_batch_kernel(const float* xs, uint32_t d, const uint32_t* labels,
+                                    uint32_t L, const uint32_t* order, uint64_t b0, uint32_t rows,
+                                    float* xb, uint32_t* lb) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  const uint64_t w = d > L ? d : L;
+  if (i >= (uint64_t)rows * w) return;
+  const uint64_t r = i / w, j = i % w;
+  const uint64_t src = order[b0 + r];
+  if (j < d) xb[r * d + j] = xs[src * d + j];
+  if (j < L) lb[r * L + j] = labels[src * L + j];
+}
+
+// key = (fallback, top part) for the query order; iota payload.
+__global__ void query_key_kernel(const uint32_t* top, const float* conf, uint64_t n,
+                                 uint32_t probe, float threshold, uint32_t parts, uint32_t* key,
+                                 uint32_t* iota, uint8_t* fallback) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const bool fb = !(conf[r] >= threshold);
+  fallback[r] = fb ? 1 : 0;
+  key[r] = fb ? parts : top[r * probe];
+  iota[r] = (uint32_t)r;
+}
+
+__global__ void point_key_kernel(const uint32_t* top, uint64_t n, uint32_t probe, uint32_t* key,
+                                 uint32_t* iota) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  key[r] = top[r * probe];
+  iota[r] = (uint32_t)r;
+}
+
+__global__ void inverse_kernel(const uint32_t* perm, uint64_t n, uint32_t* inv) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) inv[perm[i]] = (uint32_t)i;
+}
+
+__global__ void compose_kernel(const uint32_t* qrows, const uint32_t* slot_of_row, uint64_t n,
+                               uint32_t* q_point) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) q_point[i] = slot_of_row[qrows[i]];
+}
+
+__global__ void part_starts_kernel(const uint32_t* sorted, uint64_t n, uint32_t parts,
+                                   uint32_t* starts) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > parts) return;
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (sorted[mid] < c) lo = mid + 1; else hi = mid;
+  }
+  starts[c] = (uint32_t)lo;
+}
+
+constexpr uint32_t kProbeThreads = 256;
+
+// One CTA per block of query slots: the tiles of the union of its queries' probed parts
+// (a bitmap over tiles), or every tile when one of them falls back. Count pass (list
+// NULL): the number of tiles into len[B]; fill pass: the tiles in increasing order at
+// list + off[B].
+__global__ void __launch_bounds__(kProbeThreads)
+probe_tiles_kernel(const uint32_t* qrows, uint64_t n, const uint32_t* top, uint32_t probe,
+                   const uint8_t* fallback, const uint32_t* part_start, uint32_t n_tiles,
+                   uint32_t block, uint64_t* len, const uint64_t* off, uint32_t* list) {
+  extern __shared__ uint32_t bits[];  // n_tiles bits
+  __shared__ int any_fallback;
+  __shared__ uint32_t word_base[kProbeThreads + 1];
+  const uint32_t words = (n_tiles + 31) / 32;
+  for (uint32_t w = threadIdx.x; w < words; w += kProbeThreads) bits[w] = 0;
+  if (threadIdx.x == 0) any_fallback = 0;
+  __syncthreads();
+  const uint64_t q0 = blockIdx.x * (uint64_t)block;
+  for (uint32_t i = threadIdx.x; i < block; i += kProbeThreads) {
+    const uint64_t q = q0 + i;
+    if (q >= n) break;
+    const uint32_t row = qrows[q];
+    if (fallback[row]) {
+      any_fallback = 1;
+      continue;
+    }
+    for (uint32_t t = 0; t < probe; ++t) {
+      const uint32_t p = top[(uint64_t)row * probe + t];
+      const uint32_t a = part_start[p], e = part_start[p + 1];
+      if (a == e) continue;
+      for (uint32_t tile = a >> 7; tile <= (e - 1) >> 7; ++tile)
+        atomicOr(&bits[tile >> 5], 1u << (tile & 31));
+    }
+  }
+  __syncthreads();
+  if (any_fallback) {
+    if (!list) {
+      if (threadIdx.x == 0) len[blockIdx.x] = n_tiles;
+      return;
+    }
+    for (uint32_t t = threadIdx.x; t < n_tiles; t += kProbeThreads) list[off[blockIdx.x] + t] = t;
+    return;
+  }
+  // Per thread a run of words, their popcounts scanned in thread order.
+  const uint32_t per = (words + kProbeThreads - 1) / kProbeThreads;
+  const uint32_t w0 = threadIdx.x * per, w1 = min(words, w0 + per);
+  uint32_t c = 0;
+  for (uint32_t w = w0; w < w1; ++w) c += __popc(bits[w]);
+  word_base[threadIdx.x] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0;
+    for (uint32_t t = 0; t < kProbeThreads; ++t) {
+      const uint32_t v = word_base[t];
+      word_base[t] = acc;
+      acc += v;
+    }
+    word_base[kProbeThreads] = acc;
+  }
+  __syncthreads();
+  if (!list) {
+    if (threadIdx.x == 0) len[blockIdx.x] = word_base[kProbeThreads];
+    return;
+  }
+  uint64_t at = off[blockIdx.x] + word_base[threadIdx.x];
+  for (uint32_t w = w0; w < w1; ++w) {
+    uint32_t b = bits[w];
+    while (b) {
+      const int j = __ffs(b) - 1;
+      b &= b - 1;
+      list[at++] = w * 32 + j;
+    }
+  }
+}
+
+void sort_u32_pairs(const uint32_t* key, const uint32_t* val, uint64_t n, int bits,
+                    DeviceBuffer<uint32_t>& key_out, DeviceBuffer<uint32_t>& val_out,
+                    cudaStream_t s) {
+  key_out.alloc(n, s);
+  val_out.alloc(n, s);
+  size_t temp = 0;
+  KG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, key, key_out.ptr, val, val_out.ptr,
+                                          (int)n, 0, bits, s));
+  DeviceBuffer<unsigned char> scratch(temp, s);
+  KG_CUDA(cub::DeviceRadixSort::SortPairs(scratch.ptr, temp, key, key_out.ptr, val, val_out.ptr,
+                                          (int)n, 0, bits, s));
+}
+
+int bits_for_value(uint64_t v) {
+  int b = 1;
+  while (b < 32 && (1ull << b) <= v) ++b;
+  return b;
+}
+
+// The network's top parts for n rows of x (chunks of 65,536 rows).
+void learned_probe(const Mlp& mlp, const float* x, uint64_t n, uint32_t width, uint32_t probe,
+                   uint32_t* top, float* conf, cudaStream_t s) {
+  const uint64_t chunk = 65536;
+  MlpBatch b;
+  b.alloc(mlp.sh, (uint32_t)std::min<uint64_t>(chunk, n), s);
+  for (uint64_t r0 = 0; r0 < n; r0 += chunk) {
+    const uint32_t rows = (uint32_t)std::min<uint64_t>(chunk, n - r0);
+    b.rows = rows;
+    mlp.forward(x + r0 * width, width, b, s);
+    top_parts(b.z3.ptr, rows, mlp.sh.parts, probe, top + r0 * probe, conf + r0, s);
+  }
+}
+
+}  // namespace
+
+}  // namespace kg
+
+using namespace kg;
+
+extern "C" {
+
+kg_status kg_learned_layout(uint32_t din, uint32_t hidden, uint32_t parts, uint64_t* offsets,
+                            uint64_t* total) {
+  return guarded([&] {
+    if (!offsets || !total) fail(KG_ERR_INVALID, "kg_learned_layout: NULL argument");
+    MlpShape sh;
+    sh.din = din;
+    sh.hidden = hidden;
+    sh.parts = parts;
+    sh.layout();
+    for (int l = 0; l < 3; ++l) {
+      offsets[2 * l] = sh.w_off[l];
+      offsets[2 * l + 1] = sh.b_off[l];
+    }
+    *total = sh.total;
+  });
+}
+
+kg_status kg_learned_gradients(kg_ctx* ctx, uint32_t din, uint32_t hidden, uint32_t parts,
+                               const float* params, const float* x, uint32_t rows,
+                               const uint32_t* labels, uint32_t n_labels, float* grads,
+                               float* row_loss, float* logits) {
+  return guarded([&] {
+    if (!ctx || !params || !x || !labels || !grads || !row_loss)
+      fail(KG_ERR_INVALID, "kg_learned_gradients: NULL argument");
+    if (!din || !hidden || !parts || !rows || !n_labels)
+      fail(KG_ERR_INVALID, "kg_learned_gradients: a zero size");
+    use_device(ctx);
+    cudaStream_t s = ctx->stream;
+    Mlp mlp;
+    mlp.init(din, hidden, parts, 0, s);
+    mlp.set_params(params, s);
+    DeviceBuffer<float> hx;
+    const float* dx = device_view(x, (uint64_t)rows * din, hx, s);
+    DeviceBuffer<uint32_t> hl;
+    const uint32_t* dl = device_view(labels, (uint64_t)rows * n_labels, hl, s);
+    MlpBatch b;
+    b.alloc(mlp.sh, rows, s);
+    mlp.forward(dx, din, b, s);
+    mlp.backward(dl, n_labels, b, s);
+    KG_CUDA(cudaMemcpyAsync(grads, mlp.grads.ptr, mlp.sh.total * 4, cudaMemcpyDefault, s));
+    KG_CUDA(cudaMemcpyAsync(row_loss, b.row_loss.ptr, (uint64_t)rows * 4, cudaMemcpyDefault, s));
+    if (logits)
+      KG_CUDA(cudaMemcpyAsync(logits, b.z3.ptr, (uint64_t)rows * parts * 4, cudaMemcpyDefault, s));
+    wait_stream(ctx, s);
+  });
+}
+
+kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32_t width,
+                         uint32_t n_components, uint32_t n_neighbors,
+                         const kg_learned_params* params, uint64_t* indptr, uint32_t* indices,
+                         float* distances, kg_learned_stats* stats) {
+  return guarded([&] {
+    if (!ctx || !embedding || !params || !indptr || !indices || !distances)
+      fail(KG_ERR_INVALID, "kg_knn_learned: NULL argument");
+    uint32_t k = 0, d = 0;
+    check_search_args(n, width, n_components, n_neighbors, k, d);
+    const kg_learned_params P = *params;
+    if (P.n_parts < 2 || P.n_parts > 65536)
+      fail(KG_ERR_INVALID, "kg_knn_learned: n_parts in 2..65536");
+    if (P.n_probe < 1 || P.n_probe > P.n_parts || P.n_probe > 64)
+      fail(KG_ERR_INVALID, "kg_knn_learned: n_probe in 1..min(64, n_parts)");
+    if (P.hidden < 1 || P.batch < 1 || !(P.learning_rate > 0.0f))
+      fail(KG_ERR_INVALID, "kg_knn_learned: hidden, batch and learning_rate must be positive");
+    if (d + 3 > 64) fail(KG_ERR_INVALID, "kg_knn_learned: more than 61 components");
+    use_device(ctx);
+    cudaStream_t s = ctx->stream;
+    ctx->total = n;
+    ctx->done = 0;
+    DeviceBuffer<float> hold;
+    const float* x = device_view(embedding, n * width, hold, s);
+    check_finite(x, n, width, d, s);
+    Trace trace(s, "knn_learned");
+    auto now = [] { return std::chrono::steady_clock::now(); };
+    auto ms_since = [&](std::chrono::steady_clock::time_point t) {
+      return std::chrono::duration<double, std::milli>(now() - t).count();
+    };
+    const uint32_t parts = P.n_parts, probe = P.n_probe, L = k + 1;
+
+    // 1-3. The sample, its exact graph, its parts, the network.
+    auto t_train = now();
+    const uint64_t m = std::max<uint64_t>(std::min<uint64_t>(P.train_cells ? P.train_cells : n, n),
+                                          std::min<uint64_t>(n, (uint64_t)n_neighbors + 1));
+    DeviceBuffer<float> xs(m * d, s);
+    strided_rows_kernel<<<blocks_for(m * d, 256), 256, 0, s>>>(x, n, width, d, m, xs.ptr);
+    KG_LAUNCH_CHECK();
+    KnnResult sg;
+    knn_core(ctx, xs.ptr, m, d, d, k, nullptr, sg, trace);
+    trace.mark("sample graph");
+    Clusters cl;
+    cluster_rows(xs.ptr, m, d, d, std::min<uint32_t>(parts, (uint32_t)m), 10, m, cl, s);
+    DeviceBuffer<uint32_t> labels(m * L, s);
+    target_labels_kernel<<<blocks_for(m, 256), 256, 0, s>>>(cl.label.ptr, sg.row.ptr, m, k,
+                                                            labels.ptr);
+    KG_LAUNCH_CHECK();
+    trace.mark("sample parts");
+    Mlp mlp;
+    mlp.init(d, P.hidden, parts, P.seed, s);
+    const uint32_t batch = (uint32_t)std::min<uint64_t>(P.batch, m);
+    MlpBatch b;
+    b.alloc(mlp.sh, batch, s);
+    DeviceBuffer<float> xb((uint64_t)batch * d, s);
+    DeviceBuffer<uint32_t> lb((uint64_t)batch * L, s);
+    DeviceBuffer<unsigned long long> skey(m, s), skey_sorted(m, s);
+    DeviceBuffer<uint32_t> sidx(m, s), order(m, s);
+    size_t temp = 0;
+    KG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, skey.ptr, skey_sorted.ptr, sidx.ptr,
+                                            order.ptr, (int)m, 0, 64, s));
+    DeviceBuffer<unsigned char> scratch(temp, s);
+    for (uint32_t e = 0; e < P.epochs; ++e) {
+      check_cancel(ctx);
+      shuffle_keys_kernel<<<blocks_for(m, 256), 256, 0, s>>>(m, P.seed, e, skey.ptr, sidx.ptr);
+      KG_LAUNCH_CHECK();
+      KG_CUDA(cub::DeviceRadixSort::SortPairs(scratch.ptr, temp, skey.ptr, skey_sorted.ptr,
+                                              sidx.ptr, order.ptr, (int)m, 0, 64, s));
+      for (uint64_t b0 = 0; b0 + batch <= m; b0 += batch) {
+        const uint64_t w = std::max(d, L);
+        gather_batch_kernel<<<blocks_for((uint64_t)batch * w, 256), 256, 0, s>>>(
+            xs.ptr, d, labels.ptr, L, order.ptr, b0, batch, xb.ptr, lb.ptr);
+        KG_LAUNCH_CHECK();
+        mlp.forward(xb.ptr, d, b, s);
+        mlp.backward(lb.ptr, L, b, s);
+        mlp.adam(P.learning_rate, s);
+      }
+    }
+    float final_loss = NAN;
+    if (P.epochs) {
+      std::vector<float> rl(batch);
+      KG_CUDA(cudaMemcpyAsync(rl.data(), b.row_loss.ptr, batch * 4ull, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaStreamSynchronize(s));
+      double acc = 0.0;
+      for (float v : rl) acc += v;
+      final_loss = (float)(acc / batch);
+    }
+    KG_CUDA(cudaStreamSynchronize(s));
+    const double train_ms = ms_since(t_train);
+    trace.mark("training");
+
+    // 4. Every row's parts.
+    auto t_index = now();
+    DeviceBuffer<uint32_t> top(n * probe, s);
+    DeviceBuffer<float> conf(n, s);
+    learned_probe(mlp, x, n, width, probe, top.ptr, conf.ptr, s);
+    KG_CUDA(cudaStreamSynchronize(s));
+    const double index_ms = ms_since(t_index);
+    trace.mark("index");
+
+    // 5. The restricted exact search.
+    auto t_search = now();
+    uint64_t fallback_rows = 0, scanned_tiles = 0;
+    PlanBuilder plan = [&](const float*, uint64_t nn, uint32_t, uint32_t, double, ScanPlan& sp,
+                           Trace& tr) {
+      DeviceBuffer<uint32_t> key(nn, s), iota(nn, s), key_sorted;
+      DeviceBuffer<uint8_t> fallback(nn, s);
+      // Points: by top part.
+      point_key_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(top.ptr, nn, probe, key.ptr, iota.ptr);
+      KG_LAUNCH_CHECK();
+      sort_u32_pairs(key.ptr, iota.ptr, nn, bits_for_value(parts), key_sorted, sp.prows, s);
+      DeviceBuffer<uint32_t> part_start((uint64_t)parts + 1, s);
+      part_starts_kernel<<<blocks_for((uint64_t)parts + 1, 256), 256, 0, s>>>(
+          key_sorted.ptr, nn, parts, part_start.ptr);
+      KG_LAUNCH_CHECK();
+      DeviceBuffer<uint32_t> slot_of_row(nn, s);
+      inverse_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(sp.prows.ptr, nn, slot_of_row.ptr);
+      KG_LAUNCH_CHECK();
+      // Queries: by (fallback, top part).
+      query_key_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(top.ptr, conf.ptr, nn, probe,
+                                                           P.confidence, parts, key.ptr, iota.ptr,
+                                                           fallback.ptr);
+      KG_LAUNCH_CHECK();
+      sort_u32_pairs(key.ptr, iota.ptr, nn, bits_for_value(parts + 1), key_sorted, sp.qrows, s);
+      sp.q_point.alloc(nn, s);
+      compose_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(sp.qrows.ptr, slot_of_row.ptr, nn,
+                                                         sp.q_point.ptr);
+      KG_LAUNCH_CHECK();
+      // The blocks' tile lists (count, scan, fill).
+      const uint64_t n_blocks = (nn + kTcQueryBlock - 1) / kTcQueryBlock;
+      const uint32_t n_tiles = (uint32_t)((nn + 127) / 128);
+      const size_t smem = (size_t)((n_tiles + 31) / 32) * 4;
+      if (smem > 200 * 1024)
+        fail(KG_ERR_INVALID, "kg_knn_learned: too many rows for the tile bitmap");
+      static std::once_flag attr;
+      std::call_once(attr, [] {
+        KG_CUDA(cudaFuncSetAttribute(probe_tiles_kernel,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+      });
+      DeviceBuffer<uint64_t> len(n_blocks + 1, s);
+      len.zero();
+      probe_tiles_kernel<<<(unsigned)n_blocks, kProbeThreads, smem, s>>>(
+          sp.qrows.ptr, nn, top.ptr, probe, fallback.ptr, part_start.ptr, n_tiles, kTcQueryBlock,
+          len.ptr, nullptr, nullptr);
+      KG_LAUNCH_CHECK();
+      sp.list_off.alloc(n_blocks + 1, s);
+      size_t t2 = 0;
+      KG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, t2, len.ptr, sp.list_off.ptr, n_blocks + 1, s));
+      DeviceBuffer<unsigned char> sc2(t2, s);
+      KG_CUDA(cub::DeviceScan::ExclusiveSum(sc2.ptr, t2, len.ptr, sp.list_off.ptr, n_blocks + 1, s));
+      uint64_t total = 0;
+      KG_CUDA(cudaMemcpyAsync(&total, sp.list_off.ptr + n_blocks, 8, cudaMemcpyDeviceToHost, s));
+      std::vector<uint8_t> hf(nn);
+      KG_CUDA(cudaMemcpyAsync(hf.data(), fallback.ptr, nn, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaStreamSynchronize(s));
+      fallback_rows = 0;
+      for (uint8_t v : hf) fallback_rows += v;
+      scanned_tiles = total;
+      sp.list_tiles.alloc(std::max<uint64_t>(total, 1), s);
+      probe_tiles_kernel<<<(unsigned)n_blocks, kProbeThreads, smem, s>>>(
+          sp.qrows.ptr, nn, top.ptr, probe, fallback.ptr, part_start.ptr, n_tiles, kTcQueryBlock,
+          len.ptr, sp.list_off.ptr, sp.list_tiles.ptr);
+      KG_LAUNCH_CHECK();
+      tr.mark("probe lists");
+    };
+    KnnResult r;
+    knn_core(ctx, x, n, width, d, k, &plan, r, trace);
+    write_graph(r, n, k, indptr, indices, distances, s);
+    wait_stream(ctx, s);
+    const double search_ms = ms_since(t_search);
+    trace.mark("graph");
+    ctx->done = n;
+    if (stats) {
+      stats->fallback_rows = fallback_rows;
+      stats->scanned_tiles = scanned_tiles;
+      stats->candidates = r.candidates;
+      stats->rows_full = r.rows_full;
+      stats->train_ms = train_ms;
+      stats->index_ms = index_ms;
+      stats->search_ms = search_ms;
+      stats->final_loss = final_loss;
+    }
+  });
+}
+
+}  // extern "C"

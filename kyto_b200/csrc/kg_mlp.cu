@@ -1,0 +1,377 @@
+// The learned partitioner's network (kg_mlp.cuh): forward, backward and Adam on the
+// device. Every reduction runs in a fixed order (no float atomics), so training is
+// bit-reproducible run to run.
+#include "kg_mlp.cuh"
+
+#include <cmath>
+
+namespace kg {
+
+namespace {
+
+constexpr int kBM = 64, kBN = 64, kBK = 16;  // GEMM block tile
+constexpr int kGemmThreads = 256;            // 16 x 16 threads, 4 x 4 outputs each
+
+enum : int { kEpiStore = 0, kEpiBiasReluBf16 = 1, kEpiMaskRelu = 2, kEpiBias = 3 };
+
+__device__ __forceinline__ float as_f32(float v) { return v; }
+__device__ __forceinline__ float as_f32(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+// C (M x N, row stride ldc) = op(A) (M x K) . op(B) (K x N), f32 sums of bf16 or f32
+// operands in k order per output (each output is one thread's running sum over the k
+// tiles: a fixed order). A(m,k) = TA ? A[k*lda+m] : A[m*lda+k]; B(k,n) = TB ? B[n*ldb+k]
+// : B[k*ldb+n]. Epilogues: store; + bias then ReLU rounded to bf16 into h (C keeps the
+// pre-activation); C * (z > 0) (the ReLU's backward); + bias.
+template <class TA, class TB, bool TRA, bool TRB, int EPI>
+__global__ void __launch_bounds__(kGemmThreads)
+gemm_kernel(int M, int N, int K, const TA* __restrict__ A, int lda, const TB* __restrict__ B,
+            int ldb, float* __restrict__ C, int ldc, const float* __restrict__ bias,
+            __nv_bfloat16* __restrict__ h, int ldh, const float* __restrict__ z, int ldz) {
+  __shared__ float as[kBK][kBM + 4];
+  __shared__ float bs[kBK][kBN + 4];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+  float acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
+  for (int k0 = 0; k0 < K; k0 += kBK) {
+    // 64 x 16 of A and 16 x 64 of B, 4 elements a thread each.
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int idx = threadIdx.x + e * kGemmThreads;  // 0..1023
+      int mm, kk;
+      if (TRA) {  // consecutive threads along m
+        mm = idx & 63;
+        kk = idx >> 6;
+      } else {    // consecutive threads along k
+        kk = idx & 15;
+        mm = idx >> 4;
+      }
+      const int gm = m0 + mm, gk = k0 + kk;
+      float v = 0.0f;
+      if (gm < M && gk < K) v = as_f32(TRA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk]);
+      as[kk][mm] = v;
+      int nn, kb;
+      if (TRB) {
+        kb = idx & 15;
+        nn = idx >> 4;
+      } else {
+        nn = idx & 63;
+        kb = idx >> 6;
+      }
+      const int gn = n0 + nn, gkb = k0 + kb;
+      float w = 0.0f;
+      if (gn < N && gkb < K) w = as_f32(TRB ? B[(size_t)gn * ldb + gkb] : B[(size_t)gkb * ldb + gn]);
+      bs[kb][nn] = w;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kBK; ++kk) {
+      float a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = as[kk][ty * 4 + i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = bs[kk][tx * 4 + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int gm = m0 + ty * 4 + i;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gn = n0 + tx * 4 + j;
+      if (gn >= N) continue;
+      float v = acc[i][j];
+      if (EPI == kEpiBiasReluBf16 || EPI == kEpiBias) v += bias[gn];
+      if (EPI == kEpiMaskRelu) v = z[(size_t)gm * ldz + gn] > 0.0f ? v : 0.0f;
+      C[(size_t)gm * ldc + gn] = v;
+      if (EPI == kEpiBiasReluBf16) h[(size_t)gm * ldh + gn] = __float2bfloat16_rn(fmaxf(v, 0.0f));
+    }
+  }
+}
+
+template <class TA, class TB, bool TRA, bool TRB, int EPI>
+void gemm(int M, int N, int K, const TA* A, int lda, const TB* B, int ldb, float* C, int ldc,
+          cudaStream_t s, const float* bias = nullptr, __nv_bfloat16* h = nullptr, int ldh = 0,
+          const float* z = nullptr, int ldz = 0) {
+  if (M == 0 || N == 0) return;
+  dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM);
+  gemm_kernel<TA, TB, TRA, TRB, EPI><<<grid, kGemmThreads, 0, s>>>(M, N, K, A, lda, B, ldb, C, ldc,
+                                                                   bias, h, ldh, z, ldz);
+  KG_LAUNCH_CHECK();
+}
+
+// x (rows x din, stride ldx) rounded to bf16.
+__global__ void to_bf16_rows_kernel(const float* x, uint64_t rows, uint32_t din, uint64_t ldx,
+                                    __nv_bfloat16* out) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= rows * din) return;
+  uint64_t r = i / din, c = i % din;
+  out[i] = __float2bfloat16_rn(x[r * ldx + c]);
+}
+
+// One warp per row: p = softmax(z); dz = (p - t) / rows with t the share of each part
+// among the row's L labels; row_loss = -(1/L) sum over labels of log p[label].
+__global__ void softmax_xent_kernel(const float* z, uint32_t rows, uint32_t parts,
+                                    const uint32_t* labels, uint32_t L, float* dz,
+                                    float* row_loss) {
+  const uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  if (row >= rows) return;
+  const float* zr = z + (uint64_t)row * parts;
+  float m = -INFINITY;
+  for (uint32_t p = lane; p < parts; p += 32) m = fmaxf(m, zr[p]);
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+  float sum = 0.0f;
+  for (uint32_t p = lane; p < parts; p += 32) sum += __expf(zr[p] - m);
+  for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+  const float inv_rows = 1.0f / (float)rows, inv_sum = 1.0f / sum;
+  float* dr = dz + (uint64_t)row * parts;
+  for (uint32_t p = lane; p < parts; p += 32) dr[p] = __expf(zr[p] - m) * inv_sum * inv_rows;
+  __syncwarp();
+  if (lane == 0) {
+    const float share = inv_rows / (float)L;
+    const float log_sum = logf(sum);
+    float loss = 0.0f;
+    for (uint32_t j = 0; j < L; ++j) {
+      const uint32_t p = labels[(uint64_t)row * L + j];
+      dr[p] -= share;
+      loss -= zr[p] - m - log_sum;
+    }
+    row_loss[row] = loss / (float)L;
+  }
+}
+
+// out[c] = sum over rows of a[r * ld + c], 16 row classes per column summed in order,
+// then the classes in order.
+__global__ void __launch_bounds__(1024)
+column_sums_kernel(const float* a, uint32_t rows, uint32_t cols, uint32_t ld, float* out) {
+  __shared__ float part[16][64];
+  const uint32_t c = blockIdx.x * 64 + (threadIdx.x & 63u), cls = threadIdx.x >> 6;
+  float t = 0.0f;
+  if (c < cols)
+    for (uint32_t r = cls; r < rows; r += 16) t += a[(uint64_t)r * ld + c];
+  part[cls][threadIdx.x & 63u] = t;
+  __syncthreads();
+  if (cls == 0 && c < cols) {
+    float u = 0.0f;
+    for (int k = 0; k < 16; ++k) u += part[k][threadIdx.x & 63u];
+    out[c] = u;
+  }
+}
+
+__global__ void adam_kernel(float* p, const float* g, float* m, float* v, uint64_t n, float lr,
+                            float b1, float b2, float c1, float c2, float eps) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+__global__ void refresh_kernel(const float* p, uint64_t n, __nv_bfloat16* wb) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) wb[i] = __float2bfloat16_rn(p[i]);
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+// He-uniform weights U(-sqrt(6/fan_in), sqrt(6/fan_in)) from a counter-based stream
+// (SplitMix64 of seed and position); biases stay zero.
+__global__ void init_kernel(float* p, uint64_t begin, uint64_t n, uint32_t fan_in,
+                            uint64_t seed) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t bits = mix64(seed * 0x9E3779B97F4A7C15ull + begin + i + 1);
+  const double u = (double)(bits >> 11) * 0x1p-53;  // [0, 1)
+  const double lim = sqrt(6.0 / (double)fan_in);
+  p[begin + i] = (float)((2.0 * u - 1.0) * lim);
+}
+
+// Top `probe` parts per row by logit (descending, ties to the lower part): one warp per
+// row, `probe` rounds of a warp argmax; the confidence is their summed softmax.
+__global__ void top_parts_kernel(const float* z, uint64_t rows, uint32_t parts, uint32_t probe,
+                                 uint32_t* top, float* conf) {
+  const uint64_t row = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  if (row >= rows) return;
+  const float* zr = z + row * parts;
+  float m = -INFINITY;
+  for (uint32_t p = lane; p < parts; p += 32) m = fmaxf(m, zr[p]);
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+  float sum = 0.0f;
+  for (uint32_t p = lane; p < parts; p += 32) sum += __expf(zr[p] - m);
+  for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+  float picked = 0.0f;
+  uint32_t prev_p = 0xFFFFFFFFu;
+  float prev_v = INFINITY;
+  for (uint32_t t = 0; t < probe; ++t) {
+    // The best (value, part) strictly after (prev_v, prev_p) in the order.
+    float bv = -INFINITY;
+    uint32_t bp = 0xFFFFFFFFu;
+    for (uint32_t p = lane; p < parts; p += 32) {
+      const float v = zr[p];
+      const bool after = v < prev_v || (v == prev_v && p > prev_p);
+      if (after && (v > bv || (v == bv && p < bp))) {
+        bv = v;
+        bp = p;
+      }
+    }
+    for (int o = 16; o; o >>= 1) {
+      const float ov = __shfl_xor_sync(0xFFFFFFFFu, bv, o);
+      const uint32_t op = __shfl_xor_sync(0xFFFFFFFFu, bp, o);
+      if (ov > bv || (ov == bv && op < bp)) {
+        bv = ov;
+        bp = op;
+      }
+    }
+    if (lane == 0) top[row * probe + t] = bp;
+    picked += __expf(bv - m);
+    prev_v = bv;
+    prev_p = bp;
+  }
+  if (lane == 0) conf[row] = picked / sum;
+}
+
+}  // namespace
+
+void MlpShape::layout() {
+  uint64_t o = 0;
+  auto take = [&](uint64_t n) {
+    uint64_t at = o;
+    o += (n + 3) & ~3ull;
+    return at;
+  };
+  for (int l = 0; l < 3; ++l) {
+    w_off[l] = take((uint64_t)out(l) * in(l));
+    b_off[l] = take(out(l));
+  }
+  total = o;
+}
+
+void MlpBatch::alloc(const MlpShape& sh, uint32_t n, cudaStream_t s) {
+  rows = n;
+  h0.alloc((uint64_t)n * sh.din, s);
+  h1.alloc((uint64_t)n * sh.hidden, s);
+  h2.alloc((uint64_t)n * sh.hidden, s);
+  z1.alloc((uint64_t)n * sh.hidden, s);
+  z2.alloc((uint64_t)n * sh.hidden, s);
+  z3.alloc((uint64_t)n * sh.parts, s);
+  dz3.alloc((uint64_t)n * sh.parts, s);
+  dz2.alloc((uint64_t)n * sh.hidden, s);
+  dz1.alloc((uint64_t)n * sh.hidden, s);
+  row_loss.alloc(n, s);
+}
+
+void Mlp::init(uint32_t din, uint32_t hidden, uint32_t parts, uint64_t seed, cudaStream_t s) {
+  sh.din = din;
+  sh.hidden = hidden;
+  sh.parts = parts;
+  sh.layout();
+  params.alloc(sh.total, s);
+  params.zero();
+  grads.alloc(sh.total, s);
+  grads.zero();
+  m1.alloc(sh.total, s);
+  m1.zero();
+  m2.alloc(sh.total, s);
+  m2.zero();
+  wb.alloc(sh.total, s);
+  for (int l = 0; l < 3; ++l) {
+    uint64_t nw = (uint64_t)sh.out(l) * sh.in(l);
+    init_kernel<<<blocks_for(nw, 256), 256, 0, s>>>(params.ptr, sh.w_off[l], nw, sh.in(l), seed);
+    KG_LAUNCH_CHECK();
+  }
+  step = 0;
+  refresh(s);
+}
+
+void Mlp::set_params(const float* src, cudaStream_t s) {
+  KG_CUDA(cudaMemcpyAsync(params.ptr, src, sh.total * 4, cudaMemcpyDefault, s));
+  refresh(s);
+}
+
+void Mlp::refresh(cudaStream_t s) {
+  refresh_kernel<<<blocks_for(sh.total, 256), 256, 0, s>>>(params.ptr, sh.total, wb.ptr);
+  KG_LAUNCH_CHECK();
+}
+
+void Mlp::forward(const float* x, uint64_t ldx, MlpBatch& b, cudaStream_t s) const {
+  const int n = (int)b.rows, din = (int)sh.din, h = (int)sh.hidden, P = (int)sh.parts;
+  to_bf16_rows_kernel<<<blocks_for((uint64_t)n * din, 256), 256, 0, s>>>(x, n, din, ldx, b.h0.ptr);
+  KG_LAUNCH_CHECK();
+  const __nv_bfloat16* W = wb.ptr;
+  const float* bias = params.ptr;
+  // z = h W^T + b: W is out x in row-major, so B(k, n) = W[n * in + k].
+  gemm<__nv_bfloat16, __nv_bfloat16, false, true, kEpiBiasReluBf16>(
+      n, h, din, b.h0.ptr, din, W + sh.w_off[0], din, b.z1.ptr, h, s, bias + sh.b_off[0],
+      b.h1.ptr, h);
+  gemm<__nv_bfloat16, __nv_bfloat16, false, true, kEpiBiasReluBf16>(
+      n, h, h, b.h1.ptr, h, W + sh.w_off[1], h, b.z2.ptr, h, s, bias + sh.b_off[1], b.h2.ptr, h);
+  gemm<__nv_bfloat16, __nv_bfloat16, false, true, kEpiBias>(
+      n, P, h, b.h2.ptr, h, W + sh.w_off[2], h, b.z3.ptr, P, s, bias + sh.b_off[2]);
+}
+
+void Mlp::backward(const uint32_t* labels, uint32_t L, MlpBatch& b, cudaStream_t s) {
+  const int n = (int)b.rows, din = (int)sh.din, h = (int)sh.hidden, P = (int)sh.parts;
+  softmax_xent_kernel<<<blocks_for((uint64_t)n * 32, 256), 256, 0, s>>>(
+      b.z3.ptr, n, P, labels, L, b.dz3.ptr, b.row_loss.ptr);
+  KG_LAUNCH_CHECK();
+  const __nv_bfloat16* W = wb.ptr;
+  float* G = grads.ptr;
+  // Layer 3: dW3 = dz3^T h2 (P x h), db3 = column sums of dz3, dz2 = (dz3 W3) * (z2 > 0).
+  gemm<float, __nv_bfloat16, true, false, kEpiStore>(P, h, n, b.dz3.ptr, P, b.h2.ptr, h,
+                                                     G + sh.w_off[2], h, s);
+  column_sums_kernel<<<(P + 63) / 64, 1024, 0, s>>>(b.dz3.ptr, n, P, P, G + sh.b_off[2]);
+  KG_LAUNCH_CHECK();
+  gemm<float, __nv_bfloat16, false, false, kEpiMaskRelu>(n, h, P, b.dz3.ptr, P, W + sh.w_off[2],
+                                                         h, b.dz2.ptr, h, s, nullptr, nullptr, 0,
+                                                         b.z2.ptr, h);
+  // Layer 2.
+  gemm<float, __nv_bfloat16, true, false, kEpiStore>(h, h, n, b.dz2.ptr, h, b.h1.ptr, h,
+                                                     G + sh.w_off[1], h, s);
+  column_sums_kernel<<<(h + 63) / 64, 1024, 0, s>>>(b.dz2.ptr, n, h, h, G + sh.b_off[1]);
+  KG_LAUNCH_CHECK();
+  gemm<float, __nv_bfloat16, false, false, kEpiMaskRelu>(n, h, h, b.dz2.ptr, h, W + sh.w_off[1],
+                                                         h, b.dz1.ptr, h, s, nullptr, nullptr, 0,
+                                                         b.z1.ptr, h);
+  // Layer 1.
+  gemm<float, __nv_bfloat16, true, false, kEpiStore>(h, din, n, b.dz1.ptr, h, b.h0.ptr, din,
+                                                     G + sh.w_off[0], din, s);
+  column_sums_kernel<<<(h + 63) / 64, 1024, 0, s>>>(b.dz1.ptr, n, h, h, G + sh.b_off[0]);
+  KG_LAUNCH_CHECK();
+}
+
+void Mlp::adam(float lr, cudaStream_t s) {
+  ++step;
+  const float c1 = 1.0f - (float)std::pow(0.9, (double)step);
+  const float c2 = 1.0f - (float)std::pow(0.999, (double)step);
+  adam_kernel<<<blocks_for(sh.total, 256), 256, 0, s>>>(params.ptr, grads.ptr, m1.ptr, m2.ptr,
+                                                        sh.total, lr, 0.9f, 0.999f, c1, c2, 1e-8f);
+  KG_LAUNCH_CHECK();
+  refresh(s);
+}
+
+void top_parts(const float* logits, uint64_t rows, uint32_t parts, uint32_t probe, uint32_t* top,
+               float* confidence, cudaStream_t s) {
+  top_parts_kernel<<<blocks_for(rows * 32, 256), 256, 0, s>>>(logits, rows, parts, probe, top,
+                                                             confidence);
+  KG_LAUNCH_CHECK();
+}
+
+}  // namespace kg

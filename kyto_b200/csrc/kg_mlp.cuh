@@ -1,0 +1,62 @@
+// The learned partitioner's network: a BF16 MLP d -> h -> h -> P (ReLU between) with f32
+// master weights, trained with Adam on soft targets, and its inference. Hand-written
+// kernels (kg_mlp.cu): a tiled SIMT GEMM with f32 accumulation over bf16 or f32
+// operands and fused bias/ReLU/mask epilogues, a warp-per-row softmax cross-entropy,
+// fixed-order column sums, Adam, and the bf16 weight refresh.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include <cstdint>
+
+#include "kg_internal.cuh"
+
+namespace kg {
+
+struct MlpShape {
+  uint32_t din = 0, hidden = 0, parts = 0;
+  // Offsets (floats) of W1 (hidden x din), b1, W2 (hidden x hidden), b2, W3 (parts x
+  // hidden), b3 in the packed parameter vector (each a multiple of 4).
+  uint64_t w_off[3] = {0, 0, 0}, b_off[3] = {0, 0, 0};
+  uint64_t total = 0;
+  uint32_t in(int l) const { return l == 0 ? din : hidden; }
+  uint32_t out(int l) const { return l == 2 ? parts : hidden; }
+  void layout();
+};
+
+// Activations of one batch (rows x widths), kept for the backward pass.
+struct MlpBatch {
+  uint32_t rows = 0;
+  DeviceBuffer<__nv_bfloat16> h0, h1, h2;  // inputs of the three layers
+  DeviceBuffer<float> z1, z2, z3;          // pre-activations (z3: the logits)
+  DeviceBuffer<float> dz3, dz2, dz1;       // gradients
+  DeviceBuffer<float> row_loss;
+  void alloc(const MlpShape& sh, uint32_t rows, cudaStream_t s);
+};
+
+class Mlp {
+ public:
+  MlpShape sh;
+  DeviceBuffer<float> params, grads, m1, m2;
+  DeviceBuffer<__nv_bfloat16> wb;  // bf16 copy of the packed parameters
+  uint64_t step = 0;
+
+  void init(uint32_t din, uint32_t hidden, uint32_t parts, uint64_t seed, cudaStream_t s);
+  void set_params(const float* host_or_device, cudaStream_t s);
+  // The bf16 copy from the f32 masters.
+  void refresh(cudaStream_t s);
+  // x: b.rows x din f32 (row stride ldx floats) -> logits in b.z3.
+  void forward(const float* x, uint64_t ldx, MlpBatch& b, cudaStream_t s) const;
+  // Soft-target cross-entropy of the logits in b.z3 (labels: rows x L part indices; a
+  // row's target is the share of each part among its L labels) and every gradient into
+  // `grads`; the per-row losses stay in b.row_loss.
+  void backward(const uint32_t* labels, uint32_t L, MlpBatch& b, cudaStream_t s);
+  void adam(float lr, cudaStream_t s);
+};
+
+// The top `probe` parts of each row of logits (rows x parts, f32) by probability
+// (descending, ties to the lower part) and their summed probability.
+void top_parts(const float* logits, uint64_t rows, uint32_t parts, uint32_t probe,
+               uint32_t* top, float* confidence, cudaStream_t s);
+
+}  // namespace kg
