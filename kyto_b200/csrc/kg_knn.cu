@@ -551,12 +551,16 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
   DeviceBuffer<unsigned long long> n_cand(1, s);
   n_cand.zero();
   double filter_ms = 0, rank_ms = 0;
-  // The filter: the tensor-core GEMM (fp16, or bf16 on request) when the components
-  // and the three norm columns fit one 64-wide operand row; the SIMT filter otherwise
-  // or on request (KYTO_GPU_KNN_FILTER=simt|fp16|bf16). All give the same graph.
+  // The filter: the tensor-core GEMM (fp16, split fp16 hi/lo, or bf16 on request) when
+  // the components and the three norm columns fit one 64-wide operand row; the SIMT
+  // filter otherwise or on request (KYTO_GPU_KNN_FILTER=simt|fp16|split|bf16). All give
+  // the same graph.
   const char* choice = std::getenv("KYTO_GPU_KNN_FILTER");
   std::string filter = choice ? choice : "fp16";
-  bool tc = !brute && d + 3 <= 64 && (filter == "fp16" || filter == "bf16");
+  bool tc = !brute && d + 3 <= 64 && (filter == "fp16" || filter == "bf16" || filter == "split");
+  const FilterKind kind = filter == "bf16"    ? FilterKind::Bf16
+                          : filter == "split" ? FilterKind::Split
+                                              : FilterKind::Fp16;
   if (brute) {
     uint32_t one = 1;
     std::vector<uint32_t> all(n, one);
@@ -571,7 +575,7 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
     const double scale = tc_scale(x, n, width, d, mean.ptr, max_sq.ptr, s);
     ScanPlan sp;
     if (plan) {
-      (*plan)(x, n, width, d, scale, sp, trace);
+      (*plan)(x, n, width, d, scale, filter_query_block(kind), sp, trace);
     } else {
       // The rows sorted by a Morton code of their first three centred components, so
       // a query block's own tiles hold its nearest points and the scan starts there.
@@ -588,7 +592,7 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
     scan.list_stride = sp.list_stride;
     const uint32_t* prows = sp.prows.ptr ? sp.prows.ptr : sp.qrows.ptr;
     tc_filter(ctx, s, x, width, d, sp.qrows.ptr, prows, scan, mean.ptr, scale, max_sq.ptr,
-              filter == "bf16", k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
+              kind, k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
               qn2.ptr, slack_d.ptr, &trace);
     filter_ms += tf.stop_ms();
     check_cancel(ctx);

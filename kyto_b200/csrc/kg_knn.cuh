@@ -39,8 +39,10 @@ struct ScanPlan {
   DeviceBuffer<uint64_t> list_off;
   uint64_t list_stride = 0;
 };
+// Builds the filter's scan for query blocks of qblock slots.
 using PlanBuilder = std::function<void(const float* x, uint64_t n, uint32_t width, uint32_t d,
-                                       double scale, ScanPlan& plan, Trace& trace)>;
+                                       double scale, uint32_t qblock, ScanPlan& plan,
+                                       Trace& trace)>;
 
 void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t d, uint32_t k,
               const PlanBuilder* plan, KnnResult& out, Trace& trace);

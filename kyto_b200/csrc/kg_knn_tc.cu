@@ -9,13 +9,20 @@
 // every point within twice the proven slack of the k-th, appended to the query's
 // candidate slice. Candidates are then ranked by exact f64 keys (kg_knn.cu).
 //
+// Split operands (hi and lo fp16 parts of each component, two 64-wide sub-tiles per
+// row) make the key three products, q_hi.p_hi + q_hi.p_lo + q_lo.p_hi, missing only
+// q_lo.p_lo: the slack then comes from the f32 accumulation (about 2^-14 |q| R) rather
+// than from fp16 rounding (2^-9 |q| R), which keeps the candidate sets near k where
+// tight clusters sit far from the mean.
+//
 // CTA layout (one persistent CTA per SM, 320 threads):
 //   warps 0-7  epilogue: thread t owns query t of the CTA's 256-query block (TMEM lane
 //              32*(warp%4)+lane of accumulator warp/4);
 //   warp 8     TMA producer: the block's two 128-query operand tiles, then 128-point
-//              tiles through a ring of kStages shared-memory stages;
+//              tiles through a ring of shared-memory stages;
 //   warp 9     MMA issuer: per point tile, two M=128 N=128 K=64 products (one per
-//              128-query half) into one of two TMEM accumulator buffers.
+//              128-query half; three each with split operands) into one of two TMEM
+//              accumulator buffers.
 // TMEM: 2 buffers x (2 halves x 128 columns) = 512 columns, f32.
 #include <cudaTypedefs.h>
 #include <cuda_bf16.h>
@@ -40,18 +47,27 @@ using namespace sm100;
 constexpr int kTcQueries = (int)kTcQueryBlock;
 constexpr int kTcPoints = 128;
 constexpr int kTcK = 64;  // operand width (fp16 elements, one 128-byte swizzle row)
-constexpr int kStages = 6;
 constexpr uint32_t kTileBytes = 128u * 128u;  // 128 rows x 64 fp16
 constexpr int kEpiWarps = 8;
 constexpr int kTcThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kEndOfBlock = 0xFFFFFFFFu;
 
+// SUBS: 64-wide sub-tiles per operand row (1: fp16 or bf16; 2: split hi and lo). KR: the
+// register top-k width (16, 32) or 0 (the k smallest in local memory, any k).
+template <int KR, int SUBS>
+struct TcShape {
+  static constexpr int kStages = SUBS == 1 ? 6 : (KR == 32 ? 2 : 3);
+  static constexpr int kTopK = KR == 0 ? 1 : KR + 1;  // odd row stride: no bank conflicts
+};
+
+template <int KR, int SUBS>
 struct TcSmem {
-  uint8_t a[2][kTileBytes];          // the query block's two operand tiles
-  uint8_t b[kStages][kTileBytes];    // point tiles
-  float scratch[kEpiWarps * 32][33]; // a thread's 32 keys when some may pass
-  float topk[kEpiWarps * 32][33];    // a thread's k smallest keys (k <= 32)
+  static constexpr int kStages = TcShape<KR, SUBS>::kStages;
+  uint8_t a[2][SUBS][kTileBytes];     // the query block's two 128-row halves
+  uint8_t b[kStages][SUBS][kTileBytes];  // point tiles
+  float scratch[kEpiWarps * 32][33];  // a thread's 32 keys when some may pass
+  float topk[kEpiWarps * 32][TcShape<KR, SUBS>::kTopK];  // a thread's k smallest keys
   uint64_t full[kStages], empty[kStages];
   uint64_t tmem_full[2], tmem_empty[2];
   uint64_t a_full, a_empty, drained;
@@ -62,7 +78,13 @@ struct TcSmem {
   uint32_t tmem_base;
   int abort;
 };
-constexpr size_t kTcSmemBytes = sizeof(TcSmem) + 1024;  // + alignment slack
+template <int KR, int SUBS>
+constexpr size_t tc_smem_bytes() {
+  return sizeof(TcSmem<KR, SUBS>) + 1024;  // + alignment slack
+}
+static_assert(tc_smem_bytes<32, 1>() <= 227 * 1024 && tc_smem_bytes<16, 2>() <= 227 * 1024 &&
+                  tc_smem_bytes<32, 2>() <= 227 * 1024 && tc_smem_bytes<0, 2>() <= 227 * 1024,
+              "filter shared memory");
 
 __device__ __forceinline__ float round_up_f32d(double v) {
   float r = (float)v;
@@ -203,8 +225,9 @@ __device__ __forceinline__ void tc_offer_chunk(QueryState& st, float* smallest, 
   }
 }
 
-// KR: the register top-k width used on offers (k <= KR), or 0 for any k.
-template <int KR>
+// KR: the register top-k width used on offers (k <= KR), or 0 for any k. SUBS: operand
+// sub-tiles (1: one fp16/bf16 product; 2: split, three fp16 products).
+template <int KR, int SUBS>
 __global__ void __launch_bounds__(kTcThreads, 1)
 knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
                      const __grid_constant__ CUtensorMap tmap_p, FilterScan scan, uint32_t k,
@@ -214,7 +237,9 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
   extern __shared__ uint8_t smem_raw[];
   // Aligned to 1024 bytes by an offset into the __shared__ array itself, so the compiler
   // keeps every access in the shared state space (no generic loads and stores).
-  TcSmem& sm = *reinterpret_cast<TcSmem*>(smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u));
+  using Smem = TcSmem<KR, SUBS>;
+  constexpr int kStages = Smem::kStages;
+  Smem& sm = *reinterpret_cast<Smem*>(smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u));
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const uint64_t n_q = scan.n_q, n_p = scan.n_p;
@@ -266,9 +291,11 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
         ok = mbar_wait(&sm.a_empty, (bi & 1) ^ 1, abort);
         if (ok) {
           for (int w = 0; w < kEpiWarps; ++w) u_max[(bi & 1) * kEpiWarps + w] = INFINITY;
-          mbar_arrive_expect_tx(&sm.a_full, 2 * kTileBytes);
-          tma_load_2d(sm.a[0], &tmap_q, &sm.a_full, 0, (int32_t)(qb * kTcQueries));
-          tma_load_2d(sm.a[1], &tmap_q, &sm.a_full, 0, (int32_t)(qb * kTcQueries + 128));
+          mbar_arrive_expect_tx(&sm.a_full, 2 * SUBS * kTileBytes);
+          for (int h = 0; h < 2; ++h)
+            for (int sub = 0; sub < SUBS; ++sub)
+              tma_load_2d(sm.a[h][sub], &tmap_q, &sm.a_full, sub * kTcK,
+                          (int32_t)(qb * kTcQueries + h * 128));
         }
       }
       ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
@@ -288,8 +315,14 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
         const uint32_t lt = __shfl_sync(0xFFFFFFFFu, win_tile, at);
         const float lb2 = __shfl_sync(0xFFFFFFFFu, win_lb2, at);
         if (i < len && scan.list_lb2) {
-          float u = u_max[(bi & 1) * kEpiWarps];
-          for (int w = 1; w < kEpiWarps; ++w) u = fmaxf(u, u_max[(bi & 1) * kEpiWarps + w]);
+          // One lane reads the bounds (the epilogue may be writing them) and the warp
+          // takes its value, so every lane makes the same choice.
+          float u = 0.0f;
+          if (lane == 0) {
+            u = u_max[(bi & 1) * kEpiWarps];
+            for (int w = 1; w < kEpiWarps; ++w) u = fmaxf(u, u_max[(bi & 1) * kEpiWarps + w]);
+          }
+          u = __shfl_sync(0xFFFFFFFFu, u, 0);
           if (lb2 > u) continue;
         }
         bool end = false;
@@ -311,8 +344,10 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
                                       ? lt
                                       : (uint32_t)((i + qb * (kTcQueries / kTcPoints)) % n_tiles);
               sm.stage_tile[s] = pt;
-              mbar_arrive_expect_tx(&sm.full[s], kTileBytes);
-              tma_load_2d(sm.b[s], &tmap_p, &sm.full[s], 0, (int32_t)(pt * kTcPoints));
+              mbar_arrive_expect_tx(&sm.full[s], SUBS * kTileBytes);
+              for (int sub = 0; sub < SUBS; ++sub)
+                tma_load_2d(sm.b[s][sub], &tmap_p, &sm.full[s], sub * kTcK,
+                            (int32_t)(pt * kTcPoints));
               issued_phase[s] = (int)ph;
             }
           }
@@ -337,7 +372,6 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
       uint64_t it = 0;
       uint32_t bi = 0;
       bool ok = true;
-      const uint32_t a0 = smem_addr(sm.a[0]), a1 = smem_addr(sm.a[1]);
       for (uint64_t qb = blockIdx.x; qb < n_qblocks && ok; qb += gridDim.x, ++bi) {
         if (!mbar_wait(&sm.a_full, bi & 1, abort)) break;
         tc_fence_after();
@@ -360,13 +394,22 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
             ++it;
             break;
           }
-          const uint32_t bsm = smem_addr(sm.b[s]);
           const uint32_t d0 = tmem + ab * 256u, d1 = d0 + 128u;
+          // Products (A sub-tile, B sub-tile): (0, 0) alone, or for split operands
+          // [-2q_hi, 1, 1, 1 | -2q_lo] and [p_hi, h1, h2, h3 | p_lo] the pairs (0, 0),
+          // (0, 1), (1, 0): q_hi.p_hi + norm, q_hi.p_lo, q_lo.p_hi (the norm columns meet
+          // zeros in the other two).
 #pragma unroll
-          for (int kk = 0; kk < kTcK / 16; ++kk) {
-            const uint64_t bd = desc_k_sw128(bsm + kk * 32);
-            mma_f16(d0, desc_k_sw128(a0 + kk * 32), bd, idesc, kk > 0);
-            mma_f16(d1, desc_k_sw128(a1 + kk * 32), bd, idesc, kk > 0);
+          for (int t = 0; t < (SUBS == 1 ? 1 : 3); ++t) {
+            const int sa = t == 2 ? 1 : 0, sb = t == 1 ? 1 : 0;
+            const uint32_t bsm = smem_addr(sm.b[s][sb]);
+            const uint32_t a0 = smem_addr(sm.a[0][sa]), a1 = smem_addr(sm.a[1][sa]);
+#pragma unroll
+            for (int kk = 0; kk < kTcK / 16; ++kk) {
+              const uint64_t bd = desc_k_sw128(bsm + kk * 32);
+              mma_f16(d0, desc_k_sw128(a0 + kk * 32), bd, idesc, (t | kk) > 0);
+              mma_f16(d1, desc_k_sw128(a1 + kk * 32), bd, idesc, (t | kk) > 0);
+            }
           }
           mma_commit(&sm.empty[s]);
           mbar_arrive(&sm.tmem_full[ab]);
@@ -545,6 +588,80 @@ __global__ void tc_operands_kernel(const float* x, uint64_t n, uint32_t width, u
   slack2[r] = round_up_f32d(2.0 * e);
 }
 
+// The split operands, one warp per row (lane j: components j and j + 32): rows
+// centred (f64) and scaled by 2^e, each component c as hi = fp16(c) and lo = fp16(c - hi).
+// Query row [-2hi, 1, 1, 1, 0... | -2lo, 0...], point row [hi, h1, h2, h3, 0... | lo,
+// 0...] (h1..h3 the scaled squared norm in three parts), 128 fp16 each; per query the
+// centred squared norm (unscaled) and the slack.
+__global__ void tc_split_operands_kernel(const float* x, uint64_t n, uint32_t width, uint32_t d,
+                                         const uint32_t* rows, const double* mean, double scale,
+                                         const double* max_sq, bool query, __half* out,
+                                         double* qn2, float* slack2, double* slack_d) {
+  const uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31;
+  if (r >= n) return;
+  const float* xr = x + (uint64_t)(rows ? rows[r] : r) * width;
+  double cs[2], n2 = 0.0, n2s = 0.0;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t j = lane + 32u * h;
+    cs[h] = 0.0;
+    if (j < d) {
+      const double c = (double)xr[j] - mean[j];
+      cs[h] = c * scale;
+      n2 += c * c;
+      n2s += cs[h] * cs[h];
+    }
+  }
+  for (int o = 16; o; o >>= 1) {
+    n2 += __shfl_xor_sync(0xFFFFFFFFu, n2, o);
+    n2s += __shfl_xor_sync(0xFFFFFFFFu, n2s, o);
+  }
+  // The squared norm in three parts (each rounded from what the previous left).
+  const __half h1 = __float2half_rn((float)n2s);
+  const double r2 = n2s - (double)__half2float(h1);
+  const __half h2 = __float2half_rn((float)r2);
+  const __half h3 = __float2half_rn((float)(r2 - (double)__half2float(h2)));
+  __half* o = out + r * (2 * kTcK);
+  const __half zero = __float2half_rn(0.0f), one = __float2half_rn(1.0f);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const uint32_t j = lane + 32u * h;
+    __half hi = zero, lo = zero, head = zero;
+    if (j < d) {
+      hi = __float2half_rn((float)cs[h]);
+      lo = __float2half_rn((float)(cs[h] - (double)__half2float(hi)));
+      if (query) {  // -2 hi, -2 lo: exact, a power-of-two multiple
+        hi = __float2half_rn(-2.0f * __half2float(hi));
+        lo = __float2half_rn(-2.0f * __half2float(lo));
+      }
+      head = hi;
+    } else if (j < d + 3) {
+      head = query ? one : (j == d ? h1 : j == d + 1 ? h2 : h3);
+    }
+    o[j] = head;
+    o[kTcK + j] = lo;
+  }
+  if (!query || lane != 0) return;
+  qn2[r] = n2;
+  // The bound of |A - s^2 (D - |q|^2)| (scaled units): the dropped -2 lo.lo and the
+  // components' residuals, 2((3u^2 + 5u^3)|q||p| + 2.01 eta sqrt(d)(|q| + |p|) + 10 d
+  // eta^2) with u = 2^-11 (both roundings f64 -> f32 -> fp16) and eta = 2^-25 (fp16's
+  // subnormal half-step); the norm's three parts u^3 |p|^2 + 2 eta; the f32
+  // accumulation gamma (2|q||p| + |p|^2) with gamma = 2^-15 (three products of 64
+  // terms in twelve K = 16 steps, truncating adds); and f64 rounding of the exact key;
+  // |p| bounded by the largest row norm R. Doubled, as kyto doubles its own.
+  const double u = 0x1p-11, eta = 0x1p-25, gamma = 0x1p-15, tiny = 0x1p-40;
+  const double qs = sqrt(n2s), rs = sqrt(*max_sq) * scale, dd = (double)d;
+  double e = 2.0 * (3.0 * u * u + 5.0 * u * u * u) * qs * rs +
+             4.02 * eta * sqrt(dd) * (qs + rs) + 20.0 * dd * eta * eta +
+             2.0 * u * u * u * rs * rs + 2.0 * eta + gamma * (2.02 * qs * rs + 1.02 * rs * rs) +
+             tiny * (qs + rs) * (qs + rs);
+  e *= 2.0;
+  slack_d[r] = e / (scale * scale);
+  slack2[r] = round_up_f32d(2.0 * e);
+}
+
 // The largest centred squared norm, f64.
 __global__ void centred_norm_kernel(const float* x, uint64_t n, uint32_t width, uint32_t d,
                                     const double* mean, double* sq) {
@@ -577,13 +694,13 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// A [rows x 64] 16-bit row-major matrix, boxes of 128 rows x 64 (one 128-byte swizzle
-// row each), zero fill past the last row.
-CUtensorMap tile_map(const void* base, uint64_t rows, bool bf16) {
+// A [rows x cols] 16-bit row-major matrix (cols a multiple of 64), boxes of 128 rows x
+// 64 (one 128-byte swizzle row each), zero fill past the last row.
+CUtensorMap tile_map(const void* base, uint64_t rows, bool bf16, uint32_t cols = kTcK) {
   CUtensorMap m;
   std::memset(&m, 0, sizeof(m));
-  cuuint64_t dims[2] = {(cuuint64_t)kTcK, (cuuint64_t)rows};
-  cuuint64_t strides[1] = {(cuuint64_t)kTcK * 2};
+  cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
   cuuint32_t box[2] = {(cuuint32_t)kTcK, 128};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = encode_fn()(&m, bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
@@ -619,55 +736,81 @@ double tc_scale(const float* x, uint64_t n, uint32_t width, uint32_t d, const do
   return scale;
 }
 
+uint32_t filter_query_block(FilterKind) { return kTcQueryBlock; }
+
+namespace {
+
+template <int KR, int SUBS>
+void launch_filter(unsigned grid, cudaStream_t s, const CUtensorMap& mq, const CUtensorMap& mp,
+                   const FilterScan& scan, uint32_t k, const float* slack2, uint32_t idesc,
+                   uint32_t cap, float* cand_key, uint32_t* cand_row, uint32_t* cand_count,
+                   float* threshold, int* err) {
+  static std::once_flag attr;
+  std::call_once(attr, [] {
+    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<KR, SUBS>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)tc_smem_bytes<KR, SUBS>()));
+  });
+  knn_filter_tc_kernel<KR, SUBS><<<grid, kTcThreads, tc_smem_bytes<KR, SUBS>(), s>>>(
+      mq, mp, scan, k, slack2, idesc, cap, cand_key, cand_row, cand_count, threshold, err);
+}
+
+}  // namespace
+
 void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint32_t width, uint32_t d,
                const uint32_t* qrows, const uint32_t* prows, FilterScan scan,
-               const double* mean, double scale, const double* max_sq, bool bf16, uint32_t k,
-               uint32_t cap, float* cand_key, uint32_t* cand_row, uint32_t* cand_count,
-               float* threshold, double* qn2, double* slack_d, Trace* trace) {
+               const double* mean, double scale, const double* max_sq, FilterKind kind,
+               uint32_t k, uint32_t cap, float* cand_key, uint32_t* cand_row,
+               uint32_t* cand_count, float* threshold, double* qn2, double* slack_d,
+               Trace* trace) {
   if (d + 3 > (uint32_t)kTcK) fail(KG_ERR_INVALID, "tensor-core filter: more than 61 components");
   const uint64_t n_q = scan.n_q, n_p = scan.n_p;
-  const double u = bf16 ? 0x1p-8 : 0x1p-11;
-  const double eta = bf16 ? 0x1p-134 : 0x1p-25;
-  DeviceBuffer<uint16_t> aq(n_q * kTcK, s), bp(n_p * kTcK, s);
+  const bool split = kind == FilterKind::Split, bf16 = kind == FilterKind::Bf16;
+  const uint32_t width_op = split ? 2u * kTcK : (uint32_t)kTcK;
+  DeviceBuffer<uint16_t> aq(n_q * width_op, s), bp(n_p * width_op, s);
   DeviceBuffer<float> slack2(n_q, s);
-  if (bf16) {
-    tc_operands_kernel<__nv_bfloat16><<<blocks_for(n_q, 128), 128, 0, s>>>(
-        x, n_q, width, d, qrows, mean, scale, u, eta, max_sq, true, (__nv_bfloat16*)aq.ptr, qn2,
-        slack2.ptr, slack_d);
-    tc_operands_kernel<__nv_bfloat16><<<blocks_for(n_p, 128), 128, 0, s>>>(
-        x, n_p, width, d, prows, mean, scale, u, eta, max_sq, false, (__nv_bfloat16*)bp.ptr,
-        nullptr, nullptr, nullptr);
+  if (split) {
+    tc_split_operands_kernel<<<blocks_for(n_q * 32, 256), 256, 0, s>>>(
+        x, n_q, width, d, qrows, mean, scale, max_sq, true, (__half*)aq.ptr, qn2, slack2.ptr,
+        slack_d);
+    tc_split_operands_kernel<<<blocks_for(n_p * 32, 256), 256, 0, s>>>(
+        x, n_p, width, d, prows, mean, scale, max_sq, false, (__half*)bp.ptr, nullptr, nullptr,
+        nullptr);
   } else {
-    tc_operands_kernel<__half><<<blocks_for(n_q, 128), 128, 0, s>>>(
-        x, n_q, width, d, qrows, mean, scale, u, eta, max_sq, true, (__half*)aq.ptr, qn2,
-        slack2.ptr, slack_d);
-    tc_operands_kernel<__half><<<blocks_for(n_p, 128), 128, 0, s>>>(
-        x, n_p, width, d, prows, mean, scale, u, eta, max_sq, false, (__half*)bp.ptr, nullptr,
-        nullptr, nullptr);
+    const double u = bf16 ? 0x1p-8 : 0x1p-11;
+    const double eta = bf16 ? 0x1p-134 : 0x1p-25;
+    if (bf16) {
+      tc_operands_kernel<__nv_bfloat16><<<blocks_for(n_q, 128), 128, 0, s>>>(
+          x, n_q, width, d, qrows, mean, scale, u, eta, max_sq, true, (__nv_bfloat16*)aq.ptr,
+          qn2, slack2.ptr, slack_d);
+      tc_operands_kernel<__nv_bfloat16><<<blocks_for(n_p, 128), 128, 0, s>>>(
+          x, n_p, width, d, prows, mean, scale, u, eta, max_sq, false, (__nv_bfloat16*)bp.ptr,
+          nullptr, nullptr, nullptr);
+    } else {
+      tc_operands_kernel<__half><<<blocks_for(n_q, 128), 128, 0, s>>>(
+          x, n_q, width, d, qrows, mean, scale, u, eta, max_sq, true, (__half*)aq.ptr, qn2,
+          slack2.ptr, slack_d);
+      tc_operands_kernel<__half><<<blocks_for(n_p, 128), 128, 0, s>>>(
+          x, n_p, width, d, prows, mean, scale, u, eta, max_sq, false, (__half*)bp.ptr, nullptr,
+          nullptr, nullptr);
+    }
   }
   KG_LAUNCH_CHECK();
   if (trace) trace->mark("filter operands");
-  CUtensorMap mq = tile_map(aq.ptr, n_q, bf16), mp = tile_map(bp.ptr, n_p, bf16);
-  static std::once_flag attr;
-  std::call_once(attr, [] {
-    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<16>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes));
-    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<32>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes));
-    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<0>,
-                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemBytes));
-  });
+  CUtensorMap mq = tile_map(aq.ptr, n_q, bf16, width_op), mp = tile_map(bp.ptr, n_p, bf16, width_op);
   DeviceBuffer<int> err(1, s);
   err.zero();
   scan.qn2 = qn2;
   scan.s2 = scale * scale;
-  uint64_t n_qblocks = (n_q + kTcQueries - 1) / kTcQueries;
-  unsigned grid = (unsigned)std::min<uint64_t>(n_qblocks, (uint64_t)ctx->sm_count);
-  uint32_t idesc = idesc_f32acc(bf16 ? 1u : 0u, 128, kTcPoints);
-  auto kernel = k <= 16 ? knn_filter_tc_kernel<16>
-                : k <= 32 ? knn_filter_tc_kernel<32> : knn_filter_tc_kernel<0>;
-  kernel<<<grid, kTcThreads, kTcSmemBytes, s>>>(mq, mp, scan, k, slack2.ptr, idesc, cap, cand_key,
-                                                cand_row, cand_count, threshold, err.ptr);
+  const uint64_t n_qblocks = (n_q + kTcQueries - 1) / kTcQueries;
+  const unsigned grid = (unsigned)std::min<uint64_t>(n_qblocks, (uint64_t)ctx->sm_count);
+  const uint32_t idesc = idesc_f32acc(bf16 ? 1u : 0u, 128, kTcPoints);
+  const int kr = k <= 16 ? 16 : k <= 32 ? 32 : 0;
+  auto launch = kr == 16 ? (split ? launch_filter<16, 2> : launch_filter<16, 1>)
+                : kr == 32 ? (split ? launch_filter<32, 2> : launch_filter<32, 1>)
+                           : (split ? launch_filter<0, 2> : launch_filter<0, 1>);
+  launch(grid, s, mq, mp, scan, k, slack2.ptr, idesc, cap, cand_key, cand_row, cand_count,
+         threshold, err.ptr);
   KG_LAUNCH_CHECK();
   if (trace) trace->mark("filter kernel");
   int h_err = 0;

@@ -9,10 +9,17 @@ namespace kg {
 
 constexpr uint32_t kTcCap = 512;             // candidate slots per query
 constexpr uint32_t kTcCandidateLimit = 256;  // candidates kept after a compaction, at most
-constexpr uint32_t kTcQueryBlock = 256;      // query slots per block of the filter
+constexpr uint32_t kTcQueryBlock = 256;      // query slots per block of the fp16/bf16 filter
+
+// The filter's operands: fp16 or bf16 (one 64-wide row: the components and the norm), or
+// split (fp16 hi and lo parts, three products; a slack 2^5 times smaller than fp16's).
+enum class FilterKind { Fp16, Bf16, Split };
+
+// Query slots per block of the filter of this kind (the blocks tile lists are built for).
+uint32_t filter_query_block(FilterKind kind);
 
 // What one filter launch scans. Query slot q is row qrows[q] of x, point slot p row
-// prows[p]; each block of 256 query slots scans its list of point tiles (128 slots) in
+// prows[p]; each block of query slots (filter_query_block) scans its list of point tiles (128 slots) in
 // order, or every tile from its own when list_tiles is NULL, skipping a listed tile whose
 // bound (list_lb2, scaled squared distance) exceeds every query's threshold + s^2 |q|^2.
 struct FilterScan {
@@ -40,9 +47,10 @@ double tc_scale(const float* x, uint64_t n, uint32_t width, uint32_t d, const do
 // scale^2: the approximate squared distance is key / scale^2 + qn2.
 void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint32_t width, uint32_t d,
                const uint32_t* qrows, const uint32_t* prows, FilterScan scan,
-               const double* mean, double scale, const double* max_sq, bool bf16, uint32_t k,
-               uint32_t cap, float* cand_key, uint32_t* cand_row, uint32_t* cand_count,
-               float* threshold, double* qn2, double* slack_d, Trace* trace = nullptr);
+               const double* mean, double scale, const double* max_sq, FilterKind kind,
+               uint32_t k, uint32_t cap, float* cand_key, uint32_t* cand_row,
+               uint32_t* cand_count, float* threshold, double* qn2, double* slack_d,
+               Trace* trace = nullptr);
 
 void max_kernel_launch(const double* v, uint64_t n, double* out, cudaStream_t s);
 

@@ -386,8 +386,8 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
     // 5. The restricted exact search.
     auto t_search = now();
     uint64_t fallback_rows = 0, scanned_tiles = 0;
-    PlanBuilder plan = [&](const float*, uint64_t nn, uint32_t, uint32_t, double, ScanPlan& sp,
-                           Trace& tr) {
+    PlanBuilder plan = [&](const float*, uint64_t nn, uint32_t, uint32_t, double,
+                           uint32_t qblock, ScanPlan& sp, Trace& tr) {
       DeviceBuffer<uint32_t> key(nn, s), iota(nn, s), key_sorted;
       DeviceBuffer<uint8_t> fallback(nn, s);
       // Points: by top part.
@@ -412,7 +412,7 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
                                                          sp.q_point.ptr);
       KG_LAUNCH_CHECK();
       // The blocks' tile lists (count, scan, fill).
-      const uint64_t n_blocks = (nn + kTcQueryBlock - 1) / kTcQueryBlock;
+      const uint64_t n_blocks = (nn + qblock - 1) / qblock;
       const uint32_t n_tiles = (uint32_t)((nn + 127) / 128);
       const size_t smem = (size_t)((n_tiles + 31) / 32) * 4;
       if (smem > 200 * 1024)
@@ -425,7 +425,7 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
       DeviceBuffer<uint64_t> len(n_blocks + 1, s);
       len.zero();
       probe_tiles_kernel<<<(unsigned)n_blocks, kProbeThreads, smem, s>>>(
-          sp.qrows.ptr, nn, top.ptr, probe, fallback.ptr, part_start.ptr, n_tiles, kTcQueryBlock,
+          sp.qrows.ptr, nn, top.ptr, probe, fallback.ptr, part_start.ptr, n_tiles, qblock,
           len.ptr, nullptr, nullptr);
       KG_LAUNCH_CHECK();
       sp.list_off.alloc(n_blocks + 1, s);
@@ -443,7 +443,7 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
       scanned_tiles = total;
       sp.list_tiles.alloc(std::max<uint64_t>(total, 1), s);
       probe_tiles_kernel<<<(unsigned)n_blocks, kProbeThreads, smem, s>>>(
-          sp.qrows.ptr, nn, top.ptr, probe, fallback.ptr, part_start.ptr, n_tiles, kTcQueryBlock,
+          sp.qrows.ptr, nn, top.ptr, probe, fallback.ptr, part_start.ptr, n_tiles, qblock,
           len.ptr, sp.list_off.ptr, sp.list_tiles.ptr);
       KG_LAUNCH_CHECK();
       tr.mark("probe lists");

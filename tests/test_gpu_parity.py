@@ -217,10 +217,11 @@ def test_knn_clusters_ties_and_duplicates(ctx):
     _graph_equal(K.neighbors(pts, 31, ctx=ctx), O.neighbors(pts, 31))
 
 
-@pytest.mark.parametrize("candidate_filter", ["fp16", "bf16", "simt"])
+@pytest.mark.parametrize("candidate_filter", ["fp16", "split", "bf16", "simt"])
 def test_knn_every_filter_gives_the_exact_graph(ctx, monkeypatch, candidate_filter):
-    # The tensor-core filter in fp16 or bf16 (wider slack, more candidates) and the
-    # SIMT f32 filter all end in the same exact ranking.
+    # The tensor-core filter in fp16, split fp16 (hi and lo parts, a tighter slack) or
+    # bf16 (wider slack, more candidates) and the SIMT f32 filter all end in the same
+    # exact ranking.
     monkeypatch.setenv("KYTO_GPU_KNN_FILTER", candidate_filter)
     pts, _ = synthetic.gaussian_mixture(5000, 50, 30, seed=11, device="cpu")
     pts[40:60] = pts[3]
@@ -229,11 +230,31 @@ def test_knn_every_filter_gives_the_exact_graph(ctx, monkeypatch, candidate_filt
     assert gpu.stats.candidates >= 5000 * 15
 
 
-def test_knn_tensor_core_tiles_past_the_end(ctx):
-    # n not a multiple of the 128-point tile or the 256-query block; one CTA per SM
-    # walks several query blocks (more blocks than SMs).
+@pytest.mark.parametrize("candidate_filter", ["fp16", "split"])
+def test_knn_tensor_core_tiles_past_the_end(ctx, monkeypatch, candidate_filter):
+    # n not a multiple of the 128-point tile or the query block; one CTA per SM walks
+    # several query blocks (more blocks than SMs).
+    monkeypatch.setenv("KYTO_GPU_KNN_FILTER", candidate_filter)
     pts, _ = synthetic.gaussian_mixture(148 * 256 + 77, 12, 25, seed=12, device="cpu")
     _graph_equal(K.neighbors(pts, 10, ctx=ctx), O.neighbors(pts, 10))
+
+
+def test_knn_split_filter_keeps_tight_clusters_off_the_full_search(ctx, monkeypatch):
+    # Components with sigma 0.2 hold hundreds of points inside fp16's slack (2^-9 of
+    # |q| R), so their queries overflow the candidate slots and search every row; the
+    # split operands' slack (about 2^-14 of |q| R) keeps them near k. Same graph.
+    pts, _ = synthetic.gaussian_mixture(20_000, 50, 40, seed=13, device="cpu")
+    ref = O.neighbors(pts, 15)
+    stats = {}
+    for f in ("fp16", "split"):
+        monkeypatch.setenv("KYTO_GPU_KNN_FILTER", f)
+        g = K.neighbors(pts, 15, ctx=ctx)
+        _graph_equal(g, ref)
+        stats[f] = g.stats
+    assert stats["fp16"].rows_full > 500, stats["fp16"].rows_full
+    assert stats["split"].rows_full * 20 <= stats["fp16"].rows_full, (
+        stats["split"].rows_full, stats["fp16"].rows_full)
+    assert stats["split"].candidates < stats["fp16"].candidates
 
 
 @pytest.mark.parametrize("n_neighbors,n_components", [(2, None), (16, 7), (64, 1)])

@@ -69,7 +69,9 @@ def _recall(graph: K.Graph, exact: K.Graph) -> float:
     return hits / b.size
 
 
-def test_learned_search_recall_and_what_training_gains():
+@pytest.mark.parametrize("candidate_filter", ["fp16", "split"])
+def test_learned_search_recall_and_what_training_gains(monkeypatch, candidate_filter):
+    monkeypatch.setenv("KYTO_GPU_KNN_FILTER", candidate_filter)
     x, _ = synthetic.gaussian_mixture(60_000, dim=50, n_components=60, seed=3, device="cpu")
     x = np.ascontiguousarray(x, dtype=np.float32)
     ctx = K.Context(0)
@@ -95,7 +97,9 @@ def test_learned_search_recall_and_what_training_gains():
     assert s1.scanned_tiles < 0.5 * n_tiles * n_blocks
 
 
-def test_confidence_above_one_falls_back_to_the_exact_graph():
+@pytest.mark.parametrize("candidate_filter", ["fp16", "split"])
+def test_confidence_above_one_falls_back_to_the_exact_graph(monkeypatch, candidate_filter):
+    monkeypatch.setenv("KYTO_GPU_KNN_FILTER", candidate_filter)
     x, _ = synthetic.gaussian_mixture(5_000, dim=20, n_components=10, seed=4, device="cpu")
     x = np.ascontiguousarray(x, dtype=np.float32)
     ctx = K.Context(0)
