@@ -162,8 +162,10 @@ def run_step(args, ctx, indptr, idx, vals, out, host: bool):
     return stats
 
 
-def cpu_baseline(args, x, vals, embedding) -> dict:
-    """kyto's CPU path (the oracle's C++ restatement) on a bounded sample."""
+def cpu_baseline(args, x, vals, embedding, ctx) -> dict:
+    """kyto's CPU path (the oracle's C++ restatement) on a bounded sample, and the
+    device PCA of the same sample against it (singular values, principal angles)."""
+    import kyto_b200 as K
     from oracle import oracle as O
 
     threads = O.max_threads()
@@ -171,8 +173,18 @@ def cpu_baseline(args, x, vals, embedding) -> dict:
     e = int(x.indptr[s])
     sub = O.Csr(x.indptr[: s + 1], x.indices[:e], vals[:e], args.genes)
     t0 = time.perf_counter()
-    O.pca(sub, args.components, 0)
+    ref = O.pca(sub, args.components, 0)
     t_pca = time.perf_counter() - t0
+    dev = K.pca(sub.indptr, sub.indices, sub.values, args.genes, args.components, seed=0,
+                ctx=ctx)
+    # Singular values sigma_i = sqrt(variance_i (n - 1)): relative error of the device's
+    # against the oracle's (f64 dense steps); the subspace's largest principal angle.
+    sv_err = float(np.max(np.abs(np.sqrt(dev.variance) - np.sqrt(ref.variance))
+                          / np.sqrt(ref.variance)))
+    qa, _ = np.linalg.qr(dev.loadings.astype(np.float64))
+    qb, _ = np.linalg.qr(ref.loadings.astype(np.float64))
+    cosines = np.linalg.svd(qa.T @ qb, compute_uv=False)
+    angle = float(np.arccos(np.clip(cosines.min(), -1.0, 1.0)))
     q = min(args.cpu_knn_queries, args.cells)
     t0 = time.perf_counter()
     O.knn_exact_sample(embedding, args.neighbors, 0, q)
@@ -185,6 +197,9 @@ def cpu_baseline(args, x, vals, embedding) -> dict:
                    f"{q:,} query cells against all {args.cells:,} ({t_knn:.2f} s); "
                    f"cells/s = 1/(PCA s per cell + kNN s per query)"),
         "pca_s_per_cell": t_pca / s, "knn_s_per_query": t_knn / q,
+        "pca_accuracy": {"cells": s, "singular_value_max_rel_err": sv_err,
+                         "largest_principal_angle_rad": angle,
+                         "against": "f64 oracle (kyto's CPU PCA restated) on the same sample"},
     }
 
 
@@ -296,7 +311,7 @@ def main() -> int:
         sess.run()
         emb = sess.results().embedding
         sess.close()
-        cpu = cpu_baseline(args, x, vals, emb)
+        cpu = cpu_baseline(args, x, vals, emb, ctx)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world,

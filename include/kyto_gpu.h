@@ -58,6 +58,8 @@ typedef struct kg_pca kg_pca;
 /* Open device `device` (a CUDA ordinal). Replaces DeviceKernels::open
  * (crates/kyto-gpu/src/launch.rs:81-93). */
 KG_API kg_status kg_open(int device, kg_ctx** out);
+/* Close a context; every PCA session begun on it must be freed first (a freed session
+ * returns its stream and solver handles to the context for the next session). */
 KG_API void kg_close(kg_ctx* ctx);
 
 /* The last error's message, NUL-terminated into buf (truncated to len); returns the
@@ -198,8 +200,6 @@ KG_API kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t n_ro
                        uint64_t* indptr, uint32_t* indices, float* distances,
                        kg_knn_stats* stats);
 
-/* ---------------------------------------------------------------- diagnostics ----- */
-
 /* ------------------------------------------------------- learned-partition kNN ---- */
 
 /* No counterpart in kyto: the north star's learned form. A BF16 MLP (n_components ->
@@ -256,6 +256,8 @@ KG_API kg_status kg_learned_gradients(kg_ctx* ctx, uint32_t din, uint32_t hidden
                                       uint32_t rows, const uint32_t* labels,
                                       uint32_t n_labels, float* grads, float* row_loss,
                                       float* logits);
+
+/* ---------------------------------------------------------------- diagnostics ----- */
 
 /* Kernels of this library launched since it was loaded (library calls such as cuBLAS
  * not counted): lets a benchmark state how many of its own kernels a timed region ran.

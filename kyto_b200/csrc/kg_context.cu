@@ -54,6 +54,12 @@ void kg_close(kg_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  for (const kg_ctx::SessionRes& r : ctx->free_res) {
+    cudaStreamSynchronize(r.stream);
+    cusolverDnDestroy(r.cusolver);
+    cublasDestroy(r.cublas);
+    cudaStreamDestroy(r.stream);
+  }
   if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
   if (ctx->cublas) cublasDestroy(ctx->cublas);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);

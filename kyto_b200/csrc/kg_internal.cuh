@@ -153,6 +153,16 @@ struct kg_ctx {
   cublasHandle_t cublas = nullptr;
   cusolverDnHandle_t cusolver = nullptr;
   std::mutex handles;  // cuBLAS/cuSOLVER handles are bound to one stream at a time
+  // Session resources (a stream with its own cuBLAS and cuSOLVER handles) returned by
+  // finished PCA sessions, reused by the next: creating and destroying the handles
+  // (and their workspaces) costs far more than a session's dense steps.
+  struct SessionRes {
+    cudaStream_t stream = nullptr;
+    cublasHandle_t cublas = nullptr;
+    cusolverDnHandle_t cusolver = nullptr;
+  };
+  std::mutex res_mu;
+  std::vector<SessionRes> free_res;
   const volatile int32_t* cancel = nullptr;
   std::atomic<uint64_t> done{0}, total{0};
   int sm_count = 0;

@@ -423,12 +423,11 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
     }
   } else {
     // ------------------------------------------------------------ epilogue --------
-    // Per tile: the 128 keys come out of TMEM 64 columns at a time and only their
-    // minimum per 32-column chunk is kept (few registers: no spills in the hot loop).
-    // A chunk whose minimum reaches the threshold (rare once it has fallen) is read
-    // again by the whole warp (tcgen05.ld is warp-wide) and its passing keys offered.
-    // The threshold and overflow flag stay in registers; after offers the warp
-    // publishes its largest threshold + s^2 |q|^2 for the producer's bound checks.
+    // Per tile: the 128 keys come out of TMEM into registers and the accumulator is
+    // released; a 32-key chunk whose minimum reaches the threshold (rare once it has
+    // fallen) has its passing keys offered by its lane alone. The threshold and
+    // overflow flag stay in registers; after offers the warp publishes its largest
+    // threshold + s^2 |q|^2 for the producer's bound checks.
     const uint32_t half = (uint32_t)warp >> 2, quad = (uint32_t)warp & 3;
     float* my = sm.scratch[threadIdx.x];
     float local_smallest[KR == 0 ? kMaxK : 1];
@@ -465,35 +464,29 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           break;
         }
         const uint32_t base = tmem + ((quad * 32u) << 16) + ab * 256u + half * 128u;
-        float mins[kTcPoints / 32];
+        // All 128 keys into registers with one wait; the accumulator goes back to the
+        // MMA warp at once.
+        uint32_t r[kTcPoints / 32][32];
 #pragma unroll
-        for (int hf = 0; hf < kTcPoints / 64; ++hf) {
-          uint32_t r0[32], r1[32];
-          tmem_ld_32(base + hf * 64u, r0);
-          tmem_ld_32(base + hf * 64u + 32u, r1);
-          tmem_wait_ld();
-          mins[2 * hf] = min_of_32(r0);
-          mins[2 * hf + 1] = min_of_32(r1);
-        }
+        for (int c = 0; c < kTcPoints / 32; ++c) tmem_ld_32(base + c * 32u, r[c]);
+        tmem_wait_ld();
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.tmem_empty[ab]);
         uint32_t hits = 0;
 #pragma unroll
-        for (int c = 0; c < kTcPoints / 32; ++c) hits |= (live && mins[c] <= th ? 1u : 0u) << c;
-        uint32_t any = __reduce_or_sync(0xFFFFFFFFu, hits);
-        const bool offered = any != 0;
-#pragma unroll 1
-        while (any) {
-          const int c = __ffs(any) - 1;
-          any &= any - 1;
-          uint32_t r[32];
-          tmem_ld_32(base + c * 32u, r);
-          tmem_wait_ld();
+        for (int c = 0; c < kTcPoints / 32; ++c)
+          hits |= (live && min_of_32(r[c]) <= th ? 1u : 0u) << c;
+        const bool offered = __any_sync(0xFFFFFFFFu, hits != 0);
+        // Each lane offers its own passing keys, chunk by chunk in column order (the
+        // threshold only falls while they are offered), through its scratch row.
+#pragma unroll
+        for (int c = 0; c < kTcPoints / 32; ++c) {
           if (!((hits >> c) & 1u) || !live) continue;
-          // Only the keys at or under the threshold, in column order (the threshold
-          // only falls while they are offered).
           uint32_t mask = 0;
 #pragma unroll
           for (int j = 0; j < 32; ++j) {
-            const float key = __uint_as_float(r[j]);
+            const float key = __uint_as_float(r[c][j]);
             my[j] = key;
             mask |= (key <= th ? 1u : 0u) << j;
           }
@@ -503,9 +496,6 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           th = st.th;
           live = !st.overflowed;
         }
-        tc_fence_before();
-        __syncwarp();
-        if (lane == 0) mbar_arrive(&sm.tmem_empty[ab]);
         if (offered && scan.list_lb2) {
           // An overflowed query is searched in full later: it no longer bounds the scan.
           const float u = active && live ? round_up_f32d((double)th + s2qn2) : -INFINITY;

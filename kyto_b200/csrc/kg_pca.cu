@@ -970,8 +970,6 @@ struct kg_pca {
 
   ~kg_pca() {
     if (stream) cudaStreamSynchronize(stream);
-    if (cusolver) cusolverDnDestroy(cusolver);
-    if (cublas) cublasDestroy(cublas);
     gene_map.reset();
     set_genes.reset();
     indptr.reset();
@@ -981,9 +979,16 @@ struct kg_pca {
     embedding.reset();
     loadings.reset();
     means.reset();
-    if (stream) {
-      cudaStreamSynchronize(stream);
-      cudaStreamDestroy(stream);
+    if (stream) cudaStreamSynchronize(stream);
+    // The stream and handles go back to the context for the next session (a stream
+    // with all three: they were made together and stay bound to each other).
+    if (ctx && stream && cublas && cusolver) {
+      std::lock_guard<std::mutex> lock(ctx->res_mu);
+      ctx->free_res.push_back({stream, cublas, cusolver});
+    } else {
+      if (cusolver) cusolverDnDestroy(cusolver);
+      if (cublas) cublasDestroy(cublas);
+      if (stream) cudaStreamDestroy(stream);
     }
   }
 
@@ -1471,11 +1476,25 @@ kg_status kg_pca_begin(kg_ctx* ctx, const kg_pca_params* params, kg_pca** out) {
     auto* p = new kg_pca();
     try {
       p->ctx = ctx;
-      KG_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
-      KG_CUBLAS(cublasCreate(&p->cublas));
-      KG_CUBLAS(cublasSetStream(p->cublas, p->stream));
-      KG_CUSOLVER(cusolverDnCreate(&p->cusolver));
-      KG_CUSOLVER(cusolverDnSetStream(p->cusolver, p->stream));
+      {
+        std::lock_guard<std::mutex> lock(ctx->res_mu);
+        if (!ctx->free_res.empty()) {
+          const kg_ctx::SessionRes r = ctx->free_res.back();
+          ctx->free_res.pop_back();
+          p->stream = r.stream;
+          p->cublas = r.cublas;
+          p->cusolver = r.cusolver;
+        }
+      }
+      if (!p->stream) KG_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+      if (!p->cublas) {
+        KG_CUBLAS(cublasCreate(&p->cublas));
+        KG_CUBLAS(cublasSetStream(p->cublas, p->stream));
+      }
+      if (!p->cusolver) {
+        KG_CUSOLVER(cusolverDnCreate(&p->cusolver));
+        KG_CUSOLVER(cusolverDnSetStream(p->cusolver, p->stream));
+      }
       p->k = params->n_components;
       p->stream_genes = params->n_genes;
       p->seed = params->seed;
