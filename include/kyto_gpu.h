@@ -200,6 +200,52 @@ KG_API kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t n_ro
                        uint64_t* indptr, uint32_t* indices, float* distances,
                        kg_knn_stats* stats);
 
+/* Exact kNN of a batch of samples in one search (the north star's batching form): sample
+ * s is rows [sample_rows[s], sample_rows[s + 1]) of `embedding` (sample_rows: host array
+ * of n_samples + 1 offsets from 0 to n_rows); each row gets the n_neighbors - 1 nearest
+ * rows of its own sample, exactly as kg_knn_exact on that sample alone. One filter launch
+ * covers every sample (each block of query rows scans only its samples' point tiles).
+ * Outputs: the samples' CSR graphs one after another: sample s's indptr (its rows + 1
+ * entries, from 0) at indptr + sample_rows[s] + s (n_rows + n_samples entries in all),
+ * its columns (numbered from its own first row) and distances at
+ * sample_rows[s] * (n_neighbors - 1). */
+KG_API kg_status kg_knn_batch(kg_ctx* ctx, const float* embedding, uint64_t n_rows,
+                              uint32_t width, uint32_t n_components, uint32_t n_neighbors,
+                              const uint64_t* sample_rows, uint32_t n_samples,
+                              uint64_t* indptr, uint32_t* indices, float* distances,
+                              kg_knn_stats* stats);
+
+/* One sample of a batch: a CSR block (as kg_pca_push_block takes it). */
+typedef struct kg_batch_sample {
+  const uint64_t* indptr;
+  const uint32_t* indices;
+  const void* values;
+  kg_dtype dtype;
+  uint32_t reserved;
+  uint64_t n_rows;
+} kg_batch_sample;
+
+typedef struct kg_batch_stats {
+  double pca_ms;           /* all samples' PCA (host wall time) */
+  double knn_ms;           /* the batched search and its graphs */
+  uint32_t workers;        /* PCA sessions run at once */
+  uint32_t reserved;
+  kg_knn_stats knn;        /* the batched search's counters */
+} kg_batch_stats;
+
+/* The batching form end to end: kyto's pca(n_components, seed) and neighbors(n_neighbors)
+ * on each of n_samples samples of uneven sizes (each as kg_pca_begin/push/run and
+ * kg_knn_exact on that sample alone would give it). The samples' PCA sessions run
+ * concurrently, each on its own stream with its own solver handles, so the GPU
+ * interleaves the small samples' kernels; the embeddings are then searched in one
+ * batched kNN launch (kg_knn_batch). Outputs: embedding (all samples' rows one after
+ * another, n_components each, f32), variance (n_samples x n_components), and the
+ * graphs laid out as kg_knn_batch's. */
+KG_API kg_status kg_pca_knn_batch(kg_ctx* ctx, const kg_pca_params* params, uint32_t n_samples,
+                                  const kg_batch_sample* samples, uint32_t n_neighbors,
+                                  float* embedding, double* variance, uint64_t* indptr,
+                                  uint32_t* indices, float* distances, kg_batch_stats* stats);
+
 /* ------------------------------------------------------- learned-partition kNN ---- */
 
 /* No counterpart in kyto: the north star's learned form. A BF16 MLP (n_components ->
@@ -209,7 +255,10 @@ KG_API kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t n_ro
  * shuffles of `batch` rows); every row then gets its n_probe most probable parts, lives
  * in the most probable one, and is searched exactly (kg_knn_exact's filter and re-rank)
  * among the rows of the parts its block of 256 query rows probes, or against every row
- * when the probed parts' summed probability is below `confidence`. */
+ * when the probed parts' summed probability is below `confidence`. That probability
+ * is the softmax at a temperature calibrated on the sample (the one whose confidence
+ * best predicts, by log loss, that a sample row's exact neighbours live in the parts it
+ * probes). */
 typedef struct kg_learned_params {
   uint32_t n_parts;        /* partitions (>= 2) */
   uint32_t hidden;         /* hidden width */
@@ -232,7 +281,7 @@ typedef struct kg_learned_stats {
   double index_ms;         /* every row's parts */
   double search_ms;        /* the restricted exact search and the graph */
   float final_loss;        /* mean cross-entropy of the last training batch */
-  float reserved;
+  float temperature;       /* the confidence's calibrated temperature (logits scale) */
 } kg_learned_stats;
 
 /* The graph (as kg_knn_exact's: CSR, rows sorted by column, f32 distances) of each

@@ -39,7 +39,8 @@ EXPORTS = (
     "kg_open", "kg_close", "kg_last_error", "kg_set_cancel_flag", "kg_progress",
     "kg_normalize_log1p", "kg_hvg_moments", "kg_hvg_moments_noalloc", "kg_hvg_seurat",
     "kg_pca_begin", "kg_pca_push_block", "kg_pca_run", "kg_pca_results", "kg_pca_info",
-    "kg_pca_embedding_device", "kg_pca_free", "kg_knn_exact", "kg_knn_learned",
+    "kg_pca_embedding_device", "kg_pca_free", "kg_pca_knn_batch", "kg_knn_exact",
+    "kg_knn_batch", "kg_knn_learned",
     "kg_learned_layout", "kg_learned_gradients", "kg_diag_kernel_launches",
 )
 
@@ -62,6 +63,36 @@ class _PcaParams(ctypes.Structure):
         ("target_sum", ctypes.c_double),
         ("log1p", ctypes.c_int32),
         ("reserved", ctypes.c_uint32),
+    ]
+
+
+class KnnStats(ctypes.Structure):
+    _fields_ = [
+        ("candidates", ctypes.c_uint64),
+        ("rows_full", ctypes.c_uint64),
+        ("filter_ms", ctypes.c_double),
+        ("rank_ms", ctypes.c_double),
+    ]
+
+
+class _BatchSample(ctypes.Structure):
+    _fields_ = [
+        ("indptr", ctypes.c_void_p),
+        ("indices", ctypes.c_void_p),
+        ("values", ctypes.c_void_p),
+        ("dtype", ctypes.c_int32),
+        ("reserved", ctypes.c_uint32),
+        ("n_rows", ctypes.c_uint64),
+    ]
+
+
+class BatchStats(ctypes.Structure):
+    _fields_ = [
+        ("pca_ms", ctypes.c_double),
+        ("knn_ms", ctypes.c_double),
+        ("workers", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+        ("knn", KnnStats),
     ]
 
 
@@ -98,16 +129,7 @@ class LearnedStats(ctypes.Structure):
         ("index_ms", ctypes.c_double),
         ("search_ms", ctypes.c_double),
         ("final_loss", ctypes.c_float),
-        ("reserved", ctypes.c_float),
-    ]
-
-
-class KnnStats(ctypes.Structure):
-    _fields_ = [
-        ("candidates", ctypes.c_uint64),
-        ("rows_full", ctypes.c_uint64),
-        ("filter_ms", ctypes.c_double),
-        ("rank_ms", ctypes.c_double),
+        ("temperature", ctypes.c_float),
     ]
 
 
@@ -139,6 +161,10 @@ def library() -> ctypes.CDLL:
             "kg_pca_info": [P, P, P, P],
             "kg_pca_embedding_device": [P, ctypes.POINTER(P)],
             "kg_knn_exact": [P, P, U64, U32, U32, U32, P, P, P, ctypes.POINTER(KnnStats)],
+            "kg_knn_batch": [P, P, U64, U32, U32, U32, P, U32, P, P, P,
+                             ctypes.POINTER(KnnStats)],
+            "kg_pca_knn_batch": [P, ctypes.POINTER(_PcaParams), U32, ctypes.POINTER(_BatchSample),
+                                 U32, P, P, P, P, P, ctypes.POINTER(BatchStats)],
             "kg_knn_learned": [P, P, U64, U32, U32, U32, ctypes.POINTER(LearnedParams), P, P, P,
                                ctypes.POINTER(LearnedStats)],
             "kg_learned_layout": [U32, U32, U32, P, P],
@@ -420,6 +446,77 @@ def neighbors(embedding, n_neighbors: int = 15, n_components: int | None = None,
                                   int(n_neighbors), _ptr(indptr), _ptr(indices), _ptr(dist),
                                   ctypes.byref(stats)))
     return Graph(indptr, indices, dist, stats)
+
+
+def neighbors_batch(embeddings, n_neighbors: int = 15, n_components: int | None = None,
+                    ctx: Context | None = None) -> list[Graph]:
+    """Exact ``neighbors`` of every sample of a batch in one search (kg_knn_batch): one
+    graph per sample, each equal to ``neighbors`` of that sample alone."""
+    ctx = ctx or default_context()
+    mats = [np.ascontiguousarray(e, dtype=np.float32) for e in embeddings]
+    if not mats:
+        raise ValueError("neighbors_batch: no samples")
+    width = mats[0].shape[1]
+    sizes = np.array([m.shape[0] for m in mats], dtype=np.uint64)
+    first = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    x = np.ascontiguousarray(np.concatenate(mats, axis=0))
+    n, S = int(first[-1]), len(mats)
+    k = int(n_neighbors) - 1
+    indptr = np.empty(n + S, dtype=np.uint64)
+    indices = np.empty(max(n * k, 0), dtype=np.uint32)
+    dist = np.empty(max(n * k, 0), dtype=np.float32)
+    stats = KnnStats()
+    _check(library().kg_knn_batch(ctx.handle, _ptr(x), n, width,
+                                  0 if n_components is None else int(n_components),
+                                  int(n_neighbors), _ptr(first), S, _ptr(indptr),
+                                  _ptr(indices), _ptr(dist), ctypes.byref(stats)))
+    out = []
+    for s in range(S):
+        a, b = int(first[s]), int(first[s + 1])
+        out.append(Graph(indptr[a + s:b + s + 1].copy(), indices[a * k:b * k].copy(),
+                         dist[a * k:b * k].copy(), stats))
+    return out
+
+
+def pca_neighbors_batch(samples, n_genes: int, n_components: int = 30, n_neighbors: int = 15,
+                        seed: int = 0, target_sum: float | None = None, log1p: bool = False,
+                        ctx: Context | None = None):
+    """The batching form (kg_pca_knn_batch): ``pca`` then exact ``neighbors`` on each
+    sample, every sample a CSR block ``(indptr, indices, values)``. Returns one
+    ``(PcaResult, Graph)`` per sample (loadings and means not returned: None) and the
+    batch's counters."""
+    ctx = ctx or default_context()
+    keep = []
+    arr = (_BatchSample * len(samples))()
+    for i, (indptr, indices, values) in enumerate(samples):
+        indptr, indices = _u64(indptr), _u32(indices)
+        keep += [indptr, indices, values]
+        n_rows = (len(indptr) if isinstance(indptr, np.ndarray) else indptr.shape[0]) - 1
+        arr[i] = _BatchSample(_ptr(indptr), _ptr(indices), _ptr(values), _dtype_code(values), 0,
+                              n_rows)
+    sizes = [int(arr[i].n_rows) for i in range(len(samples))]
+    n, S, kc, k = sum(sizes), len(samples), int(n_components), int(n_neighbors) - 1
+    p = _PcaParams(kc, int(n_genes), int(seed), None,
+                   math.nan if target_sum is None else float(target_sum), int(bool(log1p)), 0)
+    emb = np.empty((n, kc), dtype=np.float32)
+    var = np.empty((S, kc), dtype=np.float64)
+    indptr = np.empty(n + S, dtype=np.uint64)
+    indices = np.empty(max(n * k, 0), dtype=np.uint32)
+    dist = np.empty(max(n * k, 0), dtype=np.float32)
+    stats = BatchStats()
+    _check(library().kg_pca_knn_batch(ctx.handle, ctypes.byref(p), S, arr, int(n_neighbors),
+                                      _ptr(emb), _ptr(var), _ptr(indptr), _ptr(indices),
+                                      _ptr(dist), ctypes.byref(stats)))
+    out, a = [], 0
+    for s, m in enumerate(sizes):
+        b = a + m
+        res = PcaResult(embedding=emb[a:b].copy(), loadings=None, variance=var[s].copy(),
+                        variance_ratio=None, means=None, passes_run=0)
+        g = Graph(indptr[a + s:b + s + 1].copy(), indices[a * k:b * k].copy(),
+                  dist[a * k:b * k].copy(), stats.knn)
+        out.append((res, g))
+        a = b
+    return out, stats
 
 
 def neighbors_learned(embedding, n_neighbors: int = 15, n_components: int | None = None,

@@ -12,6 +12,7 @@
 //  3. full rows: flagged rows searched against every row with exact keys.
 // So every row is the CPU's brute-force row, bit for bit.
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 #include <cub/device/device_segmented_radix_sort.cuh>
 
 #include <algorithm>
@@ -148,21 +149,65 @@ __device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 10 bits -> every t
   return v;
 }
 
-__global__ void morton_kernel(const float* x, uint64_t n, uint32_t width, uint32_t dims,
-                              const double* mean, const float* lo_hi, uint32_t* key,
-                              uint32_t* row) {
-  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (r >= n) return;
+__device__ __forceinline__ uint32_t morton_code(const float* xr, uint32_t dims,
+                                                const double* mean, const float* lo_hi) {
   uint32_t code = 0;
   for (uint32_t j = 0; j < dims; ++j) {
-    float v = (float)((double)x[r * width + j] - mean[j]);
+    float v = (float)((double)xr[j] - mean[j]);
     float span = lo_hi[2 * j + 1] - lo_hi[2 * j];
     float t = span > 0.0f ? (v - lo_hi[2 * j]) / span : 0.0f;
     uint32_t q = (uint32_t)fminf(fmaxf(t * 1023.0f, 0.0f), 1023.0f);
     code |= spread3(q) << j;
   }
-  key[r] = code;
+  return code;
+}
+
+__global__ void morton_kernel(const float* x, uint64_t n, uint32_t width, uint32_t dims,
+                              const double* mean, const float* lo_hi, uint32_t* key,
+                              uint32_t* row) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  key[r] = morton_code(x + r * width, dims, mean, lo_hi);
   row[r] = (uint32_t)r;
+}
+
+// The batch's order key: the row's sample, then its Morton code.
+__global__ void batch_morton_kernel(const float* x, uint64_t n, uint32_t width, uint32_t dims,
+                                    const double* mean, const float* lo_hi,
+                                    const uint32_t* row_sample, unsigned long long* key,
+                                    uint32_t* row) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  key[r] = ((unsigned long long)row_sample[r] << 32) | morton_code(x + r * width, dims, mean, lo_hi);
+  row[r] = (uint32_t)r;
+}
+
+// Per query slot its sample (the batch's order is sample-major).
+__global__ void slot_sample_kernel(const uint32_t* qrows, const uint32_t* row_sample, uint64_t n,
+                                  uint32_t* slot_sample) {
+  uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (q < n) slot_sample[q] = row_sample[qrows[q]];
+}
+
+// A batch's tile lists: the block of query slots [qb * block, ...) scans the point tiles
+// of the samples it holds (a contiguous range, the samples being contiguous in slot
+// order), from its own tile on, wrapping inside the range. len pass (list NULL) or fill.
+__global__ void batch_lists_kernel(const uint32_t* slot_sample, const uint64_t* sample_first,
+                                   uint64_t n, uint32_t block, uint64_t n_blocks,
+                                   uint64_t* len, const uint64_t* off, uint32_t* list) {
+  const uint64_t qb = blockIdx.x;
+  if (qb >= n_blocks) return;
+  const uint64_t q0 = qb * block, q1 = (q0 + block < n ? q0 + block : n) - 1;
+  const uint64_t p0 = sample_first[slot_sample[q0]], p1 = sample_first[slot_sample[q1] + 1];
+  const uint32_t t0 = (uint32_t)(p0 / 128), t1 = (uint32_t)((p1 - 1) / 128);
+  const uint32_t count = t1 - t0 + 1;
+  if (!list) {
+    if (threadIdx.x == 0) len[qb] = count;
+    return;
+  }
+  const uint32_t own = min(max((uint32_t)(q0 / 128), t0), t1);
+  for (uint32_t i = threadIdx.x; i < count; i += blockDim.x)
+    list[off[qb] + i] = t0 + (own - t0 + i) % count;
 }
 
 // The rows in Morton order of their first (up to) three centred components: nearby rows
@@ -182,6 +227,28 @@ void spatial_order(const float* x, uint64_t n, uint32_t width, uint32_t d, const
   DeviceBuffer<unsigned char> scratch(temp, s);
   KG_CUDA(cub::DeviceRadixSort::SortPairs(scratch.ptr, temp, key.ptr, key_sorted.ptr, rows.ptr,
                                           perm.ptr, (int)n, 0, 30, s));
+}
+
+// The batch's rows sample by sample, each sample in Morton order: a query block's own
+// tiles hold its nearest points, and each sample's rows are one contiguous slot range.
+void batch_order(const float* x, uint64_t n, uint32_t width, uint32_t d, const double* mean,
+                 const float* lo_hi, const KnnBatch& batch, DeviceBuffer<uint32_t>& perm,
+                 cudaStream_t s) {
+  uint32_t dims = d < 3 ? d : 3;
+  DeviceBuffer<unsigned long long> key(n, s), key_sorted(n, s);
+  DeviceBuffer<uint32_t> rows(n, s);
+  batch_morton_kernel<<<blocks_for(n, 256), 256, 0, s>>>(x, n, width, dims, mean, lo_hi,
+                                                         batch.row_sample.ptr, key.ptr, rows.ptr);
+  KG_LAUNCH_CHECK();
+  perm.alloc(n, s);
+  int end_bit = 32;
+  while (end_bit < 64 && (1ull << (end_bit - 32)) < batch.first.size()) ++end_bit;
+  size_t temp = 0;
+  KG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, key.ptr, key_sorted.ptr, rows.ptr,
+                                          perm.ptr, (int)n, 0, end_bit, s));
+  DeviceBuffer<unsigned char> scratch(temp, s);
+  KG_CUDA(cub::DeviceRadixSort::SortPairs(scratch.ptr, temp, key.ptr, key_sorted.ptr, rows.ptr,
+                                          perm.ptr, (int)n, 0, end_bit, s));
 }
 
 // *out = the largest of v[0..n) (all >= 0), on the stream.
@@ -435,15 +502,22 @@ __global__ void rank_kernel(const float* __restrict__ x, uint32_t width, uint32_
 }
 
 // One CTA per flagged row: every other row's exact key, the k best by (key, row).
+// With a batch (row_sample), only the rows of the row's own sample.
 __global__ void full_rows_kernel(const float* __restrict__ x, uint64_t n, uint32_t width,
                                  uint32_t d, uint32_t k, const uint32_t* rows_list,
+                                 const uint32_t* row_sample, const uint64_t* sample_first,
                                  double* out_key, uint32_t* out_row) {
   uint64_t q = rows_list[blockIdx.x];
   const float* qrow = x + q * width;
   double keys[kMaxK];
   uint32_t idx[kMaxK];
   uint32_t len = 0;
-  for (uint64_t p = threadIdx.x; p < n; p += blockDim.x) {
+  uint64_t lo = 0, hi = n;
+  if (row_sample) {
+    lo = sample_first[row_sample[q]];
+    hi = sample_first[row_sample[q] + 1];
+  }
+  for (uint64_t p = lo + threadIdx.x; p < hi; p += blockDim.x) {
     if (p == q) continue;
     offer(keys, idx, len, k, exact_key(qrow, x + p * width, d), (uint32_t)p);
   }
@@ -530,7 +604,7 @@ struct Timer {
 // into out.key / out.row (n x k). `plan` chooses the tensor-core filter's scan (NULL:
 // the rows in a spatial order, each query block scanning every tile from its own).
 void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t d, uint32_t k,
-              const PlanBuilder* plan, KnnResult& out, Trace& trace) {
+              const PlanBuilder* plan, KnnResult& out, Trace& trace, const KnnBatch* batch) {
   cudaStream_t s = ctx->stream;
   DeviceBuffer<double> mean(d, s), squares(n, s), slack(n, s), largest(1, s);
   DeviceBuffer<float> rows(n * kDim, s), offsets(n, s), lo_hi(6, s);
@@ -558,6 +632,8 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
   const char* choice = std::getenv("KYTO_GPU_KNN_FILTER");
   std::string filter = choice ? choice : "fp16";
   bool tc = !brute && d + 3 <= 64 && (filter == "fp16" || filter == "bf16" || filter == "split");
+  if (batch && !brute && !tc)
+    fail(KG_ERR_INVALID, "batched neighbors: the tensor-core filter (at most 61 components)");
   const FilterKind kind = filter == "bf16"    ? FilterKind::Bf16
                           : filter == "split" ? FilterKind::Split
                                               : FilterKind::Fp16;
@@ -574,8 +650,40 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
     Timer tf(s);
     const double scale = tc_scale(x, n, width, d, mean.ptr, max_sq.ptr, s);
     ScanPlan sp;
+    DeviceBuffer<uint32_t> slot_sample;
     if (plan) {
       (*plan)(x, n, width, d, scale, filter_query_block(kind), sp, trace);
+    } else if (batch) {
+      // Samples one after another, each in Morton order; each query block scans the
+      // tiles of the samples it holds.
+      batch_order(x, n, width, d, mean.ptr, lo_hi.ptr, *batch, sp.qrows, s);
+      slot_sample.alloc(n, s);
+      slot_sample_kernel<<<blocks_for(n, 256), 256, 0, s>>>(sp.qrows.ptr, batch->row_sample.ptr,
+                                                            n, slot_sample.ptr);
+      KG_LAUNCH_CHECK();
+      const uint32_t qblock = filter_query_block(kind);
+      const uint64_t n_blocks = (n + qblock - 1) / qblock;
+      DeviceBuffer<uint64_t> len(n_blocks + 1, s);
+      len.zero();
+      batch_lists_kernel<<<(unsigned)n_blocks, 128, 0, s>>>(
+          slot_sample.ptr, batch->d_first.ptr, n, qblock, n_blocks, len.ptr, nullptr, nullptr);
+      KG_LAUNCH_CHECK();
+      sp.list_off.alloc(n_blocks + 1, s);
+      size_t temp = 0;
+      KG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, len.ptr, sp.list_off.ptr,
+                                            n_blocks + 1, s));
+      DeviceBuffer<unsigned char> scratch(temp, s);
+      KG_CUDA(cub::DeviceScan::ExclusiveSum(scratch.ptr, temp, len.ptr, sp.list_off.ptr,
+                                            n_blocks + 1, s));
+      uint64_t total = 0;
+      KG_CUDA(cudaMemcpyAsync(&total, sp.list_off.ptr + n_blocks, 8, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaStreamSynchronize(s));
+      sp.list_tiles.alloc(std::max<uint64_t>(total, 1), s);
+      batch_lists_kernel<<<(unsigned)n_blocks, 128, 0, s>>>(slot_sample.ptr, batch->d_first.ptr,
+                                                            n, qblock, n_blocks, len.ptr,
+                                                            sp.list_off.ptr, sp.list_tiles.ptr);
+      KG_LAUNCH_CHECK();
+      trace.mark("scan order");
     } else {
       // The rows sorted by a Morton code of their first three centred components, so
       // a query block's own tiles hold its nearest points and the scan starts there.
@@ -590,6 +698,10 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
     scan.list_lb2 = sp.list_lb2.ptr;
     scan.list_off = sp.list_off.ptr;
     scan.list_stride = sp.list_stride;
+    if (batch) {
+      scan.slot_sample = slot_sample.ptr;
+      scan.sample_first = batch->d_first.ptr;
+    }
     const uint32_t* prows = sp.prows.ptr ? sp.prows.ptr : sp.qrows.ptr;
     tc_filter(ctx, s, x, width, d, sp.qrows.ptr, prows, scan, mean.ptr, scale, max_sq.ptr,
               kind, k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
@@ -645,8 +757,9 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
     for (uint64_t a = 0; a < h_full; a += 65535) {
       check_cancel(ctx);
       unsigned blocks = (unsigned)std::min<uint64_t>(65535, h_full - a);
-      full_rows_kernel<<<blocks, kFullWarps * 32, 0, s>>>(x, n, width, d, k, list.ptr + a,
-                                                          out.key.ptr, out.row.ptr);
+      full_rows_kernel<<<blocks, kFullWarps * 32, 0, s>>>(
+          x, n, width, d, k, list.ptr + a, batch ? batch->row_sample.ptr : nullptr,
+          batch ? batch->d_first.ptr : nullptr, out.key.ptr, out.row.ptr);
       KG_LAUNCH_CHECK();
     }
     rank_ms += tr.stop_ms();
@@ -698,6 +811,37 @@ void check_finite(const float* x, uint64_t n, uint32_t width, uint32_t d, cudaSt
                              std::to_string(first % width) + " is not finite");
 }
 
+// A batch's graphs: sample s's CSR (indptr of n_s + 1 entries at indptr + first[s] + s,
+// columns relative to its first row) and entries at first[s] * k, rows sorted by column.
+__global__ void batch_graph_kernel(const double* keys, const uint32_t* rows, uint64_t n,
+                                   uint32_t k, const uint32_t* row_sample,
+                                   const uint64_t* first, uint64_t* indptr, uint32_t* indices,
+                                   float* distances) {
+  uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const uint32_t smp = row_sample[r];
+  const uint64_t f = first[smp];
+  uint64_t* ip = indptr + f + smp;
+  if (r == f) ip[0] = 0;
+  ip[r - f + 1] = (r - f + 1) * (uint64_t)k;
+  const double* kr = keys + r * k;
+  const uint32_t* rr = rows + r * k;
+  uint32_t* oi = indices + r * k;
+  float* od = distances + r * k;
+  for (uint32_t i = 0; i < k; ++i) {
+    const uint32_t row = rr[i] - (uint32_t)f;
+    const float dist = (float)sqrt(kr[i]);
+    uint32_t at = i;
+    while (at > 0 && oi[at - 1] > row) {
+      oi[at] = oi[at - 1];
+      od[at] = od[at - 1];
+      --at;
+    }
+    oi[at] = row;
+    od[at] = dist;
+  }
+}
+
 // The CSR graph (rows sorted by column, f32 sqrt of the key) into host or device memory.
 void write_graph(const KnnResult& r, uint64_t n, uint32_t k, uint64_t* indptr, uint32_t* indices,
                  float* distances, cudaStream_t s) {
@@ -726,9 +870,99 @@ void write_graph(const KnnResult& r, uint64_t n, uint32_t k, uint64_t* indptr, u
   KG_CUDA(cudaStreamSynchronize(s));
 }
 
+// The batch's search and graphs (kg_knn_batch after its checks; x on the device).
+void knn_batch_run(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t d,
+                   uint32_t k, const std::vector<uint64_t>& first, uint64_t* indptr,
+                   uint32_t* indices, float* distances, kg_knn_stats* stats) {
+  cudaStream_t s = ctx->stream;
+  const uint32_t n_samples = (uint32_t)first.size() - 1;
+  ctx->total = n;
+  ctx->done = 0;
+  Trace trace(s, "knn_batch");
+  KnnBatch batch;
+  batch.first = first;
+  batch.d_first.alloc(n_samples + 1, s);
+  KG_CUDA(cudaMemcpyAsync(batch.d_first.ptr, batch.first.data(), (n_samples + 1) * 8ull,
+                          cudaMemcpyHostToDevice, s));
+  std::vector<uint32_t> rs(n);
+  for (uint32_t smp = 0; smp < n_samples; ++smp)
+    std::fill(rs.begin() + batch.first[smp], rs.begin() + batch.first[smp + 1], smp);
+  batch.row_sample.alloc(n, s);
+  KG_CUDA(cudaMemcpyAsync(batch.row_sample.ptr, rs.data(), n * 4, cudaMemcpyHostToDevice, s));
+  KnnResult r;
+  knn_core(ctx, x, n, width, d, k, nullptr, r, trace, &batch);
+  // The graphs (host or device outputs).
+  const bool dev_out = is_device_pointer(indptr);
+  DeviceBuffer<uint64_t> g_indptr;
+  DeviceBuffer<uint32_t> g_idx;
+  DeviceBuffer<float> g_dist;
+  uint64_t* gi = indptr;
+  uint32_t* gx = indices;
+  float* gd = distances;
+  if (!dev_out) {
+    g_indptr.alloc(n + n_samples, s);
+    g_idx.alloc(n * k, s);
+    g_dist.alloc(n * k, s);
+    gi = g_indptr.ptr;
+    gx = g_idx.ptr;
+    gd = g_dist.ptr;
+  }
+  batch_graph_kernel<<<blocks_for(n, 128), 128, 0, s>>>(r.key.ptr, r.row.ptr, n, k,
+                                                        batch.row_sample.ptr, batch.d_first.ptr,
+                                                        gi, gx, gd);
+  KG_LAUNCH_CHECK();
+  if (!dev_out) {
+    KG_CUDA(cudaMemcpyAsync(indptr, gi, (n + n_samples) * 8, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaMemcpyAsync(indices, gx, n * k * 4, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaMemcpyAsync(distances, gd, n * k * 4, cudaMemcpyDeviceToHost, s));
+  }
+  trace.mark("graph");
+  wait_stream(ctx, s);
+  ctx->done = n;
+  if (stats) {
+    stats->candidates = r.candidates;
+    stats->rows_full = r.rows_full;
+    stats->filter_ms = r.filter_ms;
+    stats->rank_ms = r.rank_ms;
+  }
+}
+
 }  // namespace kg
 
 using namespace kg;
+
+extern "C" kg_status kg_knn_batch(kg_ctx* ctx, const float* embedding, uint64_t n,
+                                  uint32_t width, uint32_t n_components, uint32_t n_neighbors,
+                                  const uint64_t* sample_rows, uint32_t n_samples,
+                                  uint64_t* indptr, uint32_t* indices, float* distances,
+                                  kg_knn_stats* stats) {
+  return guarded([&] {
+    if (!ctx || !embedding || !sample_rows || !indptr || !indices || !distances)
+      fail(KG_ERR_INVALID, "kg_knn_batch: NULL argument");
+    if (n_samples == 0) fail(KG_ERR_INVALID, "kg_knn_batch: no samples");
+    KnnBatch batch;
+    batch.first.assign(sample_rows, sample_rows + n_samples + 1);
+    if (batch.first[0] != 0 || batch.first[n_samples] != n)
+      fail(KG_ERR_INVALID, "kg_knn_batch: sample_rows must run from 0 to n_rows");
+    uint32_t k = 0, d = 0;
+    for (uint32_t smp = 0; smp < n_samples; ++smp) {
+      if (batch.first[smp + 1] < batch.first[smp])
+        fail(KG_ERR_INVALID, "kg_knn_batch: sample_rows must not decrease");
+      const uint64_t ns = batch.first[smp + 1] - batch.first[smp];
+      try {
+        check_search_args(ns, width, n_components, n_neighbors, k, d);
+      } catch (const Error& e) {
+        fail(e.status, "sample " + std::to_string(smp) + ": " + e.message);
+      }
+    }
+    use_device(ctx);
+    cudaStream_t s = ctx->stream;
+    DeviceBuffer<float> hold;
+    const float* x = device_view(embedding, n * width, hold, s);
+    check_finite(x, n, width, d, s);
+    knn_batch_run(ctx, x, n, width, d, k, batch.first, indptr, indices, distances, stats);
+  });
+}
 
 extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t n,
                                   uint32_t width, uint32_t n_components,

@@ -3,6 +3,7 @@
 
 #include <cstdint>
 #include <functional>
+#include <vector>
 
 #include "kg_internal.cuh"
 
@@ -32,6 +33,14 @@ struct KnnResult {
 // same row; each block of 256 query slots scans its list of point tiles (list_off CSR, or
 // list_stride entries a block; no list: every tile from the block's own), skipping
 // tiles on their list_lb2 bounds when given.
+// A batch of samples searched at once: sample s is rows [first[s], first[s + 1]) of x,
+// and a row's neighbours come from its own sample only.
+struct KnnBatch {
+  std::vector<uint64_t> first;         // n_samples + 1 row offsets (host)
+  DeviceBuffer<uint64_t> d_first;      // the same on the device
+  DeviceBuffer<uint32_t> row_sample;   // per row: its sample
+};
+
 struct ScanPlan {
   DeviceBuffer<uint32_t> qrows, prows, q_point;
   DeviceBuffer<uint32_t> list_tiles;
@@ -45,7 +54,11 @@ using PlanBuilder = std::function<void(const float* x, uint64_t n, uint32_t widt
                                        Trace& trace)>;
 
 void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t d, uint32_t k,
-              const PlanBuilder* plan, KnnResult& out, Trace& trace);
+              const PlanBuilder* plan, KnnResult& out, Trace& trace,
+              const KnnBatch* batch = nullptr);
+void knn_batch_run(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t d,
+                   uint32_t k, const std::vector<uint64_t>& first, uint64_t* indptr,
+                   uint32_t* indices, float* distances, kg_knn_stats* stats);
 void check_search_args(uint64_t n, uint32_t width, uint32_t n_components, uint32_t n_neighbors,
                        uint32_t& k, uint32_t& d);
 void check_finite(const float* x, uint64_t n, uint32_t width, uint32_t d, cudaStream_t s);

@@ -168,7 +168,8 @@ __device__ __noinline__ void tc_offer(QueryState& st, float* smallest, uint32_t 
 }
 
 // Offer the keys of one 32-point chunk selected by `mask` (bit j: point p0 + j, key
-// keys[j]), in column order, to the query's state. For k <= KR the query's k smallest
+// keys[j]), in column order, to the query's state; points outside [lo, n) and the query's
+// own slot q are skipped. For k <= KR the query's k smallest
 // keys (smallest[0..KR) in the thread's shared-memory slice, ascending, +inf past those
 // seen) move into registers for the chunk: an insertion is 2 KR branch-free min/max
 // (v[i] = max(v[i-1], min(v[i], key)) on the old values), no dependent memory access.
@@ -176,7 +177,8 @@ __device__ __noinline__ void tc_offer(QueryState& st, float* smallest, uint32_t 
 template <int KR>
 __device__ __forceinline__ void tc_offer_chunk(QueryState& st, float* smallest, uint32_t k,
                                                double slack2, const float* keys, uint32_t mask,
-                                               uint64_t p0, uint64_t q, uint64_t n, float* ck,
+                                               uint64_t p0, uint64_t q, uint64_t lo, uint64_t n,
+                                               float* ck,
                                                uint32_t* cr, uint32_t cap) {
   if constexpr (KR == 0) {
     while (mask && !st.overflowed) {
@@ -184,7 +186,7 @@ __device__ __forceinline__ void tc_offer_chunk(QueryState& st, float* smallest, 
       mask &= mask - 1;
       const float key = keys[j];
       const uint64_t p = p0 + j;
-      if (key <= st.th && p < n && p != q)
+      if (key <= st.th && p >= lo && p < n && p != q)
         tc_offer(st, smallest, k, slack2, key, (uint32_t)p, ck, cr, cap);
     }
   } else {
@@ -200,7 +202,7 @@ __device__ __forceinline__ void tc_offer_chunk(QueryState& st, float* smallest, 
       mask &= mask - 1;
       const float key = keys[j];
       const uint64_t p = p0 + j;
-      if (!(key <= st.th) || p >= n || p == q) continue;
+      if (!(key <= st.th) || p < lo || p >= n || p == q) continue;
       if (key < kth) {
         float prev = v[0];
         v[0] = fminf(v[0], key);
@@ -439,6 +441,13 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
       const uint64_t q = qb * kTcQueries + half * 128 + quad * 32 + lane;
       const bool active = q < n_q;
       const uint64_t self = active ? (scan.q_point ? scan.q_point[q] : q) : ~0ull;
+      // The point slots the query may take (its own sample's, or every slot).
+      uint64_t p_lo = 0, p_hi = n_p;
+      if (active && scan.slot_sample) {
+        const uint32_t smp = scan.slot_sample[q];
+        p_lo = scan.sample_first[smp];
+        p_hi = scan.sample_first[smp + 1];
+      }
       const double s2qn2 = active && scan.qn2 ? scan.s2 * scan.qn2[q] : 0.0;
       QueryState st{INFINITY, 0, 0, 64, false};
       if (KR > 0)
@@ -492,7 +501,7 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           }
           const uint64_t p0 = (uint64_t)pt * kTcPoints + c * 32;
           st.th = th;
-          tc_offer_chunk<KR>(st, smallest, k, sl2, my, mask, p0, self, n_p, ck, cr, cap);
+          tc_offer_chunk<KR>(st, smallest, k, sl2, my, mask, p0, self, p_lo, p_hi, ck, cr, cap);
           th = st.th;
           live = !st.overflowed;
         }

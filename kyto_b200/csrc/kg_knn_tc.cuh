@@ -32,6 +32,10 @@ struct FilterScan {
                                          // at list_off[qb + 1] (or NULL: qb * list_stride,
                                          // list_stride entries each)
   uint64_t list_stride = 0;
+  const uint32_t* slot_sample = nullptr;  // per query slot its sample (NULL: one sample):
+  const uint64_t* sample_first = nullptr; // a query takes only the point slots
+                                          // [sample_first[s], sample_first[s + 1]) of its
+                                          // sample s (a batch of samples searched at once)
   const double* qn2 = nullptr;           // per query slot |q - mean|^2 (set by tc_filter)
   double s2 = 1.0;                       // scale^2 (set by tc_filter)
 };

@@ -8,9 +8,12 @@
 //   2. partitions: k-means of the sample into P parts (kg_cluster.cuh);
 //   3. training: soft targets = the parts of a row and of its k neighbours, soft-target
 //      cross-entropy, Adam, `epochs` passes of seeded shuffles;
-//   4. index: the network's top-`probe` parts for every row (their summed softmax is the
-//      confidence), each row stored in its top part;
-//   5. search: query slots sorted by (fallback, top part); each block of 256 query slots
+//   4. calibration: the softmax temperature whose confidence (the probed parts' summed
+//      softmax) best predicts, by log loss over the sample, that a row's exact
+//      neighbours live in the parts it probes;
+//   5. index: the network's top-`probe` parts for every row and their confidence at that
+//      temperature, each row stored in its top part;
+//   6. search: query slots sorted by (fallback, top part); each block of 256 query slots
 //      scans the tiles of the union of its queries' probed parts (every tile if one of
 //      them falls back), then the exact re-rank.
 #include <cuda_bf16.h>
@@ -215,9 +218,11 @@ int bits_for_value(uint64_t v) {
   return b;
 }
 
-// The network's top parts for n rows of x (chunks of 65,536 rows).
+// The network's top parts for n rows of x (chunks of 65,536 rows) and their confidence
+// at each of n_temps temperatures (device array temps): conf[t * n + row].
 void learned_probe(const Mlp& mlp, const float* x, uint64_t n, uint32_t width, uint32_t probe,
-                   uint32_t* top, float* conf, cudaStream_t s) {
+                   const float* temps, uint32_t n_temps, uint32_t* top, float* conf,
+                   cudaStream_t s) {
   const uint64_t chunk = 65536;
   MlpBatch b;
   b.alloc(mlp.sh, (uint32_t)std::min<uint64_t>(chunk, n), s);
@@ -225,9 +230,31 @@ void learned_probe(const Mlp& mlp, const float* x, uint64_t n, uint32_t width, u
     const uint32_t rows = (uint32_t)std::min<uint64_t>(chunk, n - r0);
     b.rows = rows;
     mlp.forward(x + r0 * width, width, b, s);
-    top_parts(b.z3.ptr, rows, mlp.sh.parts, probe, top + r0 * probe, conf + r0, s);
+    top_parts(b.z3.ptr, rows, mlp.sh.parts, probe, top + r0 * probe, conf + r0, n, s, temps,
+              n_temps);
   }
 }
+
+// contained[i] = 1 if every neighbour of sample row i (its k graph rows) lives in a part
+// row i probes (a row lives in its top part): the event the confidence should predict.
+__global__ void contained_kernel(const uint32_t* top, uint32_t probe, const uint32_t* nbr,
+                                 uint64_t m, uint32_t k, uint8_t* contained) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  bool all = true;
+  for (uint32_t j = 0; j < k && all; ++j) {
+    const uint32_t home = top[(uint64_t)nbr[i * k + j] * probe];
+    bool in = false;
+    for (uint32_t t = 0; t < probe; ++t) in |= top[i * probe + t] == home;
+    all = in;
+  }
+  contained[i] = all ? 1 : 0;
+}
+
+// The temperatures the calibration tries (1: the network's own softmax).
+constexpr float kTemps[] = {1.0f, 1.25f, 1.5f, 2.0f, 2.5f, 3.0f, 4.0f, 5.0f,
+                            6.0f, 8.0f, 10.0f, 12.0f, 16.0f};
+constexpr uint32_t kNumTemps = sizeof(kTemps) / sizeof(kTemps[0]);
 
 }  // namespace
 
@@ -374,11 +401,46 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
     const double train_ms = ms_since(t_train);
     trace.mark("training");
 
-    // 4. Every row's parts.
+    // 4. Calibration: the temperature whose confidence best predicts (log loss) that a
+    // sample row's exact neighbours live in the parts it probes.
+    float temperature = 1.0f;
+    DeviceBuffer<float> d_temps(kNumTemps, s);
+    KG_CUDA(cudaMemcpyAsync(d_temps.ptr, kTemps, sizeof(kTemps), cudaMemcpyHostToDevice, s));
+    {
+      DeviceBuffer<uint32_t> stop(m * probe, s);
+      DeviceBuffer<float> sconf(kNumTemps * m, s);
+      learned_probe(mlp, xs.ptr, m, d, probe, d_temps.ptr, kNumTemps, stop.ptr, sconf.ptr, s);
+      DeviceBuffer<uint8_t> cont(m, s);
+      contained_kernel<<<blocks_for(m, 256), 256, 0, s>>>(stop.ptr, probe, sg.row.ptr, m, k,
+                                                          cont.ptr);
+      KG_LAUNCH_CHECK();
+      std::vector<float> hconf(kNumTemps * m);
+      std::vector<uint8_t> hcont(m);
+      KG_CUDA(cudaMemcpyAsync(hconf.data(), sconf.ptr, hconf.size() * 4, cudaMemcpyDeviceToHost,
+                              s));
+      KG_CUDA(cudaMemcpyAsync(hcont.data(), cont.ptr, m, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaStreamSynchronize(s));
+      double best = INFINITY;
+      for (uint32_t t = 0; t < kNumTemps; ++t) {
+        double loss = 0.0;
+        for (uint64_t i = 0; i < m; ++i) {
+          const double p = std::min(std::max((double)hconf[t * m + i], 1e-6), 1.0 - 1e-6);
+          loss -= hcont[i] ? std::log(p) : std::log1p(-p);
+        }
+        if (loss < best) {
+          best = loss;
+          temperature = kTemps[t];
+        }
+      }
+    }
+    trace.mark("calibration");
+
+    // 5. Every row's parts.
     auto t_index = now();
     DeviceBuffer<uint32_t> top(n * probe, s);
     DeviceBuffer<float> conf(n, s);
-    learned_probe(mlp, x, n, width, probe, top.ptr, conf.ptr, s);
+    KG_CUDA(cudaMemcpyAsync(d_temps.ptr, &temperature, 4, cudaMemcpyHostToDevice, s));
+    learned_probe(mlp, x, n, width, probe, d_temps.ptr, 1, top.ptr, conf.ptr, s);
     KG_CUDA(cudaStreamSynchronize(s));
     const double index_ms = ms_since(t_index);
     trace.mark("index");
@@ -464,6 +526,7 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
       stats->index_ms = index_ms;
       stats->search_ms = search_ms;
       stats->final_loss = final_loss;
+      stats->temperature = temperature;
     }
   });
 }

@@ -203,10 +203,13 @@ __global__ void init_kernel(float* p, uint64_t begin, uint64_t n, uint32_t fan_i
   p[begin + i] = (float)((2.0 * u - 1.0) * lim);
 }
 
-// Top `probe` parts per row by logit (descending, ties to the lower part): one warp per
-// row, `probe` rounds of a warp argmax; the confidence is their summed softmax.
+// The top `probe` parts of each row's logits (ties to the lower part): one warp per
+// row, `probe` rounds of a warp argmax. The confidence is their summed softmax at each
+// temperature temps[t] (the logits times temps[t]): conf[t * conf_stride + row].
+constexpr uint32_t kMaxTemps = 16;
 __global__ void top_parts_kernel(const float* z, uint64_t rows, uint32_t parts, uint32_t probe,
-                                 uint32_t* top, float* conf) {
+                                 const float* temps, uint32_t n_temps, uint32_t* top,
+                                 float* conf, uint64_t conf_stride) {
   const uint64_t row = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const unsigned lane = threadIdx.x & 31u;
   if (row >= rows) return;
@@ -214,10 +217,8 @@ __global__ void top_parts_kernel(const float* z, uint64_t rows, uint32_t parts, 
   float m = -INFINITY;
   for (uint32_t p = lane; p < parts; p += 32) m = fmaxf(m, zr[p]);
   for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
-  float sum = 0.0f;
-  for (uint32_t p = lane; p < parts; p += 32) sum += __expf(zr[p] - m);
-  for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
-  float picked = 0.0f;
+  float picked[kMaxTemps];
+  for (uint32_t t = 0; t < n_temps; ++t) picked[t] = 0.0f;
   uint32_t prev_p = 0xFFFFFFFFu;
   float prev_v = INFINITY;
   for (uint32_t t = 0; t < probe; ++t) {
@@ -241,11 +242,16 @@ __global__ void top_parts_kernel(const float* z, uint64_t rows, uint32_t parts, 
       }
     }
     if (lane == 0) top[row * probe + t] = bp;
-    picked += __expf(bv - m);
+    for (uint32_t i = 0; i < n_temps; ++i) picked[i] += __expf(temps[i] * (bv - m));
     prev_v = bv;
     prev_p = bp;
   }
-  if (lane == 0) conf[row] = picked / sum;
+  for (uint32_t i = 0; i < n_temps; ++i) {
+    float sum = 0.0f;
+    for (uint32_t p = lane; p < parts; p += 32) sum += __expf(temps[i] * (zr[p] - m));
+    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+    if (lane == 0) conf[i * conf_stride + row] = picked[i] / sum;
+  }
 }
 
 }  // namespace
@@ -368,9 +374,12 @@ void Mlp::adam(float lr, cudaStream_t s) {
 }
 
 void top_parts(const float* logits, uint64_t rows, uint32_t parts, uint32_t probe, uint32_t* top,
-               float* confidence, cudaStream_t s) {
-  top_parts_kernel<<<blocks_for(rows * 32, 256), 256, 0, s>>>(logits, rows, parts, probe, top,
-                                                             confidence);
+               float* confidence, uint64_t conf_stride, cudaStream_t s, const float* temps,
+               uint32_t n_temps) {
+  if (n_temps < 1 || n_temps > kMaxTemps) fail(KG_ERR_INVALID, "top_parts: 1..16 temperatures");
+  top_parts_kernel<<<blocks_for(rows * 32, 256), 256, 0, s>>>(logits, rows, parts, probe, temps,
+                                                             n_temps, top, confidence,
+                                                             conf_stride);
   KG_LAUNCH_CHECK();
 }
 

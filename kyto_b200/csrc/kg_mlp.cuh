@@ -56,7 +56,11 @@ class Mlp {
 
 // The top `probe` parts of each row of logits (rows x parts, f32) by probability
 // (descending, ties to the lower part) and their summed probability.
+// Each row's top `probe` parts and, for each of n_temps temperatures (device array
+// temps; the logits are multiplied by each), the parts' summed softmax:
+// confidence[t * conf_stride + row].
 void top_parts(const float* logits, uint64_t rows, uint32_t parts, uint32_t probe,
-               uint32_t* top, float* confidence, cudaStream_t s);
+               uint32_t* top, float* confidence, uint64_t conf_stride, cudaStream_t s,
+               const float* temps, uint32_t n_temps);
 
 }  // namespace kg

@@ -13,10 +13,15 @@
 #include <string>
 
 #include <algorithm>
+#include <atomic>
+#include <memory>
+#include <exception>
+#include <thread>
 #include <cmath>
 #include <vector>
 
 #include "kg_internal.cuh"
+#include "kg_knn.cuh"
 #include "kg_maps.cuh"
 #include "kg_spmm.cuh"
 #include "kg_spmm_tc.cuh"
@@ -1464,74 +1469,164 @@ void kg_pca::run() {
   ran = true;
 }
 
+namespace kg {
+
+// A new session on ctx (kyto's PcaAccumulator::new, pca.rs:343-403): a pooled stream and
+// solver handles, the gene map checked and uploaded.
+kg_pca* make_session(kg_ctx* ctx, const kg_pca_params* params) {
+  if (params->n_components == 0) fail(KG_ERR_INVALID, "pca: n_components must be at least 1");
+  if (params->n_genes == 0) fail(KG_ERR_INVALID, "pca: blocks of 0 genes");
+  use_device(ctx);
+  auto* p = new kg_pca();
+  try {
+    p->ctx = ctx;
+    {
+      std::lock_guard<std::mutex> lock(ctx->res_mu);
+      if (!ctx->free_res.empty()) {
+        const kg_ctx::SessionRes r = ctx->free_res.back();
+        ctx->free_res.pop_back();
+        p->stream = r.stream;
+        p->cublas = r.cublas;
+        p->cusolver = r.cusolver;
+      }
+    }
+    if (!p->stream) KG_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+    if (!p->cublas) {
+      KG_CUBLAS(cublasCreate(&p->cublas));
+      KG_CUBLAS(cublasSetStream(p->cublas, p->stream));
+    }
+    if (!p->cusolver) {
+      KG_CUSOLVER(cusolverDnCreate(&p->cusolver));
+      KG_CUSOLVER(cusolverDnSetStream(p->cusolver, p->stream));
+    }
+    p->k = params->n_components;
+    p->stream_genes = params->n_genes;
+    p->seed = params->seed;
+    p->target_sum = params->target_sum;
+    p->log1p = params->log1p;
+    if (params->gene_map) {
+      std::vector<uint32_t> map(params->n_genes), set;
+      KG_CUDA(cudaMemcpy(map.data(), params->gene_map, params->n_genes * 4ull,
+                         cudaMemcpyDefault));
+      uint32_t next = 0;
+      for (uint32_t i = 0; i < params->n_genes; ++i) {
+        if (map[i] == kNoGene) continue;
+        if (map[i] != next)
+          fail(KG_ERR_INVALID, "pca: gene_map must number the kept genes 0, 1, ... in order");
+        set.push_back(i);
+        ++next;
+      }
+      p->n_genes = next;
+      p->gene_map.alloc(params->n_genes, p->stream);
+      KG_CUDA(cudaMemcpyAsync(p->gene_map.ptr, map.data(), map.size() * 4, cudaMemcpyHostToDevice,
+                              p->stream));
+      p->set_genes.alloc(set.size(), p->stream);
+      if (!set.empty())
+        KG_CUDA(cudaMemcpyAsync(p->set_genes.ptr, set.data(), set.size() * 4,
+                                cudaMemcpyHostToDevice, p->stream));
+      KG_CUDA(cudaStreamSynchronize(p->stream));
+    } else {
+      p->n_genes = params->n_genes;
+    }
+    p->width = std::min<uint32_t>(p->k + kOversamples, p->n_genes);
+    p->indptr.alloc(1, p->stream);
+    p->indptr.zero();
+  } catch (...) {
+    delete p;
+    throw;
+  }
+  return p;
+}
+
+}  // namespace kg
+
 extern "C" {
+
+kg_status kg_pca_knn_batch(kg_ctx* ctx, const kg_pca_params* params, uint32_t n_samples,
+                           const kg_batch_sample* samples, uint32_t n_neighbors,
+                           float* embedding, double* variance, uint64_t* indptr,
+                           uint32_t* indices, float* distances, kg_batch_stats* stats) {
+  return guarded([&] {
+    if (!ctx || !params || !samples || !embedding || !indptr || !indices || !distances)
+      fail(KG_ERR_INVALID, "kg_pca_knn_batch: NULL argument");
+    if (n_samples == 0) fail(KG_ERR_INVALID, "kg_pca_knn_batch: no samples");
+    const uint32_t kc = params->n_components;
+    std::vector<uint64_t> first(n_samples + 1, 0);
+    uint32_t k = 0, d = 0;
+    for (uint32_t i = 0; i < n_samples; ++i) {
+      const kg_batch_sample& b = samples[i];
+      if (b.n_rows && (!b.indptr || !b.indices || !b.values))
+        fail(KG_ERR_INVALID, "kg_pca_knn_batch: sample " + std::to_string(i) + ": NULL array");
+      try {
+        check_search_args(b.n_rows, kc, kc, n_neighbors, k, d);
+      } catch (const Error& e) {
+        fail(e.status, "sample " + std::to_string(i) + ": " + e.message);
+      }
+      first[i + 1] = first[i] + b.n_rows;
+    }
+    const uint64_t n = first[n_samples];
+    use_device(ctx);
+    cudaStream_t s = ctx->stream;
+    DeviceBuffer<float> emb_all(n * kc, s);
+    KG_CUDA(cudaStreamSynchronize(s));
+    std::vector<double> var_all((size_t)n_samples * kc);
+    // The samples' PCA: workers take the next sample until none is left; each session
+    // has its own stream, so the small samples' kernels run side by side.
+    const auto t0 = std::chrono::steady_clock::now();
+    const unsigned workers = std::min<unsigned>(n_samples, 8);
+    std::atomic<uint32_t> next{0};
+    std::vector<std::exception_ptr> errors(workers);
+    std::vector<std::thread> pool;
+    for (unsigned w = 0; w < workers; ++w) {
+      pool.emplace_back([&, w] {
+        try {
+          KG_CUDA(cudaSetDevice(ctx->device));
+          for (;;) {
+            const uint32_t i = next.fetch_add(1);
+            if (i >= n_samples) break;
+            check_cancel(ctx);
+            std::unique_ptr<kg_pca> p(make_session(ctx, params));
+            const kg_batch_sample& b = samples[i];
+            p->push(b.indptr, b.indices, b.values, b.dtype, b.n_rows, nullptr);
+            p->run();
+            KG_CUDA(cudaMemcpyAsync(emb_all.ptr + first[i] * kc, p->embedding.ptr,
+                                    b.n_rows * kc * 4ull, cudaMemcpyDeviceToDevice, p->stream));
+            KG_CUDA(cudaStreamSynchronize(p->stream));
+            std::memcpy(&var_all[(size_t)i * kc], p->variance.data(), kc * 8ull);
+          }
+        } catch (...) {
+          errors[w] = std::current_exception();
+          next.store(n_samples);
+        }
+      });
+    }
+    for (std::thread& t : pool) t.join();
+    for (const std::exception_ptr& e : errors)
+      if (e) std::rethrow_exception(e);
+    const double pca_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    // Every sample's neighbours in one batched search.
+    const auto t1 = std::chrono::steady_clock::now();
+    kg_knn_stats ks{};
+    knn_batch_run(ctx, emb_all.ptr, n, kc, d, k, first, indptr, indices, distances, &ks);
+    KG_CUDA(cudaMemcpyAsync(embedding, emb_all.ptr, n * kc * 4ull, cudaMemcpyDefault, s));
+    wait_stream(ctx, s);
+    if (variance) std::memcpy(variance, var_all.data(), var_all.size() * 8);
+    if (stats) {
+      stats->pca_ms = pca_ms;
+      stats->knn_ms = std::chrono::duration<double, std::milli>(
+                          std::chrono::steady_clock::now() - t1).count();
+      stats->workers = workers;
+      stats->knn = ks;
+    }
+  });
+}
 
 kg_status kg_pca_begin(kg_ctx* ctx, const kg_pca_params* params, kg_pca** out) {
   return guarded([&] {
     if (!ctx || !params || !out) fail(KG_ERR_INVALID, "kg_pca_begin: NULL argument");
     *out = nullptr;
-    if (params->n_components == 0) fail(KG_ERR_INVALID, "pca: n_components must be at least 1");
-    if (params->n_genes == 0) fail(KG_ERR_INVALID, "pca: blocks of 0 genes");
-    use_device(ctx);
-    auto* p = new kg_pca();
-    try {
-      p->ctx = ctx;
-      {
-        std::lock_guard<std::mutex> lock(ctx->res_mu);
-        if (!ctx->free_res.empty()) {
-          const kg_ctx::SessionRes r = ctx->free_res.back();
-          ctx->free_res.pop_back();
-          p->stream = r.stream;
-          p->cublas = r.cublas;
-          p->cusolver = r.cusolver;
-        }
-      }
-      if (!p->stream) KG_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
-      if (!p->cublas) {
-        KG_CUBLAS(cublasCreate(&p->cublas));
-        KG_CUBLAS(cublasSetStream(p->cublas, p->stream));
-      }
-      if (!p->cusolver) {
-        KG_CUSOLVER(cusolverDnCreate(&p->cusolver));
-        KG_CUSOLVER(cusolverDnSetStream(p->cusolver, p->stream));
-      }
-      p->k = params->n_components;
-      p->stream_genes = params->n_genes;
-      p->seed = params->seed;
-      p->target_sum = params->target_sum;
-      p->log1p = params->log1p;
-      if (params->gene_map) {
-        std::vector<uint32_t> map(params->n_genes), set;
-        KG_CUDA(cudaMemcpy(map.data(), params->gene_map, params->n_genes * 4ull,
-                           cudaMemcpyDefault));
-        uint32_t next = 0;
-        for (uint32_t i = 0; i < params->n_genes; ++i) {
-          if (map[i] == kNoGene) continue;
-          if (map[i] != next)
-            fail(KG_ERR_INVALID, "pca: gene_map must number the kept genes 0, 1, ... in order");
-          set.push_back(i);
-          ++next;
-        }
-        p->n_genes = next;
-        p->gene_map.alloc(params->n_genes, p->stream);
-        KG_CUDA(cudaMemcpyAsync(p->gene_map.ptr, map.data(), map.size() * 4, cudaMemcpyHostToDevice,
-                                p->stream));
-        p->set_genes.alloc(set.size(), p->stream);
-        if (!set.empty())
-          KG_CUDA(cudaMemcpyAsync(p->set_genes.ptr, set.data(), set.size() * 4,
-                                  cudaMemcpyHostToDevice, p->stream));
-        KG_CUDA(cudaStreamSynchronize(p->stream));
-      } else {
-        p->n_genes = params->n_genes;
-      }
-      p->width = std::min<uint32_t>(p->k + kOversamples, p->n_genes);
-      p->indptr.alloc(1, p->stream);
-      p->indptr.zero();
-    } catch (...) {
-      delete p;
-      throw;
-    }
-    *out = p;
+    *out = make_session(ctx, params);
   });
 }
 

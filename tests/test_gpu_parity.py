@@ -293,3 +293,49 @@ def test_knn_huge_norms_search_every_row(ctx):
     pts[5] = 1e18
     gpu = K.neighbors(pts, 5, ctx=ctx)
     _graph_equal(gpu, O.neighbors(pts, 5))
+
+
+@pytest.mark.parametrize("candidate_filter", ["fp16", "split"])
+def test_knn_batch_equals_each_sample_alone(ctx, monkeypatch, candidate_filter):
+    # Samples of uneven sizes (not multiples of the 128-row tile or the 256-row query
+    # block, one as small as n_neighbors) searched in one launch: every sample's graph
+    # equals the exact search of that sample alone, with columns numbered from its own
+    # first row.
+    monkeypatch.setenv("KYTO_GPU_KNN_FILTER", candidate_filter)
+    rng = np.random.default_rng(21)
+    sizes = [16, 300, 1000, 2049, 77, 5000, 130]
+    samples = []
+    for i, m in enumerate(sizes):
+        pts, _ = synthetic.gaussian_mixture(m, 30, 5, seed=30 + i, device="cpu")
+        samples.append(pts + rng.normal(0, 5, 30).astype(np.float32))  # each its own offset
+    samples[2][10:20] = samples[2][3]  # duplicates inside one sample
+    graphs = K.neighbors_batch(samples, 16, ctx=ctx)
+    assert len(graphs) == len(samples)
+    for pts, g in zip(samples, graphs):
+        _graph_equal(g, O.neighbors(pts, 16))
+
+
+def test_knn_batch_refusals(ctx):
+    small = np.zeros((4, 3), np.float32)
+    with pytest.raises(K.KytoError) as e:
+        K.neighbors_batch([np.ones((40, 3), np.float32), small], 5, ctx=ctx)
+    assert e.value.code == "KY-E215" and "sample 1" in str(e.value)
+
+
+def test_pca_neighbors_batch_equals_each_sample_alone(ctx):
+    # The batching form: samples of uneven sizes, PCA 30 + kNN 15 each, sessions run side
+    # by side and one batched search; each sample's embedding, variances and graph equal
+    # the single-sample calls' bit for bit.
+    sizes = [500, 3100, 257, 1200, 9000, 640]
+    samples = []
+    for i, m in enumerate(sizes):
+        x = synthetic.counts_csr(m, 400, 40, 4, 30, seed=50 + i, device="cpu")
+        samples.append((x.indptr, x.indices, x.values))
+    out, stats = K.pca_neighbors_batch(samples, 400, 30, 15, seed=0, target_sum=1e4, log1p=True,
+                                       ctx=ctx)
+    assert stats.workers == len(sizes)
+    for (indptr, idx, vals), (res, g) in zip(samples, out):
+        one = K.pca(indptr, idx, vals, 400, 30, seed=0, target_sum=1e4, log1p=True, ctx=ctx)
+        assert np.array_equal(res.embedding.view(np.uint32), one.embedding.view(np.uint32))
+        assert np.array_equal(res.variance.view(np.uint64), one.variance.view(np.uint64))
+        _graph_equal(g, K.neighbors(one.embedding, 15, ctx=ctx))
