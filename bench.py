@@ -13,6 +13,12 @@ One step = the whole path over the whole dataset: push the CSR to the PCA sessio
   the input and device->host copy of the graph inside every step.
 Inputs (4.8 GB) are larger than L2 (126 MB), so no flush is needed between steps.
 
+On one GPU the line also carries the metric's second half and the batching form:
+- ``learned_vs_exact``: the learned-partition kNN against the exact search on 4M x 50
+  Gaussian-mixture points (speed-up and recall@15 judged by the exact graph);
+- ``batching``: 64 samples of uneven sizes (PCA 30 + kNN 15 each) through the batching
+  form against one sample at a time.
+
 ``--impl reference``: kyto's CPU algorithms (the C++ restatement in oracle/, all host
 threads) timed on a bounded sample of the same workload: the PCA over a subset of the
 cells (all 11 passes) and the exact search of a subset of query cells against every
@@ -56,6 +62,10 @@ def parse() -> argparse.Namespace:
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-pca-cells", type=int, default=40_000)
     ap.add_argument("--cpu-knn-queries", type=int, default=1024)
+    ap.add_argument("--learned-cells", type=int, default=4_000_000,
+                    help="C5 learned-vs-exact comparison rows (0: skip)")
+    ap.add_argument("--batch-samples", type=int, default=64,
+                    help="C4 batching-form samples (0: skip)")
     return ap.parse_args()
 
 
@@ -203,6 +213,105 @@ def cpu_baseline(args, x, vals, embedding, ctx) -> dict:
     }
 
 
+def learned_vs_exact(n: int, ctx) -> dict:
+    """C5: n x 50 f32 points from a 200-component Gaussian mixture (weights Dirichlet(1),
+    isotropic sigma log-uniform [0.2, 2]); the learned-partition kNN (1,024 parts, BF16
+    MLP 50-256-256-1024 trained on the device on the exact graph of a 200,000-row sample,
+    top-8 probes, fallback below 0.9 confidence) against the exact search, recall@15
+    judged by the exact graph. Times: host wall clock around each call, inputs on the
+    device, after one untimed call of each (the filter kind tuning is cached)."""
+    import torch
+
+    import kyto_b200 as K
+    from kyto_b200 import synthetic
+
+    x, _ = synthetic.gaussian_mixture(n, dim=50, n_components=200, spread=3.0, seed=5,
+                                      device="cuda")
+    xd = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float32)).cuda()
+    k = 14
+    params = K.LearnedParams(n_parts=1024, hidden=256, n_probe=8, confidence=0.9,
+                             train_cells=200_000, epochs=6, batch=4096, seed=0)
+
+    def graph(fn):
+        out = (torch.empty(n + 1, dtype=torch.int64, device="cuda"),
+               torch.empty(n * k, dtype=torch.int32, device="cuda"),
+               torch.empty(n * k, dtype=torch.float32, device="cuda"))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        st = fn(out)
+        torch.cuda.synchronize()
+        return out, st, time.perf_counter() - t0
+
+    def exact(out):
+        st = K.KnnStats()
+        K._check(K.library().kg_knn_exact(ctx.handle, K._ptr(xd), n, 50, 0, 15, K._ptr(out[0]),
+                                          K._ptr(out[1]), K._ptr(out[2]), K.ctypes.byref(st)))
+        return st
+
+    def learned(out):
+        st = K.LearnedStats()
+        K._check(K.library().kg_knn_learned(ctx.handle, K._ptr(xd), n, 50, 0, 15,
+                                            K.ctypes.byref(params), K._ptr(out[0]),
+                                            K._ptr(out[1]), K._ptr(out[2]),
+                                            K.ctypes.byref(st)))
+        return st
+
+    graph(exact)
+    ex, ex_st, t_ex = graph(exact)
+    graph(learned)
+    le, le_st, t_le = graph(learned)
+    a = le[1].view(n, k).long()
+    b = ex[1].view(n, k).long()
+    hits = 0
+    for i in range(0, n, 250_000):
+        hits += int((a[i:i + 250_000, :, None] == b[i:i + 250_000, None, :]).any(2).sum())
+    return {
+        "workload": (f"{n:,} x 50 f32 Gaussian mixture (200 components, Dirichlet(1) weights, "
+                     "sigma log-uniform [0.2, 2]), k = 15 (14 stored)"),
+        "exact_ms": t_ex * 1e3, "learned_ms": t_le * 1e3, "speedup": t_ex / t_le,
+        "recall_at_15": hits / (n * k),
+        "learned": {"train_ms": le_st.train_ms, "index_ms": le_st.index_ms,
+                    "search_ms": le_st.search_ms, "fallback_rows": le_st.fallback_rows,
+                    "scanned_tiles": le_st.scanned_tiles, "temperature": le_st.temperature,
+                    "final_loss": le_st.final_loss},
+        "exact": {"filter_ms": ex_st.filter_ms, "rank_ms": ex_st.rank_ms,
+                  "rows_searched_in_full": ex_st.rows_full},
+    }
+
+
+def batching(n_samples: int, ctx) -> dict:
+    """C4: n_samples samples x 2,000 genes, cells log-uniform [500, 80,000] (seed 1),
+    ~600 stored values per cell; PCA 30 + kNN 15 each through the batching form
+    (kg_pca_knn_batch), against the same calls one sample at a time."""
+    import kyto_b200 as K
+    from kyto_b200 import synthetic
+
+    rng = np.random.default_rng(1)
+    sizes = np.exp(rng.uniform(np.log(500), np.log(80_000), n_samples)).astype(int)
+    samples = []
+    for i, m in enumerate(sizes):
+        c = synthetic.counts_csr(int(m), 2000, 600.0, 20, 100, seed=100 + i, device="cuda")
+        samples.append((c.indptr, c.indices, c.values))
+    kw = dict(target_sum=1e4, log1p=True, ctx=ctx)
+    K.pca_neighbors_batch(samples[:4], 2000, 30, 15, **kw)
+    t0 = time.perf_counter()
+    out, st = K.pca_neighbors_batch(samples, 2000, 30, 15, **kw)
+    t_batch = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for ip, ix, v in samples:
+        r = K.pca(ip, ix, v, 2000, 30, seed=0, **kw)
+        K.neighbors(r.embedding, 15, ctx=ctx)
+    t_one = time.perf_counter() - t0
+    cells = int(sizes.sum())
+    return {
+        "workload": (f"{n_samples} samples x 2,000 genes, {cells:,} cells (log-uniform "
+                     "500-80,000 a sample), PCA 30 + exact kNN 15 each, host CSR in"),
+        "batch_ms": t_batch * 1e3, "cells_per_s": cells / t_batch,
+        "one_at_a_time_ms": t_one * 1e3, "speedup": t_one / t_batch,
+        "pca_ms": st.pca_ms, "knn_ms": st.knn_ms, "workers": st.workers,
+    }
+
+
 def main() -> int:
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -312,6 +421,16 @@ def main() -> int:
         emb = sess.results().embedding
         sess.close()
         cpu = cpu_baseline(args, x, vals, emb, ctx)
+    extra = {}
+    if rank == 0 and world == 1:
+        for name, fn, on in (("learned_vs_exact", learned_vs_exact, args.learned_cells),
+                             ("batching", batching, args.batch_samples)):
+            if not on:
+                continue
+            try:
+                extra[name] = fn(on, ctx)
+            except Exception as e:  # a side measurement never costs the main line
+                extra[name] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "cells/s", "n_gpus": world,
@@ -324,6 +443,7 @@ def main() -> int:
                        "l2": "inputs (>4 GB) larger than L2; no flush"},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
             "clocks": clk, "gpu_launches": launches, "knn": knn_stats,
+            **extra,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -250,15 +250,16 @@ KG_API kg_status kg_pca_knn_batch(kg_ctx* ctx, const kg_pca_params* params, uint
 
 /* No counterpart in kyto: the north star's learned form. A BF16 MLP (n_components ->
  * hidden -> hidden -> n_parts, ReLU) is trained on the device on the exact kNN graph of
- * train_cells evenly strided rows (targets: the k-means parts of a row and of its
- * n_neighbors - 1 neighbours; soft-target cross-entropy, Adam, `epochs` seeded
- * shuffles of `batch` rows); every row then gets its n_probe most probable parts, lives
- * in the most probable one, and is searched exactly (kg_knn_exact's filter and re-rank)
- * among the rows of the parts its block of 256 query rows probes, or against every row
- * when the probed parts' summed probability is below `confidence`. That probability
- * is the softmax at a temperature calibrated on the sample (the one whose confidence
- * best predicts, by log loss, that a sample row's exact neighbours live in the parts it
- * probes). */
+ * train_cells evenly strided rows (it starts as the k-means parts' nearest-centre
+ * classifier; targets: the parts of a row and of its n_neighbors - 1 neighbours;
+ * soft-target cross-entropy, Adam, `epochs` seeded shuffles of `batch` rows). Every row
+ * then gets its n_probe most probable parts and lives in the most probable one; rows in
+ * that order form blocks of 256 query rows, and a row is searched exactly (kg_knn_exact's
+ * filter and re-rank) among the rows of the parts its block probes (the union of the
+ * block's rows' n_probe parts), or against every row when its probability in those
+ * parts is below `confidence`. The probability is the softmax at a temperature
+ * calibrated on the sample: the one whose top-n_probe mass best predicts, by
+ * cross-entropy, the share of a sample row's exact neighbours living in those parts. */
 typedef struct kg_learned_params {
   uint32_t n_parts;        /* partitions (>= 2) */
   uint32_t hidden;         /* hidden width */
@@ -268,9 +269,12 @@ typedef struct kg_learned_params {
   uint32_t epochs;         /* passes over the sample */
   uint32_t batch;          /* rows per training step */
   float learning_rate;     /* Adam's */
-  uint32_t reserved;
+  uint32_t flags;          /* KG_LEARNED_RANDOM_INIT: start from random weights instead of
+                              the sample's nearest-part classifier */
   uint64_t seed;
 } kg_learned_params;
+
+#define KG_LEARNED_RANDOM_INIT 1u
 
 typedef struct kg_learned_stats {
   uint64_t fallback_rows;  /* rows searched against every row (low confidence) */

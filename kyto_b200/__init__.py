@@ -22,6 +22,7 @@ LIB_PATH = _HERE / "libkyto_gpu.so"
 
 KG_OK, KG_ERR_INVALID, KG_ERR_DEVICE, KG_ERR_OOM, KG_CANCELLED, KG_ERR_TIMEOUT, KG_ERR_STATE = range(7)
 KG_U32, KG_F32 = 0, 1
+KG_LEARNED_RANDOM_INIT = 1
 NO_GENE = 0xFFFFFFFF
 
 # kyto's error registry (errors.toml): the status a call returns -> kyto's code.
@@ -109,14 +110,15 @@ class LearnedParams(ctypes.Structure):
         ("epochs", ctypes.c_uint32),
         ("batch", ctypes.c_uint32),
         ("learning_rate", ctypes.c_float),
-        ("reserved", ctypes.c_uint32),
+        ("flags", ctypes.c_uint32),
         ("seed", ctypes.c_uint64),
     ]
 
     def __init__(self, n_parts=1024, hidden=256, n_probe=8, confidence=0.9,
-                 train_cells=200_000, epochs=6, batch=4096, learning_rate=1e-3, seed=0):
+                 train_cells=200_000, epochs=6, batch=4096, learning_rate=1e-3, seed=0,
+                 random_init=False):
         super().__init__(n_parts, hidden, n_probe, confidence, train_cells, epochs, batch,
-                         learning_rate, 0, seed)
+                         learning_rate, KG_LEARNED_RANDOM_INIT if random_init else 0, seed)
 
 
 class LearnedStats(ctypes.Structure):

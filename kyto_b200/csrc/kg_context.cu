@@ -54,6 +54,8 @@ void kg_close(kg_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  ctx->knn_ws.reset();
+  cudaStreamSynchronize(ctx->stream);
   for (const kg_ctx::SessionRes& r : ctx->free_res) {
     cudaStreamSynchronize(r.stream);
     cusolverDnDestroy(r.cusolver);

@@ -163,6 +163,10 @@ struct kg_ctx {
   };
   std::mutex res_mu;
   std::vector<SessionRes> free_res;
+  // The exact kNN's candidate slices (n x 512 keys and rows: 16 GB at 4M rows), kept and
+  // grown between calls so a search does not wait on the pool for them; the searches
+  // of one context run one at a time on its stream.
+  kg::DeviceBuffer<uint8_t> knn_ws;
   const volatile int32_t* cancel = nullptr;
   std::atomic<uint64_t> done{0}, total{0};
   int sm_count = 0;

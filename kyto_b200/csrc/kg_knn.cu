@@ -19,6 +19,9 @@
 #include <cfloat>
 #include <cmath>
 #include <vector>
+#include <tuple>
+#include <mutex>
+#include <map>
 
 #include <cstdlib>
 #include <string>
@@ -577,6 +580,25 @@ __global__ void compact_flags_kernel(const uint32_t* flag, uint64_t n, uint32_t*
   if (r < n && flag[r]) list[atomicAdd(count, 1u)] = (uint32_t)r;
 }
 
+// The query slots whose candidates overflowed.
+__global__ void overflow_slots_kernel(const uint32_t* cand_count, uint64_t n, uint32_t* list,
+                                      unsigned int* count) {
+  uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (q < n && cand_count[q] == kOverflow) list[atomicAdd(count, 1u)] = (uint32_t)q;
+}
+
+// The retry's query slots: retry slot j is slot slots[j] of the first pass.
+__global__ void retry_slots_kernel(const uint32_t* slots, uint64_t m, const uint32_t* qrows,
+                                   const uint32_t* q_point, const uint32_t* slot_sample,
+                                   uint32_t* r_qrows, uint32_t* r_qpoint, uint32_t* r_sample) {
+  uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const uint32_t q = slots[j];
+  r_qrows[j] = qrows[q];
+  r_qpoint[j] = q_point ? q_point[q] : q;
+  if (slot_sample) r_sample[j] = slot_sample[q];
+}
+
 namespace {
 
 struct Timer {
@@ -599,6 +621,136 @@ struct Timer {
 };
 
 }  // namespace
+
+// ---------------------------------------------------------------- filter tuning ----
+
+// The pilot's scan: pilot block i is block blocks[i] of the plan (its query slots, its
+// tile list, or every tile from its own when the plan has none). len pass (list NULL)
+// then fill; pilot query slot j of block i is plan slot blocks[i] * block + j.
+__global__ void pilot_plan_kernel(const uint64_t* blocks, uint64_t n_pilot, uint32_t block,
+                                  uint64_t n, const uint32_t* qrows, const uint32_t* q_point,
+                                  const uint32_t* slot_sample, const uint32_t* list_tiles,
+                                  const uint64_t* list_off, uint64_t list_stride,
+                                  uint32_t n_tiles, uint64_t* len, const uint64_t* off,
+                                  uint32_t* p_qrows, uint32_t* p_qpoint, uint32_t* p_sample,
+                                  uint32_t* p_list) {
+  const uint64_t i = blockIdx.x;
+  if (i >= n_pilot) return;
+  const uint64_t qb = blocks[i];
+  uint64_t l0 = 0, count = n_tiles;
+  if (list_tiles) {
+    l0 = list_off ? list_off[qb] : qb * list_stride;
+    count = list_off ? list_off[qb + 1] - l0 : list_stride;
+  }
+  if (!p_list) {
+    if (threadIdx.x == 0) len[i] = count;
+    return;
+  }
+  for (uint32_t j = threadIdx.x; j < block; j += blockDim.x) {
+    const uint64_t src = qb * block + j, dst = i * block + j;
+    if (src >= n) continue;
+    p_qrows[dst] = qrows[src];
+    p_qpoint[dst] = q_point ? q_point[src] : (uint32_t)src;
+    if (slot_sample) p_sample[dst] = slot_sample[src];
+  }
+  const uint32_t own = (uint32_t)((qb * block / 128) % n_tiles);
+  for (uint64_t t = threadIdx.x; t < count; t += blockDim.x)
+    p_list[off[i] + t] = list_tiles ? list_tiles[l0 + t] : (uint32_t)((own + t) % n_tiles);
+}
+
+// The filter kind (fp16 or split operands) that ends the search soonest on this data,
+// measured: each kind filters up to one query block per SM (blocks spread over the
+// scan) against every point, and the estimate is its time scaled to all blocks plus its
+// overflowed queries' full-row searches (1.65e-10 s per point and 50 components, as
+// measured on B200). The kinds return the same graph, so the choice only moves time;
+// it is kept per (rows, components, k) class for later calls in the process.
+FilterKind tune_filter_kind(kg_ctx* ctx, cudaStream_t s, const float* x, uint64_t n,
+                            uint32_t width, uint32_t d, uint32_t k, const ScanPlan& sp,
+                            const FilterScan& scan, const uint32_t* prows, const double* mean,
+                            double scale, const double* max_sq) {
+  static std::mutex mu;
+  static std::map<std::tuple<int, uint32_t, uint32_t>, FilterKind> cache;
+  int n_bits = 0;
+  while (n_bits < 63 && (1ull << n_bits) < n) ++n_bits;
+  const auto key = std::make_tuple(n_bits, d, k);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) return it->second;
+  }
+  const uint32_t block = kTcQueryBlock;
+  const uint64_t n_blocks = (n + block - 1) / block;
+  const uint32_t n_tiles = (uint32_t)((n + 127) / 128);
+  const uint64_t n_pilot = std::min<uint64_t>(n_blocks, (uint64_t)ctx->sm_count);
+  std::vector<uint64_t> h_blocks(n_pilot);
+  for (uint64_t i = 0; i < n_pilot; ++i) h_blocks[i] = i * n_blocks / n_pilot;
+  DeviceBuffer<uint64_t> blocks(n_pilot, s), len(n_pilot + 1, s), off(n_pilot + 1, s);
+  KG_CUDA(cudaMemcpyAsync(blocks.ptr, h_blocks.data(), n_pilot * 8, cudaMemcpyHostToDevice, s));
+  pilot_plan_kernel<<<(unsigned)n_pilot, 256, 0, s>>>(
+      blocks.ptr, n_pilot, block, n, sp.qrows.ptr, scan.q_point, scan.slot_sample,
+      scan.list_tiles, scan.list_off, scan.list_stride, n_tiles, len.ptr, nullptr, nullptr,
+      nullptr, nullptr, nullptr);
+  KG_LAUNCH_CHECK();
+  std::vector<uint64_t> h_off(n_pilot + 1, 0);
+  KG_CUDA(cudaMemcpyAsync(h_off.data() + 1, len.ptr, n_pilot * 8, cudaMemcpyDeviceToHost, s));
+  KG_CUDA(cudaStreamSynchronize(s));
+  for (uint64_t i = 0; i < n_pilot; ++i) h_off[i + 1] += h_off[i];
+  KG_CUDA(cudaMemcpyAsync(off.ptr, h_off.data(), (n_pilot + 1) * 8, cudaMemcpyHostToDevice, s));
+  // Pilot slots past the last row (a partial last block) stay inactive: n_q stops there.
+  const uint64_t last = h_blocks[n_pilot - 1];
+  const uint64_t n_q = std::min<uint64_t>(n_pilot * block, (n_pilot - 1) * block + (n - last * block));
+  DeviceBuffer<uint32_t> p_qrows(n_pilot * block, s), p_qpoint(n_pilot * block, s);
+  DeviceBuffer<uint32_t> p_sample(scan.slot_sample ? n_pilot * block : 0, s);
+  DeviceBuffer<uint32_t> p_list(std::max<uint64_t>(h_off[n_pilot], 1), s);
+  pilot_plan_kernel<<<(unsigned)n_pilot, 256, 0, s>>>(
+      blocks.ptr, n_pilot, block, n, sp.qrows.ptr, scan.q_point, scan.slot_sample,
+      scan.list_tiles, scan.list_off, scan.list_stride, n_tiles, len.ptr, off.ptr, p_qrows.ptr,
+      p_qpoint.ptr, p_sample.ptr, p_list.ptr);
+  KG_LAUNCH_CHECK();
+  FilterScan ps = scan;
+  ps.n_q = n_q;
+  ps.q_point = p_qpoint.ptr;
+  ps.slot_sample = scan.slot_sample ? p_sample.ptr : nullptr;
+  ps.list_tiles = p_list.ptr;
+  ps.list_lb2 = nullptr;
+  ps.list_off = off.ptr;
+  ps.list_stride = 0;
+  const uint32_t cap = kTcCap;
+  DeviceBuffer<float> ck(n_q * cap, s), th(n_q, s);
+  DeviceBuffer<uint32_t> cr(n_q * cap, s), cc(n_q, s);
+  DeviceBuffer<double> qn2(n_q, s), sl(n_q, s);
+  const double per_point = 1.65e-10 * std::max<double>(d, 1) / 50.0;
+  FilterKind best = FilterKind::Fp16;
+  double best_cost = INFINITY;
+  for (FilterKind kind : {FilterKind::Fp16, FilterKind::Split}) {
+    cudaEvent_t a, b;
+    KG_CUDA(cudaEventCreate(&a));
+    KG_CUDA(cudaEventCreate(&b));
+    KG_CUDA(cudaEventRecord(a, s));
+    tc_filter(ctx, s, x, width, d, p_qrows.ptr, prows, ps, mean, scale, max_sq, kind, k, cap,
+              ck.ptr, cr.ptr, cc.ptr, th.ptr, qn2.ptr, sl.ptr, nullptr);
+    KG_CUDA(cudaEventRecord(b, s));
+    KG_CUDA(cudaEventSynchronize(b));
+    float ms = 0.0f;
+    KG_CUDA(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    std::vector<uint32_t> h_cc(n_q);
+    KG_CUDA(cudaMemcpyAsync(h_cc.data(), cc.ptr, n_q * 4, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+    uint64_t over = 0;
+    for (uint32_t c : h_cc) over += c == kOverflow;
+    const double cost = ms * 1e-3 * (double)n_blocks / (double)n_pilot +
+                        (double)over / (double)n_q * (double)n * (double)n * per_point;
+    if (cost < best_cost) {
+      best_cost = cost;
+      best = kind;
+    }
+  }
+  std::lock_guard<std::mutex> lock(mu);
+  cache[key] = best;
+  return best;
+}
 
 // The exact search on device rows: every row's k nearest other rows by (kyto key, row)
 // into out.key / out.row (n x k). `plan` chooses the tensor-core filter's scan (NULL:
@@ -630,11 +782,12 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
   // filter otherwise or on request (KYTO_GPU_KNN_FILTER=simt|fp16|split|bf16). All give
   // the same graph.
   const char* choice = std::getenv("KYTO_GPU_KNN_FILTER");
-  std::string filter = choice ? choice : "fp16";
-  bool tc = !brute && d + 3 <= 64 && (filter == "fp16" || filter == "bf16" || filter == "split");
+  std::string filter = choice ? choice : "auto";
+  bool tc = !brute && d + 3 <= 64 &&
+            (filter == "auto" || filter == "fp16" || filter == "bf16" || filter == "split");
   if (batch && !brute && !tc)
     fail(KG_ERR_INVALID, "batched neighbors: the tensor-core filter (at most 61 components)");
-  const FilterKind kind = filter == "bf16"    ? FilterKind::Bf16
+  FilterKind kind = filter == "bf16"    ? FilterKind::Bf16
                           : filter == "split" ? FilterKind::Split
                                               : FilterKind::Fp16;
   if (brute) {
@@ -644,8 +797,15 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
   } else if (tc) {
     check_cancel(ctx);
     const uint32_t cap = kTcCap;
-    DeviceBuffer<float> cand_key(n * cap, s), thr(n, s);
-    DeviceBuffer<uint32_t> cand_row(n * cap, s), cand_count(n, s);
+    const size_t slice = (size_t)n * cap * 4;
+    if (ctx->knn_ws.count < 2 * slice) {
+      ctx->knn_ws.reset();
+      ctx->knn_ws.alloc(2 * slice, s);
+    }
+    float* cand_key = reinterpret_cast<float*>(ctx->knn_ws.ptr);
+    uint32_t* cand_row = reinterpret_cast<uint32_t*>(ctx->knn_ws.ptr + slice);
+    DeviceBuffer<float> thr(n, s);
+    DeviceBuffer<uint32_t> cand_count(n, s);
     DeviceBuffer<double> qn2(n, s), slack_d(n, s), max_sq(1, s);
     Timer tf(s);
     const double scale = tc_scale(x, n, width, d, mean.ptr, max_sq.ptr, s);
@@ -703,18 +863,71 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
       scan.sample_first = batch->d_first.ptr;
     }
     const uint32_t* prows = sp.prows.ptr ? sp.prows.ptr : sp.qrows.ptr;
+    if (filter == "auto") {
+      kind = tune_filter_kind(ctx, s, x, n, width, d, k, sp, scan, prows, mean.ptr, scale,
+                              max_sq.ptr);
+      trace.mark("filter tuning");
+    }
+    DeviceBuffer<uint16_t> point_ops;  // kept for the overflow retry
     tc_filter(ctx, s, x, width, d, sp.qrows.ptr, prows, scan, mean.ptr, scale, max_sq.ptr,
-              kind, k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
-              qn2.ptr, slack_d.ptr, &trace);
+              kind, k, cap, cand_key, cand_row, cand_count.ptr, thr.ptr,
+              qn2.ptr, slack_d.ptr, &trace, &point_ops);
     filter_ms += tf.stop_ms();
     check_cancel(ctx);
     Timer tr(s);
     rank_kernel<<<blocks_for(n * 32, kRankWarps * 32), kRankWarps * 32, 0, s>>>(
-        x, width, d, 0, n, k, cap, cand_key.ptr, cand_row.ptr, cand_count.ptr, thr.ptr,
+        x, width, d, 0, n, k, cap, cand_key, cand_row, cand_count.ptr, thr.ptr,
         slack_d.ptr, 1.0 / (scale * scale), qn2.ptr, sp.qrows.ptr, prows, out.key.ptr,
         out.row.ptr, full_flag.ptr, n_cand.ptr);
     KG_LAUNCH_CHECK();
     rank_ms += tr.stop_ms();
+    // Queries whose candidates overflowed (more than the slots hold within the slack of
+    // their k-th: dense regions) get a second filter pass with room for kTcRetryCap
+    // candidates, scanning every point tile; only those that overflow again are searched
+    // in full below. The retry's rank overwrites their entries and flags.
+    DeviceBuffer<uint32_t> over(n, s);
+    DeviceBuffer<unsigned int> n_over(1, s);
+    n_over.zero();
+    overflow_slots_kernel<<<blocks_for(n, 256), 256, 0, s>>>(cand_count.ptr, n, over.ptr,
+                                                             n_over.ptr);
+    KG_LAUNCH_CHECK();
+    unsigned int h_over = 0;
+    KG_CUDA(cudaMemcpyAsync(&h_over, n_over.ptr, 4, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+    for (uint64_t r0 = 0; r0 < h_over; r0 += kTcRetryChunk) {
+      check_cancel(ctx);
+      const uint64_t m = std::min<uint64_t>(kTcRetryChunk, h_over - r0);
+      DeviceBuffer<uint32_t> r_qrows(m, s), r_qpoint(m, s), r_sample(batch ? m : 0, s);
+      retry_slots_kernel<<<blocks_for(m, 256), 256, 0, s>>>(
+          over.ptr + r0, m, sp.qrows.ptr, sp.q_point.ptr, batch ? slot_sample.ptr : nullptr,
+          r_qrows.ptr, r_qpoint.ptr, r_sample.ptr);
+      KG_LAUNCH_CHECK();
+      FilterScan rs = scan;
+      rs.n_q = m;
+      rs.q_point = r_qpoint.ptr;
+      rs.slot_sample = batch ? r_sample.ptr : nullptr;
+      rs.list_tiles = nullptr;
+      rs.list_lb2 = nullptr;
+      rs.list_off = nullptr;
+      rs.list_stride = 0;
+      DeviceBuffer<float> r_key(m * kTcRetryCap, s), r_thr(m, s);
+      DeviceBuffer<uint32_t> r_row(m * kTcRetryCap, s), r_count(m, s);
+      DeviceBuffer<double> r_qn2(m, s), r_slack(m, s);
+      Timer trf(s);
+      tc_filter(ctx, s, x, width, d, r_qrows.ptr, prows, rs, mean.ptr, scale, max_sq.ptr, kind,
+                k, kTcRetryCap, r_key.ptr, r_row.ptr, r_count.ptr, r_thr.ptr, r_qn2.ptr,
+                r_slack.ptr, nullptr, &point_ops);
+      filter_ms += trf.stop_ms();
+      Timer trr(s);
+      rank_kernel<<<blocks_for(m * 32, kRankWarps * 32), kRankWarps * 32, 0, s>>>(
+          x, width, d, 0, m, k, kTcRetryCap, r_key.ptr, r_row.ptr, r_count.ptr, r_thr.ptr,
+          r_slack.ptr, 1.0 / (scale * scale), r_qn2.ptr, r_qrows.ptr, prows, out.key.ptr,
+          out.row.ptr, full_flag.ptr, n_cand.ptr);
+      KG_LAUNCH_CHECK();
+      rank_ms += trr.stop_ms();
+    }
+    out.retried = h_over;
+    trace.mark("overflow retry");
     ctx->done = n;
   } else {
     const uint32_t cap = kCandidateCap;

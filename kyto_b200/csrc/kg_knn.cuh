@@ -24,7 +24,7 @@ constexpr int kFullWarps = 8;
 struct KnnResult {
   DeviceBuffer<double> key;    // n x k, ascending by (key, row)
   DeviceBuffer<uint32_t> row;
-  uint64_t candidates = 0, rows_full = 0;
+  uint64_t candidates = 0, rows_full = 0, retried = 0;
   double filter_ms = 0, rank_ms = 0;
 };
 

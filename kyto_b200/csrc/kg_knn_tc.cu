@@ -131,7 +131,7 @@ __device__ __noinline__ void tc_compact(QueryState& st, float* ck, uint32_t* cr,
     }
   }
   st.count = kept;
-  if (st.count > kTcCandidateLimit) st.overflowed = true;
+  if (st.count > (cap >> 1)) st.overflowed = true;
   st.compact_at = min(max(2 * st.count, 64u), cap);
 }
 
@@ -174,6 +174,21 @@ __device__ __noinline__ void tc_offer(QueryState& st, float* smallest, uint32_t 
 // seen) move into registers for the chunk: an insertion is 2 KR branch-free min/max
 // (v[i] = max(v[i-1], min(v[i], key)) on the old values), no dependent memory access.
 // Inline: a call here would save and restore the epilogue's live registers each time.
+// v[kb] for a power-of-two KR: a tree of selects on the bits of kb (depth log2 KR).
+template <int KR>
+__device__ __forceinline__ float select_kth(const float (&v)[KR], uint32_t kb) {
+  float a[KR];
+#pragma unroll
+  for (int i = 0; i < KR; ++i) a[i] = v[i];
+#pragma unroll
+  for (int lvl = 0; (KR >> lvl) > 1; ++lvl) {
+    const bool hi = (kb >> lvl) & 1u;
+#pragma unroll
+    for (int i = 0; i < (KR >> (lvl + 1)); ++i) a[i] = hi ? a[2 * i + 1] : a[2 * i];
+  }
+  return a[0];
+}
+
 template <int KR>
 __device__ __forceinline__ void tc_offer_chunk(QueryState& st, float* smallest, uint32_t k,
                                                double slack2, const float* keys, uint32_t mask,
@@ -190,12 +205,15 @@ __device__ __forceinline__ void tc_offer_chunk(QueryState& st, float* smallest, 
         tc_offer(st, smallest, k, slack2, key, (uint32_t)p, ck, cr, cap);
     }
   } else {
+    static_assert((KR & (KR - 1)) == 0, "register top-k width: a power of two");
     float v[KR];
 #pragma unroll
     for (int i = 0; i < KR; ++i) v[i] = smallest[i];
-    float kth = v[0];
-#pragma unroll
-    for (int i = 1; i < KR; ++i) kth = (i == (int)k - 1) ? v[i] : kth;
+    const uint32_t kb = k - 1;
+    // The slack as the f32 it was rounded up to: the threshold kth + slack rounded up in
+    // one f32 add (__fadd_ru: never below the exact sum).
+    const float sl2f = (float)slack2;
+    float kth = select_kth<KR>(v, kb);
     bool changed = false;
     while (mask && !st.overflowed) {
       const int j = __ffs(mask) - 1;
@@ -212,10 +230,8 @@ __device__ __forceinline__ void tc_offer_chunk(QueryState& st, float* smallest, 
           v[i] = fmaxf(prev, fminf(cur, key));
           prev = cur;
         }
-        kth = v[0];
-#pragma unroll
-        for (int i = 1; i < KR; ++i) kth = (i == (int)k - 1) ? v[i] : kth;
-        if (kth < INFINITY) st.th = round_up_f32d((double)kth + slack2);
+        kth = select_kth<KR>(v, kb);
+        if (kth < INFINITY) st.th = __fadd_ru(kth, sl2f);
         changed = true;
       }
       if (key <= st.th) tc_append(st, key, (uint32_t)p, ck, cr, cap);
@@ -761,20 +777,27 @@ void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint32_t width, uint
                const double* mean, double scale, const double* max_sq, FilterKind kind,
                uint32_t k, uint32_t cap, float* cand_key, uint32_t* cand_row,
                uint32_t* cand_count, float* threshold, double* qn2, double* slack_d,
-               Trace* trace) {
+               Trace* trace, DeviceBuffer<uint16_t>* point_ops) {
   if (d + 3 > (uint32_t)kTcK) fail(KG_ERR_INVALID, "tensor-core filter: more than 61 components");
   const uint64_t n_q = scan.n_q, n_p = scan.n_p;
   const bool split = kind == FilterKind::Split, bf16 = kind == FilterKind::Bf16;
   const uint32_t width_op = split ? 2u * kTcK : (uint32_t)kTcK;
-  DeviceBuffer<uint16_t> aq(n_q * width_op, s), bp(n_p * width_op, s);
+  // The point operands: built here, or the caller's from an earlier call on the same
+  // points, kind, centre and scale (kept in *point_ops when given).
+  DeviceBuffer<uint16_t> own;
+  DeviceBuffer<uint16_t>& bp = point_ops ? *point_ops : own;
+  const bool build_points = bp.count != n_p * width_op;
+  if (build_points) bp.alloc(n_p * width_op, s);
+  DeviceBuffer<uint16_t> aq(n_q * width_op, s);
   DeviceBuffer<float> slack2(n_q, s);
   if (split) {
     tc_split_operands_kernel<<<blocks_for(n_q * 32, 256), 256, 0, s>>>(
         x, n_q, width, d, qrows, mean, scale, max_sq, true, (__half*)aq.ptr, qn2, slack2.ptr,
         slack_d);
-    tc_split_operands_kernel<<<blocks_for(n_p * 32, 256), 256, 0, s>>>(
-        x, n_p, width, d, prows, mean, scale, max_sq, false, (__half*)bp.ptr, nullptr, nullptr,
-        nullptr);
+    if (build_points)
+      tc_split_operands_kernel<<<blocks_for(n_p * 32, 256), 256, 0, s>>>(
+          x, n_p, width, d, prows, mean, scale, max_sq, false, (__half*)bp.ptr, nullptr, nullptr,
+          nullptr);
   } else {
     const double u = bf16 ? 0x1p-8 : 0x1p-11;
     const double eta = bf16 ? 0x1p-134 : 0x1p-25;
@@ -782,16 +805,18 @@ void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint32_t width, uint
       tc_operands_kernel<__nv_bfloat16><<<blocks_for(n_q, 128), 128, 0, s>>>(
           x, n_q, width, d, qrows, mean, scale, u, eta, max_sq, true, (__nv_bfloat16*)aq.ptr,
           qn2, slack2.ptr, slack_d);
-      tc_operands_kernel<__nv_bfloat16><<<blocks_for(n_p, 128), 128, 0, s>>>(
-          x, n_p, width, d, prows, mean, scale, u, eta, max_sq, false, (__nv_bfloat16*)bp.ptr,
-          nullptr, nullptr, nullptr);
+      if (build_points)
+        tc_operands_kernel<__nv_bfloat16><<<blocks_for(n_p, 128), 128, 0, s>>>(
+            x, n_p, width, d, prows, mean, scale, u, eta, max_sq, false, (__nv_bfloat16*)bp.ptr,
+            nullptr, nullptr, nullptr);
     } else {
       tc_operands_kernel<__half><<<blocks_for(n_q, 128), 128, 0, s>>>(
           x, n_q, width, d, qrows, mean, scale, u, eta, max_sq, true, (__half*)aq.ptr, qn2,
           slack2.ptr, slack_d);
-      tc_operands_kernel<__half><<<blocks_for(n_p, 128), 128, 0, s>>>(
-          x, n_p, width, d, prows, mean, scale, u, eta, max_sq, false, (__half*)bp.ptr, nullptr,
-          nullptr, nullptr);
+      if (build_points)
+        tc_operands_kernel<__half><<<blocks_for(n_p, 128), 128, 0, s>>>(
+            x, n_p, width, d, prows, mean, scale, u, eta, max_sq, false, (__half*)bp.ptr, nullptr,
+            nullptr, nullptr);
     }
   }
   KG_LAUNCH_CHECK();

@@ -7,8 +7,11 @@
 
 namespace kg {
 
-constexpr uint32_t kTcCap = 512;             // candidate slots per query
-constexpr uint32_t kTcCandidateLimit = 256;  // candidates kept after a compaction, at most
+constexpr uint32_t kTcCap = 512;             // candidate slots per query (a query
+                                             // overflows when more than half stay after
+                                             // a compaction)
+constexpr uint32_t kTcRetryCap = 8192;       // slots per query in the overflow retry
+constexpr uint64_t kTcRetryChunk = 65536;    // queries per retry pass
 constexpr uint32_t kTcQueryBlock = 256;      // query slots per block of the fp16/bf16 filter
 
 // The filter's operands: fp16 or bf16 (one 64-wide row: the components and the norm), or
@@ -54,7 +57,7 @@ void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint32_t width, uint
                const double* mean, double scale, const double* max_sq, FilterKind kind,
                uint32_t k, uint32_t cap, float* cand_key, uint32_t* cand_row,
                uint32_t* cand_count, float* threshold, double* qn2, double* slack_d,
-               Trace* trace = nullptr);
+               Trace* trace = nullptr, DeviceBuffer<uint16_t>* point_ops = nullptr);
 
 void max_kernel_launch(const double* v, uint64_t n, double* out, cudaStream_t s);
 

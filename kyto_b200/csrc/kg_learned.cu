@@ -6,16 +6,21 @@
 //
 //   1. sample: m evenly strided rows; their exact graph (the exact search itself);
 //   2. partitions: k-means of the sample into P parts (kg_cluster.cuh);
-//   3. training: soft targets = the parts of a row and of its k neighbours, soft-target
-//      cross-entropy, Adam, `epochs` passes of seeded shuffles;
+//   3. training: the network starts as the parts' nearest-centre classifier (or from
+//      random weights on request); soft targets = the parts of a row and of its k
+//      neighbours, soft-target cross-entropy, Adam, `epochs` passes of seeded shuffles;
 //   4. calibration: the softmax temperature whose confidence (the probed parts' summed
-//      softmax) best predicts, by log loss over the sample, that a row's exact
-//      neighbours live in the parts it probes;
-//   5. index: the network's top-`probe` parts for every row and their confidence at that
-//      temperature, each row stored in its top part;
-//   6. search: query slots sorted by (fallback, top part); each block of 256 query slots
-//      scans the tiles of the union of its queries' probed parts (every tile if one of
-//      them falls back), then the exact re-rank.
+//      softmax) best predicts, by cross-entropy over the sample, the share of a row's
+//      exact neighbours that live in the parts it probes;
+//   5. index: the network's top-`probe` parts for every row (each row stored in its top
+//      part) and its 32 most probable parts with their probabilities at that
+//      temperature;
+//   6. confidence: the rows in top-part order form provisional blocks of 256 query
+//      slots; a row's confidence is its probability in the parts its block probes (the
+//      union of its rows' top-`probe` parts), and it falls back below the threshold;
+//   7. search: query slots sorted by (fallback, top part); each block of 256 query slots
+//      scans the tiles of the parts of the provisional blocks its rows came from (every
+//      tile if one of them falls back), then the exact re-rank.
 #include <cuda_bf16.h>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -125,36 +130,57 @@ __global__ void part_starts_kernel(const uint32_t* sorted, uint64_t n, uint32_t 
 }
 
 constexpr uint32_t kProbeThreads = 256;
+constexpr uint32_t kMassParts = 32;  // parts per row whose probabilities the index keeps
 
 // One CTA per block of query slots: the tiles of the union of its queries' probed parts
 // (a bitmap over tiles), or every tile when one of them falls back. Count pass (list
 // NULL): the number of tiles into len[B]; fill pass: the tiles in increasing order at
 // list + off[B].
 __global__ void __launch_bounds__(kProbeThreads)
-probe_tiles_kernel(const uint32_t* qrows, uint64_t n, const uint32_t* top, uint32_t probe,
-                   const uint8_t* fallback, const uint32_t* part_start, uint32_t n_tiles,
-                   uint32_t block, uint64_t* len, const uint64_t* off, uint32_t* list) {
-  extern __shared__ uint32_t bits[];  // n_tiles bits
+probe_tiles_kernel(const uint32_t* qrows, uint64_t n, const uint32_t* prov_of_row,
+                   const uint32_t* prov_parts, uint32_t pwords, const uint8_t* fallback,
+                   const uint32_t* part_start, uint32_t n_tiles, uint32_t block, uint64_t* len,
+                   const uint64_t* off, uint32_t* list) {
+  // Dynamic shared memory: n_tiles bits of tiles, then pwords words of parts.
+  extern __shared__ uint32_t bits[];
+  uint32_t* parts_bm = bits + (n_tiles + 31) / 32;
   __shared__ int any_fallback;
   __shared__ uint32_t word_base[kProbeThreads + 1];
+  __shared__ uint32_t prov[kProbeThreads];
   const uint32_t words = (n_tiles + 31) / 32;
   for (uint32_t w = threadIdx.x; w < words; w += kProbeThreads) bits[w] = 0;
+  for (uint32_t w = threadIdx.x; w < pwords; w += kProbeThreads) parts_bm[w] = 0;
   if (threadIdx.x == 0) any_fallback = 0;
   __syncthreads();
+  // The parts of every provisional block a row of this block came from (a run of rows
+  // from the same one contributes its bitmap once).
   const uint64_t q0 = blockIdx.x * (uint64_t)block;
-  for (uint32_t i = threadIdx.x; i < block; i += kProbeThreads) {
-    const uint64_t q = q0 + i;
-    if (q >= n) break;
-    const uint32_t row = qrows[q];
-    if (fallback[row]) {
-      any_fallback = 1;
-      continue;
+  for (uint32_t i0 = 0; i0 < block; i0 += kProbeThreads) {
+    const uint64_t q = q0 + i0 + threadIdx.x;
+    uint32_t b = 0xFFFFFFFFu;
+    if (i0 + threadIdx.x < block && q < n) {
+      const uint32_t row = qrows[q];
+      if (fallback[row]) any_fallback = 1;
+      else b = prov_of_row[row];
     }
-    for (uint32_t t = 0; t < probe; ++t) {
-      const uint32_t p = top[(uint64_t)row * probe + t];
-      const uint32_t a = part_start[p], e = part_start[p + 1];
+    prov[threadIdx.x] = b;
+    __syncthreads();
+    if (b != 0xFFFFFFFFu && (threadIdx.x == 0 || prov[threadIdx.x - 1] != b))
+      for (uint32_t w = 0; w < pwords; ++w) {
+        const uint32_t v = prov_parts[(uint64_t)b * pwords + w];
+        if (v) atomicOr(&parts_bm[w], v);
+      }
+    __syncthreads();
+  }
+  // The tiles of those parts.
+  for (uint32_t pw = 0; pw < pwords; ++pw) {
+    uint32_t v = parts_bm[pw];
+    while (v) {
+      const uint32_t part = pw * 32 + (uint32_t)(__ffs(v) - 1);
+      v &= v - 1;
+      const uint32_t a = part_start[part], e = part_start[part + 1];
       if (a == e) continue;
-      for (uint32_t tile = a >> 7; tile <= (e - 1) >> 7; ++tile)
+      for (uint32_t tile = (a >> 7) + threadIdx.x; tile <= (e - 1) >> 7; tile += kProbeThreads)
         atomicOr(&bits[tile >> 5], 1u << (tile & 31));
     }
   }
@@ -222,7 +248,8 @@ int bits_for_value(uint64_t v) {
 // at each of n_temps temperatures (device array temps): conf[t * n + row].
 void learned_probe(const Mlp& mlp, const float* x, uint64_t n, uint32_t width, uint32_t probe,
                    const float* temps, uint32_t n_temps, uint32_t* top, float* conf,
-                   cudaStream_t s) {
+                   cudaStream_t s, uint32_t n_mass = 0, uint16_t* mass_part = nullptr,
+                   float* mass_prob = nullptr) {
   const uint64_t chunk = 65536;
   MlpBatch b;
   b.alloc(mlp.sh, (uint32_t)std::min<uint64_t>(chunk, n), s);
@@ -231,24 +258,83 @@ void learned_probe(const Mlp& mlp, const float* x, uint64_t n, uint32_t width, u
     b.rows = rows;
     mlp.forward(x + r0 * width, width, b, s);
     top_parts(b.z3.ptr, rows, mlp.sh.parts, probe, top + r0 * probe, conf + r0, n, s, temps,
-              n_temps);
+              n_temps, n_mass, mass_part ? mass_part + r0 * n_mass : nullptr,
+              mass_prob ? mass_prob + r0 * n_mass : nullptr);
   }
 }
 
-// contained[i] = 1 if every neighbour of sample row i (its k graph rows) lives in a part
-// row i probes (a row lives in its top part): the event the confidence should predict.
-__global__ void contained_kernel(const uint32_t* top, uint32_t probe, const uint32_t* nbr,
-                                 uint64_t m, uint32_t k, uint8_t* contained) {
+// covered[i] = the share of sample row i's k graph neighbours that live in a part row i
+// probes (a row lives in its top part): what the confidence should predict.
+__global__ void covered_kernel(const uint32_t* top, uint32_t probe, const uint32_t* nbr,
+                               uint64_t m, uint32_t k, float* covered) {
   const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= m) return;
-  bool all = true;
-  for (uint32_t j = 0; j < k && all; ++j) {
+  uint32_t hits = 0;
+  for (uint32_t j = 0; j < k; ++j) {
     const uint32_t home = top[(uint64_t)nbr[i * k + j] * probe];
     bool in = false;
     for (uint32_t t = 0; t < probe; ++t) in |= top[i * probe + t] == home;
-    all = in;
+    hits += in ? 1u : 0u;
   }
-  contained[i] = all ? 1 : 0;
+  covered[i] = (float)hits / (float)k;
+}
+
+// Per provisional block (rows in top-part order, `block` slots a block): the parts its
+// rows probe, as a bitmap of pwords words.
+__global__ void block_parts_kernel(const uint32_t* rows, uint64_t n, const uint32_t* top,
+                                   uint32_t probe, uint32_t block, uint32_t pwords,
+                                   uint32_t* bitmap) {
+  extern __shared__ uint32_t pb[];
+  for (uint32_t w = threadIdx.x; w < pwords; w += blockDim.x) pb[w] = 0;
+  __syncthreads();
+  const uint64_t q0 = blockIdx.x * (uint64_t)block;
+  for (uint32_t i = threadIdx.x; i < block; i += blockDim.x) {
+    const uint64_t q = q0 + i;
+    if (q >= n) break;
+    const uint32_t row = rows[q];
+    for (uint32_t t = 0; t < probe; ++t) {
+      const uint32_t part = top[(uint64_t)row * probe + t];
+      atomicOr(&pb[part >> 5], 1u << (part & 31));
+    }
+  }
+  __syncthreads();
+  for (uint32_t w = threadIdx.x; w < pwords; w += blockDim.x)
+    bitmap[(uint64_t)blockIdx.x * pwords + w] = pb[w];
+}
+
+// Each row's confidence: its probability (over its n_mass most probable parts) in the
+// parts its provisional block probes, which its search will probe (it is searched in at
+// least those); and the row's provisional block.
+__global__ void union_conf_kernel(const uint32_t* rows, uint64_t n, uint32_t block,
+                                  const uint32_t* bitmap, uint32_t pwords,
+                                  const uint16_t* mass_part, const float* mass_prob,
+                                  uint32_t n_mass, uint32_t* prov_of_row, float* conf) {
+  const uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const uint32_t row = rows[q];
+  const uint64_t b = q / block;
+  prov_of_row[row] = (uint32_t)b;
+  const uint32_t* bm = bitmap + b * pwords;
+  float c = 0.0f;
+  for (uint32_t j = 0; j < n_mass; ++j) {
+    const uint32_t part = mass_part[(uint64_t)row * n_mass + j];
+    if ((bm[part >> 5] >> (part & 31)) & 1u) c += mass_prob[(uint64_t)row * n_mass + j];
+  }
+  conf[row] = c;
+}
+
+// The squared distance of each sample row to its cluster's centre (f64).
+__global__ void sq_to_centre_kernel(const float* xs, uint64_t m, uint32_t d, const uint32_t* label,
+                                    const double* centre, uint32_t ldc, double* out) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const double* c = centre + (uint64_t)label[i] * ldc;
+  double s = 0.0;
+  for (uint32_t j = 0; j < d; ++j) {
+    const double v = (double)xs[i * d + j] - c[j];
+    s += v * v;
+  }
+  out[i] = s;
 }
 
 // The temperatures the calibration tries (1: the network's own softmax).
@@ -361,6 +447,23 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
     trace.mark("sample parts");
     Mlp mlp;
     mlp.init(d, P.hidden, parts, P.seed, s);
+    if (!(P.flags & KG_LEARNED_RANDOM_INIT) && P.hidden >= 2 * d) {
+      // Start from the parts' own nearest-centre classifier, at the scale 1 / (mean
+      // squared distance of a sample row to its centre), and let training move it
+      // toward where the rows' neighbours live.
+      DeviceBuffer<double> sq(m, s);
+      sq_to_centre_kernel<<<blocks_for(m, 256), 256, 0, s>>>(xs.ptr, m, d, cl.label.ptr,
+                                                             cl.centre.ptr, kClusterDim, sq.ptr);
+      KG_LAUNCH_CHECK();
+      std::vector<double> hsq(m);
+      KG_CUDA(cudaMemcpyAsync(hsq.data(), sq.ptr, m * 8, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaStreamSynchronize(s));
+      double mean_sq = 0.0;
+      for (double v : hsq) mean_sq += v;
+      mean_sq /= (double)m;
+      const float beta = mean_sq > 0.0 ? (float)(1.0 / mean_sq) : 1.0f;
+      mlp.init_from_centres(cl.centre.ptr, cl.K, kClusterDim, beta, s);
+    }
     const uint32_t batch = (uint32_t)std::min<uint64_t>(P.batch, m);
     MlpBatch b;
     b.alloc(mlp.sh, batch, s);
@@ -401,8 +504,8 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
     const double train_ms = ms_since(t_train);
     trace.mark("training");
 
-    // 4. Calibration: the temperature whose confidence best predicts (log loss) that a
-    // sample row's exact neighbours live in the parts it probes.
+    // 4. Calibration: the temperature whose confidence best predicts (cross-entropy) the
+    // share of a sample row's exact neighbours that live in the parts it probes.
     float temperature = 1.0f;
     DeviceBuffer<float> d_temps(kNumTemps, s);
     KG_CUDA(cudaMemcpyAsync(d_temps.ptr, kTemps, sizeof(kTemps), cudaMemcpyHostToDevice, s));
@@ -410,22 +513,21 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
       DeviceBuffer<uint32_t> stop(m * probe, s);
       DeviceBuffer<float> sconf(kNumTemps * m, s);
       learned_probe(mlp, xs.ptr, m, d, probe, d_temps.ptr, kNumTemps, stop.ptr, sconf.ptr, s);
-      DeviceBuffer<uint8_t> cont(m, s);
-      contained_kernel<<<blocks_for(m, 256), 256, 0, s>>>(stop.ptr, probe, sg.row.ptr, m, k,
-                                                          cont.ptr);
+      DeviceBuffer<float> cov(m, s);
+      covered_kernel<<<blocks_for(m, 256), 256, 0, s>>>(stop.ptr, probe, sg.row.ptr, m, k,
+                                                        cov.ptr);
       KG_LAUNCH_CHECK();
-      std::vector<float> hconf(kNumTemps * m);
-      std::vector<uint8_t> hcont(m);
+      std::vector<float> hconf(kNumTemps * m), hcov(m);
       KG_CUDA(cudaMemcpyAsync(hconf.data(), sconf.ptr, hconf.size() * 4, cudaMemcpyDeviceToHost,
                               s));
-      KG_CUDA(cudaMemcpyAsync(hcont.data(), cont.ptr, m, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaMemcpyAsync(hcov.data(), cov.ptr, m * 4, cudaMemcpyDeviceToHost, s));
       KG_CUDA(cudaStreamSynchronize(s));
       double best = INFINITY;
       for (uint32_t t = 0; t < kNumTemps; ++t) {
         double loss = 0.0;
         for (uint64_t i = 0; i < m; ++i) {
           const double p = std::min(std::max((double)hconf[t * m + i], 1e-6), 1.0 - 1e-6);
-          loss -= hcont[i] ? std::log(p) : std::log1p(-p);
+          loss -= hcov[i] * std::log(p) + (1.0 - hcov[i]) * std::log1p(-p);
         }
         if (loss < best) {
           best = loss;
@@ -439,8 +541,13 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
     auto t_index = now();
     DeviceBuffer<uint32_t> top(n * probe, s);
     DeviceBuffer<float> conf(n, s);
+    // Each row's most probable parts with their probabilities: the mass its search covers.
+    const uint32_t n_mass = std::min<uint32_t>(kMassParts, parts);
+    DeviceBuffer<uint16_t> mass_part(n * n_mass, s);
+    DeviceBuffer<float> mass_prob(n * n_mass, s);
     KG_CUDA(cudaMemcpyAsync(d_temps.ptr, &temperature, 4, cudaMemcpyHostToDevice, s));
-    learned_probe(mlp, x, n, width, probe, d_temps.ptr, 1, top.ptr, conf.ptr, s);
+    learned_probe(mlp, x, n, width, probe, d_temps.ptr, 1, top.ptr, conf.ptr, s, n_mass,
+                  mass_part.ptr, mass_prob.ptr);
     KG_CUDA(cudaStreamSynchronize(s));
     const double index_ms = ms_since(t_index);
     trace.mark("index");
@@ -463,8 +570,24 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
       DeviceBuffer<uint32_t> slot_of_row(nn, s);
       inverse_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(sp.prows.ptr, nn, slot_of_row.ptr);
       KG_LAUNCH_CHECK();
+      // Confidence: the rows in top-part order form provisional query blocks; a row's
+      // confidence is its probability in the parts its provisional block probes, and its
+      // final block will probe at least those (the union over its rows' provisional
+      // blocks).
+      const uint64_t n_prov = (nn + qblock - 1) / qblock;
+      const uint32_t pwords = (parts + 31) / 32;
+      DeviceBuffer<uint32_t> prov_parts(n_prov * pwords, s), prov_of_row(nn, s);
+      DeviceBuffer<float> uconf(nn, s);
+      block_parts_kernel<<<(unsigned)n_prov, 256, pwords * 4, s>>>(
+          sp.prows.ptr, nn, top.ptr, probe, qblock, pwords, prov_parts.ptr);
+      KG_LAUNCH_CHECK();
+      union_conf_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(sp.prows.ptr, nn, qblock,
+                                                            prov_parts.ptr, pwords, mass_part.ptr,
+                                                            mass_prob.ptr, n_mass,
+                                                            prov_of_row.ptr, uconf.ptr);
+      KG_LAUNCH_CHECK();
       // Queries: by (fallback, top part).
-      query_key_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(top.ptr, conf.ptr, nn, probe,
+      query_key_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(top.ptr, uconf.ptr, nn, probe,
                                                            P.confidence, parts, key.ptr, iota.ptr,
                                                            fallback.ptr);
       KG_LAUNCH_CHECK();
@@ -476,7 +599,7 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
       // The blocks' tile lists (count, scan, fill).
       const uint64_t n_blocks = (nn + qblock - 1) / qblock;
       const uint32_t n_tiles = (uint32_t)((nn + 127) / 128);
-      const size_t smem = (size_t)((n_tiles + 31) / 32) * 4;
+      const size_t smem = (size_t)((n_tiles + 31) / 32 + pwords) * 4;
       if (smem > 200 * 1024)
         fail(KG_ERR_INVALID, "kg_knn_learned: too many rows for the tile bitmap");
       static std::once_flag attr;
@@ -487,8 +610,8 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
       DeviceBuffer<uint64_t> len(n_blocks + 1, s);
       len.zero();
       probe_tiles_kernel<<<(unsigned)n_blocks, kProbeThreads, smem, s>>>(
-          sp.qrows.ptr, nn, top.ptr, probe, fallback.ptr, part_start.ptr, n_tiles, qblock,
-          len.ptr, nullptr, nullptr);
+          sp.qrows.ptr, nn, prov_of_row.ptr, prov_parts.ptr, pwords, fallback.ptr,
+          part_start.ptr, n_tiles, qblock, len.ptr, nullptr, nullptr);
       KG_LAUNCH_CHECK();
       sp.list_off.alloc(n_blocks + 1, s);
       size_t t2 = 0;
@@ -505,8 +628,8 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
       scanned_tiles = total;
       sp.list_tiles.alloc(std::max<uint64_t>(total, 1), s);
       probe_tiles_kernel<<<(unsigned)n_blocks, kProbeThreads, smem, s>>>(
-          sp.qrows.ptr, nn, top.ptr, probe, fallback.ptr, part_start.ptr, n_tiles, qblock,
-          len.ptr, sp.list_off.ptr, sp.list_tiles.ptr);
+          sp.qrows.ptr, nn, prov_of_row.ptr, prov_parts.ptr, pwords, fallback.ptr,
+          part_start.ptr, n_tiles, qblock, len.ptr, sp.list_off.ptr, sp.list_tiles.ptr);
       KG_LAUNCH_CHECK();
       tr.mark("probe lists");
     };

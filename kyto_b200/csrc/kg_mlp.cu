@@ -209,7 +209,8 @@ __global__ void init_kernel(float* p, uint64_t begin, uint64_t n, uint32_t fan_i
 constexpr uint32_t kMaxTemps = 16;
 __global__ void top_parts_kernel(const float* z, uint64_t rows, uint32_t parts, uint32_t probe,
                                  const float* temps, uint32_t n_temps, uint32_t* top,
-                                 float* conf, uint64_t conf_stride) {
+                                 float* conf, uint64_t conf_stride, uint32_t n_mass,
+                                 uint16_t* mass_part, float* mass_prob) {
   const uint64_t row = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const unsigned lane = threadIdx.x & 31u;
   if (row >= rows) return;
@@ -217,11 +218,17 @@ __global__ void top_parts_kernel(const float* z, uint64_t rows, uint32_t parts, 
   float m = -INFINITY;
   for (uint32_t p = lane; p < parts; p += 32) m = fmaxf(m, zr[p]);
   for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+  float sum0 = 0.0f;  // the first temperature's normaliser, for the kept probabilities
+  if (n_mass) {
+    for (uint32_t p = lane; p < parts; p += 32) sum0 += __expf(temps[0] * (zr[p] - m));
+    for (int o = 16; o; o >>= 1) sum0 += __shfl_xor_sync(0xFFFFFFFFu, sum0, o);
+  }
   float picked[kMaxTemps];
   for (uint32_t t = 0; t < n_temps; ++t) picked[t] = 0.0f;
   uint32_t prev_p = 0xFFFFFFFFu;
   float prev_v = INFINITY;
-  for (uint32_t t = 0; t < probe; ++t) {
+  const uint32_t rounds = max(probe, n_mass);
+  for (uint32_t t = 0; t < rounds; ++t) {
     // The best (value, part) strictly after (prev_v, prev_p) in the order.
     float bv = -INFINITY;
     uint32_t bp = 0xFFFFFFFFu;
@@ -241,8 +248,14 @@ __global__ void top_parts_kernel(const float* z, uint64_t rows, uint32_t parts, 
         bp = op;
       }
     }
-    if (lane == 0) top[row * probe + t] = bp;
-    for (uint32_t i = 0; i < n_temps; ++i) picked[i] += __expf(temps[i] * (bv - m));
+    if (t < n_mass && lane == 0) {
+      mass_part[row * n_mass + t] = (uint16_t)bp;
+      mass_prob[row * n_mass + t] = __expf(temps[0] * (bv - m)) / sum0;
+    }
+    if (t < probe) {
+      if (lane == 0) top[row * probe + t] = bp;
+      for (uint32_t i = 0; i < n_temps; ++i) picked[i] += __expf(temps[i] * (bv - m));
+    }
     prev_v = bv;
     prev_p = bp;
   }
@@ -304,6 +317,52 @@ void Mlp::init(uint32_t din, uint32_t hidden, uint32_t parts, uint64_t seed, cud
     KG_LAUNCH_CHECK();
   }
   step = 0;
+  refresh(s);
+}
+
+__global__ void centre_init_kernel(float* p, MlpShape sh, const double* c, uint32_t K,
+                                   uint32_t ldc, float beta) {
+  const uint32_t din = sh.din, H = sh.hidden, P = sh.parts;
+  const uint64_t n1 = 2ull * din * din, n2 = 2ull * din * H, n3 = (uint64_t)P * H;
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n1) {  // W1 rows 0..2din: +e_r, then -e_(r - din)
+    const uint64_t r = i / din, j = i % din;
+    p[sh.w_off[0] + r * din + j] = r < din ? (j == r ? 1.0f : 0.0f) : (j == r - din ? -1.0f : 0.0f);
+    return;
+  }
+  i -= n1;
+  if (i < n2) {  // W2 rows 0..2din: the identity on units 0..2din
+    const uint64_t r = i / H, j = i % H;
+    p[sh.w_off[1] + r * H + j] = j == r ? 1.0f : 0.0f;
+    return;
+  }
+  i -= n2;
+  if (i < n3) {  // W3: 2 beta c_j on relu(x), -2 beta c_j on relu(-x), 0 elsewhere
+    const uint64_t r = i / H, j = i % H;
+    float v = 0.0f;
+    if (r < K && j < din) v = (float)(2.0 * beta * c[r * ldc + j]);
+    else if (r < K && j < 2ull * din) v = (float)(-2.0 * beta * c[r * ldc + (j - din)]);
+    p[sh.w_off[2] + r * H + j] = v;
+    return;
+  }
+  i -= n3;
+  if (i < P) {  // b3: -beta |c_j|^2 (a part without a centre: far below the others)
+    double sq = 0.0;
+    if (i < K)
+      for (uint32_t j = 0; j < din; ++j) sq += c[i * ldc + j] * c[i * ldc + j];
+    p[sh.b_off[2] + i] = i < K ? (float)(-beta * sq) : -1e4f;
+  }
+}
+
+void Mlp::init_from_centres(const double* centres, uint32_t K, uint32_t ldc, float beta,
+                            cudaStream_t s) {
+  if (sh.hidden < 2 * sh.din) fail(KG_ERR_INVALID, "centre init: hidden below 2 x inputs");
+  if (K > sh.parts) fail(KG_ERR_INVALID, "centre init: more centres than parts");
+  const uint64_t total = 2ull * sh.din * sh.din + 2ull * sh.din * sh.hidden +
+                         (uint64_t)sh.parts * sh.hidden + sh.parts;
+  centre_init_kernel<<<blocks_for(total, 256), 256, 0, s>>>(params.ptr, sh, centres, K, ldc,
+                                                            beta);
+  KG_LAUNCH_CHECK();
   refresh(s);
 }
 
@@ -375,11 +434,13 @@ void Mlp::adam(float lr, cudaStream_t s) {
 
 void top_parts(const float* logits, uint64_t rows, uint32_t parts, uint32_t probe, uint32_t* top,
                float* confidence, uint64_t conf_stride, cudaStream_t s, const float* temps,
-               uint32_t n_temps) {
+               uint32_t n_temps, uint32_t n_mass, uint16_t* mass_part, float* mass_prob) {
   if (n_temps < 1 || n_temps > kMaxTemps) fail(KG_ERR_INVALID, "top_parts: 1..16 temperatures");
+  if (n_mass > parts || parts > 65536) fail(KG_ERR_INVALID, "top_parts: kept parts");
   top_parts_kernel<<<blocks_for(rows * 32, 256), 256, 0, s>>>(logits, rows, parts, probe, temps,
                                                              n_temps, top, confidence,
-                                                             conf_stride);
+                                                             conf_stride, n_mass, mass_part,
+                                                             mass_prob);
   KG_LAUNCH_CHECK();
 }
 

@@ -42,6 +42,13 @@ class Mlp {
   uint64_t step = 0;
 
   void init(uint32_t din, uint32_t hidden, uint32_t parts, uint64_t seed, cudaStream_t s);
+  // Set the network to the nearest-centre classifier of K centres (device, K x ldc f64;
+  // part j = centre j, K <= parts): logit j = beta (2 c_j.x - |c_j|^2), i.e.
+  // -beta |x - c_j|^2 up to a per-row constant. The first 2 din hidden units carry
+  // relu(x) and relu(-x) through both layers; the other units keep their random weights
+  // with no say in the logits yet. Needs hidden >= 2 din.
+  void init_from_centres(const double* centres, uint32_t K, uint32_t ldc, float beta,
+                         cudaStream_t s);
   void set_params(const float* host_or_device, cudaStream_t s);
   // The bf16 copy from the f32 masters.
   void refresh(cudaStream_t s);
@@ -54,13 +61,14 @@ class Mlp {
   void adam(float lr, cudaStream_t s);
 };
 
-// The top `probe` parts of each row of logits (rows x parts, f32) by probability
-// (descending, ties to the lower part) and their summed probability.
 // Each row's top `probe` parts and, for each of n_temps temperatures (device array
 // temps; the logits are multiplied by each), the parts' summed softmax:
-// confidence[t * conf_stride + row].
+// confidence[t * conf_stride + row]. With n_mass, also each row's n_mass most probable
+// parts and their probabilities at the first temperature (mass_part, mass_prob: rows x
+// n_mass).
 void top_parts(const float* logits, uint64_t rows, uint32_t parts, uint32_t probe,
                uint32_t* top, float* confidence, uint64_t conf_stride, cudaStream_t s,
-               const float* temps, uint32_t n_temps);
+               const float* temps, uint32_t n_temps, uint32_t n_mass = 0,
+               uint16_t* mass_part = nullptr, float* mass_prob = nullptr);
 
 }  // namespace kg

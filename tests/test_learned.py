@@ -79,18 +79,25 @@ def test_learned_search_recall_and_what_training_gains(monkeypatch, candidate_fi
     common = dict(n_parts=512, hidden=128, n_probe=8, confidence=0.0, train_cells=30_000,
                   batch=2048, learning_rate=2e-3, seed=1)
     g1, s1 = K.neighbors_learned(x, 15, params=K.LearnedParams(epochs=8, **common), ctx=ctx)
-    g0, s0 = K.neighbors_learned(x, 15, params=K.LearnedParams(epochs=0, **common), ctx=ctx)
-    r1, r0 = _recall(g1, exact), _recall(g0, exact)
+    # Without training: the network as initialised, the k-means parts' nearest-centre
+    # classifier (k-means centroid probing), and random weights.
+    gk, sk = K.neighbors_learned(x, 15, params=K.LearnedParams(epochs=0, **common), ctx=ctx)
+    g0, s0 = K.neighbors_learned(x, 15, params=K.LearnedParams(epochs=0, random_init=True,
+                                                               **common), ctx=ctx)
+    r1, rk, r0 = _recall(g1, exact), _recall(gk, exact), _recall(g0, exact)
     # Every distance returned is the true distance of its pair (the exact re-rank).
     n = x.shape[0]
     rows = np.repeat(np.arange(n), 14)
     d_true = np.sqrt(((x[rows].astype(np.float64) - x[g1.indices.astype(np.int64)]) ** 2).sum(1))
     np.testing.assert_allclose(g1.distances, d_true, rtol=1e-5, atol=1e-5)
     assert s1.fallback_rows == 0 and np.isfinite(s1.final_loss)
-    # What training gains: the trained network's proposals find the neighbours while the
-    # query blocks scan a fraction of the tiles an untrained network's proposals make
-    # them scan (random parts spread over nearly every tile).
+    # What training gains: the trained network's proposals find more of the neighbours
+    # than k-means centroid probing while its query blocks scan fewer tiles, and a
+    # fraction of the tiles an untrained random network makes them scan (random parts
+    # spread over nearly every tile).
     assert r1 > 0.95, r1
+    assert r1 >= rk and s1.scanned_tiles < sk.scanned_tiles, (r1, rk, s1.scanned_tiles,
+                                                              sk.scanned_tiles)
     assert s1.scanned_tiles < 0.5 * s0.scanned_tiles, (s1.scanned_tiles, s0.scanned_tiles, r1, r0)
     n_tiles = (n + 127) // 128
     n_blocks = (n + 255) // 256
