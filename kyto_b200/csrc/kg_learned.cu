@@ -389,6 +389,7 @@ kg_status kg_learned_gradients(kg_ctx* ctx, uint32_t din, uint32_t hidden, uint3
     b.alloc(mlp.sh, rows, s);
     mlp.forward(dx, din, b, s);
     mlp.backward(dl, n_labels, b, s);
+    mlp.check(s);
     KG_CUDA(cudaMemcpyAsync(grads, mlp.grads.ptr, mlp.sh.total * 4, cudaMemcpyDefault, s));
     KG_CUDA(cudaMemcpyAsync(row_loss, b.row_loss.ptr, (uint64_t)rows * 4, cudaMemcpyDefault, s));
     if (logits)
@@ -501,6 +502,7 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
       final_loss = (float)(acc / batch);
     }
     KG_CUDA(cudaStreamSynchronize(s));
+    mlp.check(s);
     const double train_ms = ms_since(t_train);
     trace.mark("training");
 
@@ -548,6 +550,7 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
     KG_CUDA(cudaMemcpyAsync(d_temps.ptr, &temperature, 4, cudaMemcpyHostToDevice, s));
     learned_probe(mlp, x, n, width, probe, d_temps.ptr, 1, top.ptr, conf.ptr, s, n_mass,
                   mass_part.ptr, mass_prob.ptr);
+    mlp.check(s);
     KG_CUDA(cudaStreamSynchronize(s));
     const double index_ms = ms_since(t_index);
     trace.mark("index");

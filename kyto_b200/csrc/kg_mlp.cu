@@ -4,8 +4,14 @@
 #include "kg_mlp.cuh"
 
 #include <cmath>
+#include <mutex>
+
+#include "kg_sm100.cuh"
+#include "kg_tma.cuh"
 
 namespace kg {
+
+using namespace sm100;
 
 namespace {
 
@@ -109,13 +115,154 @@ void gemm(int M, int N, int K, const TA* A, int lda, const TB* B, int ldb, float
   KG_LAUNCH_CHECK();
 }
 
-// x (rows x din, stride ldx) rounded to bf16.
+// x (rows x din, stride ldx) rounded to bf16, rows of ld0 >= din (zeros past din).
 __global__ void to_bf16_rows_kernel(const float* x, uint64_t rows, uint32_t din, uint64_t ldx,
-                                    __nv_bfloat16* out) {
+                                    uint32_t ld0, __nv_bfloat16* out) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (i >= rows * din) return;
-  uint64_t r = i / din, c = i % din;
-  out[i] = __float2bfloat16_rn(x[r * ldx + c]);
+  if (i >= rows * ld0) return;
+  uint64_t r = i / ld0, c = i % ld0;
+  out[i] = __float2bfloat16_rn(c < din ? x[r * ldx + c] : 0.0f);
+}
+
+// ---------------------------------------------------------------- tensor-core layers --
+//
+// One layer's z = A W^T + b on the 5th-generation tensor cores: A (rows x K bf16, K a
+// multiple of 64 up to 256) and W (N x K bf16, row-major: K-major like A), f32 sums in
+// tensor memory. One CTA per 128-row x tn-column tile (tn = min(N, 256)), 128 threads:
+// thread 0 loads every K block of both tiles by TMA (128-byte swizzle) and issues the
+// MMAs (M = 128, N = tn, K = 16); then each thread reads its row from TMEM and writes
+// z (f32) and, for a hidden layer, h = bf16(relu(z)).
+constexpr int kTcRows = 128, kTcNMax = 256, kTcKMax = 256, kTcKBox = 64;
+
+struct MlpTcSmem {
+  uint8_t a[kTcKMax / kTcKBox][kTcRows * 128];  // K blocks of the rows' tile
+  uint8_t b[kTcKMax / kTcKBox][kTcNMax * 128];  // K blocks of the weights' tile
+  uint64_t full, done;
+  uint32_t tmem_base;
+  int abort;
+};
+constexpr size_t kMlpTcSmemBytes = sizeof(MlpTcSmem) + 1024;
+static_assert(kMlpTcSmemBytes <= 227 * 1024, "MLP layer shared memory");
+
+template <int EPI>
+__global__ void __launch_bounds__(128, 1)
+mlp_tc_kernel(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb,
+              int M, int K, int tn, uint32_t idesc, const float* __restrict__ bias, float* z,
+              int ldz, __nv_bfloat16* h, int ldh, int* error) {
+  extern __shared__ uint8_t smem_raw[];
+  MlpTcSmem& sm = *reinterpret_cast<MlpTcSmem*>(smem_raw + ((1024u - (smem_addr(smem_raw) & 1023u)) & 1023u));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.y * kTcRows, n0 = blockIdx.x * tn;
+  const int kb = K / kTcKBox;
+  volatile int* abort = &sm.abort;
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.full, 1);
+    mbar_init(&sm.done, 1);
+    sm.abort = 0;
+    fence_mbar_init();
+  }
+  if (warp == 0) tmem_alloc(&sm.tmem_base, kTcNMax);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sm.tmem_base;
+  if (threadIdx.x == 0) {
+    prefetch_tmap(&ta);
+    prefetch_tmap(&tb);
+    mbar_arrive_expect_tx(&sm.full, (uint32_t)kb * (uint32_t)(kTcRows + tn) * 128u);
+    for (int j = 0; j < kb; ++j) {
+      tma_load_2d(sm.a[j], &ta, &sm.full, j * kTcKBox, m0);
+      tma_load_2d(sm.b[j], &tb, &sm.full, j * kTcKBox, n0);
+    }
+    if (mbar_wait(&sm.full, 0, abort)) {
+      tc_fence_after();
+      for (int j = 0; j < kb; ++j) {
+        const uint32_t aa = smem_addr(sm.a[j]), bb = smem_addr(sm.b[j]);
+#pragma unroll
+        for (int kk = 0; kk < kTcKBox / 16; ++kk)
+          mma_f16(tmem, desc_k_sw128(aa + kk * 32), desc_k_sw128(bb + kk * 32), idesc,
+                  (j | kk) > 0);
+      }
+    } else {
+      // The loads never all landed: let them finish (bounded) before the CTA leaves.
+      for (uint32_t i = 0; i < kWaitPolls && !mbar_try_wait(&sm.full, 0); ++i) __nanosleep(64);
+    }
+    mma_commit(&sm.done);
+  }
+  __syncwarp();
+  const bool ok = mbar_wait(&sm.done, 0, abort);
+  tc_fence_after();
+  __syncwarp();
+  if (ok && !*abort) {
+    const int row = m0 + warp * 32 + lane;
+    for (int c = 0; c < tn / 32; ++c) {
+      uint32_t r[32];
+      tmem_ld_32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c * 32u, r);
+      tmem_wait_ld();
+      if (row >= M) continue;
+      const int n = n0 + c * 32;
+      float v[32];
+#pragma unroll
+      for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]) + bias[n + j];
+      float4* zp = reinterpret_cast<float4*>(z + (size_t)row * ldz + n);
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
+        zp[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+      if (EPI == kEpiBiasReluBf16) {
+        uint32_t packed[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const __nv_bfloat162 pr =
+              __floats2bfloat162_rn(fmaxf(v[2 * j], 0.0f), fmaxf(v[2 * j + 1], 0.0f));
+          packed[j] = *reinterpret_cast<const uint32_t*>(&pr);
+        }
+        uint4* hp = reinterpret_cast<uint4*>(h + (size_t)row * ldh + n);
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          hp[j] = make_uint4(packed[4 * j], packed[4 * j + 1], packed[4 * j + 2], packed[4 * j + 3]);
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (*abort && threadIdx.x == 0) atomicExch(error, 1);
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, kTcNMax);
+  }
+}
+
+template <int EPI>
+void mlp_tc_gemm(int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv_bfloat16* W,
+                 int ldw, const float* bias, float* z, int ldz, __nv_bfloat16* h, int ldh,
+                 int* error, cudaStream_t s) {
+  if (M == 0) return;
+  const int tn = N < kTcNMax ? N : kTcNMax;
+  if (K % kTcKBox || K > kTcKMax || tn % 32 || N % tn)
+    fail(KG_ERR_INVALID, "MLP layer: shape outside the tensor-core tiles");
+  static std::once_flag attr;
+  std::call_once(attr, [] {
+    KG_CUDA(cudaFuncSetAttribute(mlp_tc_kernel<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kMlpTcSmemBytes));
+  });
+  const CUtensorMap ta = tma_map_2d_16bit(A, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (uint64_t)K,
+                                          (uint64_t)M, (uint64_t)lda * 2, kTcKBox, kTcRows);
+  const CUtensorMap tb = tma_map_2d_16bit(W, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, (uint64_t)K,
+                                          (uint64_t)N, (uint64_t)ldw * 2, kTcKBox, (uint32_t)tn);
+  const uint32_t idesc = idesc_f32acc(1u, kTcRows, (uint32_t)tn);
+  dim3 grid((unsigned)(N / tn), (unsigned)((M + kTcRows - 1) / kTcRows));
+  mlp_tc_kernel<EPI><<<grid, 128, kMlpTcSmemBytes, s>>>(ta, tb, M, K, tn, idesc, bias, z, ldz, h,
+                                                        ldh, error);
+  KG_LAUNCH_CHECK();
+}
+
+// W1 (hidden x din) as bf16 rows of 64 (zeros past din): the first layer's tensor-core
+// operand.
+__global__ void pad_w1_kernel(const float* w1, uint32_t hidden, uint32_t din, __nv_bfloat16* out) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= (uint64_t)hidden * 64) return;
+  const uint64_t r = i / 64, c = i % 64;
+  out[i] = __float2bfloat16_rn(c < din ? w1[r * din + c] : 0.0f);
 }
 
 // One warp per row: p = softmax(z); dz = (p - t) / rows with t the share of each part
@@ -271,9 +418,9 @@ __global__ void top_parts_kernel(const float* z, uint64_t rows, uint32_t parts, 
 
 void MlpShape::layout() {
   uint64_t o = 0;
-  auto take = [&](uint64_t n) {
+  auto take = [&](uint64_t n) {  // 8 elements: 16-byte aligned as bf16 too
     uint64_t at = o;
-    o += (n + 3) & ~3ull;
+    o += (n + 7) & ~7ull;
     return at;
   };
   for (int l = 0; l < 3; ++l) {
@@ -285,7 +432,7 @@ void MlpShape::layout() {
 
 void MlpBatch::alloc(const MlpShape& sh, uint32_t n, cudaStream_t s) {
   rows = n;
-  h0.alloc((uint64_t)n * sh.din, s);
+  h0.alloc((uint64_t)n * sh.h0_ld(), s);
   h1.alloc((uint64_t)n * sh.hidden, s);
   h2.alloc((uint64_t)n * sh.hidden, s);
   z1.alloc((uint64_t)n * sh.hidden, s);
@@ -311,6 +458,9 @@ void Mlp::init(uint32_t din, uint32_t hidden, uint32_t parts, uint64_t seed, cud
   m2.alloc(sh.total, s);
   m2.zero();
   wb.alloc(sh.total, s);
+  if (sh.tensor_cores()) w1p.alloc((uint64_t)sh.hidden * 64, s);
+  tc_error.alloc(1, s);
+  tc_error.zero();
   for (int l = 0; l < 3; ++l) {
     uint64_t nw = (uint64_t)sh.out(l) * sh.in(l);
     init_kernel<<<blocks_for(nw, 256), 256, 0, s>>>(params.ptr, sh.w_off[l], nw, sh.in(l), seed);
@@ -374,17 +524,40 @@ void Mlp::set_params(const float* src, cudaStream_t s) {
 void Mlp::refresh(cudaStream_t s) {
   refresh_kernel<<<blocks_for(sh.total, 256), 256, 0, s>>>(params.ptr, sh.total, wb.ptr);
   KG_LAUNCH_CHECK();
+  if (sh.tensor_cores()) {
+    pad_w1_kernel<<<blocks_for((uint64_t)sh.hidden * 64, 256), 256, 0, s>>>(
+        params.ptr + sh.w_off[0], sh.hidden, sh.din, w1p.ptr);
+    KG_LAUNCH_CHECK();
+  }
+}
+
+void Mlp::check(cudaStream_t s) const {
+  int h = 0;
+  KG_CUDA(cudaMemcpyAsync(&h, tc_error.ptr, 4, cudaMemcpyDeviceToHost, s));
+  KG_CUDA(cudaStreamSynchronize(s));
+  if (h) fail(KG_ERR_TIMEOUT, "an MLP layer on the tensor cores gave up waiting on its loads");
 }
 
 void Mlp::forward(const float* x, uint64_t ldx, MlpBatch& b, cudaStream_t s) const {
   const int n = (int)b.rows, din = (int)sh.din, h = (int)sh.hidden, P = (int)sh.parts;
-  to_bf16_rows_kernel<<<blocks_for((uint64_t)n * din, 256), 256, 0, s>>>(x, n, din, ldx, b.h0.ptr);
+  const int ld0 = (int)sh.h0_ld();
+  to_bf16_rows_kernel<<<blocks_for((uint64_t)n * ld0, 256), 256, 0, s>>>(x, n, din, ldx, ld0,
+                                                                        b.h0.ptr);
   KG_LAUNCH_CHECK();
   const __nv_bfloat16* W = wb.ptr;
   const float* bias = params.ptr;
+  if (sh.tensor_cores()) {
+    mlp_tc_gemm<kEpiBiasReluBf16>(n, h, ld0, b.h0.ptr, ld0, w1p.ptr, ld0, bias + sh.b_off[0],
+                                  b.z1.ptr, h, b.h1.ptr, h, tc_error.ptr, s);
+    mlp_tc_gemm<kEpiBiasReluBf16>(n, h, h, b.h1.ptr, h, W + sh.w_off[1], h, bias + sh.b_off[1],
+                                  b.z2.ptr, h, b.h2.ptr, h, tc_error.ptr, s);
+    mlp_tc_gemm<kEpiBias>(n, P, h, b.h2.ptr, h, W + sh.w_off[2], h, bias + sh.b_off[2], b.z3.ptr,
+                          P, nullptr, 0, tc_error.ptr, s);
+    return;
+  }
   // z = h W^T + b: W is out x in row-major, so B(k, n) = W[n * in + k].
   gemm<__nv_bfloat16, __nv_bfloat16, false, true, kEpiBiasReluBf16>(
-      n, h, din, b.h0.ptr, din, W + sh.w_off[0], din, b.z1.ptr, h, s, bias + sh.b_off[0],
+      n, h, din, b.h0.ptr, ld0, W + sh.w_off[0], din, b.z1.ptr, h, s, bias + sh.b_off[0],
       b.h1.ptr, h);
   gemm<__nv_bfloat16, __nv_bfloat16, false, true, kEpiBiasReluBf16>(
       n, h, h, b.h1.ptr, h, W + sh.w_off[1], h, b.z2.ptr, h, s, bias + sh.b_off[1], b.h2.ptr, h);
@@ -416,8 +589,8 @@ void Mlp::backward(const uint32_t* labels, uint32_t L, MlpBatch& b, cudaStream_t
                                                          h, b.dz1.ptr, h, s, nullptr, nullptr, 0,
                                                          b.z1.ptr, h);
   // Layer 1.
-  gemm<float, __nv_bfloat16, true, false, kEpiStore>(h, din, n, b.dz1.ptr, h, b.h0.ptr, din,
-                                                     G + sh.w_off[0], din, s);
+  gemm<float, __nv_bfloat16, true, false, kEpiStore>(h, din, n, b.dz1.ptr, h, b.h0.ptr,
+                                                     (int)sh.h0_ld(), G + sh.w_off[0], din, s);
   column_sums_kernel<<<(h + 63) / 64, 1024, 0, s>>>(b.dz1.ptr, n, h, h, G + sh.b_off[0]);
   KG_LAUNCH_CHECK();
 }

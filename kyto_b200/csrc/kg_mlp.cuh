@@ -22,6 +22,15 @@ struct MlpShape {
   uint32_t in(int l) const { return l == 0 ? din : hidden; }
   uint32_t out(int l) const { return l == 2 ? parts : hidden; }
   void layout();
+  // The layers run on the tensor cores (a shape their tiles take: din <= 64, hidden a
+  // multiple of 64 up to 256, parts a multiple of 32 up to 256 or of 256), else on the
+  // SIMT GEMM.
+  bool tensor_cores() const {
+    return din <= 64 && hidden % 64 == 0 && hidden <= 256 && parts % 32 == 0 &&
+           (parts <= 256 || parts % 256 == 0);
+  }
+  // The row stride of the first layer's bf16 input (64 on the tensor cores).
+  uint32_t h0_ld() const { return tensor_cores() ? 64u : din; }
 };
 
 // Activations of one batch (rows x widths), kept for the backward pass.
@@ -39,6 +48,8 @@ class Mlp {
   MlpShape sh;
   DeviceBuffer<float> params, grads, m1, m2;
   DeviceBuffer<__nv_bfloat16> wb;  // bf16 copy of the packed parameters
+  DeviceBuffer<__nv_bfloat16> w1p; // W1 as bf16 rows of 64 (the tensor-core layer's operand)
+  DeviceBuffer<int> tc_error;      // set if a tensor-core layer gave up waiting
   uint64_t step = 0;
 
   void init(uint32_t din, uint32_t hidden, uint32_t parts, uint64_t seed, cudaStream_t s);
@@ -59,6 +70,8 @@ class Mlp {
   // `grads`; the per-row losses stay in b.row_loss.
   void backward(const uint32_t* labels, uint32_t L, MlpBatch& b, cudaStream_t s);
   void adam(float lr, cudaStream_t s);
+  // Fails (KG_ERR_TIMEOUT) if a tensor-core layer gave up waiting since init.
+  void check(cudaStream_t s) const;
 };
 
 // Each row's top `probe` parts and, for each of n_temps temperatures (device array
