@@ -861,7 +861,7 @@ struct TcHeld {
     sm = sm_count;
     build_blocked(indptr, col, val, n, g, nnz, false, bx, s);
     trace.mark("blocked X");
-    build_blocked(indptr, col, val, n, g, nnz, true, bxt, s);
+    transpose_blocked(bx, bxt, s);
     trace.mark("blocked X^T");
     dt_hi.alloc(64 * n_ld, s);
     dt_lo.alloc(64 * n_ld, s);

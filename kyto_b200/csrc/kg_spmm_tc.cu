@@ -560,6 +560,111 @@ __global__ void blocked_values_kernel(const uint64_t* ptr, const uint32_t* col, 
   }
 }
 
+// ---------------------------------------------------------------- the transpose --
+//
+// X^T's blocked layout from X's (no pass over the CSR, no atomics). Block (G, c) of X^T
+// (genes 128 G.., cells 32 c..) holds the 32 cell rows 32 (c % 4).. of the four X blocks
+// (tile c / 4, gene chunks 4 G ..4 G + 3), transposed: its gene row 32 i + j has bit l set
+// where X block (c / 4, 4 G + i) has a value at cell row 32 (c % 4) + l, gene column j.
+// One warp per X^T block; lane l reads cell row 32 (c % 4) + l of each source block.
+
+// Source block i of X^T block (G, c), or ~0 past X's gene chunks.
+__device__ __forceinline__ uint64_t transpose_source(uint32_t G, uint32_t c, int i,
+                                                     uint32_t x_chunks) {
+  const uint32_t chunk = 4 * G + (uint32_t)i;
+  return chunk < x_chunks ? (uint64_t)(c / 4) * x_chunks + chunk : ~0ull;
+}
+
+__global__ void transpose_count_kernel(const uint64_t* x_off, const uint8_t* x_data,
+                                       uint32_t x_chunks, uint32_t t_tiles, uint32_t t_chunks,
+                                       uint32_t* counts) {
+  const uint64_t b = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  if (b >= (uint64_t)t_tiles * t_chunks) return;
+  const uint32_t G = (uint32_t)(b / t_chunks), c = (uint32_t)(b % t_chunks);
+  uint32_t count = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const uint64_t src = transpose_source(G, c, i, x_chunks);
+    if (src == ~0ull || x_off[src + 1] == x_off[src]) continue;
+    const uint32_t* masks = reinterpret_cast<const uint32_t*>(x_data + x_off[src] * 16);
+    count += __popc(masks[32 * (c % 4) + lane]);
+  }
+  for (int o = 16; o; o >>= 1) count += __shfl_xor_sync(0xFFFFFFFFu, count, o);
+  if (lane == 0) counts[b] = count;
+}
+
+__global__ void transpose_fill_kernel(const uint64_t* x_off, const uint8_t* x_data,
+                                      uint32_t x_chunks, uint32_t t_tiles, uint32_t t_chunks,
+                                      const uint64_t* t_off, uint8_t* t_data) {
+  const uint64_t b = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  if (b >= (uint64_t)t_tiles * t_chunks || t_off[b + 1] == t_off[b]) return;
+  const uint32_t G = (uint32_t)(b / t_chunks), c = (uint32_t)(b % t_chunks);
+  const uint32_t group = c % 4;  // the source blocks' cell rows 32 group..
+  uint32_t src_mask[4], src_pre[4], mine[4];
+  const float* src_vals[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    src_mask[i] = 0;
+    src_pre[i] = 0;
+    src_vals[i] = nullptr;
+    const uint64_t src = transpose_source(G, c, i, x_chunks);
+    if (src != ~0ull && x_off[src + 1] != x_off[src]) {
+      const uint8_t* blk = x_data + x_off[src] * 16;
+      const uint32_t* masks = reinterpret_cast<const uint32_t*>(blk);
+      src_vals[i] = reinterpret_cast<const float*>(blk + kMaskBytes);
+      src_mask[i] = masks[32 * group + lane];
+      // Values of the source block before cell row 32 group + lane (rows in order).
+      uint32_t base = 0;
+      for (uint32_t q = 0; q < group; ++q) base += __popc(masks[32 * q + lane]);
+      for (int o = 16; o; o >>= 1) base += __shfl_xor_sync(0xFFFFFFFFu, base, o);
+      const uint32_t v = __popc(src_mask[i]);
+      uint32_t incl = v;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+        if (lane >= o) incl += t;
+      }
+      src_pre[i] = base + incl - v;
+    }
+    // The 32 x 32 bit transpose: gene j's cell mask is the ballot of bit j.
+    mine[i] = 0;
+#pragma unroll 4
+    for (int j = 0; j < 32; ++j) {
+      const uint32_t t = __ballot_sync(0xFFFFFFFFu, (src_mask[i] >> j) & 1u);
+      if ((int)lane == j) mine[i] = t;
+    }
+  }
+  uint8_t* out = t_data + t_off[b] * 16;
+  uint32_t* out_masks = reinterpret_cast<uint32_t*>(out);
+  float* out_vals = reinterpret_cast<float*>(out + kMaskBytes);
+  uint32_t carry = 0;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    out_masks[32 * i + lane] = mine[i];
+    // This gene row's first value: the values of the X^T rows before it.
+    const uint32_t v = __popc(mine[i]);
+    uint32_t incl = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    uint32_t at = carry + incl - v;
+    carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
+    // Cells in order: cell l's value sits at its rank in source block i.
+    const uint32_t below = (1u << lane) - 1u;  // gene columns before this lane's
+    const float* sv = src_vals[i];
+    const uint32_t mi = mine[i];
+    for (int l = 0; l < 32; ++l) {
+      const uint32_t pre = __shfl_sync(0xFFFFFFFFu, src_pre[i], l);
+      const uint32_t m = __shfl_sync(0xFFFFFFFFu, src_mask[i], l);
+      const uint32_t has = (mi >> l) & 1u;
+      if (has) out_vals[at] = sv[pre + __popc(m & below)];
+      at += has;
+    }
+  }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   static std::once_flag once;
@@ -634,6 +739,36 @@ void build_blocked(const uint64_t* ptr, const uint32_t* col, const float* val, u
         ptr, col, val, n_rows, transpose, out.n_chunks, out.off.ptr, prefix.ptr, out.data.ptr);
     KG_LAUNCH_CHECK();
   }
+}
+
+void transpose_blocked(const Blocked& x, Blocked& out, cudaStream_t s) {
+  out.rows = x.K;
+  out.K = x.rows;
+  out.n_tiles = (uint32_t)((out.rows + kRows - 1) / kRows);
+  out.n_chunks = (uint32_t)((out.K + kChunk - 1) / kChunk);
+  const uint64_t nb = (uint64_t)out.n_tiles * out.n_chunks;
+  DeviceBuffer<uint32_t> counts(nb, s);
+  transpose_count_kernel<<<blocks_for(nb * 32, 256), 256, 0, s>>>(
+      x.off.ptr, x.data.ptr, x.n_chunks, out.n_tiles, out.n_chunks, counts.ptr);
+  KG_LAUNCH_CHECK();
+  out.off.alloc(nb + 1, s);
+  block_units_kernel<<<blocks_for(nb + 1, 256), 256, 0, s>>>(counts.ptr, nb, out.off.ptr);
+  KG_LAUNCH_CHECK();
+  counts.reset();
+  size_t temp = 0;
+  KG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, out.off.ptr, out.off.ptr, nb + 1, s));
+  DeviceBuffer<unsigned char> scratch(temp, s);
+  KG_CUDA(cub::DeviceScan::ExclusiveSum(scratch.ptr, temp, out.off.ptr, out.off.ptr, nb + 1, s));
+  uint64_t units = 0;
+  KG_CUDA(cudaMemcpyAsync(&units, out.off.ptr + nb, 8, cudaMemcpyDeviceToHost, s));
+  KG_CUDA(cudaStreamSynchronize(s));
+  out.bytes = units * 16;
+  out.data.alloc(std::max<uint64_t>(out.bytes, 16), s);
+  // Padding past a block's values must read as zero (the expansion loads past the end).
+  out.data.zero();
+  transpose_fill_kernel<<<blocks_for(nb * 32, 256), 256, 0, s>>>(
+      x.off.ptr, x.data.ptr, x.n_chunks, out.n_tiles, out.n_chunks, out.off.ptr, out.data.ptr);
+  KG_LAUNCH_CHECK();
 }
 
 void spmm_tc(const SpmmArgs& a, cudaStream_t s) {

@@ -28,6 +28,10 @@ struct Blocked {
 void build_blocked(const uint64_t* ptr, const uint32_t* col, const float* val, uint64_t n_rows,
                    uint64_t n_cols, uint64_t nnz, bool transpose, Blocked& out, cudaStream_t s);
 
+// The blocked layout of X^T from X's (bit-transposed blocks, values moved by rank): the
+// same bytes build_blocked(..., transpose = true) writes.
+void transpose_blocked(const Blocked& x, Blocked& out, cudaStream_t s);
+
 enum : int { kOutRows = 0, kOutPartial = 1 };
 enum : int { kValuePlain = 0, kValueCentredSquare = 1, kValueOne = 2 };
 
