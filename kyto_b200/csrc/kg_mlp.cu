@@ -3,6 +3,7 @@
 // bit-reproducible run to run.
 #include "kg_mlp.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 
@@ -605,11 +606,102 @@ void Mlp::adam(float lr, cudaStream_t s) {
   refresh(s);
 }
 
+// The same selection for rows of at most 1,024 parts with the row held in registers
+// (lane l: parts l, l + 32, ...): each lane keeps its best part not yet taken, a round
+// takes the warp's best of those (ties to the lower part) and only the lane that gave it
+// looks again. Parts, probabilities and sums come out in the same order and bits as
+// top_parts_kernel's.
+constexpr uint32_t kRegParts = 32;  // parts a lane holds
+__global__ void top_parts_reg_kernel(const float* z, uint64_t rows, uint32_t parts,
+                                     uint32_t probe, const float* temps, uint32_t n_temps,
+                                     uint32_t* top, float* conf, uint64_t conf_stride,
+                                     uint32_t n_mass, uint16_t* mass_part, float* mass_prob) {
+  const uint64_t row = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  if (row >= rows) return;
+  const float* zr = z + row * parts;
+  float v[kRegParts];
+#pragma unroll
+  for (uint32_t j = 0; j < kRegParts; ++j) {
+    const uint32_t p = lane + 32 * j;
+    v[j] = p < parts ? zr[p] : -INFINITY;
+  }
+  float m = -INFINITY;
+#pragma unroll
+  for (uint32_t j = 0; j < kRegParts; ++j)
+    if (lane + 32 * j < parts) m = fmaxf(m, v[j]);
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+  auto lane_sum = [&](float t) {
+    float sum = 0.0f;
+#pragma unroll
+    for (uint32_t j = 0; j < kRegParts; ++j)
+      if (lane + 32 * j < parts) sum += __expf(t * (v[j] - m));
+    for (int o = 16; o; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+    return sum;
+  };
+  const float sum0 = n_mass ? lane_sum(temps[0]) : 0.0f;
+  // The lane's best part not yet taken: (value, slot j), the lowest slot on ties.
+  uint32_t taken = 0;
+  auto lane_best = [&](float& bv, uint32_t& bj) {
+    bv = -INFINITY;
+    bj = 0xFFFFFFFFu;
+#pragma unroll
+    for (uint32_t j = 0; j < kRegParts; ++j) {
+      const bool live = lane + 32 * j < parts && !((taken >> j) & 1u);
+      if (live && (v[j] > bv || bj == 0xFFFFFFFFu)) {
+        bv = v[j];
+        bj = j;
+      }
+    }
+  };
+  float lv;
+  uint32_t lj;
+  lane_best(lv, lj);
+  float picked[kMaxTemps];
+  for (uint32_t t = 0; t < n_temps; ++t) picked[t] = 0.0f;
+  const uint32_t rounds = max(probe, n_mass);
+  for (uint32_t t = 0; t < rounds; ++t) {
+    float bv = lv;
+    uint32_t bp = lj == 0xFFFFFFFFu ? 0xFFFFFFFFu : lane + 32 * lj;
+    for (int o = 16; o; o >>= 1) {
+      const float ov = __shfl_xor_sync(0xFFFFFFFFu, bv, o);
+      const uint32_t op = __shfl_xor_sync(0xFFFFFFFFu, bp, o);
+      if (op != 0xFFFFFFFFu && (bp == 0xFFFFFFFFu || ov > bv || (ov == bv && op < bp))) {
+        bv = ov;
+        bp = op;
+      }
+    }
+    if (t < n_mass && lane == 0) {
+      mass_part[row * n_mass + t] = (uint16_t)bp;
+      mass_prob[row * n_mass + t] = __expf(temps[0] * (bv - m)) / sum0;
+    }
+    if (t < probe) {
+      if (lane == 0) top[row * probe + t] = bp;
+      for (uint32_t i = 0; i < n_temps; ++i) picked[i] += __expf(temps[i] * (bv - m));
+    }
+    if (bp != 0xFFFFFFFFu && bp % 32 == lane) {
+      taken |= 1u << (bp / 32);
+      lane_best(lv, lj);
+    }
+  }
+  for (uint32_t i = 0; i < n_temps; ++i) {
+    const float sum = lane_sum(temps[i]);
+    if (lane == 0) conf[i * conf_stride + row] = picked[i] / sum;
+  }
+}
+
 void top_parts(const float* logits, uint64_t rows, uint32_t parts, uint32_t probe, uint32_t* top,
                float* confidence, uint64_t conf_stride, cudaStream_t s, const float* temps,
                uint32_t n_temps, uint32_t n_mass, uint16_t* mass_part, float* mass_prob) {
   if (n_temps < 1 || n_temps > kMaxTemps) fail(KG_ERR_INVALID, "top_parts: 1..16 temperatures");
   if (n_mass > parts || parts > 65536) fail(KG_ERR_INVALID, "top_parts: kept parts");
+  if (parts <= 32 * kRegParts && std::max(probe, n_mass) <= parts) {
+    top_parts_reg_kernel<<<blocks_for(rows * 32, 256), 256, 0, s>>>(
+        logits, rows, parts, probe, temps, n_temps, top, confidence, conf_stride, n_mass,
+        mass_part, mass_prob);
+    KG_LAUNCH_CHECK();
+    return;
+  }
   top_parts_kernel<<<blocks_for(rows * 32, 256), 256, 0, s>>>(logits, rows, parts, probe, temps,
                                                              n_temps, top, confidence,
                                                              conf_stride, n_mass, mass_part,

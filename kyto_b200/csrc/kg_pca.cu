@@ -1018,6 +1018,7 @@ void kg_pca::push(const uint64_t* in_indptr, const uint32_t* in_idx, const void*
   if (dtype != KG_U32 && dtype != KG_F32) fail(KG_ERR_INVALID, "unknown dtype");
   if (n_rows == 0) return;
   cudaStream_t s = stream;
+  Trace trace(s, "pca_push");
   DeviceBuffer<uint64_t> hp, hc;
   const uint64_t* d_indptr = device_view(in_indptr, n_rows + 1, hp, s);
   uint64_t ends[2];
@@ -1030,8 +1031,10 @@ void kg_pca::push(const uint64_t* in_indptr, const uint32_t* in_idx, const void*
   const uint32_t* d_idx = device_view(in_idx, bnnz, hi, s);
   const void* d_values = device_view((const uint32_t*)in_values, bnnz, hv, s);
   check_indices(d_idx, bnnz, stream_genes, s);
+  trace.mark("checks");
   DeviceBuffer<float> mapped(bnnz, s);
   map_block(d_indptr, d_values, dtype, n_rows, bnnz, target_sum, log1p, mapped.ptr, s);
+  trace.mark("map");
   // Kept entries per row, then their offsets after the held entries.
   DeviceBuffer<uint64_t> kept(n_rows + 1, s);
   kept.zero();
@@ -1048,10 +1051,12 @@ void kg_pca::push(const uint64_t* in_indptr, const uint32_t* in_idx, const void*
   KG_CUDA(cudaStreamSynchronize(s));
   add_offset_kernel<<<blocks_for(n_rows + 1, 256), 256, 0, s>>>(kept.ptr, n_rows + 1, nnz);
   KG_LAUNCH_CHECK();
+  trace.mark("kept counts");
   grow(indptr, n_cells + 1, n_cells + n_rows + 1);
   grow(col, nnz, nnz + added);
   grow(val, nnz, nnz + added);
   grow(cells, n_cells, n_cells + n_rows);
+  trace.mark("held buffers");
   KG_CUDA(cudaMemcpyAsync(indptr.ptr + n_cells, kept.ptr, (n_rows + 1) * 8,
                           cudaMemcpyDeviceToDevice, s));
   write_kept_kernel<<<blocks_for(n_rows * 32, threads), threads, 0, s>>>(
@@ -1074,6 +1079,7 @@ void kg_pca::push(const uint64_t* in_indptr, const uint32_t* in_idx, const void*
   n_cells += n_rows;
   nnz += added;
   KG_CUDA(cudaStreamSynchronize(s));
+  trace.mark("held block");
 }
 
 namespace {
