@@ -66,6 +66,8 @@ def parse() -> argparse.Namespace:
                     help="C5 learned-vs-exact comparison rows (0: skip)")
     ap.add_argument("--batch-samples", type=int, default=64,
                     help="C4 batching-form samples (0: skip)")
+    ap.add_argument("--reserve-gb", type=int, default=40,
+                    help="device memory reserved for the library's pool at open (kg_reserve)")
     return ap.parse_args()
 
 
@@ -258,6 +260,13 @@ def learned_vs_exact(n: int, ctx) -> dict:
 
     graph(exact)
     ex, ex_st, t_ex = graph(exact)
+    # The same exact search scanning every tile of every query block (the rows in Morton
+    # order, no lists, no bounds): the brute-force work kyto's exact search does.
+    os.environ["KYTO_GPU_KNN_ORDER"] = "morton"
+    try:
+        _, fs_st, t_fs = graph(exact)
+    finally:
+        del os.environ["KYTO_GPU_KNN_ORDER"]
     graph(learned)
     le, le_st, t_le = graph(learned)
     a = le[1].view(n, k).long()
@@ -270,12 +279,16 @@ def learned_vs_exact(n: int, ctx) -> dict:
                      "sigma log-uniform [0.2, 2]), k = 15 (14 stored)"),
         "exact_ms": t_ex * 1e3, "learned_ms": t_le * 1e3, "speedup": t_ex / t_le,
         "recall_at_15": hits / (n * k),
+        "exact_full_scan_ms": t_fs * 1e3, "speedup_vs_full_scan": t_fs / t_le,
         "learned": {"train_ms": le_st.train_ms, "index_ms": le_st.index_ms,
                     "search_ms": le_st.search_ms, "fallback_rows": le_st.fallback_rows,
                     "scanned_tiles": le_st.scanned_tiles, "temperature": le_st.temperature,
                     "final_loss": le_st.final_loss},
         "exact": {"filter_ms": ex_st.filter_ms, "rank_ms": ex_st.rank_ms,
-                  "rows_searched_in_full": ex_st.rows_full},
+                  "rows_searched_in_full": ex_st.rows_full,
+                  "tiles_scanned": ex_st.tiles_scanned, "tiles_total": ex_st.tiles_total},
+        "exact_full_scan": {"filter_ms": fs_st.filter_ms, "rank_ms": fs_st.rank_ms,
+                            "tiles_scanned": fs_st.tiles_scanned},
     }
 
 
@@ -334,6 +347,8 @@ def main() -> int:
 
     ctx = K.Context(local)
     K._default = ctx
+    # A serving process reserves the pool once at open; no step then grows it mid-call.
+    ctx.reserve(args.reserve_gb << 30)
     x, vals, d_indptr, d_idx, d_vals = make_data(args, rank)
     n, k = args.cells, args.neighbors - 1
     out_dev = (torch.empty(n + 1, dtype=torch.int64, device="cuda"),
@@ -369,7 +384,8 @@ def main() -> int:
         filter_ms.append(st.filter_ms)
         knn_stats = {"candidates_per_row": st.candidates / args.cells,
                      "rows_searched_in_full": st.rows_full,
-                     "filter_ms": st.filter_ms, "rank_ms": st.rank_ms}
+                     "filter_ms": st.filter_ms, "rank_ms": st.rank_ms,
+                     "tiles_scanned": st.tiles_scanned, "tiles_total": st.tiles_total}
     stop.record()
     barrier()
     clk = clocks.stop()
@@ -440,7 +456,8 @@ def main() -> int:
             "config": {"workload": WORKLOAD, "cells": n, "genes": args.genes,
                        "nnz": x.nnz, "n_components": d, "n_neighbors": args.neighbors,
                        "parallelism": f"replicas x{world}",
-                       "l2": "inputs (>4 GB) larger than L2; no flush"},
+                       "l2": "inputs (>4 GB) larger than L2; no flush",
+                       "pool_reserve_gb": args.reserve_gb},
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
             "clocks": clk, "gpu_launches": launches, "knn": knn_stats,
             **extra,

@@ -71,6 +71,13 @@ KG_API size_t kg_last_error(const kg_ctx* ctx, char* buf, size_t len);
  * called at neighbors_gpu.rs:95). NULL clears it. */
 KG_API kg_status kg_set_cancel_flag(kg_ctx* ctx, const volatile int32_t* flag);
 
+/* Reserve `bytes` of device memory for the context's allocations up front (kept by the
+ * device's stream-ordered pool until the process ends): later calls carve their buffers
+ * out of it instead of growing the pool, whose driver calls can block the host for tens to
+ * hundreds of milliseconds mid-call. No kyto counterpart (a deployment knob of this
+ * library); 0 does nothing. */
+KG_API kg_status kg_reserve(kg_ctx* ctx, uint64_t bytes);
+
 /* Work done / total of the running or last call, in cells (all passes counted), as
  * RunControl::progress. */
 KG_API kg_status kg_progress(const kg_ctx* ctx, uint64_t* done, uint64_t* total);
@@ -185,6 +192,9 @@ typedef struct kg_knn_stats {
                               its candidates complete) */
   double filter_ms;        /* device time of the candidate filter */
   double rank_ms;          /* device time of the exact re-rank (and full rows) */
+  uint64_t tiles_scanned;  /* (query block, point tile) products the filter computed */
+  uint64_t tiles_total;    /* of the query blocks x point tiles a full scan computes (the
+                              rest skipped on proven distance bounds or not listed) */
 } kg_knn_stats;
 
 /* Each row's n_neighbors - 1 nearest other rows of `embedding` (n_rows x width f32,

@@ -37,7 +37,7 @@ KYTO_CODE = {
 
 # Every entry point of include/kyto_gpu.h.
 EXPORTS = (
-    "kg_open", "kg_close", "kg_last_error", "kg_set_cancel_flag", "kg_progress",
+    "kg_open", "kg_close", "kg_last_error", "kg_set_cancel_flag", "kg_reserve", "kg_progress",
     "kg_normalize_log1p", "kg_hvg_moments", "kg_hvg_moments_noalloc", "kg_hvg_seurat",
     "kg_pca_begin", "kg_pca_push_block", "kg_pca_run", "kg_pca_results", "kg_pca_info",
     "kg_pca_embedding_device", "kg_pca_free", "kg_pca_knn_batch", "kg_knn_exact",
@@ -73,6 +73,8 @@ class KnnStats(ctypes.Structure):
         ("rows_full", ctypes.c_uint64),
         ("filter_ms", ctypes.c_double),
         ("rank_ms", ctypes.c_double),
+        ("tiles_scanned", ctypes.c_uint64),
+        ("tiles_total", ctypes.c_uint64),
     ]
 
 
@@ -150,6 +152,7 @@ def library() -> ctypes.CDLL:
             "kg_open": [ctypes.c_int, ctypes.POINTER(P)],
             "kg_last_error": [P, ctypes.c_char_p, ctypes.c_size_t],
             "kg_set_cancel_flag": [P, P],
+            "kg_reserve": [P, U64],
             "kg_progress": [P, P, P],
             "kg_normalize_log1p": [P, P, P, ctypes.c_int, U64, ctypes.c_double, I32, P],
             "kg_hvg_moments": [P, P, P, P, ctypes.c_int, U64, U32, ctypes.c_double, I32, P, P, P],
@@ -229,6 +232,11 @@ class Context:
 
     def set_cancel_flag(self, flag: np.ndarray | None) -> None:
         _check(library().kg_set_cancel_flag(self._h, _ptr(flag)))
+
+    def reserve(self, nbytes: int) -> None:
+        """Reserve ``nbytes`` of device memory for this library's buffers up front
+        (kg_reserve): later calls do not grow the device pool mid-call."""
+        _check(library().kg_reserve(self._h, int(nbytes)))
 
     def progress(self) -> tuple[int, int]:
         done, total = ctypes.c_uint64(), ctypes.c_uint64()

@@ -8,6 +8,23 @@ std::string& last_error() {
   thread_local std::string message;
   return message;
 }
+
+void trace_slow_alloc(size_t bytes, double ms) {
+  int device = 0;
+  cudaMemPool_t pool;
+  uint64_t reserved = 0, used = 0;
+  size_t free_b = 0, total_b = 0;
+  if (cudaGetDevice(&device) == cudaSuccess &&
+      cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+  }
+  cudaMemGetInfo(&free_b, &total_b);
+  std::fprintf(stderr,
+               "[kyto_gpu trace] slow allocation: %.3f GB in %.1f ms (pool reserved %.2f GB, "
+               "used %.2f GB; device free %.2f GB)\n",
+               bytes / 1e9, ms, reserved / 1e9, used / 1e9, free_b / 1e9);
+}
 }  // namespace kg
 
 extern "C" {
@@ -82,6 +99,19 @@ kg_status kg_set_cancel_flag(kg_ctx* ctx, const volatile int32_t* flag) {
   return kg::guarded([&] {
     if (!ctx) kg::fail(KG_ERR_INVALID, "kg_set_cancel_flag: ctx is NULL");
     ctx->cancel = flag;
+  });
+}
+
+kg_status kg_reserve(kg_ctx* ctx, uint64_t bytes) {
+  return kg::guarded([&] {
+    if (!ctx) kg::fail(KG_ERR_INVALID, "kg_reserve: ctx is NULL");
+    if (!bytes) return;
+    KG_CUDA(cudaSetDevice(ctx->device));
+    // The pool's release threshold is the maximum (kg_open): a freed block stays reserved.
+    void* p = nullptr;
+    KG_CUDA(cudaMallocAsync(&p, bytes, ctx->stream));
+    KG_CUDA(cudaFreeAsync(p, ctx->stream));
+    KG_CUDA(cudaStreamSynchronize(ctx->stream));
   });
 }
 

@@ -77,6 +77,17 @@ extern std::atomic<uint64_t> g_launches;
 // The calling thread's last error message (kg_last_error).
 std::string& last_error();
 
+// Whether KYTO_GPU_TRACE is set (read once).
+inline bool trace_on() {
+  static const bool on = std::getenv("KYTO_GPU_TRACE") != nullptr;
+  return on;
+}
+
+// Under KYTO_GPU_TRACE, an allocation whose host call took over 2 ms is reported with
+// its size and the device pool's reserved and used bytes after it (the pool grows, and
+// the call blocks, when no free range of the pool fits the request).
+void trace_slow_alloc(size_t bytes, double ms);
+
 // A device allocation, stream-ordered (cudaMallocAsync / cudaFreeAsync).
 template <class T>
 struct DeviceBuffer {
@@ -105,7 +116,15 @@ struct DeviceBuffer {
     reset();
     stream = s;
     count = n;
-    if (n) KG_CUDA(cudaMallocAsync((void**)&ptr, n * sizeof(T), s));
+    if (!n) return;
+    if (!trace_on()) {
+      KG_CUDA(cudaMallocAsync((void**)&ptr, n * sizeof(T), s));
+      return;
+    }
+    auto t0 = std::chrono::steady_clock::now();
+    KG_CUDA(cudaMallocAsync((void**)&ptr, n * sizeof(T), s));
+    double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    if (ms > 2.0) trace_slow_alloc(n * sizeof(T), ms);
   }
   void reset() noexcept {
     if (ptr) cudaFreeAsync(ptr, stream);
@@ -225,7 +244,7 @@ struct Trace {
   };
   std::vector<Mark> marks;
   Trace(cudaStream_t st, const char* call) : s(st), what(call) {
-    on = std::getenv("KYTO_GPU_TRACE") != nullptr;
+    on = trace_on();
     mark("start");
   }
   void mark(const char* name) {

@@ -14,6 +14,7 @@
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_segmented_radix_sort.cuh>
+#include <cub/device/device_segmented_sort.cuh>
 
 #include <algorithm>
 #include <cfloat>
@@ -26,6 +27,7 @@
 #include <cstdlib>
 #include <string>
 
+#include "kg_cluster.cuh"
 #include "kg_internal.cuh"
 #include "kg_knn.cuh"
 #include "kg_knn_tc.cuh"
@@ -230,6 +232,189 @@ void spatial_order(const float* x, uint64_t n, uint32_t width, uint32_t d, const
   DeviceBuffer<unsigned char> scratch(temp, s);
   KG_CUDA(cub::DeviceRadixSort::SortPairs(scratch.ptr, temp, key.ptr, key_sorted.ptr, rows.ptr,
                                           perm.ptr, (int)n, 0, 30, s));
+}
+
+// ------------------------------------------------------ bounded scan lists ---------
+// The rows ordered by k-means part, so a block of query slots and a tile of point slots
+// each hold rows close together in all d components; every query block's list holds every
+// tile, nearest first, each with a lower bound on the distance between its rows and the
+// block's (two balls). The filter skips a tile whose bound exceeds every query's threshold:
+// no row in it can pass, so the graph is the same as the full scan's.
+
+// Centre (the f64 mean of the group's centred rows), radius (the largest distance of a
+// group row from it, rounded up) and box (each component's smallest and largest centred
+// value) of each group of `size` consecutive slots; per-component arrays are written
+// component-major (c_t[j * n_groups + g]). One 64-thread block per group.
+__global__ void __launch_bounds__(64)
+group_balls_kernel(const float* x, uint32_t width, uint32_t d, const double* mean,
+                   const uint32_t* rows, uint64_t n, uint32_t size, uint64_t n_groups,
+                   double* centre_t, double* lo_t, double* hi_t, double* radius) {
+  const uint64_t g = blockIdx.x;
+  const uint64_t s0 = g * size, s1 = min(s0 + size, n);
+  __shared__ double c[kDim];
+  __shared__ double red[64];
+  const uint32_t j = threadIdx.x;
+  double lo = 0.0, hi = 0.0;
+  if (j < d) {
+    double sum = 0.0;
+    lo = INFINITY;
+    hi = -INFINITY;
+    for (uint64_t sl = s0; sl < s1; ++sl) {
+      const double v = (double)x[(uint64_t)rows[sl] * width + j] - mean[j];
+      sum += v;
+      lo = fmin(lo, v);
+      hi = fmax(hi, v);
+    }
+    c[j] = sum / (double)(s1 - s0);
+  }
+  __syncthreads();
+  double worst = 0.0;
+  for (uint64_t sl = s0 + threadIdx.x; sl < s1; sl += blockDim.x) {
+    const float* xr = x + (uint64_t)rows[sl] * width;
+    double acc = 0.0;
+    for (uint32_t jj = 0; jj < d; ++jj) {
+      const double t = ((double)xr[jj] - mean[jj]) - c[jj];
+      acc += t * t;
+    }
+    worst = fmax(worst, acc);
+  }
+  red[threadIdx.x] = worst;
+  __syncthreads();
+  for (int o = 32; o; o >>= 1) {
+    if ((int)threadIdx.x < o) red[threadIdx.x] = fmax(red[threadIdx.x], red[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) radius[g] = sqrt(red[0]) * (1.0 + 0x1p-40);
+  centre_t[(uint64_t)j * n_groups + g] = j < d ? c[j] : 0.0;
+  lo_t[(uint64_t)j * n_groups + g] = lo;
+  hi_t[(uint64_t)j * n_groups + g] = hi;
+}
+
+// Per (query block, tile), two lower bounds on the distance between a row of the block
+// and a row of the tile: the balls' |c_b - c_t| - r_b - r_t (triangle inequality) and the
+// boxes' sqrt(sum_j gap_j^2) (gap_j: how far apart the two boxes are in component j). The
+// larger, less a margin for the rounding of the centred rows and at least 0, is kept as a
+// scaled squared distance rounded down, packed with the centre distance into the sort key
+// (bound, then centre distance); the tile as the value. kBoundBlocks query blocks per CTA
+// share each tile's reads.
+constexpr int kBoundBlocks = 8;
+__global__ void __launch_bounds__(256)
+ball_bounds_kernel(const double* bc_t, const double* blo_t, const double* bhi_t,
+                   const double* br, uint64_t n_blocks, const double* tc_t, const double* tlo_t,
+                   const double* thi_t, const double* tr, uint32_t n_tiles, uint32_t d,
+                   double s2, double margin, unsigned long long* key, uint32_t* tile) {
+  __shared__ double cb[kBoundBlocks][kDim], lb_[kBoundBlocks][kDim], hb[kBoundBlocks][kDim];
+  const uint64_t b0 = (uint64_t)blockIdx.x * kBoundBlocks;
+  for (uint32_t i = threadIdx.x; i < kBoundBlocks * kDim; i += blockDim.x) {
+    const uint32_t bb = i / kDim, j = i % kDim;
+    const bool in = b0 + bb < n_blocks && j < d;
+    const uint64_t at = (uint64_t)j * n_blocks + b0 + bb;
+    cb[bb][j] = in ? bc_t[at] : 0.0;
+    lb_[bb][j] = in ? blo_t[at] : 0.0;
+    hb[bb][j] = in ? bhi_t[at] : 0.0;
+  }
+  __syncthreads();
+  double rb[kBoundBlocks];
+#pragma unroll
+  for (int bb = 0; bb < kBoundBlocks; ++bb) rb[bb] = b0 + bb < n_blocks ? br[b0 + bb] : 0.0;
+  for (uint32_t t = threadIdx.x; t < n_tiles; t += blockDim.x) {
+    double acc[kBoundBlocks], box[kBoundBlocks];
+#pragma unroll
+    for (int bb = 0; bb < kBoundBlocks; ++bb) acc[bb] = box[bb] = 0.0;
+    for (uint32_t j = 0; j < d; ++j) {
+      const uint64_t at = (uint64_t)j * n_tiles + t;
+      const double v = tc_t[at], tl = tlo_t[at], th = thi_t[at];
+#pragma unroll
+      for (int bb = 0; bb < kBoundBlocks; ++bb) {
+        const double u = cb[bb][j] - v;
+        acc[bb] = fma(u, u, acc[bb]);
+        const double gap = fmax(fmax(tl - hb[bb][j], lb_[bb][j] - th), 0.0);
+        box[bb] = fma(gap, gap, box[bb]);
+      }
+    }
+    const double rt = tr[t];
+#pragma unroll
+    for (int bb = 0; bb < kBoundBlocks; ++bb) {
+      if (b0 + bb >= n_blocks) break;
+      const double dist = sqrt(acc[bb]);
+      const double ball = dist * (1.0 - 0x1p-40) - rb[bb] - rt;
+      const double boxd = sqrt(box[bb]) * (1.0 - 0x1p-40);
+      const double lb = fmax(fmax(ball, boxd) - margin, 0.0);
+      const float lb2 = __double2float_rd(s2 * lb * lb * (1.0 - 0x1p-40));
+      const float near = __double2float_rn(dist);
+      const uint64_t at = (b0 + bb) * (uint64_t)n_tiles + t;
+      key[at] = ((unsigned long long)__float_as_uint(lb2) << 32) | __float_as_uint(near);
+      tile[at] = t;
+    }
+  }
+}
+
+__global__ void key_bounds_kernel(const unsigned long long* key, uint64_t count, float* lb2) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    lb2[i] = __uint_as_float((uint32_t)(key[i] >> 32));
+}
+
+// The bounded scan of the exact search (qrows, list_tiles, list_lb2, list_stride,
+// list_sorted of sp): rows by k-means part (about 1,024 rows a part); bounds with
+// skipping when `skip`, else the same lists without bounds. Returns false (sp untouched)
+// when the lists would not fit the sort's 32-bit sizes or `max_bytes` of scratch.
+bool bounded_scan(const float* x, uint64_t n, uint32_t width, uint32_t d, const double* mean,
+                  double scale, double max_norm, uint32_t qblock, bool skip, uint64_t max_bytes,
+                  ScanPlan& sp, cudaStream_t s, Trace& trace) {
+  const uint64_t n_blocks = (n + qblock - 1) / qblock;
+  const uint32_t n_tiles = (uint32_t)((n + kTile - 1) / kTile);
+  const uint64_t entries = n_blocks * n_tiles;
+  if (entries > (uint64_t)INT32_MAX || entries * 28 > max_bytes) return false;
+  Clusters cl;
+  const uint32_t parts = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(n / 1024, 1), 4096);
+  cluster_rows(x, n, width, d, parts, 5, 131072, cl, s);
+  trace.mark("scan parts");
+  DeviceBuffer<double> bc((uint64_t)kDim * n_blocks, s), blo((uint64_t)kDim * n_blocks, s),
+      bhi((uint64_t)kDim * n_blocks, s), br(n_blocks, s);
+  DeviceBuffer<double> tc((uint64_t)kDim * n_tiles, s), tlo((uint64_t)kDim * n_tiles, s),
+      thi((uint64_t)kDim * n_tiles, s), tr(n_tiles, s);
+  group_balls_kernel<<<(unsigned)n_blocks, 64, 0, s>>>(x, width, d, mean, cl.perm.ptr, n, qblock,
+                                                       n_blocks, bc.ptr, blo.ptr, bhi.ptr, br.ptr);
+  KG_LAUNCH_CHECK();
+  group_balls_kernel<<<n_tiles, 64, 0, s>>>(x, width, d, mean, cl.perm.ptr, n, kTile, n_tiles,
+                                            tc.ptr, tlo.ptr, thi.ptr, tr.ptr);
+  KG_LAUNCH_CHECK();
+  DeviceBuffer<unsigned long long> key(entries, s), key_sorted(entries, s);
+  DeviceBuffer<uint32_t> tile(entries, s);
+  sp.list_tiles.alloc(entries, s);
+  // Margin: the centred rows' f64 rounding, far below any bound that prunes.
+  const double margin = 0x1p-30 * max_norm;
+  ball_bounds_kernel<<<(unsigned)((n_blocks + kBoundBlocks - 1) / kBoundBlocks), 256, 0, s>>>(
+      bc.ptr, blo.ptr, bhi.ptr, br.ptr, n_blocks, tc.ptr, tlo.ptr, thi.ptr, tr.ptr, n_tiles, d,
+      scale * scale, margin, key.ptr, tile.ptr);
+  KG_LAUNCH_CHECK();
+  trace.mark("scan bounds");
+  DeviceBuffer<int> off(n_blocks + 1, s);
+  std::vector<int> h_off(n_blocks + 1);
+  for (uint64_t b = 0; b <= n_blocks; ++b) h_off[b] = (int)(b * n_tiles);
+  KG_CUDA(cudaMemcpyAsync(off.ptr, h_off.data(), (n_blocks + 1) * sizeof(int),
+                          cudaMemcpyHostToDevice, s));
+  size_t temp = 0;
+  KG_CUDA(cub::DeviceSegmentedSort::StableSortPairs(
+      nullptr, temp, key.ptr, key_sorted.ptr, tile.ptr, sp.list_tiles.ptr, (int)entries,
+      (int)n_blocks, off.ptr, off.ptr + 1, s));
+  DeviceBuffer<unsigned char> scratch(temp, s);
+  KG_CUDA(cub::DeviceSegmentedSort::StableSortPairs(
+      scratch.ptr, temp, key.ptr, key_sorted.ptr, tile.ptr, sp.list_tiles.ptr, (int)entries,
+      (int)n_blocks, off.ptr, off.ptr + 1, s));
+  if (skip) {
+    sp.list_lb2.alloc(entries, s);
+    key_bounds_kernel<<<std::min<uint64_t>(blocks_for(entries, 256), 8192), 256, 0, s>>>(
+        key_sorted.ptr, entries, sp.list_lb2.ptr);
+    KG_LAUNCH_CHECK();
+  }
+  // The host offsets must outlive the copy.
+  KG_CUDA(cudaStreamSynchronize(s));
+  sp.qrows = std::move(cl.perm);
+  sp.list_stride = n_tiles;
+  sp.list_sorted = true;
+  return true;
 }
 
 // The batch's rows sample by sample, each sample in Morton order: a query block's own
@@ -713,6 +898,8 @@ FilterKind tune_filter_kind(kg_ctx* ctx, cudaStream_t s, const float* x, uint64_
   ps.slot_sample = scan.slot_sample ? p_sample.ptr : nullptr;
   ps.list_tiles = p_list.ptr;
   ps.list_lb2 = nullptr;
+  ps.list_sorted = false;
+  ps.tiles_scanned = nullptr;
   ps.list_off = off.ptr;
   ps.list_stride = 0;
   const uint32_t cap = kTcCap;
@@ -742,6 +929,13 @@ FilterKind tune_filter_kind(kg_ctx* ctx, cudaStream_t s, const float* x, uint64_
     for (uint32_t c : h_cc) over += c == kOverflow;
     const double cost = ms * 1e-3 * (double)n_blocks / (double)n_pilot +
                         (double)over / (double)n_q * (double)n * (double)n * per_point;
+    if (trace_on())
+      std::fprintf(stderr,
+                   "[kyto_gpu trace] filter pilot %s: %.3f ms for %llu blocks, %llu of %llu "
+                   "queries overflowed, estimate %.1f ms\n",
+                   kind == FilterKind::Split ? "split" : "fp16", ms,
+                   (unsigned long long)n_pilot, (unsigned long long)over,
+                   (unsigned long long)n_q, cost * 1e3);
     if (cost < best_cost) {
       best_cost = cost;
       best = kind;
@@ -845,9 +1039,22 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
       KG_LAUNCH_CHECK();
       trace.mark("scan order");
     } else {
-      // The rows sorted by a Morton code of their first three centred components, so
-      // a query block's own tiles hold its nearest points and the scan starts there.
-      spatial_order(x, n, width, d, mean.ptr, lo_hi.ptr, sp.qrows, s);
+      // By default the bounded scan (rows by k-means part, nearest tiles first, far tiles
+      // skipped on their bounds); KYTO_GPU_KNN_ORDER=cluster keeps its order and lists
+      // without skipping, =morton the rows sorted by a Morton code of their first three
+      // centred components, each query block scanning every tile from its own (also
+      // when the lists would not fit).
+      const char* ord = std::getenv("KYTO_GPU_KNN_ORDER");
+      const std::string order = ord ? ord : "bounded";
+      bool listed = false;
+      if (order != "morton") {
+        size_t free_b = 0, total_b = 0;
+        KG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+        listed = bounded_scan(x, n, width, d, mean.ptr, scale, std::sqrt(h_largest),
+                              filter_query_block(kind), order != "cluster", free_b / 3, sp, s,
+                              trace);
+      }
+      if (!listed) spatial_order(x, n, width, d, mean.ptr, lo_hi.ptr, sp.qrows, s);
       trace.mark("scan order");
     }
     FilterScan scan;
@@ -858,6 +1065,7 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
     scan.list_lb2 = sp.list_lb2.ptr;
     scan.list_off = sp.list_off.ptr;
     scan.list_stride = sp.list_stride;
+    scan.list_sorted = sp.list_sorted;
     if (batch) {
       scan.slot_sample = slot_sample.ptr;
       scan.sample_first = batch->d_first.ptr;
@@ -869,10 +1077,20 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
       trace.mark("filter tuning");
     }
     DeviceBuffer<uint16_t> point_ops;  // kept for the overflow retry
+    DeviceBuffer<unsigned long long> tiles(1, s);
+    tiles.zero();
+    scan.tiles_scanned = tiles.ptr;
     tc_filter(ctx, s, x, width, d, sp.qrows.ptr, prows, scan, mean.ptr, scale, max_sq.ptr,
               kind, k, cap, cand_key, cand_row, cand_count.ptr, thr.ptr,
               qn2.ptr, slack_d.ptr, &trace, &point_ops);
     filter_ms += tf.stop_ms();
+    {
+      unsigned long long h_tiles = 0;
+      KG_CUDA(cudaMemcpyAsync(&h_tiles, tiles.ptr, 8, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaStreamSynchronize(s));
+      out.tiles_scanned = h_tiles;
+      out.tiles_total = ((n + kTcQueryBlock - 1) / kTcQueryBlock) * ((n + kTile - 1) / kTile);
+    }
     check_cancel(ctx);
     Timer tr(s);
     rank_kernel<<<blocks_for(n * 32, kRankWarps * 32), kRankWarps * 32, 0, s>>>(
@@ -910,6 +1128,8 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
       rs.list_lb2 = nullptr;
       rs.list_off = nullptr;
       rs.list_stride = 0;
+      rs.list_sorted = false;
+      rs.tiles_scanned = nullptr;
       DeviceBuffer<float> r_key(m * kTcRetryCap, s), r_thr(m, s);
       DeviceBuffer<uint32_t> r_row(m * kTcRetryCap, s), r_count(m, s);
       DeviceBuffer<double> r_qn2(m, s), r_slack(m, s);
@@ -1137,6 +1357,8 @@ void knn_batch_run(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint
     stats->rows_full = r.rows_full;
     stats->filter_ms = r.filter_ms;
     stats->rank_ms = r.rank_ms;
+    stats->tiles_scanned = r.tiles_scanned;
+    stats->tiles_total = r.tiles_total;
   }
 }
 
@@ -1205,6 +1427,8 @@ extern "C" kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t 
       stats->rows_full = r.rows_full;
       stats->filter_ms = r.filter_ms;
       stats->rank_ms = r.rank_ms;
+      stats->tiles_scanned = r.tiles_scanned;
+      stats->tiles_total = r.tiles_total;
     }
   });
 }

@@ -25,6 +25,7 @@ struct KnnResult {
   DeviceBuffer<double> key;    // n x k, ascending by (key, row)
   DeviceBuffer<uint32_t> row;
   uint64_t candidates = 0, rows_full = 0, retried = 0;
+  uint64_t tiles_scanned = 0, tiles_total = 0;  // the filter's block-tile products
   double filter_ms = 0, rank_ms = 0;
 };
 
@@ -47,6 +48,7 @@ struct ScanPlan {
   DeviceBuffer<float> list_lb2;
   DeviceBuffer<uint64_t> list_off;
   uint64_t list_stride = 0;
+  bool list_sorted = false;  // each block's list ascending by bound
 };
 // Builds the filter's scan for query blocks of qblock slots.
 using PlanBuilder = std::function<void(const float* x, uint64_t n, uint32_t width, uint32_t d,

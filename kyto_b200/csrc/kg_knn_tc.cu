@@ -299,7 +299,7 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
       prefetch_tmap(&tmap_q);
       prefetch_tmap(&tmap_p);
     }
-    uint64_t it = 0;
+    uint64_t it = 0, loaded = 0;
     uint32_t bi = 0;
     int issued_phase[kStages];
     for (int s = 0; s < kStages; ++s) issued_phase[s] = -1;
@@ -341,7 +341,12 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
             for (int w = 1; w < kEpiWarps; ++w) u = fmaxf(u, u_max[(bi & 1) * kEpiWarps + w]);
           }
           u = __shfl_sync(0xFFFFFFFFu, u, 0);
-          if (lb2 > u) continue;
+          if (lb2 > u) {
+            // Ascending bounds: every later tile is skipped too (the thresholds only
+            // fall), so the block's scan ends here.
+            if (scan.list_sorted) i = len - 1;
+            continue;
+          }
         }
         bool end = false;
         if (lane == 0) {
@@ -367,6 +372,7 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
                 tma_load_2d(sm.b[s][sub], &tmap_p, &sm.full[s], sub * kTcK,
                             (int32_t)(pt * kTcPoints));
               issued_phase[s] = (int)ph;
+              ++loaded;
             }
           }
         }
@@ -376,6 +382,7 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
         if (!ok || end) break;
       }
     }
+    if (lane == 0 && scan.tiles_scanned) atomicAdd(scan.tiles_scanned, (unsigned long long)loaded);
     // Every load issued has landed before the CTA may leave (bounded, own loop).
     if (lane == 0) {
       for (int s = 0; s < kStages; ++s) {
@@ -522,8 +529,11 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           live = !st.overflowed;
         }
         if (offered && scan.list_lb2) {
-          // An overflowed query is searched in full later: it no longer bounds the scan.
-          const float u = active && live ? round_up_f32d((double)th + s2qn2) : -INFINITY;
+          // A point is offered only if its key is at most th; its key is at least
+          // s^2 (D - |q|^2) - slack, so no point farther than th + s^2 |q|^2 + slack
+          // (scaled squared distance) can be. An overflowed query is searched in full
+          // later: it no longer bounds the scan.
+          const float u = active && live ? round_up_f32d((double)th + s2qn2 + sl2) : -INFINITY;
           float um = u;
           for (int o = 16; o; o >>= 1) um = fmaxf(um, __shfl_xor_sync(0xFFFFFFFFu, um, o));
           if (lane == 0) u_max[(bi & 1) * kEpiWarps + warp] = um;
@@ -824,6 +834,9 @@ void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint32_t width, uint
   CUtensorMap mq = tile_map(aq.ptr, n_q, bf16, width_op), mp = tile_map(bp.ptr, n_p, bf16, width_op);
   DeviceBuffer<int> err(1, s);
   err.zero();
+  unsigned long long tiles_before = 0;
+  if (trace_on() && scan.tiles_scanned)
+    KG_CUDA(cudaMemcpyAsync(&tiles_before, scan.tiles_scanned, 8, cudaMemcpyDeviceToHost, s));
   scan.qn2 = qn2;
   scan.s2 = scale * scale;
   const uint64_t n_qblocks = (n_q + kTcQueries - 1) / kTcQueries;
@@ -841,6 +854,16 @@ void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint32_t width, uint
   KG_CUDA(cudaMemcpyAsync(&h_err, err.ptr, 4, cudaMemcpyDeviceToHost, s));
   wait_stream(ctx, s);
   if (h_err) fail(KG_ERR_TIMEOUT, "the tensor-core kNN filter gave up waiting on its pipeline");
+  if (trace_on() && scan.tiles_scanned) {
+    unsigned long long h_tiles = 0;
+    KG_CUDA(cudaMemcpyAsync(&h_tiles, scan.tiles_scanned, 8, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+    h_tiles -= tiles_before;
+    const double all = (double)n_qblocks * (double)((n_p + kTcPoints - 1) / kTcPoints);
+    std::fprintf(stderr, "[kyto_gpu trace] filter %s: %llu block-tile products of %.0f (%.2f%%)%s\n",
+                 split ? "split" : bf16 ? "bf16" : "fp16", h_tiles, all, 100.0 * h_tiles / all,
+                 scan.list_lb2 ? ", with bounds" : "");
+  }
 }
 
 }  // namespace kg

@@ -24,7 +24,8 @@ uint32_t filter_query_block(FilterKind kind);
 // What one filter launch scans. Query slot q is row qrows[q] of x, point slot p row
 // prows[p]; each block of query slots (filter_query_block) scans its list of point tiles (128 slots) in
 // order, or every tile from its own when list_tiles is NULL, skipping a listed tile whose
-// bound (list_lb2, scaled squared distance) exceeds every query's threshold + s^2 |q|^2.
+// bound (list_lb2, a lower bound of the scaled squared distance between the tile's rows and
+// the block's) exceeds every live query's threshold + s^2 |q|^2 + its slack.
 struct FilterScan {
   uint64_t n_q = 0, n_p = 0;
   const uint32_t* q_point = nullptr;     // query slot -> point slot of the same row (NULL:
@@ -35,10 +36,13 @@ struct FilterScan {
                                          // at list_off[qb + 1] (or NULL: qb * list_stride,
                                          // list_stride entries each)
   uint64_t list_stride = 0;
+  bool list_sorted = false;              // each block's bounds ascend: the first skipped
+                                         // tile ends the block's scan
   const uint32_t* slot_sample = nullptr;  // per query slot its sample (NULL: one sample):
   const uint64_t* sample_first = nullptr; // a query takes only the point slots
                                           // [sample_first[s], sample_first[s + 1]) of its
                                           // sample s (a batch of samples searched at once)
+  unsigned long long* tiles_scanned = nullptr;  // when set: += tiles the launch multiplied
   const double* qn2 = nullptr;           // per query slot |q - mean|^2 (set by tc_filter)
   double s2 = 1.0;                       // scale^2 (set by tc_filter)
 };

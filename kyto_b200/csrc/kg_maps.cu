@@ -78,28 +78,32 @@ void launch_normalize(const uint64_t* indptr, const void* values, uint64_t n_row
   KG_LAUNCH_CHECK();
 }
 
-// Device f32 map outputs of a (device) CSR block; inexact is a device int (or NULL).
+// The device flag of inexact_counts_kernel for a block about to be normalized (left
+// unallocated, NULL, when no u32 count of the block can need rounding).
+void inexact_flag(const void* d_values, kg_dtype dtype, uint64_t nnz, double target_sum,
+                  DeviceBuffer<int>& flag, cudaStream_t stream) {
+  if (dtype != KG_U32 || std::isnan(target_sum) || !nnz) return;
+  flag.alloc(1, stream);
+  flag.zero();
+  unsigned threads = 256;
+  unsigned blocks = std::min<unsigned>(blocks_for(nnz, threads), 4096);
+  inexact_counts_kernel<<<blocks, threads, 0, stream>>>((const uint32_t*)d_values, nnz,
+                                                        flag.ptr);
+  KG_LAUNCH_CHECK();
+}
+
+// Device f32 map outputs of a (device) CSR block.
 void map_block(const uint64_t* d_indptr, const void* d_values, kg_dtype dtype,
                uint64_t n_rows, uint64_t nnz, double target_sum, int do_log1p,
                float* d_out, cudaStream_t stream) {
   DeviceBuffer<int> inexact;
-  const int* flag = nullptr;
-  if (dtype == KG_U32 && !std::isnan(target_sum) && nnz) {
-    inexact.alloc(1, stream);
-    inexact.zero();
-    unsigned threads = 256;
-    unsigned blocks = std::min<unsigned>(blocks_for(nnz, threads), 4096);
-    inexact_counts_kernel<<<blocks, threads, 0, stream>>>((const uint32_t*)d_values, nnz,
-                                                          inexact.ptr);
-    KG_LAUNCH_CHECK();
-    flag = inexact.ptr;
-  }
+  inexact_flag(d_values, dtype, nnz, target_sum, inexact, stream);
   if (dtype == KG_U32)
-    launch_normalize<uint32_t>(d_indptr, d_values, n_rows, target_sum, do_log1p, flag,
+    launch_normalize<uint32_t>(d_indptr, d_values, n_rows, target_sum, do_log1p, inexact.ptr,
                                d_out, stream);
   else
-    launch_normalize<float>(d_indptr, d_values, n_rows, target_sum, do_log1p, flag, d_out,
-                            stream);
+    launch_normalize<float>(d_indptr, d_values, n_rows, target_sum, do_log1p, inexact.ptr,
+                            d_out, stream);
 }
 
 // seurat's transformed value and its f32 square (hvg_pass.rs:189-206).

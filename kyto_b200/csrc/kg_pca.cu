@@ -29,9 +29,8 @@
 namespace kg {
 
 // Declared in kg_maps.cu.
-void map_block(const uint64_t* d_indptr, const void* d_values, kg_dtype dtype,
-               uint64_t n_rows, uint64_t nnz, double target_sum, int do_log1p,
-               float* d_out, cudaStream_t stream);
+void inexact_flag(const void* d_values, kg_dtype dtype, uint64_t nnz, double target_sum,
+                  DeviceBuffer<int>& flag, cudaStream_t stream);
 template <class P>
 void sort_by_gene(const uint32_t* genes, const P* payload, uint64_t nnz, uint32_t n_genes,
                   DeviceBuffer<uint32_t>& genes_out, DeviceBuffer<P>& payload_out,
@@ -47,25 +46,34 @@ constexpr double kDropTolerance = 1e-10;  // pca_dense.rs:30
 
 // ----------------------------------------------------------------- pack kernels ----
 
-// Kept entries per row (genes mapped into the PCA's set), one warp per row.
-__global__ void count_kept_kernel(const uint64_t* indptr, const uint32_t* idx,
-                                  uint64_t n_rows, const uint32_t* gene_map,
-                                  uint64_t* kept) {
+// Kept entries per row (genes mapped into the PCA's set), one warp per row, and the
+// row's normalize divisor (kg_maps.cuh: every 8-lane group of the warp sums the row in
+// kyto's lane order and gets the same divisor) when divisor is not NULL.
+template <class V>
+__global__ void count_kept_kernel(const uint64_t* indptr, const uint32_t* idx, const V* values,
+                                  uint64_t n_rows, const uint32_t* gene_map, float target32,
+                                  const int* inexact, uint64_t* kept, float* divisor) {
   uint64_t row = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   unsigned lane = threadIdx.x & 31u;
-  if (row >= n_rows) return;
+  if (row >= n_rows) return;  // whole warps leave together
   uint64_t s = indptr[row], e = indptr[row + 1];
   uint64_t count = 0;
   for (uint64_t i = s + lane; i < e; i += 32)
     count += (gene_map == nullptr || gene_map[idx[i]] != kNoGene);
   for (int o = 16; o; o >>= 1) count += __shfl_down_sync(0xFFFFFFFFu, count, o);
   if (lane == 0) kept[row] = count;
+  if (divisor) {
+    float d = row_divisor(values, s, e, target32, inexact && *inexact);
+    if (lane == 0) divisor[row] = d;
+  }
 }
 
 // Writes each row's kept entries in order at out_ptr[row] (warp per row, ballot
-// compaction keeps the row's gene order).
-__global__ void write_kept_kernel(const uint64_t* indptr, const uint32_t* idx,
-                                  const float* mapped, uint64_t n_rows,
+// compaction keeps the row's gene order), each value mapped on the way: f32(v) / the
+// row's divisor (when divisor is not NULL), then log1p (kg_maps.cuh).
+template <class V>
+__global__ void write_kept_kernel(const uint64_t* indptr, const uint32_t* idx, const V* values,
+                                  const float* divisor, int do_log1p, uint64_t n_rows,
                                   const uint32_t* gene_map, const uint64_t* out_ptr,
                                   uint32_t* col, float* val) {
   uint64_t row = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -73,6 +81,7 @@ __global__ void write_kept_kernel(const uint64_t* indptr, const uint32_t* idx,
   if (row >= n_rows) return;
   uint64_t s = indptr[row], e = indptr[row + 1];
   uint64_t base = out_ptr[row];
+  const float d = divisor ? divisor[row] : 1.0f;
   for (uint64_t i0 = s; i0 < e; i0 += 32) {
     uint64_t i = i0 + lane;
     bool in = i < e;
@@ -83,7 +92,7 @@ __global__ void write_kept_kernel(const uint64_t* indptr, const uint32_t* idx,
     if (keep) {
       uint64_t at = base + __popc(ballot & ((1u << lane) - 1u));
       col[at] = p;
-      val[at] = mapped[i];
+      val[at] = mapped_value(values, i, divisor != nullptr, d, do_log1p != 0);
     }
     base += __popc(ballot);
   }
@@ -1032,15 +1041,24 @@ void kg_pca::push(const uint64_t* in_indptr, const uint32_t* in_idx, const void*
   const void* d_values = device_view((const uint32_t*)in_values, bnnz, hv, s);
   check_indices(d_idx, bnnz, stream_genes, s);
   trace.mark("checks");
-  DeviceBuffer<float> mapped(bnnz, s);
-  map_block(d_indptr, d_values, dtype, n_rows, bnnz, target_sum, log1p, mapped.ptr, s);
-  trace.mark("map");
-  // Kept entries per row, then their offsets after the held entries.
+  // Kept entries per row and the rows' normalize divisors, then the kept entries'
+  // offsets after the held entries; the maps run inside write_kept.
+  const bool normalize = !std::isnan(target_sum);
+  DeviceBuffer<int> inexact;
+  inexact_flag(d_values, dtype, bnnz, target_sum, inexact, s);
   DeviceBuffer<uint64_t> kept(n_rows + 1, s);
+  DeviceBuffer<float> divisor;
+  if (normalize) divisor.alloc(n_rows, s);
   kept.zero();
   unsigned threads = 256;
-  count_kept_kernel<<<blocks_for(n_rows * 32, threads), threads, 0, s>>>(
-      d_indptr, d_idx, n_rows, gene_map.ptr, kept.ptr);
+  if (dtype == KG_U32)
+    count_kept_kernel<uint32_t><<<blocks_for(n_rows * 32, threads), threads, 0, s>>>(
+        d_indptr, d_idx, (const uint32_t*)d_values, n_rows, gene_map.ptr, (float)target_sum,
+        inexact.ptr, kept.ptr, divisor.ptr);
+  else
+    count_kept_kernel<float><<<blocks_for(n_rows * 32, threads), threads, 0, s>>>(
+        d_indptr, d_idx, (const float*)d_values, n_rows, gene_map.ptr, (float)target_sum,
+        inexact.ptr, kept.ptr, divisor.ptr);
   KG_LAUNCH_CHECK();
   size_t temp = 0;
   KG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, kept.ptr, kept.ptr, n_rows + 1, s));
@@ -1059,8 +1077,14 @@ void kg_pca::push(const uint64_t* in_indptr, const uint32_t* in_idx, const void*
   trace.mark("held buffers");
   KG_CUDA(cudaMemcpyAsync(indptr.ptr + n_cells, kept.ptr, (n_rows + 1) * 8,
                           cudaMemcpyDeviceToDevice, s));
-  write_kept_kernel<<<blocks_for(n_rows * 32, threads), threads, 0, s>>>(
-      d_indptr, d_idx, mapped.ptr, n_rows, gene_map.ptr, kept.ptr, col.ptr, val.ptr);
+  if (dtype == KG_U32)
+    write_kept_kernel<uint32_t><<<blocks_for(n_rows * 32, threads), threads, 0, s>>>(
+        d_indptr, d_idx, (const uint32_t*)d_values, divisor.ptr, log1p, n_rows, gene_map.ptr,
+        kept.ptr, col.ptr, val.ptr);
+  else
+    write_kept_kernel<float><<<blocks_for(n_rows * 32, threads), threads, 0, s>>>(
+        d_indptr, d_idx, (const float*)d_values, divisor.ptr, log1p, n_rows, gene_map.ptr,
+        kept.ptr, col.ptr, val.ptr);
   KG_LAUNCH_CHECK();
   if (in_cells) {
     const uint64_t* d_cells = device_view(in_cells, n_rows, hc, s);

@@ -262,6 +262,27 @@ def test_knn_split_filter_keeps_tight_clusters_off_the_full_search(ctx, monkeypa
     assert g.stats.rows_full == 0
 
 
+@pytest.mark.parametrize("candidate_filter", ["fp16", "split"])
+def test_knn_bounds_skip_far_tiles_and_keep_the_graph(ctx, monkeypatch, candidate_filter):
+    # Well-separated clusters: the bounded scan (rows by k-means part, each query block's
+    # tiles nearest first) proves most tiles hold no neighbour of the block and skips
+    # them; the same order without bounds, and the Morton order, scan every tile. All
+    # three give the oracle's graph.
+    monkeypatch.setenv("KYTO_GPU_KNN_FILTER", candidate_filter)
+    pts, _ = synthetic.gaussian_mixture(30_000, 50, 24, spread=6.0, seed=21, device="cpu")
+    ref = O.neighbors(pts, 15)
+    got = {}
+    for order in ("bounded", "cluster", "morton"):
+        monkeypatch.setenv("KYTO_GPU_KNN_ORDER", order)
+        g = K.neighbors(pts, 15, ctx=ctx)
+        _graph_equal(g, ref)
+        got[order] = g.stats
+    total = got["bounded"].tiles_total
+    assert total == ((30_000 + 255) // 256) * ((30_000 + 127) // 128)
+    assert got["cluster"].tiles_scanned == total and got["morton"].tiles_scanned == total
+    assert 0 < got["bounded"].tiles_scanned < total // 2, (got["bounded"].tiles_scanned, total)
+
+
 @pytest.mark.parametrize("n_neighbors,n_components", [(2, None), (16, 7), (64, 1)])
 def test_knn_edges(ctx, n_neighbors, n_components):
     pts, _ = synthetic.gaussian_mixture(1500, 50, 10, seed=9, device="cpu")
