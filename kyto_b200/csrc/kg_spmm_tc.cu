@@ -190,22 +190,23 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
         const bool present = sm.present[ls] != 0;
         const uint32_t* masks = reinterpret_cast<const uint32_t*>(st.blk);
         const float* vals = reinterpret_cast<const float*>(st.blk + kMaskBytes);
-        // The row's first value: the stored values of the rows before it (the earlier
-        // warps' rows summed by every warp, then a scan inside the warp).
+        // The row's first value: the stored values of the rows before it. The earlier
+        // warps' rows: one warp-wide add of each lane's popcounts; the rows before it in
+        // this warp: an exclusive scan of the row counts (at most 32, 6 bits) built from
+        // one ballot per bit, popcounts of the lower lanes' bits, no dependent shuffles.
         uint32_t mword = 0, base = 0;
         if (present) {
           mword = masks[r];
           uint32_t before = 0;
           for (int q = 0; q < warp; ++q) before += __popc(masks[q * 32 + lane]);
+          before = __reduce_add_sync(0xFFFFFFFFu, before);
+          const uint32_t cnt = __popc(mword);
+          const uint32_t lower = (1u << lane) - 1u;
+          uint32_t excl = 0;
 #pragma unroll
-          for (int o = 16; o; o >>= 1) before += __shfl_xor_sync(0xFFFFFFFFu, before, o);
-          uint32_t incl = __popc(mword);
-#pragma unroll
-          for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-            if (lane >= o) incl += v;
-          }
-          base = before + incl - __popc(mword);
+          for (int b = 0; b < 6; ++b)
+            excl += (uint32_t)__popc(__ballot_sync(0xFFFFFFFFu, (cnt >> b) & 1u) & lower) << b;
+          base = before + excl;
         }
         // Branch-free: every column's value is loaded from its would-be rank (the rank
         // of the next stored value for an empty cell: still inside the stage buffer,
