@@ -282,7 +282,8 @@ def learned_vs_exact(n: int, ctx) -> dict:
         "exact_full_scan_ms": t_fs * 1e3, "speedup_vs_full_scan": t_fs / t_le,
         "learned": {"train_ms": le_st.train_ms, "index_ms": le_st.index_ms,
                     "search_ms": le_st.search_ms, "fallback_rows": le_st.fallback_rows,
-                    "scanned_tiles": le_st.scanned_tiles, "temperature": le_st.temperature,
+                    "scanned_tiles": le_st.scanned_tiles,
+                    "tiles_computed": le_st.tiles_computed, "temperature": le_st.temperature,
                     "final_loss": le_st.final_loss},
         "exact": {"filter_ms": ex_st.filter_ms, "rank_ms": ex_st.rank_ms,
                   "rows_searched_in_full": ex_st.rows_full,

@@ -288,7 +288,8 @@ typedef struct kg_learned_params {
 
 typedef struct kg_learned_stats {
   uint64_t fallback_rows;  /* rows searched against every row (low confidence) */
-  uint64_t scanned_tiles;  /* point tiles (128 rows) the query blocks scanned, in all */
+  uint64_t scanned_tiles;  /* point tiles (128 rows) in the query blocks' probe lists, in
+                              all: what the network proposes */
   uint64_t candidates;     /* approximate candidates ranked by their exact keys */
   uint64_t rows_full;      /* rows searched in full by the exact re-rank's own checks */
   double train_ms;         /* sample graph, parts and training (host wall time) */
@@ -296,6 +297,8 @@ typedef struct kg_learned_stats {
   double search_ms;        /* the restricted exact search and the graph */
   float final_loss;        /* mean cross-entropy of the last training batch */
   float temperature;       /* the confidence's calibrated temperature (logits scale) */
+  uint64_t tiles_computed; /* of those, the (block, tile) products the filter computed (the
+                              rest skipped on proven distance bounds) */
 } kg_learned_stats;
 
 /* The graph (as kg_knn_exact's: CSR, rows sorted by column, f32 distances) of each

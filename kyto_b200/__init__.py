@@ -134,6 +134,7 @@ class LearnedStats(ctypes.Structure):
         ("search_ms", ctypes.c_double),
         ("final_loss", ctypes.c_float),
         ("temperature", ctypes.c_float),
+        ("tiles_computed", ctypes.c_uint64),
     ]
 
 

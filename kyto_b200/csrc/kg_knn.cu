@@ -243,12 +243,14 @@ void spatial_order(const float* x, uint64_t n, uint32_t width, uint32_t d, const
 
 // Centre (the f64 mean of the group's centred rows), radius (the largest distance of a
 // group row from it, rounded up) and box (each component's smallest and largest centred
-// value) of each group of `size` consecutive slots; per-component arrays are written
-// component-major (c_t[j * n_groups + g]). One 64-thread block per group.
+// value) of each group of `size` consecutive slots; component j of group g is written at
+// g * g_stride + j * j_stride of each per-component array (component-major: g_stride 1,
+// j_stride n_groups; group-major: 64 and 1). One 64-thread block per group.
 __global__ void __launch_bounds__(64)
 group_balls_kernel(const float* x, uint32_t width, uint32_t d, const double* mean,
-                   const uint32_t* rows, uint64_t n, uint32_t size, uint64_t n_groups,
-                   double* centre_t, double* lo_t, double* hi_t, double* radius) {
+                   const uint32_t* rows, uint64_t n, uint32_t size, uint64_t g_stride,
+                   uint64_t j_stride, double* centre_t, double* lo_t, double* hi_t,
+                   double* radius) {
   const uint64_t g = blockIdx.x;
   const uint64_t s0 = g * size, s1 = min(s0 + size, n);
   __shared__ double c[kDim];
@@ -285,9 +287,10 @@ group_balls_kernel(const float* x, uint32_t width, uint32_t d, const double* mea
     __syncthreads();
   }
   if (threadIdx.x == 0) radius[g] = sqrt(red[0]) * (1.0 + 0x1p-40);
-  centre_t[(uint64_t)j * n_groups + g] = j < d ? c[j] : 0.0;
-  lo_t[(uint64_t)j * n_groups + g] = lo;
-  hi_t[(uint64_t)j * n_groups + g] = hi;
+  const uint64_t at = g * g_stride + (uint64_t)j * j_stride;
+  centre_t[at] = j < d ? c[j] : 0.0;
+  lo_t[at] = lo;
+  hi_t[at] = hi;
 }
 
 // Per (query block, tile), two lower bounds on the distance between a row of the block
@@ -375,9 +378,10 @@ bool bounded_scan(const float* x, uint64_t n, uint32_t width, uint32_t d, const 
   DeviceBuffer<double> tc((uint64_t)kDim * n_tiles, s), tlo((uint64_t)kDim * n_tiles, s),
       thi((uint64_t)kDim * n_tiles, s), tr(n_tiles, s);
   group_balls_kernel<<<(unsigned)n_blocks, 64, 0, s>>>(x, width, d, mean, cl.perm.ptr, n, qblock,
-                                                       n_blocks, bc.ptr, blo.ptr, bhi.ptr, br.ptr);
+                                                       1, n_blocks, bc.ptr, blo.ptr, bhi.ptr,
+                                                       br.ptr);
   KG_LAUNCH_CHECK();
-  group_balls_kernel<<<n_tiles, 64, 0, s>>>(x, width, d, mean, cl.perm.ptr, n, kTile, n_tiles,
+  group_balls_kernel<<<n_tiles, 64, 0, s>>>(x, width, d, mean, cl.perm.ptr, n, kTile, 1, n_tiles,
                                             tc.ptr, tlo.ptr, thi.ptr, tr.ptr);
   KG_LAUNCH_CHECK();
   DeviceBuffer<unsigned long long> key(entries, s), key_sorted(entries, s);
@@ -415,6 +419,108 @@ bool bounded_scan(const float* x, uint64_t n, uint32_t width, uint32_t d, const 
   sp.list_stride = n_tiles;
   sp.list_sorted = true;
   return true;
+}
+
+// The bounds of a given CSR of lists (block b's tiles at list_tiles[off[b] .. off[b + 1])):
+// one CTA per block (its ball and box in shared memory), a warp per entry reading the
+// tile's group-major ball and box; the same bound and sort key as ball_bounds_kernel.
+__global__ void __launch_bounds__(256)
+list_bounds_kernel(const uint64_t* off, const uint32_t* list_tiles, const double* bc,
+                   const double* blo, const double* bhi, const double* br, const double* tc,
+                   const double* tlo, const double* thi, const double* tr, uint32_t d, double s2,
+                   double margin, unsigned long long* key) {
+  __shared__ double cb[kDim], lb_[kDim], hb[kDim];
+  const uint64_t b = blockIdx.x;
+  for (uint32_t j = threadIdx.x; j < kDim; j += blockDim.x) {
+    const bool in = j < d;
+    cb[j] = in ? bc[b * kDim + j] : 0.0;
+    lb_[j] = in ? blo[b * kDim + j] : 0.0;
+    hb[j] = in ? bhi[b * kDim + j] : 0.0;
+  }
+  __syncthreads();
+  const double rb = br[b];
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  for (uint64_t i = off[b] + warp; i < off[b + 1]; i += warps) {
+    const uint32_t t = list_tiles[i];
+    double acc = 0.0, box = 0.0;
+    for (uint32_t j = lane; j < d; j += 32) {
+      const uint64_t at = (uint64_t)t * kDim + j;
+      const double u = cb[j] - tc[at];
+      acc = fma(u, u, acc);
+      const double gap = fmax(fmax(tlo[at] - hb[j], lb_[j] - thi[at]), 0.0);
+      box = fma(gap, gap, box);
+    }
+    for (int o = 16; o; o >>= 1) {
+      acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+      box += __shfl_xor_sync(0xFFFFFFFFu, box, o);
+    }
+    if (lane == 0) {
+      const double dist = sqrt(acc);
+      const double ball = dist * (1.0 - 0x1p-40) - rb - tr[t];
+      const double boxd = sqrt(box) * (1.0 - 0x1p-40);
+      const double lb = fmax(fmax(ball, boxd) - margin, 0.0);
+      const float lb2 = __double2float_rd(s2 * lb * lb * (1.0 - 0x1p-40));
+      key[i] = ((unsigned long long)__float_as_uint(lb2) << 32) |
+               __float_as_uint(__double2float_rn(dist));
+    }
+  }
+}
+
+// Bounds for a plan's own CSR lists (the learned form's probe lists): each entry's bound
+// as in bounded_scan, each block's list sorted by (bound, centre distance), skipping on.
+// Leaves sp untouched when the lists exceed the sort's 32-bit sizes.
+void bound_lists(const float* x, uint64_t n_q, uint64_t n_p, uint32_t width, uint32_t d,
+                 const double* mean, double scale, double max_norm, uint32_t qblock,
+                 ScanPlan& sp, cudaStream_t s) {
+  const uint64_t n_blocks = (n_q + qblock - 1) / qblock;
+  const uint32_t n_tiles = (uint32_t)((n_p + kTile - 1) / kTile);
+  uint64_t entries = 0;
+  KG_CUDA(cudaMemcpyAsync(&entries, sp.list_off.ptr + n_blocks, 8, cudaMemcpyDeviceToHost, s));
+  KG_CUDA(cudaStreamSynchronize(s));
+  if (!entries || entries > (uint64_t)INT32_MAX) return;
+  const uint32_t* prows = sp.prows.ptr ? sp.prows.ptr : sp.qrows.ptr;
+  DeviceBuffer<double> bc((uint64_t)kDim * n_blocks, s), blo((uint64_t)kDim * n_blocks, s),
+      bhi((uint64_t)kDim * n_blocks, s), br(n_blocks, s);
+  DeviceBuffer<double> tc((uint64_t)kDim * n_tiles, s), tlo((uint64_t)kDim * n_tiles, s),
+      thi((uint64_t)kDim * n_tiles, s), tr(n_tiles, s);
+  group_balls_kernel<<<(unsigned)n_blocks, 64, 0, s>>>(x, width, d, mean, sp.qrows.ptr, n_q,
+                                                       qblock, kDim, 1, bc.ptr, blo.ptr, bhi.ptr,
+                                                       br.ptr);
+  KG_LAUNCH_CHECK();
+  group_balls_kernel<<<n_tiles, 64, 0, s>>>(x, width, d, mean, prows, n_p, kTile, kDim, 1, tc.ptr,
+                                            tlo.ptr, thi.ptr, tr.ptr);
+  KG_LAUNCH_CHECK();
+  DeviceBuffer<unsigned long long> key(entries, s), key_sorted(entries, s);
+  list_bounds_kernel<<<(unsigned)n_blocks, 256, 0, s>>>(
+      sp.list_off.ptr, sp.list_tiles.ptr, bc.ptr, blo.ptr, bhi.ptr, br.ptr, tc.ptr, tlo.ptr,
+      thi.ptr, tr.ptr, d, scale * scale, 0x1p-30 * max_norm, key.ptr);
+  KG_LAUNCH_CHECK();
+  std::vector<uint64_t> h_off(n_blocks + 1);
+  KG_CUDA(cudaMemcpyAsync(h_off.data(), sp.list_off.ptr, (n_blocks + 1) * 8,
+                          cudaMemcpyDeviceToHost, s));
+  KG_CUDA(cudaStreamSynchronize(s));
+  std::vector<int> h_ioff(n_blocks + 1);
+  for (uint64_t b = 0; b <= n_blocks; ++b) h_ioff[b] = (int)h_off[b];
+  DeviceBuffer<int> ioff(n_blocks + 1, s);
+  KG_CUDA(cudaMemcpyAsync(ioff.ptr, h_ioff.data(), (n_blocks + 1) * sizeof(int),
+                          cudaMemcpyHostToDevice, s));
+  DeviceBuffer<uint32_t> tiles_sorted(entries, s);
+  size_t temp = 0;
+  KG_CUDA(cub::DeviceSegmentedSort::StableSortPairs(
+      nullptr, temp, key.ptr, key_sorted.ptr, sp.list_tiles.ptr, tiles_sorted.ptr, (int)entries,
+      (int)n_blocks, ioff.ptr, ioff.ptr + 1, s));
+  DeviceBuffer<unsigned char> scratch(temp, s);
+  KG_CUDA(cub::DeviceSegmentedSort::StableSortPairs(
+      scratch.ptr, temp, key.ptr, key_sorted.ptr, sp.list_tiles.ptr, tiles_sorted.ptr,
+      (int)entries, (int)n_blocks, ioff.ptr, ioff.ptr + 1, s));
+  sp.list_lb2.alloc(entries, s);
+  key_bounds_kernel<<<std::min<uint64_t>(blocks_for(entries, 256), 8192), 256, 0, s>>>(
+      key_sorted.ptr, entries, sp.list_lb2.ptr);
+  KG_LAUNCH_CHECK();
+  // The host offsets must outlive the copy.
+  KG_CUDA(cudaStreamSynchronize(s));
+  sp.list_tiles = std::move(tiles_sorted);
+  sp.list_sorted = true;
 }
 
 // The batch's rows sample by sample, each sample in Morton order: a query block's own
@@ -1007,6 +1113,15 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
     DeviceBuffer<uint32_t> slot_sample;
     if (plan) {
       (*plan)(x, n, width, d, scale, filter_query_block(kind), sp, trace);
+      // Bounds for the plan's lists too (unless KYTO_GPU_KNN_ORDER=cluster or morton
+      // asks for scans without skipping).
+      const char* ord = std::getenv("KYTO_GPU_KNN_ORDER");
+      if (sp.list_tiles.ptr && sp.list_off.ptr && !sp.list_lb2.ptr &&
+          (!ord || std::string(ord) == "bounded")) {
+        bound_lists(x, n, n, width, d, mean.ptr, scale, std::sqrt(h_largest),
+                    filter_query_block(kind), sp, s);
+        trace.mark("scan bounds");
+      }
     } else if (batch) {
       // Samples one after another, each in Morton order; each query block scans the
       // tiles of the samples it holds.

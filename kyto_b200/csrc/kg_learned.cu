@@ -653,6 +653,7 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
       stats->search_ms = search_ms;
       stats->final_loss = final_loss;
       stats->temperature = temperature;
+      stats->tiles_computed = r.tiles_scanned;
     }
   });
 }

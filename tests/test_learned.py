@@ -102,6 +102,8 @@ def test_learned_search_recall_and_what_training_gains(monkeypatch, candidate_fi
     n_tiles = (n + 127) // 128
     n_blocks = (n + 255) // 256
     assert s1.scanned_tiles < 0.5 * n_tiles * n_blocks
+    # The distance bounds skip listed tiles that cannot hold a neighbour of the block.
+    assert 0 < s1.tiles_computed <= s1.scanned_tiles, (s1.tiles_computed, s1.scanned_tiles)
 
 
 @pytest.mark.parametrize("candidate_filter", ["fp16", "split"])
