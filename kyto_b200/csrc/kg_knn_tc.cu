@@ -52,6 +52,7 @@ constexpr int kEpiWarps = 8;
 constexpr int kTcThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kEndOfBlock = 0xFFFFFFFFu;
+constexpr uint32_t kNoBlock = 0xFFFFFFFFu;  // no query block left: the CTA's roles stop
 
 // SUBS: 64-wide sub-tiles per operand row (1: fp16 or bf16; 2: split hi and lo). KR: the
 // register top-k width (16, 32) or 0 (the k smallest in local memory, any k).
@@ -73,6 +74,8 @@ struct TcSmem {
   uint64_t a_full, a_empty, drained;
   uint32_t stage_tile[kStages];      // the point tile in a stage, or kEndOfBlock
   uint32_t acc_tile[2];              // the point tile in an accumulator, or kEndOfBlock
+  uint32_t block_id[2];              // per block parity: the query block, or kNoBlock
+  uint32_t acc_block[2];             // the query block of an accumulator's item
   float u_max[2][kEpiWarps];         // per block parity and epilogue warp: the largest
                                      // threshold + s^2 |q|^2 of its queries
   uint32_t tmem_base;
@@ -304,20 +307,34 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
     int issued_phase[kStages];
     for (int s = 0; s < kStages; ++s) issued_phase[s] = -1;
     bool ok = true;
-    for (uint64_t qb = blockIdx.x; qb < n_qblocks && ok; qb += gridDim.x, ++bi) {
+    // Query blocks: the CTA's first is its own index, the next ones come from a counter
+    // shared by every CTA (blocks of very different list lengths then even out); the
+    // block index goes to the MMA warp beside the query tiles, and kNoBlock when none is
+    // left.
+    for (;; ++bi) {
+      uint64_t qb = 0;
       if (lane == 0) {
         ok = mbar_wait(&sm.a_empty, (bi & 1) ^ 1, abort);
         if (ok) {
-          for (int w = 0; w < kEpiWarps; ++w) u_max[(bi & 1) * kEpiWarps + w] = INFINITY;
-          mbar_arrive_expect_tx(&sm.a_full, 2 * SUBS * kTileBytes);
-          for (int h = 0; h < 2; ++h)
-            for (int sub = 0; sub < SUBS; ++sub)
-              tma_load_2d(sm.a[h][sub], &tmap_q, &sm.a_full, sub * kTcK,
-                          (int32_t)(qb * kTcQueries + h * 128));
+          qb = bi == 0 ? (uint64_t)blockIdx.x
+                       : (uint64_t)gridDim.x + atomicAdd(scan.block_counter, 1u);
+          if (qb >= n_qblocks) {
+            sm.block_id[bi & 1] = kNoBlock;
+            mbar_arrive(&sm.a_full);
+          } else {
+            for (int w = 0; w < kEpiWarps; ++w) u_max[(bi & 1) * kEpiWarps + w] = INFINITY;
+            sm.block_id[bi & 1] = (uint32_t)qb;
+            mbar_arrive_expect_tx(&sm.a_full, 2 * SUBS * kTileBytes);
+            for (int h = 0; h < 2; ++h)
+              for (int sub = 0; sub < SUBS; ++sub)
+                tma_load_2d(sm.a[h][sub], &tmap_q, &sm.a_full, sub * kTcK,
+                            (int32_t)(qb * kTcQueries + h * 128));
+          }
         }
       }
       ok = __shfl_sync(0xFFFFFFFFu, ok, 0);
-      if (!ok) break;
+      qb = __shfl_sync(0xFFFFFFFFu, qb, 0);
+      if (!ok || qb >= n_qblocks) break;
       const uint64_t l0 = scan.list_off ? scan.list_off[qb] : qb * scan.list_stride;
       const uint64_t len = !scan.list_tiles ? n_tiles
                            : scan.list_off  ? scan.list_off[qb + 1] - l0
@@ -381,6 +398,7 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
         ++it;
         if (!ok || end) break;
       }
+      if (!ok) break;
     }
     if (lane == 0 && scan.tiles_scanned) atomicAdd(scan.tiles_scanned, (unsigned long long)loaded);
     // Every load issued has landed before the CTA may leave (bounded, own loop).
@@ -397,9 +415,21 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
       uint64_t it = 0;
       uint32_t bi = 0;
       bool ok = true;
-      for (uint64_t qb = blockIdx.x; qb < n_qblocks && ok; qb += gridDim.x, ++bi) {
+      for (;; ++bi) {
         if (!mbar_wait(&sm.a_full, bi & 1, abort)) break;
         tc_fence_after();
+        const uint32_t qb = sm.block_id[bi & 1];
+        if (qb == kNoBlock) {
+          // The end of the CTA's work goes to the epilogue through one accumulator.
+          const uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
+          if (!mbar_wait(&sm.tmem_empty[ab], aph ^ 1, abort)) break;
+          sm.acc_tile[ab] = kEndOfBlock;
+          sm.acc_block[ab] = kNoBlock;
+          mbar_arrive(&sm.tmem_full[ab]);
+          mbar_arrive(&sm.tmem_full[ab]);
+          ++it;
+          break;
+        }
         for (;; ++it) {
           const int s = (int)(it % kStages);
           const uint32_t ph = (uint32_t)((it / kStages) & 1);
@@ -412,6 +442,7 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           tc_fence_after();
           const uint32_t pt = sm.stage_tile[s];
           sm.acc_tile[ab] = pt;
+          sm.acc_block[ab] = qb;
           if (pt == kEndOfBlock) {
             mbar_arrive(&sm.empty[s]);
             mbar_arrive(&sm.tmem_full[ab]);
@@ -440,7 +471,8 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           mbar_arrive(&sm.tmem_full[ab]);
           mma_commit(&sm.tmem_full[ab]);
         }
-        if (ok) mma_commit(&sm.a_empty);
+        if (!ok) break;
+        mma_commit(&sm.a_empty);
       }
       // No product may still be running when TMEM is released.
       mma_commit(&sm.drained);
@@ -460,7 +492,22 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
     uint64_t it = 0;
     uint32_t bi = 0;
     bool ok = true;
-    for (uint64_t qb = blockIdx.x; qb < n_qblocks && ok; qb += gridDim.x, ++bi) {
+    for (;; ++bi) {
+      // The block's first item names the block (or the end of the CTA's work).
+      {
+        const uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
+        if (!mbar_wait(&sm.tmem_full[ab], aph, abort)) break;
+      }
+      tc_fence_after();
+      __syncwarp();
+      const uint32_t qb32 = sm.acc_block[(uint32_t)(it & 1)];
+      if (qb32 == kNoBlock) {
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&sm.tmem_empty[(uint32_t)(it & 1)]);
+        ++it;
+        break;
+      }
+      const uint64_t qb = qb32;
       const uint64_t q = qb * kTcQueries + half * 128 + quad * 32 + lane;
       const bool active = q < n_q;
       const uint64_t self = active ? (scan.q_point ? scan.q_point[q] : q) : ~0ull;
@@ -480,14 +527,16 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
       const double sl2 = active ? (double)slack2[q] : 0.0;
       float* ck = cand_key + (active ? q : 0) * (uint64_t)cap;
       uint32_t* cr = cand_row + (active ? q : 0) * (uint64_t)cap;
-      for (;; ++it) {
+      for (bool first = true;; ++it, first = false) {
         const uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
-        if (!mbar_wait(&sm.tmem_full[ab], aph, abort)) {
-          ok = false;
-          break;
+        if (!first) {
+          if (!mbar_wait(&sm.tmem_full[ab], aph, abort)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          __syncwarp();
         }
-        tc_fence_after();
-        __syncwarp();
         const uint32_t pt = sm.acc_tile[ab];
         if (pt == kEndOfBlock) {
           __syncwarp();
@@ -543,6 +592,7 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
         cand_count[q] = st.overflowed ? kOverflow : st.count;
         threshold_out[q] = th;
       }
+      if (!ok) break;
     }
   }
   __syncwarp();
@@ -834,6 +884,9 @@ void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint32_t width, uint
   CUtensorMap mq = tile_map(aq.ptr, n_q, bf16, width_op), mp = tile_map(bp.ptr, n_p, bf16, width_op);
   DeviceBuffer<int> err(1, s);
   err.zero();
+  DeviceBuffer<unsigned int> counter(1, s);
+  counter.zero();
+  scan.block_counter = counter.ptr;
   unsigned long long tiles_before = 0;
   if (trace_on() && scan.tiles_scanned)
     KG_CUDA(cudaMemcpyAsync(&tiles_before, scan.tiles_scanned, 8, cudaMemcpyDeviceToHost, s));

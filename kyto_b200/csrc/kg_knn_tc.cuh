@@ -43,6 +43,8 @@ struct FilterScan {
                                           // [sample_first[s], sample_first[s + 1]) of its
                                           // sample s (a batch of samples searched at once)
   unsigned long long* tiles_scanned = nullptr;  // when set: += tiles the launch multiplied
+  unsigned int* block_counter = nullptr;  // query blocks handed out past the first wave
+                                          // (zero before the launch; set by tc_filter)
   const double* qn2 = nullptr;           // per query slot |q - mean|^2 (set by tc_filter)
   double s2 = 1.0;                       // scale^2 (set by tc_filter)
 };
