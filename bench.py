@@ -417,8 +417,8 @@ def main() -> int:
         e2e = {"value": world * n / (ems / 1e3), "unit": "cells/s", "ms_per_step": ems,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
-    # DRAM bytes (read + write) of the filter launch on this workload, from the one-pass
-    # capture summarised in profiles/knn_filter_dram_1m.md (fp16 kind, bounded scan).
+    # DRAM bytes (read + write) of the filter launch on this workload, from a one-pass ncu
+    # capture of the 1M launch (fp16 kind, bounded scan; its summary is under profiles/).
     filter_traffic_1m = 164.27e9 + 2.50e9
     pk = peaks()
     d = args.components
@@ -431,7 +431,7 @@ def main() -> int:
         "frac": achieved / pk["bf16_tflops"],
         "traffic": filter_traffic_1m if (n == 1_000_000 and d == 50) else None,
         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one capture "
-                          "of the 1M launch (profiles/knn_filter_dram_1m.md)",
+                          "of the 1M launch (summary in profiles/)",
         "peak_source": f"{pk['source']} (bf16 burst)", "launch_ms": f_ms,
         "algorithmic": f"2*n^2*d = {fl:.3e} flop per launch (n={n}, d={d})",
     }
