@@ -1600,10 +1600,20 @@ kg_status kg_pca_knn_batch(kg_ctx* ctx, const kg_pca_params* params, uint32_t n_
     DeviceBuffer<float> emb_all(n * kc, s);
     KG_CUDA(cudaStreamSynchronize(s));
     std::vector<double> var_all((size_t)n_samples * kc);
-    // The samples' PCA: workers take the next sample until none is left; each session
-    // has its own stream, so the small samples' kernels run side by side.
+    // The samples' PCA: workers take the next sample, largest first, until none is left
+    // (the largest samples do not start last and become the tail); each session has its
+    // own stream, so the small samples' kernels run side by side. KYTO_GPU_BATCH_WORKERS
+    // sets the worker count (default 8).
     const auto t0 = std::chrono::steady_clock::now();
-    const unsigned workers = std::min<unsigned>(n_samples, 8);
+    unsigned max_workers = 8;
+    if (const char* w = std::getenv("KYTO_GPU_BATCH_WORKERS"))
+      max_workers = (unsigned)std::max(1, std::min(64, std::atoi(w)));
+    const unsigned workers = std::min<unsigned>(n_samples, max_workers);
+    std::vector<uint32_t> order(n_samples);
+    for (uint32_t i = 0; i < n_samples; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+      return samples[a].n_rows > samples[b].n_rows;
+    });
     std::atomic<uint32_t> next{0};
     std::vector<std::exception_ptr> errors(workers);
     std::vector<std::thread> pool;
@@ -1612,8 +1622,9 @@ kg_status kg_pca_knn_batch(kg_ctx* ctx, const kg_pca_params* params, uint32_t n_
         try {
           KG_CUDA(cudaSetDevice(ctx->device));
           for (;;) {
-            const uint32_t i = next.fetch_add(1);
-            if (i >= n_samples) break;
+            const uint32_t at = next.fetch_add(1);
+            if (at >= n_samples) break;
+            const uint32_t i = order[at];
             check_cancel(ctx);
             std::unique_ptr<kg_pca> p(make_session(ctx, params));
             const kg_batch_sample& b = samples[i];
