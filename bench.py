@@ -174,6 +174,36 @@ def run_step(args, ctx, indptr, idx, vals, out, host: bool):
     return stats
 
 
+def connectivities_timing(args, ctx, graph) -> dict:
+    """The step after the search (the next row of the path): UMAP connectivities of the
+    timed step's 1M-row graph, device arrays in and out, CUDA-event timed (median of 3
+    after one warm-up)."""
+    import torch
+
+    import kyto_b200 as K
+
+    n, k = args.cells, args.neighbors - 1
+    out = (torch.empty(n + 1, dtype=torch.int64, device="cuda"),
+           torch.empty(2 * n * k, dtype=torch.int32, device="cuda"),
+           torch.empty(2 * n * k, dtype=torch.float32, device="cuda"))
+    nnz = K.ctypes.c_uint64()
+    times = []
+    for i in range(4):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        K._check(K.library().kg_connectivities(ctx.handle, K._ptr(graph[0]), K._ptr(graph[1]),
+                                               K._ptr(graph[2]), n, args.neighbors,
+                                               K._ptr(out[0]), K._ptr(out[1]), K._ptr(out[2]),
+                                               K.ctypes.byref(nnz)))
+        b.record()
+        torch.cuda.synchronize()
+        if i:
+            times.append(a.elapsed_time(b))
+    return {"workload": f"{n:,} rows x {k} neighbours (the timed step's graph)",
+            "ms": statistics.median(times), "nnz": int(nnz.value)}
+
+
 def cpu_baseline(args, x, vals, embedding, ctx) -> dict:
     """kyto's CPU path (the oracle's C++ restatement) on a bounded sample, and the
     device PCA of the same sample against it (singular values, principal angles)."""
@@ -307,7 +337,8 @@ def batching(n_samples: int, ctx) -> dict:
         c = synthetic.counts_csr(int(m), 2000, 600.0, 20, 100, seed=100 + i, device="cuda")
         samples.append((c.indptr, c.indices, c.values))
     kw = dict(target_sum=1e4, log1p=True, ctx=ctx)
-    K.pca_neighbors_batch(samples[:4], 2000, 30, 15, **kw)
+    # Warm-up: the whole batch once, so every worker's pooled session resources exist.
+    K.pca_neighbors_batch(samples, 2000, 30, 15, **kw)
     t0 = time.perf_counter()
     out, st = K.pca_neighbors_batch(samples, 2000, 30, 15, **kw)
     t_batch = time.perf_counter() - t0
@@ -446,6 +477,10 @@ def main() -> int:
         cpu = cpu_baseline(args, x, vals, emb, ctx)
     extra = {}
     if rank == 0 and world == 1:
+        try:
+            extra["connectivities"] = connectivities_timing(args, ctx, out_dev)
+        except Exception as e:  # a side measurement never costs the main line
+            extra["connectivities"] = {"error": f"{type(e).__name__}: {e}"}
         for name, fn, on in (("learned_vs_exact", learned_vs_exact, args.learned_cells),
                              ("batching", batching, args.batch_samples)):
             if not on:

@@ -256,6 +256,27 @@ KG_API kg_status kg_pca_knn_batch(kg_ctx* ctx, const kg_pca_params* params, uint
                                   float* embedding, double* variance, uint64_t* indptr,
                                   uint32_t* indices, float* distances, kg_batch_stats* stats);
 
+/* ---------------------------------------------------------------- connectivities -- */
+
+/* scanpy's UMAP connectivities of a kNN graph (pp.neighbors(method="umap"): umap-learn's
+ * fuzzy_simplicial_set with set_op_mix_ratio 1, local_connectivity 1), as kyto computes
+ * them: per row rho (its smallest distance above 0) and sigma (a 64-step f64 bisection to
+ * log2(n_neighbors) within 1e-5, floored at 1e-3 of the row's mean distance, of every
+ * distance for rows whose distances are all 0), memberships exp(-max(0, d - rho) / sigma)
+ * in f32 (0 for an entry naming its own row), and the fuzzy union w + w^T - w o w^T in f32
+ * with zeros dropped. Input: a graph as kg_knn_exact writes it (indptr n_rows + 1 = r *
+ * (n_neighbors - 1); each row's columns strictly increasing; f32 distances), host or
+ * device pointers. Output: the symmetric CSR (out_indptr n_rows + 1, columns increasing in
+ * each row) with *out_nnz entries; out_indices / out_weights must hold
+ * 2 * n_rows * (n_neighbors - 1) entries. Replaces kyto's
+ * connectivities::connectivities (crates/kyto-exec/src/connectivities.rs:84-131), called
+ * at pipeline.rs:638 and umap.rs:607. */
+KG_API kg_status kg_connectivities(kg_ctx* ctx, const uint64_t* indptr, const uint32_t* indices,
+                                   const float* distances, uint64_t n_rows,
+                                   uint32_t n_neighbors, uint64_t* out_indptr,
+                                   uint32_t* out_indices, float* out_weights,
+                                   uint64_t* out_nnz);
+
 /* ------------------------------------------------------- learned-partition kNN ---- */
 
 /* No counterpart in kyto: the north star's learned form. A BF16 MLP (n_components ->

@@ -42,7 +42,7 @@ EXPORTS = (
     "kg_pca_begin", "kg_pca_push_block", "kg_pca_run", "kg_pca_results", "kg_pca_info",
     "kg_pca_embedding_device", "kg_pca_free", "kg_pca_knn_batch", "kg_knn_exact",
     "kg_knn_batch", "kg_knn_learned",
-    "kg_learned_layout", "kg_learned_gradients", "kg_diag_kernel_launches",
+    "kg_learned_layout", "kg_learned_gradients", "kg_diag_kernel_launches", "kg_connectivities",
 )
 
 
@@ -167,6 +167,7 @@ def library() -> ctypes.CDLL:
             "kg_pca_info": [P, P, P, P],
             "kg_pca_embedding_device": [P, ctypes.POINTER(P)],
             "kg_knn_exact": [P, P, U64, U32, U32, U32, P, P, P, ctypes.POINTER(KnnStats)],
+            "kg_connectivities": [P, P, P, P, U64, U32, P, P, P, ctypes.POINTER(U64)],
             "kg_knn_batch": [P, P, U64, U32, U32, U32, P, U32, P, P, P,
                              ctypes.POINTER(KnnStats)],
             "kg_pca_knn_batch": [P, ctypes.POINTER(_PcaParams), U32, ctypes.POINTER(_BatchSample),
@@ -457,6 +458,36 @@ def neighbors(embedding, n_neighbors: int = 15, n_components: int | None = None,
                                   int(n_neighbors), _ptr(indptr), _ptr(indices), _ptr(dist),
                                   ctypes.byref(stats)))
     return Graph(indptr, indices, dist, stats)
+
+
+@dataclass
+class Connectivities:
+    """kyto's ConnectivityGraph: symmetric CSR, columns increasing in each row, f32
+    weights in (0, 1]."""
+
+    indptr: np.ndarray
+    indices: np.ndarray
+    weights: np.ndarray
+
+
+def connectivities(graph: Graph, ctx: Context | None = None) -> Connectivities:
+    """kyto's ``connectivities`` of a neighbour graph (scanpy's UMAP weights): the graph as
+    ``neighbors`` returns it, n_neighbors - 1 entries a row."""
+    ctx = ctx or default_context()
+    indptr = np.ascontiguousarray(graph.indptr, dtype=np.uint64)
+    indices = np.ascontiguousarray(graph.indices, dtype=np.uint32)
+    dist = np.ascontiguousarray(graph.distances, dtype=np.float32)
+    n = len(indptr) - 1
+    k = len(indices) // n if n else 0
+    out_indptr = np.empty(n + 1, dtype=np.uint64)
+    out_indices = np.empty(max(2 * n * k, 1), dtype=np.uint32)
+    out_weights = np.empty(max(2 * n * k, 1), dtype=np.float32)
+    nnz = ctypes.c_uint64()
+    _check(library().kg_connectivities(ctx.handle, _ptr(indptr), _ptr(indices), _ptr(dist), n,
+                                       k + 1, _ptr(out_indptr), _ptr(out_indices),
+                                       _ptr(out_weights), ctypes.byref(nnz)))
+    m = nnz.value
+    return Connectivities(out_indptr, out_indices[:m].copy(), out_weights[:m].copy())
 
 
 def neighbors_batch(embeddings, n_neighbors: int = 15, n_components: int | None = None,

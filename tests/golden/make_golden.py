@@ -14,6 +14,8 @@ What it writes (all small ``.npz`` files beside this script):
 - ``pbmc3k_neighbors.npz``: scanpy's pbmc3k ``X_pca`` (2,700 x 50) and its exact 15-NN
   distance graph (``tests/fixtures/reference/pbmc3k/{pca,neighbors}.npz``); pbmc3k's
   raw counts are a download and are not needed for the kNN fixture.
+- ``{synthetic,pbmc3k}_connectivities.npz``: scanpy's distance graph and its UMAP
+  ``connectivities`` (the same ``neighbors.npz`` files).
 
 Usage: ``python tests/golden/make_golden.py /path/to/kyto``
 """
@@ -93,6 +95,18 @@ def main(kyto: Path) -> None:
         indices=pnn["distances/indices"],
         distances=pnn["distances/data"],
     )
+    # scanpy's UMAP connectivities of those distance graphs (float64 distances in, the
+    # float32 fuzzy-union weights out).
+    for name, graph in (("synthetic", nn), ("pbmc3k", pnn)):
+        np.savez_compressed(
+            HERE / f"{name}_connectivities.npz",
+            dist_indptr=graph["distances/indptr"],
+            dist_indices=graph["distances/indices"],
+            dist_data=graph["distances/data"],
+            indptr=graph["connectivities/indptr"],
+            indices=graph["connectivities/indices"],
+            weights=graph["connectivities/data"],
+        )
 
 
 if __name__ == "__main__":

@@ -365,3 +365,80 @@ def test_pca_neighbors_batch_equals_each_sample_alone(ctx):
         assert np.array_equal(res.embedding.view(np.uint32), one.embedding.view(np.uint32))
         assert np.array_equal(res.variance.view(np.uint64), one.variance.view(np.uint64))
         _graph_equal(g, K.neighbors(one.embedding, 15, ctx=ctx))
+
+
+# ------------------------------------------------------------ connectivities ----------
+
+from oracle import connectivities as OC  # noqa: E402
+
+
+def _conn_equal_edges(gpu, ref):
+    assert np.array_equal(gpu.indptr, np.asarray(ref[0], dtype=np.uint64))
+    assert np.array_equal(gpu.indices, np.asarray(ref[1], dtype=np.uint32))
+
+
+@pytest.mark.parametrize("name", ["synthetic", "pbmc3k"])
+def test_connectivities_match_scanpy_and_the_oracle(ctx, name):
+    # Scanpy's own distance graph in (kyto's connectivities_parity.rs): the same edges as
+    # scanpy's connectivities, weights within 1e-5, and the oracle's weights.
+    g = load_golden(f"{name}_connectivities")
+    ip = g["dist_indptr"].astype(np.uint64)
+    k = int(ip[1] - ip[0])
+    graph = K.Graph(ip, g["dist_indices"].astype(np.uint32), g["dist_data"].astype(np.float32))
+    gpu = K.connectivities(graph, ctx=ctx)
+    _conn_equal_edges(gpu, (g["indptr"], g["indices"]))
+    assert np.abs(gpu.weights.astype(np.float64) - g["weights"]).max() <= 1e-5
+    ref = OC.connectivities(ip, graph.indices, graph.distances, k + 1)
+    _conn_equal_edges(gpu, ref)
+    assert np.abs(gpu.weights.astype(np.float64) - ref[2]).max() <= 1e-6
+    assert (gpu.weights.view(np.uint32) == ref[2].view(np.uint32)).mean() > 0.999
+
+
+def test_connectivities_known_answers_on_the_device(ctx):
+    # kyto's connectivities.rs in-file cases (:279-397) through the C ABI.
+    def graph(rows):
+        k = len(rows[0])
+        return K.Graph(np.arange(len(rows) + 1, dtype=np.uint64) * k,
+                       np.array([c for row in rows for c, _ in row], dtype=np.uint32),
+                       np.array([d for row in rows for _, d in row], dtype=np.float32))
+
+    line = K.connectivities(graph([[(1, 1.0), (2, 3.0)], [(0, 1.0), (2, 2.0)],
+                                   [(0, 3.0), (1, 2.0)]]), ctx=ctx)
+    assert line.indptr.tolist() == [0, 2, 4, 6] and line.indices.tolist() == [1, 2, 0, 2, 0, 1]
+    assert line.weights[0] == 1.0 and 0.0 < line.weights[1] < 1.0
+    same = K.connectivities(graph([[(1, 0.0), (2, 0.0)], [(0, 0.0), (2, 0.0)],
+                                   [(0, 0.0), (1, 0.0)]]), ctx=ctx)
+    assert same.weights.tolist() == [1.0] * 6
+    far = K.connectivities(graph([[(1, 1.0), (2, 1.0), (3, 1e6)], [(0, 1.0), (2, 1.0), (3, 1.0)],
+                                  [(0, 1.0), (1, 1.0), (3, 1.0)],
+                                  [(0, 1e6), (1, 1.0), (2, 1.0)]]), ctx=ctx)
+    assert far.indptr.tolist() == [0, 2, 5, 8, 10]
+    assert far.indices.tolist() == [1, 2, 0, 2, 3, 0, 1, 3, 1, 2]
+
+
+def test_connectivities_of_the_device_graph_with_duplicate_groups(ctx):
+    # A 20,000-row graph from the device search, with a group of 30 identical rows (their
+    # distances all 0: rho 0, the global floor) and rows listing ties: the oracle's edges
+    # and weights.
+    pts, _ = synthetic.gaussian_mixture(20_000, 30, 25, seed=17, device="cpu")
+    pts[500:530] = pts[499]
+    graph = K.neighbors(pts, 15, ctx=ctx)
+    gpu = K.connectivities(graph, ctx=ctx)
+    ref = OC.connectivities(graph.indptr, graph.indices, graph.distances, 15)
+    _conn_equal_edges(gpu, ref)
+    assert np.abs(gpu.weights.astype(np.float64) - ref[2]).max() <= 1e-6
+    assert (gpu.weights.view(np.uint32) == ref[2].view(np.uint32)).mean() > 0.999
+    rows = np.repeat(np.arange(20_000), np.diff(gpu.indptr.astype(np.int64)))
+    dense_pairs = set(zip(rows.tolist(), gpu.indices.tolist()))
+    assert all((c, r) in dense_pairs for r, c in list(dense_pairs)[:5000])  # symmetric
+
+
+def test_connectivities_refusals(ctx):
+    g = K.Graph(np.array([0, 2, 3], dtype=np.uint64), np.array([1, 0, 0], dtype=np.uint32),
+                np.ones(3, dtype=np.float32))
+    with pytest.raises(K.KytoError):
+        K.connectivities(g, ctx=ctx)  # uneven rows
+    g = K.Graph(np.array([0, 2, 4], dtype=np.uint64), np.array([1, 0, 1, 0], dtype=np.uint32),
+                np.ones(4, dtype=np.float32))
+    with pytest.raises(K.KytoError):
+        K.connectivities(g, ctx=ctx)  # columns not increasing in row 1

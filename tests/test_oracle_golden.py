@@ -143,3 +143,69 @@ def test_ties_go_to_the_lower_row():
     keys, rows, _ = O.knn_ranked(pts, 3)
     assert rows[0].tolist() == [1, 2]
     assert rows[1].tolist() == [3, 0]
+
+
+# ------------------------------------------------------------ connectivities ----------
+
+from oracle import connectivities as OC  # noqa: E402
+
+
+def _golden_connectivities(name):
+    g = load_golden(f"{name}_connectivities")
+    ip = g["dist_indptr"]
+    k = int(ip[1] - ip[0])
+    return g, k
+
+
+@pytest.mark.parametrize("name", ["synthetic", "pbmc3k"])
+def test_connectivities_match_scanpy(name):
+    # kyto's connectivities_parity.rs: scanpy's own distances in, the same edges out and
+    # every weight within connectivities.weights (1e-5 absolute).
+    g, k = _golden_connectivities(name)
+    indptr, indices, weights = OC.connectivities(g["dist_indptr"], g["dist_indices"],
+                                                 g["dist_data"].astype(np.float32), k + 1)
+    assert np.array_equal(indptr, g["indptr"].astype(np.uint64))
+    assert np.array_equal(indices, g["indices"].astype(np.uint32))
+    diff = np.abs(weights.astype(np.float64) - g["weights"].astype(np.float64))
+    assert diff.max() <= 1e-5, diff.max()
+    # The f32 exponential rounded once from f64 against numba's expf: a few last bits.
+    assert (weights.view(np.uint32) == g["weights"].view(np.uint32)).mean() > 0.99
+
+
+def _graph(rows):
+    k = len(rows[0])
+    indptr = np.arange(len(rows) + 1, dtype=np.uint64) * k
+    indices = np.array([c for row in rows for c, _ in row], dtype=np.uint32)
+    dist = np.array([d for row in rows for _, d in row], dtype=np.float32)
+    return indptr, indices, dist, k + 1
+
+
+def test_connectivities_known_answers():
+    # The in-file cases of kyto's connectivities.rs tests (:279-397).
+    line = _graph([[(1, 1.0), (2, 3.0)], [(0, 1.0), (2, 2.0)], [(0, 3.0), (1, 2.0)]])
+    ip, ix, w = OC.connectivities(*line)
+    assert ip.tolist() == [0, 2, 4, 6] and ix.tolist() == [1, 2, 0, 2, 0, 1]
+    dense = np.zeros((3, 3), dtype=np.float32)
+    for r in range(3):
+        dense[r, ix[ip[r]:ip[r + 1]]] = w[ip[r]:ip[r + 1]]
+    assert np.array_equal(dense, dense.T)
+    assert dense[0, 1] == 1.0 and dense[1, 2] >= 1.0 - np.finfo(np.float32).eps
+    assert 0.0 < dense[0, 2] < 1.0
+    # sigma's floor rounds once, as umap: bits 983688805.
+    ranked = np.array([[0, 0, 0, 0, 2.4006681, 2.417103, 2.4605973, 2.4799116, 2.5937085]],
+                      dtype=np.float32)
+    sigma, rho = OC.smooth_knn(ranked, 10)
+    assert rho[0] == np.float32(2.4006681) and int(sigma.view(np.uint32)[0]) == 983688805
+    # Duplicates weigh one, the row itself zero (dropped by the union).
+    dup = _graph([[(1, 0.0), (2, 1.0)], [(0, 0.0), (2, 1.0)], [(1, 1.0), (2, 0.0)]])
+    ip, ix, w = OC.connectivities(*dup)
+    assert ip.tolist() == [0, 2, 4, 6] and ix.tolist() == [1, 2, 0, 2, 0, 1]
+    assert w[0] == 1.0 and np.all((w > 0) & (w <= 1))
+    # Rows of zero distances take the global floor: every membership 1.
+    same = _graph([[(1, 0.0), (2, 0.0)], [(0, 0.0), (2, 0.0)], [(0, 0.0), (1, 0.0)]])
+    assert OC.connectivities(*same)[2].tolist() == [1.0] * 6
+    # Underflowing weights are dropped unless the other side holds them.
+    far = _graph([[(1, 1.0), (2, 1.0), (3, 1e6)], [(0, 1.0), (2, 1.0), (3, 1.0)],
+                  [(0, 1.0), (1, 1.0), (3, 1.0)], [(0, 1e6), (1, 1.0), (2, 1.0)]])
+    ip, ix, _ = OC.connectivities(*far)
+    assert ip.tolist() == [0, 2, 5, 8, 10] and ix.tolist() == [1, 2, 0, 2, 3, 0, 1, 3, 1, 2]
