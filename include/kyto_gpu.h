@@ -71,11 +71,21 @@ KG_API size_t kg_last_error(const kg_ctx* ctx, char* buf, size_t len);
  * called at neighbors_gpu.rs:95). NULL clears it. */
 KG_API kg_status kg_set_cancel_flag(kg_ctx* ctx, const volatile int32_t* flag);
 
-/* Reserve `bytes` of device memory for the context's allocations up front (kept by the
- * device's stream-ordered pool until the process ends): later calls carve their buffers
- * out of it instead of growing the pool, whose driver calls can block the host for tens to
- * hundreds of milliseconds mid-call. No kyto counterpart (a deployment knob of this
- * library); 0 does nothing. */
+/* How long a call waits for its device work before it returns KG_ERR_TIMEOUT (default
+ * 900 s). The host stops waiting; the work already queued on the device still runs to its
+ * end, and may still write the call's outputs: synchronize the device (or close the
+ * context) before reusing or freeing them. No kyto counterpart (kyto's GPU calls block
+ * without a limit); a deadline for serving processes. */
+KG_API kg_status kg_set_wait_limit(kg_ctx* ctx, double seconds);
+
+/* Reserve `bytes` of device memory for the library's allocations up front. Every device
+ * buffer of this library comes from its own stream-ordered pool on the device (created at
+ * the first kg_open there, never the device's default pool), which keeps what it frees
+ * until the process ends: later calls carve their buffers out of the reserve instead of
+ * growing the pool, whose driver calls can block the host for tens to hundreds of
+ * milliseconds mid-call. Other allocators in the process (a PyTorch caching allocator, a
+ * CuPy pool) cannot use memory this pool holds. No kyto counterpart (a deployment knob of
+ * this library); 0 does nothing. */
 KG_API kg_status kg_reserve(kg_ctx* ctx, uint64_t bytes);
 
 /* Work done / total of the running or last call, in cells (all passes counted), as
@@ -117,8 +127,11 @@ KG_API kg_status kg_hvg_moments(kg_ctx* ctx, const uint64_t* indptr, const uint3
  * - at most 1,048,576 stored values per block and 65,536 genes; larger inputs return
  *   KG_ERR_INVALID before any launch.
  * Its scratch is one fixed 22.1 MB array of static device memory per device. The first
- * call on a device sets it up (cudaGetSymbolAddress, which loads the code module there),
- * so make that call before any stream capture. Every call on a device shares the
+ * call on a device sets it up (cudaGetSymbolAddress, which loads the code module there
+ * and with it the array): that first call takes the 22.1 MB from the device and can
+ * itself fail with KG_ERR_OOM on a full device, so make it early (at start-up, before
+ * the device fills and before any stream capture); later calls take no memory. Every
+ * call on a device shares the
  * array: calls that overlap in time (two contexts on one device from two threads, or a
  * call made while the kernels of a call that returned KG_CANCELLED or KG_ERR_TIMEOUT
  * still run) race on it and give wrong results. */
@@ -181,6 +194,22 @@ KG_API kg_status kg_pca_info(const kg_pca* pca, uint64_t* n_cells, uint32_t* n_p
 /* The device address of the f32 embedding (n_cells x k) after run, valid until
  * kg_pca_free: lets kg_knn_exact search it without a host round trip. */
 KG_API kg_status kg_pca_embedding_device(const kg_pca* pca, const float** out);
+
+/* Device time of the last run's sparse x dense products (the PCA's HBM-bound hot loop:
+ * the sketch X^T Omega, each pass's X Q and X^T W, the embedding pass X V, and the gene
+ * statistics), from CUDA events around each launch on the session's stream, with their
+ * algorithmic bytes (8 nnz + 4 (n + 1) + 4 g l + 4 n l each, l the product's width): the
+ * figures a roofline of the products is computed from. No kyto counterpart (kyto's
+ * GPU path times nothing); zero launches when the products ran on the SIMT path. */
+typedef struct kg_pca_stats {
+  uint32_t product_launches;
+  uint32_t passes_run;
+  double product_ms;
+  double product_bytes;
+  double run_ms;           /* kg_pca_run's host wall time */
+} kg_pca_stats;
+
+KG_API kg_status kg_pca_run_stats(const kg_pca* pca, kg_pca_stats* out);
 
 KG_API void kg_pca_free(kg_pca* pca);
 
@@ -350,6 +379,26 @@ KG_API kg_status kg_learned_gradients(kg_ctx* ctx, uint32_t din, uint32_t hidden
  * not counted): lets a benchmark state how many of its own kernels a timed region ran.
  * No counterpart in kyto (diagnostics only). */
 KG_API kg_status kg_diag_kernel_launches(uint64_t* count);
+
+/* The library's device pool on `device`: bytes reserved from the driver, bytes in use by
+ * live buffers, and the high-water mark of bytes in use (reset to the current use when
+ * reset_high is nonzero). Any pointer may be NULL. No kyto counterpart (diagnostics). */
+KG_API kg_status kg_diag_pool_usage(int device, uint64_t* reserved, uint64_t* used,
+                                    uint64_t* used_high, int32_t reset_high);
+
+/* Test hook: after `after` more device allocations by this library, every allocation fails
+ * as out of memory (the call returns KG_ERR_OOM and frees what it allocated); UINT64_MAX
+ * turns the injection off. No kyto counterpart (tests the KG_ERR_OOM path without
+ * exhausting a GPU). */
+KG_API kg_status kg_diag_fail_allocations(uint64_t after);
+
+/* Omega's rows as the device PCA draws them (pca.rs:936-950, omega_row: SplitMix64
+ * seeded from (seed, cells[r]), values (x >> 11) 2^-52 - 1), n x width f64 row-major;
+ * cells host or device, out host or device, width 1..64. The device kernels of the PCA
+ * take Omega from the same generator; this export lets a test pin its bits against
+ * kyto's. No kyto counterpart (diagnostics only). */
+KG_API kg_status kg_diag_omega(kg_ctx* ctx, uint64_t seed, const uint64_t* cells, uint64_t n,
+                               uint32_t width, double* out);
 
 #ifdef __cplusplus
 }

@@ -43,6 +43,8 @@ EXPORTS = (
     "kg_pca_embedding_device", "kg_pca_free", "kg_pca_knn_batch", "kg_knn_exact",
     "kg_knn_batch", "kg_knn_learned",
     "kg_learned_layout", "kg_learned_gradients", "kg_diag_kernel_launches", "kg_connectivities",
+    "kg_pca_run_stats", "kg_diag_omega", "kg_diag_pool_usage", "kg_diag_fail_allocations",
+    "kg_set_wait_limit",
 )
 
 
@@ -75,6 +77,19 @@ class KnnStats(ctypes.Structure):
         ("rank_ms", ctypes.c_double),
         ("tiles_scanned", ctypes.c_uint64),
         ("tiles_total", ctypes.c_uint64),
+    ]
+
+
+class PcaStats(ctypes.Structure):
+    """kg_pca_stats: the last run's sparse x dense products (device ms from CUDA events
+    around each launch, algorithmic bytes) and the run's host wall time."""
+
+    _fields_ = [
+        ("product_launches", ctypes.c_uint32),
+        ("passes_run", ctypes.c_uint32),
+        ("product_ms", ctypes.c_double),
+        ("product_bytes", ctypes.c_double),
+        ("run_ms", ctypes.c_double),
     ]
 
 
@@ -154,6 +169,7 @@ def library() -> ctypes.CDLL:
             "kg_last_error": [P, ctypes.c_char_p, ctypes.c_size_t],
             "kg_set_cancel_flag": [P, P],
             "kg_reserve": [P, U64],
+            "kg_set_wait_limit": [P, ctypes.c_double],
             "kg_progress": [P, P, P],
             "kg_normalize_log1p": [P, P, P, ctypes.c_int, U64, ctypes.c_double, I32, P],
             "kg_hvg_moments": [P, P, P, P, ctypes.c_int, U64, U32, ctypes.c_double, I32, P, P, P],
@@ -177,6 +193,10 @@ def library() -> ctypes.CDLL:
             "kg_learned_layout": [U32, U32, U32, P, P],
             "kg_learned_gradients": [P, U32, U32, U32, P, P, U32, P, U32, P, P, P],
             "kg_diag_kernel_launches": [P],
+            "kg_pca_run_stats": [P, ctypes.POINTER(PcaStats)],
+            "kg_diag_omega": [P, U64, P, U64, U32, P],
+            "kg_diag_pool_usage": [ctypes.c_int, P, P, P, I32],
+            "kg_diag_fail_allocations": [U64],
         }
         for name, args in sig.items():
             fn = getattr(lib, name)
@@ -240,6 +260,10 @@ class Context:
         (kg_reserve): later calls do not grow the device pool mid-call."""
         _check(library().kg_reserve(self._h, int(nbytes)))
 
+    def set_wait_limit(self, seconds: float) -> None:
+        """Seconds a call waits for its device work before KG_ERR_TIMEOUT."""
+        _check(library().kg_set_wait_limit(self._h, float(seconds)))
+
     def progress(self) -> tuple[int, int]:
         done, total = ctypes.c_uint64(), ctypes.c_uint64()
         _check(library().kg_progress(self._h, ctypes.byref(done), ctypes.byref(total)))
@@ -272,6 +296,29 @@ def _u64(a):
 
 def _u32(a):
     return np.ascontiguousarray(a, dtype=np.uint32) if isinstance(a, np.ndarray) else a
+
+
+def omega(seed: int, cells, width: int, ctx: Context | None = None) -> np.ndarray:
+    """Omega's rows as the device PCA draws them (kg_diag_omega): len(cells) x width f64."""
+    ctx = ctx or default_context()
+    cells = np.ascontiguousarray(cells, dtype=np.uint64)
+    out = np.empty((len(cells), int(width)))
+    _check(library().kg_diag_omega(ctx.handle, int(seed), _ptr(cells), len(cells), int(width),
+                                   _ptr(out)))
+    return out
+
+
+def pool_usage(device: int = 0, reset_high: bool = False) -> dict:
+    """The library's device pool: reserved, used and high-water bytes (kg_diag_pool_usage)."""
+    r, u, h = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    _check(library().kg_diag_pool_usage(int(device), ctypes.byref(r), ctypes.byref(u),
+                                        ctypes.byref(h), int(bool(reset_high))))
+    return {"reserved": r.value, "used": u.value, "used_high": h.value}
+
+
+def fail_allocations(after: int | None) -> None:
+    """Test hook: fail every allocation after ``after`` more (None: stop failing)."""
+    _check(library().kg_diag_fail_allocations(0xFFFFFFFFFFFFFFFF if after is None else int(after)))
 
 
 def kernel_launches() -> int:
@@ -380,6 +427,11 @@ class PcaSession:
         n, g, p = ctypes.c_uint64(), ctypes.c_uint32(), ctypes.c_uint32()
         _check(library().kg_pca_info(self._h, ctypes.byref(n), ctypes.byref(g), ctypes.byref(p)))
         return n.value, g.value, p.value
+
+    def stats(self) -> PcaStats:
+        st = PcaStats()
+        _check(library().kg_pca_run_stats(self._h, ctypes.byref(st)))
+        return st
 
     def embedding_device_ptr(self) -> int:
         out = ctypes.c_void_p()

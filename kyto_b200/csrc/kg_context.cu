@@ -3,6 +3,27 @@
 
 namespace kg {
 std::atomic<uint64_t> g_launches{0};
+std::atomic<uint64_t> g_allocs_left{UINT64_MAX};
+
+cudaMemPool_t device_pool(int device) {
+  static std::mutex mu;
+  static std::vector<cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> lock(mu);
+  if ((size_t)device >= pools.size()) pools.resize((size_t)device + 1, nullptr);
+  if (!pools[device]) {
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    cudaMemPool_t pool = nullptr;
+    KG_CUDA(cudaMemPoolCreate(&pool, &props));
+    uint64_t threshold = UINT64_MAX;
+    KG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    pools[device] = pool;
+  }
+  return pools[device];
+}
 
 std::string& last_error() {
   thread_local std::string message;
@@ -11,11 +32,10 @@ std::string& last_error() {
 
 void trace_slow_alloc(size_t bytes, double ms) {
   int device = 0;
-  cudaMemPool_t pool;
   uint64_t reserved = 0, used = 0;
   size_t free_b = 0, total_b = 0;
-  if (cudaGetDevice(&device) == cudaSuccess &&
-      cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+  if (cudaGetDevice(&device) == cudaSuccess) {
+    cudaMemPool_t pool = device_pool(device);
     cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
     cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
   }
@@ -51,11 +71,9 @@ kg_status kg_open(int device, kg_ctx** out) {
       KG_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
       KG_CUBLAS(cublasCreate(&ctx->cublas));
       KG_CUSOLVER(cusolverDnCreate(&ctx->cusolver));
-      // Pool memory stays with the pool between calls (no release to the OS).
-      cudaMemPool_t pool;
-      KG_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
-      uint64_t threshold = UINT64_MAX;
-      KG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+      // The library's own pool on this device (memory it frees stays there between
+      // calls; the device's default pool is left as the process set it).
+      kg::device_pool(device);
     } catch (...) {
       if (ctx->cusolver) cusolverDnDestroy(ctx->cusolver);
       if (ctx->cublas) cublasDestroy(ctx->cublas);
@@ -102,14 +120,22 @@ kg_status kg_set_cancel_flag(kg_ctx* ctx, const volatile int32_t* flag) {
   });
 }
 
+kg_status kg_set_wait_limit(kg_ctx* ctx, double seconds) {
+  return kg::guarded([&] {
+    if (!ctx) kg::fail(KG_ERR_INVALID, "kg_set_wait_limit: ctx is NULL");
+    if (!(seconds > 0.0)) kg::fail(KG_ERR_INVALID, "kg_set_wait_limit: seconds must be > 0");
+    ctx->wait_limit_s = seconds;
+  });
+}
+
 kg_status kg_reserve(kg_ctx* ctx, uint64_t bytes) {
   return kg::guarded([&] {
     if (!ctx) kg::fail(KG_ERR_INVALID, "kg_reserve: ctx is NULL");
     if (!bytes) return;
     KG_CUDA(cudaSetDevice(ctx->device));
-    // The pool's release threshold is the maximum (kg_open): a freed block stays reserved.
+    // The library pool's release threshold is the maximum: a freed block stays reserved.
     void* p = nullptr;
-    KG_CUDA(cudaMallocAsync(&p, bytes, ctx->stream));
+    KG_CUDA(cudaMallocFromPoolAsync(&p, bytes, kg::device_pool(ctx->device), ctx->stream));
     KG_CUDA(cudaFreeAsync(p, ctx->stream));
     KG_CUDA(cudaStreamSynchronize(ctx->stream));
   });
@@ -121,6 +147,25 @@ kg_status kg_progress(const kg_ctx* ctx, uint64_t* done, uint64_t* total) {
     if (done) *done = ctx->done.load();
     if (total) *total = ctx->total.load();
   });
+}
+
+kg_status kg_diag_pool_usage(int device, uint64_t* reserved, uint64_t* used,
+                             uint64_t* used_high, int32_t reset_high) {
+  return kg::guarded([&] {
+    int n = 0;
+    KG_CUDA(cudaGetDeviceCount(&n));
+    if (device < 0 || device >= n) kg::fail(KG_ERR_INVALID, "kg_diag_pool_usage: no such device");
+    cudaMemPool_t pool = kg::device_pool(device);
+    uint64_t v = 0;
+    if (reserved) KG_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, reserved));
+    if (used) KG_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, used));
+    if (used_high) KG_CUDA(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemHigh, used_high));
+    if (reset_high) KG_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrUsedMemHigh, &v));
+  });
+}
+
+kg_status kg_diag_fail_allocations(uint64_t after) {
+  return kg::guarded([&] { kg::g_allocs_left.store(after); });
 }
 
 kg_status kg_diag_kernel_launches(uint64_t* count) {

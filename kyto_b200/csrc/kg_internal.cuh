@@ -88,7 +88,19 @@ inline bool trace_on() {
 // the call blocks, when no free range of the pool fits the request).
 void trace_slow_alloc(size_t bytes, double ms);
 
-// A device allocation, stream-ordered (cudaMallocAsync / cudaFreeAsync).
+// The library's own stream-ordered memory pool on `device` (created at the first use,
+// kept until the process ends), with its release threshold at the maximum: memory this
+// library frees stays with its pool for the next call instead of going back to the
+// driver, and no other allocator's pool (the device's default pool, which a PyTorch or
+// CuPy process may use) has its threshold changed.
+cudaMemPool_t device_pool(int device);
+
+// Allocation failures injected for tests (kg_diag_fail_allocations): after `n` more
+// allocations every allocation fails as out of memory, until the count is reset.
+extern std::atomic<uint64_t> g_allocs_left;
+
+// A device allocation, stream-ordered (cudaMallocFromPoolAsync on the library's pool /
+// cudaFreeAsync).
 template <class T>
 struct DeviceBuffer {
   T* ptr = nullptr;
@@ -117,12 +129,24 @@ struct DeviceBuffer {
     stream = s;
     count = n;
     if (!n) return;
+    if (g_allocs_left.load(std::memory_order_relaxed) != UINT64_MAX) {
+      uint64_t left = g_allocs_left.load();
+      while (left != UINT64_MAX && left > 0 && !g_allocs_left.compare_exchange_weak(left, left - 1)) {
+      }
+      if (left == 0) {
+        count = 0;
+        fail_cuda(cudaErrorMemoryAllocation, "an injected allocation failure", __FILE__, __LINE__);
+      }
+    }
+    int device = 0;
+    KG_CUDA(cudaGetDevice(&device));
+    cudaMemPool_t pool = device_pool(device);
     if (!trace_on()) {
-      KG_CUDA(cudaMallocAsync((void**)&ptr, n * sizeof(T), s));
+      KG_CUDA(cudaMallocFromPoolAsync((void**)&ptr, n * sizeof(T), pool, s));
       return;
     }
     auto t0 = std::chrono::steady_clock::now();
-    KG_CUDA(cudaMallocAsync((void**)&ptr, n * sizeof(T), s));
+    KG_CUDA(cudaMallocFromPoolAsync((void**)&ptr, n * sizeof(T), pool, s));
     double ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (ms > 2.0) trace_slow_alloc(n * sizeof(T), ms);
   }

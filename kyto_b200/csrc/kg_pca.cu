@@ -131,16 +131,24 @@ __device__ __forceinline__ uint64_t splitmix_mix(uint64_t v) {
   return v ^ (v >> 31);
 }
 
+// A cell's Omega stream: seeded from (seed, the cell's table position), then one
+// value in [-1, 1) per column (pca.rs:936-950). Every kernel that needs Omega draws it
+// from these two functions.
+__device__ __forceinline__ uint64_t omega_state(uint64_t seed, uint64_t cell) {
+  return splitmix_mix(seed ^ splitmix_mix(cell + 0x9E3779B97F4A7C15ull));
+}
+__device__ __forceinline__ double omega_next(uint64_t& state) {
+  state += 0x9E3779B97F4A7C15ull;
+  return __dadd_rn((double)(splitmix_mix(state) >> 11) * 0x1p-52, -1.0);
+}
+
 __global__ void omega_kernel(const uint64_t* cells, uint64_t n, uint32_t width,
                              uint64_t seed, double* out) {
   uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (r >= n) return;
-  uint64_t state = splitmix_mix(seed ^ splitmix_mix(cells[r] + 0x9E3779B97F4A7C15ull));
+  uint64_t state = omega_state(seed, cells[r]);
   double* row = out + r * (uint64_t)width;
-  for (uint32_t j = 0; j < width; ++j) {
-    state += 0x9E3779B97F4A7C15ull;
-    row[j] = __dadd_rn((double)(splitmix_mix(state) >> 11) * 0x1p-52, -1.0);
-  }
+  for (uint32_t j = 0; j < width; ++j) row[j] = omega_next(state);
 }
 
 // D^T = [1 ... 1; 0 ...] (row 0 ones over the n cells, everything else zero).
@@ -751,13 +759,12 @@ __global__ void omega_t_kernel(const uint64_t* cells, uint64_t n, uint32_t width
   __shared__ double red[8][64];
   uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   bool live = r < n;
-  uint64_t state = live ? splitmix_mix(seed ^ splitmix_mix(cells[r] + 0x9E3779B97F4A7C15ull)) : 0;
+  uint64_t state = live ? omega_state(seed, cells[r]) : 0;
   const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
   for (uint32_t j = 0; j < 64; ++j) {
     float hi = 0.0f, lo = 0.0f;
     if (live && j < width) {
-      state += 0x9E3779B97F4A7C15ull;
-      double om = __dadd_rn((double)(splitmix_mix(state) >> 11) * 0x1p-52, -1.0);
+      double om = omega_next(state);
       hi = tf32_rna((float)om);
       lo = tf32_rna((float)(om - (double)hi));
     }
@@ -853,9 +860,66 @@ __global__ void unpack_rows_kernel(const uint64_t* packed, uint64_t n, uint32_t*
 
 // The held input for the tensor-core products: X and X^T in the blocked layout
 // (kg_spmm_tc.cuh), and the D^T buffers the passes fill.
+// Device time and algorithmic bytes of a session's sparse x dense products: a CUDA event
+// pair around each launch on the session's stream, read once the run has finished.
+struct ProductClock {
+  struct Launch {
+    cudaEvent_t a = nullptr, b = nullptr;
+    double bytes = 0.0;
+  };
+  std::vector<Launch> launches;
+  cudaStream_t s = nullptr;
+  void begin(cudaStream_t st, double bytes) {
+    s = st;
+    Launch l;
+    l.bytes = bytes;
+    if (cudaEventCreate(&l.a) != cudaSuccess || cudaEventCreate(&l.b) != cudaSuccess) {
+      cudaGetLastError();
+      return;
+    }
+    cudaEventRecord(l.a, s);
+    launches.push_back(l);
+  }
+  void end() {
+    if (!launches.empty()) cudaEventRecord(launches.back().b, s);
+  }
+  // Sums over the launches (after the stream finished); releases the events.
+  void collect(uint32_t& count, double& ms, double& bytes) {
+    count = 0;
+    ms = 0.0;
+    bytes = 0.0;
+    for (Launch& l : launches) {
+      float t = 0.0f;
+      if (cudaEventElapsedTime(&t, l.a, l.b) == cudaSuccess) {
+        ++count;
+        ms += t;
+        bytes += l.bytes;
+      } else {
+        cudaGetLastError();
+      }
+    }
+    release();
+  }
+  void release() {
+    for (Launch& l : launches) {
+      if (l.a) cudaEventDestroy(l.a);
+      if (l.b) cudaEventDestroy(l.b);
+    }
+    launches.clear();
+  }
+  ~ProductClock() { release(); }
+};
+
 struct TcHeld {
   static constexpr uint64_t kSegChunks = 512;  // K-chunks (16,384 cells) per X^T work item
-  uint64_t n = 0, g = 0, n_ld = 0, g_ld = 0;
+  uint64_t n = 0, g = 0, n_ld = 0, g_ld = 0, nnz = 0;
+  ProductClock clock;
+  // A product's algorithmic bytes, S (rows x K, nnz values) . D (K x l) read once and
+  // the rows x l result written once: 8 nnz + 4 (n + 1) + 4 g l + 4 n l (f32 values and
+  // u32 indices, row offsets, the dense operand and result in f32).
+  double product_bytes(uint32_t l) const {
+    return 8.0 * (double)nnz + 4.0 * (double)(n + 1) + 4.0 * (double)g * l + 4.0 * (double)n * l;
+  }
   Blocked bx, bxt;
   DeviceBuffer<float> dt_hi, dt_lo;    // 64 x n_ld: Omega^T or W^T
   DeviceBuffer<float> qt_hi, qt_lo;    // 64 x g_ld: Q^T or V^T
@@ -865,6 +929,7 @@ struct TcHeld {
              uint32_t n_genes, uint64_t nnz, int sm_count, cudaStream_t s, Trace& trace) {
     n = n_rows;
     g = n_genes;
+    this->nnz = nnz;
     n_ld = (n + 3) & ~3ull;
     g_ld = (g + 3) & ~3ull;
     sm = sm_count;
@@ -913,7 +978,9 @@ struct TcHeld {
     a.out.mode = kOutPartial;
     a.out.partial = partial.ptr;
     a.sm_count = sm;
+    clock.begin(s, product_bytes(w));
     spmm_tc(a, s);
+    clock.end();
     reduce_segments_kernel<<<blocks_for(g * w, 256), 256, 0, s>>>(partial.ptr, (uint32_t)segs,
                                                                   (uint32_t)g, w, out);
     KG_LAUNCH_CHECK();
@@ -946,7 +1013,9 @@ struct TcHeld {
     }
     a.out.rows_f32 = rows_f32;
     a.sm_count = sm;
+    clock.begin(s, product_bytes(w));
     spmm_tc(a, s);
+    clock.end();
     if (wsums) {
       sum_blocks_kernel<<<1, 1024, 0, s>>>(colsum.ptr, tiles, w, wsums);
       KG_LAUNCH_CHECK();
@@ -981,6 +1050,9 @@ struct kg_pca {
   DeviceBuffer<double> means;
   std::vector<double> variance, variance_ratio;
   const char* products_engine = "";
+  // The last run's sparse x dense products (kg_pca_run_stats).
+  uint32_t product_launches = 0;
+  double product_ms = 0.0, product_bytes = 0.0, run_ms = 0.0;
 
   ~kg_pca() {
     if (stream) cudaStreamSynchronize(stream);
@@ -1481,6 +1553,7 @@ void kg_pca::run() {
       loadings64.ptr, g, k, set_genes.ptr, stream_genes, loadings.ptr);
   KG_LAUNCH_CHECK();
   wait_stream(c, s);
+  th.clock.collect(product_launches, product_ms, product_bytes);
   ++passes_run;
   c->done += n;
   double total = 0.0;
@@ -1686,7 +1759,40 @@ kg_status kg_pca_run(kg_pca* pca) {
   return guarded([&] {
     if (!pca) fail(KG_ERR_INVALID, "kg_pca_run: NULL argument");
     use_device(pca->ctx);
+    const auto t0 = std::chrono::steady_clock::now();
     pca->run();
+    pca->run_ms =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+  });
+}
+
+kg_status kg_pca_run_stats(const kg_pca* pca, kg_pca_stats* out) {
+  return guarded([&] {
+    if (!pca || !out) fail(KG_ERR_INVALID, "kg_pca_run_stats: NULL argument");
+    if (!pca->ran) fail(KG_ERR_STATE, "kg_pca_run_stats before kg_pca_run");
+    out->product_launches = pca->product_launches;
+    out->passes_run = pca->passes_run;
+    out->product_ms = pca->product_ms;
+    out->product_bytes = pca->product_bytes;
+    out->run_ms = pca->run_ms;
+  });
+}
+
+kg_status kg_diag_omega(kg_ctx* ctx, uint64_t seed, const uint64_t* cells, uint64_t n,
+                        uint32_t width, double* out) {
+  return guarded([&] {
+    if (!ctx || !cells || !out) fail(KG_ERR_INVALID, "kg_diag_omega: NULL argument");
+    if (width == 0 || width > 64) fail(KG_ERR_INVALID, "kg_diag_omega: width must be 1..64");
+    if (n == 0) return;
+    use_device(ctx);
+    cudaStream_t s = ctx->stream;
+    DeviceBuffer<uint64_t> hc;
+    const uint64_t* d_cells = device_view(cells, n, hc, s);
+    DeviceBuffer<double> omega(n * width, s);
+    omega_kernel<<<blocks_for(n, 128), 128, 0, s>>>(d_cells, n, width, seed, omega.ptr);
+    KG_LAUNCH_CHECK();
+    KG_CUDA(cudaMemcpyAsync(out, omega.ptr, n * width * 8ull, cudaMemcpyDefault, s));
+    wait_stream(ctx, s);
   });
 }
 

@@ -56,6 +56,13 @@ def lib() -> ctypes.CDLL:
         _lib = ctypes.CDLL(str(LIB_PATH))
         _lib.ko_knn_exact.restype = ctypes.c_uint64
         _lib.ko_knn_exact_range.restype = ctypes.c_uint64
+        _lib.ko_knn_prepare.restype = ctypes.c_void_p
+        _lib.ko_knn_prepare.argtypes = [_P, _U64, _U32]
+        _lib.ko_knn_search.restype = ctypes.c_uint64
+        _lib.ko_knn_search.argtypes = [ctypes.c_void_p, _U32, _U64, _U64, _P, _P]
+        _lib.ko_knn_free.argtypes = [ctypes.c_void_p]
+        _lib.ko_knn_search_rows.restype = ctypes.c_uint64
+        _lib.ko_knn_search_rows.argtypes = [ctypes.c_void_p, _U32, _P, _U64, _P, _P]
         _lib.ko_key.restype = ctypes.c_double
         _lib.ko_key.argtypes = [_P, _U32, _U64, _U64]
         _lib.ko_max_threads.restype = ctypes.c_int
@@ -233,6 +240,32 @@ def hvg_seurat(sums, squares, positives, n_cells: int, n_top_genes: int | None):
 # ----------------------------------------------------------------------------------
 # PCA (crates/kyto-exec/src/pca.rs, pca_dense.rs)
 # ----------------------------------------------------------------------------------
+def omega_rows(seed: int, cells: np.ndarray, width: int) -> np.ndarray:
+    """Omega's rows for the cells at these table positions (pca.rs:936-950, omega_row):
+    len(cells) x width f64."""
+    cells = np.ascontiguousarray(cells, dtype=np.uint64)
+    out = np.empty((len(cells), int(width)))
+    lib().ko_omega_rows(_U64(seed), _ptr(cells), _U64(len(cells)), _U32(width), _ptr(out))
+    return out
+
+
+def _splitmix_mix(v: int) -> int:
+    m = (1 << 64) - 1
+    v = ((v ^ (v >> 30)) * 0xBF58476D1CE4E5B9) & m
+    v = ((v ^ (v >> 27)) * 0x94D049BB133111EB) & m
+    return v ^ (v >> 31)
+
+
+def omega_row_reference(seed: int, cell: int, width: int) -> list[float]:
+    """pca.rs:936-950 in pure Python integers (checks the C restatement's bits)."""
+    m = (1 << 64) - 1
+    golden = 0x9E3779B97F4A7C15
+    state = _splitmix_mix((seed ^ _splitmix_mix((cell + golden) & m)) & m)
+    out = []
+    for _ in range(width):
+        state = (state + golden) & m
+        out.append(float(_splitmix_mix(state) >> 11) * 2.0**-52 - 1.0)
+    return out
 def extend_basis(basis: np.ndarray, block: np.ndarray) -> np.ndarray:
     """pca_dense.rs:105-129: CGS twice, thin SVD, keep sigma > 1e-10 |block|_F."""
     scale = float(np.linalg.norm(block))
@@ -336,7 +369,7 @@ def pca(x: Csr, n_components: int, seed: int = 0, gene_set: np.ndarray | None = 
     width = min(k + PCA_OVERSAMPLES, n_genes)
     L = lib()
     common = (_ptr(x.indptr), _ptr(x.indices), _ptr(values), _U64(n_rows),
-              _ptr(gene_map), _U32(n_genes))
+              _ptr(gene_map), _U32(stream_genes), _U32(n_genes))
 
     # Pass 0: sketch.
     sums = np.empty(n_genes)
@@ -466,6 +499,49 @@ def knn_exact_sample(points: np.ndarray, n_neighbors: int, q_begin: int, q_end: 
     fb = lib().ko_knn_exact_range(_ptr(points), _U64(n), _U32(width), _U32(k), _U64(q_begin),
                                   _U64(q_end), _ptr(keys), _ptr(rows))
     return keys, rows, int(fb)
+
+
+class KnnIndex:
+    """kyto's CPU exact search split as kyto splits it (neighbors_exact.rs:98-160
+    ``Prepared::new``, then ``search_block`` per 128 queries): ``prepare`` centres the
+    rows, computes the offsets and slacks and lays out the point tiles once; ``search``
+    ranks any range of query rows against every row. The timed CPU baseline pays the
+    setup once and samples the per-query cost on enough queries to keep every host
+    thread busy."""
+
+    def __init__(self, points: np.ndarray):
+        self.points = np.ascontiguousarray(points, dtype=np.float32)
+        n, width = self.points.shape
+        self.n, self.width = n, width
+        self._h = lib().ko_knn_prepare(_ptr(self.points), n, width)
+
+    def search(self, n_neighbors: int, q_begin: int, q_end: int):
+        """(keys, rows, fallbacks) of queries [q_begin, q_end), ranked by (key, row)."""
+        k = int(n_neighbors) - 1
+        keys = np.empty((q_end - q_begin, k))
+        rows = np.empty((q_end - q_begin, k), dtype=np.uint32)
+        fb = lib().ko_knn_search(self._h, k, q_begin, q_end, _ptr(keys), _ptr(rows))
+        return keys, rows, int(fb)
+
+    def search_rows(self, n_neighbors: int, rows: np.ndarray):
+        """(keys, rows, fallbacks) of the given query rows, in their order."""
+        rows = np.ascontiguousarray(rows, dtype=np.uint64)
+        k = int(n_neighbors) - 1
+        keys = np.empty((len(rows), k))
+        out = np.empty((len(rows), k), dtype=np.uint32)
+        fb = lib().ko_knn_search_rows(self._h, k, _ptr(rows), len(rows), _ptr(keys), _ptr(out))
+        return keys, out, int(fb)
+
+    def close(self) -> None:
+        if self._h:
+            lib().ko_knn_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def neighbors(points: np.ndarray, n_neighbors: int = 15, method: str = "brute") -> Graph:
