@@ -175,6 +175,19 @@ KG_API kg_status kg_pca_push_block(kg_pca* pca, const uint64_t* indptr, const ui
                             const void* values, kg_dtype dtype, uint64_t n_rows,
                             const uint64_t* cells);
 
+/* kg_pca_push_block without waiting: the block's host->device copies and pack kernels
+ * are queued on the session's own stream and the call returns at once, so the copies
+ * (cudaMemcpyAsync, truly asynchronous from pinned host memory) run beside other work on
+ * the device, such as another session's passes or a kNN search (kyto's streaming of
+ * store blocks through pinned buffers, kyto-exec/src/block_stream.rs:65-303). The host
+ * arrays stay in use until kg_pca_run returns: the caller keeps them alive and
+ * unchanged until then. Gene indices are checked when the run starts (KG_ERR_INVALID
+ * there); without a gene map and with a host indptr the call does not wait on the
+ * device at all. */
+KG_API kg_status kg_pca_push_block_async(kg_pca* pca, const uint64_t* indptr,
+                                         const uint32_t* indices, const void* values,
+                                         kg_dtype dtype, uint64_t n_rows, const uint64_t* cells);
+
 /* Run all passes on the device (pass 0 sketch, 9 Krylov products, the embedding pass)
  * with the FP64 orthonormalisation and Rayleigh-Ritz steps between them. Replaces
  * the folds of pca/gpu.rs:149-219 and PcaAccumulator::end_pass (pca.rs:699-801). */
@@ -391,6 +404,20 @@ KG_API kg_status kg_diag_pool_usage(int device, uint64_t* reserved, uint64_t* us
  * turns the injection off. No kyto counterpart (tests the KG_ERR_OOM path without
  * exhausting a GPU). */
 KG_API kg_status kg_diag_fail_allocations(uint64_t after);
+
+/* One of the PCA's tensor-core products on a caller's CSR matrix (n_rows x n_cols, f32
+ * values, columns strictly increasing in each row; host or device arrays), through the
+ * same blocked layout and kernel the PCA uses: out (rows x width, column-major f64) =
+ * S D, with S the matrix (transposed = 0: rows = n_rows, K = n_cols) or its transpose
+ * (transposed = 1: rows = n_cols, K = n_rows), each stored value first mapped by
+ * value_mode (0: as is; 1: (v - row_means[row])^2; 2: 1), and D the K x width
+ * column-major f64 `dense` (value modes 1 and 2: D is a column of ones and `dense` is
+ * ignored). width 1..64, n_cols <= 65,535. No kyto counterpart (diagnostics: lets a test
+ * check the layout and the product against a plain f64 product). */
+KG_API kg_status kg_diag_spmm(kg_ctx* ctx, const uint64_t* indptr, const uint32_t* indices,
+                              const float* values, uint64_t n_rows, uint32_t n_cols,
+                              int32_t transposed, int32_t value_mode, const double* row_means,
+                              const double* dense, uint32_t width, double* out);
 
 /* Omega's rows as the device PCA draws them (pca.rs:936-950, omega_row: SplitMix64
  * seeded from (seed, cells[r]), values (x >> 11) 2^-52 - 1), n x width f64 row-major;

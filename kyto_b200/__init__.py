@@ -44,7 +44,7 @@ EXPORTS = (
     "kg_knn_batch", "kg_knn_learned",
     "kg_learned_layout", "kg_learned_gradients", "kg_diag_kernel_launches", "kg_connectivities",
     "kg_pca_run_stats", "kg_diag_omega", "kg_diag_pool_usage", "kg_diag_fail_allocations",
-    "kg_set_wait_limit",
+    "kg_set_wait_limit", "kg_diag_spmm", "kg_pca_push_block_async",
 )
 
 
@@ -178,6 +178,7 @@ def library() -> ctypes.CDLL:
             "kg_hvg_seurat": [P, P, P, U64, U32, ctypes.c_int64, P, P, P, P],
             "kg_pca_begin": [P, ctypes.POINTER(_PcaParams), ctypes.POINTER(P)],
             "kg_pca_push_block": [P, P, P, P, ctypes.c_int, U64, P],
+            "kg_pca_push_block_async": [P, P, P, P, ctypes.c_int, U64, P],
             "kg_pca_run": [P],
             "kg_pca_results": [P, P, P, P, P, P],
             "kg_pca_info": [P, P, P, P],
@@ -197,6 +198,7 @@ def library() -> ctypes.CDLL:
             "kg_diag_omega": [P, U64, P, U64, U32, P],
             "kg_diag_pool_usage": [ctypes.c_int, P, P, P, I32],
             "kg_diag_fail_allocations": [U64],
+            "kg_diag_spmm": [P, P, P, P, U64, U32, I32, I32, P, P, U32, P],
         }
         for name, args in sig.items():
             fn = getattr(lib, name)
@@ -296,6 +298,30 @@ def _u64(a):
 
 def _u32(a):
     return np.ascontiguousarray(a, dtype=np.uint32) if isinstance(a, np.ndarray) else a
+
+
+def product(indptr, indices, values, n_cols: int, dense=None, transposed: bool = False,
+            value_mode: int = 0, row_means=None, width: int | None = None,
+            ctx: Context | None = None) -> np.ndarray:
+    """One of the PCA's tensor-core products (kg_diag_spmm): S D as f64, rows x width."""
+    ctx = ctx or default_context()
+    indptr = _u64(indptr)
+    n_rows = len(indptr) - 1
+    rows = n_cols if transposed else n_rows
+    K = n_rows if transposed else n_cols
+    if dense is not None:
+        dense = np.asfortranarray(dense, dtype=np.float64)
+        assert dense.shape[0] == K
+        width = dense.shape[1]
+    width = int(width or 1)
+    out = np.empty((width, rows))  # column-major rows x width
+    means = None if row_means is None else np.ascontiguousarray(row_means, dtype=np.float64)
+    _check(library().kg_diag_spmm(
+        ctx.handle, _ptr(indptr), _ptr(_u32(indices)),
+        _ptr(np.ascontiguousarray(values, dtype=np.float32)), n_rows, int(n_cols),
+        int(bool(transposed)), int(value_mode), _ptr(means),
+        None if dense is None else dense.ctypes.data_as(ctypes.c_void_p), width, _ptr(out)))
+    return out.T
 
 
 def omega(seed: int, cells, width: int, ctx: Context | None = None) -> np.ndarray:
@@ -413,15 +439,24 @@ class PcaSession:
         self.n_components = int(n_components)
         self.n_genes = int(n_genes)
 
-    def push(self, indptr, indices, values, cells=None) -> None:
+    def push(self, indptr, indices, values, cells=None, wait: bool = True) -> None:
+        """Push the next block. ``wait=False`` queues its copies and returns at once
+        (kg_pca_push_block_async): the arrays must stay alive and unchanged until
+        ``run()`` returns (the session keeps references to them until then)."""
         indptr, indices = _u64(indptr), _u32(indices)
         n_rows = (len(indptr) if isinstance(indptr, np.ndarray) else indptr.shape[0]) - 1
-        _check(library().kg_pca_push_block(
-            self._h, _ptr(indptr), _ptr(indices), _ptr(values), _dtype_code(values), n_rows,
-            _ptr(_u64(cells) if cells is not None else None)))
+        fn = library().kg_pca_push_block if wait else library().kg_pca_push_block_async
+        cells = _u64(cells) if cells is not None else None
+        _check(fn(self._h, _ptr(indptr), _ptr(indices), _ptr(values), _dtype_code(values),
+                  n_rows, _ptr(cells)))
+        if not wait:
+            self._held = getattr(self, "_held", []) + [indptr, indices, values, cells]
 
     def run(self) -> None:
-        _check(library().kg_pca_run(self._h))
+        try:
+            _check(library().kg_pca_run(self._h))
+        finally:
+            self._held = []
 
     def info(self) -> tuple[int, int, int]:
         n, g, p = ctypes.c_uint64(), ctypes.c_uint32(), ctypes.c_uint32()

@@ -8,6 +8,7 @@
 // products, the blocks) are f64 column-major for cuBLAS/cuSOLVER; per-cell matrices
 // (Omega, W, the embedding rows) are row-major n x w.
 #include <cub/device/device_scan.cuh>
+#include <cuda_fp16.h>
 
 #include <cstdlib>
 #include <string>
@@ -49,17 +50,26 @@ constexpr double kDropTolerance = 1e-10;  // pca_dense.rs:30
 // Kept entries per row (genes mapped into the PCA's set), one warp per row, and the
 // row's normalize divisor (kg_maps.cuh: every 8-lane group of the warp sums the row in
 // kyto's lane order and gets the same divisor) when divisor is not NULL.
+// A gene index at or past the stream's genes is never kept and sets *bad (an
+// asynchronous push checks the indices only when the run starts).
 template <class V>
 __global__ void count_kept_kernel(const uint64_t* indptr, const uint32_t* idx, const V* values,
-                                  uint64_t n_rows, const uint32_t* gene_map, float target32,
-                                  const int* inexact, uint64_t* kept, float* divisor) {
+                                  uint64_t n_rows, const uint32_t* gene_map, uint32_t n_genes,
+                                  float target32, const int* inexact, uint64_t* kept,
+                                  float* divisor, unsigned int* bad) {
   uint64_t row = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   unsigned lane = threadIdx.x & 31u;
   if (row >= n_rows) return;  // whole warps leave together
   uint64_t s = indptr[row], e = indptr[row + 1];
   uint64_t count = 0;
-  for (uint64_t i = s + lane; i < e; i += 32)
-    count += (gene_map == nullptr || gene_map[idx[i]] != kNoGene);
+  for (uint64_t i = s + lane; i < e; i += 32) {
+    const uint32_t gi = idx[i];
+    if (gi >= n_genes) {
+      atomicOr(bad, 1u);
+      continue;
+    }
+    count += (gene_map == nullptr || gene_map[gi] != kNoGene);
+  }
   for (int o = 16; o; o >>= 1) count += __shfl_down_sync(0xFFFFFFFFu, count, o);
   if (lane == 0) kept[row] = count;
   if (divisor) {
@@ -74,8 +84,8 @@ __global__ void count_kept_kernel(const uint64_t* indptr, const uint32_t* idx, c
 template <class V>
 __global__ void write_kept_kernel(const uint64_t* indptr, const uint32_t* idx, const V* values,
                                   const float* divisor, int do_log1p, uint64_t n_rows,
-                                  const uint32_t* gene_map, const uint64_t* out_ptr,
-                                  uint32_t* col, float* val) {
+                                  const uint32_t* gene_map, uint32_t n_genes,
+                                  const uint64_t* out_ptr, uint32_t* col, float* val) {
   uint64_t row = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   unsigned lane = threadIdx.x & 31u;
   if (row >= n_rows) return;
@@ -86,7 +96,7 @@ __global__ void write_kept_kernel(const uint64_t* indptr, const uint32_t* idx, c
     uint64_t i = i0 + lane;
     bool in = i < e;
     uint32_t p = kNoGene;
-    if (in) p = gene_map ? gene_map[idx[i]] : idx[i];
+    if (in && idx[i] < n_genes) p = gene_map ? gene_map[idx[i]] : idx[i];
     bool keep = in && p != kNoGene;
     unsigned ballot = __ballot_sync(0xFFFFFFFFu, keep);
     if (keep) {
@@ -115,6 +125,12 @@ __global__ void gather_csc_kernel(const uint32_t* perm, const uint32_t* row_of,
     csc_row[i] = row_of[e];
     csc_val[i] = val[e];
   }
+}
+
+// Cell positions first, first + 1, ... (a block pushed without its cells' positions).
+__global__ void iota64_kernel(uint64_t* out, uint64_t n, uint64_t first) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) out[i] = first + i;
 }
 
 __global__ void add_offset_kernel(uint64_t* p, uint64_t n, uint64_t offset) {
@@ -151,12 +167,13 @@ __global__ void omega_kernel(const uint64_t* cells, uint64_t n, uint32_t width,
   for (uint32_t j = 0; j < width; ++j) row[j] = omega_next(state);
 }
 
-// D^T = [1 ... 1; 0 ...] (row 0 ones over the n cells, everything else zero).
-__global__ void fill_rows_kernel(float* hi, float* lo, uint64_t n, uint64_t ld) {
+// D^T = [1 ... 1; 0 ...] in the dense layout (row 0: ones over the n cells, scale 0; all
+// else zero).
+__global__ void fill_rows_kernel(uint16_t* t, uint64_t n, uint64_t ld) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i >= 64 * ld) return;
-  hi[i] = (i < n) ? 1.0f : 0.0f;
-  lo[i] = 0.0f;
+  const uint64_t k = i % 64, r = (i / 64) * 32 + k;  // row 0's column r (hi parts)
+  t[i] = (i < ld && k < 32 && r < n) ? (uint16_t)0x3C00u : (uint16_t)0;
 }
 
 __global__ void fill_kernel(double* p, uint64_t n, double v) {
@@ -731,49 +748,61 @@ __global__ void gather_unit_columns_kernel(const double* a, uint32_t g, uint32_t
 
 // ------------------------------------------------ tensor-core product support -------
 
-__device__ __forceinline__ float tf32_rna(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
+// A value times 2^scale as the two fp16 parts of the products' dense operand
+// (kg_spmm_tc.cuh): hi = fp16(y), lo = fp16(y - hi).
+__device__ __forceinline__ void split_half(double v, double mul, uint16_t& hi, uint16_t& lo) {
+  const double y = v * mul;
+  const __half h = __double2half(y);
+  hi = __half_as_ushort(h);
+  lo = __half_as_ushort(__double2half(y - (double)__half2float(h)));
 }
 
-// D^T in two tf32 parts from a g x w column-major f64 matrix: t[j][r] for j < 64,
-// r < ld (zero past w columns and g rows).
+// The value the products see for a split value (hi + lo, unscaled).
+__device__ __forceinline__ double joined(uint16_t hi, uint16_t lo, double inv) {
+  return ((double)__half2float(__ushort_as_half(hi)) +
+          (double)__half2float(__ushort_as_half(lo))) * inv;
+}
+
+// D^T in the dense layout (row length ld halves, values times 2^scale) from a g x w
+// column-major f64 matrix: thread per (j, r), r < ld / 2 (zero past w columns and g
+// rows).
 __global__ void split_t_kernel(const double* cm, uint32_t g, uint32_t w, uint64_t ld,
-                               float* t_hi, float* t_lo) {
+                               int scale, uint16_t* t) {
+  const uint64_t half = ld / 2;
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (i >= 64 * ld) return;
-  uint32_t j = (uint32_t)(i / ld);
-  uint64_t r = i % ld;
+  if (i >= 64 * half) return;
+  uint32_t j = (uint32_t)(i / half);
+  uint64_t r = i % half;
   double v = (j < w && r < g) ? cm[(uint64_t)j * g + r] : 0.0;
-  float hi = tf32_rna((float)v);
-  t_hi[i] = hi;
-  t_lo[i] = tf32_rna((float)(v - (double)hi));
+  uint16_t hi, lo;
+  split_half(v, ldexp(1.0, scale), hi, lo);
+  uint16_t* at = t + (uint64_t)j * ld + (r / 32) * 64 + (r % 32);
+  at[0] = hi;
+  at[32] = lo;
 }
 
-// Omega^T in two tf32 parts, 64 x ld (rows past width zero); and each block's Omega
-// column sums (of the parts, f64, a fixed tree) for the centring.
+// Omega^T in the dense layout (values times 2^scale; rows past width zero), and each
+// block's Omega column sums of the split values (as the products see them; f64, a fixed
+// tree) for the centring.
 __global__ void omega_t_kernel(const uint64_t* cells, uint64_t n, uint32_t width,
-                               uint64_t seed, uint64_t ld, float* t_hi, float* t_lo,
+                               uint64_t seed, uint64_t ld, int scale, uint16_t* t,
                                double* block_sums) {
   __shared__ double red[8][64];
   uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   bool live = r < n;
   uint64_t state = live ? omega_state(seed, cells[r]) : 0;
   const unsigned warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const double mul = ldexp(1.0, scale), inv = ldexp(1.0, -scale);
   for (uint32_t j = 0; j < 64; ++j) {
-    float hi = 0.0f, lo = 0.0f;
-    if (live && j < width) {
-      double om = omega_next(state);
-      hi = tf32_rna((float)om);
-      lo = tf32_rna((float)(om - (double)hi));
-    }
-    if (r < ld) {
-      t_hi[(uint64_t)j * ld + r] = hi;
-      t_lo[(uint64_t)j * ld + r] = lo;
+    uint16_t hi = 0, lo = 0;
+    if (live && j < width) split_half(omega_next(state), mul, hi, lo);
+    if (r < ld / 2) {
+      uint16_t* at = t + (uint64_t)j * ld + (r / 32) * 64 + (r % 32);
+      at[0] = hi;
+      at[32] = lo;
     }
     if (j < width) {
-      double sv = (double)hi + (double)lo;
+      double sv = joined(hi, lo, inv);
       for (int o = 16; o; o >>= 1) sv += __shfl_xor_sync(0xFFFFFFFFu, sv, o);
       if (lane == 0) red[warp][j] = sv;
     }
@@ -912,7 +941,8 @@ struct ProductClock {
 
 struct TcHeld {
   static constexpr uint64_t kSegChunks = 512;  // K-chunks (16,384 cells) per X^T work item
-  uint64_t n = 0, g = 0, n_ld = 0, g_ld = 0, nnz = 0;
+  static constexpr int kUnitScale = 14;        // |Omega|, |Q|, |V| <= 1: parts times 2^14
+  uint64_t n = 0, g = 0, nnz = 0;
   ProductClock clock;
   // A product's algorithmic bytes, S (rows x K, nnz values) . D (K x l) read once and
   // the rows x l result written once: 8 nnz + 4 (n + 1) + 4 g l + 4 n l (f32 values and
@@ -921,8 +951,11 @@ struct TcHeld {
     return 8.0 * (double)nnz + 4.0 * (double)(n + 1) + 4.0 * (double)g * l + 4.0 * (double)n * l;
   }
   Blocked bx, bxt;
-  DeviceBuffer<float> dt_hi, dt_lo;    // 64 x n_ld: Omega^T or W^T
-  DeviceBuffer<float> qt_hi, qt_lo;    // 64 x g_ld: Q^T or V^T
+  DeviceBuffer<uint16_t> dt;   // 64 x dense_ld(n): Omega^T, the ones row or W^T
+  DeviceBuffer<uint16_t> qt;   // 64 x dense_ld(g): Q^T or V^T
+  int dt_scale = 0;
+  double mean_norm = 0.0;      // |mu| (the gene means), for the bound on W's entries
+  DeviceBuffer<int> error;     // set by a product whose bounded wait ran out
   int sm = 148;
 
   void build(const uint64_t* indptr, const uint32_t* col, const float* val, uint64_t n_rows,
@@ -930,26 +963,37 @@ struct TcHeld {
     n = n_rows;
     g = n_genes;
     this->nnz = nnz;
-    n_ld = (n + 3) & ~3ull;
-    g_ld = (g + 3) & ~3ull;
     sm = sm_count;
-    build_blocked(indptr, col, val, n, g, nnz, false, bx, s);
+    build_blocked(indptr, col, val, n, g, nnz, bx, s);
     trace.mark("blocked X");
     transpose_blocked(bx, bxt, s);
     trace.mark("blocked X^T");
-    dt_hi.alloc(64 * n_ld, s);
-    dt_lo.alloc(64 * n_ld, s);
-    qt_hi.alloc(64 * g_ld, s);
-    qt_lo.alloc(64 * g_ld, s);
+    dt.alloc(64 * dense_ld(n), s);
+    dt.zero();
+    qt.alloc(64 * dense_ld(g), s);
+    qt.zero();
+    error.alloc(1, s);
+    error.zero();
+  }
+
+  // Whether a product gave up waiting (reads the flag: synchronises the stream).
+  void check(cudaStream_t s) {
+    if (!error.ptr) return;
+    int h = 0;
+    KG_CUDA(cudaMemcpyAsync(&h, error.ptr, 4, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+    if (h) fail(KG_ERR_TIMEOUT, "a tensor-core product gave up waiting on its pipeline");
   }
 
   // out (g x width column-major) = X^T Omega; omega_sums (width).
   void sketch(const uint64_t* cells, uint32_t width, uint64_t seed, double* out,
               double* omega_sums, cudaStream_t s) {
-    unsigned nb = blocks_for(n_ld, 256);
+    const uint64_t ld = dense_ld(n);
+    unsigned nb = blocks_for(ld / 2, 256);
     DeviceBuffer<double> bsum((uint64_t)nb * 64, s);
-    omega_t_kernel<<<nb, 256, 0, s>>>(cells, n, width, seed, n_ld, dt_hi.ptr, dt_lo.ptr, bsum.ptr);
+    omega_t_kernel<<<nb, 256, 0, s>>>(cells, n, width, seed, ld, kUnitScale, dt.ptr, bsum.ptr);
     KG_LAUNCH_CHECK();
+    dt_scale = kUnitScale;
     sum_blocks_kernel<<<1, 1024, 0, s>>>(bsum.ptr, nb, width, omega_sums);
     KG_LAUNCH_CHECK();
     transposed(width, out, s);
@@ -957,8 +1001,10 @@ struct TcHeld {
 
   // D^T = a row of ones (the stored values' gene sums, counts, squares).
   void ones_column() {
-    fill_rows_kernel<<<blocks_for(64 * n_ld, 256), 256, 0, dt_hi.stream>>>(dt_hi.ptr, dt_lo.ptr, n, n_ld);
+    const uint64_t ld = dense_ld(n);
+    fill_rows_kernel<<<blocks_for(64 * ld, 256), 256, 0, dt.stream>>>(dt.ptr, n, ld);
     KG_LAUNCH_CHECK();
+    dt_scale = 0;
   }
 
   // out (g x w column-major) = X^T W with W^T in dt (the stored values mapped by
@@ -972,12 +1018,13 @@ struct TcHeld {
     a.row_means = row_means;
     a.s = &bxt;
     a.seg_chunks = kSegChunks;
-    a.dt_hi = dt_hi.ptr;
-    a.dt_lo = dt_lo.ptr;
-    a.ld_t = n_ld;
+    a.dt = dt.ptr;
+    a.ld_t = dense_ld(n);
+    a.dt_scale = dt_scale;
     a.out.mode = kOutPartial;
     a.out.partial = partial.ptr;
     a.sm_count = sm;
+    a.error = error.ptr;
     clock.begin(s, product_bytes(w));
     spmm_tc(a, s);
     clock.end();
@@ -986,37 +1033,42 @@ struct TcHeld {
     KG_LAUNCH_CHECK();
   }
 
-  // Rows of X M - offsets for M = m (g x w column-major): as W^T into dt (with the
-  // column sums into wsums) or as f32 rows into rows_f32.
+  // Rows of X M - offsets for M = m (g x w column-major, orthonormal columns): as W^T into
+  // dt (with the column sums into wsums) or as f32 rows into rows_f32.
   void rows(const double* m, uint32_t w, const double* offsets, double* wsums, float* rows_f32,
             cudaStream_t s) {
-    split_t_kernel<<<blocks_for(64 * g_ld, 256), 256, 0, s>>>(m, (uint32_t)g, w, g_ld,
-                                                              qt_hi.ptr, qt_lo.ptr);
+    const uint64_t ldq = dense_ld(g);
+    split_t_kernel<<<blocks_for(64 * ldq / 2, 256), 256, 0, s>>>(m, (uint32_t)g, w, ldq,
+                                                                 kUnitScale, qt.ptr);
     KG_LAUNCH_CHECK();
     uint64_t tiles = (n + 127) / 128;
     DeviceBuffer<double> colsum;
     SpmmArgs a;
     a.s = &bx;
     a.seg_chunks = bx.n_chunks;
-    a.dt_hi = qt_hi.ptr;
-    a.dt_lo = qt_lo.ptr;
-    a.ld_t = g_ld;
+    a.dt = qt.ptr;
+    a.ld_t = ldq;
+    a.dt_scale = kUnitScale;
     a.out.mode = kOutRows;
     a.out.width = w;
     a.out.offsets = offsets;
     if (wsums) {
+      // |w_ij| = |(x_i - mu) . q_j| <= |x_i| + |mu| (unit columns q_j), with room to
+      // spare for their rounding: the parts of W^T stay below 2^15.
       colsum.alloc(tiles * 64, s);
-      a.out.t_hi = dt_hi.ptr;
-      a.out.t_lo = dt_lo.ptr;
-      a.out.ld_t = n_ld;
+      a.out.t = dt.ptr;
+      a.out.ld_t = dense_ld(n);
+      a.out.t_scale = part_scale(2.0 * (bx.max_row_norm + mean_norm));
       a.out.colsum_partial = colsum.ptr;
     }
     a.out.rows_f32 = rows_f32;
     a.sm_count = sm;
+    a.error = error.ptr;
     clock.begin(s, product_bytes(w));
     spmm_tc(a, s);
     clock.end();
     if (wsums) {
+      dt_scale = a.out.t_scale;
       sum_blocks_kernel<<<1, 1024, 0, s>>>(colsum.ptr, tiles, w, wsums);
       KG_LAUNCH_CHECK();
     }
@@ -1043,6 +1095,8 @@ struct kg_pca {
   DeviceBuffer<float> val;
   DeviceBuffer<uint64_t> cells;
   uint64_t n_cells = 0, nnz = 0, next_cell = 0;
+  // Set by the pack kernels when a pushed gene index is out of range (checked at run).
+  DeviceBuffer<unsigned int> bad_index;
   // Results.
   bool ran = false;
   uint32_t passes_run = 0;
@@ -1089,29 +1143,40 @@ struct kg_pca {
   }
 
   void push(const uint64_t* h_indptr, const uint32_t* h_idx, const void* h_values,
-            kg_dtype dtype, uint64_t n_rows, const uint64_t* h_cells);
+            kg_dtype dtype, uint64_t n_rows, const uint64_t* h_cells, bool async);
   void run();
 };
 
 void kg_pca::push(const uint64_t* in_indptr, const uint32_t* in_idx, const void* in_values,
-                  kg_dtype dtype, uint64_t n_rows, const uint64_t* in_cells) {
+                  kg_dtype dtype, uint64_t n_rows, const uint64_t* in_cells, bool async) {
   if (ran) fail(KG_ERR_STATE, "kg_pca_push_block after kg_pca_run");
   if (dtype != KG_U32 && dtype != KG_F32) fail(KG_ERR_INVALID, "unknown dtype");
   if (n_rows == 0) return;
   cudaStream_t s = stream;
   Trace trace(s, "pca_push");
-  DeviceBuffer<uint64_t> hp, hc;
-  const uint64_t* d_indptr = device_view(in_indptr, n_rows + 1, hp, s);
+  // The block's first and last offsets: read in place from host memory; from device
+  // memory through one copy.
   uint64_t ends[2];
-  KG_CUDA(cudaMemcpyAsync(&ends[0], d_indptr, 8, cudaMemcpyDefault, s));
-  KG_CUDA(cudaMemcpyAsync(&ends[1], d_indptr + n_rows, 8, cudaMemcpyDefault, s));
-  KG_CUDA(cudaStreamSynchronize(s));
+  DeviceBuffer<uint64_t> hp, hc;
+  if (is_device_pointer(in_indptr)) {
+    KG_CUDA(cudaMemcpyAsync(&ends[0], in_indptr, 8, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaMemcpyAsync(&ends[1], in_indptr + n_rows, 8, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+  } else {
+    ends[0] = in_indptr[0];
+    ends[1] = in_indptr[n_rows];
+  }
   if (ends[0] != 0) fail(KG_ERR_INVALID, "a block's indptr must start at 0");
+  const uint64_t* d_indptr = device_view(in_indptr, n_rows + 1, hp, s);
   uint64_t bnnz = ends[1];
   DeviceBuffer<uint32_t> hi, hv;
   const uint32_t* d_idx = device_view(in_idx, bnnz, hi, s);
   const void* d_values = device_view((const uint32_t*)in_values, bnnz, hv, s);
-  check_indices(d_idx, bnnz, stream_genes, s);
+  if (!bad_index.ptr) {
+    bad_index.alloc(1, s);
+    bad_index.zero();
+  }
+  if (!async) check_indices(d_idx, bnnz, stream_genes, s);
   trace.mark("checks");
   // Kept entries per row and the rows' normalize divisors, then the kept entries'
   // offsets after the held entries; the maps run inside write_kept.
@@ -1125,20 +1190,24 @@ void kg_pca::push(const uint64_t* in_indptr, const uint32_t* in_idx, const void*
   unsigned threads = 256;
   if (dtype == KG_U32)
     count_kept_kernel<uint32_t><<<blocks_for(n_rows * 32, threads), threads, 0, s>>>(
-        d_indptr, d_idx, (const uint32_t*)d_values, n_rows, gene_map.ptr, (float)target_sum,
-        inexact.ptr, kept.ptr, divisor.ptr);
+        d_indptr, d_idx, (const uint32_t*)d_values, n_rows, gene_map.ptr, stream_genes,
+        (float)target_sum, inexact.ptr, kept.ptr, divisor.ptr, bad_index.ptr);
   else
     count_kept_kernel<float><<<blocks_for(n_rows * 32, threads), threads, 0, s>>>(
-        d_indptr, d_idx, (const float*)d_values, n_rows, gene_map.ptr, (float)target_sum,
-        inexact.ptr, kept.ptr, divisor.ptr);
+        d_indptr, d_idx, (const float*)d_values, n_rows, gene_map.ptr, stream_genes,
+        (float)target_sum, inexact.ptr, kept.ptr, divisor.ptr, bad_index.ptr);
   KG_LAUNCH_CHECK();
   size_t temp = 0;
   KG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, kept.ptr, kept.ptr, n_rows + 1, s));
   DeviceBuffer<unsigned char> scratch(temp, s);
   KG_CUDA(cub::DeviceScan::ExclusiveSum(scratch.ptr, temp, kept.ptr, kept.ptr, n_rows + 1, s));
-  uint64_t added = 0;
-  KG_CUDA(cudaMemcpyAsync(&added, kept.ptr + n_rows, 8, cudaMemcpyDeviceToHost, s));
-  KG_CUDA(cudaStreamSynchronize(s));
+  // Kept entries: every entry when every gene is kept (an out-of-range index makes the
+  // run fail before the held input is used), else counted on the device.
+  uint64_t added = bnnz;
+  if (gene_map.ptr) {
+    KG_CUDA(cudaMemcpyAsync(&added, kept.ptr + n_rows, 8, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+  }
   add_offset_kernel<<<blocks_for(n_rows + 1, 256), 256, 0, s>>>(kept.ptr, n_rows + 1, nnz);
   KG_LAUNCH_CHECK();
   trace.mark("kept counts");
@@ -1152,29 +1221,34 @@ void kg_pca::push(const uint64_t* in_indptr, const uint32_t* in_idx, const void*
   if (dtype == KG_U32)
     write_kept_kernel<uint32_t><<<blocks_for(n_rows * 32, threads), threads, 0, s>>>(
         d_indptr, d_idx, (const uint32_t*)d_values, divisor.ptr, log1p, n_rows, gene_map.ptr,
-        kept.ptr, col.ptr, val.ptr);
+        stream_genes, kept.ptr, col.ptr, val.ptr);
   else
     write_kept_kernel<float><<<blocks_for(n_rows * 32, threads), threads, 0, s>>>(
         d_indptr, d_idx, (const float*)d_values, divisor.ptr, log1p, n_rows, gene_map.ptr,
-        kept.ptr, col.ptr, val.ptr);
+        stream_genes, kept.ptr, col.ptr, val.ptr);
   KG_LAUNCH_CHECK();
   if (in_cells) {
     const uint64_t* d_cells = device_view(in_cells, n_rows, hc, s);
     KG_CUDA(cudaMemcpyAsync(cells.ptr + n_cells, d_cells, n_rows * 8, cudaMemcpyDeviceToDevice, s));
-    std::vector<uint64_t> last(1);
-    KG_CUDA(cudaMemcpyAsync(last.data(), d_cells + n_rows - 1, 8, cudaMemcpyDefault, s));
-    KG_CUDA(cudaStreamSynchronize(s));
-    next_cell = last[0] + 1;
+    uint64_t last = 0;
+    if (is_device_pointer(in_cells)) {
+      KG_CUDA(cudaMemcpyAsync(&last, in_cells + n_rows - 1, 8, cudaMemcpyDeviceToHost, s));
+      KG_CUDA(cudaStreamSynchronize(s));
+    } else {
+      last = in_cells[n_rows - 1];
+    }
+    next_cell = last + 1;
   } else {
-    std::vector<uint64_t> pos(n_rows);
-    for (uint64_t r = 0; r < n_rows; ++r) pos[r] = next_cell + r;
-    KG_CUDA(cudaMemcpyAsync(cells.ptr + n_cells, pos.data(), n_rows * 8, cudaMemcpyHostToDevice, s));
+    iota64_kernel<<<blocks_for(n_rows, 256), 256, 0, s>>>(cells.ptr + n_cells, n_rows, next_cell);
+    KG_LAUNCH_CHECK();
     next_cell += n_rows;
-    KG_CUDA(cudaStreamSynchronize(s));
   }
   n_cells += n_rows;
   nnz += added;
-  KG_CUDA(cudaStreamSynchronize(s));
+  // A synchronous push returns once the block is on the device (the caller may then
+  // reuse its host arrays); an asynchronous one leaves the copies and kernels queued on
+  // the session's stream (its host arrays stay in use until kg_pca_run returns).
+  if (!async) KG_CUDA(cudaStreamSynchronize(s));
   trace.mark("held block");
 }
 
@@ -1298,6 +1372,14 @@ void kg_pca::run() {
   if (ran) fail(KG_ERR_STATE, "kg_pca_run called twice");
   kg_ctx* c = ctx;
   cudaStream_t s = stream;
+  if (bad_index.ptr) {
+    unsigned int bad = 0;
+    KG_CUDA(cudaMemcpyAsync(&bad, bad_index.ptr, 4, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+    if (bad)
+      fail(KG_ERR_INVALID, "a pushed block holds a gene index at or past its " +
+                               std::to_string(stream_genes) + " genes");
+  }
   const uint64_t n = n_cells;
   const uint32_t g = n_genes;
   if (n < 2)
@@ -1314,11 +1396,12 @@ void kg_pca::run() {
   c->done = 0;
 
   Trace trace(s, "pca");
-  // The products run on the tensor cores (tf32 parts, f32 sums of at most 512 terms
-  // flushed into f64) when the genes fit 16-bit positions, the block one 64-column tile,
-  // and no gene's mean dwarfs its spread (the rows are centred after the product, so
-  // the products' relative error is scaled by |mean| / sd: at most 64, about 2^-15);
-  // else on the SIMT pipes in f64 (kyto's arithmetic, any data).
+  // The products run on the tensor cores (fp16 hi/lo parts of both operands, about 2^-22
+  // each; f32 sums of at most 512 terms flushed into f64) when the genes fit 16-bit
+  // positions, the block one 64-column tile, the values span at most 2^30, and no gene's
+  // mean dwarfs its spread (the rows are centred after the product, so the products'
+  // relative error is scaled by |mean| / sd: at most 64, about 2^-16); else on the SIMT
+  // pipes in f64 (kyto's arithmetic, any data).
   const char* pchoice = std::getenv("KYTO_GPU_PCA_PRODUCTS");
   bool tc = g <= 65535 && l <= 64 && k <= 64 && !(pchoice && std::string(pchoice) == "simt");
   means.alloc(g, s);
@@ -1351,6 +1434,10 @@ void kg_pca::run() {
     KG_CUDA(cudaMemcpyAsync(h_cnt.data(), cnt.ptr, g * 8ull, cudaMemcpyDeviceToHost, s));
     KG_CUDA(cudaStreamSynchronize(s));
     check_means();
+    th.check(s);
+    double mn = 0.0;
+    for (uint32_t i = 0; i < g; ++i) mn += h_means[i] * h_means[i];
+    th.mean_norm = std::sqrt(mn);
     colptr[0] = 0;
     for (uint32_t i = 0; i < g; ++i) colptr[i + 1] = colptr[i] + (uint64_t)std::llround(h_cnt[i]);
     double worst_ratio = 0.0;
@@ -1359,8 +1446,14 @@ void kg_pca::run() {
       double var = (squares[i] + (double)(n - stored) * h_means[i] * h_means[i]) / (double)n;
       if (var > 0.0) worst_ratio = std::max(worst_ratio, h_means[i] * h_means[i] / var);
     }
-    if (worst_ratio > 4096.0) {
+    // The values' fp16 parts keep 22 bits of each value down to 2^-18 of the largest and
+    // an absolute 2^-39 of it below: data spanning more than 2^30, or scaled out of f32's
+    // comfortable range, goes to the f64 path.
+    const bool range_ok = th.bx.min_abs == 0.0 || th.bx.max_abs / th.bx.min_abs <= 0x1p30;
+    const bool scale_ok = th.bx.scale >= -100 && th.bx.scale <= 100;
+    if (worst_ratio > 4096.0 || !range_ok || !scale_ok) {
       tc = false;
+      th.clock.release();
       th = TcHeld();
     }
     trace.mark("gene statistics");
@@ -1553,6 +1646,7 @@ void kg_pca::run() {
       loadings64.ptr, g, k, set_genes.ptr, stream_genes, loadings.ptr);
   KG_LAUNCH_CHECK();
   wait_stream(c, s);
+  if (tc) th.check(s);
   th.clock.collect(product_launches, product_ms, product_bytes);
   ++passes_run;
   c->done += n;
@@ -1701,7 +1795,7 @@ kg_status kg_pca_knn_batch(kg_ctx* ctx, const kg_pca_params* params, uint32_t n_
             check_cancel(ctx);
             std::unique_ptr<kg_pca> p(make_session(ctx, params));
             const kg_batch_sample& b = samples[i];
-            p->push(b.indptr, b.indices, b.values, b.dtype, b.n_rows, nullptr);
+            p->push(b.indptr, b.indices, b.values, b.dtype, b.n_rows, nullptr, false);
             p->run();
             KG_CUDA(cudaMemcpyAsync(emb_all.ptr + first[i] * kc, p->embedding.ptr,
                                     b.n_rows * kc * 4ull, cudaMemcpyDeviceToDevice, p->stream));
@@ -1751,7 +1845,18 @@ kg_status kg_pca_push_block(kg_pca* pca, const uint64_t* indptr, const uint32_t*
     if (!pca || (n_rows && (!indptr || !indices || !values)))
       fail(KG_ERR_INVALID, "kg_pca_push_block: NULL argument");
     use_device(pca->ctx);
-    pca->push(indptr, indices, values, dtype, n_rows, cells);
+    pca->push(indptr, indices, values, dtype, n_rows, cells, false);
+  });
+}
+
+kg_status kg_pca_push_block_async(kg_pca* pca, const uint64_t* indptr, const uint32_t* indices,
+                                  const void* values, kg_dtype dtype, uint64_t n_rows,
+                                  const uint64_t* cells) {
+  return guarded([&] {
+    if (!pca || (n_rows && (!indptr || !indices || !values)))
+      fail(KG_ERR_INVALID, "kg_pca_push_block_async: NULL argument");
+    use_device(pca->ctx);
+    pca->push(indptr, indices, values, dtype, n_rows, cells, true);
   });
 }
 
@@ -1775,6 +1880,90 @@ kg_status kg_pca_run_stats(const kg_pca* pca, kg_pca_stats* out) {
     out->product_ms = pca->product_ms;
     out->product_bytes = pca->product_bytes;
     out->run_ms = pca->run_ms;
+  });
+}
+
+kg_status kg_diag_spmm(kg_ctx* ctx, const uint64_t* indptr, const uint32_t* indices,
+                       const float* values, uint64_t n_rows, uint32_t n_cols,
+                       int32_t transposed, int32_t value_mode, const double* row_means,
+                       const double* dense, uint32_t width, double* out) {
+  return guarded([&] {
+    if (!ctx || !indptr || !out || (!dense && value_mode == kValuePlain))
+      fail(KG_ERR_INVALID, "kg_diag_spmm: NULL argument");
+    if (width == 0 || width > 64) fail(KG_ERR_INVALID, "kg_diag_spmm: width must be 1..64");
+    if (value_mode < kValuePlain || value_mode > kValueOne)
+      fail(KG_ERR_INVALID, "kg_diag_spmm: unknown value mode");
+    if (n_cols > 65535) fail(KG_ERR_INVALID, "kg_diag_spmm: at most 65,535 columns");
+    use_device(ctx);
+    cudaStream_t s = ctx->stream;
+    DeviceBuffer<uint64_t> hp;
+    const uint64_t* d_ptr = device_view(indptr, n_rows + 1, hp, s);
+    uint64_t nnz = 0;
+    KG_CUDA(cudaMemcpyAsync(&nnz, d_ptr + n_rows, 8, cudaMemcpyDefault, s));
+    KG_CUDA(cudaStreamSynchronize(s));
+    DeviceBuffer<uint32_t> hi_idx;
+    DeviceBuffer<float> hv;
+    const uint32_t* d_idx = device_view(indices, nnz, hi_idx, s);
+    const float* d_val = device_view(values, nnz, hv, s);
+    Blocked bx, bxt;
+    build_blocked(d_ptr, d_idx, d_val, n_rows, n_cols, nnz, bx, s);
+    const Blocked* sp = &bx;
+    if (transposed) {
+      transpose_blocked(bx, bxt, s);
+      sp = &bxt;
+    }
+    const uint64_t rows = sp->rows, K = sp->K, ld = dense_ld(K);
+    DeviceBuffer<double> hd;
+    int dscale = 0;
+    DeviceBuffer<uint16_t> dt(64 * ld, s);
+    if (value_mode == kValuePlain) {
+      std::vector<double> h((size_t)K * width);
+      KG_CUDA(cudaMemcpyAsync(h.data(), dense, h.size() * 8, cudaMemcpyDefault, s));
+      KG_CUDA(cudaStreamSynchronize(s));
+      double mx = 0.0;
+      for (double v : h) mx = std::max(mx, std::fabs(v));
+      dscale = part_scale(mx);
+      hd.alloc(h.size(), s);
+      KG_CUDA(cudaMemcpyAsync(hd.ptr, h.data(), h.size() * 8, cudaMemcpyHostToDevice, s));
+      split_t_kernel<<<blocks_for(64 * ld / 2, 256), 256, 0, s>>>(hd.ptr, (uint32_t)K, width, ld,
+                                                                  dscale, dt.ptr);
+      KG_LAUNCH_CHECK();
+    } else {
+      fill_rows_kernel<<<blocks_for(64 * ld, 256), 256, 0, s>>>(dt.ptr, K, ld);
+      KG_LAUNCH_CHECK();
+    }
+    DeviceBuffer<double> hm;
+    const double* d_means = nullptr;
+    if (value_mode == kValueCentredSquare) {
+      if (!row_means) fail(KG_ERR_INVALID, "kg_diag_spmm: centred squares need row_means");
+      d_means = device_view(row_means, rows, hm, s);
+    }
+    constexpr uint64_t kSeg = 512;
+    const uint64_t segs = (sp->n_chunks + kSeg - 1) / kSeg;
+    DeviceBuffer<double> partial(std::max<uint64_t>(segs, 1) * rows * 64, s), res(rows * width, s);
+    DeviceBuffer<int> err(1, s);
+    err.zero();
+    SpmmArgs a;
+    a.s = sp;
+    a.value_mode = value_mode;
+    a.row_means = d_means;
+    a.seg_chunks = kSeg;
+    a.dt = dt.ptr;
+    a.ld_t = ld;
+    a.dt_scale = dscale;
+    a.out.mode = kOutPartial;
+    a.out.partial = partial.ptr;
+    a.sm_count = ctx->sm_count;
+    a.error = err.ptr;
+    spmm_tc(a, s);
+    reduce_segments_kernel<<<blocks_for(rows * width, 256), 256, 0, s>>>(
+        partial.ptr, (uint32_t)segs, (uint32_t)rows, width, res.ptr);
+    KG_LAUNCH_CHECK();
+    KG_CUDA(cudaMemcpyAsync(out, res.ptr, rows * width * 8, cudaMemcpyDefault, s));
+    int h_err = 0;
+    KG_CUDA(cudaMemcpyAsync(&h_err, err.ptr, 4, cudaMemcpyDeviceToHost, s));
+    wait_stream(ctx, s);
+    if (h_err) fail(KG_ERR_TIMEOUT, "the tensor-core product gave up waiting on its pipeline");
   });
 }
 

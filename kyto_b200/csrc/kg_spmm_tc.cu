@@ -1,32 +1,35 @@
 // The PCA's sparse x dense products on the 5th-generation tensor cores.
 //
-//   C (rows x 64) = S (rows x K, sparse, f32 values) . D (K x 64)
+//   C (rows x 64) = S (rows x K, sparse) . D (K x 64)
 //
 // S is the held input X (rows = cells, K = genes) for X Q and the embedding pass, or X^T
 // (rows = genes, K = cells) for X^T W, the sketch and the gene statistics; both are kept
-// in the bitmask block layout of kg_spmm_tc.cuh (128 rows x 32 columns per block). D
-// comes as D^T (64 x K) in two tf32 parts (hi + lo), K-major f32. Each 128 x 32 block of
-// S is expanded straight into tensor memory (one thread per row: its mask word and
-// values become the row's 32 hi and 32 lo tf32 parts, stored into its TMEM lane) and
-// multiplied by three TF32 MMAs that read A from TMEM and D^T from shared memory
-// (hi.hi + hi.lo + lo.hi: the f32 operands to about 2^-21), accumulated in TMEM over at
-// most kFlushChunks chunks and then added into f64 registers (no f32 sum runs over more
-// than 512 terms). Shared memory carries only the loads (D^T tiles and blocks), so the
-// MMAs' operand reads do not compete with the expansion for it.
+// in the blocked layout of kg_spmm_tc.cuh (128 rows x 32 columns a block, column masks,
+// values as fp16 hi/lo pairs of the scaled value). D comes as D^T in the same two fp16
+// parts (the dense layout of kg_spmm_tc.cuh). Each 128 x 32 block of S is expanded
+// straight into tensor memory (one thread per row: for each column the warp reads
+// consecutive value words, conflict-free) as a 128 x 32 hi tile and a lo tile, and
+// multiplied by three kind::f16 MMAs per 16 K that read A from TMEM and D^T from shared
+// memory (hi.hi + hi.lo + lo.hi: both operands to about 2^-22, as three tf32 products
+// give, at twice their rate), accumulated in TMEM over at most kFlushChunks chunks and
+// then added into f64 registers (no f32 sum runs over more than 512 terms); the scales
+// come off in f64 at the end (powers of two, exact).
 //
 // Per CTA (persistent, 320 threads) and per K-chunk of a work item (tile, K segment):
-//   warp 8      loads: the chunk's D^T tiles (64 x 32, two parts, TMA) and the block (one
-//               bulk copy) into one of kLoadStages stages; the next 32 blocks are
-//               prefetched into L2 ahead of their copies;
-//   warps 0-3   expand: thread r writes row r of the chunk's A tile (hi and lo parts)
-//               into TMEM lane r of one of two A buffers;
-//   warp 9      MMA: 12 tcgen05.mma (kind::tf32, A from TMEM, M=128 N=64 K=8) into one
-//               of two TMEM accumulators;
+//   warp 8      loads: the chunk's D^T tile (64 x (32 hi + 32 lo) fp16, one TMA box) and
+//               the block (one bulk copy) into one of kLoadStages stages; the next 32
+//               blocks are prefetched into L2 ahead of their copies;
+//   warps 0-3   expand: lane l of warp q writes row 32 q + l of the chunk's A tiles (16 hi
+//               and 16 lo words, two fp16 a word) into TMEM lane 32 q + l of one of
+//               kABufs A buffers;
+//   warp 9      MMA: 6 tcgen05.mma (kind::f16, A from TMEM, M=128 N=64 K=16) into one of
+//               two TMEM accumulators;
 //   warps 4-7   drain: TMEM -> f64 registers per flush group; at the end of the item the
-//               rows (C - offsets, as tf32 parts of C^T, f32 rows and column sums) or the
-//               segment's f64 partial.
-// HBM sees each block once per product (its mask and values: 512 + 4 nnz bytes) and
+//               rows (C - offsets, as the next product's D^T, f32 rows and column sums) or
+//               the segment's f64 partial.
+// HBM sees each block once per product (its masks and values: 512 + 4 nnz bytes) and
 // D^T about once per pass over it (L2 serves the other tiles of a segment).
+#include <cuda_fp16.h>
 #include <cudaTypedefs.h>
 #include <cub/device/device_scan.cuh>
 
@@ -39,42 +42,54 @@
 #include "kg_internal.cuh"
 #include "kg_sm100.cuh"
 #include "kg_spmm_tc.cuh"
+#include "kg_tma.cuh"
 
 namespace kg {
 
 using namespace sm100;
 
+int part_scale(double bound) {
+  if (!(bound > 0.0) || !std::isfinite(bound)) return 0;
+  int e = 0;
+  std::frexp(bound, &e);  // bound in [2^(e-1), 2^e)
+  return 15 - e;
+}
+
 namespace {
 
 constexpr int kRows = 128;              // rows per tile (M)
-constexpr int kChunk = 32;              // K per chunk (one 128-byte swizzle row of f32)
+constexpr int kChunk = 32;              // K per chunk (a block's columns)
 constexpr int kN = 64;                  // output columns (N)
-constexpr int kLoadStages = 6;
+constexpr int kLoadStages = 8;
 constexpr int kFlushChunks = 16;        // K-chunks summed in f32 before the f64 flush
-constexpr uint32_t kBBytes = kN * 128;  // 8 KB: 64 rows x 32 f32
+constexpr uint32_t kBBytes = kN * 128;  // 8 KB: 64 rows x (32 hi + 32 lo) fp16
 constexpr uint32_t kMaskBytes = kRows * 4;
 constexpr uint32_t kBlockMaxBytes = kMaskBytes + kRows * kChunk * 4;
-constexpr int kProducerWarps = 4;
-constexpr int kEpilogueWarps = 4;
-constexpr int kSpThreads = (kProducerWarps + kEpilogueWarps + 2) * 32;
-// TMEM columns: two 64-column f32 accumulators (0..127), then two A buffers of 64
-// columns (hi parts in the first 32, lo parts in the next 32; lane = row of the tile).
+constexpr int kExpandWarps = 4;
+constexpr int kDrainWarps = 4;
+constexpr int kSpThreads = (kExpandWarps + kDrainWarps + 2) * 32;
+constexpr int kABufs = 4;
+// TMEM columns: two 64-column f32 accumulators (0..127), then kABufs A buffers of 32
+// columns (16 words of hi parts, then 16 of lo parts; lane = row of the tile).
 constexpr uint32_t kTmemColsS = 256;
-constexpr uint32_t kAccCols = 64, kABase = 128, kACols = 64;
+constexpr uint32_t kAccCols = 64, kABase = 128, kACols = 32;
+static_assert(kABase + kABufs * kACols <= kTmemColsS, "TMEM columns");
 
 struct LoadStage {
-  uint8_t b_hi[kBBytes];
-  uint8_t b_lo[kBBytes];
-  uint8_t blk[(kBlockMaxBytes + 1023) / 1024 * 1024];  // mask words, then the values
+  uint8_t b[kBBytes];
+  uint8_t blk[(kBlockMaxBytes + 1023) / 1024 * 1024];  // masks, then the values
 };
 // Swizzled tiles (TMA destinations, MMA operands) start on 1024-byte boundaries.
 static_assert(sizeof(LoadStage) % 1024 == 0, "load stage size");
 
 struct SpSmem {
   LoadStage st[kLoadStages];
-  double colsum[2][kEpilogueWarps][kN];
+  double colsum[2][kDrainWarps][kN];
+  // Per expand warp, per column of the current block: its mask word for the warp's 32
+  // rows and the rank of its first value there.
+  alignas(16) uint2 meta[kExpandWarps][kChunk];
   uint64_t ld_full[kLoadStages], ld_empty[kLoadStages];
-  uint64_t a_full[2], a_empty[2];
+  uint64_t a_full[kABufs], a_empty[kABufs];
   uint64_t cs_ready;
   uint64_t acc_full[2], acc_empty[2];
   uint64_t drained;
@@ -85,12 +100,6 @@ struct SpSmem {
 constexpr size_t kSpSmemBytes = sizeof(SpSmem) + 1024;
 static_assert(kSpSmemBytes <= 227 * 1024, "SpMM shared memory");
 static_assert(offsetof(SpSmem, st) % 1024 == 0, "tile alignment");
-
-__device__ __forceinline__ float tf32_round(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
-}
 
 // A 1D bulk copy global -> shared, counted in bytes on `bar` (16-byte aligned, size a
 // multiple of 16).
@@ -110,6 +119,19 @@ __device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes
                : "memory");
 }
 
+// The two fp16 parts of x (hi = fp16(x), lo = fp16(x - hi)) in one word, hi low.
+__device__ __forceinline__ uint32_t split_pair(float x) {
+  const __half hi = __float2half_rn(x);
+  const __half lo = __float2half_rn(x - __half2float(hi));
+  return (uint32_t)__half_as_ushort(hi) | ((uint32_t)__half_as_ushort(lo) << 16);
+}
+
+// hi + lo of a pair word (exact in f32: 22 significant bits at most).
+__device__ __forceinline__ float pair_value(uint32_t w) {
+  return __half2float(__ushort_as_half((unsigned short)(w & 0xFFFFu))) +
+         __half2float(__ushort_as_half((unsigned short)(w >> 16)));
+}
+
 struct Geometry {
   uint32_t n_tiles, n_chunks, seg_chunks, n_segs;
   __device__ __forceinline__ uint64_t items() const { return (uint64_t)n_tiles * n_segs; }
@@ -127,11 +149,19 @@ struct Geometry {
   }
 };
 
-__global__ void __launch_bounds__(kSpThreads, 1)
-spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
-               const __grid_constant__ CUtensorMap tmap_lo, const uint64_t* __restrict__ off,
-               const uint8_t* __restrict__ data, uint64_t rows, Geometry geo, int value_mode,
-               const double* __restrict__ row_means, SpmmOut out, int* error) {
+// How the expansion maps each stored value: the mode, and for centred squares the factor
+// that undoes S's scale and the one that scales the squares.
+struct ValueMap {
+  int mode;
+  float unscale, sq_scale;
+};
+
+// One CTA per SM: up to 200 registers a thread (the drain warps hold 64 f64 sums).
+__global__ void __maxnreg__(200)
+spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __restrict__ off,
+               const uint8_t* __restrict__ data, uint64_t rows, Geometry geo, ValueMap vmap,
+               const double* __restrict__ row_means, double out_scale, SpmmOut out,
+               int* error) {
   extern __shared__ uint8_t smem_raw[];
   // Aligned to 1024 bytes by an offset into the __shared__ array itself, so the compiler
   // keeps every access in the shared state space (no generic loads and stores).
@@ -144,15 +174,17 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
   if (threadIdx.x == 0) {
     for (int s = 0; s < kLoadStages; ++s) {
       mbar_init(&sm.ld_full[s], 1);
-      mbar_init(&sm.ld_empty[s], kProducerWarps + 1);  // the expanders and the MMA commit
+      mbar_init(&sm.ld_empty[s], kExpandWarps + 1);  // the expanders and the MMA commit
+    }
+    for (int b = 0; b < kABufs; ++b) {
+      mbar_init(&sm.a_full[b], kExpandWarps);
+      mbar_init(&sm.a_empty[b], 1);
     }
     for (int b = 0; b < 2; ++b) {
-      mbar_init(&sm.a_full[b], kProducerWarps);
-      mbar_init(&sm.a_empty[b], 1);
       mbar_init(&sm.acc_full[b], 1);
-      mbar_init(&sm.acc_empty[b], kEpilogueWarps);
+      mbar_init(&sm.acc_empty[b], kDrainWarps);
     }
-    mbar_init(&sm.cs_ready, kEpilogueWarps);
+    mbar_init(&sm.cs_ready, kDrainWarps);
     mbar_init(&sm.drained, 1);
     sm.abort = 0;
     fence_mbar_init();
@@ -163,9 +195,11 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
   tc_fence_after();
   const uint32_t tmem = sm.tmem_base;
 
-  if (warp < kProducerWarps) {
+  if (warp < kExpandWarps) {
     // ----------------------------------------------------------- expand -------------
-    const uint32_t r = threadIdx.x;  // the row of the tile this thread writes (0..127)
+    const uint32_t q = (uint32_t)warp;        // rows 32 q .. 32 q + 31 of each block
+    const uint32_t lt = (1u << lane) - 1u;    // the lanes (rows) before this one
+    const uint4* meta4 = reinterpret_cast<const uint4*>(sm.meta[q]);
     uint64_t it = 0;
     bool ok = true;
     for (uint64_t w = blockIdx.x; w < n_items && ok; w += gridDim.x) {
@@ -173,83 +207,81 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
       geo.item(w, tile, seg);
       const uint32_t nc = geo.chunks(seg);
       float mean_r = 0.0f;
-      if (value_mode == kValueCentredSquare) {
-        const uint64_t row = (uint64_t)tile * kRows + r;
+      if (vmap.mode == kValueCentredSquare) {
+        const uint64_t row = (uint64_t)tile * kRows + q * 32u + lane;
         mean_r = row < rows ? (float)row_means[row] : 0.0f;
       }
       for (uint32_t c = 0; c < nc; ++c, ++it) {
         const int ls = (int)(it % kLoadStages);
         const uint32_t lph = (uint32_t)((it / kLoadStages) & 1);
-        const uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
+        const uint32_t ab = (uint32_t)(it % kABufs), aph = (uint32_t)((it / kABufs) & 1);
         if (!mbar_wait(&sm.ld_full[ls], lph, abort) || !mbar_wait(&sm.a_empty[ab], aph ^ 1, abort)) {
           ok = false;
           break;
         }
         tc_fence_after();
         const LoadStage& st = sm.st[ls];
-        const bool present = sm.present[ls] != 0;
         const uint32_t* masks = reinterpret_cast<const uint32_t*>(st.blk);
-        const float* vals = reinterpret_cast<const float*>(st.blk + kMaskBytes);
-        // The row's first value: the stored values of the rows before it. The earlier
-        // warps' rows: one warp-wide add of each lane's popcounts; the rows before it in
-        // this warp: an exclusive scan of the row counts (at most 32, 6 bits) built from
-        // one ballot per bit, popcounts of the lower lanes' bits, no dependent shuffles.
-        uint32_t mword = 0, base = 0;
-        if (present) {
-          mword = masks[r];
-          uint32_t before = 0;
-          for (int q = 0; q < warp; ++q) before += __popc(masks[q * 32 + lane]);
-          before = __reduce_add_sync(0xFFFFFFFFu, before);
-          const uint32_t cnt = __popc(mword);
-          const uint32_t lower = (1u << lane) - 1u;
+        const uint32_t* vals = reinterpret_cast<const uint32_t*>(st.blk + kMaskBytes);
+        // Lane c: column c's mask word for this warp's rows, and the rank of its first
+        // value there (the values of the columns before c, then of c's rows in the warps
+        // before this one). The exclusive scan of the column counts (at most 128, 8 bits)
+        // takes one ballot per bit.
+        uint32_t m_own = 0, base = 0;
+        if (sm.present[ls]) {
+          uint32_t colcount = 0, pre = 0;
+#pragma unroll
+          for (int qq = 0; qq < 4; ++qq) {
+            const uint32_t mw = masks[qq * 32 + lane];
+            const uint32_t cnt = __popc(mw);
+            colcount += cnt;
+            if (qq < (int)q) pre += cnt;
+            if (qq == (int)q) m_own = mw;
+          }
           uint32_t excl = 0;
 #pragma unroll
-          for (int b = 0; b < 6; ++b)
-            excl += (uint32_t)__popc(__ballot_sync(0xFFFFFFFFu, (cnt >> b) & 1u) & lower) << b;
-          base = before + excl;
+          for (int b = 0; b < 8; ++b)
+            excl += (uint32_t)__popc(__ballot_sync(0xFFFFFFFFu, (colcount >> b) & 1u) & lt) << b;
+          base = excl + pre;
         }
-        // Branch-free: every column's value is loaded from its would-be rank (the rank
-        // of the next stored value for an empty cell: still inside the stage buffer,
-        // which holds 4,224 values) and kept only where the mask bit is set, so all 32
-        // loads issue back to back.
-        float v[kChunk];
+        sm.meta[q][lane] = make_uint2(m_own, base);
+        __syncwarp();
+        // Row (32 q + lane) of the A tiles: for each column, the value at its rank if the
+        // row stores one (lanes that do read consecutive words; the others read a
+        // neighbour's and drop it), two columns a word, hi parts then lo parts.
+        uint32_t words[32];
 #pragma unroll
-        for (int col = 0; col < kChunk; ++col) {
-          const uint32_t below = col ? __popc(mword & ((1u << col) - 1u)) : 0u;
-          const float x = vals[base + below];
-          v[col] = ((mword >> col) & 1u) ? x : 0.0f;
-        }
-        if (value_mode == kValueCentredSquare) {
-#pragma unroll
-          for (int col = 0; col < kChunk; ++col) {
-            const float d = v[col] - mean_r;
-            v[col] = ((mword >> col) & 1u) ? d * d : 0.0f;
+        for (int c2 = 0; c2 < 16; ++c2) {
+          const uint4 mm = meta4[c2];  // (mask, rank) of columns 2 c2 and 2 c2 + 1
+          uint32_t x0 = vals[mm.y + __popc(mm.x & lt)];
+          uint32_t x1 = vals[mm.w + __popc(mm.z & lt)];
+          const bool h0 = (mm.x >> lane) & 1u, h1 = (mm.z >> lane) & 1u;
+          if (vmap.mode == kValueOne) {
+            x0 = 0x3C00u;  // fp16 1.0, low part 0
+            x1 = 0x3C00u;
+          } else if (vmap.mode == kValueCentredSquare) {
+            const float d0 = pair_value(x0) * vmap.unscale - mean_r;
+            const float d1 = pair_value(x1) * vmap.unscale - mean_r;
+            x0 = split_pair(d0 * d0 * vmap.sq_scale);
+            x1 = split_pair(d1 * d1 * vmap.sq_scale);
           }
-        } else if (value_mode == kValueOne) {
-#pragma unroll
-          for (int col = 0; col < kChunk; ++col) v[col] = ((mword >> col) & 1u) ? 1.0f : 0.0f;
+          x0 = h0 ? x0 : 0u;
+          x1 = h1 ? x1 : 0u;
+          words[c2] = __byte_perm(x0, x1, 0x5410);       // hi parts of both columns
+          words[16 + c2] = __byte_perm(x0, x1, 0x7632);  // lo parts
         }
-        // Row r of the A tile (tf32 hi and lo parts) into TMEM lane r, where the MMA reads it.
-        uint32_t hi[kChunk], lo[kChunk];
-#pragma unroll
-        for (int col = 0; col < kChunk; ++col) {
-          const float h = tf32_round(v[col]);
-          hi[col] = __float_as_uint(h);
-          lo[col] = __float_as_uint(v[col] - h);
-        }
-        const uint32_t arow = tmem + (((uint32_t)warp * 32u) << 16) + kABase + ab * kACols;
-        tmem_st_32(arow, hi);
-        tmem_st_32(arow + 32u, lo);
+        const uint32_t arow = tmem + ((q * 32u) << 16) + kABase + ab * kACols;
+        tmem_st_32(arow, words);
         tmem_wait_st();
         tc_fence_before();
-        __syncwarp();
+        __syncwarp();  // every lane has read meta before the next block rewrites it
         if (lane == 0) {
           mbar_arrive(&sm.a_full[ab]);
           mbar_arrive(&sm.ld_empty[ls]);
         }
       }
     }
-  } else if (warp < kProducerWarps + kEpilogueWarps) {
+  } else if (warp < kExpandWarps + kDrainWarps) {
     // ----------------------------------------------------------- drain TMEM ---------
     const uint32_t quad = (uint32_t)warp & 3u;  // warps 4..7 -> TMEM lanes 32*quad..
     const uint32_t i = quad * 32u + lane;
@@ -287,22 +319,30 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
       }
       if (!ok) break;
       if (out.mode == kOutRows) {
-        // C = S D - offsets: the next product's D^T (tf32 parts), the f32 rows, and this
+        // C = S D - offsets: the next product's D^T (fp16 parts), the f32 rows, and this
         // tile's column sums (fixed tree: warp shuffles, then the 4 warps in order).
         const bool live = row < rows;
+        const double t_mul = ldexp(1.0, out.t_scale), t_inv = ldexp(1.0, -out.t_scale);
+        uint16_t* t_row = out.t ? out.t + (row / 32) * 64 + (row % 32) : nullptr;
 #pragma unroll
         for (int j = 0; j < kN; ++j) {
-          double cval = live && j < (int)out.width ? acc[j] - out.offsets[j] : 0.0;
-          float hi = tf32_round((float)cval);
-          float lo = tf32_round((float)(cval - (double)hi));
-          if (live && out.t_hi) {
-            out.t_hi[(uint64_t)j * out.ld_t + row] = hi;
-            out.t_lo[(uint64_t)j * out.ld_t + row] = lo;
+          const double cval =
+              live && j < (int)out.width ? acc[j] * out_scale - out.offsets[j] : 0.0;
+          double seen = cval;
+          if (out.t) {
+            const double y = cval * t_mul;
+            const __half hi = __double2half(y);
+            const __half lo = __double2half(y - (double)__half2float(hi));
+            seen = ((double)__half2float(hi) + (double)__half2float(lo)) * t_inv;
+            if (live) {
+              t_row[(uint64_t)j * out.ld_t] = __half_as_ushort(hi);
+              t_row[(uint64_t)j * out.ld_t + 32] = __half_as_ushort(lo);
+            }
           }
           if (live && out.rows_f32 && j < (int)out.width)
             out.rows_f32[row * (uint64_t)out.width + j] = (float)cval;
           if (out.colsum_partial) {
-            double sv = (double)hi + (double)lo;
+            double sv = seen;
             for (int o = 16; o; o >>= 1) sv += __shfl_xor_sync(0xFFFFFFFFu, sv, o);
             if (lane == 0) sm.colsum[item_no & 1][quad][j] = sv;
           }
@@ -324,18 +364,15 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
       } else if (row < rows) {
         double* dst = out.partial + ((uint64_t)seg * rows + row) * kN;
 #pragma unroll
-        for (int j = 0; j < kN; ++j) dst[j] = acc[j];
+        for (int j = 0; j < kN; ++j) dst[j] = acc[j] * out_scale;
       }
     }
-  } else if (warp == kProducerWarps + kEpilogueWarps) {
+  } else if (warp == kExpandWarps + kDrainWarps) {
     // ----------------------------------------------------------- loads --------------
     // Lane 0 issues; the warp reads the item's block offsets 32 at a time ahead of it,
     // and each window's successor (or the next item's first window) is prefetched into
     // L2 while this one is copied.
-    if (lane == 0) {
-      prefetch_tmap(&tmap_hi);
-      prefetch_tmap(&tmap_lo);
-    }
+    if (lane == 0) prefetch_tmap(&tmap_dt);
     uint64_t it = 0;
     int issued_phase[kLoadStages];
     for (int s = 0; s < kLoadStages; ++s) issued_phase[s] = -1;
@@ -384,10 +421,8 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
             const uint32_t chunk = seg * geo.seg_chunks + c;
             const uint32_t bytes = (uint32_t)((e1 - e0) * 16);
             sm.present[s] = bytes ? 1u : 0u;
-            mbar_arrive_expect_tx(&sm.ld_full[s], 2 * kBBytes + bytes);
-            const int32_t x = (int32_t)(chunk * kChunk);
-            tma_load_2d(sm.st[s].b_hi, &tmap_hi, &sm.ld_full[s], x, 0);
-            tma_load_2d(sm.st[s].b_lo, &tmap_lo, &sm.ld_full[s], x, 0);
+            mbar_arrive_expect_tx(&sm.ld_full[s], kBBytes + bytes);
+            tma_load_2d(sm.st[s].b, &tmap_dt, &sm.ld_full[s], (int32_t)(chunk * 64), 0);
             if (bytes) bulk_load(sm.st[s].blk, data + e0 * 16, bytes, &sm.ld_full[s]);
             issued_phase[s] = (int)ph;
           }
@@ -406,7 +441,7 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
   } else {
     // ----------------------------------------------------------- MMA ----------------
     if (lane == 0) {
-      const uint32_t idesc = idesc_f32acc(2u, kRows, kN);  // tf32 x tf32 -> f32
+      const uint32_t idesc = idesc_f32acc(0u, kRows, kN);  // f16 x f16 -> f32
       uint64_t it = 0, fg = 0;
       bool ok = true;
       for (uint64_t w = blockIdx.x; w < n_items && ok; w += gridDim.x) {
@@ -422,21 +457,22 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
           }
           const int ls = (int)(it % kLoadStages);
           const uint32_t lph = (uint32_t)((it / kLoadStages) & 1);
-          const uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
+          const uint32_t ab = (uint32_t)(it % kABufs), aph = (uint32_t)((it / kABufs) & 1);
           if (!mbar_wait(&sm.ld_full[ls], lph, abort) || !mbar_wait(&sm.a_full[ab], aph, abort)) {
             ok = false;
             break;
           }
           tc_fence_after();
           const uint32_t d = tmem + b * kAccCols;
-          const uint32_t ah = tmem + kABase + ab * kACols, al = ah + 32u;
-          const uint32_t bh = smem_addr(sm.st[ls].b_hi), bl = smem_addr(sm.st[ls].b_lo);
+          const uint32_t ah = tmem + kABase + ab * kACols, al = ah + 16u;
+          const uint32_t bs = smem_addr(sm.st[ls].b);
 #pragma unroll
-          for (int kk = 0; kk < kChunk / 8; ++kk) {
-            const uint32_t o = kk * 32;  // 8 tf32 of K: 32 bytes of a B row, 8 A columns
-            mma_tf32_ts(d, ah + kk * 8, desc_k_sw128(bh + o), idesc, (in_group | kk) != 0);
-            mma_tf32_ts(d, ah + kk * 8, desc_k_sw128(bl + o), idesc, 1);
-            mma_tf32_ts(d, al + kk * 8, desc_k_sw128(bh + o), idesc, 1);
+          for (int kk = 0; kk < kChunk / 16; ++kk) {
+            // 16 K: 8 A columns (pairs), 32 bytes of a B row; B's lo parts 64 bytes on.
+            const uint32_t o = kk * 32;
+            mma_f16_ts(d, ah + kk * 8, desc_k_sw128(bs + o), idesc, (in_group | kk) != 0);
+            mma_f16_ts(d, ah + kk * 8, desc_k_sw128(bs + 64 + o), idesc, 1);
+            mma_f16_ts(d, al + kk * 8, desc_k_sw128(bs + o), idesc, 1);
           }
           mma_commit(&sm.ld_empty[ls]);
           mma_commit(&sm.a_empty[ab]);
@@ -462,19 +498,46 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_hi,
 
 // ------------------------------------------------------------------ builders -------
 
+// Per row: the sum of squared values (f64) into the largest so far, and the largest and
+// smallest nonzero |value| (non-negative doubles compare as their bit patterns).
+__global__ void csr_stats_kernel(const uint64_t* ptr, const float* val, uint64_t n_rows,
+                                 unsigned long long* max_sq, unsigned long long* max_abs,
+                                 unsigned long long* min_abs) {
+  uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  unsigned lane = threadIdx.x & 31u;
+  if (r >= n_rows) return;
+  double sq = 0.0, hi = 0.0, lo = INFINITY;
+  for (uint64_t i = ptr[r] + lane; i < ptr[r + 1]; i += 32) {
+    const double v = fabs((double)val[i]);
+    sq += v * v;
+    hi = fmax(hi, v);
+    if (v > 0.0) lo = fmin(lo, v);
+    if (v != v) hi = v;  // a NaN dominates
+  }
+  for (int o = 16; o; o >>= 1) {
+    sq += __shfl_xor_sync(0xFFFFFFFFu, sq, o);
+    const double h2 = __shfl_xor_sync(0xFFFFFFFFu, hi, o);
+    hi = (hi != hi) ? hi : ((h2 != h2) ? h2 : fmax(hi, h2));
+    lo = fmin(lo, __shfl_xor_sync(0xFFFFFFFFu, lo, o));
+  }
+  if (lane == 0) {
+    atomicMax(max_sq, (unsigned long long)__double_as_longlong(sq));
+    atomicMax(max_abs, (unsigned long long)__double_as_longlong(hi));
+    atomicMin(min_abs, (unsigned long long)__double_as_longlong(lo));
+  }
+}
+
 // The block of a stored value, and its row (in the tile) and column (in the chunk).
-__device__ __forceinline__ void locate(uint64_t r, uint32_t c, bool transpose, uint32_t n_chunks,
+__device__ __forceinline__ void locate(uint64_t r, uint32_t c, uint32_t n_chunks,
                                        uint64_t& block, uint32_t& br, uint32_t& bc) {
-  uint64_t orow = transpose ? c : r;  // row of the output layout
-  uint64_t ocol = transpose ? r : c;
-  block = (orow / kRows) * n_chunks + ocol / kChunk;
-  br = (uint32_t)(orow % kRows);
-  bc = (uint32_t)(ocol % kChunk);
+  block = (r / kRows) * n_chunks + c / kChunk;
+  br = (uint32_t)(r % kRows);
+  bc = (uint32_t)(c % kChunk);
 }
 
 // Stored values per block (warp per CSR row; lanes whose values share a block add once).
 __global__ void blocked_count_kernel(const uint64_t* ptr, const uint32_t* col, uint64_t n_rows,
-                                     bool transpose, uint32_t n_chunks, uint32_t* counts) {
+                                     uint32_t n_chunks, uint32_t* counts) {
   uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   unsigned lane = threadIdx.x & 31u;
   if (r >= n_rows) return;
@@ -485,7 +548,7 @@ __global__ void blocked_count_kernel(const uint64_t* ptr, const uint32_t* col, u
     if (!in) continue;
     uint64_t block;
     uint32_t br, bc;
-    locate(r, col[i], transpose, n_chunks, block, br, bc);
+    locate(r, col[i], n_chunks, block, br, bc);
     unsigned same = __match_any_sync(active, block);
     if ((unsigned)__ffs(same) - 1 == lane) atomicAdd(&counts[block], (uint32_t)__popc(same));
   }
@@ -499,75 +562,77 @@ __global__ void block_units_kernel(const uint32_t* counts, uint64_t n, uint64_t*
   if (i == n) units[i] = 0;
 }
 
-// Mask bits: bit c of word r of a block marks the value at (row r, column c). Lanes that
-// hit the same word OR their bits together first.
+// Column masks: bit (row % 32) of word (row / 32) * 32 + column marks a stored value. The
+// lanes of a CSR row hit different columns, so one row's values never share a word.
 __global__ void blocked_mask_kernel(const uint64_t* ptr, const uint32_t* col, uint64_t n_rows,
-                                    bool transpose, uint32_t n_chunks, const uint64_t* off,
-                                    uint8_t* data) {
-  uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  unsigned lane = threadIdx.x & 31u;
-  if (r >= n_rows) return;
-  for (uint64_t i0 = ptr[r]; i0 < ptr[r + 1]; i0 += 32) {
-    uint64_t i = i0 + lane;
-    bool in = i < ptr[r + 1];
-    unsigned active = __ballot_sync(0xFFFFFFFFu, in);
-    if (!in) continue;
-    uint64_t block;
-    uint32_t br, bc;
-    locate(r, col[i], transpose, n_chunks, block, br, bc);
-    uint32_t* word = reinterpret_cast<uint32_t*>(data + off[block] * 16) + br;
-    unsigned same = __match_any_sync(active, reinterpret_cast<uint64_t>(word));
-    uint32_t bits = __reduce_or_sync(same, 1u << bc);
-    if ((unsigned)__ffs(same) - 1 == lane) atomicOr(word, bits);
-  }
-}
-
-// prefix[b * 128 + row]: the values of block b in the rows before `row` (warp per block).
-__global__ void row_prefix_kernel(const uint64_t* off, const uint8_t* data, uint64_t n_blocks,
-                                  uint16_t* prefix) {
-  uint64_t b = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  unsigned lane = threadIdx.x & 31u;
-  if (b >= n_blocks || off[b + 1] == off[b]) return;
-  const uint32_t* masks = reinterpret_cast<const uint32_t*>(data + off[b] * 16);
-  uint32_t carry = 0;
-  for (int q = 0; q < kRows / 32; ++q) {
-    uint32_t v = __popc(masks[q * 32 + lane]);
-    uint32_t incl = v;
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    prefix[b * kRows + q * 32 + lane] = (uint16_t)(carry + incl - v);
-    carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
-  }
-}
-
-// Each value at its rank in its block (rows in order, columns in order inside a row).
-__global__ void blocked_values_kernel(const uint64_t* ptr, const uint32_t* col, const float* val,
-                                      uint64_t n_rows, bool transpose, uint32_t n_chunks,
-                                      const uint64_t* off, const uint16_t* prefix,
-                                      uint8_t* data) {
+                                    uint32_t n_chunks, const uint64_t* off, uint8_t* data) {
   uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   unsigned lane = threadIdx.x & 31u;
   if (r >= n_rows) return;
   for (uint64_t i = ptr[r] + lane; i < ptr[r + 1]; i += 32) {
     uint64_t block;
     uint32_t br, bc;
-    locate(r, col[i], transpose, n_chunks, block, br, bc);
+    locate(r, col[i], n_chunks, block, br, bc);
+    uint32_t* word = reinterpret_cast<uint32_t*>(data + off[block] * 16) + (br / 32) * 32 + bc;
+    atomicOr(word, 1u << (br % 32));
+  }
+}
+
+// prefix[b * 128 + q * 32 + c]: the values of block b before its rows 32 q.. of column c
+// (the columns before c, then column c's earlier row quarters); warp per block.
+__global__ void col_prefix_kernel(const uint64_t* off, const uint8_t* data, uint64_t n_blocks,
+                                  uint16_t* prefix) {
+  uint64_t b = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  unsigned lane = threadIdx.x & 31u;
+  if (b >= n_blocks || off[b + 1] == off[b]) return;
+  const uint32_t* masks = reinterpret_cast<const uint32_t*>(data + off[b] * 16);
+  uint32_t cnt[4], total = 0;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    cnt[q] = __popc(masks[q * 32 + lane]);
+    total += cnt[q];
+  }
+  uint32_t incl = total;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    if ((int)lane >= o) incl += t;
+  }
+  uint32_t at = incl - total;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    prefix[b * kRows + q * 32 + lane] = (uint16_t)at;
+    at += cnt[q];
+  }
+}
+
+// Each value, scaled and split, at its rank in its block.
+__global__ void blocked_values_kernel(const uint64_t* ptr, const uint32_t* col, const float* val,
+                                      uint64_t n_rows, uint32_t n_chunks, const uint64_t* off,
+                                      const uint16_t* prefix, int scale, uint8_t* data) {
+  uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  unsigned lane = threadIdx.x & 31u;
+  if (r >= n_rows) return;
+  for (uint64_t i = ptr[r] + lane; i < ptr[r + 1]; i += 32) {
+    uint64_t block;
+    uint32_t br, bc;
+    locate(r, col[i], n_chunks, block, br, bc);
     uint8_t* blk = data + off[block] * 16;
-    const uint32_t word = reinterpret_cast<const uint32_t*>(blk)[br];
-    const uint32_t rank = prefix[block * kRows + br] + __popc(word & ((1u << bc) - 1u));
-    reinterpret_cast<float*>(blk + kMaskBytes)[rank] = val[i];
+    const uint32_t wi = (br / 32) * 32 + bc;
+    const uint32_t word = reinterpret_cast<const uint32_t*>(blk)[wi];
+    const uint32_t rank = prefix[block * kRows + wi] + __popc(word & ((1u << (br % 32)) - 1u));
+    reinterpret_cast<uint32_t*>(blk + kMaskBytes)[rank] = split_pair(ldexpf(val[i], scale));
   }
 }
 
 // ---------------------------------------------------------------- the transpose --
 //
 // X^T's blocked layout from X's (no pass over the CSR, no atomics). Block (G, c) of X^T
-// (genes 128 G.., cells 32 c..) holds the 32 cell rows 32 (c % 4).. of the four X blocks
-// (tile c / 4, gene chunks 4 G ..4 G + 3), transposed: its gene row 32 i + j has bit l set
-// where X block (c / 4, 4 G + i) has a value at cell row 32 (c % 4) + l, gene column j.
-// One warp per X^T block; lane l reads cell row 32 (c % 4) + l of each source block.
+// (genes 128 G.., cells 32 c..) holds row quarter i from X block (tile c / 4, gene chunk
+// 4 G + i), whose cell rows 32 (c % 4) + l it transposes: X^T's mask word i * 32 + l (gene
+// rows 32 i.., cell column l) has bit j set where X's mask word (c % 4) * 32 + j (cell
+// rows 32 (c % 4).., gene column j) has bit l. One warp per X^T block: lane j holds X's
+// word for gene column j of each source; a ballot per (l, i) forms X^T's word and places
+// the values of column l, gene rows in order.
 
 // Source block i of X^T block (G, c), or ~0 past X's gene chunks.
 __device__ __forceinline__ uint64_t transpose_source(uint32_t G, uint32_t c, int i,
@@ -602,116 +667,81 @@ __global__ void transpose_fill_kernel(const uint64_t* x_off, const uint8_t* x_da
   const unsigned lane = threadIdx.x & 31u;
   if (b >= (uint64_t)t_tiles * t_chunks || t_off[b + 1] == t_off[b]) return;
   const uint32_t G = (uint32_t)(b / t_chunks), c = (uint32_t)(b % t_chunks);
-  const uint32_t group = c % 4;  // the source blocks' cell rows 32 group..
-  uint32_t src_mask[4], src_pre[4], mine[4];
-  const float* src_vals[4];
+  const uint32_t g = c % 4;  // the source blocks' cell row quarter
+  const uint32_t lt = (1u << lane) - 1u;
+  uint32_t src_mask[4], src_rank[4];
+  const uint32_t* src_vals[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     src_mask[i] = 0;
-    src_pre[i] = 0;
+    src_rank[i] = 0;
     src_vals[i] = nullptr;
     const uint64_t src = transpose_source(G, c, i, x_chunks);
     if (src != ~0ull && x_off[src + 1] != x_off[src]) {
       const uint8_t* blk = x_data + x_off[src] * 16;
       const uint32_t* masks = reinterpret_cast<const uint32_t*>(blk);
-      src_vals[i] = reinterpret_cast<const float*>(blk + kMaskBytes);
-      src_mask[i] = masks[32 * group + lane];
-      // Values of the source block before cell row 32 group + lane (rows in order).
-      uint32_t base = 0;
-      for (uint32_t q = 0; q < group; ++q) base += __popc(masks[32 * q + lane]);
-      for (int o = 16; o; o >>= 1) base += __shfl_xor_sync(0xFFFFFFFFu, base, o);
-      const uint32_t v = __popc(src_mask[i]);
-      uint32_t incl = v;
+      src_vals[i] = reinterpret_cast<const uint32_t*>(blk + kMaskBytes);
+      // Gene column j = lane of the source: its first value (the columns before it, then
+      // its rows before quarter g).
+      uint32_t total = 0, before = 0;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t mw = masks[q * 32 + lane];
+        total += __popc(mw);
+        if (q < (int)g) before += __popc(mw);
+        if (q == (int)g) src_mask[i] = mw;
+      }
+      uint32_t incl = total;
       for (int o = 1; o < 32; o <<= 1) {
         const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if (lane >= o) incl += t;
+        if ((int)lane >= o) incl += t;
       }
-      src_pre[i] = base + incl - v;
-    }
-    // The 32 x 32 bit transpose: gene j's cell mask is the ballot of bit j.
-    mine[i] = 0;
-#pragma unroll 4
-    for (int j = 0; j < 32; ++j) {
-      const uint32_t t = __ballot_sync(0xFFFFFFFFu, (src_mask[i] >> j) & 1u);
-      if ((int)lane == j) mine[i] = t;
+      src_rank[i] = incl - total + before;
     }
   }
   uint8_t* out = t_data + t_off[b] * 16;
   uint32_t* out_masks = reinterpret_cast<uint32_t*>(out);
-  float* out_vals = reinterpret_cast<float*>(out + kMaskBytes);
-  uint32_t carry = 0;
+  uint32_t* out_vals = reinterpret_cast<uint32_t*>(out + kMaskBytes);
+  uint32_t mine[4] = {0, 0, 0, 0};
+  uint32_t at = 0;  // values placed so far (column-major order)
+  for (int l = 0; l < 32; ++l) {
+    const uint32_t below_l = (1u << l) - 1u;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    out_masks[32 * i + lane] = mine[i];
-    // This gene row's first value: the values of the X^T rows before it.
-    const uint32_t v = __popc(mine[i]);
-    uint32_t incl = v;
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-      if (lane >= o) incl += t;
-    }
-    uint32_t at = carry + incl - v;
-    carry += __shfl_sync(0xFFFFFFFFu, incl, 31);
-    // Cells in order: cell l's value sits at its rank in source block i.
-    const uint32_t below = (1u << lane) - 1u;  // gene columns before this lane's
-    const float* sv = src_vals[i];
-    const uint32_t mi = mine[i];
-    for (int l = 0; l < 32; ++l) {
-      const uint32_t pre = __shfl_sync(0xFFFFFFFFu, src_pre[i], l);
-      const uint32_t m = __shfl_sync(0xFFFFFFFFu, src_mask[i], l);
-      const uint32_t has = (mi >> l) & 1u;
-      if (has) out_vals[at] = sv[pre + __popc(m & below)];
-      at += has;
+    for (int i = 0; i < 4; ++i) {
+      const bool has = (src_mask[i] >> l) & 1u;
+      const uint32_t m = __ballot_sync(0xFFFFFFFFu, has);  // X^T word i * 32 + l
+      if ((int)lane == l) mine[i] = m;
+      if (has) out_vals[at + __popc(m & lt)] = src_vals[i][src_rank[i] + __popc(src_mask[i] & below_l)];
+      at += __popc(m);
     }
   }
-}
-
-PFN_cuTensorMapEncodeTiled_v12000 encode() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault,
-                                         &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-  });
-  if (!fn) fail(KG_ERR_DEVICE, "cuTensorMapEncodeTiled is not available from the driver");
-  return fn;
-}
-
-// D^T part: 64 rows x K f32 (row stride ld floats), boxes of 64 rows x 32 columns.
-CUtensorMap dt_map(const float* base, uint64_t K, uint64_t ld) {
-  CUtensorMap m;
-  std::memset(&m, 0, sizeof(m));
-  cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)kN};
-  cuuint64_t strides[1] = {(cuuint64_t)ld * 4};
-  cuuint32_t box[2] = {(cuuint32_t)kChunk, (cuuint32_t)kN};
-  cuuint32_t estr[2] = {1, 1};
-  CUresult r = encode()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims,
-                        strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS)
-    fail(KG_ERR_DEVICE, "cuTensorMapEncodeTiled (D^T) failed: " + std::to_string((int)r));
-  return m;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) out_masks[32 * i + lane] = mine[i];
 }
 
 }  // namespace
 
 void build_blocked(const uint64_t* ptr, const uint32_t* col, const float* val, uint64_t n_rows,
-                   uint64_t n_cols, uint64_t nnz, bool transpose, Blocked& out, cudaStream_t s) {
-  out.rows = transpose ? n_cols : n_rows;
-  out.K = transpose ? n_rows : n_cols;
+                   uint64_t n_cols, uint64_t nnz, Blocked& out, cudaStream_t s) {
+  out.rows = n_rows;
+  out.K = n_cols;
   out.n_tiles = (uint32_t)((out.rows + kRows - 1) / kRows);
   out.n_chunks = (uint32_t)((out.K + kChunk - 1) / kChunk);
   const uint64_t nb = (uint64_t)out.n_tiles * out.n_chunks;
+  // The values' range (the scale of their fp16 parts) and the largest row norm.
+  DeviceBuffer<unsigned long long> st(3, s);
+  const unsigned long long init[3] = {0ull, 0ull, 0x7FF0000000000000ull};  // 0, 0, +inf
+  KG_CUDA(cudaMemcpyAsync(st.ptr, init, sizeof init, cudaMemcpyHostToDevice, s));
+  if (nnz) {
+    csr_stats_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(ptr, val, n_rows, st.ptr,
+                                                                  st.ptr + 1, st.ptr + 2);
+    KG_LAUNCH_CHECK();
+  }
   DeviceBuffer<uint32_t> counts(nb, s);
   counts.zero();
   if (nnz) {
-    blocked_count_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(
-        ptr, col, n_rows, transpose, out.n_chunks, counts.ptr);
+    blocked_count_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(ptr, col, n_rows,
+                                                                      out.n_chunks, counts.ptr);
     KG_LAUNCH_CHECK();
   }
   out.off.alloc(nb + 1, s);
@@ -723,21 +753,30 @@ void build_blocked(const uint64_t* ptr, const uint32_t* col, const float* val, u
   DeviceBuffer<unsigned char> scratch(temp, s);
   KG_CUDA(cub::DeviceScan::ExclusiveSum(scratch.ptr, temp, out.off.ptr, out.off.ptr, nb + 1, s));
   uint64_t units = 0;
+  unsigned long long h_st[3];
   KG_CUDA(cudaMemcpyAsync(&units, out.off.ptr + nb, 8, cudaMemcpyDeviceToHost, s));
+  KG_CUDA(cudaMemcpyAsync(h_st, st.ptr, sizeof h_st, cudaMemcpyDeviceToHost, s));
   KG_CUDA(cudaStreamSynchronize(s));
+  double d[3];
+  std::memcpy(d, h_st, sizeof d);
+  out.max_row_norm = std::sqrt(d[0]);
+  out.max_abs = d[1];
+  out.min_abs = std::isinf(d[2]) ? 0.0 : d[2];
+  out.scale = part_scale(out.max_abs);
   out.bytes = units * 16;
   out.data.alloc(std::max<uint64_t>(out.bytes, 16), s);
+  // Padding past a block's values must read as zero (the expansion may load one past).
   out.data.zero();
   if (nnz) {
     blocked_mask_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(
-        ptr, col, n_rows, transpose, out.n_chunks, out.off.ptr, out.data.ptr);
+        ptr, col, n_rows, out.n_chunks, out.off.ptr, out.data.ptr);
     KG_LAUNCH_CHECK();
     DeviceBuffer<uint16_t> prefix(nb * kRows, s);
-    row_prefix_kernel<<<blocks_for(nb * 32, 256), 256, 0, s>>>(out.off.ptr, out.data.ptr, nb,
+    col_prefix_kernel<<<blocks_for(nb * 32, 256), 256, 0, s>>>(out.off.ptr, out.data.ptr, nb,
                                                                prefix.ptr);
     KG_LAUNCH_CHECK();
     blocked_values_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(
-        ptr, col, val, n_rows, transpose, out.n_chunks, out.off.ptr, prefix.ptr, out.data.ptr);
+        ptr, col, val, n_rows, out.n_chunks, out.off.ptr, prefix.ptr, out.scale, out.data.ptr);
     KG_LAUNCH_CHECK();
   }
 }
@@ -747,6 +786,10 @@ void transpose_blocked(const Blocked& x, Blocked& out, cudaStream_t s) {
   out.K = x.rows;
   out.n_tiles = (uint32_t)((out.rows + kRows - 1) / kRows);
   out.n_chunks = (uint32_t)((out.K + kChunk - 1) / kChunk);
+  out.scale = x.scale;
+  out.max_abs = x.max_abs;
+  out.min_abs = x.min_abs;
+  out.max_row_norm = 0.0;  // not tracked for the transpose
   const uint64_t nb = (uint64_t)out.n_tiles * out.n_chunks;
   DeviceBuffer<uint32_t> counts(nb, s);
   transpose_count_kernel<<<blocks_for(nb * 32, 256), 256, 0, s>>>(
@@ -765,7 +808,6 @@ void transpose_blocked(const Blocked& x, Blocked& out, cudaStream_t s) {
   KG_CUDA(cudaStreamSynchronize(s));
   out.bytes = units * 16;
   out.data.alloc(std::max<uint64_t>(out.bytes, 16), s);
-  // Padding past a block's values must read as zero (the expansion loads past the end).
   out.data.zero();
   transpose_fill_kernel<<<blocks_for(nb * 32, 256), 256, 0, s>>>(
       x.off.ptr, x.data.ptr, x.n_chunks, out.n_tiles, out.n_chunks, out.off.ptr, out.data.ptr);
@@ -780,7 +822,10 @@ void spmm_tc(const SpmmArgs& a, cudaStream_t s) {
     KG_CUDA(cudaFuncSetAttribute(spmm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)kSpSmemBytes));
   });
-  if (a.ld_t % 4 != 0) fail(KG_ERR_INVALID, "spmm: D^T row stride must be a multiple of 4");
+  if (a.ld_t != dense_ld(b.K)) fail(KG_ERR_INVALID, "spmm: D^T row length must be dense_ld(K)");
+  if (a.out.mode == kOutRows && a.out.t && a.out.ld_t != dense_ld(b.rows))
+    fail(KG_ERR_INVALID, "spmm: the output D^T row length must be dense_ld(rows)");
+  if (!a.error) fail(KG_ERR_INVALID, "spmm: no error flag");
   Geometry geo;
   geo.n_tiles = b.n_tiles;
   geo.n_chunks = b.n_chunks;
@@ -788,19 +833,28 @@ void spmm_tc(const SpmmArgs& a, cudaStream_t s) {
   geo.n_segs = (geo.n_chunks + geo.seg_chunks - 1) / geo.seg_chunks;
   if (a.out.mode == kOutRows && geo.n_segs != 1)
     fail(KG_ERR_INVALID, "spmm: row output needs one K segment");
-  CUtensorMap mh = dt_map(a.dt_hi, b.K, a.ld_t), ml = dt_map(a.dt_lo, b.K, a.ld_t);
-  DeviceBuffer<int> err(1, s);
-  err.zero();
+  // S's stored values enter the MMA times 2^a_scale (the stored scale, 0 for the ones,
+  // a square's own scale for the centred squares), D^T times 2^dt_scale.
+  ValueMap vm;
+  vm.mode = a.value_mode;
+  vm.unscale = ldexpf(1.0f, -b.scale);
+  int a_scale = b.scale;
+  vm.sq_scale = 1.0f;
+  if (a.value_mode == kValueOne) {
+    a_scale = 0;
+  } else if (a.value_mode == kValueCentredSquare) {
+    // (v - mean)^2 <= (|v| + |mean|)^2 <= (2 max|v|)^2.
+    a_scale = part_scale(4.0 * b.max_abs * b.max_abs);
+    vm.sq_scale = ldexpf(1.0f, a_scale);
+  }
+  const double out_scale = std::ldexp(1.0, -(a_scale + a.dt_scale));
+  CUtensorMap m = tma_map_2d_16bit(a.dt, CU_TENSOR_MAP_DATA_TYPE_FLOAT16, a.ld_t, kN,
+                                   a.ld_t * 2, 64, kN);
   uint64_t items = (uint64_t)geo.n_tiles * geo.n_segs;
   unsigned grid = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(items, (uint64_t)a.sm_count));
-  spmm_tc_kernel<<<grid, kSpThreads, kSpSmemBytes, s>>>(mh, ml, b.off.ptr, b.data.ptr, b.rows,
-                                                        geo, a.value_mode, a.row_means, a.out,
-                                                        err.ptr);
+  spmm_tc_kernel<<<grid, kSpThreads, kSpSmemBytes, s>>>(m, b.off.ptr, b.data.ptr, b.rows, geo, vm,
+                                                        a.row_means, out_scale, a.out, a.error);
   KG_LAUNCH_CHECK();
-  int h = 0;
-  KG_CUDA(cudaMemcpyAsync(&h, err.ptr, 4, cudaMemcpyDeviceToHost, s));
-  KG_CUDA(cudaStreamSynchronize(s));
-  if (h) fail(KG_ERR_TIMEOUT, "the tensor-core SpMM gave up waiting on its pipeline");
 }
 
 }  // namespace kg

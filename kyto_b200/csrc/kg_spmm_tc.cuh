@@ -1,5 +1,5 @@
-// The tensor-core sparse x dense product of the PCA (kg_spmm_tc.cu) and the blocked
-// sparse layout it reads.
+// The tensor-core sparse x dense product of the PCA (kg_spmm_tc.cu), the blocked sparse
+// layout it reads and the dense operand layout it takes.
 #pragma once
 
 #include <cstdint>
@@ -10,27 +10,45 @@ namespace kg {
 
 // A sparse matrix (rows x K) cut into blocks of 128 rows x 32 columns. Block
 // b = tile * n_chunks + chunk starts at byte 16 * off[b] of `data` and is empty
-// (off[b + 1] == off[b]) or holds 128 mask words (bit c of word r: a value at row r,
-// column c of the block) followed by its values, rows in order and columns in order
-// inside a row, padded to a multiple of 4 floats: 16-byte aligned, one bulk copy each.
-// At the benchmark's 30% density that is 512 + 4 nnz bytes a block, against 6 nnz for
-// 16-bit positions beside the values.
+// (off[b + 1] == off[b]) or holds 128 column mask words followed by its values:
+//  - mask word q * 32 + c has bit l set where row 32 q + l of the block stores a value in
+//    column c;
+//  - the values follow column by column, rows in order inside a column, padded to a
+//    multiple of 4 words (16 bytes, one bulk copy per block);
+//  - a value is one 32-bit word holding x = value * 2^scale in two fp16 parts: bits 0-15
+//    hi = fp16(x), bits 16-31 lo = fp16(x - hi) (together about 22 bits of x).
+// Column order makes the product's expansion conflict-free: for one column, the threads of
+// a warp (one row each) read consecutive words. At the benchmark's 33% density a block is
+// 512 + 4 nnz bytes, against 8 nnz for a u32 index and an f32 value.
 struct Blocked {
   uint64_t rows = 0, K = 0;
   uint32_t n_tiles = 0, n_chunks = 0;
   uint64_t bytes = 0;
-  DeviceBuffer<uint64_t> off;   // n_tiles * n_chunks + 1 offsets, 16-byte units
+  int scale = 0;            // values stored times 2^scale (largest |x| in [2^14, 2^15))
+  double max_abs = 0.0;     // the largest |value| and the smallest nonzero one
+  double min_abs = 0.0;
+  double max_row_norm = 0.0;  // the largest row's Euclidean norm (rows of the matrix)
+  DeviceBuffer<uint64_t> off;  // n_tiles * n_chunks + 1 offsets, 16-byte units
   DeviceBuffer<uint8_t> data;
 };
 
 // The blocked layout of a CSR matrix (n_rows x n_cols, u32 column indices, each row's
-// columns strictly increasing), or of its transpose (rows = the CSR's columns).
+// columns strictly increasing).
 void build_blocked(const uint64_t* ptr, const uint32_t* col, const float* val, uint64_t n_rows,
-                   uint64_t n_cols, uint64_t nnz, bool transpose, Blocked& out, cudaStream_t s);
+                   uint64_t n_cols, uint64_t nnz, Blocked& out, cudaStream_t s);
 
-// The blocked layout of X^T from X's (bit-transposed blocks, values moved by rank): the
-// same bytes build_blocked(..., transpose = true) writes.
+// The blocked layout of X^T from X's (bit-transposed masks, values moved by rank; the
+// same scale).
 void transpose_blocked(const Blocked& x, Blocked& out, cudaStream_t s);
+
+// The dense operand D (K x 64) as the products read it: D^T, 64 rows of fp16 parts of
+// each value times 2^scale, interleaved by chunk: for chunk c, row j holds the 32 high
+// parts of D[32c .. 32c+31][j] and then their 32 low parts (128 bytes, one TMA box row).
+// Rows are `ld` halves long (ld = 64 * chunks, chunks = ceil(K / 32)).
+inline uint64_t dense_ld(uint64_t K) { return (K + 31) / 32 * 64; }
+
+// The exponent that puts the largest magnitude `bound` in [2^14, 2^15) (0 for 0).
+int part_scale(double bound);
 
 enum : int { kOutRows = 0, kOutPartial = 1 };
 enum : int { kValuePlain = 0, kValueCentredSquare = 1, kValueOne = 2 };
@@ -41,12 +59,13 @@ struct SpmmOut {
   uint32_t width = 64;             // columns of C that carry data (<= 64)
   // kOutRows (one K segment): row r of C minus `offsets` (width f64 values) ...
   const double* offsets = nullptr;
-  float* t_hi = nullptr;           // ... as C^T split in two tf32 parts (64 x ld_t f32),
-  float* t_lo = nullptr;
-  uint64_t ld_t = 0;
+  uint16_t* t = nullptr;           // ... as the next product's D^T (dense layout above,
+  uint64_t ld_t = 0;               //     row length ld_t halves, values times 2^t_scale),
+  int t_scale = 0;
   float* rows_f32 = nullptr;       // ... as f32 rows (rows x width),
-  double* colsum_partial = nullptr;  // ... and the column sums of t_hi + t_lo per tile
-                                     // of 128 rows (n_tiles x 64 f64).
+  double* colsum_partial = nullptr;  // ... and the column sums of the rounded rows (as
+                                     // the next product sees them) per tile of 128 rows
+                                     // (n_tiles x 64 f64).
   // kOutPartial: each K segment's C as f64 (segments x rows x 64).
   double* partial = nullptr;
 };
@@ -57,13 +76,16 @@ struct SpmmArgs {
                                    // kValueOne: 1 for every stored value
   const double* row_means = nullptr;
   uint64_t seg_chunks = 0;         // K-chunks (32 columns) per work item
-  const float* dt_hi = nullptr;    // D^T, 64 x K, tf32 parts, row stride ld_t floats
-  const float* dt_lo = nullptr;
-  uint64_t ld_t = 0;
+  const uint16_t* dt = nullptr;    // D^T in the dense layout, row length ld_t halves,
+  uint64_t ld_t = 0;               // values times 2^dt_scale
+  int dt_scale = 0;
   SpmmOut out;
   int sm_count = 148;
+  int* error = nullptr;            // set to 1 if a bounded wait ran out (device flag)
 };
 
+// Launches the product on stream s (no host synchronisation; `error` reports a pipeline
+// that gave up waiting).
 void spmm_tc(const SpmmArgs& a, cudaStream_t s);
 
 }  // namespace kg
