@@ -58,7 +58,9 @@ constexpr uint32_t kNoBlock = 0xFFFFFFFFu;  // no query block left: the CTA's ro
 // register top-k width (16, 32) or 0 (the k smallest in local memory, any k).
 template <int KR, int SUBS>
 struct TcShape {
-  static constexpr int kStages = SUBS == 1 ? 6 : (KR == 32 ? 2 : 3);
+  // Point-tile stages: as many as shared memory holds beside the query tiles, the
+  // scratch rows and the top-k rows (KR == 0 keeps its k smallest in local memory).
+  static constexpr int kStages = SUBS == 1 ? (KR == 32 ? 7 : 8) : (KR == 32 ? 2 : 3);
   static constexpr int kTopK = KR == 0 ? 1 : KR + 1;  // odd row stride: no bank conflicts
 };
 

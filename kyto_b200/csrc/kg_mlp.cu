@@ -29,21 +29,30 @@ __device__ __forceinline__ float as_f32(__nv_bfloat16 v) { return __bfloat162flo
 // tiles: a fixed order). A(m,k) = TA ? A[k*lda+m] : A[m*lda+k]; B(k,n) = TB ? B[n*ldb+k]
 // : B[k*ldb+n]. Epilogues: store; + bias then ReLU rounded to bf16 into h (C keeps the
 // pre-activation); C * (z > 0) (the ReLU's backward); + bias.
+// Split over K (gridDim.z > 1, the store epilogue only): slice z sums k in
+// [z * kslice, (z + 1) * kslice) and writes its M x N partial at C + z * M * N (row
+// stride N); split_sum_kernel then adds the slices in order.
 template <class TA, class TB, bool TRA, bool TRB, int EPI>
 __global__ void __launch_bounds__(kGemmThreads)
 gemm_kernel(int M, int N, int K, const TA* __restrict__ A, int lda, const TB* __restrict__ B,
             int ldb, float* __restrict__ C, int ldc, const float* __restrict__ bias,
-            __nv_bfloat16* __restrict__ h, int ldh, const float* __restrict__ z, int ldz) {
+            __nv_bfloat16* __restrict__ h, int ldh, const float* __restrict__ z, int ldz,
+            int kslice) {
   __shared__ float as[kBK][kBM + 4];
   __shared__ float bs[kBK][kBN + 4];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+  const int k_begin = (int)blockIdx.z * kslice, k_end = min(K, k_begin + kslice);
+  if (gridDim.z > 1) {
+    C += (size_t)blockIdx.z * M * N;
+    ldc = N;
+  }
   float acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0.0f;
-  for (int k0 = 0; k0 < K; k0 += kBK) {
+  for (int k0 = k_begin; k0 < k_end; k0 += kBK) {
     // 64 x 16 of A and 16 x 64 of B, 4 elements a thread each.
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
@@ -58,7 +67,7 @@ gemm_kernel(int M, int N, int K, const TA* __restrict__ A, int lda, const TB* __
       }
       const int gm = m0 + mm, gk = k0 + kk;
       float v = 0.0f;
-      if (gm < M && gk < K) v = as_f32(TRA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk]);
+      if (gm < M && gk < k_end) v = as_f32(TRA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk]);
       as[kk][mm] = v;
       int nn, kb;
       if (TRB) {
@@ -70,7 +79,7 @@ gemm_kernel(int M, int N, int K, const TA* __restrict__ A, int lda, const TB* __
       }
       const int gn = n0 + nn, gkb = k0 + kb;
       float w = 0.0f;
-      if (gn < N && gkb < K) w = as_f32(TRB ? B[(size_t)gn * ldb + gkb] : B[(size_t)gkb * ldb + gn]);
+      if (gn < N && gkb < k_end) w = as_f32(TRB ? B[(size_t)gn * ldb + gkb] : B[(size_t)gkb * ldb + gn]);
       bs[kb][nn] = w;
     }
     __syncthreads();
@@ -105,14 +114,42 @@ gemm_kernel(int M, int N, int K, const TA* __restrict__ A, int lda, const TB* __
   }
 }
 
+// C (row stride ldc) = the sum of `splits` M x N slices (row stride N) in slice order.
+__global__ void split_sum_kernel(const float* part, int splits, int M, int N, float* C, int ldc) {
+  const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i >= (uint64_t)M * N) return;
+  float t = 0.0f;
+  for (int z = 0; z < splits; ++z) t += part[(uint64_t)z * M * N + i];
+  C[(i / N) * (uint64_t)ldc + i % N] = t;
+}
+
 template <class TA, class TB, bool TRA, bool TRB, int EPI>
 void gemm(int M, int N, int K, const TA* A, int lda, const TB* B, int ldb, float* C, int ldc,
           cudaStream_t s, const float* bias = nullptr, __nv_bfloat16* h = nullptr, int ldh = 0,
           const float* z = nullptr, int ldz = 0) {
   if (M == 0 || N == 0) return;
   dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM);
-  gemm_kernel<TA, TB, TRA, TRB, EPI><<<grid, kGemmThreads, 0, s>>>(M, N, K, A, lda, B, ldb, C, ldc,
-                                                                   bias, h, ldh, z, ldz);
+  // A long K over few output tiles (the weight gradients: K = the batch's rows) is split
+  // so that about two waves of CTAs run; the slices' partial sums are added in a fixed
+  // order, so the result is the same run to run.
+  int splits = 1;
+  if (EPI == kEpiStore) {
+    const int tiles = (int)(grid.x * grid.y);
+    while (tiles * splits < 256 && K / (splits * 2) >= 4 * kBK) splits *= 2;
+  }
+  const int kslice = ((K + splits - 1) / splits + kBK - 1) / kBK * kBK;
+  grid.z = splits;
+  if (splits == 1) {
+    gemm_kernel<TA, TB, TRA, TRB, EPI><<<grid, kGemmThreads, 0, s>>>(
+        M, N, K, A, lda, B, ldb, C, ldc, bias, h, ldh, z, ldz, K);
+    KG_LAUNCH_CHECK();
+    return;
+  }
+  DeviceBuffer<float> part((size_t)splits * M * N, s);
+  gemm_kernel<TA, TB, TRA, TRB, EPI><<<grid, kGemmThreads, 0, s>>>(
+      M, N, K, A, lda, B, ldb, part.ptr, N, bias, h, ldh, z, ldz, kslice);
+  KG_LAUNCH_CHECK();
+  split_sum_kernel<<<blocks_for((uint64_t)M * N, 256), 256, 0, s>>>(part.ptr, splits, M, N, C, ldc);
   KG_LAUNCH_CHECK();
 }
 
