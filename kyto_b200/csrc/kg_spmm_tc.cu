@@ -156,8 +156,10 @@ struct ValueMap {
   float unscale, sq_scale;
 };
 
-// One CTA per SM: up to 200 registers a thread (the drain warps hold 64 f64 sums).
-__global__ void __maxnreg__(200)
+// One CTA per SM. The register file is split over the SM's four sub-partitions, so ten
+// warps fit only at 168 registers a thread (three warps on two of them); the drain warps'
+// 64 f64 sums spill a little in the once-per-item epilogue.
+__global__ void __launch_bounds__(kSpThreads, 1)
 spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __restrict__ off,
                const uint8_t* __restrict__ data, uint64_t rows, Geometry geo, ValueMap vmap,
                const double* __restrict__ row_means, double out_scale, SpmmOut out,
