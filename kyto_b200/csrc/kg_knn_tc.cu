@@ -33,6 +33,8 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <string>
+#include <type_traits>
 #include <vector>
 
 #include "kg_internal.cuh"
@@ -72,12 +74,12 @@ struct TcSmem {
   float scratch[kEpiWarps * 32][33];  // a thread's 32 keys when some may pass
   float topk[kEpiWarps * 32][TcShape<KR, SUBS>::kTopK];  // a thread's k smallest keys
   uint64_t full[kStages], empty[kStages];
-  uint64_t tmem_full[2], tmem_empty[2];
+  uint64_t tmem_full[3], tmem_empty[3];  // per accumulator slot (two or three in use)
   uint64_t a_full, a_empty, drained;
   uint32_t stage_tile[kStages];      // the point tile in a stage, or kEndOfBlock
-  uint32_t acc_tile[2];              // the point tile in an accumulator, or kEndOfBlock
+  uint32_t acc_tile[3];              // the point tile in an accumulator slot, or kEndOfBlock
   uint32_t block_id[2];              // per block parity: the query block, or kNoBlock
-  uint32_t acc_block[2];             // the query block of an accumulator's item
+  uint32_t acc_block[3];             // the query block of a slot's item
   float u_max[2][kEpiWarps];         // per block parity and epilogue warp: the largest
                                      // threshold + s^2 |q|^2 of its queries
   uint32_t tmem_base;
@@ -249,8 +251,14 @@ __device__ __forceinline__ void tc_offer_chunk(QueryState& st, float* smallest, 
 }
 
 // KR: the register top-k width used on offers (k <= KR), or 0 for any k. SUBS: operand
-// sub-tiles (1: one fp16/bf16 product; 2: split, three fp16 products).
-template <int KR, int SUBS>
+// sub-tiles (1: one fp16/bf16 product; 2: split, three fp16 products). TA: the query
+// block's tiles are copied into tensor memory once per block (tcgen05.cp) and the MMAs
+// read A there, so each MMA reads only its point tile from shared memory (half the
+// operand bytes at N = 128); the accumulators are then three 128-column slots, one query
+// half each (a tile's two halves in consecutive slots), each released by its half's four
+// epilogue warps. Otherwise A is read from shared memory and the accumulators are two
+// slots of both halves (256 columns).
+template <int KR, int SUBS, bool TA>
 __global__ void __launch_bounds__(kTcThreads, 1)
 knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
                      const __grid_constant__ CUtensorMap tmap_p, FilterScan scan, uint32_t k,
@@ -270,15 +278,19 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
   const uint32_t n_tiles = (uint32_t)((n_p + kTcPoints - 1) / kTcPoints);
   volatile int* abort = &sm.abort;
 
+  // TMEM columns with TA: the query halves' A operands (32 columns a 64-wide sub-tile),
+  // then the three slots.
+  constexpr uint32_t kSlotBase = 64u * SUBS;
+  static_assert(!TA || kSlotBase + 3 * 128 <= kTmemCols, "filter TMEM columns");
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&sm.full[s], 1);
       mbar_init(&sm.empty[s], 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < (TA ? 3 : 2); ++b) {
       // Two arrivals: the MMA thread's own (releasing acc_tile) and the MMAs' commit.
       mbar_init(&sm.tmem_full[b], 2);
-      mbar_init(&sm.tmem_empty[b], kEpiWarps);
+      mbar_init(&sm.tmem_empty[b], TA ? kEpiWarps / 2 : kEpiWarps);
     }
     mbar_init(&sm.a_full, 1);
     mbar_init(&sm.a_empty, 1);
@@ -411,6 +423,99 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           __nanosleep(64);
       }
     }
+  } else if (warp == kEpiWarps + 1 && TA) {
+    // ------------------------------------------------- MMA issuer (A in TMEM) -------
+    if (lane == 0) {
+      uint64_t it = 0, item = 0;  // item: the slot sequence (two per tile, halves 0, 1)
+      uint32_t bi = 0;
+      bool ok = true;
+      auto next_slot = [&](uint32_t& sl) -> bool {
+        sl = (uint32_t)(item % 3);
+        return mbar_wait(&sm.tmem_empty[sl], (uint32_t)((item / 3) & 1) ^ 1, abort);
+      };
+      auto marker = [&](uint32_t block) -> bool {
+        for (int h = 0; h < 2; ++h) {
+          uint32_t sl;
+          if (!next_slot(sl)) return false;
+          sm.acc_tile[sl] = kEndOfBlock;
+          sm.acc_block[sl] = block;
+          mbar_arrive(&sm.tmem_full[sl]);
+          mbar_arrive(&sm.tmem_full[sl]);
+          ++item;
+        }
+        return true;
+      };
+      for (;; ++bi) {
+        if (!mbar_wait(&sm.a_full, bi & 1, abort)) break;
+        tc_fence_after();
+        const uint32_t qb = sm.block_id[bi & 1];
+        if (qb == kNoBlock) {
+          marker(kNoBlock);
+          break;
+        }
+        // The block's query tiles into TMEM (after the previous block's MMAs, in issue
+        // order); their shared memory goes back to the producer once the copies are done.
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int sub = 0; sub < SUBS; ++sub) {
+            const uint32_t asm_ = smem_addr(sm.a[h][sub]);
+            const uint32_t at = tmem + (uint32_t)(h * 32 * SUBS + sub * 32);
+#pragma unroll
+            for (int kk = 0; kk < kTcK / 16; ++kk)
+              tmem_cp_128x256b(at + kk * 8, desc_k_sw128(asm_ + kk * 32));
+          }
+        mma_commit(&sm.a_empty);
+        for (;; ++it) {
+          const int s = (int)(it % kStages);
+          const uint32_t ph = (uint32_t)((it / kStages) & 1);
+          if (!mbar_wait(&sm.full[s], ph, abort)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t pt = sm.stage_tile[s];
+          if (pt == kEndOfBlock) {
+            mbar_arrive(&sm.empty[s]);
+            ok = marker(qb);
+            ++it;
+            break;
+          }
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            uint32_t sl;
+            if (!next_slot(sl)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            sm.acc_tile[sl] = pt;
+            sm.acc_block[sl] = qb;
+            const uint32_t d = tmem + kSlotBase + sl * 128u;
+            // Products (A sub-tile, B sub-tile): (0, 0) alone, or for split operands
+            // (0, 0), (0, 1), (1, 0) (see below).
+#pragma unroll
+            for (int t = 0; t < (SUBS == 1 ? 1 : 3); ++t) {
+              const int sa = t == 2 ? 1 : 0, sb = t == 1 ? 1 : 0;
+              const uint32_t bsm = smem_addr(sm.b[s][sb]);
+              const uint32_t a = tmem + (uint32_t)(h * 32 * SUBS + sa * 32);
+#pragma unroll
+              for (int kk = 0; kk < kTcK / 16; ++kk)
+                mma_f16_ts(d, a + kk * 8, desc_k_sw128(bsm + kk * 32), idesc, (t | kk) > 0);
+            }
+            if (h == 1) mma_commit(&sm.empty[s]);
+            mbar_arrive(&sm.tmem_full[sl]);
+            mma_commit(&sm.tmem_full[sl]);
+            ++item;
+          }
+          if (!ok) break;
+        }
+        if (!ok) break;
+      }
+      // No product may still be running when TMEM is released.
+      mma_commit(&sm.drained);
+      for (uint32_t i = 0; i < kWaitPolls && !mbar_try_wait(&sm.drained, 0); ++i) __nanosleep(64);
+    }
   } else if (warp == kEpiWarps + 1) {
     // ------------------------------------------------------------ MMA issuer ------
     if (lane == 0) {
@@ -488,6 +593,22 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
     // overflow flag stay in registers; after offers the warp publishes its largest
     // threshold + s^2 |q|^2 for the producer's bound checks.
     const uint32_t half = (uint32_t)warp >> 2, quad = (uint32_t)warp & 3;
+    // The warp's i-th item: with TA, the half's slot sequence (items 2 i + half of the
+    // MMA warp's, three slots of 128 columns); else the two shared slots, this half's 128
+    // columns of each.
+    auto slot_of = [&](uint64_t i, uint32_t& sl, uint32_t& ph) {
+      if (TA) {
+        const uint64_t g = 2 * i + half;
+        sl = (uint32_t)(g % 3);
+        ph = (uint32_t)((g / 3) & 1);
+      } else {
+        sl = (uint32_t)(i & 1);
+        ph = (uint32_t)((i >> 1) & 1);
+      }
+    };
+    auto slot_cols = [&](uint32_t sl) -> uint32_t {
+      return TA ? kSlotBase + sl * 128u : sl * 256u + half * 128u;
+    };
     float* my = sm.scratch[threadIdx.x];
     float local_smallest[KR == 0 ? kMaxK : 1];
     float* smallest = KR == 0 ? local_smallest : sm.topk[threadIdx.x];
@@ -497,15 +618,18 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
     for (;; ++bi) {
       // The block's first item names the block (or the end of the CTA's work).
       {
-        const uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
+        uint32_t ab, aph;
+        slot_of(it, ab, aph);
         if (!mbar_wait(&sm.tmem_full[ab], aph, abort)) break;
       }
       tc_fence_after();
       __syncwarp();
-      const uint32_t qb32 = sm.acc_block[(uint32_t)(it & 1)];
+      uint32_t first_slot, first_ph;
+      slot_of(it, first_slot, first_ph);
+      const uint32_t qb32 = sm.acc_block[first_slot];
       if (qb32 == kNoBlock) {
         __syncwarp();
-        if (lane == 0) mbar_arrive(&sm.tmem_empty[(uint32_t)(it & 1)]);
+        if (lane == 0) mbar_arrive(&sm.tmem_empty[first_slot]);
         ++it;
         break;
       }
@@ -530,7 +654,8 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
       float* ck = cand_key + (active ? q : 0) * (uint64_t)cap;
       uint32_t* cr = cand_row + (active ? q : 0) * (uint64_t)cap;
       for (bool first = true;; ++it, first = false) {
-        const uint32_t ab = (uint32_t)(it & 1), aph = (uint32_t)((it >> 1) & 1);
+        uint32_t ab, aph;
+        slot_of(it, ab, aph);
         if (!first) {
           if (!mbar_wait(&sm.tmem_full[ab], aph, abort)) {
             ok = false;
@@ -546,7 +671,7 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           ++it;
           break;
         }
-        const uint32_t base = tmem + ((quad * 32u) << 16) + ab * 256u + half * 128u;
+        const uint32_t base = tmem + ((quad * 32u) << 16) + slot_cols(ab);
         // All 128 keys into registers with one wait; the accumulator goes back to the
         // MMA warp at once.
         uint32_t r[kTcPoints / 32][32];
@@ -817,19 +942,26 @@ uint32_t filter_query_block(FilterKind) { return kTcQueryBlock; }
 
 namespace {
 
-template <int KR, int SUBS>
+template <int KR, int SUBS, bool TA>
 void launch_filter(unsigned grid, cudaStream_t s, const CUtensorMap& mq, const CUtensorMap& mp,
                    const FilterScan& scan, uint32_t k, const float* slack2, uint32_t idesc,
                    uint32_t cap, float* cand_key, uint32_t* cand_row, uint32_t* cand_count,
                    float* threshold, int* err) {
   static std::once_flag attr;
   std::call_once(attr, [] {
-    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<KR, SUBS>,
+    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<KR, SUBS, TA>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)tc_smem_bytes<KR, SUBS>()));
   });
-  knn_filter_tc_kernel<KR, SUBS><<<grid, kTcThreads, tc_smem_bytes<KR, SUBS>(), s>>>(
+  knn_filter_tc_kernel<KR, SUBS, TA><<<grid, kTcThreads, tc_smem_bytes<KR, SUBS>(), s>>>(
       mq, mp, scan, k, slack2, idesc, cap, cand_key, cand_row, cand_count, threshold, err);
+}
+
+// The filter's query operand: in tensor memory (the default) or read from shared memory
+// by every MMA (KYTO_GPU_FILTER_A=smem); both give the same keys.
+bool filter_a_in_tmem() {
+  const char* v = std::getenv("KYTO_GPU_FILTER_A");
+  return !(v && std::string(v) == "smem");
 }
 
 }  // namespace
@@ -898,9 +1030,13 @@ void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint32_t width, uint
   const unsigned grid = (unsigned)std::min<uint64_t>(n_qblocks, (uint64_t)ctx->sm_count);
   const uint32_t idesc = idesc_f32acc(bf16 ? 1u : 0u, 128, kTcPoints);
   const int kr = k <= 16 ? 16 : k <= 32 ? 32 : 0;
-  auto launch = kr == 16 ? (split ? launch_filter<16, 2> : launch_filter<16, 1>)
-                : kr == 32 ? (split ? launch_filter<32, 2> : launch_filter<32, 1>)
-                           : (split ? launch_filter<0, 2> : launch_filter<0, 1>);
+  auto pick = [&](auto ta) {
+    constexpr bool TA = decltype(ta)::value;
+    return kr == 16 ? (split ? launch_filter<16, 2, TA> : launch_filter<16, 1, TA>)
+           : kr == 32 ? (split ? launch_filter<32, 2, TA> : launch_filter<32, 1, TA>)
+                      : (split ? launch_filter<0, 2, TA> : launch_filter<0, 1, TA>);
+  };
+  auto launch = filter_a_in_tmem() ? pick(std::true_type{}) : pick(std::false_type{});
   launch(grid, s, mq, mp, scan, k, slack2.ptr, idesc, cap, cand_key, cand_row, cand_count,
          threshold, err.ptr);
   KG_LAUNCH_CHECK();

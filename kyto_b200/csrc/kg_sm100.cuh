@@ -162,6 +162,14 @@ __device__ __forceinline__ void mma_f16_ts(uint32_t d_tmem, uint32_t a_tmem, uin
       : "memory");
 }
 
+// Copy a 128-row x 32-byte slice of a shared-memory operand (described by `sdesc`, as an
+// MMA would read it) into TMEM at taddr: row r to lane r, its 32 bytes (16 16-bit
+// elements, in K order) to 8 consecutive 32-bit columns. Asynchronous, in issue order with
+// the thread's MMAs; tcgen05.commit tracks its completion.
+__device__ __forceinline__ void tmem_cp_128x256b(uint32_t taddr, uint64_t sdesc) {
+  asm volatile("tcgen05.cp.cta_group::1.128x256b [%0], %1;" ::"r"(taddr), "l"(sdesc) : "memory");
+}
+
 // Arrive on `bar` once every tcgen05 operation this thread issued so far completes.
 __device__ __forceinline__ void mma_commit(uint64_t* bar) {
   asm volatile(

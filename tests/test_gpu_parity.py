@@ -442,3 +442,25 @@ def test_connectivities_refusals(ctx):
                 np.ones(4, dtype=np.float32))
     with pytest.raises(K.KytoError):
         K.connectivities(g, ctx=ctx)  # columns not increasing in row 1
+
+
+@pytest.mark.parametrize("candidate_filter", ["fp16", "split", "bf16"])
+def test_filter_query_operand_in_tmem_or_smem_gives_the_same_keys(ctx, monkeypatch,
+                                                                  candidate_filter):
+    # The filter's MMAs read the query tiles from tensor memory (copied once per block) or
+    # from shared memory: the same products, so the same approximate keys, candidates,
+    # full-row searches and graph bits; and on ordinary data no row needs a full search.
+    monkeypatch.setenv("KYTO_GPU_KNN_FILTER", candidate_filter)
+    x, _ = synthetic.gaussian_mixture(60_000, dim=50, n_components=40, seed=21, device="cpu")
+    monkeypatch.setenv("KYTO_GPU_FILTER_A", "smem")
+    a = K.neighbors(x, 15, ctx=ctx)
+    monkeypatch.setenv("KYTO_GPU_FILTER_A", "tmem")
+    b = K.neighbors(x, 15, ctx=ctx)
+    assert np.array_equal(a.indices, b.indices)
+    assert np.array_equal(a.distances.view(np.uint32), b.distances.view(np.uint32))
+    assert a.stats.candidates == b.stats.candidates
+    assert a.stats.rows_full == b.stats.rows_full == 0
+    o = O.neighbors(x[:5000], 15, method="exact")
+    c = K.neighbors(x[:5000], 15, ctx=ctx)
+    assert np.array_equal(c.indices, o.indices)
+    assert np.array_equal(c.distances.view(np.uint32), o.distances.view(np.uint32))
