@@ -893,7 +893,7 @@ __global__ void retry_slots_kernel(const uint32_t* slots, uint64_t m, const uint
 namespace {
 
 struct Timer {
-  cudaEvent_t a, b;
+  cudaEvent_t a = nullptr, b = nullptr;
   cudaStream_t s;
   explicit Timer(cudaStream_t st) : s(st) {
     KG_CUDA(cudaEventCreate(&a));
@@ -905,10 +905,14 @@ struct Timer {
     KG_CUDA(cudaEventSynchronize(b));
     float ms = 0;
     KG_CUDA(cudaEventElapsedTime(&ms, a, b));
-    cudaEventDestroy(a);
-    cudaEventDestroy(b);
     return ms;
   }
+  ~Timer() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+  Timer(const Timer&) = delete;
+  Timer& operator=(const Timer&) = delete;
 };
 
 }  // namespace

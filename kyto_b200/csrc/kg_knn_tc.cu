@@ -60,9 +60,8 @@ constexpr uint32_t kNoBlock = 0xFFFFFFFFu;  // no query block left: the CTA's ro
 // register top-k width (16, 32) or 0 (the k smallest in local memory, any k).
 template <int KR, int SUBS>
 struct TcShape {
-  // Point-tile stages: as many as shared memory holds beside the query tiles, the
-  // scratch rows and the top-k rows (KR == 0 keeps its k smallest in local memory).
-  static constexpr int kStages = SUBS == 1 ? (KR == 32 ? 7 : 8) : (KR == 32 ? 2 : 3);
+  // Point-tile stages (six measured faster than eight on the 1M benchmark embedding).
+  static constexpr int kStages = SUBS == 1 ? 6 : (KR == 32 ? 2 : 3);
   static constexpr int kTopK = KR == 0 ? 1 : KR + 1;  // odd row stride: no bank conflicts
 };
 
@@ -1041,9 +1040,11 @@ void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint32_t width, uint
          threshold, err.ptr);
   KG_LAUNCH_CHECK();
   if (trace) trace->mark("filter kernel");
+  // The bounded host wait first: a copy into h_err must never outlive this frame.
+  wait_stream(ctx, s);
   int h_err = 0;
   KG_CUDA(cudaMemcpyAsync(&h_err, err.ptr, 4, cudaMemcpyDeviceToHost, s));
-  wait_stream(ctx, s);
+  KG_CUDA(cudaStreamSynchronize(s));
   if (h_err) fail(KG_ERR_TIMEOUT, "the tensor-core kNN filter gave up waiting on its pipeline");
   if (trace_on() && scan.tiles_scanned) {
     unsigned long long h_tiles = 0;

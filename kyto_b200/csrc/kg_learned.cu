@@ -249,7 +249,7 @@ int bits_for_value(uint64_t v) {
 void learned_probe(const Mlp& mlp, const float* x, uint64_t n, uint32_t width, uint32_t probe,
                    const float* temps, uint32_t n_temps, uint32_t* top, float* conf,
                    cudaStream_t s, uint32_t n_mass = 0, uint16_t* mass_part = nullptr,
-                   float* mass_prob = nullptr) {
+                   float* mass_prob = nullptr, Trace* trace = nullptr) {
   const uint64_t chunk = 65536;
   MlpBatch b;
   b.alloc(mlp.sh, (uint32_t)std::min<uint64_t>(chunk, n), s);
@@ -257,9 +257,11 @@ void learned_probe(const Mlp& mlp, const float* x, uint64_t n, uint32_t width, u
     const uint32_t rows = (uint32_t)std::min<uint64_t>(chunk, n - r0);
     b.rows = rows;
     mlp.forward(x + r0 * width, width, b, s);
+    if (trace) trace->mark("index forward");
     top_parts(b.z3.ptr, rows, mlp.sh.parts, probe, top + r0 * probe, conf + r0, n, s, temps,
               n_temps, n_mass, mass_part ? mass_part + r0 * n_mass : nullptr,
               mass_prob ? mass_prob + r0 * n_mass : nullptr);
+    if (trace) trace->mark("index top parts");
   }
 }
 
@@ -548,8 +550,9 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
     DeviceBuffer<uint16_t> mass_part(n * n_mass, s);
     DeviceBuffer<float> mass_prob(n * n_mass, s);
     KG_CUDA(cudaMemcpyAsync(d_temps.ptr, &temperature, 4, cudaMemcpyHostToDevice, s));
+    trace.mark("index setup");
     learned_probe(mlp, x, n, width, probe, d_temps.ptr, 1, top.ptr, conf.ptr, s, n_mass,
-                  mass_part.ptr, mass_prob.ptr);
+                  mass_part.ptr, mass_prob.ptr, &trace);
     mlp.check(s);
     KG_CUDA(cudaStreamSynchronize(s));
     const double index_ms = ms_since(t_index);

@@ -1960,9 +1960,10 @@ kg_status kg_diag_spmm(kg_ctx* ctx, const uint64_t* indptr, const uint32_t* indi
         partial.ptr, (uint32_t)segs, (uint32_t)rows, width, res.ptr);
     KG_LAUNCH_CHECK();
     KG_CUDA(cudaMemcpyAsync(out, res.ptr, rows * width * 8, cudaMemcpyDefault, s));
-    int h_err = 0;
-    KG_CUDA(cudaMemcpyAsync(&h_err, err.ptr, 4, cudaMemcpyDeviceToHost, s));
     wait_stream(ctx, s);
+    int h_err = 0;  // read after the bounded wait: no copy outlives this frame
+    KG_CUDA(cudaMemcpyAsync(&h_err, err.ptr, 4, cudaMemcpyDeviceToHost, s));
+    KG_CUDA(cudaStreamSynchronize(s));
     if (h_err) fail(KG_ERR_TIMEOUT, "the tensor-core product gave up waiting on its pipeline");
   });
 }
