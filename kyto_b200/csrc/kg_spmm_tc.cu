@@ -251,29 +251,34 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
         // Row (32 q + lane) of the A tiles: for each column, the value at its rank if the
         // row stores one (lanes that do read consecutive words; the others read a
         // neighbour's and drop it), two columns a word, hi parts then lo parts.
-        uint32_t words[32];
-#pragma unroll
-        for (int c2 = 0; c2 < 16; ++c2) {
-          const uint4 mm = meta4[c2];  // (mask, rank) of columns 2 c2 and 2 c2 + 1
-          uint32_t x0 = vals[mm.y + __popc(mm.x & lt)];
-          uint32_t x1 = vals[mm.w + __popc(mm.z & lt)];
-          const bool h0 = (mm.x >> lane) & 1u, h1 = (mm.z >> lane) & 1u;
-          if (vmap.mode == kValueOne) {
-            x0 = 0x3C00u;  // fp16 1.0, low part 0
-            x1 = 0x3C00u;
-          } else if (vmap.mode == kValueCentredSquare) {
-            const float d0 = pair_value(x0) * vmap.unscale - mean_r;
-            const float d1 = pair_value(x1) * vmap.unscale - mean_r;
-            x0 = split_pair(d0 * d0 * vmap.sq_scale);
-            x1 = split_pair(d1 * d1 * vmap.sq_scale);
-          }
-          x0 = h0 ? x0 : 0u;
-          x1 = h1 ? x1 : 0u;
-          words[c2] = __byte_perm(x0, x1, 0x5410);       // hi parts of both columns
-          words[16 + c2] = __byte_perm(x0, x1, 0x7632);  // lo parts
-        }
+        // Two halves of 8 column pairs each: hi words to columns 8 h.., lo words to 16 + 8 h..
         const uint32_t arow = tmem + ((q * 32u) << 16) + kABase + ab * kACols;
-        tmem_st_32(arow, words);
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh) {
+          uint32_t hw[8], lw[8];
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const uint4 mm = meta4[8 * hh + i];  // (mask, rank) of columns 2 c2, 2 c2 + 1
+            uint32_t x0 = vals[mm.y + __popc(mm.x & lt)];
+            uint32_t x1 = vals[mm.w + __popc(mm.z & lt)];
+            const bool h0 = (mm.x >> lane) & 1u, h1 = (mm.z >> lane) & 1u;
+            if (vmap.mode == kValueOne) {
+              x0 = 0x3C00u;  // fp16 1.0, low part 0
+              x1 = 0x3C00u;
+            } else if (vmap.mode == kValueCentredSquare) {
+              const float d0 = pair_value(x0) * vmap.unscale - mean_r;
+              const float d1 = pair_value(x1) * vmap.unscale - mean_r;
+              x0 = split_pair(d0 * d0 * vmap.sq_scale);
+              x1 = split_pair(d1 * d1 * vmap.sq_scale);
+            }
+            x0 = h0 ? x0 : 0u;
+            x1 = h1 ? x1 : 0u;
+            hw[i] = __byte_perm(x0, x1, 0x5410);  // hi parts of both columns
+            lw[i] = __byte_perm(x0, x1, 0x7632);  // lo parts
+          }
+          tmem_st_8(arow + 8u * hh, hw);
+          tmem_st_8(arow + 16u + 8u * hh, lw);
+        }
         tmem_wait_st();
         tc_fence_before();
         __syncwarp();  // every lane has read meta before the next block rewrites it
@@ -306,14 +311,14 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
         }
         tc_fence_after();
         __syncwarp();
-        // One 32-column half at a time (fewer live registers beside the f64 sums).
+        // 16 columns at a time (few live registers beside the 64 f64 sums).
 #pragma unroll
-        for (int hf = 0; hf < 2; ++hf) {
-          uint32_t rr[32];
-          tmem_ld_32(tmem + ((quad * 32u) << 16) + b * kAccCols + hf * 32u, rr);
+        for (int hf = 0; hf < 4; ++hf) {
+          uint32_t rr[16];
+          tmem_ld_16(tmem + ((quad * 32u) << 16) + b * kAccCols + hf * 16u, rr);
           tmem_wait_ld();
 #pragma unroll
-          for (int j = 0; j < 32; ++j) acc[hf * 32 + j] += (double)__uint_as_float(rr[j]);
+          for (int j = 0; j < 16; ++j) acc[hf * 16 + j] += (double)__uint_as_float(rr[j]);
         }
         tc_fence_before();
         __syncwarp();
