@@ -1231,6 +1231,9 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
     unsigned int h_over = 0;
     KG_CUDA(cudaMemcpyAsync(&h_over, n_over.ptr, 4, cudaMemcpyDeviceToHost, s));
     KG_CUDA(cudaStreamSynchronize(s));
+    if (trace_on())
+      std::fprintf(stderr, "[kyto_gpu trace] filter: %u of %llu queries overflowed (retried)\n",
+                   h_over, (unsigned long long)n);
     for (uint64_t r0 = 0; r0 < h_over; r0 += kTcRetryChunk) {
       check_cancel(ctx);
       const uint64_t m = std::min<uint64_t>(kTcRetryChunk, h_over - r0);
