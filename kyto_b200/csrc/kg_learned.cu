@@ -265,6 +265,28 @@ void learned_probe(const Mlp& mlp, const float* x, uint64_t n, uint32_t width, u
   }
 }
 
+// loss[t] = - sum over i of cov_i log p_ti + (1 - cov_i) log(1 - p_ti), p clamped to
+// [1e-6, 1 - 1e-6], in f64: one CTA per temperature, each thread a fixed stride of rows,
+// then a fixed tree (the same bits run to run).
+__global__ void __launch_bounds__(256)
+calibration_loss_kernel(const float* conf, const float* cov, uint64_t m, double* loss) {
+  __shared__ double part[256];
+  const uint32_t t = blockIdx.x;
+  double acc = 0.0;
+  for (uint64_t i = threadIdx.x; i < m; i += blockDim.x) {
+    const double p = fmin(fmax((double)conf[t * m + i], 1e-6), 1.0 - 1e-6);
+    const double c = (double)cov[i];
+    acc -= c * log(p) + (1.0 - c) * log1p(-p);
+  }
+  part[threadIdx.x] = acc;
+  __syncthreads();
+  for (uint32_t o = blockDim.x / 2; o; o >>= 1) {
+    if (threadIdx.x < o) part[threadIdx.x] += part[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) loss[t] = part[0];
+}
+
 // covered[i] = the share of sample row i's k graph neighbours that live in a part row i
 // probes (a row lives in its top part): what the confidence should predict.
 __global__ void covered_kernel(const uint32_t* top, uint32_t probe, const uint32_t* nbr,
@@ -521,20 +543,16 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
       covered_kernel<<<blocks_for(m, 256), 256, 0, s>>>(stop.ptr, probe, sg.row.ptr, m, k,
                                                         cov.ptr);
       KG_LAUNCH_CHECK();
-      std::vector<float> hconf(kNumTemps * m), hcov(m);
-      KG_CUDA(cudaMemcpyAsync(hconf.data(), sconf.ptr, hconf.size() * 4, cudaMemcpyDeviceToHost,
-                              s));
-      KG_CUDA(cudaMemcpyAsync(hcov.data(), cov.ptr, m * 4, cudaMemcpyDeviceToHost, s));
+      DeviceBuffer<double> dloss(kNumTemps, s);
+      calibration_loss_kernel<<<kNumTemps, 256, 0, s>>>(sconf.ptr, cov.ptr, m, dloss.ptr);
+      KG_LAUNCH_CHECK();
+      double hloss[kNumTemps];
+      KG_CUDA(cudaMemcpyAsync(hloss, dloss.ptr, sizeof hloss, cudaMemcpyDeviceToHost, s));
       KG_CUDA(cudaStreamSynchronize(s));
       double best = INFINITY;
       for (uint32_t t = 0; t < kNumTemps; ++t) {
-        double loss = 0.0;
-        for (uint64_t i = 0; i < m; ++i) {
-          const double p = std::min(std::max((double)hconf[t * m + i], 1e-6), 1.0 - 1e-6);
-          loss -= hcov[i] * std::log(p) + (1.0 - hcov[i]) * std::log1p(-p);
-        }
-        if (loss < best) {
-          best = loss;
+        if (hloss[t] < best) {
+          best = hloss[t];
           temperature = kTemps[t];
         }
       }
