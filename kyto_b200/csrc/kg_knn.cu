@@ -11,6 +11,8 @@
 //     (too many, or an approximate key outside its slack) is flagged;
 //  3. full rows: flagged rows searched against every row with exact keys.
 // So every row is the CPU's brute-force row, bit for bit.
+#include <cub/device/device_select.cuh>
+#include <cub/iterator/counting_input_iterator.cuh>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 #include <cub/device/device_segmented_radix_sort.cuh>
@@ -871,11 +873,10 @@ __global__ void compact_flags_kernel(const uint32_t* flag, uint64_t n, uint32_t*
   if (r < n && flag[r]) list[atomicAdd(count, 1u)] = (uint32_t)r;
 }
 
-// The query slots whose candidates overflowed.
-__global__ void overflow_slots_kernel(const uint32_t* cand_count, uint64_t n, uint32_t* list,
-                                      unsigned int* count) {
+// Whether each query slot's candidates overflowed (1) or not (0).
+__global__ void overflow_flags_kernel(const uint32_t* cand_count, uint64_t n, uint8_t* flag) {
   uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (q < n && cand_count[q] == kOverflow) list[atomicAdd(count, 1u)] = (uint32_t)q;
+  if (q < n) flag[q] = cand_count[q] == kOverflow ? 1 : 0;
 }
 
 // The retry's query slots: retry slot j is slot slots[j] of the first pass.
@@ -1225,9 +1226,20 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
     DeviceBuffer<uint32_t> over(n, s);
     DeviceBuffer<unsigned int> n_over(1, s);
     n_over.zero();
-    overflow_slots_kernel<<<blocks_for(n, 256), 256, 0, s>>>(cand_count.ptr, n, over.ptr,
-                                                             n_over.ptr);
-    KG_LAUNCH_CHECK();
+    {
+      // The overflowed slots in slot order (a stable compaction: the retry's blocks, and
+      // with them every count the search reports, are the same run to run).
+      DeviceBuffer<uint8_t> oflag(n, s);
+      overflow_flags_kernel<<<blocks_for(n, 256), 256, 0, s>>>(cand_count.ptr, n, oflag.ptr);
+      KG_LAUNCH_CHECK();
+      cub::CountingInputIterator<uint32_t> slots(0);
+      size_t tb = 0;
+      KG_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, slots, oflag.ptr, over.ptr, n_over.ptr,
+                                         (int64_t)n, s));
+      DeviceBuffer<unsigned char> tmp(tb, s);
+      KG_CUDA(cub::DeviceSelect::Flagged(tmp.ptr, tb, slots, oflag.ptr, over.ptr, n_over.ptr,
+                                         (int64_t)n, s));
+    }
     unsigned int h_over = 0;
     KG_CUDA(cudaMemcpyAsync(&h_over, n_over.ptr, 4, cudaMemcpyDeviceToHost, s));
     KG_CUDA(cudaStreamSynchronize(s));

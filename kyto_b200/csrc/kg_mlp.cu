@@ -649,10 +649,16 @@ void Mlp::adam(float lr, cudaStream_t s) {
 // looks again. Parts, probabilities and sums come out in the same order and bits as
 // top_parts_kernel's.
 constexpr uint32_t kRegParts = 32;  // parts a lane holds
-__global__ void top_parts_reg_kernel(const float* z, uint64_t rows, uint32_t parts,
-                                     uint32_t probe, const float* temps, uint32_t n_temps,
-                                     uint32_t* top, float* conf, uint64_t conf_stride,
-                                     uint32_t n_mass, uint16_t* mass_part, float* mass_prob) {
+__device__ __forceinline__ uint32_t order_key(float v) {
+  const uint32_t b = __float_as_uint(v);
+  return b ^ ((b >> 31) ? 0xFFFFFFFFu : 0x80000000u);  // unsigned order = float order
+}
+
+__global__ void __launch_bounds__(256)
+top_parts_reg_kernel(const float* z, uint64_t rows, uint32_t parts, uint32_t probe,
+                     const float* temps, uint32_t n_temps, uint32_t* top, float* conf,
+                     uint64_t conf_stride, uint32_t n_mass, uint16_t* mass_part,
+                     float* mass_prob) {
   const uint64_t row = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const unsigned lane = threadIdx.x & 31u;
   if (row >= rows) return;
@@ -665,8 +671,7 @@ __global__ void top_parts_reg_kernel(const float* z, uint64_t rows, uint32_t par
   }
   float m = -INFINITY;
 #pragma unroll
-  for (uint32_t j = 0; j < kRegParts; ++j)
-    if (lane + 32 * j < parts) m = fmaxf(m, v[j]);
+  for (uint32_t j = 0; j < kRegParts; ++j) m = fmaxf(m, v[j]);
   for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
   auto lane_sum = [&](float t) {
     float sum = 0.0f;
@@ -677,51 +682,92 @@ __global__ void top_parts_reg_kernel(const float* z, uint64_t rows, uint32_t par
     return sum;
   };
   const float sum0 = n_mass ? lane_sum(temps[0]) : 0.0f;
-  // The lane's best part not yet taken: (value, slot j), the lowest slot on ties.
+  // The lane's four best parts not yet taken, best first (value, then the lower slot on
+  // ties), kept sorted; refilled from every slot when they run out.
   uint32_t taken = 0;
-  auto lane_best = [&](float& bv, uint32_t& bj) {
-    bv = -INFINITY;
-    bj = 0xFFFFFFFFu;
+  float cv[4];
+  uint32_t cj[4];
+  auto refill = [&]() {
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      cv[i] = -INFINITY;
+      cj[i] = 0xFFFFFFFFu;
+    }
 #pragma unroll
     for (uint32_t j = 0; j < kRegParts; ++j) {
-      const bool live = lane + 32 * j < parts && !((taken >> j) & 1u);
-      if (live && (v[j] > bv || bj == 0xFFFFFFFFu)) {
-        bv = v[j];
-        bj = j;
+      if (lane + 32 * j >= parts || ((taken >> j) & 1u)) continue;
+      float x = v[j];
+      uint32_t xj = j;
+      // Insert (strictly greater moves ahead: an earlier slot stays ahead on ties).
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const bool ahead = cj[i] == 0xFFFFFFFFu || x > cv[i];
+        const float tv = cv[i];
+        const uint32_t tj = cj[i];
+        cv[i] = ahead ? x : cv[i];
+        cj[i] = ahead ? xj : cj[i];
+        x = ahead ? tv : x;
+        xj = ahead ? tj : xj;
       }
     }
   };
-  float lv;
-  uint32_t lj;
-  lane_best(lv, lj);
+  refill();
   float picked[kMaxTemps];
-  for (uint32_t t = 0; t < n_temps; ++t) picked[t] = 0.0f;
+#pragma unroll
+  for (uint32_t t = 0; t < kMaxTemps; ++t) picked[t] = 0.0f;
+  // Round t's part and value are kept by lane t % 32 (rounds 32..63 in the second pair).
+  uint32_t my_part0 = 0u, my_part1 = 0u;
+  float my_val0 = 0.0f, my_val1 = 0.0f;
   const uint32_t rounds = max(probe, n_mass);
   for (uint32_t t = 0; t < rounds; ++t) {
-    float bv = lv;
-    uint32_t bp = lj == 0xFFFFFFFFu ? 0xFFFFFFFFu : lane + 32 * lj;
-    for (int o = 16; o; o >>= 1) {
-      const float ov = __shfl_xor_sync(0xFFFFFFFFu, bv, o);
-      const uint32_t op = __shfl_xor_sync(0xFFFFFFFFu, bp, o);
-      if (op != 0xFFFFFFFFu && (bp == 0xFFFFFFFFu || ov > bv || (ov == bv && op < bp))) {
-        bv = ov;
-        bp = op;
+    // The warp's best: the largest value, then the lowest part among the lanes with it.
+    const bool live = cj[0] != 0xFFFFFFFFu;
+    const uint32_t key = live ? order_key(cv[0]) : 0u;
+    const uint32_t kmax = __reduce_max_sync(0xFFFFFFFFu, key);
+    const uint32_t mine = (live && key == kmax) ? lane + 32 * cj[0] : 0xFFFFFFFFu;
+    const uint32_t bp = __reduce_min_sync(0xFFFFFFFFu, mine);
+    const float bv = __shfl_sync(0xFFFFFFFFu, cv[0], bp & 31u);
+    if ((t & 31u) == lane) {
+      if (t < 32) {
+        my_part0 = bp;
+        my_val0 = bv;
+      } else {
+        my_part1 = bp;
+        my_val1 = bv;
       }
     }
-    if (t < n_mass && lane == 0) {
-      mass_part[row * n_mass + t] = (uint16_t)bp;
-      mass_prob[row * n_mass + t] = __expf(temps[0] * (bv - m)) / sum0;
-    }
     if (t < probe) {
-      if (lane == 0) top[row * probe + t] = bp;
-      for (uint32_t i = 0; i < n_temps; ++i) picked[i] += __expf(temps[i] * (bv - m));
+#pragma unroll
+      for (uint32_t i = 0; i < kMaxTemps; ++i)
+        if (i < n_temps) picked[i] += __expf(temps[i] * (bv - m));
     }
-    if (bp != 0xFFFFFFFFu && bp % 32 == lane) {
+    if (bp % 32 == lane) {
       taken |= 1u << (bp / 32);
-      lane_best(lv, lj);
+      cv[0] = cv[1];
+      cj[0] = cj[1];
+      cv[1] = cv[2];
+      cj[1] = cj[2];
+      cv[2] = cv[3];
+      cj[2] = cj[3];
+      cv[3] = -INFINITY;
+      cj[3] = 0xFFFFFFFFu;
+      if (cj[0] == 0xFFFFFFFFu) refill();
     }
   }
-  for (uint32_t i = 0; i < n_temps; ++i) {
+#pragma unroll
+  for (uint32_t h = 0; h < 2; ++h) {
+    const uint32_t t = lane + 32 * h;
+    const uint32_t part = h ? my_part1 : my_part0;
+    const float val = h ? my_val1 : my_val0;
+    if (t < probe) top[row * probe + t] = part;
+    if (t < n_mass) {
+      mass_part[row * n_mass + t] = (uint16_t)part;
+      mass_prob[row * n_mass + t] = __expf(temps[0] * (val - m)) / sum0;
+    }
+  }
+#pragma unroll
+  for (uint32_t i = 0; i < kMaxTemps; ++i) {
+    if (i >= n_temps) break;
     const float sum = lane_sum(temps[i]);
     if (lane == 0) conf[i * conf_stride + row] = picked[i] / sum;
   }
