@@ -879,16 +879,88 @@ __global__ void overflow_flags_kernel(const uint32_t* cand_count, uint64_t n, ui
   if (q < n) flag[q] = cand_count[q] == kOverflow ? 1 : 0;
 }
 
+// Slots whose list does not cover their row: marked overflowed, so they are searched
+// over every tile with the overflowed queries.
+__global__ void force_overflow_kernel(const uint8_t* q_full, uint64_t n, uint32_t* cand_count) {
+  const uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (q < n && q_full[q]) cand_count[q] = kOverflow;
+}
+
 // The retry's query slots: retry slot j is slot slots[j] of the first pass.
-__global__ void retry_slots_kernel(const uint32_t* slots, uint64_t m, const uint32_t* qrows,
+// The retry's query slots: `copies` copies of the m overflowed slots, each padded to mq
+// slots (a whole number of query blocks) by repeating the last; copy c scans its own
+// range of the point tiles.
+__global__ void retry_slots_kernel(const uint32_t* slots, uint64_t m, uint64_t mq,
+                                   uint32_t copies, const uint32_t* qrows,
                                    const uint32_t* q_point, const uint32_t* slot_sample,
                                    uint32_t* r_qrows, uint32_t* r_qpoint, uint32_t* r_sample) {
-  uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (v >= mq * copies) return;
+  const uint64_t j = v % mq;
+  const uint32_t q = slots[j < m ? j : m - 1];
+  r_qrows[v] = qrows[q];
+  r_qpoint[v] = q_point ? q_point[q] : q;
+  if (slot_sample) r_sample[v] = slot_sample[q];
+}
+
+// The retry's tile lists: block b = c * nb + j (copy c, query block j) scans the tiles
+// [c * n_tiles / copies, (c + 1) * n_tiles / copies). One CTA per block.
+__global__ void retry_lists_kernel(uint64_t nb, uint32_t copies, uint32_t n_tiles,
+                                   uint64_t* off, uint32_t* list) {
+  const uint64_t b = blockIdx.x;
+  const uint64_t c = b / nb, j = b % nb;
+  const uint32_t t0 = (uint32_t)(c * n_tiles / copies), t1 = (uint32_t)((c + 1) * n_tiles / copies);
+  // The copies before c hold nb blocks of their own range each: nb * t0 entries.
+  const uint64_t o = nb * (uint64_t)t0 + j * (uint64_t)(t1 - t0);
+  if (threadIdx.x == 0) {
+    off[b] = o;
+    if (b + 1 == nb * copies) off[b + 1] = nb * (uint64_t)n_tiles;
+  }
+  for (uint32_t t = t0 + threadIdx.x; t < t1; t += blockDim.x) list[o + (t - t0)] = t;
+}
+
+// One warp per overflowed query j: its copies' candidates merged into one slice of `cap`
+// slots. The merged threshold is the smallest copy's: every copy kept each of its points
+// whose key is at most its own threshold (at least the smallest), and the copy with the
+// smallest threshold holds k keys below it; so the keys at most the smallest threshold,
+// over all copies, are what one pass over every tile would keep. Any copy overflowed, or
+// more than `cap` merged keys: the query overflows again.
+__global__ void retry_merge_kernel(uint64_t m, uint64_t mq, uint32_t copies, uint32_t copy_cap,
+                                   const float* key, const uint32_t* row, const uint32_t* count,
+                                   const float* thr, uint32_t cap, float* m_key,
+                                   uint32_t* m_row, uint32_t* m_count, float* m_thr) {
+  const uint64_t j = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
   if (j >= m) return;
-  const uint32_t q = slots[j];
-  r_qrows[j] = qrows[q];
-  r_qpoint[j] = q_point ? q_point[q] : q;
-  if (slot_sample) r_sample[j] = slot_sample[q];
+  float th = INFINITY;
+  bool over = false;
+  for (uint32_t c = 0; c < copies; ++c) {
+    const uint64_t v = c * mq + j;
+    over |= count[v] == kOverflow;
+    th = fminf(th, thr[v]);
+  }
+  uint32_t n_out = 0;
+  const unsigned lt = (1u << lane) - 1u;
+  for (uint32_t c = 0; c < copies && !over; ++c) {
+    const uint64_t v = c * mq + j;
+    const uint32_t cnt = count[v];
+    for (uint32_t i0 = 0; i0 < cnt; i0 += 32) {
+      const uint32_t i = i0 + lane;
+      const float kk = i < cnt ? key[v * copy_cap + i] : INFINITY;
+      const bool pass = i < cnt && kk <= th;
+      const unsigned b = __ballot_sync(0xFFFFFFFFu, pass);
+      const uint32_t at = n_out + (uint32_t)__popc(b & lt);
+      if (pass && at < cap) {
+        m_key[j * cap + at] = kk;
+        m_row[j * cap + at] = row[v * copy_cap + i];
+      }
+      n_out += (uint32_t)__popc(b);
+    }
+  }
+  if (lane == 0) {
+    m_count[j] = over || n_out > cap ? kOverflow : n_out;
+    m_thr[j] = th;
+  }
 }
 
 namespace {
@@ -1203,6 +1275,11 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
     tc_filter(ctx, s, x, width, d, sp.qrows.ptr, prows, scan, mean.ptr, scale, max_sq.ptr,
               kind, k, cap, cand_key, cand_row, cand_count.ptr, thr.ptr,
               qn2.ptr, slack_d.ptr, &trace, &point_ops);
+    if (sp.q_full.ptr) {
+      force_overflow_kernel<<<blocks_for(n, 256), 256, 0, s>>>(sp.q_full.ptr, n,
+                                                               cand_count.ptr);
+      KG_LAUNCH_CHECK();
+    }
     filter_ms += tf.stop_ms();
     {
       unsigned long long h_tiles = 0;
@@ -1246,16 +1323,28 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
     if (trace_on())
       std::fprintf(stderr, "[kyto_gpu trace] filter: %u of %llu queries overflowed (retried)\n",
                    h_over, (unsigned long long)n);
+    // A few overflowed queries would keep a few CTAs busy over every tile while the rest
+    // idle: the tiles are split into ranges, each range searched by its own copy of the
+    // queries (query blocks x copies about twice the SMs), and the copies merged.
+    const uint32_t qblock = filter_query_block(kind);
+    const uint32_t n_tiles_all = (uint32_t)((n + kTile - 1) / kTile);
     for (uint64_t r0 = 0; r0 < h_over; r0 += kTcRetryChunk) {
       check_cancel(ctx);
       const uint64_t m = std::min<uint64_t>(kTcRetryChunk, h_over - r0);
-      DeviceBuffer<uint32_t> r_qrows(m, s), r_qpoint(m, s), r_sample(batch ? m : 0, s);
-      retry_slots_kernel<<<blocks_for(m, 256), 256, 0, s>>>(
-          over.ptr + r0, m, sp.qrows.ptr, sp.q_point.ptr, batch ? slot_sample.ptr : nullptr,
-          r_qrows.ptr, r_qpoint.ptr, r_sample.ptr);
+      const uint64_t nb = (m + qblock - 1) / qblock, mq = nb * qblock;
+      uint64_t copies = std::max<uint64_t>(1, (2 * (uint64_t)ctx->sm_count + nb - 1) / nb);
+      copies = std::min<uint64_t>(copies, std::max<uint64_t>(1, kTcRetrySplitSlots / mq));
+      copies = std::min<uint64_t>(copies, n_tiles_all);
+      const uint32_t nc = (uint32_t)copies;
+      const uint32_t copy_cap = nc > 1 ? kTcRetrySplitCap : kTcRetryCap;
+      const uint64_t mv = mq * nc;
+      DeviceBuffer<uint32_t> r_qrows(mv, s), r_qpoint(mv, s), r_sample(batch ? mv : 0, s);
+      retry_slots_kernel<<<blocks_for(mv, 256), 256, 0, s>>>(
+          over.ptr + r0, m, mq, nc, sp.qrows.ptr, sp.q_point.ptr,
+          batch ? slot_sample.ptr : nullptr, r_qrows.ptr, r_qpoint.ptr, r_sample.ptr);
       KG_LAUNCH_CHECK();
       FilterScan rs = scan;
-      rs.n_q = m;
+      rs.n_q = mv;
       rs.q_point = r_qpoint.ptr;
       rs.slot_sample = batch ? r_sample.ptr : nullptr;
       rs.list_tiles = nullptr;
@@ -1264,19 +1353,52 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
       rs.list_stride = 0;
       rs.list_sorted = false;
       rs.tiles_scanned = nullptr;
-      DeviceBuffer<float> r_key(m * kTcRetryCap, s), r_thr(m, s);
-      DeviceBuffer<uint32_t> r_row(m * kTcRetryCap, s), r_count(m, s);
-      DeviceBuffer<double> r_qn2(m, s), r_slack(m, s);
+      DeviceBuffer<uint64_t> r_off;
+      DeviceBuffer<uint32_t> r_list;
+      if (nc > 1) {
+        r_off.alloc(nb * nc + 1, s);
+        r_list.alloc(nb * (uint64_t)n_tiles_all, s);
+        retry_lists_kernel<<<(unsigned)(nb * nc), 256, 0, s>>>(nb, nc, n_tiles_all, r_off.ptr,
+                                                               r_list.ptr);
+        KG_LAUNCH_CHECK();
+        rs.list_tiles = r_list.ptr;
+        rs.list_off = r_off.ptr;
+      }
+      DeviceBuffer<float> r_key(mv * copy_cap, s), r_thr(mv, s);
+      DeviceBuffer<uint32_t> r_row(mv * copy_cap, s), r_count(mv, s);
+      DeviceBuffer<double> r_qn2(mv, s), r_slack(mv, s);
       Timer trf(s);
       tc_filter(ctx, s, x, width, d, r_qrows.ptr, prows, rs, mean.ptr, scale, max_sq.ptr, kind,
-                k, kTcRetryCap, r_key.ptr, r_row.ptr, r_count.ptr, r_thr.ptr, r_qn2.ptr,
+                k, copy_cap, r_key.ptr, r_row.ptr, r_count.ptr, r_thr.ptr, r_qn2.ptr,
                 r_slack.ptr, nullptr, &point_ops);
       filter_ms += trf.stop_ms();
       Timer trr(s);
+      // Copy 0's slots 0..m-1 are the overflowed queries in order (their rows, norms and
+      // slacks); the merged candidates replace the copies'.
+      DeviceBuffer<float> m_key, m_thr;
+      DeviceBuffer<uint32_t> m_row, m_count;
+      const float* use_key = r_key.ptr;
+      const uint32_t* use_row = r_row.ptr;
+      const uint32_t* use_count = r_count.ptr;
+      const float* use_thr = r_thr.ptr;
+      if (nc > 1) {
+        m_key.alloc(m * kTcRetryCap, s);
+        m_row.alloc(m * kTcRetryCap, s);
+        m_count.alloc(m, s);
+        m_thr.alloc(m, s);
+        retry_merge_kernel<<<blocks_for(m * 32, 256), 256, 0, s>>>(
+            m, mq, nc, copy_cap, r_key.ptr, r_row.ptr, r_count.ptr, r_thr.ptr, kTcRetryCap,
+            m_key.ptr, m_row.ptr, m_count.ptr, m_thr.ptr);
+        KG_LAUNCH_CHECK();
+        use_key = m_key.ptr;
+        use_row = m_row.ptr;
+        use_count = m_count.ptr;
+        use_thr = m_thr.ptr;
+      }
       rank_kernel<<<blocks_for(m * 32, kRankWarps * 32), kRankWarps * 32, 0, s>>>(
-          x, width, d, 0, m, k, kTcRetryCap, r_key.ptr, r_row.ptr, r_count.ptr, r_thr.ptr,
-          r_slack.ptr, 1.0 / (scale * scale), r_qn2.ptr, r_qrows.ptr, prows, out.key.ptr,
-          out.row.ptr, full_flag.ptr, n_cand.ptr);
+          x, width, d, 0, m, k, nc > 1 ? kTcRetryCap : copy_cap, use_key, use_row, use_count,
+          use_thr, r_slack.ptr, 1.0 / (scale * scale), r_qn2.ptr, r_qrows.ptr, prows,
+          out.key.ptr, out.row.ptr, full_flag.ptr, n_cand.ptr);
       KG_LAUNCH_CHECK();
       rank_ms += trr.stop_ms();
     }

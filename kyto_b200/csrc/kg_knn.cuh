@@ -48,7 +48,9 @@ struct ScanPlan {
   DeviceBuffer<float> list_lb2;
   DeviceBuffer<uint64_t> list_off;
   uint64_t list_stride = 0;
-  bool list_sorted = false;  // each block's list ascending by bound
+  bool list_sorted = false;  // each block's list ascending by bound  // Per query slot (or empty): 1 where the slot's list does not cover its row, which is
+  // then searched over every tile with the overflowed queries.
+  DeviceBuffer<uint8_t> q_full;
 };
 // Builds the filter's scan for query blocks of qblock slots.
 using PlanBuilder = std::function<void(const float* x, uint64_t n, uint32_t width, uint32_t d,

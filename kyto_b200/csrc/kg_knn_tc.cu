@@ -55,6 +55,7 @@ constexpr int kTcThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kEndOfBlock = 0xFFFFFFFFu;
 constexpr uint32_t kNoBlock = 0xFFFFFFFFu;  // no query block left: the CTA's roles stop
+enum : int { kAmSmem = 0, kAmTmem = 1, kAmHalf = 2 };  // the filter's A operand modes
 
 // SUBS: 64-wide sub-tiles per operand row (1: fp16 or bf16; 2: split hi and lo). KR: the
 // register top-k width (16, 32) or 0 (the k smallest in local memory, any k).
@@ -73,10 +74,10 @@ struct TcSmem {
   float scratch[kEpiWarps * 32][33];  // a thread's 32 keys when some may pass
   float topk[kEpiWarps * 32][TcShape<KR, SUBS>::kTopK];  // a thread's k smallest keys
   uint64_t full[kStages], empty[kStages];
-  uint64_t tmem_full[3], tmem_empty[3];  // per accumulator slot (two or three in use)
+  uint64_t tmem_full[4], tmem_empty[4];  // per accumulator slot (two to four in use)
   uint64_t a_full, a_empty, drained;
   uint32_t stage_tile[kStages];      // the point tile in a stage, or kEndOfBlock
-  uint32_t acc_tile[3];              // the point tile in an accumulator slot, or kEndOfBlock
+  uint32_t acc_tile[4];              // the point tile in an accumulator slot, or kEndOfBlock
   uint32_t block_id[2];              // per block parity: the query block, or kNoBlock
   uint32_t acc_block[3];             // the query block of a slot's item
   float u_max[2][kEpiWarps];         // per block parity and epilogue warp: the largest
@@ -250,14 +251,18 @@ __device__ __forceinline__ void tc_offer_chunk(QueryState& st, float* smallest, 
 }
 
 // KR: the register top-k width used on offers (k <= KR), or 0 for any k. SUBS: operand
-// sub-tiles (1: one fp16/bf16 product; 2: split, three fp16 products). TA: the query
-// block's tiles are copied into tensor memory once per block (tcgen05.cp) and the MMAs
-// read A there, so each MMA reads only its point tile from shared memory (half the
-// operand bytes at N = 128); the accumulators are then three 128-column slots, one query
-// half each (a tile's two halves in consecutive slots), each released by its half's four
-// epilogue warps. Otherwise A is read from shared memory and the accumulators are two
-// slots of both halves (256 columns).
-template <int KR, int SUBS, bool TA>
+// sub-tiles (1: one fp16/bf16 product; 2: split, three fp16 products). AM, where the
+// query operand lives and how the accumulators are cut:
+//   kAmSmem  A read from shared memory by every MMA; two accumulator slots of both
+//            query halves (256 columns), each released by all eight epilogue warps;
+//   kAmTmem  the query block's tiles copied into tensor memory once per block
+//            (tcgen05.cp) and read there, so each MMA reads only its point tile from
+//            shared memory (half the operand bytes at N = 128); three 128-column slots,
+//            one query half each (a tile's two halves in consecutive slots), each
+//            released by its half's four epilogue warps;
+//   kAmHalf  A from shared memory, four 128-column half slots as with kAmTmem: the MMA
+//            warp may run three half products ahead of the epilogue instead of two.
+template <int KR, int SUBS, int AM>
 __global__ void __launch_bounds__(kTcThreads, 1)
 knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
                      const __grid_constant__ CUtensorMap tmap_p, FilterScan scan, uint32_t k,
@@ -277,19 +282,22 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
   const uint32_t n_tiles = (uint32_t)((n_p + kTcPoints - 1) / kTcPoints);
   volatile int* abort = &sm.abort;
 
-  // TMEM columns with TA: the query halves' A operands (32 columns a 64-wide sub-tile),
-  // then the three slots.
-  constexpr uint32_t kSlotBase = 64u * SUBS;
-  static_assert(!TA || kSlotBase + 3 * 128 <= kTmemCols, "filter TMEM columns");
+  // TMEM columns with A in TMEM: the query halves' A operands (32 columns a 64-wide
+  // sub-tile), then the three slots; with half slots and A in shared memory, four slots.
+  constexpr bool TA = AM == kAmTmem;
+  constexpr bool HS = AM != kAmSmem;
+  constexpr uint32_t kHalfSlots = TA ? 3u : 4u;
+  constexpr uint32_t kSlotBase = TA ? 64u * SUBS : 0u;
+  static_assert(!HS || kSlotBase + kHalfSlots * 128 <= kTmemCols, "filter TMEM columns");
   if (threadIdx.x == 0) {
     for (int s = 0; s < kStages; ++s) {
       mbar_init(&sm.full[s], 1);
       mbar_init(&sm.empty[s], 1);
     }
-    for (int b = 0; b < (TA ? 3 : 2); ++b) {
+    for (int b = 0; b < (HS ? (int)kHalfSlots : 2); ++b) {
       // Two arrivals: the MMA thread's own (releasing acc_tile) and the MMAs' commit.
       mbar_init(&sm.tmem_full[b], 2);
-      mbar_init(&sm.tmem_empty[b], TA ? kEpiWarps / 2 : kEpiWarps);
+      mbar_init(&sm.tmem_empty[b], HS ? kEpiWarps / 2 : kEpiWarps);
     }
     mbar_init(&sm.a_full, 1);
     mbar_init(&sm.a_empty, 1);
@@ -422,15 +430,15 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           __nanosleep(64);
       }
     }
-  } else if (warp == kEpiWarps + 1 && TA) {
-    // ------------------------------------------------- MMA issuer (A in TMEM) -------
+  } else if (warp == kEpiWarps + 1 && HS) {
+    // ------------------------------------------------- MMA issuer (half slots) ------
     if (lane == 0) {
       uint64_t it = 0, item = 0;  // item: the slot sequence (two per tile, halves 0, 1)
       uint32_t bi = 0;
       bool ok = true;
       auto next_slot = [&](uint32_t& sl) -> bool {
-        sl = (uint32_t)(item % 3);
-        return mbar_wait(&sm.tmem_empty[sl], (uint32_t)((item / 3) & 1) ^ 1, abort);
+        sl = (uint32_t)(item % kHalfSlots);
+        return mbar_wait(&sm.tmem_empty[sl], (uint32_t)((item / kHalfSlots) & 1) ^ 1, abort);
       };
       auto marker = [&](uint32_t block) -> bool {
         for (int h = 0; h < 2; ++h) {
@@ -452,19 +460,22 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           marker(kNoBlock);
           break;
         }
-        // The block's query tiles into TMEM (after the previous block's MMAs, in issue
-        // order); their shared memory goes back to the producer once the copies are done.
+        if (TA) {
+          // The block's query tiles into TMEM (after the previous block's MMAs, in issue
+          // order); their shared memory goes back to the producer once the copies are
+          // done.
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
+          for (int h = 0; h < 2; ++h)
 #pragma unroll
-          for (int sub = 0; sub < SUBS; ++sub) {
-            const uint32_t asm_ = smem_addr(sm.a[h][sub]);
-            const uint32_t at = tmem + (uint32_t)(h * 32 * SUBS + sub * 32);
+            for (int sub = 0; sub < SUBS; ++sub) {
+              const uint32_t asm_ = smem_addr(sm.a[h][sub]);
+              const uint32_t at = tmem + (uint32_t)(h * 32 * SUBS + sub * 32);
 #pragma unroll
-            for (int kk = 0; kk < kTcK / 16; ++kk)
-              tmem_cp_128x256b(at + kk * 8, desc_k_sw128(asm_ + kk * 32));
-          }
-        mma_commit(&sm.a_empty);
+              for (int kk = 0; kk < kTcK / 16; ++kk)
+                tmem_cp_128x256b(at + kk * 8, desc_k_sw128(asm_ + kk * 32));
+            }
+          mma_commit(&sm.a_empty);
+        }
         for (;; ++it) {
           const int s = (int)(it % kStages);
           const uint32_t ph = (uint32_t)((it / kStages) & 1);
@@ -476,6 +487,8 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           const uint32_t pt = sm.stage_tile[s];
           if (pt == kEndOfBlock) {
             mbar_arrive(&sm.empty[s]);
+            // A in shared memory: free once the block's MMAs are done.
+            if (!TA) mma_commit(&sm.a_empty);
             ok = marker(qb);
             ++it;
             break;
@@ -497,10 +510,18 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
             for (int t = 0; t < (SUBS == 1 ? 1 : 3); ++t) {
               const int sa = t == 2 ? 1 : 0, sb = t == 1 ? 1 : 0;
               const uint32_t bsm = smem_addr(sm.b[s][sb]);
-              const uint32_t a = tmem + (uint32_t)(h * 32 * SUBS + sa * 32);
+              if (TA) {
+                const uint32_t a = tmem + (uint32_t)(h * 32 * SUBS + sa * 32);
 #pragma unroll
-              for (int kk = 0; kk < kTcK / 16; ++kk)
-                mma_f16_ts(d, a + kk * 8, desc_k_sw128(bsm + kk * 32), idesc, (t | kk) > 0);
+                for (int kk = 0; kk < kTcK / 16; ++kk)
+                  mma_f16_ts(d, a + kk * 8, desc_k_sw128(bsm + kk * 32), idesc, (t | kk) > 0);
+              } else {
+                const uint32_t asm_ = smem_addr(sm.a[h][sa]);
+#pragma unroll
+                for (int kk = 0; kk < kTcK / 16; ++kk)
+                  mma_f16(d, desc_k_sw128(asm_ + kk * 32), desc_k_sw128(bsm + kk * 32), idesc,
+                          (t | kk) > 0);
+              }
             }
             if (h == 1) mma_commit(&sm.empty[s]);
             mbar_arrive(&sm.tmem_full[sl]);
@@ -592,21 +613,21 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
     // overflow flag stay in registers; after offers the warp publishes its largest
     // threshold + s^2 |q|^2 for the producer's bound checks.
     const uint32_t half = (uint32_t)warp >> 2, quad = (uint32_t)warp & 3;
-    // The warp's i-th item: with TA, the half's slot sequence (items 2 i + half of the
-    // MMA warp's, three slots of 128 columns); else the two shared slots, this half's 128
-    // columns of each.
+    // The warp's i-th item: with half slots, the half's slot sequence (items 2 i + half
+    // of the MMA warp's, kHalfSlots slots of 128 columns); else the two shared slots,
+    // this half's 128 columns of each.
     auto slot_of = [&](uint64_t i, uint32_t& sl, uint32_t& ph) {
-      if (TA) {
+      if (HS) {
         const uint64_t g = 2 * i + half;
-        sl = (uint32_t)(g % 3);
-        ph = (uint32_t)((g / 3) & 1);
+        sl = (uint32_t)(g % kHalfSlots);
+        ph = (uint32_t)((g / kHalfSlots) & 1);
       } else {
         sl = (uint32_t)(i & 1);
         ph = (uint32_t)((i >> 1) & 1);
       }
     };
     auto slot_cols = [&](uint32_t sl) -> uint32_t {
-      return TA ? kSlotBase + sl * 128u : sl * 256u + half * 128u;
+      return HS ? kSlotBase + sl * 128u : sl * 256u + half * 128u;
     };
     float* my = sm.scratch[threadIdx.x];
     float local_smallest[KR == 0 ? kMaxK : 1];
@@ -941,27 +962,29 @@ uint32_t filter_query_block(FilterKind) { return kTcQueryBlock; }
 
 namespace {
 
-template <int KR, int SUBS, bool TA>
+template <int KR, int SUBS, int AM>
 void launch_filter(unsigned grid, cudaStream_t s, const CUtensorMap& mq, const CUtensorMap& mp,
                    const FilterScan& scan, uint32_t k, const float* slack2, uint32_t idesc,
                    uint32_t cap, float* cand_key, uint32_t* cand_row, uint32_t* cand_count,
                    float* threshold, int* err) {
   static std::once_flag attr;
   std::call_once(attr, [] {
-    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<KR, SUBS, TA>,
+    KG_CUDA(cudaFuncSetAttribute(knn_filter_tc_kernel<KR, SUBS, AM>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)tc_smem_bytes<KR, SUBS>()));
   });
-  knn_filter_tc_kernel<KR, SUBS, TA><<<grid, kTcThreads, tc_smem_bytes<KR, SUBS>(), s>>>(
+  knn_filter_tc_kernel<KR, SUBS, AM><<<grid, kTcThreads, tc_smem_bytes<KR, SUBS>(), s>>>(
       mq, mp, scan, k, slack2, idesc, cap, cand_key, cand_row, cand_count, threshold, err);
 }
 
-// The filter's query operand: read from shared memory by every MMA (the default: 194 ms
-// against 238 ms for the 1M benchmark search on a B200) or copied into tensor memory once
-// per block (KYTO_GPU_FILTER_A=tmem); both give the same keys.
-bool filter_a_in_tmem() {
+// The filter's query operand and accumulator slots (KYTO_GPU_FILTER_A): "smem" (the
+// default: 194 ms against 238 ms for "tmem" on the 1M benchmark search on a B200),
+// "tmem", or "half" (shared memory, four half slots); all give the same keys.
+int filter_a_mode() {
   const char* v = std::getenv("KYTO_GPU_FILTER_A");
-  return v && std::string(v) == "tmem";
+  if (v && std::string(v) == "tmem") return kAmTmem;
+  if (v && std::string(v) == "half") return kAmHalf;
+  return kAmSmem;
 }
 
 }  // namespace
@@ -1030,13 +1053,16 @@ void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint32_t width, uint
   const unsigned grid = (unsigned)std::min<uint64_t>(n_qblocks, (uint64_t)ctx->sm_count);
   const uint32_t idesc = idesc_f32acc(bf16 ? 1u : 0u, 128, kTcPoints);
   const int kr = k <= 16 ? 16 : k <= 32 ? 32 : 0;
-  auto pick = [&](auto ta) {
-    constexpr bool TA = decltype(ta)::value;
-    return kr == 16 ? (split ? launch_filter<16, 2, TA> : launch_filter<16, 1, TA>)
-           : kr == 32 ? (split ? launch_filter<32, 2, TA> : launch_filter<32, 1, TA>)
-                      : (split ? launch_filter<0, 2, TA> : launch_filter<0, 1, TA>);
+  auto pick = [&](auto am) {
+    constexpr int AM = decltype(am)::value;
+    return kr == 16 ? (split ? launch_filter<16, 2, AM> : launch_filter<16, 1, AM>)
+           : kr == 32 ? (split ? launch_filter<32, 2, AM> : launch_filter<32, 1, AM>)
+                      : (split ? launch_filter<0, 2, AM> : launch_filter<0, 1, AM>);
   };
-  auto launch = filter_a_in_tmem() ? pick(std::true_type{}) : pick(std::false_type{});
+  const int am = filter_a_mode();
+  auto launch = am == kAmTmem   ? pick(std::integral_constant<int, kAmTmem>{})
+                : am == kAmHalf ? pick(std::integral_constant<int, kAmHalf>{})
+                                : pick(std::integral_constant<int, kAmSmem>{});
   launch(grid, s, mq, mp, scan, k, slack2.ptr, idesc, cap, cand_key, cand_row, cand_count,
          threshold, err.ptr);
   KG_LAUNCH_CHECK();

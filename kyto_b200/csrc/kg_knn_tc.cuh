@@ -12,6 +12,9 @@ constexpr uint32_t kTcCap = 512;             // candidate slots per query (a que
                                              // a compaction)
 constexpr uint32_t kTcRetryCap = 8192;       // slots per query in the overflow retry
 constexpr uint64_t kTcRetryChunk = 65536;    // queries per retry pass
+constexpr uint32_t kTcRetrySplitCap = 4096;  // slots per query copy when a retry's tiles
+                                             // are split between copies of its queries
+constexpr uint64_t kTcRetrySplitSlots = 32768;  // query slots over all copies, at most
 constexpr uint32_t kTcQueryBlock = 256;      // query slots per block of the fp16/bf16 filter
 
 // The filter's operands: fp16 or bf16 (one 64-wide row: the components and the norm), or

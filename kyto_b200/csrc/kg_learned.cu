@@ -15,12 +15,16 @@
 //   5. index: the network's top-`probe` parts for every row (each row stored in its top
 //      part) and its 32 most probable parts with their probabilities at that
 //      temperature;
-//   6. confidence: the rows in top-part order form provisional blocks of 256 query
-//      slots; a row's confidence is its probability in the parts its block probes (the
-//      union of its rows' top-`probe` parts), and it falls back below the threshold;
-//   7. search: query slots sorted by (fallback, top part); each block of 256 query slots
-//      scans the tiles of the parts of the provisional blocks its rows came from (every
-//      tile if one of them falls back), then the exact re-rank.
+//   6. confidence: the rows in part order (a row's top three parts, most probable
+//      first, so rows sharing their top part sit together and nearby rows nearer still)
+//      form provisional blocks of 256 query slots; a row's confidence is its
+//      probability in the parts its block probes (the union of its rows' top-`probe`
+//      parts), and it falls back below the threshold;
+//   7. search: query slots sorted by (fallback, part order); each block of 256 query
+//      slots scans the tiles of the parts of the provisional blocks its confident rows
+//      came from, then the exact re-rank; fallback rows are searched over every tile
+//      with the filter's overflowed queries (the tiles split into ranges between copies
+//      of those queries, so they spread over every SM).
 #include <cuda_bf16.h>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
@@ -28,6 +32,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <vector>
 
 #include "kg_cluster.cuh"
@@ -86,23 +91,37 @@ __global__ void gather_batch_kernel(const float* xs, uint32_t d, const uint32_t*
   if (j < L) lb[r * L + j] = labels[src * L + j];
 }
 
-// key = (fallback, top part) for the query order; iota payload.
+// A row's order key: its `levels` most probable parts, most probable first, pb bits
+// each. Rows sharing their first part are one contiguous run, and inside it rows sharing
+// their second (third) part sit together: nearby rows in nearby slots.
+__device__ __forceinline__ unsigned long long part_key(const uint32_t* top, uint64_t r,
+                                                       uint32_t probe, uint32_t levels,
+                                                       uint32_t pb) {
+  unsigned long long key = 0;
+  for (uint32_t l = 0; l < levels; ++l) key = (key << pb) | top[r * probe + l];
+  return key;
+}
+
+// key = (fallback, part key) for the query order (a fallback row: the part `parts`,
+// lower levels 0); iota payload.
 __global__ void query_key_kernel(const uint32_t* top, const float* conf, uint64_t n,
-                                 uint32_t probe, float threshold, uint32_t parts, uint32_t* key,
-                                 uint32_t* iota, uint8_t* fallback) {
+                                 uint32_t probe, uint32_t levels, uint32_t pb, float threshold,
+                                 uint32_t parts, unsigned long long* key, uint32_t* iota,
+                                 uint8_t* fallback) {
   uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (r >= n) return;
   const bool fb = !(conf[r] >= threshold);
   fallback[r] = fb ? 1 : 0;
-  key[r] = fb ? parts : top[r * probe];
+  key[r] = fb ? (unsigned long long)parts << (pb * (levels - 1))
+              : part_key(top, r, probe, levels, pb);
   iota[r] = (uint32_t)r;
 }
 
-__global__ void point_key_kernel(const uint32_t* top, uint64_t n, uint32_t probe, uint32_t* key,
-                                 uint32_t* iota) {
+__global__ void point_key_kernel(const uint32_t* top, uint64_t n, uint32_t probe, uint32_t levels,
+                                 uint32_t pb, unsigned long long* key, uint32_t* iota) {
   uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (r >= n) return;
-  key[r] = top[r * probe];
+  key[r] = part_key(top, r, probe, levels, pb);
   iota[r] = (uint32_t)r;
 }
 
@@ -111,20 +130,27 @@ __global__ void inverse_kernel(const uint32_t* perm, uint64_t n, uint32_t* inv) 
   if (i < n) inv[perm[i]] = (uint32_t)i;
 }
 
+__global__ void full_slots_kernel(const uint32_t* qrows, const uint8_t* fallback, uint64_t n,
+                                  uint8_t* q_full) {
+  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (i < n) q_full[i] = fallback[qrows[i]];
+}
+
 __global__ void compose_kernel(const uint32_t* qrows, const uint32_t* slot_of_row, uint64_t n,
                                uint32_t* q_point) {
   uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
   if (i < n) q_point[i] = slot_of_row[qrows[i]];
 }
 
-__global__ void part_starts_kernel(const uint32_t* sorted, uint64_t n, uint32_t parts,
-                                   uint32_t* starts) {
+// starts[c] = the first slot whose key's top part (key >> shift) is at least c.
+__global__ void part_starts_kernel(const unsigned long long* sorted, uint64_t n, uint32_t parts,
+                                   uint32_t shift, uint32_t* starts) {
   const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c > parts) return;
   uint64_t lo = 0, hi = n;
   while (lo < hi) {
     const uint64_t mid = (lo + hi) >> 1;
-    if (sorted[mid] < c) lo = mid + 1; else hi = mid;
+    if ((sorted[mid] >> shift) < c) lo = mid + 1; else hi = mid;
   }
   starts[c] = (uint32_t)lo;
 }
@@ -132,10 +158,10 @@ __global__ void part_starts_kernel(const uint32_t* sorted, uint64_t n, uint32_t 
 constexpr uint32_t kProbeThreads = 256;
 constexpr uint32_t kMassParts = 32;  // parts per row whose probabilities the index keeps
 
-// One CTA per block of query slots: the tiles of the union of its queries' probed parts
-// (a bitmap over tiles), or every tile when one of them falls back. Count pass (list
-// NULL): the number of tiles into len[B]; fill pass: the tiles in increasing order at
-// list + off[B].
+// One CTA per block of query slots: the tiles of the union of the probed parts of its
+// queries that do not fall back (a bitmap over tiles; a fallback row is searched over
+// every tile apart from the blocks). Count pass (list NULL): the number of tiles into
+// len[B]; fill pass: the tiles in increasing order at list + off[B].
 __global__ void __launch_bounds__(kProbeThreads)
 probe_tiles_kernel(const uint32_t* qrows, uint64_t n, const uint32_t* prov_of_row,
                    const uint32_t* prov_parts, uint32_t pwords, const uint8_t* fallback,
@@ -144,13 +170,11 @@ probe_tiles_kernel(const uint32_t* qrows, uint64_t n, const uint32_t* prov_of_ro
   // Dynamic shared memory: n_tiles bits of tiles, then pwords words of parts.
   extern __shared__ uint32_t bits[];
   uint32_t* parts_bm = bits + (n_tiles + 31) / 32;
-  __shared__ int any_fallback;
   __shared__ uint32_t word_base[kProbeThreads + 1];
   __shared__ uint32_t prov[kProbeThreads];
   const uint32_t words = (n_tiles + 31) / 32;
   for (uint32_t w = threadIdx.x; w < words; w += kProbeThreads) bits[w] = 0;
   for (uint32_t w = threadIdx.x; w < pwords; w += kProbeThreads) parts_bm[w] = 0;
-  if (threadIdx.x == 0) any_fallback = 0;
   __syncthreads();
   // The parts of every provisional block a row of this block came from (a run of rows
   // from the same one contributes its bitmap once).
@@ -160,8 +184,7 @@ probe_tiles_kernel(const uint32_t* qrows, uint64_t n, const uint32_t* prov_of_ro
     uint32_t b = 0xFFFFFFFFu;
     if (i0 + threadIdx.x < block && q < n) {
       const uint32_t row = qrows[q];
-      if (fallback[row]) any_fallback = 1;
-      else b = prov_of_row[row];
+      if (!fallback[row]) b = prov_of_row[row];
     }
     prov[threadIdx.x] = b;
     __syncthreads();
@@ -185,14 +208,6 @@ probe_tiles_kernel(const uint32_t* qrows, uint64_t n, const uint32_t* prov_of_ro
     }
   }
   __syncthreads();
-  if (any_fallback) {
-    if (!list) {
-      if (threadIdx.x == 0) len[blockIdx.x] = n_tiles;
-      return;
-    }
-    for (uint32_t t = threadIdx.x; t < n_tiles; t += kProbeThreads) list[off[blockIdx.x] + t] = t;
-    return;
-  }
   // Per thread a run of words, their popcounts scanned in thread order.
   const uint32_t per = (words + kProbeThreads - 1) / kProbeThreads;
   const uint32_t w0 = threadIdx.x * per, w1 = min(words, w0 + per);
@@ -225,8 +240,8 @@ probe_tiles_kernel(const uint32_t* qrows, uint64_t n, const uint32_t* prov_of_ro
   }
 }
 
-void sort_u32_pairs(const uint32_t* key, const uint32_t* val, uint64_t n, int bits,
-                    DeviceBuffer<uint32_t>& key_out, DeviceBuffer<uint32_t>& val_out,
+void sort_key_pairs(const unsigned long long* key, const uint32_t* val, uint64_t n, int bits,
+                    DeviceBuffer<unsigned long long>& key_out, DeviceBuffer<uint32_t>& val_out,
                     cudaStream_t s) {
   key_out.alloc(n, s);
   val_out.alloc(n, s);
@@ -236,6 +251,14 @@ void sort_u32_pairs(const uint32_t* key, const uint32_t* val, uint64_t n, int bi
   DeviceBuffer<unsigned char> scratch(temp, s);
   KG_CUDA(cub::DeviceRadixSort::SortPairs(scratch.ptr, temp, key, key_out.ptr, val, val_out.ptr,
                                           (int)n, 0, bits, s));
+}
+
+// How many of a row's most probable parts order the rows (KYTO_GPU_LEARNED_LEVELS, 1-3;
+// default 3).
+uint32_t order_levels() {
+  const char* e = std::getenv("KYTO_GPU_LEARNED_LEVELS");
+  const int v = e ? std::atoi(e) : 3;
+  return (uint32_t)std::min(3, std::max(1, v));
 }
 
 int bits_for_value(uint64_t v) {
@@ -581,15 +604,20 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
     uint64_t fallback_rows = 0, scanned_tiles = 0;
     PlanBuilder plan = [&](const float*, uint64_t nn, uint32_t, uint32_t, double,
                            uint32_t qblock, ScanPlan& sp, Trace& tr) {
-      DeviceBuffer<uint32_t> key(nn, s), iota(nn, s), key_sorted;
+      DeviceBuffer<unsigned long long> key(nn, s), key_sorted;
+      DeviceBuffer<uint32_t> iota(nn, s);
       DeviceBuffer<uint8_t> fallback(nn, s);
-      // Points: by top part.
-      point_key_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(top.ptr, nn, probe, key.ptr, iota.ptr);
+      // Points: by their first `levels` parts.
+      const uint32_t pb = (uint32_t)bits_for_value(parts);
+      const uint32_t levels = std::min<uint32_t>({order_levels(), probe, 64 / pb});
+      const int key_bits = (int)(pb * levels);
+      point_key_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(top.ptr, nn, probe, levels, pb,
+                                                           key.ptr, iota.ptr);
       KG_LAUNCH_CHECK();
-      sort_u32_pairs(key.ptr, iota.ptr, nn, bits_for_value(parts), key_sorted, sp.prows, s);
+      sort_key_pairs(key.ptr, iota.ptr, nn, key_bits, key_sorted, sp.prows, s);
       DeviceBuffer<uint32_t> part_start((uint64_t)parts + 1, s);
       part_starts_kernel<<<blocks_for((uint64_t)parts + 1, 256), 256, 0, s>>>(
-          key_sorted.ptr, nn, parts, part_start.ptr);
+          key_sorted.ptr, nn, parts, pb * (levels - 1), part_start.ptr);
       KG_LAUNCH_CHECK();
       DeviceBuffer<uint32_t> slot_of_row(nn, s);
       inverse_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(sp.prows.ptr, nn, slot_of_row.ptr);
@@ -611,12 +639,16 @@ kg_status kg_knn_learned(kg_ctx* ctx, const float* embedding, uint64_t n, uint32
                                                             prov_of_row.ptr, uconf.ptr);
       KG_LAUNCH_CHECK();
       // Queries: by (fallback, top part).
-      query_key_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(top.ptr, uconf.ptr, nn, probe,
-                                                           P.confidence, parts, key.ptr, iota.ptr,
-                                                           fallback.ptr);
+      query_key_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(top.ptr, uconf.ptr, nn, probe, levels,
+                                                           pb, P.confidence, parts, key.ptr,
+                                                           iota.ptr, fallback.ptr);
       KG_LAUNCH_CHECK();
-      sort_u32_pairs(key.ptr, iota.ptr, nn, bits_for_value(parts + 1), key_sorted, sp.qrows, s);
+      sort_key_pairs(key.ptr, iota.ptr, nn, key_bits, key_sorted, sp.qrows, s);
       sp.q_point.alloc(nn, s);
+      sp.q_full.alloc(nn, s);
+      full_slots_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(sp.qrows.ptr, fallback.ptr, nn,
+                                                           sp.q_full.ptr);
+      KG_LAUNCH_CHECK();
       compose_kernel<<<blocks_for(nn, 256), 256, 0, s>>>(sp.qrows.ptr, slot_of_row.ptr, nn,
                                                          sp.q_point.ptr);
       KG_LAUNCH_CHECK();

@@ -242,7 +242,8 @@ def test_knn_tensor_core_tiles_past_the_end(ctx, monkeypatch, candidate_filter):
 def test_knn_split_filter_keeps_tight_clusters_off_the_full_search(ctx, monkeypatch):
     # Components with sigma 0.2 hold hundreds of points inside fp16's slack (2^-9 of
     # |q| R), so their queries overflow the 512 candidate slots and go through the
-    # overflow retry (8,192 slots, every tile); the split operands' slack (about 2^-14 of
+    # overflow retry (every tile, the tiles split into ranges between copies of the
+    # overflowed queries and the copies' candidates merged); the split operands' slack (about 2^-14 of
     # |q| R) keeps them near k. Same graph either way, and no row searched in full.
     pts, _ = synthetic.gaussian_mixture(20_000, 50, 40, seed=13, device="cpu")
     ref = O.neighbors(pts, 15)
@@ -448,18 +449,24 @@ def test_connectivities_refusals(ctx):
 def test_filter_query_operand_in_tmem_or_smem_gives_the_same_keys(ctx, monkeypatch,
                                                                   candidate_filter):
     # The filter's MMAs read the query tiles from tensor memory (copied once per block) or
-    # from shared memory: the same products, so the same approximate keys, candidates,
-    # full-row searches and graph bits; and on ordinary data no row needs a full search.
+    # from shared memory, into two whole or three or four half accumulator slots: the same
+    # products, so the same approximate keys, candidates, full-row searches and graph
+    # bits; and on ordinary data no row needs a full search with fp16 or split operands
+    # (bf16's 8-bit significands leave slacks wide enough that some rows keep too many
+    # candidates and are searched in full, the same rows every way).
     monkeypatch.setenv("KYTO_GPU_KNN_FILTER", candidate_filter)
     x, _ = synthetic.gaussian_mixture(60_000, dim=50, n_components=40, seed=21, device="cpu")
     monkeypatch.setenv("KYTO_GPU_FILTER_A", "smem")
     a = K.neighbors(x, 15, ctx=ctx)
-    monkeypatch.setenv("KYTO_GPU_FILTER_A", "tmem")
-    b = K.neighbors(x, 15, ctx=ctx)
-    assert np.array_equal(a.indices, b.indices)
-    assert np.array_equal(a.distances.view(np.uint32), b.distances.view(np.uint32))
-    assert a.stats.candidates == b.stats.candidates
-    assert a.stats.rows_full == b.stats.rows_full == 0
+    for mode in ("tmem", "half"):  # A in tensor memory; A in shared memory, half slots
+        monkeypatch.setenv("KYTO_GPU_FILTER_A", mode)
+        b = K.neighbors(x, 15, ctx=ctx)
+        assert np.array_equal(a.indices, b.indices), mode
+        assert np.array_equal(a.distances.view(np.uint32), b.distances.view(np.uint32)), mode
+        assert a.stats.candidates == b.stats.candidates, mode
+        assert a.stats.rows_full == b.stats.rows_full, mode
+    if candidate_filter != "bf16":
+        assert a.stats.rows_full == 0
     o = O.neighbors(x[:5000], 15, method="exact")
     c = K.neighbors(x[:5000], 15, ctx=ctx)
     assert np.array_equal(c.indices, o.indices)
