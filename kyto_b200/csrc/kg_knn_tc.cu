@@ -79,9 +79,12 @@ struct TcSmem {
   uint32_t stage_tile[kStages];      // the point tile in a stage, or kEndOfBlock
   uint32_t acc_tile[4];              // the point tile in an accumulator slot, or kEndOfBlock
   uint32_t block_id[2];              // per block parity: the query block, or kNoBlock
-  uint32_t acc_block[3];             // the query block of a slot's item
-  float u_max[2][kEpiWarps];         // per block parity and epilogue warp: the largest
-                                     // threshold + s^2 |q|^2 of its queries
+  uint32_t acc_block[4];             // the query block of a slot's item
+  // Per epilogue warp: the largest threshold + s^2 |q|^2 + slack of its live queries
+  // (low word, f32 bits) in the query block of the high word. A value is used only by
+  // that block's scan: an epilogue running behind (a short block before it) cannot
+  // hand an older block's thresholds to the producer.
+  unsigned long long u_pub[kEpiWarps];
   uint32_t tmem_base;
   int abort;
 };
@@ -303,6 +306,7 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
     mbar_init(&sm.a_empty, 1);
     mbar_init(&sm.drained, 1);
     sm.abort = 0;
+    for (int w = 0; w < kEpiWarps; ++w) sm.u_pub[w] = (unsigned long long)kNoBlock << 32;
     fence_mbar_init();
   }
   if (warp == 0) tmem_alloc(&sm.tmem_base, kTmemCols);
@@ -310,7 +314,7 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = sm.tmem_base;
-  volatile float* u_max = &sm.u_max[0][0];
+  volatile unsigned long long* u_pub = sm.u_pub;
 
   if (warp == kEpiWarps) {
     // ------------------------------------------------------------ TMA producer ----
@@ -343,7 +347,6 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
             sm.block_id[bi & 1] = kNoBlock;
             mbar_arrive(&sm.a_full);
           } else {
-            for (int w = 0; w < kEpiWarps; ++w) u_max[(bi & 1) * kEpiWarps + w] = INFINITY;
             sm.block_id[bi & 1] = (uint32_t)qb;
             mbar_arrive_expect_tx(&sm.a_full, 2 * SUBS * kTileBytes);
             for (int h = 0; h < 2; ++h)
@@ -375,8 +378,14 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           // takes its value, so every lane makes the same choice.
           float u = 0.0f;
           if (lane == 0) {
-            u = u_max[(bi & 1) * kEpiWarps];
-            for (int w = 1; w < kEpiWarps; ++w) u = fmaxf(u, u_max[(bi & 1) * kEpiWarps + w]);
+            u = -INFINITY;
+            for (int w = 0; w < kEpiWarps; ++w) {
+              const unsigned long long v = u_pub[w];
+              // A warp yet to publish for this block bounds nothing.
+              u = (uint32_t)(v >> 32) == (uint32_t)qb ? fmaxf(u, __uint_as_float((uint32_t)v))
+                                                      : INFINITY;
+              if (u == INFINITY) break;
+            }
           }
           u = __shfl_sync(0xFFFFFFFFu, u, 0);
           if (lb2 > u) {
@@ -732,7 +741,7 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           const float u = active && live ? round_up_f32d((double)th + s2qn2 + sl2) : -INFINITY;
           float um = u;
           for (int o = 16; o; o >>= 1) um = fmaxf(um, __shfl_xor_sync(0xFFFFFFFFu, um, o));
-          if (lane == 0) u_max[(bi & 1) * kEpiWarps + warp] = um;
+          if (lane == 0) u_pub[warp] = ((unsigned long long)qb32 << 32) | __float_as_uint(um);
         }
       }
       if (active && ok) {

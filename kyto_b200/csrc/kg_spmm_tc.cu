@@ -65,10 +65,8 @@ constexpr int kFlushChunks = 16;        // K-chunks summed in f32 before the f64
 constexpr uint32_t kBBytes = kN * 128;  // 8 KB: 64 rows x (32 hi + 32 lo) fp16
 constexpr uint32_t kMaskBytes = kRows * 4;
 constexpr uint32_t kBlockMaxBytes = kMaskBytes + kRows * kChunk * 4;
-// Two expand warps per sub-partition (rows 32 q.. of a block, one half of its columns
-// each) and two drain warps (rows 32 q.., one half of the 64 output columns each).
-constexpr int kExpandWarps = 8;
-constexpr int kDrainWarps = 8;
+constexpr int kExpandWarps = 4;
+constexpr int kDrainWarps = 4;
 constexpr int kSpThreads = (kExpandWarps + kDrainWarps + 2) * 32;
 constexpr int kABufs = 4;
 // TMEM columns: two 64-column f32 accumulators (0..127), then kABufs A buffers of 32
@@ -86,7 +84,7 @@ static_assert(sizeof(LoadStage) % 1024 == 0, "load stage size");
 
 struct SpSmem {
   LoadStage st[kLoadStages];
-  double colsum[2][4][kN];  // per item parity, per 32-row quarter of the tile
+  double colsum[2][kDrainWarps][kN];
   // Per expand warp, per column of the current block: its mask word for the warp's 32
   // rows and the rank of its first value there.
   alignas(16) uint2 meta[kExpandWarps][kChunk];
@@ -158,9 +156,9 @@ struct ValueMap {
   float unscale, sq_scale;
 };
 
-// One CTA per SM, 18 warps (at most 112 registers a thread): each drain warp keeps 32
-// f64 sums, and two expand warps per sub-partition hide each other's shared-memory
-// latency.
+// One CTA per SM. The register file is split over the SM's four sub-partitions, so ten
+// warps fit only at 168 registers a thread (three warps on two of them); the drain warps'
+// 64 f64 sums spill a little in the once-per-item epilogue.
 __global__ void __launch_bounds__(kSpThreads, 1)
 spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __restrict__ off,
                const uint8_t* __restrict__ data, uint64_t rows, Geometry geo, ValueMap vmap,
@@ -201,10 +199,9 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
 
   if (warp < kExpandWarps) {
     // ----------------------------------------------------------- expand -------------
-    const uint32_t q = (uint32_t)warp & 3u;   // rows 32 q .. 32 q + 31 of each block
-    const int hh = warp >> 2;                 // column pairs 8 hh .. 8 hh + 7
+    const uint32_t q = (uint32_t)warp;        // rows 32 q .. 32 q + 31 of each block
     const uint32_t lt = (1u << lane) - 1u;    // the lanes (rows) before this one
-    const uint4* meta4 = reinterpret_cast<const uint4*>(sm.meta[warp]);
+    const uint4* meta4 = reinterpret_cast<const uint4*>(sm.meta[q]);
     uint64_t it = 0;
     bool ok = true;
     for (uint64_t w = blockIdx.x; w < n_items && ok; w += gridDim.x) {
@@ -249,14 +246,15 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
             excl += (uint32_t)__popc(__ballot_sync(0xFFFFFFFFu, (colcount >> b) & 1u) & lt) << b;
           base = excl + pre;
         }
-        sm.meta[warp][lane] = make_uint2(m_own, base);
+        sm.meta[q][lane] = make_uint2(m_own, base);
         __syncwarp();
         // Row (32 q + lane) of the A tiles: for each column, the value at its rank if the
         // row stores one (lanes that do read consecutive words; the others read a
         // neighbour's and drop it), two columns a word, hi parts then lo parts.
-        // This warp's 8 column pairs: hi words to columns 8 hh.., lo words to 16 + 8 hh..
+        // Two halves of 8 column pairs each: hi words to columns 8 h.., lo words to 16 + 8 h..
         const uint32_t arow = tmem + ((q * 32u) << 16) + kABase + ab * kACols;
-        {
+#pragma unroll
+        for (int hh = 0; hh < 2; ++hh) {
           uint32_t hw[8], lw[8];
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
@@ -292,9 +290,7 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
     }
   } else if (warp < kExpandWarps + kDrainWarps) {
     // ----------------------------------------------------------- drain TMEM ---------
-    const uint32_t quad = (uint32_t)warp & 3u;  // TMEM lanes 32 quad .. (rows of the tile)
-    const uint32_t half = (uint32_t)(warp - kExpandWarps) >> 2;  // columns 32 half ..
-    constexpr int kH = kN / 2;
+    const uint32_t quad = (uint32_t)warp & 3u;  // warps 4..7 -> TMEM lanes 32*quad..
     const uint32_t i = quad * 32u + lane;
     uint64_t fg = 0, item_no = 0;
     bool ok = true;
@@ -302,9 +298,9 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
       uint32_t tile, seg;
       geo.item(w, tile, seg);
       const uint64_t row = (uint64_t)tile * kRows + i;
-      double acc[kH];
+      double acc[kN];
 #pragma unroll
-      for (int j = 0; j < kH; ++j) acc[j] = 0.0;
+      for (int j = 0; j < kN; ++j) acc[j] = 0.0;
       const uint32_t nc = geo.chunks(seg);
       const uint32_t groups = (nc + kFlushChunks - 1) / kFlushChunks;
       for (uint32_t gr = 0; gr < groups; ++gr, ++fg) {
@@ -315,10 +311,11 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
         }
         tc_fence_after();
         __syncwarp();
+        // 16 columns at a time (few live registers beside the 64 f64 sums).
 #pragma unroll
-        for (int hf = 0; hf < 2; ++hf) {
+        for (int hf = 0; hf < 4; ++hf) {
           uint32_t rr[16];
-          tmem_ld_16(tmem + ((quad * 32u) << 16) + b * kAccCols + half * kH + hf * 16u, rr);
+          tmem_ld_16(tmem + ((quad * 32u) << 16) + b * kAccCols + hf * 16u, rr);
           tmem_wait_ld();
 #pragma unroll
           for (int j = 0; j < 16; ++j) acc[hf * 16 + j] += (double)__uint_as_float(rr[j]);
@@ -330,15 +327,14 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
       if (!ok) break;
       if (out.mode == kOutRows) {
         // C = S D - offsets: the next product's D^T (fp16 parts), the f32 rows, and this
-        // tile's column sums (fixed tree: warp shuffles, then the 4 quarters in order).
+        // tile's column sums (fixed tree: warp shuffles, then the 4 warps in order).
         const bool live = row < rows;
         const double t_mul = ldexp(1.0, out.t_scale), t_inv = ldexp(1.0, -out.t_scale);
         uint16_t* t_row = out.t ? out.t + (row / 32) * 64 + (row % 32) : nullptr;
 #pragma unroll
-        for (int jj = 0; jj < kH; ++jj) {
-          const int j = (int)half * kH + jj;
+        for (int j = 0; j < kN; ++j) {
           const double cval =
-              live && j < (int)out.width ? acc[jj] * out_scale - out.offsets[j] : 0.0;
+              live && j < (int)out.width ? acc[j] * out_scale - out.offsets[j] : 0.0;
           double seen = cval;
           if (out.t) {
             const double y = cval * t_mul;
@@ -359,22 +355,23 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
           }
         }
         if (out.colsum_partial) {
-          // The four quarters' sums in a fixed order (double-buffered by item, so a warp
-          // running one item ahead cannot overwrite what the quarter-0 warps still read).
+          // The four warps' sums in a fixed order (double-buffered by item, so a warp
+          // running one item ahead cannot overwrite what warp 4 still reads).
           __syncwarp();
           if (lane == 0) mbar_arrive(&sm.cs_ready);
           if (!mbar_wait(&sm.cs_ready, (uint32_t)(item_no & 1), abort)) break;
           if (quad == 0) {
             const double(*cs)[kN] = sm.colsum[item_no & 1];
-            const int j = (int)half * kH + lane;
-            const double tsum = ((cs[0][j] + cs[1][j]) + cs[2][j]) + cs[3][j];
-            out.colsum_partial[(uint64_t)tile * kN + j] = tsum;
+            for (int j = lane; j < kN; j += 32) {
+              double tsum = ((cs[0][j] + cs[1][j]) + cs[2][j]) + cs[3][j];
+              out.colsum_partial[(uint64_t)tile * kN + j] = tsum;
+            }
           }
         }
       } else if (row < rows) {
-        double* dst = out.partial + ((uint64_t)seg * rows + row) * kN + half * kH;
+        double* dst = out.partial + ((uint64_t)seg * rows + row) * kN;
 #pragma unroll
-        for (int j = 0; j < kH; ++j) dst[j] = acc[j] * out_scale;
+        for (int j = 0; j < kN; ++j) dst[j] = acc[j] * out_scale;
       }
     }
   } else if (warp == kExpandWarps + kDrainWarps) {
