@@ -363,13 +363,21 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
       const uint64_t len = !scan.list_tiles ? n_tiles
                            : scan.list_off  ? scan.list_off[qb + 1] - l0
                                             : scan.list_stride;
-      uint32_t win_tile = 0;
-      float win_lb2 = 0.0f;
+      // The list is read 32 entries a window, the next window's loads issued a window
+      // ahead (their latency hides behind 32 tiles).
+      uint32_t win_tile = 0, nxt_tile = 0;
+      float win_lb2 = 0.0f, nxt_lb2 = 0.0f;
+      auto load_window = [&](uint64_t i0, uint32_t& t, float& b) {
+        t = i0 + lane < len ? scan.list_tiles[l0 + i0 + lane] : 0u;
+        b = (scan.list_lb2 && i0 + lane < len) ? scan.list_lb2[l0 + i0 + lane] : 0.0f;
+      };
+      if (scan.list_tiles) load_window(0, nxt_tile, nxt_lb2);
       for (uint64_t i = 0;; ++i) {
         const uint32_t at = (uint32_t)(i & 31);
         if (at == 0 && scan.list_tiles) {
-          win_tile = i + lane < len ? scan.list_tiles[l0 + i + lane] : 0u;
-          win_lb2 = (scan.list_lb2 && i + lane < len) ? scan.list_lb2[l0 + i + lane] : 0.0f;
+          win_tile = nxt_tile;
+          win_lb2 = nxt_lb2;
+          if (i + 32 < len) load_window(i + 32, nxt_tile, nxt_lb2);
         }
         const uint32_t lt = __shfl_sync(0xFFFFFFFFu, win_tile, at);
         const float lb2 = __shfl_sync(0xFFFFFFFFu, win_lb2, at);
@@ -378,14 +386,16 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
           // takes its value, so every lane makes the same choice.
           float u = 0.0f;
           if (lane == 0) {
+            // All eight words loaded at once; a warp yet to publish for this block bounds
+            // nothing.
+            unsigned long long v[kEpiWarps];
+#pragma unroll
+            for (int w = 0; w < kEpiWarps; ++w) v[w] = u_pub[w];
             u = -INFINITY;
-            for (int w = 0; w < kEpiWarps; ++w) {
-              const unsigned long long v = u_pub[w];
-              // A warp yet to publish for this block bounds nothing.
-              u = (uint32_t)(v >> 32) == (uint32_t)qb ? fmaxf(u, __uint_as_float((uint32_t)v))
-                                                      : INFINITY;
-              if (u == INFINITY) break;
-            }
+#pragma unroll
+            for (int w = 0; w < kEpiWarps; ++w)
+              u = (uint32_t)(v[w] >> 32) == (uint32_t)qb ? fmaxf(u, __uint_as_float((uint32_t)v[w]))
+                                                         : INFINITY;
           }
           u = __shfl_sync(0xFFFFFFFFu, u, 0);
           if (lb2 > u) {

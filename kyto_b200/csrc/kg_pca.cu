@@ -966,7 +966,7 @@ struct TcHeld {
     sm = sm_count;
     build_blocked(indptr, col, val, n, g, nnz, bx, s);
     trace.mark("blocked X");
-    transpose_blocked(bx, bxt, s);
+    transpose_blocked(indptr, col, val, n, g, nnz, bx, bxt, s);
     trace.mark("blocked X^T");
     dt.alloc(64 * dense_ld(n), s);
     dt.zero();
@@ -1909,7 +1909,7 @@ kg_status kg_diag_spmm(kg_ctx* ctx, const uint64_t* indptr, const uint32_t* indi
     build_blocked(d_ptr, d_idx, d_val, n_rows, n_cols, nnz, bx, s);
     const Blocked* sp = &bx;
     if (transposed) {
-      transpose_blocked(bx, bxt, s);
+      transpose_blocked(d_ptr, d_idx, d_val, n_rows, n_cols, nnz, bx, bxt, s);
       sp = &bxt;
     }
     const uint64_t rows = sp->rows, K = sp->K, ld = dense_ld(K);

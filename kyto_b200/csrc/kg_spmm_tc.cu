@@ -63,8 +63,9 @@ constexpr int kN = 64;                  // output columns (N)
 constexpr int kLoadStages = 8;
 constexpr int kFlushChunks = 16;        // K-chunks summed in f32 before the f64 flush
 constexpr uint32_t kBBytes = kN * 128;  // 8 KB: 64 rows x (32 hi + 32 lo) fp16
-constexpr uint32_t kMaskBytes = kRows * 4;
-constexpr uint32_t kBlockMaxBytes = kMaskBytes + kRows * kChunk * 4;
+constexpr uint32_t kHeaderBytes = 64 * 8;  // (mask, base) per row quarter and column pair
+constexpr uint32_t kBlockMaxBytes = kHeaderBytes + kRows * (kChunk / 2) * 8;
+constexpr uint32_t kAbsentHi = 0x8000u;  // fp16 -0: the high part of a column without a value
 constexpr int kExpandWarps = 4;
 constexpr int kDrainWarps = 4;
 constexpr int kSpThreads = (kExpandWarps + kDrainWarps + 2) * 32;
@@ -77,17 +78,16 @@ static_assert(kABase + kABufs * kACols <= kTmemColsS, "TMEM columns");
 
 struct LoadStage {
   uint8_t b[kBBytes];
-  uint8_t blk[(kBlockMaxBytes + 1023) / 1024 * 1024];  // masks, then the values
+  uint8_t blk[(kBlockMaxBytes + 1023) / 1024 * 1024];  // header, then the entries
 };
+// The expansion may read one entry past a full block's last.
+static_assert(sizeof(LoadStage::blk) >= kBlockMaxBytes + 8, "stage room past the entries");
 // Swizzled tiles (TMA destinations, MMA operands) start on 1024-byte boundaries.
 static_assert(sizeof(LoadStage) % 1024 == 0, "load stage size");
 
 struct SpSmem {
   LoadStage st[kLoadStages];
   double colsum[2][kDrainWarps][kN];
-  // Per expand warp, per column of the current block: its mask word for the warp's 32
-  // rows and the rank of its first value there.
-  alignas(16) uint2 meta[kExpandWarps][kChunk];
   uint64_t ld_full[kLoadStages], ld_empty[kLoadStages];
   uint64_t a_full[kABufs], a_empty[kABufs];
   uint64_t cs_ready;
@@ -126,11 +126,8 @@ __device__ __forceinline__ uint32_t split_pair(float x) {
   return (uint32_t)__half_as_ushort(hi) | ((uint32_t)__half_as_ushort(lo) << 16);
 }
 
-// hi + lo of a pair word (exact in f32: 22 significant bits at most).
-__device__ __forceinline__ float pair_value(uint32_t w) {
-  return __half2float(__ushort_as_half((unsigned short)(w & 0xFFFFu))) +
-         __half2float(__ushort_as_half((unsigned short)(w >> 16)));
-}
+struct ValueMap;
+__device__ __forceinline__ uint2 map_entry(uint2 e, const ValueMap& vm, float mean_r);
 
 struct Geometry {
   uint32_t n_tiles, n_chunks, seg_chunks, n_segs;
@@ -155,6 +152,27 @@ struct ValueMap {
   int mode;
   float unscale, sq_scale;
 };
+
+// An entry's two columns mapped by the value mode: kValueOne gives 1 where a column holds
+// a value, kValueCentredSquare (v - mean_r)^2 scaled; a column without a value gives 0.
+__device__ __forceinline__ uint2 map_entry(uint2 e, const ValueMap& vm, float mean_r) {
+  uint32_t hx = 0, lx = 0;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const uint32_t hi = (e.x >> (16 * k)) & 0xFFFFu, lo = (e.y >> (16 * k)) & 0xFFFFu;
+    if (hi == kAbsentHi) continue;
+    uint32_t w = 0x3C00u;  // fp16 1.0, low part 0
+    if (vm.mode == kValueCentredSquare) {
+      const float v = __half2float(__ushort_as_half((unsigned short)hi)) +
+                      __half2float(__ushort_as_half((unsigned short)lo));
+      const float d = v * vm.unscale - mean_r;
+      w = split_pair(d * d * vm.sq_scale);
+    }
+    hx |= (w & 0xFFFFu) << (16 * k);
+    lx |= (w >> 16) << (16 * k);
+  }
+  return make_uint2(hx, lx);
+}
 
 // One CTA per SM. The register file is split over the SM's four sub-partitions, so ten
 // warps fit only at 168 registers a thread (three warps on two of them); the drain warps'
@@ -201,7 +219,7 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
     // ----------------------------------------------------------- expand -------------
     const uint32_t q = (uint32_t)warp;        // rows 32 q .. 32 q + 31 of each block
     const uint32_t lt = (1u << lane) - 1u;    // the lanes (rows) before this one
-    const uint4* meta4 = reinterpret_cast<const uint4*>(sm.meta[q]);
+    const uint32_t lb = 1u << lane;
     uint64_t it = 0;
     bool ok = true;
     for (uint64_t w = blockIdx.x; w < n_items && ok; w += gridDim.x) {
@@ -223,65 +241,40 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
         }
         tc_fence_after();
         const LoadStage& st = sm.st[ls];
-        const uint32_t* masks = reinterpret_cast<const uint32_t*>(st.blk);
-        const uint32_t* vals = reinterpret_cast<const uint32_t*>(st.blk + kMaskBytes);
-        // Lane c: column c's mask word for this warp's rows, and the rank of its first
-        // value there (the values of the columns before c, then of c's rows in the warps
-        // before this one). The exclusive scan of the column counts (at most 128, 8 bits)
-        // takes one ballot per bit.
-        uint32_t m_own = 0, base = 0;
-        if (sm.present[ls]) {
-          uint32_t colcount = 0, pre = 0;
-#pragma unroll
-          for (int qq = 0; qq < 4; ++qq) {
-            const uint32_t mw = masks[qq * 32 + lane];
-            const uint32_t cnt = __popc(mw);
-            colcount += cnt;
-            if (qq < (int)q) pre += cnt;
-            if (qq == (int)q) m_own = mw;
-          }
-          uint32_t excl = 0;
-#pragma unroll
-          for (int b = 0; b < 8; ++b)
-            excl += (uint32_t)__popc(__ballot_sync(0xFFFFFFFFu, (colcount >> b) & 1u) & lt) << b;
-          base = excl + pre;
-        }
-        sm.meta[q][lane] = make_uint2(m_own, base);
-        __syncwarp();
-        // Row (32 q + lane) of the A tiles: for each column, the value at its rank if the
-        // row stores one (lanes that do read consecutive words; the others read a
-        // neighbour's and drop it), two columns a word, hi parts then lo parts.
-        // Two halves of 8 column pairs each: hi words to columns 8 h.., lo words to 16 + 8 h..
+        // This quarter's 16 (mask, base) words, two pairs a 16-byte load, and the entries.
+        const uint4* hdr = reinterpret_cast<const uint4*>(st.blk) + q * 8;
+        const uint2* ent = reinterpret_cast<const uint2*>(st.blk + kHeaderBytes);
+        const bool present = sm.present[ls] != 0;
+        // Row (32 q + lane) of the A tiles: pair p's high-part word to column p, its
+        // low-part word to column 16 + p (a row without an entry for the pair: zeros).
         const uint32_t arow = tmem + ((q * 32u) << 16) + kABase + ab * kACols;
 #pragma unroll
         for (int hh = 0; hh < 2; ++hh) {
           uint32_t hw[8], lw[8];
 #pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            const uint4 mm = meta4[8 * hh + i];  // (mask, rank) of columns 2 c2, 2 c2 + 1
-            uint32_t x0 = vals[mm.y + __popc(mm.x & lt)];
-            uint32_t x1 = vals[mm.w + __popc(mm.z & lt)];
-            const bool h0 = (mm.x >> lane) & 1u, h1 = (mm.z >> lane) & 1u;
-            if (vmap.mode == kValueOne) {
-              x0 = 0x3C00u;  // fp16 1.0, low part 0
-              x1 = 0x3C00u;
-            } else if (vmap.mode == kValueCentredSquare) {
-              const float d0 = pair_value(x0) * vmap.unscale - mean_r;
-              const float d1 = pair_value(x1) * vmap.unscale - mean_r;
-              x0 = split_pair(d0 * d0 * vmap.sq_scale);
-              x1 = split_pair(d1 * d1 * vmap.sq_scale);
+          for (int i = 0; i < 4; ++i) {
+            // Every lane loads (no divergence): a lane without an entry reads the next
+            // lane's, or one past the block's last entry (inside the stage buffer), and
+            // drops it.
+            const uint4 m = present ? hdr[4 * hh + i] : make_uint4(0u, 0u, 0u, 0u);
+            uint2 e0 = ent[m.y + __popc(m.x & lt)];
+            uint2 e1 = ent[m.w + __popc(m.z & lt)];
+            if (vmap.mode != kValuePlain) {
+              e0 = map_entry(e0, vmap, mean_r);
+              e1 = map_entry(e1, vmap, mean_r);
             }
-            x0 = h0 ? x0 : 0u;
-            x1 = h1 ? x1 : 0u;
-            hw[i] = __byte_perm(x0, x1, 0x5410);  // hi parts of both columns
-            lw[i] = __byte_perm(x0, x1, 0x7632);  // lo parts
+            const bool h0 = (m.x & lb) != 0, h1 = (m.z & lb) != 0;
+            hw[2 * i] = h0 ? e0.x : 0u;
+            lw[2 * i] = h0 ? e0.y : 0u;
+            hw[2 * i + 1] = h1 ? e1.x : 0u;
+            lw[2 * i + 1] = h1 ? e1.y : 0u;
           }
           tmem_st_8(arow + 8u * hh, hw);
           tmem_st_8(arow + 16u + 8u * hh, lw);
         }
         tmem_wait_st();
         tc_fence_before();
-        __syncwarp();  // every lane has read meta before the next block rewrites it
+        __syncwarp();  // every lane has read the stage
         if (lane == 0) {
           mbar_arrive(&sm.a_full[ab]);
           mbar_arrive(&sm.ld_empty[ls]);
@@ -534,196 +527,137 @@ __global__ void csr_stats_kernel(const uint64_t* ptr, const float* val, uint64_t
   }
 }
 
-// The block of a stored value, and its row (in the tile) and column (in the chunk).
-__device__ __forceinline__ void locate(uint64_t r, uint32_t c, uint32_t n_chunks,
-                                       uint64_t& block, uint32_t& br, uint32_t& bc) {
-  block = (r / kRows) * n_chunks + c / kChunk;
-  br = (uint32_t)(r % kRows);
-  bc = (uint32_t)(c % kChunk);
+// Where a stored value of the CSR lands: its layout row and column (the CSR's row and
+// column, or swapped for the transpose), the block, the header word (row quarter, column
+// pair) and the row's bit in that word.
+struct Place {
+  uint64_t block;
+  uint32_t word, bit, half;
+};
+__device__ __forceinline__ Place place(uint64_t r, uint32_t c, bool transposed,
+                                       uint32_t n_chunks) {
+  const uint64_t lr = transposed ? c : r, lc = transposed ? r : c;
+  Place p;
+  p.block = (lr / kRows) * n_chunks + lc / kChunk;
+  p.word = (uint32_t)((lr % kRows) / 32) * 16 + (uint32_t)((lc % kChunk) / 2);
+  p.bit = (uint32_t)(lr % 32);
+  p.half = (uint32_t)(lc % 2);
+  return p;
 }
 
-// Stored values per block (warp per CSR row; lanes whose values share a block add once).
-__global__ void blocked_count_kernel(const uint64_t* ptr, const uint32_t* col, uint64_t n_rows,
-                                     uint32_t n_chunks, uint32_t* counts) {
-  uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  unsigned lane = threadIdx.x & 31u;
+// Header masks (n_blocks x 64 words, zeroed): warp per CSR row; lanes whose values share
+// a word OR their bits together and one of them writes.
+__global__ void pair_mask_kernel(const uint64_t* ptr, const uint32_t* col, uint64_t n_rows,
+                                 bool transposed, uint32_t n_chunks, uint32_t* masks) {
+  const uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
   if (r >= n_rows) return;
   for (uint64_t i0 = ptr[r]; i0 < ptr[r + 1]; i0 += 32) {
-    uint64_t i = i0 + lane;
-    bool in = i < ptr[r + 1];
-    unsigned active = __ballot_sync(0xFFFFFFFFu, in);
+    const uint64_t i = i0 + lane;
+    const bool in = i < ptr[r + 1];
+    const unsigned active = __ballot_sync(0xFFFFFFFFu, in);
     if (!in) continue;
-    uint64_t block;
-    uint32_t br, bc;
-    locate(r, col[i], n_chunks, block, br, bc);
-    unsigned same = __match_any_sync(active, block);
-    if ((unsigned)__ffs(same) - 1 == lane) atomicAdd(&counts[block], (uint32_t)__popc(same));
+    const Place pl = place(r, col[i], transposed, n_chunks);
+    const uint64_t word = pl.block * 64 + pl.word;
+    const unsigned same = __match_any_sync(active, word);
+    const uint32_t bits = __reduce_or_sync(same, 1u << pl.bit);
+    if ((unsigned)__ffs(same) - 1 == lane) atomicOr(&masks[word], bits);
   }
 }
 
-// A block's size in 16-byte units: 128 mask words and its values padded to 4 (none for
-// an empty block).
-__global__ void block_units_kernel(const uint32_t* counts, uint64_t n, uint64_t* units) {
-  uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-  if (i < n) units[i] = counts[i] ? kMaskBytes / 16 + ((uint64_t)counts[i] + 3) / 4 : 0;
-  if (i == n) units[i] = 0;
-}
-
-// Column masks: bit (row % 32) of word (row / 32) * 32 + column marks a stored value. The
-// lanes of a CSR row hit different columns, so one row's values never share a word.
-__global__ void blocked_mask_kernel(const uint64_t* ptr, const uint32_t* col, uint64_t n_rows,
-                                    uint32_t n_chunks, const uint64_t* off, uint8_t* data) {
-  uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  unsigned lane = threadIdx.x & 31u;
-  if (r >= n_rows) return;
-  for (uint64_t i = ptr[r] + lane; i < ptr[r + 1]; i += 32) {
-    uint64_t block;
-    uint32_t br, bc;
-    locate(r, col[i], n_chunks, block, br, bc);
-    uint32_t* word = reinterpret_cast<uint32_t*>(data + off[block] * 16) + (br / 32) * 32 + bc;
-    atomicOr(word, 1u << (br % 32));
+// Per block (warp): each header word's base (the entries of the words before it) and the
+// block's size in 16-byte units (0 for a block without entries).
+__global__ void pair_base_kernel(const uint32_t* masks, uint64_t n_blocks, uint16_t* bases,
+                                 uint64_t* units) {
+  const uint64_t b = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  if (b > n_blocks) return;
+  if (b == n_blocks) {
+    if (lane == 0) units[b] = 0;
+    return;
   }
-}
-
-// prefix[b * 128 + q * 32 + c]: the values of block b before its rows 32 q.. of column c
-// (the columns before c, then column c's earlier row quarters); warp per block.
-__global__ void col_prefix_kernel(const uint64_t* off, const uint8_t* data, uint64_t n_blocks,
-                                  uint16_t* prefix) {
-  uint64_t b = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  unsigned lane = threadIdx.x & 31u;
-  if (b >= n_blocks || off[b + 1] == off[b]) return;
-  const uint32_t* masks = reinterpret_cast<const uint32_t*>(data + off[b] * 16);
-  uint32_t cnt[4], total = 0;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    cnt[q] = __popc(masks[q * 32 + lane]);
-    total += cnt[q];
-  }
-  uint32_t incl = total;
+  const uint32_t c0 = __popc(masks[b * 64 + 2 * lane]), c1 = __popc(masks[b * 64 + 2 * lane + 1]);
+  uint32_t incl = c0 + c1;
   for (int o = 1; o < 32; o <<= 1) {
-    uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+    const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
     if ((int)lane >= o) incl += t;
   }
-  uint32_t at = incl - total;
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    prefix[b * kRows + q * 32 + lane] = (uint16_t)at;
-    at += cnt[q];
-  }
+  const uint32_t excl = incl - c0 - c1;
+  bases[b * 64 + 2 * lane] = (uint16_t)excl;
+  bases[b * 64 + 2 * lane + 1] = (uint16_t)(excl + c0);
+  const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+  if (lane == 0) units[b] = total ? (kHeaderBytes + 8ull * total + 15) / 16 : 0;
 }
 
-// Each value, scaled and split, at its rank in its block.
-__global__ void blocked_values_kernel(const uint64_t* ptr, const uint32_t* col, const float* val,
-                                      uint64_t n_rows, uint32_t n_chunks, const uint64_t* off,
-                                      const uint16_t* prefix, int scale, uint8_t* data) {
-  uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  unsigned lane = threadIdx.x & 31u;
+// Per block (warp): the header, and every entry set to "no value in either column"
+// (kAbsentHi high parts, zero low parts) before the values are placed.
+__global__ void pair_header_kernel(const uint32_t* masks, const uint16_t* bases,
+                                   const uint64_t* off, uint64_t n_blocks, uint8_t* data) {
+  const uint64_t b = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  if (b >= n_blocks || off[b + 1] == off[b]) return;
+  uint2* blk = reinterpret_cast<uint2*>(data + off[b] * 16);
+  for (uint32_t h = lane; h < 64; h += 32) blk[h] = make_uint2(masks[b * 64 + h], bases[b * 64 + h]);
+  const uint64_t words = (off[b + 1] - off[b]) * 2 - 64;  // entries and the padding
+  for (uint64_t e = lane; e < words; e += 32)
+    blk[64 + e] = make_uint2(kAbsentHi | (kAbsentHi << 16), 0u);
+}
+
+// Each value, scaled and split, into its half of its entry (warp per CSR row).
+__global__ void pair_values_kernel(const uint64_t* ptr, const uint32_t* col, const float* val,
+                                   uint64_t n_rows, bool transposed, uint32_t n_chunks,
+                                   const uint64_t* off, int scale, uint8_t* data) {
+  const uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
   if (r >= n_rows) return;
   for (uint64_t i = ptr[r] + lane; i < ptr[r + 1]; i += 32) {
-    uint64_t block;
-    uint32_t br, bc;
-    locate(r, col[i], n_chunks, block, br, bc);
-    uint8_t* blk = data + off[block] * 16;
-    const uint32_t wi = (br / 32) * 32 + bc;
-    const uint32_t word = reinterpret_cast<const uint32_t*>(blk)[wi];
-    const uint32_t rank = prefix[block * kRows + wi] + __popc(word & ((1u << (br % 32)) - 1u));
-    reinterpret_cast<uint32_t*>(blk + kMaskBytes)[rank] = split_pair(ldexpf(val[i], scale));
+    const Place pl = place(r, col[i], transposed, n_chunks);
+    uint8_t* blk = data + off[pl.block] * 16;
+    const uint2 hd = reinterpret_cast<const uint2*>(blk)[pl.word];
+    const uint32_t e = hd.y + __popc(hd.x & ((1u << pl.bit) - 1u));
+    // A stored -0 is kept as +0 (-0 marks a column without a value).
+    const float x = ldexpf(val[i], scale);
+    const uint32_t w = split_pair(x == 0.0f ? 0.0f : x);
+    uint16_t* ent = reinterpret_cast<uint16_t*>(blk + kHeaderBytes + 8ull * e);
+    ent[pl.half] = (uint16_t)(w & 0xFFFFu);
+    ent[2 + pl.half] = (uint16_t)(w >> 16);
   }
 }
 
-// ---------------------------------------------------------------- the transpose --
-//
-// X^T's blocked layout from X's (no pass over the CSR, no atomics). Block (G, c) of X^T
-// (genes 128 G.., cells 32 c..) holds row quarter i from X block (tile c / 4, gene chunk
-// 4 G + i), whose cell rows 32 (c % 4) + l it transposes: X^T's mask word i * 32 + l (gene
-// rows 32 i.., cell column l) has bit j set where X's mask word (c % 4) * 32 + j (cell
-// rows 32 (c % 4).., gene column j) has bit l. One warp per X^T block: lane j holds X's
-// word for gene column j of each source; a ballot per (l, i) forms X^T's word and places
-// the values of column l, gene rows in order.
-
-// Source block i of X^T block (G, c), or ~0 past X's gene chunks.
-__device__ __forceinline__ uint64_t transpose_source(uint32_t G, uint32_t c, int i,
-                                                     uint32_t x_chunks) {
-  const uint32_t chunk = 4 * G + (uint32_t)i;
-  return chunk < x_chunks ? (uint64_t)(c / 4) * x_chunks + chunk : ~0ull;
-}
-
-__global__ void transpose_count_kernel(const uint64_t* x_off, const uint8_t* x_data,
-                                       uint32_t x_chunks, uint32_t t_tiles, uint32_t t_chunks,
-                                       uint32_t* counts) {
-  const uint64_t b = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const unsigned lane = threadIdx.x & 31u;
-  if (b >= (uint64_t)t_tiles * t_chunks) return;
-  const uint32_t G = (uint32_t)(b / t_chunks), c = (uint32_t)(b % t_chunks);
-  uint32_t count = 0;
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const uint64_t src = transpose_source(G, c, i, x_chunks);
-    if (src == ~0ull || x_off[src + 1] == x_off[src]) continue;
-    const uint32_t* masks = reinterpret_cast<const uint32_t*>(x_data + x_off[src] * 16);
-    count += __popc(masks[32 * (c % 4) + lane]);
+// The layout (rows x K) of the CSR (n_rows x n_cols) or of its transpose.
+void build_pairs(const uint64_t* ptr, const uint32_t* col, const float* val, uint64_t n_rows,
+                 uint64_t nnz, bool transposed, Blocked& out, cudaStream_t s) {
+  out.n_tiles = (uint32_t)((out.rows + kRows - 1) / kRows);
+  out.n_chunks = (uint32_t)((out.K + kChunk - 1) / kChunk);
+  const uint64_t nb = (uint64_t)out.n_tiles * out.n_chunks;
+  DeviceBuffer<uint32_t> masks(nb * 64, s);
+  masks.zero();
+  if (nnz) {
+    pair_mask_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(ptr, col, n_rows, transposed,
+                                                                  out.n_chunks, masks.ptr);
+    KG_LAUNCH_CHECK();
   }
-  for (int o = 16; o; o >>= 1) count += __shfl_xor_sync(0xFFFFFFFFu, count, o);
-  if (lane == 0) counts[b] = count;
-}
-
-__global__ void transpose_fill_kernel(const uint64_t* x_off, const uint8_t* x_data,
-                                      uint32_t x_chunks, uint32_t t_tiles, uint32_t t_chunks,
-                                      const uint64_t* t_off, uint8_t* t_data) {
-  const uint64_t b = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const unsigned lane = threadIdx.x & 31u;
-  if (b >= (uint64_t)t_tiles * t_chunks || t_off[b + 1] == t_off[b]) return;
-  const uint32_t G = (uint32_t)(b / t_chunks), c = (uint32_t)(b % t_chunks);
-  const uint32_t g = c % 4;  // the source blocks' cell row quarter
-  const uint32_t lt = (1u << lane) - 1u;
-  uint32_t src_mask[4], src_rank[4];
-  const uint32_t* src_vals[4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    src_mask[i] = 0;
-    src_rank[i] = 0;
-    src_vals[i] = nullptr;
-    const uint64_t src = transpose_source(G, c, i, x_chunks);
-    if (src != ~0ull && x_off[src + 1] != x_off[src]) {
-      const uint8_t* blk = x_data + x_off[src] * 16;
-      const uint32_t* masks = reinterpret_cast<const uint32_t*>(blk);
-      src_vals[i] = reinterpret_cast<const uint32_t*>(blk + kMaskBytes);
-      // Gene column j = lane of the source: its first value (the columns before it, then
-      // its rows before quarter g).
-      uint32_t total = 0, before = 0;
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint32_t mw = masks[q * 32 + lane];
-        total += __popc(mw);
-        if (q < (int)g) before += __popc(mw);
-        if (q == (int)g) src_mask[i] = mw;
-      }
-      uint32_t incl = total;
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
-        if ((int)lane >= o) incl += t;
-      }
-      src_rank[i] = incl - total + before;
-    }
-  }
-  uint8_t* out = t_data + t_off[b] * 16;
-  uint32_t* out_masks = reinterpret_cast<uint32_t*>(out);
-  uint32_t* out_vals = reinterpret_cast<uint32_t*>(out + kMaskBytes);
-  uint32_t mine[4] = {0, 0, 0, 0};
-  uint32_t at = 0;  // values placed so far (column-major order)
-  for (int l = 0; l < 32; ++l) {
-    const uint32_t below_l = (1u << l) - 1u;
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-      const bool has = (src_mask[i] >> l) & 1u;
-      const uint32_t m = __ballot_sync(0xFFFFFFFFu, has);  // X^T word i * 32 + l
-      if ((int)lane == l) mine[i] = m;
-      if (has) out_vals[at + __popc(m & lt)] = src_vals[i][src_rank[i] + __popc(src_mask[i] & below_l)];
-      at += __popc(m);
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < 4; ++i) out_masks[32 * i + lane] = mine[i];
+  DeviceBuffer<uint16_t> bases(nb * 64, s);
+  out.off.alloc(nb + 1, s);
+  pair_base_kernel<<<blocks_for((nb + 1) * 32, 256), 256, 0, s>>>(masks.ptr, nb, bases.ptr,
+                                                                  out.off.ptr);
+  KG_LAUNCH_CHECK();
+  size_t temp = 0;
+  KG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, out.off.ptr, out.off.ptr, nb + 1, s));
+  DeviceBuffer<unsigned char> scratch(temp, s);
+  KG_CUDA(cub::DeviceScan::ExclusiveSum(scratch.ptr, temp, out.off.ptr, out.off.ptr, nb + 1, s));
+  uint64_t units = 0;
+  KG_CUDA(cudaMemcpyAsync(&units, out.off.ptr + nb, 8, cudaMemcpyDeviceToHost, s));
+  KG_CUDA(cudaStreamSynchronize(s));
+  out.bytes = units * 16;
+  out.data.alloc(std::max<uint64_t>(out.bytes, 16), s);
+  if (!units) return;
+  pair_header_kernel<<<blocks_for(nb * 32, 256), 256, 0, s>>>(masks.ptr, bases.ptr, out.off.ptr,
+                                                              nb, out.data.ptr);
+  KG_LAUNCH_CHECK();
+  pair_values_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(
+      ptr, col, val, n_rows, transposed, out.n_chunks, out.off.ptr, out.scale, out.data.ptr);
+  KG_LAUNCH_CHECK();
 }
 
 }  // namespace
@@ -732,9 +666,6 @@ void build_blocked(const uint64_t* ptr, const uint32_t* col, const float* val, u
                    uint64_t n_cols, uint64_t nnz, Blocked& out, cudaStream_t s) {
   out.rows = n_rows;
   out.K = n_cols;
-  out.n_tiles = (uint32_t)((out.rows + kRows - 1) / kRows);
-  out.n_chunks = (uint32_t)((out.K + kChunk - 1) / kChunk);
-  const uint64_t nb = (uint64_t)out.n_tiles * out.n_chunks;
   // The values' range (the scale of their fp16 parts) and the largest row norm.
   DeviceBuffer<unsigned long long> st(3, s);
   const unsigned long long init[3] = {0ull, 0ull, 0x7FF0000000000000ull};  // 0, 0, +inf
@@ -744,24 +675,7 @@ void build_blocked(const uint64_t* ptr, const uint32_t* col, const float* val, u
                                                                   st.ptr + 1, st.ptr + 2);
     KG_LAUNCH_CHECK();
   }
-  DeviceBuffer<uint32_t> counts(nb, s);
-  counts.zero();
-  if (nnz) {
-    blocked_count_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(ptr, col, n_rows,
-                                                                      out.n_chunks, counts.ptr);
-    KG_LAUNCH_CHECK();
-  }
-  out.off.alloc(nb + 1, s);
-  block_units_kernel<<<blocks_for(nb + 1, 256), 256, 0, s>>>(counts.ptr, nb, out.off.ptr);
-  KG_LAUNCH_CHECK();
-  counts.reset();
-  size_t temp = 0;
-  KG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, out.off.ptr, out.off.ptr, nb + 1, s));
-  DeviceBuffer<unsigned char> scratch(temp, s);
-  KG_CUDA(cub::DeviceScan::ExclusiveSum(scratch.ptr, temp, out.off.ptr, out.off.ptr, nb + 1, s));
-  uint64_t units = 0;
   unsigned long long h_st[3];
-  KG_CUDA(cudaMemcpyAsync(&units, out.off.ptr + nb, 8, cudaMemcpyDeviceToHost, s));
   KG_CUDA(cudaMemcpyAsync(h_st, st.ptr, sizeof h_st, cudaMemcpyDeviceToHost, s));
   KG_CUDA(cudaStreamSynchronize(s));
   double d[3];
@@ -770,55 +684,19 @@ void build_blocked(const uint64_t* ptr, const uint32_t* col, const float* val, u
   out.max_abs = d[1];
   out.min_abs = std::isinf(d[2]) ? 0.0 : d[2];
   out.scale = part_scale(out.max_abs);
-  out.bytes = units * 16;
-  out.data.alloc(std::max<uint64_t>(out.bytes, 16), s);
-  // Padding past a block's values must read as zero (the expansion may load one past).
-  out.data.zero();
-  if (nnz) {
-    blocked_mask_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(
-        ptr, col, n_rows, out.n_chunks, out.off.ptr, out.data.ptr);
-    KG_LAUNCH_CHECK();
-    DeviceBuffer<uint16_t> prefix(nb * kRows, s);
-    col_prefix_kernel<<<blocks_for(nb * 32, 256), 256, 0, s>>>(out.off.ptr, out.data.ptr, nb,
-                                                               prefix.ptr);
-    KG_LAUNCH_CHECK();
-    blocked_values_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(
-        ptr, col, val, n_rows, out.n_chunks, out.off.ptr, prefix.ptr, out.scale, out.data.ptr);
-    KG_LAUNCH_CHECK();
-  }
+  build_pairs(ptr, col, val, n_rows, nnz, false, out, s);
 }
 
-void transpose_blocked(const Blocked& x, Blocked& out, cudaStream_t s) {
-  out.rows = x.K;
-  out.K = x.rows;
-  out.n_tiles = (uint32_t)((out.rows + kRows - 1) / kRows);
-  out.n_chunks = (uint32_t)((out.K + kChunk - 1) / kChunk);
+void transpose_blocked(const uint64_t* ptr, const uint32_t* col, const float* val,
+                       uint64_t n_rows, uint64_t n_cols, uint64_t nnz, const Blocked& x,
+                       Blocked& out, cudaStream_t s) {
+  out.rows = n_cols;
+  out.K = n_rows;
   out.scale = x.scale;
   out.max_abs = x.max_abs;
   out.min_abs = x.min_abs;
   out.max_row_norm = 0.0;  // not tracked for the transpose
-  const uint64_t nb = (uint64_t)out.n_tiles * out.n_chunks;
-  DeviceBuffer<uint32_t> counts(nb, s);
-  transpose_count_kernel<<<blocks_for(nb * 32, 256), 256, 0, s>>>(
-      x.off.ptr, x.data.ptr, x.n_chunks, out.n_tiles, out.n_chunks, counts.ptr);
-  KG_LAUNCH_CHECK();
-  out.off.alloc(nb + 1, s);
-  block_units_kernel<<<blocks_for(nb + 1, 256), 256, 0, s>>>(counts.ptr, nb, out.off.ptr);
-  KG_LAUNCH_CHECK();
-  counts.reset();
-  size_t temp = 0;
-  KG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, temp, out.off.ptr, out.off.ptr, nb + 1, s));
-  DeviceBuffer<unsigned char> scratch(temp, s);
-  KG_CUDA(cub::DeviceScan::ExclusiveSum(scratch.ptr, temp, out.off.ptr, out.off.ptr, nb + 1, s));
-  uint64_t units = 0;
-  KG_CUDA(cudaMemcpyAsync(&units, out.off.ptr + nb, 8, cudaMemcpyDeviceToHost, s));
-  KG_CUDA(cudaStreamSynchronize(s));
-  out.bytes = units * 16;
-  out.data.alloc(std::max<uint64_t>(out.bytes, 16), s);
-  out.data.zero();
-  transpose_fill_kernel<<<blocks_for(nb * 32, 256), 256, 0, s>>>(
-      x.off.ptr, x.data.ptr, x.n_chunks, out.n_tiles, out.n_chunks, out.off.ptr, out.data.ptr);
-  KG_LAUNCH_CHECK();
+  build_pairs(ptr, col, val, n_rows, nnz, true, out, s);
 }
 
 void spmm_tc(const SpmmArgs& a, cudaStream_t s) {

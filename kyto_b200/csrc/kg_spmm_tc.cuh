@@ -8,18 +8,23 @@
 
 namespace kg {
 
-// A sparse matrix (rows x K) cut into blocks of 128 rows x 32 columns. Block
+// A sparse matrix (rows x K) cut into blocks of 128 rows x 32 columns, each column pair
+// (2p, 2p + 1) stored as one entry per row that holds a value in either column. Block
 // b = tile * n_chunks + chunk starts at byte 16 * off[b] of `data` and is empty
-// (off[b + 1] == off[b]) or holds 128 column mask words followed by its values:
-//  - mask word q * 32 + c has bit l set where row 32 q + l of the block stores a value in
-//    column c;
-//  - the values follow column by column, rows in order inside a column, padded to a
-//    multiple of 4 words (16 bytes, one bulk copy per block);
-//  - a value is one 32-bit word holding x = value * 2^scale in two fp16 parts: bits 0-15
-//    hi = fp16(x), bits 16-31 lo = fp16(x - hi) (together about 22 bits of x).
-// Column order makes the product's expansion conflict-free: for one column, the threads of
-// a warp (one row each) read consecutive words. At the benchmark's 33% density a block is
-// 512 + 4 nnz bytes, against 8 nnz for a u32 index and an f32 value.
+// (off[b + 1] == off[b]) or holds a header of 64 (mask, base) words followed by its
+// entries:
+//  - header word q * 16 + p (rows 32 q .. 32 q + 31, pair p): bit l of the mask is set
+//    where row 32 q + l has an entry for pair p; base is the rank of the first such entry
+//    (entries ordered by row quarter, then pair, then row);
+//  - an entry is two 32-bit words: the fp16 high parts of the pair's two values
+//    (column 2p in bits 0-15, 2p + 1 in bits 16-31), then their fp16 low parts, where a
+//    value's parts are hi = fp16(x) and lo = fp16(x - hi) of x = value * 2^scale (about
+//    22 bits of x); a column without a value holds hi = 0x8000 (fp16 -0, which adds
+//    nothing to a product) and lo = 0, so that a stored zero (hi = +0) stays a value;
+//  - the whole block is a multiple of 16 bytes (one bulk copy).
+// A warp of the product reads one (mask, base) word per pair and, in its lanes that hold
+// an entry, consecutive 8-byte entries: two words of the tensor-core operand per pair
+// with no unpacking. At the benchmark's 33% density a block is 512 + 8 x ~1,130 bytes.
 struct Blocked {
   uint64_t rows = 0, K = 0;
   uint32_t n_tiles = 0, n_chunks = 0;
@@ -27,7 +32,7 @@ struct Blocked {
   int scale = 0;            // values stored times 2^scale (largest |x| in [2^14, 2^15))
   double max_abs = 0.0;     // the largest |value| and the smallest nonzero one
   double min_abs = 0.0;
-  double max_row_norm = 0.0;  // the largest row's Euclidean norm (rows of the matrix)
+  double max_row_norm = 0.0;  // the largest row's Euclidean norm (rows of the CSR)
   DeviceBuffer<uint64_t> off;  // n_tiles * n_chunks + 1 offsets, 16-byte units
   DeviceBuffer<uint8_t> data;
 };
@@ -37,9 +42,11 @@ struct Blocked {
 void build_blocked(const uint64_t* ptr, const uint32_t* col, const float* val, uint64_t n_rows,
                    uint64_t n_cols, uint64_t nnz, Blocked& out, cudaStream_t s);
 
-// The blocked layout of X^T from X's (bit-transposed masks, values moved by rank; the
-// same scale).
-void transpose_blocked(const Blocked& x, Blocked& out, cudaStream_t s);
+// The blocked layout of the same CSR's transpose (n_cols x n_rows), with x's scale and
+// value range (x = build_blocked of that CSR).
+void transpose_blocked(const uint64_t* ptr, const uint32_t* col, const float* val,
+                       uint64_t n_rows, uint64_t n_cols, uint64_t nnz, const Blocked& x,
+                       Blocked& out, cudaStream_t s);
 
 // The dense operand D (K x 64) as the products read it: D^T, 64 rows of fp16 parts of
 // each value times 2^scale, interleaved by chunk: for chunk c, row j holds the 32 high
