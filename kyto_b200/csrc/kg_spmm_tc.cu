@@ -66,8 +66,10 @@ constexpr uint32_t kBBytes = kN * 128;  // 8 KB: 64 rows x (32 hi + 32 lo) fp16
 constexpr uint32_t kHeaderBytes = 64 * 8;  // (mask, base) per row quarter and column pair
 constexpr uint32_t kBlockMaxBytes = kHeaderBytes + kRows * (kChunk / 2) * 8;
 constexpr uint32_t kAbsentHi = 0x8000u;  // fp16 -0: the high part of a column without a value
-constexpr int kExpandWarps = 4;
-constexpr int kDrainWarps = 4;
+// Two expand warps per sub-partition (rows 32 q.. of a block, half of its column pairs
+// each) and two drain warps (rows 32 q.., half of the 64 output columns each).
+constexpr int kExpandWarps = 8;
+constexpr int kDrainWarps = 8;
 constexpr int kSpThreads = (kExpandWarps + kDrainWarps + 2) * 32;
 constexpr int kABufs = 4;
 // TMEM columns: two 64-column f32 accumulators (0..127), then kABufs A buffers of 32
@@ -87,7 +89,7 @@ static_assert(sizeof(LoadStage) % 1024 == 0, "load stage size");
 
 struct SpSmem {
   LoadStage st[kLoadStages];
-  double colsum[2][kDrainWarps][kN];
+  double colsum[2][4][kN];  // per item parity, per 32-row quarter of the tile
   uint64_t ld_full[kLoadStages], ld_empty[kLoadStages];
   uint64_t a_full[kABufs], a_empty[kABufs];
   uint64_t cs_ready;
@@ -174,9 +176,9 @@ __device__ __forceinline__ uint2 map_entry(uint2 e, const ValueMap& vm, float me
   return make_uint2(hx, lx);
 }
 
-// One CTA per SM. The register file is split over the SM's four sub-partitions, so ten
-// warps fit only at 168 registers a thread (three warps on two of them); the drain warps'
-// 64 f64 sums spill a little in the once-per-item epilogue.
+// One CTA per SM, 18 warps: the register file is split over the SM's four sub-partitions
+// (five warps on two of them), so 96 registers a thread; each drain warp keeps 32 f64
+// sums, and two expand warps per sub-partition hide each other's latency.
 __global__ void __launch_bounds__(kSpThreads, 1)
 spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __restrict__ off,
                const uint8_t* __restrict__ data, uint64_t rows, Geometry geo, ValueMap vmap,
@@ -217,7 +219,8 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
 
   if (warp < kExpandWarps) {
     // ----------------------------------------------------------- expand -------------
-    const uint32_t q = (uint32_t)warp;        // rows 32 q .. 32 q + 31 of each block
+    const uint32_t q = (uint32_t)warp & 3u;   // rows 32 q .. 32 q + 31 of each block
+    const int hh = warp >> 2;                 // column pairs 8 hh .. 8 hh + 7
     const uint32_t lt = (1u << lane) - 1u;    // the lanes (rows) before this one
     const uint32_t lb = 1u << lane;
     uint64_t it = 0;
@@ -248,8 +251,7 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
         // Row (32 q + lane) of the A tiles: pair p's high-part word to column p, its
         // low-part word to column 16 + p (a row without an entry for the pair: zeros).
         const uint32_t arow = tmem + ((q * 32u) << 16) + kABase + ab * kACols;
-#pragma unroll
-        for (int hh = 0; hh < 2; ++hh) {
+        {
           uint32_t hw[8], lw[8];
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
@@ -283,7 +285,9 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
     }
   } else if (warp < kExpandWarps + kDrainWarps) {
     // ----------------------------------------------------------- drain TMEM ---------
-    const uint32_t quad = (uint32_t)warp & 3u;  // warps 4..7 -> TMEM lanes 32*quad..
+    const uint32_t quad = (uint32_t)warp & 3u;  // TMEM lanes 32 quad .. (rows of the tile)
+    const uint32_t half = (uint32_t)(warp - kExpandWarps) >> 2;  // columns 32 half ..
+    constexpr int kH = kN / 2;
     const uint32_t i = quad * 32u + lane;
     uint64_t fg = 0, item_no = 0;
     bool ok = true;
@@ -291,9 +295,9 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
       uint32_t tile, seg;
       geo.item(w, tile, seg);
       const uint64_t row = (uint64_t)tile * kRows + i;
-      double acc[kN];
+      double acc[kH];
 #pragma unroll
-      for (int j = 0; j < kN; ++j) acc[j] = 0.0;
+      for (int j = 0; j < kH; ++j) acc[j] = 0.0;
       const uint32_t nc = geo.chunks(seg);
       const uint32_t groups = (nc + kFlushChunks - 1) / kFlushChunks;
       for (uint32_t gr = 0; gr < groups; ++gr, ++fg) {
@@ -304,11 +308,10 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
         }
         tc_fence_after();
         __syncwarp();
-        // 16 columns at a time (few live registers beside the 64 f64 sums).
 #pragma unroll
-        for (int hf = 0; hf < 4; ++hf) {
+        for (int hf = 0; hf < 2; ++hf) {
           uint32_t rr[16];
-          tmem_ld_16(tmem + ((quad * 32u) << 16) + b * kAccCols + hf * 16u, rr);
+          tmem_ld_16(tmem + ((quad * 32u) << 16) + b * kAccCols + half * kH + hf * 16u, rr);
           tmem_wait_ld();
 #pragma unroll
           for (int j = 0; j < 16; ++j) acc[hf * 16 + j] += (double)__uint_as_float(rr[j]);
@@ -320,14 +323,15 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
       if (!ok) break;
       if (out.mode == kOutRows) {
         // C = S D - offsets: the next product's D^T (fp16 parts), the f32 rows, and this
-        // tile's column sums (fixed tree: warp shuffles, then the 4 warps in order).
+        // tile's column sums (fixed tree: warp shuffles, then the 4 quarters in order).
         const bool live = row < rows;
         const double t_mul = ldexp(1.0, out.t_scale), t_inv = ldexp(1.0, -out.t_scale);
         uint16_t* t_row = out.t ? out.t + (row / 32) * 64 + (row % 32) : nullptr;
 #pragma unroll
-        for (int j = 0; j < kN; ++j) {
+        for (int jj = 0; jj < kH; ++jj) {
+          const int j = (int)half * kH + jj;
           const double cval =
-              live && j < (int)out.width ? acc[j] * out_scale - out.offsets[j] : 0.0;
+              live && j < (int)out.width ? acc[jj] * out_scale - out.offsets[j] : 0.0;
           double seen = cval;
           if (out.t) {
             const double y = cval * t_mul;
@@ -348,23 +352,22 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
           }
         }
         if (out.colsum_partial) {
-          // The four warps' sums in a fixed order (double-buffered by item, so a warp
-          // running one item ahead cannot overwrite what warp 4 still reads).
+          // The four quarters' sums in a fixed order (double-buffered by item, so a warp
+          // running one item ahead cannot overwrite what the quarter-0 warps still read).
           __syncwarp();
           if (lane == 0) mbar_arrive(&sm.cs_ready);
           if (!mbar_wait(&sm.cs_ready, (uint32_t)(item_no & 1), abort)) break;
           if (quad == 0) {
             const double(*cs)[kN] = sm.colsum[item_no & 1];
-            for (int j = lane; j < kN; j += 32) {
-              double tsum = ((cs[0][j] + cs[1][j]) + cs[2][j]) + cs[3][j];
-              out.colsum_partial[(uint64_t)tile * kN + j] = tsum;
-            }
+            const int j = (int)half * kH + lane;
+            const double tsum = ((cs[0][j] + cs[1][j]) + cs[2][j]) + cs[3][j];
+            out.colsum_partial[(uint64_t)tile * kN + j] = tsum;
           }
         }
       } else if (row < rows) {
-        double* dst = out.partial + ((uint64_t)seg * rows + row) * kN;
+        double* dst = out.partial + ((uint64_t)seg * rows + row) * kN + half * kH;
 #pragma unroll
-        for (int j = 0; j < kN; ++j) dst[j] = acc[j] * out_scale;
+        for (int j = 0; j < kH; ++j) dst[j] = acc[j] * out_scale;
       }
     }
   } else if (warp == kExpandWarps + kDrainWarps) {
