@@ -18,7 +18,9 @@ On one GPU the line also carries the metric's second half and the batching form:
 - ``learned_vs_exact``: the learned-partition kNN against the exact search on 4M x 50
   Gaussian-mixture points (speed-up and recall@15 judged by the exact graph);
 - ``batching``: 64 samples of uneven sizes (PCA 30 + kNN 15 each) through the batching
-  form against one sample at a time.
+  form against one sample at a time;
+- ``connectivities`` (the timed step's graph) and ``hvg_moments`` (the seurat moments
+  pass over the benchmark's raw counts): the path's neighbouring rows, timed alone.
 
 ``--impl reference``: kyto's CPU algorithms (the C++ restatement in oracle/, all host
 threads) timed on a bounded sample of the same workload: the PCA over a subset of the
@@ -69,6 +71,8 @@ def parse() -> argparse.Namespace:
                     help="C5 learned-vs-exact comparison rows (0: skip)")
     ap.add_argument("--batch-samples", type=int, default=64,
                     help="C4 batching-form samples (0: skip)")
+    ap.add_argument("--hvg", type=int, default=1,
+                    help="time the HVG moments pass over the benchmark's counts (0: skip)")
     ap.add_argument("--reserve-gb", type=int, default=40,
                     help="device memory reserved for the library's pool at open (kg_reserve)")
     return ap.parse_args()
@@ -232,6 +236,36 @@ def e2e_steps(args, ctx, indptr, idx, vals, out, steps: int) -> None:
                                 args.components, 0, args.neighbors, K._ptr(out[0]),
                                 K._ptr(out[1]), K._ptr(out[2]), None))
         sess.close()
+
+
+def hvg_timing(args, ctx, x, d_indptr, d_idx) -> dict:
+    """The seurat HVG moments pass over the benchmark's raw counts (kg_hvg_moments:
+    normalize + log1p, expm1, a stable sort by gene, kyto's per-gene f64 folds), device
+    arrays in and out, CUDA-event timed (median of 3 after one warm-up)."""
+    import torch
+
+    import kyto_b200 as K
+
+    counts = torch.from_numpy(x.values.view(np.int32)).cuda()
+    g = args.genes
+    sums = torch.empty(g, dtype=torch.float64, device="cuda")
+    sq = torch.empty(g, dtype=torch.float64, device="cuda")
+    pos = torch.empty(g, dtype=torch.int64, device="cuda")
+    times = []
+    for i in range(4):
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        K._check(K.library().kg_hvg_moments(ctx.handle, K._ptr(d_indptr), K._ptr(d_idx),
+                                            K._ptr(counts), K.KG_U32, args.cells, g, 1e4, 1,
+                                            K._ptr(sums), K._ptr(sq), K._ptr(pos)))
+        b.record()
+        torch.cuda.synchronize()
+        if i:
+            times.append(a.elapsed_time(b))
+    del counts
+    return {"workload": f"{args.cells:,} cells x {g:,} genes raw counts ({x.nnz:,} stored)",
+            "ms": float(np.median(times))}
 
 
 def connectivities_timing(args, ctx, graph) -> dict:
@@ -591,6 +625,11 @@ def main() -> int:
             extra["connectivities"] = connectivities_timing(args, ctx, out_dev)
         except Exception as e:  # a side measurement never costs the main line
             extra["connectivities"] = {"error": f"{type(e).__name__}: {e}"}
+        if args.hvg:
+            try:
+                extra["hvg_moments"] = hvg_timing(args, ctx, x, d_indptr, d_idx)
+            except Exception as e:  # a side measurement never costs the main line
+                extra["hvg_moments"] = {"error": f"{type(e).__name__}: {e}"}
         for name, fn, on in (("learned_vs_exact", learned_vs_exact, args.learned_cells),
                              ("batching", batching, args.batch_samples)):
             if not on:

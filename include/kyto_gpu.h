@@ -427,6 +427,29 @@ KG_API kg_status kg_diag_spmm(kg_ctx* ctx, const uint64_t* indptr, const uint32_
 KG_API kg_status kg_diag_omega(kg_ctx* ctx, uint64_t seed, const uint64_t* cells, uint64_t n,
                                uint32_t width, double* out);
 
+/* The tuner's cache (no kyto counterpart; kyto's Config/flags layer chooses execution
+ * knobs, this caches the device choices that cannot change a result). The library tunes
+ * the kNN filter's operand kind and query-operand mode once per (GPU, shape class) and
+ * keeps the choice in a versioned JSON file: KYTO_GPU_TUNE_CACHE (a path, or "off"),
+ * else $XDG_CACHE_HOME/kyto_b200/tune.json, else $HOME/.cache/kyto_b200/tune.json;
+ * KYTO_GPU_TUNE=retune tunes again and replaces the entry. These two entry points read
+ * and write such a file directly (no GPU needed).
+ *
+ * kg_tune_lookup: the value of `field` in the choice stored for (gpu, cls) in the file
+ * at `path`, NUL-terminated into out (out_len bytes). Returns 1 when found, 0 when
+ * there is no such entry (or the file is missing, unreadable, malformed or of another
+ * version), -1 for a NULL argument or a value longer than out_len - 1. */
+KG_API int kg_tune_lookup(const char* path, const char* gpu, const char* cls,
+                          const char* field, char* out, size_t out_len);
+
+/* kg_tune_store: records the choice (keys and values: ';'-separated lists of the same
+ * length) and its measured cost (ms) for (gpu, cls) in the file at `path`, replacing an
+ * earlier entry for the same key and dropping entries of another version; the file is
+ * written to a temporary and renamed over. Returns 1 on success, 0 if the file could not
+ * be written, -1 for a NULL argument or lists of different lengths. */
+KG_API int kg_tune_store(const char* path, const char* gpu, const char* cls, const char* keys,
+                         const char* values, double ms);
+
 #ifdef __cplusplus
 }
 #endif

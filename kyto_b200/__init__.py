@@ -44,6 +44,7 @@ EXPORTS = (
     "kg_knn_batch", "kg_knn_learned",
     "kg_learned_layout", "kg_learned_gradients", "kg_diag_kernel_launches", "kg_connectivities",
     "kg_pca_run_stats", "kg_diag_omega", "kg_diag_pool_usage", "kg_diag_fail_allocations",
+    "kg_tune_lookup", "kg_tune_store",
     "kg_set_wait_limit", "kg_diag_spmm", "kg_pca_push_block_async",
 )
 
@@ -198,6 +199,10 @@ def library() -> ctypes.CDLL:
             "kg_diag_omega": [P, U64, P, U64, U32, P],
             "kg_diag_pool_usage": [ctypes.c_int, P, P, P, I32],
             "kg_diag_fail_allocations": [U64],
+            "kg_tune_lookup": [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                               ctypes.c_char_p, ctypes.c_char_p, ctypes.c_size_t],
+            "kg_tune_store": [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p,
+                              ctypes.c_char_p, ctypes.c_char_p, ctypes.c_double],
             "kg_diag_spmm": [P, P, P, P, U64, U32, I32, I32, P, P, U32, P],
         }
         for name, args in sig.items():
@@ -345,6 +350,29 @@ def pool_usage(device: int = 0, reset_high: bool = False) -> dict:
 def fail_allocations(after: int | None) -> None:
     """Test hook: fail every allocation after ``after`` more (None: stop failing)."""
     _check(library().kg_diag_fail_allocations(0xFFFFFFFFFFFFFFFF if after is None else int(after)))
+
+
+def tune_lookup(path, gpu: str, cls: str, field: str) -> str | None:
+    """The value of ``field`` in the tuner cache entry for (gpu, cls) in the file at
+    ``path`` (kg_tune_lookup), or None."""
+    buf = ctypes.create_string_buffer(256)
+    r = library().kg_tune_lookup(str(path).encode(), gpu.encode(), cls.encode(), field.encode(),
+                                 buf, len(buf))
+    if r < 0:
+        raise KytoError(KG_ERR_INVALID, "kg_tune_lookup: bad argument")
+    return buf.value.decode() if r == 1 else None
+
+
+def tune_store(path, gpu: str, cls: str, choice: dict, ms: float) -> bool:
+    """Record ``choice`` (str -> str) for (gpu, cls) in the tuner cache file at ``path``
+    (kg_tune_store); False if the file could not be written."""
+    keys = ";".join(choice)
+    values = ";".join(str(choice[k]) for k in choice)
+    r = library().kg_tune_store(str(path).encode(), gpu.encode(), cls.encode(), keys.encode(),
+                                values.encode(), float(ms))
+    if r < 0:
+        raise KytoError(KG_ERR_INVALID, "kg_tune_store: bad argument")
+    return r == 1
 
 
 def kernel_launches() -> int:

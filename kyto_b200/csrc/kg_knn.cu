@@ -33,6 +33,7 @@
 #include "kg_internal.cuh"
 #include "kg_knn.cuh"
 #include "kg_knn_tc.cuh"
+#include "kg_tune.cuh"
 
 namespace kg {
 
@@ -1032,19 +1033,47 @@ __global__ void pilot_plan_kernel(const uint64_t* blocks, uint64_t n_pilot, uint
 // overflowed queries' full-row searches (1.65e-10 s per point and 50 components, as
 // measured on B200). The kinds return the same graph, so the choice only moves time;
 // it is kept per (rows, components, k) class for later calls in the process.
-FilterKind tune_filter_kind(kg_ctx* ctx, cudaStream_t s, const float* x, uint64_t n,
-                            uint32_t width, uint32_t d, uint32_t k, const ScanPlan& sp,
-                            const FilterScan& scan, const uint32_t* prows, const double* mean,
-                            double scale, const double* max_sq) {
+// The filter's tuned operand kind and query-operand mode (neither changes a result).
+struct FilterChoice {
+  FilterKind kind = FilterKind::Fp16;
+  int a_mode = kTcAmSmem;
+};
+
+FilterChoice tune_filter_kind(kg_ctx* ctx, cudaStream_t s, const float* x, uint64_t n,
+                              uint32_t width, uint32_t d, uint32_t k, const ScanPlan& sp,
+                              const FilterScan& scan, const uint32_t* prows, const double* mean,
+                              double scale, const double* max_sq) {
+  // Two levels: this process's choices, then the cache file (kg_tune.cuh), keyed by the
+  // GPU and the shape class (rows to the next power of two, components, k, and whether
+  // the scan is a batch of samples).
   static std::mutex mu;
-  static std::map<std::tuple<int, uint32_t, uint32_t>, FilterKind> cache;
+  static std::map<std::string, FilterChoice> cache;
   int n_bits = 0;
   while (n_bits < 63 && (1ull << n_bits) < n) ++n_bits;
-  const auto key = std::make_tuple(n_bits, d, k);
+  const std::string gpu = tune_gpu_name();
+  const std::string cls = "knn_filter/n2^" + std::to_string(n_bits) + "/d" + std::to_string(d) +
+                          "/k" + std::to_string(k) + (scan.slot_sample ? "/batch" : "");
+  const std::string key = gpu + "|" + cls;
   {
     std::lock_guard<std::mutex> lock(mu);
     auto it = cache.find(key);
     if (it != cache.end()) return it->second;
+  }
+  const std::string path = tune_cache_path();
+  const char* retune = std::getenv("KYTO_GPU_TUNE");
+  TuneChoice tc;
+  if (!(retune && std::string(retune) == "retune") && tune_lookup(path, gpu, cls, tc)) {
+    FilterChoice c;
+    c.kind = tc["kind"] == "split" ? FilterKind::Split
+             : tc["kind"] == "bf16" ? FilterKind::Bf16 : FilterKind::Fp16;
+    c.a_mode = tc["a_mode"] == "tmem" ? kTcAmTmem : tc["a_mode"] == "half" ? kTcAmHalf
+                                                                           : kTcAmSmem;
+    if (trace_on())
+      std::fprintf(stderr, "[kyto_gpu trace] filter choice from %s: %s, %s\n", path.c_str(),
+                   tc["kind"].c_str(), tc["a_mode"].c_str());
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = c;
+    return c;
   }
   const uint32_t block = kTcQueryBlock;
   const uint64_t n_blocks = (n + block - 1) / block;
@@ -1090,9 +1119,14 @@ FilterKind tune_filter_kind(kg_ctx* ctx, cudaStream_t s, const float* x, uint64_
   DeviceBuffer<uint32_t> cr(n_q * cap, s), cc(n_q, s);
   DeviceBuffer<double> qn2(n_q, s), sl(n_q, s);
   const double per_point = 1.65e-10 * std::max<double>(d, 1) / 50.0;
-  FilterKind best = FilterKind::Fp16;
+  FilterChoice best;
   double best_cost = INFINITY;
-  for (FilterKind kind : {FilterKind::Fp16, FilterKind::Split}) {
+  const std::pair<FilterKind, int> tries[] = {
+      {FilterKind::Fp16, kTcAmSmem}, {FilterKind::Fp16, kTcAmHalf}, {FilterKind::Fp16, kTcAmTmem},
+      {FilterKind::Split, kTcAmSmem}, {FilterKind::Split, kTcAmHalf}, {FilterKind::Split, kTcAmTmem}};
+  for (const auto& tr : tries) {
+    const FilterKind kind = tr.first;
+    ps.a_mode = tr.second;
     cudaEvent_t a, b;
     KG_CUDA(cudaEventCreate(&a));
     KG_CUDA(cudaEventCreate(&b));
@@ -1114,16 +1148,23 @@ FilterKind tune_filter_kind(kg_ctx* ctx, cudaStream_t s, const float* x, uint64_
                         (double)over / (double)n_q * (double)n * (double)n * per_point;
     if (trace_on())
       std::fprintf(stderr,
-                   "[kyto_gpu trace] filter pilot %s: %.3f ms for %llu blocks, %llu of %llu "
+                   "[kyto_gpu trace] filter pilot %s/%s: %.3f ms for %llu blocks, %llu of %llu "
                    "queries overflowed, estimate %.1f ms\n",
-                   kind == FilterKind::Split ? "split" : "fp16", ms,
+                   kind == FilterKind::Split ? "split" : "fp16",
+                   tr.second == kTcAmTmem ? "tmem" : tr.second == kTcAmHalf ? "half" : "smem", ms,
                    (unsigned long long)n_pilot, (unsigned long long)over,
                    (unsigned long long)n_q, cost * 1e3);
     if (cost < best_cost) {
       best_cost = cost;
-      best = kind;
+      best.kind = kind;
+      best.a_mode = tr.second;
     }
   }
+  tune_store(path, gpu, cls,
+             TuneChoice{{"kind", best.kind == FilterKind::Split ? "split" : "fp16"},
+                        {"a_mode", best.a_mode == kTcAmTmem ? "tmem"
+                                   : best.a_mode == kTcAmHalf ? "half" : "smem"}},
+             best_cost * 1e3);
   std::lock_guard<std::mutex> lock(mu);
   cache[key] = best;
   return best;
@@ -1264,8 +1305,10 @@ void knn_core(kg_ctx* ctx, const float* x, uint64_t n, uint32_t width, uint32_t 
     }
     const uint32_t* prows = sp.prows.ptr ? sp.prows.ptr : sp.qrows.ptr;
     if (filter == "auto") {
-      kind = tune_filter_kind(ctx, s, x, n, width, d, k, sp, scan, prows, mean.ptr, scale,
-                              max_sq.ptr);
+      const FilterChoice fc = tune_filter_kind(ctx, s, x, n, width, d, k, sp, scan, prows,
+                                               mean.ptr, scale, max_sq.ptr);
+      kind = fc.kind;
+      scan.a_mode = fc.a_mode;
       trace.mark("filter tuning");
     }
     DeviceBuffer<uint16_t> point_ops;  // kept for the overflow retry

@@ -55,7 +55,7 @@ constexpr int kTcThreads = (kEpiWarps + 2) * 32;
 constexpr uint32_t kTmemCols = 512;
 constexpr uint32_t kEndOfBlock = 0xFFFFFFFFu;
 constexpr uint32_t kNoBlock = 0xFFFFFFFFu;  // no query block left: the CTA's roles stop
-enum : int { kAmSmem = 0, kAmTmem = 1, kAmHalf = 2 };  // the filter's A operand modes
+enum : int { kAmSmem = kTcAmSmem, kAmTmem = kTcAmTmem, kAmHalf = kTcAmHalf };
 
 // SUBS: 64-wide sub-tiles per operand row (1: fp16 or bf16; 2: split hi and lo). KR: the
 // register top-k width (16, 32) or 0 (the k smallest in local memory, any k).
@@ -996,14 +996,16 @@ void launch_filter(unsigned grid, cudaStream_t s, const CUtensorMap& mq, const C
       mq, mp, scan, k, slack2, idesc, cap, cand_key, cand_row, cand_count, threshold, err);
 }
 
-// The filter's query operand and accumulator slots (KYTO_GPU_FILTER_A): "smem" (the
-// default: 194 ms against 238 ms for "tmem" on the 1M benchmark search on a B200),
-// "tmem", or "half" (shared memory, four half slots); all give the same keys.
-int filter_a_mode() {
+// The filter's query operand and accumulator slots: KYTO_GPU_FILTER_A ("smem", "tmem"
+// or "half") when set, else the scan's tuned mode, else shared memory (194 ms against
+// 238 ms for "tmem" and 222 ms for "half" on the 1M benchmark search on a B200); all give
+// the same keys.
+int filter_a_mode(int tuned) {
   const char* v = std::getenv("KYTO_GPU_FILTER_A");
   if (v && std::string(v) == "tmem") return kAmTmem;
   if (v && std::string(v) == "half") return kAmHalf;
-  return kAmSmem;
+  if (v && std::string(v) == "smem") return kAmSmem;
+  return tuned == kAmTmem || tuned == kAmHalf ? tuned : kAmSmem;
 }
 
 }  // namespace
@@ -1078,7 +1080,7 @@ void tc_filter(kg_ctx* ctx, cudaStream_t s, const float* x, uint32_t width, uint
            : kr == 32 ? (split ? launch_filter<32, 2, AM> : launch_filter<32, 1, AM>)
                       : (split ? launch_filter<0, 2, AM> : launch_filter<0, 1, AM>);
   };
-  const int am = filter_a_mode();
+  const int am = filter_a_mode(scan.a_mode);
   auto launch = am == kAmTmem   ? pick(std::integral_constant<int, kAmTmem>{})
                 : am == kAmHalf ? pick(std::integral_constant<int, kAmHalf>{})
                                 : pick(std::integral_constant<int, kAmSmem>{});

@@ -21,6 +21,11 @@ constexpr uint32_t kTcQueryBlock = 256;      // query slots per block of the fp1
 // split (fp16 hi and lo parts, three products; a slack 2^5 times smaller than fp16's).
 enum class FilterKind { Fp16, Bf16, Split };
 
+// Where the filter's MMAs read the query operand and how its accumulators are cut (the
+// same keys every way): shared memory, two slots of both query halves; tensor memory,
+// three half slots; shared memory, four half slots.
+enum : int { kTcAmSmem = 0, kTcAmTmem = 1, kTcAmHalf = 2 };
+
 // Query slots per block of the filter of this kind (the blocks tile lists are built for).
 uint32_t filter_query_block(FilterKind kind);
 
@@ -48,6 +53,9 @@ struct FilterScan {
   unsigned long long* tiles_scanned = nullptr;  // when set: += tiles the launch multiplied
   unsigned int* block_counter = nullptr;  // query blocks handed out past the first wave
                                           // (zero before the launch; set by tc_filter)
+  int a_mode = -1;                       // the query operand's mode (kTcAmSmem, kTcAmTmem,
+                                         // kTcAmHalf), or -1: shared memory;
+                                         // KYTO_GPU_FILTER_A overrides either
   const double* qn2 = nullptr;           // per query slot |q - mean|^2 (set by tc_filter)
   double s2 = 1.0;                       // scale^2 (set by tc_filter)
 };

@@ -6,6 +6,8 @@ singular values (variances) 1e-6 relative to the FP64 oracle (the product path
 accumulates in f64), loadings/embedding columns 1e-5 of their largest value.
 """
 
+import json
+
 import numpy as np
 import pytest
 
@@ -471,3 +473,21 @@ def test_filter_query_operand_in_tmem_or_smem_gives_the_same_keys(ctx, monkeypat
     c = K.neighbors(x[:5000], 15, ctx=ctx)
     assert np.array_equal(c.indices, o.indices)
     assert np.array_equal(c.distances.view(np.uint32), o.distances.view(np.uint32))
+
+
+def test_filter_choice_is_tuned_once_and_kept_in_the_cache_file(ctx, monkeypatch, tmp_path):
+    # An unusual shape class (no earlier test tuned it in this process): the first search
+    # pilots both operand kinds in every query-operand mode, keeps the cheapest in the
+    # cache file under (GPU, class), and the graph is the oracle's whichever it picked.
+    path = tmp_path / "tune.json"
+    monkeypatch.setenv("KYTO_GPU_TUNE_CACHE", str(path))
+    monkeypatch.delenv("KYTO_GPU_KNN_FILTER", raising=False)
+    monkeypatch.delenv("KYTO_GPU_FILTER_A", raising=False)
+    pts, _ = synthetic.gaussian_mixture(3000, 7, 12, seed=31, device="cpu")
+    g = K.neighbors(pts, 9, ctx=ctx)
+    _graph_equal(g, O.neighbors(pts, 9))
+    doc = json.loads(path.read_text())
+    (entry,) = [e for e in doc["entries"] if e["class"] == "knn_filter/n2^12/d7/k8"]
+    assert entry["choice"]["kind"] in ("fp16", "split")
+    assert entry["choice"]["a_mode"] in ("smem", "tmem", "half")
+    assert "SMs" in entry["gpu"] and entry["ms"] > 0
