@@ -25,6 +25,74 @@ cudaMemPool_t device_pool(int device) {
   return pools[device];
 }
 
+thread_local bool g_stage_pageable = false;
+
+namespace {
+
+// Page-locked staging for pageable host sources: two 16 MB halves and an event each, per
+// device (events belong to a device), kept on a free list for the process's lifetime.
+constexpr size_t kStageBytes = 16u << 20;
+struct Staging {
+  void* half[2] = {nullptr, nullptr};
+  cudaEvent_t done[2] = {nullptr, nullptr};
+};
+std::mutex g_stage_mu;
+std::vector<std::vector<Staging*>> g_stage_free;
+
+Staging* take_staging(int device) {
+  {
+    std::lock_guard<std::mutex> lock(g_stage_mu);
+    if ((size_t)device < g_stage_free.size() && !g_stage_free[device].empty()) {
+      Staging* st = g_stage_free[device].back();
+      g_stage_free[device].pop_back();
+      return st;
+    }
+  }
+  auto st = std::make_unique<Staging>();
+  for (int b = 0; b < 2; ++b) {
+    KG_CUDA(cudaHostAlloc(&st->half[b], kStageBytes, cudaHostAllocPortable));
+    KG_CUDA(cudaEventCreateWithFlags(&st->done[b], cudaEventDisableTiming));
+  }
+  return st.release();
+}
+
+void give_staging(int device, Staging* st) {
+  std::lock_guard<std::mutex> lock(g_stage_mu);
+  if ((size_t)device >= g_stage_free.size()) g_stage_free.resize((size_t)device + 1);
+  g_stage_free[device].push_back(st);
+}
+
+}  // namespace
+
+void staged_copy_to_device(void* dst, const void* src, size_t bytes, cudaStream_t stream) {
+  int device = 0;
+  KG_CUDA(cudaGetDevice(&device));
+  Staging* st = take_staging(device);
+  bool used[2] = {false, false};
+  try {
+    size_t i = 0;
+    for (size_t off = 0; off < bytes; off += kStageBytes, ++i) {
+      const int b = (int)(i & 1);
+      const size_t n = std::min(kStageBytes, bytes - off);
+      // The half's previous copy has read it before the host overwrites it.
+      if (used[b]) KG_CUDA(cudaEventSynchronize(st->done[b]));
+      std::memcpy(st->half[b], (const char*)src + off, n);
+      KG_CUDA(cudaMemcpyAsync((char*)dst + off, st->half[b], n, cudaMemcpyHostToDevice, stream));
+      KG_CUDA(cudaEventRecord(st->done[b], stream));
+      used[b] = true;
+    }
+    for (int b = 0; b < 2; ++b)
+      if (used[b]) KG_CUDA(cudaEventSynchronize(st->done[b]));
+  } catch (...) {
+    // Wait (unchecked) for copies already queued before the halves go back.
+    for (int b = 0; b < 2; ++b)
+      if (used[b]) cudaEventSynchronize(st->done[b]);
+    give_staging(device, st);
+    throw;
+  }
+  give_staging(device, st);
+}
+
 std::string& last_error() {
   thread_local std::string message;
   return message;

@@ -174,16 +174,44 @@ inline bool is_device_pointer(const void* p) {
   return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// Whether p is ordinary (pageable) host memory: neither the device's nor page-locked.
+inline bool is_pageable_host(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes a{};
+  cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return true;
+  }
+  return a.type == cudaMemoryTypeUnregistered;
+}
+
+// Copies `bytes` of pageable host memory to the device through page-locked staging
+// buffers of this process (two 16 MB halves, filled by the host while the other half's
+// copy runs on `stream`), so that copies from several host threads run side by side at
+// the link's rate instead of through the driver's own staging. Returns once every byte
+// has been read from `src` and the staging buffers are free again (kg_context.cu).
+void staged_copy_to_device(void* dst, const void* src, size_t bytes, cudaStream_t stream);
+
+// Set in the batching form's worker threads: their pageable copies go through the
+// staging buffers. A single caller keeps the driver's own pageable copy, which is faster
+// than one host thread filling the staging buffers; several workers filling their own
+// staging buffers side by side are faster than the driver's copies, which serialize.
+extern thread_local bool g_stage_pageable;
+
 // `count` elements at `src` (host or device) as a device pointer: src itself when the
-// device can read it, else a copy in `holder`.
+// device can read it, else a copy in `holder` (in a batching worker, pageable sources of
+// 4 MB or more through the staging buffers).
 template <class T>
 const T* device_view(const T* src, size_t count, DeviceBuffer<T>& holder,
                      cudaStream_t stream) {
   if (is_device_pointer(src)) return src;
   holder.alloc(count, stream);
-  if (count)
-    KG_CUDA(cudaMemcpyAsync(holder.ptr, src, count * sizeof(T), cudaMemcpyHostToDevice,
-                            stream));
+  const size_t bytes = count * sizeof(T);
+  if (g_stage_pageable && bytes >= (4u << 20) && is_pageable_host(src))
+    staged_copy_to_device(holder.ptr, src, bytes, stream);
+  else if (count)
+    KG_CUDA(cudaMemcpyAsync(holder.ptr, src, bytes, cudaMemcpyHostToDevice, stream));
   return holder.ptr;
 }
 

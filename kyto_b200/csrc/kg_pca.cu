@@ -1788,6 +1788,7 @@ kg_status kg_pca_knn_batch(kg_ctx* ctx, const kg_pca_params* params, uint32_t n_
       pool.emplace_back([&, w] {
         try {
           KG_CUDA(cudaSetDevice(ctx->device));
+          g_stage_pageable = true;
           for (;;) {
             const uint32_t at = next.fetch_add(1);
             if (at >= n_samples) break;

@@ -114,12 +114,6 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
       : "memory");
 }
 
-// Prefetch [src, src + bytes) into L2 (16-byte aligned, size a multiple of 16).
-__device__ __forceinline__ void bulk_prefetch_l2(const void* src, uint32_t bytes) {
-  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(reinterpret_cast<uint64_t>(src)),
-               "r"(bytes)
-               : "memory");
-}
 
 // The two fp16 parts of x (hi = fp16(x), lo = fp16(x - hi)) in one word, hi low.
 __device__ __forceinline__ uint32_t split_pair(float x) {
@@ -372,9 +366,9 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
     }
   } else if (warp == kExpandWarps + kDrainWarps) {
     // ----------------------------------------------------------- loads --------------
-    // Lane 0 issues; the warp reads the item's block offsets 32 at a time ahead of it,
-    // and each window's successor (or the next item's first window) is prefetched into
-    // L2 while this one is copied.
+    // Lane 0 issues; the warp reads the item's block offsets 32 at a time ahead of it.
+    // (Prefetching the next 32 blocks into L2 ahead of their copies made the products 9%
+    // slower on the 1M benchmark: part of it was evicted before use and read twice.)
     if (lane == 0) prefetch_tmap(&tmap_dt);
     uint64_t it = 0;
     int issued_phase[kLoadStages];
@@ -393,23 +387,6 @@ spmm_tc_kernel(const __grid_constant__ CUtensorMap tmap_dt, const uint64_t* __re
           // offsets array holds one entry past every block).
           win = c + lane <= nc ? off[b0 + c + lane] : 0;
           win_end = lane == 0 && c + 32 <= nc ? off[b0 + c + 32] : 0;
-          if (lane == 0) {
-            uint64_t p0 = 0, p1 = 0;
-            if (c + 32 < nc) {
-              p0 = win_end;
-              p1 = off[b0 + min(c + 64, nc)];
-            } else if (w + gridDim.x < n_items) {
-              uint32_t t2, s2;
-              geo.item(w + gridDim.x, t2, s2);
-              const uint64_t nb0 = geo.first_block(t2, s2);
-              p0 = off[nb0];
-              p1 = off[nb0 + min(32u, geo.chunks(s2))];
-            }
-            for (uint64_t u = p0; u < p1; u += 4096) {  // 64 KB per prefetch
-              const uint64_t units = p1 - u < 4096 ? p1 - u : 4096;
-              bulk_prefetch_l2(data + u * 16, (uint32_t)(units * 16));
-            }
-          }
         }
         const uint64_t e0 = __shfl_sync(0xFFFFFFFFu, win, at);
         const uint64_t e1n = __shfl_sync(0xFFFFFFFFu, win, (at + 1) & 31u);
@@ -530,41 +507,163 @@ __global__ void csr_stats_kernel(const uint64_t* ptr, const float* val, uint64_t
   }
 }
 
-// Where a stored value of the CSR lands: its layout row and column (the CSR's row and
-// column, or swapped for the transpose), the block, the header word (row quarter, column
-// pair) and the row's bit in that word.
-struct Place {
-  uint64_t block;
-  uint32_t word, bit, half;
-};
-__device__ __forceinline__ Place place(uint64_t r, uint32_t c, bool transposed,
-                                       uint32_t n_chunks) {
-  const uint64_t lr = transposed ? c : r, lc = transposed ? r : c;
-  Place p;
-  p.block = (lr / kRows) * n_chunks + lc / kChunk;
-  p.word = (uint32_t)((lr % kRows) / 32) * 16 + (uint32_t)((lc % kChunk) / 2);
-  p.bit = (uint32_t)(lr % 32);
-  p.half = (uint32_t)(lc % 2);
-  return p;
+// A value's two fp16 parts (hi in bits 0-15, lo in 16-31) of x = v * 2^scale; a stored
+// -0 becomes +0 (-0 marks a column without a value).
+__device__ __forceinline__ uint32_t stored_parts(float v, int scale) {
+  const float x = ldexpf(v, scale);
+  return split_pair(x == 0.0f ? 0.0f : x);
 }
 
-// Header masks (n_blocks x 64 words, zeroed): warp per CSR row; lanes whose values share
-// a word OR their bits together and one of them writes.
-__global__ void pair_mask_kernel(const uint64_t* ptr, const uint32_t* col, uint64_t n_rows,
-                                 bool transposed, uint32_t n_chunks, uint32_t* masks) {
+// An entry from its two columns' parts words (kAbsentHi for a column without a value).
+__device__ __forceinline__ uint2 make_entry(uint32_t w0, uint32_t w1) {
+  return make_uint2((w0 & 0xFFFFu) | (w1 << 16), (w0 >> 16) | (w1 & 0xFFFF0000u));
+}
+
+__device__ __forceinline__ uint64_t lower_bound_u32(const uint32_t* a, uint64_t lo, uint64_t hi,
+                                                    uint32_t v) {
+  while (lo < hi) {
+    const uint64_t mid = (lo + hi) >> 1;
+    if (a[mid] < v) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// ----- X: layout rows = CSR rows.
+
+// Header masks: a warp per (tile, row quarter) walks its 32 rows one after another, the
+// lanes over each row's values (coalesced), setting the row's bit in the quarter's words
+// held in shared memory (a window of kMaskWindow chunks at a time); then the words go out
+// 16 per chunk. Within one row every write sets the same bit, so no atomics are needed.
+constexpr uint32_t kMaskWindow = 128;  // K-chunks a pass (8 KB of words a warp)
+constexpr int kMaskWarps = 4;
+
+__global__ void __launch_bounds__(kMaskWarps * 32)
+rows_mask_kernel(const uint64_t* ptr, const uint32_t* col, uint64_t n_rows, uint32_t n_tiles,
+                 uint32_t n_chunks, uint32_t* masks) {
+  __shared__ uint32_t words[kMaskWarps][kMaskWindow * 16];
+  const unsigned lane = threadIdx.x & 31u, wi = threadIdx.x >> 5;
+  const uint64_t wq = (uint64_t)blockIdx.x * kMaskWarps + wi;
+  if (wq >= (uint64_t)n_tiles * 4) return;
+  const uint64_t tile = wq / 4, q = wq % 4;
+  uint32_t* w = words[wi];
+  for (uint32_t c0 = 0; c0 < n_chunks; c0 += kMaskWindow) {
+    const uint32_t nch = min(kMaskWindow, n_chunks - c0);
+    for (uint32_t x = lane; x < nch * 16; x += 32) w[x] = 0;
+    __syncwarp();
+    const uint32_t g_lo = c0 * kChunk, g_hi = (c0 + nch) * kChunk;
+    for (uint32_t j = 0; j < 32; ++j) {
+      const uint64_t r = tile * kRows + q * 32 + j;
+      if (r >= n_rows) break;
+      uint64_t a = ptr[r], e = ptr[r + 1];
+      if (c0 > 0) a = lower_bound_u32(col, a, e, g_lo);
+      for (uint64_t i = a + lane; i < e; i += 32) {
+        const uint32_t c = col[i];
+        if (c >= g_hi) break;
+        const uint32_t x = (c / kChunk - c0) * 16 + (c % kChunk) / 2;
+        w[x] |= 1u << j;
+      }
+      __syncwarp();
+    }
+    for (uint32_t x = lane; x < nch * 16; x += 32)
+      masks[(tile * n_chunks + c0 + x / 16) * 64 + q * 16 + x % 16] = w[x];
+    __syncwarp();
+  }
+}
+
+// Entries: a warp per CSR row, the lanes over its values; the lane holding a pair's first
+// value writes the whole entry.
+__global__ void rows_values_kernel(const uint64_t* ptr, const uint32_t* col, const float* val,
+                                   uint64_t n_rows, uint32_t n_chunks, const uint32_t* masks,
+                                   const uint16_t* bases, const uint64_t* off, int scale,
+                                   uint8_t* data) {
   const uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const unsigned lane = threadIdx.x & 31u;
   if (r >= n_rows) return;
-  for (uint64_t i0 = ptr[r]; i0 < ptr[r + 1]; i0 += 32) {
-    const uint64_t i = i0 + lane;
-    const bool in = i < ptr[r + 1];
-    const unsigned active = __ballot_sync(0xFFFFFFFFu, in);
-    if (!in) continue;
-    const Place pl = place(r, col[i], transposed, n_chunks);
-    const uint64_t word = pl.block * 64 + pl.word;
-    const unsigned same = __match_any_sync(active, word);
-    const uint32_t bits = __reduce_or_sync(same, 1u << pl.bit);
-    if ((unsigned)__ffs(same) - 1 == lane) atomicOr(&masks[word], bits);
+  const uint64_t tile = r / kRows;
+  const uint32_t q = (uint32_t)((r % kRows) / 32), bit = (uint32_t)(r % 32);
+  const uint32_t below = (1u << bit) - 1u;
+  const uint64_t a = ptr[r], end = ptr[r + 1];
+  for (uint64_t i = a + lane; i < end; i += 32) {
+    const uint32_t c = col[i];
+    // The pair's odd column after its even one: written with it.
+    if (c % 2 == 1 && i > a && col[i - 1] == c - 1) continue;
+    uint32_t w0 = kAbsentHi, w1 = kAbsentHi;
+    if (c % 2 == 0) {
+      w0 = stored_parts(val[i], scale);
+      if (i + 1 < end && col[i + 1] == c + 1) w1 = stored_parts(val[i + 1], scale);
+    } else {
+      w1 = stored_parts(val[i], scale);
+    }
+    const uint64_t b = tile * n_chunks + c / kChunk;
+    const uint64_t h = b * 64 + q * 16 + (c % kChunk) / 2;
+    const uint32_t e = bases[h] + __popc(masks[h] & below);
+    reinterpret_cast<uint2*>(data + off[b] * 16 + kHeaderBytes)[e] = make_entry(w0, w1);
+  }
+}
+
+// ----- X^T: layout rows = CSR columns (genes), layout columns = CSR rows (cells). A warp
+// per pair of CSR rows (one column pair of the layout), lane = a group of 32 genes (one
+// header word of one block), found in each row by binary search.
+
+// Header masks: the word of (gene group, cell pair) = the genes of the group either cell
+// holds; each word written once, no atomics.
+__global__ void cols_mask_kernel(const uint64_t* ptr, const uint32_t* col, uint64_t n_rows,
+                                 uint32_t n_cols, uint32_t n_chunks, uint32_t* masks) {
+  const uint64_t pr = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  const uint64_t r0 = 2 * pr;
+  if (r0 >= n_rows) return;
+  const bool has1 = r0 + 1 < n_rows;
+  const uint64_t a0 = ptr[r0], e0 = ptr[r0 + 1];
+  const uint64_t a1 = has1 ? ptr[r0 + 1] : 0, e1 = has1 ? ptr[r0 + 2] : 0;
+  const uint32_t groups = (n_cols + 31) / 32;
+  const uint64_t kch = r0 / kChunk;
+  const uint32_t p = (uint32_t)((r0 % kChunk) / 2);
+  for (uint32_t gg = lane; gg < groups; gg += 32) {
+    const uint32_t g0 = gg * 32;
+    uint32_t bits = 0;
+    for (uint64_t i = lower_bound_u32(col, a0, e0, g0); i < e0 && col[i] < g0 + 32; ++i)
+      bits |= 1u << (col[i] - g0);
+    for (uint64_t i = lower_bound_u32(col, a1, e1, g0); i < e1 && col[i] < g0 + 32; ++i)
+      bits |= 1u << (col[i] - g0);
+    if (bits) masks[((uint64_t)(gg / 4) * n_chunks + kch) * 64 + (gg % 4) * 16 + p] = bits;
+  }
+}
+
+// Entries: per gene either cell holds, one whole entry (the two cells' parts), merged in
+// gene order.
+__global__ void cols_values_kernel(const uint64_t* ptr, const uint32_t* col, const float* val,
+                                   uint64_t n_rows, uint32_t n_cols, uint32_t n_chunks,
+                                   const uint32_t* masks, const uint16_t* bases,
+                                   const uint64_t* off, int scale, uint8_t* data) {
+  const uint64_t pr = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  const uint64_t r0 = 2 * pr;
+  if (r0 >= n_rows) return;
+  const bool has1 = r0 + 1 < n_rows;
+  const uint64_t a0 = ptr[r0], e0 = ptr[r0 + 1];
+  const uint64_t a1 = has1 ? ptr[r0 + 1] : 0, e1 = has1 ? ptr[r0 + 2] : 0;
+  const uint32_t groups = (n_cols + 31) / 32;
+  const uint64_t kch = r0 / kChunk;
+  const uint32_t p = (uint32_t)((r0 % kChunk) / 2);
+  for (uint32_t gg = lane; gg < groups; gg += 32) {
+    const uint32_t g0 = gg * 32;
+    uint64_t i = lower_bound_u32(col, a0, e0, g0), j = lower_bound_u32(col, a1, e1, g0);
+    const uint32_t gi = i < e0 ? col[i] : 0xFFFFFFFFu, gj = j < e1 ? col[j] : 0xFFFFFFFFu;
+    if (min(gi, gj) >= g0 + 32) continue;
+    const uint64_t b = (uint64_t)(gg / 4) * n_chunks + kch;
+    const uint64_t h = b * 64 + (gg % 4) * 16 + p;
+    const uint32_t m = masks[h], base = bases[h];
+    uint2* ent = reinterpret_cast<uint2*>(data + off[b] * 16 + kHeaderBytes);
+    for (;;) {
+      const uint32_t ci = i < e0 ? col[i] : 0xFFFFFFFFu, cj = j < e1 ? col[j] : 0xFFFFFFFFu;
+      const uint32_t g = min(ci, cj);
+      if (g >= g0 + 32) break;
+      uint32_t w0 = kAbsentHi, w1 = kAbsentHi;
+      if (ci == g) w0 = stored_parts(val[i++], scale);
+      if (cj == g) w1 = stored_parts(val[j++], scale);
+      ent[base + __popc(m & ((1u << (g - g0)) - 1u))] = make_entry(w0, w1);
+    }
   }
 }
 
@@ -592,8 +691,7 @@ __global__ void pair_base_kernel(const uint32_t* masks, uint64_t n_blocks, uint1
   if (lane == 0) units[b] = total ? (kHeaderBytes + 8ull * total + 15) / 16 : 0;
 }
 
-// Per block (warp): the header, and every entry set to "no value in either column"
-// (kAbsentHi high parts, zero low parts) before the values are placed.
+// Per block (warp): the header (every entry is then written whole by the values kernel).
 __global__ void pair_header_kernel(const uint32_t* masks, const uint16_t* bases,
                                    const uint64_t* off, uint64_t n_blocks, uint8_t* data) {
   const uint64_t b = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -601,30 +699,6 @@ __global__ void pair_header_kernel(const uint32_t* masks, const uint16_t* bases,
   if (b >= n_blocks || off[b + 1] == off[b]) return;
   uint2* blk = reinterpret_cast<uint2*>(data + off[b] * 16);
   for (uint32_t h = lane; h < 64; h += 32) blk[h] = make_uint2(masks[b * 64 + h], bases[b * 64 + h]);
-  const uint64_t words = (off[b + 1] - off[b]) * 2 - 64;  // entries and the padding
-  for (uint64_t e = lane; e < words; e += 32)
-    blk[64 + e] = make_uint2(kAbsentHi | (kAbsentHi << 16), 0u);
-}
-
-// Each value, scaled and split, into its half of its entry (warp per CSR row).
-__global__ void pair_values_kernel(const uint64_t* ptr, const uint32_t* col, const float* val,
-                                   uint64_t n_rows, bool transposed, uint32_t n_chunks,
-                                   const uint64_t* off, int scale, uint8_t* data) {
-  const uint64_t r = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const unsigned lane = threadIdx.x & 31u;
-  if (r >= n_rows) return;
-  for (uint64_t i = ptr[r] + lane; i < ptr[r + 1]; i += 32) {
-    const Place pl = place(r, col[i], transposed, n_chunks);
-    uint8_t* blk = data + off[pl.block] * 16;
-    const uint2 hd = reinterpret_cast<const uint2*>(blk)[pl.word];
-    const uint32_t e = hd.y + __popc(hd.x & ((1u << pl.bit) - 1u));
-    // A stored -0 is kept as +0 (-0 marks a column without a value).
-    const float x = ldexpf(val[i], scale);
-    const uint32_t w = split_pair(x == 0.0f ? 0.0f : x);
-    uint16_t* ent = reinterpret_cast<uint16_t*>(blk + kHeaderBytes + 8ull * e);
-    ent[pl.half] = (uint16_t)(w & 0xFFFFu);
-    ent[2 + pl.half] = (uint16_t)(w >> 16);
-  }
 }
 
 // The layout (rows x K) of the CSR (n_rows x n_cols) or of its transpose.
@@ -635,9 +709,16 @@ void build_pairs(const uint64_t* ptr, const uint32_t* col, const float* val, uin
   const uint64_t nb = (uint64_t)out.n_tiles * out.n_chunks;
   DeviceBuffer<uint32_t> masks(nb * 64, s);
   masks.zero();
+  // Warps: one per (tile, row quarter) of X, or one per pair of CSR rows for X^T.
+  const uint64_t warps = transposed ? (n_rows + 1) / 2 : (uint64_t)out.n_tiles * 4;
   if (nnz) {
-    pair_mask_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(ptr, col, n_rows, transposed,
-                                                                  out.n_chunks, masks.ptr);
+    if (transposed)
+      cols_mask_kernel<<<blocks_for(warps * 32, 256), 256, 0, s>>>(ptr, col, n_rows,
+                                                                   (uint32_t)out.rows,
+                                                                   out.n_chunks, masks.ptr);
+    else
+      rows_mask_kernel<<<(unsigned)((warps + kMaskWarps - 1) / kMaskWarps), kMaskWarps * 32, 0,
+                         s>>>(ptr, col, n_rows, out.n_tiles, out.n_chunks, masks.ptr);
     KG_LAUNCH_CHECK();
   }
   DeviceBuffer<uint16_t> bases(nb * 64, s);
@@ -658,8 +739,14 @@ void build_pairs(const uint64_t* ptr, const uint32_t* col, const float* val, uin
   pair_header_kernel<<<blocks_for(nb * 32, 256), 256, 0, s>>>(masks.ptr, bases.ptr, out.off.ptr,
                                                               nb, out.data.ptr);
   KG_LAUNCH_CHECK();
-  pair_values_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(
-      ptr, col, val, n_rows, transposed, out.n_chunks, out.off.ptr, out.scale, out.data.ptr);
+  if (transposed)
+    cols_values_kernel<<<blocks_for(warps * 32, 256), 256, 0, s>>>(
+        ptr, col, val, n_rows, (uint32_t)out.rows, out.n_chunks, masks.ptr, bases.ptr,
+        out.off.ptr, out.scale, out.data.ptr);
+  else
+    rows_values_kernel<<<blocks_for(n_rows * 32, 256), 256, 0, s>>>(
+        ptr, col, val, n_rows, out.n_chunks, masks.ptr, bases.ptr, out.off.ptr, out.scale,
+        out.data.ptr);
   KG_LAUNCH_CHECK();
 }
 
