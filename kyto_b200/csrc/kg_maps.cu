@@ -126,50 +126,60 @@ __global__ void column_starts_kernel(const uint32_t* sorted_genes, uint64_t nnz,
   colptr[g] = lo;
 }
 
-// One thread per gene, its cells in cell order: the bits of kyto's single-leaf fold (two
-// f64 sums in one fixed sequential order). The adds form one dependent chain a gene, so
-// the loads run ahead of them: 16-byte loads, four a round, the next round's issued
-// before this round's adds; a warp per CTA spreads the genes over the SMs.
-__global__ void __launch_bounds__(32)
+// One warp per gene, its cells in cell order: the bits of kyto's single-leaf fold (two
+// f64 sums in one fixed sequential order, made by lane 0). The other lanes keep the next
+// 128 values on their way while lane 0 folds the current 128 from shared memory, so the
+// fold's dependent adds, not the loads, set the pace; many genes' warps share an SM.
+constexpr int kMomentWarps = 4;
+constexpr int kMomentChunk = 128;
+
+__global__ void __launch_bounds__(kMomentWarps * 32)
 gene_moments_kernel(const uint64_t* colptr, const float* t, uint32_t n_genes, double* sums,
                     double* squares, uint64_t* positives) {
-  uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ float buf[kMomentWarps][2][kMomentChunk];
+  const unsigned lane = threadIdx.x & 31u, wi = threadIdx.x >> 5;
+  const uint32_t g = blockIdx.x * kMomentWarps + wi;
   if (g >= n_genes) return;
+  const uint64_t a = colptr[g], e = colptr[g + 1];
+  float nxt[kMomentChunk / 32];
+  auto load = [&](uint64_t c0) {
+#pragma unroll
+    for (int m = 0; m < kMomentChunk / 32; ++m) {
+      const uint64_t i = c0 + m * 32 + lane;
+      nxt[m] = i < e ? __ldg(t + i) : 0.0f;
+    }
+  };
+  auto stash = [&](int half) {
+#pragma unroll
+    for (int m = 0; m < kMomentChunk / 32; ++m) buf[wi][half][m * 32 + lane] = nxt[m];
+  };
   double s = 0.0, q = 0.0;
   uint64_t p = 0;
-  auto step = [&](float x) {
-    if (x > 0.0f) ++p;  // t > 0 exactly when the log1p value > 0 (expm1 keeps sign)
-    s = __dadd_rn(s, (double)x);
-    q = __dadd_rn(q, (double)__fmul_rn(x, x));
-  };
-  uint64_t i = colptr[g];
-  const uint64_t e = colptr[g + 1];
-  for (; i < e && (i & 3u); ++i) step(t[i]);  // up to a 16-byte boundary
-  const uint64_t nv = (e - i) / 4;             // whole 16-byte groups
-  const float4* src = reinterpret_cast<const float4*>(t + i);
-  const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  float4 buf[4];
-#pragma unroll
-  for (int u = 0; u < 4; ++u) buf[u] = (uint64_t)u < nv ? __ldg(src + u) : zero;
-  for (uint64_t k = 0; k < nv; k += 4) {
-    float4 nxt[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) nxt[u] = k + 4 + u < nv ? __ldg(src + k + 4 + u) : zero;
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      if (k + u >= nv) break;
-      step(buf[u].x);
-      step(buf[u].y);
-      step(buf[u].z);
-      step(buf[u].w);
+  load(a);
+  stash(0);
+  __syncwarp();
+  int half = 0;
+  for (uint64_t c0 = a; c0 < e; c0 += kMomentChunk, half ^= 1) {
+    if (c0 + kMomentChunk < e) load(c0 + kMomentChunk);
+    if (lane == 0) {
+      const uint32_t n = e - c0 < (uint64_t)kMomentChunk ? (uint32_t)(e - c0) : (uint32_t)kMomentChunk;
+      const float* v = buf[wi][half];
+      for (uint32_t j = 0; j < n; ++j) {
+        const float x = v[j];
+        if (x > 0.0f) ++p;  // t > 0 exactly when the log1p value > 0 (expm1 keeps sign)
+        s = __dadd_rn(s, (double)x);
+        q = __dadd_rn(q, (double)__fmul_rn(x, x));
+      }
     }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) buf[u] = nxt[u];
+    __syncwarp();
+    if (c0 + kMomentChunk < e) stash(half ^ 1);
+    __syncwarp();
   }
-  for (i += nv * 4; i < e; ++i) step(t[i]);
-  sums[g] = s;
-  squares[g] = q;
-  positives[g] = p;
+  if (lane == 0) {
+    sums[g] = s;
+    squares[g] = q;
+    positives[g] = p;
+  }
 }
 
 int bits_for(uint32_t n) {
@@ -311,8 +321,9 @@ kg_status kg_hvg_moments(kg_ctx* ctx, const uint64_t* indptr, const uint32_t* in
     column_starts(genes_sorted.ptr, nnz, n_genes, colptr.ptr, s);
     DeviceBuffer<double> dsum(n_genes, s), dsq(n_genes, s);
     DeviceBuffer<uint64_t> dpos(n_genes, s);
-    gene_moments_kernel<<<blocks_for(n_genes, 32), 32, 0, s>>>(
-        colptr.ptr, (const float*)t_sorted.ptr, n_genes, dsum.ptr, dsq.ptr, dpos.ptr);
+    gene_moments_kernel<<<(n_genes + kMomentWarps - 1) / kMomentWarps, kMomentWarps * 32, 0,
+                          s>>>(colptr.ptr, (const float*)t_sorted.ptr, n_genes, dsum.ptr,
+                               dsq.ptr, dpos.ptr);
     KG_LAUNCH_CHECK();
     KG_CUDA(cudaMemcpyAsync(sums, dsum.ptr, n_genes * 8ull, cudaMemcpyDefault, s));
     KG_CUDA(cudaMemcpyAsync(sums_of_squares, dsq.ptr, n_genes * 8ull, cudaMemcpyDefault, s));
@@ -561,8 +572,8 @@ kg_status kg_hvg_moments_noalloc(kg_ctx* ctx, const uint64_t* indptr, const uint
     }
     if (n_genes) {
       column_starts(keys.Current(), nnz, n_genes, colptr, s);
-      gene_moments_kernel<<<blocks_for(n_genes, 32), 32, 0, s>>>(
-          colptr, (const float*)vals.Current(), n_genes, dsum, dsq, dpos);
+      gene_moments_kernel<<<(n_genes + kMomentWarps - 1) / kMomentWarps, kMomentWarps * 32, 0,
+                            s>>>(colptr, (const float*)vals.Current(), n_genes, dsum, dsq, dpos);
       KG_LAUNCH_CHECK();
       KG_CUDA(cudaMemcpyAsync(sums, dsum, n_genes * 8ull, cudaMemcpyDefault, s));
       KG_CUDA(cudaMemcpyAsync(sums_of_squares, dsq, n_genes * 8ull, cudaMemcpyDefault, s));
