@@ -195,9 +195,10 @@ def run_step(args, ctx, indptr, idx, vals, out, host: bool):
 def e2e_steps(args, ctx, indptr, idx, vals, out, steps: int) -> None:
     """``steps`` steps through the public API from pinned host memory, as a streaming
     caller runs them: each step's CSR goes to the device by an asynchronous push
-    (kg_pca_push_block_async: its copies on the session's own stream), queued before the
-    previous step's search so the copies run beside it; each step's graph comes back to
-    host memory inside kg_knn_exact. Every step copies its own input and output."""
+    (kg_pca_push_block_async: its copies and packing kernels on the session's own
+    stream), queued before the previous step's PCA so that they run beside that step's
+    PCA and search; each step's graph comes back to host memory inside kg_knn_exact.
+    Every step copies its own input and output."""
     import kyto_b200 as K
 
     def new_session():
@@ -209,9 +210,9 @@ def e2e_steps(args, ctx, indptr, idx, vals, out, steps: int) -> None:
     nxt = new_session()
     for i in range(steps):
         sess = nxt
-        sess.run()
         if i + 1 < steps:
             nxt = new_session()
+        sess.run()
         K._check(L.kg_knn_exact(ctx.handle, sess.embedding_device_ptr(), args.cells,
                                 args.components, 0, args.neighbors, K._ptr(out[0]),
                                 K._ptr(out[1]), K._ptr(out[2]), None))
@@ -356,9 +357,9 @@ def cpu_baseline_and_parity(args, x, vals, res, graph) -> tuple[dict, dict]:
 
 def learned_vs_exact(n: int, ctx) -> dict:
     """C5: n x 50 f32 points from a 200-component Gaussian mixture (weights Dirichlet(1),
-    isotropic sigma log-uniform [0.2, 2]); the learned-partition kNN (1,024 parts, BF16
-    MLP 50-256-256-1024 trained on the device on the exact graph of a 200,000-row sample,
-    top-8 probes, fallback below 0.9 confidence) against the exact search, recall@15
+    isotropic sigma log-uniform [0.2, 2]); the learned-partition kNN (512 parts, BF16
+    MLP 50-256-256-512 trained on the device on the exact graph of a 200,000-row sample,
+    top-5 probes, fallback below 0.85 confidence) against the exact search, recall@15
     judged by the exact graph. Times: host wall clock around each call, inputs on the
     device, after one untimed call of each (the filter kind tuning is cached)."""
     import torch
@@ -370,8 +371,8 @@ def learned_vs_exact(n: int, ctx) -> dict:
                                       device="cuda")
     xd = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float32)).cuda()
     k = 14
-    params = K.LearnedParams(n_parts=1024, hidden=256, n_probe=8, confidence=0.9,
-                             train_cells=200_000, epochs=6, batch=4096, seed=0)
+    params = K.LearnedParams(n_parts=512, hidden=256, n_probe=5, confidence=0.85,
+                             train_cells=200_000, epochs=6, batch=8192, seed=0)
 
     def graph(fn):
         out = (torch.empty(n + 1, dtype=torch.int64, device="cuda"),

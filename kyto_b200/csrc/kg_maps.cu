@@ -164,6 +164,7 @@ gene_moments_kernel(const uint64_t* colptr, const float* t, uint32_t n_genes, do
     if (lane == 0) {
       const uint32_t n = e - c0 < (uint64_t)kMomentChunk ? (uint32_t)(e - c0) : (uint32_t)kMomentChunk;
       const float* v = buf[wi][half];
+#pragma unroll 8
       for (uint32_t j = 0; j < n; ++j) {
         const float x = v[j];
         if (x > 0.0f) ++p;  // t > 0 exactly when the log1p value > 0 (expm1 keeps sign)

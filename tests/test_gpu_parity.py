@@ -370,6 +370,25 @@ def test_pca_neighbors_batch_equals_each_sample_alone(ctx):
         _graph_equal(g, K.neighbors(one.embedding, 15, ctx=ctx))
 
 
+def test_pca_neighbors_batch_stages_large_host_blocks(ctx):
+    # Samples whose index and value arrays pass 4 MB are copied by the batching workers
+    # through page-locked staging buffers (16 MB halves, the second sample spanning
+    # several); the results equal the single-sample calls' (the driver's own copies)
+    # bit for bit.
+    samples = []
+    for i, (m, per_cell) in enumerate([(20_000, 60), (70_000, 80), (700, 40)]):
+        x = synthetic.counts_csr(m, 400, per_cell, 4, 30, seed=80 + i, device="cpu")
+        samples.append((x.indptr, x.indices, x.values))
+    assert samples[1][2].nbytes > (16 << 20)
+    out, _ = K.pca_neighbors_batch(samples, 400, 20, 10, seed=0, target_sum=1e4, log1p=True,
+                                   ctx=ctx)
+    for (indptr, idx, vals), (res, g) in zip(samples, out):
+        one = K.pca(indptr, idx, vals, 400, 20, seed=0, target_sum=1e4, log1p=True, ctx=ctx)
+        assert np.array_equal(res.embedding.view(np.uint32), one.embedding.view(np.uint32))
+        assert np.array_equal(res.variance.view(np.uint64), one.variance.view(np.uint64))
+        _graph_equal(g, K.neighbors(one.embedding, 10, ctx=ctx))
+
+
 # ------------------------------------------------------------ connectivities ----------
 
 from oracle import connectivities as OC  # noqa: E402
