@@ -357,9 +357,9 @@ def cpu_baseline_and_parity(args, x, vals, res, graph) -> tuple[dict, dict]:
 
 def learned_vs_exact(n: int, ctx) -> dict:
     """C5: n x 50 f32 points from a 200-component Gaussian mixture (weights Dirichlet(1),
-    isotropic sigma log-uniform [0.2, 2]); the learned-partition kNN (512 parts, BF16
-    MLP 50-256-256-512 trained on the device on the exact graph of a 200,000-row sample,
-    top-5 probes, fallback below 0.85 confidence) against the exact search, recall@15
+    isotropic sigma log-uniform [0.2, 2]); the learned-partition kNN (1,024 parts, BF16
+    MLP 50-256-256-1024 trained on the device on the exact graph of a 100,000-row sample,
+    top-4 probes, fallback below 0.3 confidence) against the exact search, recall@15
     judged by the exact graph. Times: host wall clock around each call, inputs on the
     device, after one untimed call of each (the filter kind tuning is cached)."""
     import torch
@@ -371,8 +371,8 @@ def learned_vs_exact(n: int, ctx) -> dict:
                                       device="cuda")
     xd = torch.from_numpy(np.ascontiguousarray(x, dtype=np.float32)).cuda()
     k = 14
-    params = K.LearnedParams(n_parts=512, hidden=256, n_probe=5, confidence=0.85,
-                             train_cells=200_000, epochs=6, batch=8192, seed=0)
+    params = K.LearnedParams(n_parts=1024, hidden=256, n_probe=4, confidence=0.3,
+                             train_cells=100_000, epochs=4, batch=8192, seed=0)
 
     def graph(fn):
         out = (torch.empty(n + 1, dtype=torch.int64, device="cuda"),

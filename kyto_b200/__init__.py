@@ -116,10 +116,10 @@ class BatchStats(ctypes.Structure):
 
 
 class LearnedParams(ctypes.Structure):
-    """kg_learned_params: the learned-partition kNN's settings (defaults: 512 parts,
-    256 hidden, top-5 probes, confidence 0.85, 200,000 training rows, 6 epochs of
-    8,192-row batches: the fastest setting of a sweep on a 4M-row, 200-component
-    Gaussian mixture, recall@15 0.999997)."""
+    """kg_learned_params: the learned-partition kNN's settings (defaults: 1,024 parts,
+    256 hidden, top-4 probes, fallback below confidence 0.3, 100,000 training rows, 4
+    epochs of 8,192-row batches: the fastest setting of a sweep on a 4M-row,
+    200-component Gaussian mixture at recall@15 >= 0.999)."""
 
     _fields_ = [
         ("n_parts", ctypes.c_uint32),
@@ -134,8 +134,8 @@ class LearnedParams(ctypes.Structure):
         ("seed", ctypes.c_uint64),
     ]
 
-    def __init__(self, n_parts=512, hidden=256, n_probe=5, confidence=0.85,
-                 train_cells=200_000, epochs=6, batch=8192, learning_rate=1e-3, seed=0,
+    def __init__(self, n_parts=1024, hidden=256, n_probe=4, confidence=0.3,
+                 train_cells=100_000, epochs=4, batch=8192, learning_rate=1e-3, seed=0,
                  random_init=False):
         super().__init__(n_parts, hidden, n_probe, confidence, train_cells, epochs, batch,
                          learning_rate, KG_LEARNED_RANDOM_INIT if random_init else 0, seed)

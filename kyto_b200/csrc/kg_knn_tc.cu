@@ -179,26 +179,13 @@ __device__ __noinline__ void tc_offer(QueryState& st, float* smallest, uint32_t 
 
 // Offer the keys of one 32-point chunk selected by `mask` (bit j: point p0 + j, key
 // keys[j]), in column order, to the query's state; points outside [lo, n) and the query's
-// own slot q are skipped. For k <= KR the query's k smallest
-// keys (smallest[0..KR) in the thread's shared-memory slice, ascending, +inf past those
-// seen) move into registers for the chunk: an insertion is 2 KR branch-free min/max
-// (v[i] = max(v[i-1], min(v[i], key)) on the old values), no dependent memory access.
+// own slot q are skipped. For k <= KR the query's k smallest keys live in the last k of
+// KR slots (smallest[KR - k .. KR) in the thread's shared-memory slice, ascending, +inf
+// past those seen; the first KR - k slots hold -inf), so the k-th smallest is always the
+// last slot. They move into registers for the chunk: an insertion is 2 KR branch-free
+// min/max (v[i] = max(v[i-1], min(v[i], key)) on the old values: the -inf slots stay
+// -inf and the largest falls off the end), no dependent memory access and no selection.
 // Inline: a call here would save and restore the epilogue's live registers each time.
-// v[kb] for a power-of-two KR: a tree of selects on the bits of kb (depth log2 KR).
-template <int KR>
-__device__ __forceinline__ float select_kth(const float (&v)[KR], uint32_t kb) {
-  float a[KR];
-#pragma unroll
-  for (int i = 0; i < KR; ++i) a[i] = v[i];
-#pragma unroll
-  for (int lvl = 0; (KR >> lvl) > 1; ++lvl) {
-    const bool hi = (kb >> lvl) & 1u;
-#pragma unroll
-    for (int i = 0; i < (KR >> (lvl + 1)); ++i) a[i] = hi ? a[2 * i + 1] : a[2 * i];
-  }
-  return a[0];
-}
-
 template <int KR>
 __device__ __forceinline__ void tc_offer_chunk(QueryState& st, float* smallest, uint32_t k,
                                                double slack2, const float* keys, uint32_t mask,
@@ -215,15 +202,13 @@ __device__ __forceinline__ void tc_offer_chunk(QueryState& st, float* smallest, 
         tc_offer(st, smallest, k, slack2, key, (uint32_t)p, ck, cr, cap);
     }
   } else {
-    static_assert((KR & (KR - 1)) == 0, "register top-k width: a power of two");
     float v[KR];
 #pragma unroll
     for (int i = 0; i < KR; ++i) v[i] = smallest[i];
-    const uint32_t kb = k - 1;
     // The slack as the f32 it was rounded up to: the threshold kth + slack rounded up in
     // one f32 add (__fadd_ru: never below the exact sum).
     const float sl2f = (float)slack2;
-    float kth = select_kth<KR>(v, kb);
+    float kth = v[KR - 1];
     bool changed = false;
     while (mask && !st.overflowed) {
       const int j = __ffs(mask) - 1;
@@ -240,7 +225,7 @@ __device__ __forceinline__ void tc_offer_chunk(QueryState& st, float* smallest, 
           v[i] = fmaxf(prev, fminf(cur, key));
           prev = cur;
         }
-        kth = select_kth<KR>(v, kb);
+        kth = v[KR - 1];
         if (kth < INFINITY) st.th = __fadd_ru(kth, sl2f);
         changed = true;
       }
@@ -686,7 +671,7 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
       const double s2qn2 = active && scan.qn2 ? scan.s2 * scan.qn2[q] : 0.0;
       QueryState st{INFINITY, 0, 0, 64, false};
       if (KR > 0)
-        for (int i = 0; i < KR; ++i) smallest[i] = INFINITY;
+        for (int i = 0; i < KR; ++i) smallest[i] = i < KR - (int)k ? -INFINITY : INFINITY;
       float th = INFINITY;
       bool live = active;  // not overflowed
       const double sl2 = active ? (double)slack2[q] : 0.0;
