@@ -61,8 +61,10 @@ enum : int { kAmSmem = kTcAmSmem, kAmTmem = kTcAmTmem, kAmHalf = kTcAmHalf };
 // register top-k width (16, 32) or 0 (the k smallest in local memory, any k).
 template <int KR, int SUBS>
 struct TcShape {
-  // Point-tile stages (six measured faster than eight on the 1M benchmark embedding).
-  static constexpr int kStages = SUBS == 1 ? 6 : (KR == 32 ? 2 : 3);
+  // Point-tile stages: eight where shared memory holds them (on the 1M benchmark
+  // embedding, whose 128 MB point operand overflows L2, 166 ms against 168-178 ms with six
+  // and 170 ms with seven).
+  static constexpr int kStages = SUBS == 1 ? (KR == 32 ? 6 : 8) : (KR == 32 ? 2 : 3);
   static constexpr int kTopK = KR == 0 ? 1 : KR + 1;  // odd row stride: no bank conflicts
 };
 
@@ -92,7 +94,8 @@ template <int KR, int SUBS>
 constexpr size_t tc_smem_bytes() {
   return sizeof(TcSmem<KR, SUBS>) + 1024;  // + alignment slack
 }
-static_assert(tc_smem_bytes<32, 1>() <= 227 * 1024 && tc_smem_bytes<16, 2>() <= 227 * 1024 &&
+static_assert(tc_smem_bytes<32, 1>() <= 227 * 1024 && tc_smem_bytes<16, 1>() <= 227 * 1024 &&
+                  tc_smem_bytes<0, 1>() <= 227 * 1024 && tc_smem_bytes<16, 2>() <= 227 * 1024 &&
                   tc_smem_bytes<32, 2>() <= 227 * 1024 && tc_smem_bytes<0, 2>() <= 227 * 1024,
               "filter shared memory");
 
@@ -124,46 +127,78 @@ __device__ __forceinline__ float min_of_32(const uint32_t (&r)[32]) {
 // Per-query filter state (kyto's Query, neighbors_exact.rs:196-255).
 struct QueryState {
   float th;
-  uint32_t n_small, count, compact_at;
+  uint32_t n_small, count;
   bool overflowed;
 };
 
-// Compact the query's slice against its threshold (neighbors_exact.rs:236-252): out of
-// line, it runs once per doubling of the slice.
+constexpr uint32_t kCompactRound = 16;  // slice entries read per round of a compaction
+
+// Compact the query's slice against its threshold (neighbors_exact.rs:236-252). It runs
+// between tiles, when the slice may not hold another tile's keys (tc_make_room): entries
+// above the threshold can never be neighbours and the re-rank skips any left in the
+// slice, so compacting earlier would change nothing but the cost. Out of line, called
+// where no tile's keys are live. The slice is read 16 entries a round, all loaded before
+// any is written back (a write never passes the read position), so a round waits for its
+// loads once instead of once an entry. The slice's base and cap are multiples of 16
+// entries. More than half the slice kept: the query overflows.
 __device__ __noinline__ void tc_compact(QueryState& st, float* ck, uint32_t* cr, uint32_t cap) {
   uint32_t kept = 0;
-  for (uint32_t i = 0; i < st.count; ++i) {
-    float v = ck[i];
-    if (v <= st.th) {
-      ck[kept] = v;
-      cr[kept] = cr[i];
-      ++kept;
+  for (uint32_t i = 0; i < st.count; i += kCompactRound) {
+    float v[kCompactRound];
+    uint32_t r[kCompactRound];
+    if (i + kCompactRound <= st.count) {
+#pragma unroll
+      for (uint32_t j = 0; j < kCompactRound; j += 4) {
+        const float4 a = *reinterpret_cast<const float4*>(ck + i + j);
+        const uint4 b = *reinterpret_cast<const uint4*>(cr + i + j);
+        v[j] = a.x, v[j + 1] = a.y, v[j + 2] = a.z, v[j + 3] = a.w;
+        r[j] = b.x, r[j + 1] = b.y, r[j + 2] = b.z, r[j + 3] = b.w;
+      }
+    } else {
+#pragma unroll
+      for (uint32_t j = 0; j < kCompactRound; ++j) {
+        const bool in = i + j < st.count;
+        v[j] = in ? ck[i + j] : INFINITY;
+        r[j] = in ? cr[i + j] : 0u;
+      }
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < kCompactRound; ++j) {
+      if (v[j] <= st.th) {
+        ck[kept] = v[j];
+        cr[kept] = r[j];
+        ++kept;
+      }
     }
   }
   st.count = kept;
   if (st.count > (cap >> 1)) st.overflowed = true;
-  st.compact_at = min(max(2 * st.count, 64u), cap);
 }
 
-// Append candidate (key, p) (already <= st.th) to the query's slice, compacting it
-// against the threshold when it reaches compact_at.
+// Every slice has room for a tile's keys at the start of each tile.
+static_assert(kTcCap >= 2 * 128 && kTcRetrySplitCap >= 2 * 128 && kTcRetryCap >= 2 * 128,
+              "a compacted slice keeps at most half its cap, and a tile appends 128 keys");
+
+// Between tiles: compact the slice when another tile's keys might not fit.
+__device__ __forceinline__ void tc_make_room(QueryState& st, float* ck, uint32_t* cr,
+                                             uint32_t cap, uint32_t tile) {
+  if (!st.overflowed && st.count > cap - tile) tc_compact(st, ck, cr, cap);
+}
+
+// Append candidate (key, p) (already <= st.th) to the query's slice, which has room for
+// it (tc_make_room ran before the tile).
 __device__ __forceinline__ void tc_append(QueryState& st, float key, uint32_t p, float* ck,
-                                          uint32_t* cr, uint32_t cap) {
-  if (st.count == cap) {
-    st.overflowed = true;
-    return;
-  }
+                                          uint32_t* cr) {
   ck[st.count] = key;
   cr[st.count] = p;
   ++st.count;
-  if (st.count >= st.compact_at) tc_compact(st, ck, cr, cap);
 }
 
 // Offer approximate key `key` of point `p` (already <= st.th) to the query's state: its
 // k smallest keys in local memory (any k up to kMaxK).
 __device__ __noinline__ void tc_offer(QueryState& st, float* smallest, uint32_t k,
                                       double slack2, float key, uint32_t p, float* ck,
-                                      uint32_t* cr, uint32_t cap) {
+                                      uint32_t* cr) {
   if (st.n_small < k || key < smallest[k - 1]) {
     if (st.n_small < k) ++st.n_small;
     uint32_t at = st.n_small - 1;
@@ -174,68 +209,102 @@ __device__ __noinline__ void tc_offer(QueryState& st, float* smallest, uint32_t 
     smallest[at] = key;
     if (st.n_small == k) st.th = round_up_f32d((double)smallest[k - 1] + slack2);
   }
-  if (key <= st.th) tc_append(st, key, p, ck, cr, cap);
+  if (key <= st.th) tc_append(st, key, p, ck, cr);
+}
+
+// The points p0 .. p0 + 31 a query may take: bit j set when p0 + j lies in [lo, hi) and
+// is not the query's own point slot.
+__device__ __forceinline__ uint32_t tc_valid_bits(uint64_t p0, uint64_t self, uint64_t lo,
+                                                  uint64_t hi) {
+  uint32_t m = 0xFFFFFFFFu;
+  if (p0 < lo || p0 + 32 > hi) {
+    const uint32_t a = lo <= p0 ? 0u : (uint32_t)min(lo - p0, (uint64_t)32);
+    const uint32_t b = hi <= p0 ? 0u : (uint32_t)min(hi - p0, (uint64_t)32);
+    const uint32_t below_b = b >= 32 ? 0xFFFFFFFFu : (1u << b) - 1u;
+    const uint32_t below_a = a >= 32 ? 0xFFFFFFFFu : (1u << a) - 1u;
+    m = below_b & ~below_a;
+  }
+  if (self >= p0 && self < p0 + 32) m &= ~(1u << (uint32_t)(self - p0));
+  return m;
 }
 
 // Offer the keys of one 32-point chunk selected by `mask` (bit j: point p0 + j, key
-// keys[j]), in column order, to the query's state; points outside [lo, n) and the query's
-// own slot q are skipped. For k <= KR the query's k smallest keys live in the last k of
-// KR slots (smallest[KR - k .. KR) in the thread's shared-memory slice, ascending, +inf
-// past those seen; the first KR - k slots hold -inf), so the k-th smallest is always the
-// last slot. They move into registers for the chunk: an insertion is 2 KR branch-free
-// min/max (v[i] = max(v[i-1], min(v[i], key)) on the old values: the -inf slots stay
-// -inf and the largest falls off the end), no dependent memory access and no selection.
-// Inline: a call here would save and restore the epilogue's live registers each time.
-template <int KR>
+// keys[j]), in column order, to the query's state (k > 32: the k smallest in local
+// memory, tc_offer); `mask` holds only points the query may take.
 __device__ __forceinline__ void tc_offer_chunk(QueryState& st, float* smallest, uint32_t k,
                                                double slack2, const float* keys, uint32_t mask,
-                                               uint64_t p0, uint64_t q, uint64_t lo, uint64_t n,
-                                               float* ck,
-                                               uint32_t* cr, uint32_t cap) {
-  if constexpr (KR == 0) {
-    while (mask && !st.overflowed) {
-      const int j = __ffs(mask) - 1;
-      mask &= mask - 1;
-      const float key = keys[j];
-      const uint64_t p = p0 + j;
-      if (key <= st.th && p >= lo && p < n && p != q)
-        tc_offer(st, smallest, k, slack2, key, (uint32_t)p, ck, cr, cap);
-    }
-  } else {
-    float v[KR];
+                                               uint64_t p0, float* ck, uint32_t* cr) {
+  while (mask) {
+    const int j = __ffs(mask) - 1;
+    mask &= mask - 1;
+    const float key = keys[j];
+    if (key <= st.th) tc_offer(st, smallest, k, slack2, key, (uint32_t)(p0 + j), ck, cr);
+  }
+}
+
+// Insert the keys of one 32-point chunk selected by `mask` (keys[j]) that fall below the
+// query's k-th smallest, in column order. For k <= KR the query's k smallest keys live
+// in the last k of KR slots (smallest[KR - k .. KR) in the thread's shared-memory slice,
+// ascending, +inf past those seen; the first KR - k slots hold -inf), so the k-th
+// smallest is always the last slot. They move into registers for the chunk: an
+// insertion is 2 KR branch-free min/max (v[i] = max(v[i-1], min(v[i], key)) on the old
+// values: the -inf slots stay -inf and the largest falls off the end). The threshold
+// becomes the k-th + slack (one f32 add rounded up: never below the exact sum), and
+// never rises (a bound from before, such as the first tile's, may be lower).
+template <int KR>
+__device__ __forceinline__ void tc_insert_chunk(float* smallest, float& kth, float& th,
+                                                float sl2f, const float* keys, uint32_t mask) {
+  float v[KR];
 #pragma unroll
-    for (int i = 0; i < KR; ++i) v[i] = smallest[i];
-    // The slack as the f32 it was rounded up to: the threshold kth + slack rounded up in
-    // one f32 add (__fadd_ru: never below the exact sum).
-    const float sl2f = (float)slack2;
-    float kth = v[KR - 1];
-    bool changed = false;
-    while (mask && !st.overflowed) {
-      const int j = __ffs(mask) - 1;
-      mask &= mask - 1;
-      const float key = keys[j];
-      const uint64_t p = p0 + j;
-      if (!(key <= st.th) || p < lo || p >= n || p == q) continue;
-      if (key < kth) {
-        float prev = v[0];
-        v[0] = fminf(v[0], key);
+  for (int i = 0; i < KR; ++i) v[i] = smallest[i];
+  bool changed = false;
+  while (mask) {
+    const int j = __ffs(mask) - 1;
+    mask &= mask - 1;
+    const float key = keys[j];
+    if (key < kth) {
+      float prev = v[0];
+      v[0] = fminf(v[0], key);
 #pragma unroll
-        for (int i = 1; i < KR; ++i) {
-          const float cur = v[i];
-          v[i] = fmaxf(prev, fminf(cur, key));
-          prev = cur;
-        }
-        kth = v[KR - 1];
-        if (kth < INFINITY) st.th = __fadd_ru(kth, sl2f);
-        changed = true;
+      for (int i = 1; i < KR; ++i) {
+        const float cur = v[i];
+        v[i] = fmaxf(prev, fminf(cur, key));
+        prev = cur;
       }
-      if (key <= st.th) tc_append(st, key, (uint32_t)p, ck, cr, cap);
-    }
-    if (changed) {
-#pragma unroll
-      for (int i = 0; i < KR; ++i) smallest[i] = v[i];
+      kth = v[KR - 1];
+      if (kth < INFINITY) th = fminf(th, __fadd_ru(kth, sl2f));
+      changed = true;
     }
   }
+  if (changed) {
+#pragma unroll
+    for (int i = 0; i < KR; ++i) smallest[i] = v[i];
+  }
+}
+
+// The warp appends its lanes' selected keys of one chunk to their queries' slices: lane
+// L's keys are rows[L][j] for the bits j of its mask (point p0 + j), and its query's slice
+// starts at slot q0 + L. The warp writes one lane's keys at a time, a lane a key, in
+// column order and contiguously from the lane's count (coalesced stores, no per-key
+// loop). Every lane calls it; each lane's count grows by its keys. The slices have room
+// (tc_make_room).
+__device__ __forceinline__ void tc_warp_append(uint32_t mask, uint32_t& count,
+                                               const float (*rows)[33], int lane, uint64_t q0,
+                                               uint64_t p0, uint32_t cap, float* cand_key,
+                                               uint32_t* cand_row) {
+  uint32_t pend = __ballot_sync(0xFFFFFFFFu, mask != 0);
+  while (pend) {
+    const int L = __ffs(pend) - 1;
+    pend &= pend - 1;
+    const uint32_t m = __shfl_sync(0xFFFFFFFFu, mask, L);
+    const uint32_t base = __shfl_sync(0xFFFFFFFFu, count, L);
+    if ((m >> lane) & 1u) {
+      const uint64_t at = (q0 + L) * cap + base + __popc(m & ((1u << lane) - 1u));
+      cand_key[at] = rows[L][lane];
+      cand_row[at] = (uint32_t)(p0 + lane);
+    }
+  }
+  count += __popc(mask);
 }
 
 // KR: the register top-k width used on offers (k <= KR), or 0 for any k. SUBS: operand
@@ -613,9 +682,11 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
     // ------------------------------------------------------------ epilogue --------
     // Per tile: the 128 keys come out of TMEM into registers and the accumulator is
     // released; a 32-key chunk whose minimum reaches the threshold (rare once it has
-    // fallen) has its passing keys offered by its lane alone. The threshold and
+    // fallen) has its keys below the query's k-th smallest inserted by its lane and its
+    // passing keys appended by the whole warp. The threshold, the k-th smallest and the
     // overflow flag stay in registers; after offers the warp publishes its largest
-    // threshold + s^2 |q|^2 for the producer's bound checks.
+    // threshold + s^2 |q|^2 for the producer's bound checks, and a slice that might not
+    // hold another tile's keys is compacted.
     const uint32_t half = (uint32_t)warp >> 2, quad = (uint32_t)warp & 3;
     // The warp's i-th item: with half slots, the half's slot sequence (items 2 i + half
     // of the MMA warp's, kHalfSlots slots of 128 columns); else the two shared slots,
@@ -669,12 +740,14 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
         p_hi = scan.sample_first[smp + 1];
       }
       const double s2qn2 = active && scan.qn2 ? scan.s2 * scan.qn2[q] : 0.0;
-      QueryState st{INFINITY, 0, 0, 64, false};
+      QueryState st{INFINITY, 0, 0, false};
       if (KR > 0)
         for (int i = 0; i < KR; ++i) smallest[i] = i < KR - (int)k ? -INFINITY : INFINITY;
-      float th = INFINITY;
+      float th = INFINITY, kth = INFINITY;  // kth: the k-th smallest key so far (k <= KR)
       bool live = active;  // not overflowed
       const double sl2 = active ? (double)slack2[q] : 0.0;
+      // The doubled slack as an f32 (slack2 holds f32 values, so the conversion is exact).
+      const float sl2f = (float)sl2;
       float* ck = cand_key + (active ? q : 0) * (uint64_t)cap;
       uint32_t* cr = cand_row + (active ? q : 0) * (uint64_t)cap;
       for (bool first = true;; ++it, first = false) {
@@ -705,28 +778,80 @@ knn_filter_tc_kernel(const __grid_constant__ CUtensorMap tmap_q,
         tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&sm.tmem_empty[ab]);
-        uint32_t hits = 0;
+        if (th == INFINITY && live) {
+          // No threshold yet (the block's first tile): every key would be offered. The
+          // tile's 128 keys in 16 groups of 8 have 16 minima at most M, so at least 16
+          // keys, of which at most one is the query's own, lie at or below M: with every
+          // point of the tile in the query's range and k (+1 when the query's own point is
+          // in the tile) at most 16, the k-th smallest key of the scan is at most M, and
+          // M + slack bounds every threshold the query will have. Only keys within it are
+          // offered.
+          const uint64_t t0 = (uint64_t)pt * kTcPoints;
+          const uint32_t own = self >= t0 && self < t0 + kTcPoints ? 1u : 0u;
+          if (t0 >= p_lo && t0 + kTcPoints <= p_hi && k + own <= 16u) {
+            float m = -INFINITY;
 #pragma unroll
-        for (int c = 0; c < kTcPoints / 32; ++c)
-          hits |= (live && min_of_32(r[c]) <= th ? 1u : 0u) << c;
-        const bool offered = __any_sync(0xFFFFFFFFu, hits != 0);
-        // Each lane offers its own passing keys, chunk by chunk in column order (the
-        // threshold only falls while they are offered), through its scratch row.
+            for (int c = 0; c < kTcPoints / 32; ++c)
+#pragma unroll
+              for (int g = 0; g < 4; ++g) {
+                const uint32_t* e = &r[c][8 * g];
+                const float a = min3f(__uint_as_float(e[0]), __uint_as_float(e[1]),
+                                      __uint_as_float(e[2]));
+                const float b = min3f(__uint_as_float(e[3]), __uint_as_float(e[4]),
+                                      __uint_as_float(e[5]));
+                m = fmaxf(m, min3f(a, b, fminf(__uint_as_float(e[6]), __uint_as_float(e[7]))));
+              }
+            th = __fadd_ru(m, (float)sl2);
+          }
+        }
+        uint32_t hits = 0;
+        float cmin[kTcPoints / 32];
 #pragma unroll
         for (int c = 0; c < kTcPoints / 32; ++c) {
-          if (!((hits >> c) & 1u) || !live) continue;
-          uint32_t mask = 0;
+          cmin[c] = min_of_32(r[c]);
+          hits |= (live && cmin[c] <= th ? 1u : 0u) << c;
+        }
+        const bool offered = __any_sync(0xFFFFFFFFu, hits != 0);
+        if (offered) {
+          // Chunk by chunk in column order: each lane with a key at most its threshold
+          // copies the chunk's keys to its scratch row and selects the passing ones of
+          // the points it may take; keys below its k-th smallest (rare once the threshold
+          // has fallen) go into its k smallest one by one, the threshold falling with
+          // them; then the warp appends every lane's selected keys. A key selected
+          // against the threshold from before the chunk's insertions is kept even if the
+          // threshold fell below it: the re-rank skips it.
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const float key = __uint_as_float(r[c][j]);
-            my[j] = key;
-            mask |= (key <= th ? 1u : 0u) << j;
+          for (int c = 0; c < kTcPoints / 32; ++c) {
+            const uint64_t p0 = (uint64_t)pt * kTcPoints + c * 32;
+            uint32_t mask = 0;
+            if (((hits >> c) & 1u) && live) {
+#pragma unroll
+              for (int j = 0; j < 32; ++j) {
+                const float key = __uint_as_float(r[c][j]);
+                my[j] = key;
+                mask |= (key <= th ? 1u : 0u) << j;
+              }
+              mask &= tc_valid_bits(p0, self, p_lo, p_hi);
+              if constexpr (KR > 0) {
+                if (cmin[c] < kth) tc_insert_chunk<KR>(smallest, kth, th, sl2f, my, mask);
+              } else {
+                st.th = th;
+                tc_offer_chunk(st, smallest, k, sl2, my, mask, p0, ck, cr);
+                th = st.th;
+              }
+            }
+            if constexpr (KR > 0) {
+              __syncwarp();
+              tc_warp_append(mask, st.count, &sm.scratch[warp * 32], lane, q - lane, p0, cap,
+                             cand_key, cand_row);
+              __syncwarp();
+            }
           }
-          const uint64_t p0 = (uint64_t)pt * kTcPoints + c * 32;
-          st.th = th;
-          tc_offer_chunk<KR>(st, smallest, k, sl2, my, mask, p0, self, p_lo, p_hi, ck, cr, cap);
-          th = st.th;
-          live = !st.overflowed;
+          if (live) {
+            st.th = th;
+            tc_make_room(st, ck, cr, cap, kTcPoints);
+            live = !st.overflowed;
+          }
         }
         if (offered && scan.list_lb2) {
           // A point is offered only if its key is at most th; its key is at least
