@@ -4,31 +4,31 @@
 //
 // S is the held input X (rows = cells, K = genes) for X Q and the embedding pass, or X^T
 // (rows = genes, K = cells) for X^T W, the sketch and the gene statistics; both are kept
-// in the blocked layout of kg_spmm_tc.cuh (128 rows x 32 columns a block, column masks,
-// values as fp16 hi/lo pairs of the scaled value). D comes as D^T in the same two fp16
-// parts (the dense layout of kg_spmm_tc.cuh). Each 128 x 32 block of S is expanded
-// straight into tensor memory (one thread per row: for each column the warp reads
-// consecutive value words, conflict-free) as a 128 x 32 hi tile and a lo tile, and
-// multiplied by three kind::f16 MMAs per 16 K that read A from TMEM and D^T from shared
-// memory (hi.hi + hi.lo + lo.hi: both operands to about 2^-22, as three tf32 products
-// give, at twice their rate), accumulated in TMEM over at most kFlushChunks chunks and
-// then added into f64 registers (no f32 sum runs over more than 512 terms); the scales
-// come off in f64 at the end (powers of two, exact).
+// in the pair-entry layout of kg_spmm_tc.cuh (128 rows x 32 columns a block: a header of
+// (mask, base) words per row quarter and column pair, then one 8-byte entry per row and
+// pair holding the fp16 hi/lo parts of both columns' scaled values). D comes as D^T in the
+// same two fp16 parts (the dense layout of kg_spmm_tc.cuh). Each 128 x 32 block of S is
+// expanded straight into tensor memory as a 128 x 32 hi tile and a lo tile (a lane per
+// row; a lane without an entry for a pair writes the absent value, so the loads have no
+// branches), and multiplied by three kind::f16 MMAs per 16 K that read A from TMEM and
+// D^T from shared memory (hi.hi + hi.lo + lo.hi: both operands to about 2^-22, as three
+// tf32 products give, at twice their rate), accumulated in TMEM over at most
+// kFlushChunks chunks and then added into f64 registers (no f32 sum runs over more than
+// 512 terms); the scales come off in f64 at the end (powers of two, exact).
 //
-// Per CTA (persistent, 320 threads) and per K-chunk of a work item (tile, K segment):
-//   warp 8      loads: the chunk's D^T tile (64 x (32 hi + 32 lo) fp16, one TMA box) and
-//               the block (one bulk copy) into one of kLoadStages stages; the next 32
-//               blocks are prefetched into L2 ahead of their copies;
-//   warps 0-3   expand: lane l of warp q writes row 32 q + l of the chunk's A tiles (16 hi
-//               and 16 lo words, two fp16 a word) into TMEM lane 32 q + l of one of
-//               kABufs A buffers;
-//   warp 9      MMA: 6 tcgen05.mma (kind::f16, A from TMEM, M=128 N=64 K=16) into one of
+// Per CTA (persistent, 576 threads) and per K-chunk of a work item (tile, K segment):
+//   warp 16     loads: the chunk's D^T tile (64 x (32 hi + 32 lo) fp16, one TMA box) and
+//               the block (one bulk copy) into one of kLoadStages stages;
+//   warps 0-7   expand: the 128 x 32 block in row quarters and column pairs, from the
+//               block's header words and entries into TMEM lanes of one of kABufs A
+//               buffers (16 hi and 16 lo words a row, two fp16 a word);
+//   warp 17     MMA: 6 tcgen05.mma (kind::f16, A from TMEM, M=128 N=64 K=16) into one of
 //               two TMEM accumulators;
-//   warps 4-7   drain: TMEM -> f64 registers per flush group; at the end of the item the
-//               rows (C - offsets, as the next product's D^T, f32 rows and column sums) or
-//               the segment's f64 partial.
-// HBM sees each block once per product (its masks and values: 512 + 4 nnz bytes) and
-// D^T about once per pass over it (L2 serves the other tiles of a segment).
+//   warps 8-15  drain: TMEM -> f64 registers per flush group, 32 columns a warp; at the
+//               end of the item the rows (C - offsets, as the next product's D^T, f32 rows
+//               and column sums) or the segment's f64 partial.
+// HBM sees each block once per product (512 header bytes and 8 bytes an entry) and D^T
+// about once per pass over it (L2 serves the other tiles of a segment).
 #include <cuda_fp16.h>
 #include <cudaTypedefs.h>
 #include <cub/device/device_scan.cuh>

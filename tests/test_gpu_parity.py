@@ -77,7 +77,7 @@ def _col_diff(a, b):
     return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
 
 
-# The two product engines: tensor cores (tf32 parts, f32 sums of at most 512 terms
+# The two product engines: tensor cores (fp16 hi/lo parts, f32 sums of at most 512 terms
 # flushed into f64) and the SIMT pipes (f64 throughout). Bars against the FP64 oracle:
 # variances (singular values squared) and loadings/embedding columns.
 PRODUCTS = {"tc": (2e-5, 2e-4), "simt": (1e-6, 1e-5)}
