@@ -281,6 +281,40 @@ def connectivities_timing(args, ctx, graph) -> dict:
             "ms": statistics.median(times), "nnz": int(nnz.value)}
 
 
+def precision_search(ctx, emb_ptr: int, n: int, d: int, n_neighbors: int = 30) -> dict:
+    """The precision form's search on the timed PCA's device embedding: n_neighbors 30 with
+    the bf16 tensor-core distances (f32 accumulation) picking the candidates, then their
+    exact re-rank (kyto's f64 keys of every candidate inside the filter's proven slack,
+    which holds at least the 4k candidates the form asks for). One untimed call, then
+    one timed by host wall clock around a device synchronisation."""
+    import torch
+
+    import kyto_b200 as K
+
+    k = n_neighbors - 1
+    out = (torch.empty(n + 1, dtype=torch.int64, device="cuda"),
+           torch.empty(n * k, dtype=torch.int32, device="cuda"),
+           torch.empty(n * k, dtype=torch.float32, device="cuda"))
+    st = K.KnnStats()
+    os.environ["KYTO_GPU_KNN_FILTER"] = "bf16"
+    try:
+        for _ in range(2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            K._check(K.library().kg_knn_exact(
+                ctx.handle, emb_ptr, n, d, 0, n_neighbors, K._ptr(out[0]), K._ptr(out[1]),
+                K._ptr(out[2]), K.ctypes.byref(st)))
+            torch.cuda.synchronize()
+            ms = 1e3 * (time.perf_counter() - t0)
+    finally:
+        del os.environ["KYTO_GPU_KNN_FILTER"]
+    return {"workload": f"{n:,} x {d} timed PCA embedding, n_neighbors {n_neighbors}",
+            "filter": "bf16 operands, f32 accumulation; exact f64 re-rank", "ms": ms,
+            "filter_ms": st.filter_ms, "rank_ms": st.rank_ms,
+            "candidates_per_row": st.candidates / n, "rows_searched_in_full": st.rows_full,
+            "n_neighbors": n_neighbors, "graph": tuple(t.cpu().numpy() for t in out)}
+
+
 def spread_rows(n: int, q: int) -> np.ndarray:
     """q distinct rows spread evenly over [0, n) (every part of the search's scan order
     holds some of them)."""
@@ -288,7 +322,7 @@ def spread_rows(n: int, q: int) -> np.ndarray:
     return np.unique(np.linspace(0, n - 1, q).round().astype(np.uint64))
 
 
-def cpu_baseline_and_parity(args, x, vals, res, graph) -> tuple[dict, dict]:
+def cpu_baseline_and_parity(args, x, vals, res, graph, precision=None) -> tuple[dict, dict]:
     """kyto's CPU path (the oracle's C++ restatement, all host threads) on the bench's
     workload, and the device results checked against it.
 
@@ -297,7 +331,9 @@ def cpu_baseline_and_parity(args, x, vals, res, graph) -> tuple[dict, dict]:
     - kNN: kyto's exact search prepared once over the device embedding (timed), then the
       queries of ``spread_rows`` (timed); the 1M search is estimated as setup + per-query
       time x n. The same queries' rows of the device graph (``graph``, searched on the same
-      embedding, as kyto's parity rule takes it) must equal the oracle's bit for bit."""
+      embedding, as kyto's parity rule takes it) must equal the oracle's bit for bit.
+    - ``precision``: the precision form's search (``precision_search``); 4,096 spread rows
+      of its graph are checked against the oracle's search at its n_neighbors."""
     from oracle import oracle as O
 
     n, d, k = args.cells, args.components, args.neighbors - 1
@@ -323,14 +359,28 @@ def cpu_baseline_and_parity(args, x, vals, res, graph) -> tuple[dict, dict]:
     t0 = time.perf_counter()
     keys, ranked, fallbacks = index.search_rows(args.neighbors, rows)
     t_q = time.perf_counter() - t0
+
+    def rows_equal(keys, ranked, graph, sel):
+        kk = ranked.shape[1]
+        order = np.argsort(ranked, axis=1, kind="stable")
+        o_idx = np.take_along_axis(ranked, order, axis=1)
+        o_dist = np.sqrt(np.take_along_axis(keys, order, axis=1)).astype(np.float32)
+        g_idx = graph[1].reshape(n, kk)[sel.astype(np.int64)]
+        g_dist = graph[2].reshape(n, kk)[sel.astype(np.int64)]
+        return (int(np.all(g_idx == o_idx, axis=1).sum()),
+                int(np.all(g_dist.view(np.uint32) == o_dist.view(np.uint32), axis=1).sum()))
+
+    idx_rows, dist_rows = rows_equal(keys, ranked, graph, rows)
+    wide = None
+    if precision is not None:
+        # The precision form's wider search, judged the same way on its own rows.
+        sel = spread_rows(n, 4096)
+        wkeys, wranked, wfb = index.search_rows(precision["n_neighbors"], sel)
+        wi, wd = rows_equal(wkeys, wranked, precision["graph"], sel)
+        wide = {k2: v for k2, v in precision.items() if k2 != "graph"}
+        wide.update({"query_rows": len(sel), "rows_indices_equal": wi,
+                     "rows_distances_bit_equal": wd, "oracle_full_row_searches": wfb})
     index.close()
-    order = np.argsort(ranked, axis=1, kind="stable")
-    o_idx = np.take_along_axis(ranked, order, axis=1)
-    o_dist = np.sqrt(np.take_along_axis(keys, order, axis=1)).astype(np.float32)
-    g_idx = graph[1].reshape(n, k)[rows.astype(np.int64)]
-    g_dist = graph[2].reshape(n, k)[rows.astype(np.int64)]
-    idx_rows = int(np.all(g_idx == o_idx, axis=1).sum())
-    dist_rows = int(np.all(g_dist.view(np.uint32) == o_dist.view(np.uint32), axis=1).sum())
     t_knn = t_prep + t_q / q * n
     cpu = {
         "value": n / (t_pca + t_knn), "unit": "cells/s", "cores": threads, "kind": "port",
@@ -354,6 +404,8 @@ def cpu_baseline_and_parity(args, x, vals, res, graph) -> tuple[dict, dict]:
                 "against": ("kyto's exact search (oracle) on the device PCA's embedding, "
                             "the rows of the device graph of that embedding")},
     }
+    if wide is not None:
+        parity["precision_form"] = wide
     return cpu, parity
 
 
@@ -600,8 +652,14 @@ def main() -> int:
             ctx.handle, sess.embedding_device_ptr(), n, d, 0, args.neighbors,
             K._ptr(out_dev[0]), K._ptr(out_dev[1]), K._ptr(out_dev[2]), None))
         graph = tuple(t.cpu().numpy() for t in out_dev)
+        try:
+            precision = precision_search(ctx, sess.embedding_device_ptr(), n, d)
+        except Exception as e:  # a side measurement never costs the main line
+            precision, precision_error = None, f"{type(e).__name__}: {e}"
         sess.close()
-        cpu, parity = cpu_baseline_and_parity(args, x, vals, res, graph)
+        cpu, parity = cpu_baseline_and_parity(args, x, vals, res, graph, precision)
+        if precision is None:
+            parity["precision_form"] = {"error": precision_error}
     extra = {}
     if rank == 0 and world == 1:
         try:
