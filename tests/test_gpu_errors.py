@@ -102,6 +102,10 @@ def test_cancel_mid_pca_then_the_context_works(ctx, cells):
         w.stop = True
         w.join()
         assert e.value.status == K.KG_CANCELLED and e.value.code == "KY-E503"
+        # The captured traceback holds the cancelled call's session (its held input) in
+        # a cycle through this frame: let it go now, not at some later collection.
+        del e
+        gc.collect()
         done, total = ctx.progress()
         assert 2 * n <= done < total == 11 * n
     finally:
@@ -126,6 +130,8 @@ def test_cancel_mid_knn_then_the_context_works(ctx, points):
         w.stop = True
         w.join()
         assert e.value.status == K.KG_CANCELLED and e.value.code == "KY-E503"
+        del e
+        gc.collect()
     finally:
         flag[0] = 0
         ctx.set_cancel_flag(None)
@@ -153,6 +159,9 @@ def test_injected_oom_frees_what_it_allocated(ctx, cells, points, after):
 
     _pca(ctx, cells, k=10)
     _knn(ctx, points)
+    # Objects awaiting the cyclic collector (an earlier test's failed call kept alive by
+    # its traceback) still hold pool memory: collect them before taking the baseline.
+    gc.collect()
     torch.cuda.synchronize()
     base = K.pool_usage(0)["used"]
     for call in (lambda: _pca(ctx, cells, k=10), lambda: _knn(ctx, points)):
