@@ -20,7 +20,13 @@ On one GPU the line also carries the metric's second half and the batching form:
 - ``batching``: 64 samples of uneven sizes (PCA 30 + kNN 15 each) through the batching
   form against one sample at a time;
 - ``connectivities`` (the timed step's graph) and ``hvg_moments`` (the seurat moments
-  pass over the benchmark's raw counts): the path's neighbouring rows, timed alone.
+  pass over the benchmark's raw counts): the path's neighbouring rows, timed alone;
+- ``tile_join``: the benchmark's raw counts cut into the store's default tiles and every
+  cell block joined back into CSR rows on the device (kyto's tile checks included),
+  checked bit for bit against the counts;
+- ``parity.precision_form``: the precision form's search (n_neighbors 30, bf16
+  distances, exact re-rank) on the timed 1M embedding, 4,096 rows checked against the
+  oracle.
 
 ``--impl reference``: kyto's CPU algorithms (the C++ restatement in oracle/, all host
 threads) timed on a bounded sample of the same workload: the PCA over a subset of the
@@ -249,6 +255,87 @@ def hvg_timing(args, ctx, x, d_indptr, d_idx) -> dict:
     del counts
     return {"workload": f"{args.cells:,} cells x {g:,} genes raw counts ({x.nnz:,} stored)",
             "ms": float(np.median(times))}
+
+
+def tiles_timing(args, ctx, x, d_indptr, d_idx, cell_block=4096, gene_block=1024) -> dict:
+    """The store's tile join (kg_tiles_to_csr) over the benchmark's raw counts as kyto's
+    writer tiles them by default (4,096 cells x 1,024 genes a tile): every cell block
+    joined back into CSR rows on the device (kyto's checks included), device arrays in
+    and out, CUDA-event timed over all blocks after one warm-up pass. The joined rows
+    must equal the counts' CSR bit for bit (join(tile(X)) = X: the counts hold no stored
+    zeros). The tiles are cut on the device with torch (a sort of the entries by tile and
+    row), as the store's writer lays them out (docs/format.md 4.3)."""
+    import torch
+
+    import kyto_b200 as K
+
+    n, genes, c, gs = args.cells, args.genes, cell_block, gene_block
+    n_gb, n_cb = -(-genes // gs), -(-n // c)
+    indptr = d_indptr.to(torch.int64)
+    counts = torch.from_numpy(x.values.view(np.int32)).cuda()
+    idx = d_idx.to(torch.int64)
+    rows = torch.repeat_interleave(torch.arange(n, device="cuda"), indptr[1:] - indptr[:-1])
+    gb = idx // gs
+    key = ((rows // c) * n_gb + gb) * c + rows % c
+    del rows
+    key, order = torch.sort(key, stable=True)
+    t_idx = (idx[order] - gb[order] * gs).to(torch.int32)
+    t_val = counts[order]
+    del order, gb, idx
+    per_row = torch.bincount(key, minlength=n_cb * n_gb * c).view(n_cb, n_gb, c)
+    del key
+    shards = torch.zeros(n_cb, n_gb, c + 1, dtype=torch.int32, device="cuda")
+    shards[:, :, 1:] = torch.cumsum(per_row, dim=2).to(torch.int32)
+    offsets = torch.zeros(n_cb * n_gb + 1, dtype=torch.int64, device="cuda")
+    offsets[1:] = torch.cumsum(per_row.sum(dim=2).flatten(), 0)
+    del per_row
+    nnz = int(offsets[-1])
+    out_ptr = torch.empty(n_cb * (c + 1), dtype=torch.int64, device="cuda")
+    out_idx = torch.empty(nnz, dtype=torch.int32, device="cuda")
+    out_val = torch.empty(nnz, dtype=torch.int32, device="cuda")
+    # tile_offsets from host memory, as kyto's reader holds them (it checks the whole
+    # array when it opens the layer); the shards and entries on the device.
+    h_offsets = offsets.cpu().numpy().view(np.uint64)
+    blocks = []
+    for b in range(n_cb):
+        lo = int(h_offsets[b * n_gb])
+        to = h_offsets.ctypes.data + 8 * b * n_gb
+        tb = K.TileBlock(b, min(c, n - b * c), c, gs, genes, shards[b].data_ptr(), to,
+                         t_idx.data_ptr() + 4 * lo, t_val.data_ptr() + 4 * lo, K.KG_U32, 0)
+        blocks.append((tb, out_ptr.data_ptr() + 8 * b * (c + 1), out_idx.data_ptr() + 4 * lo,
+                       out_val.data_ptr() + 4 * lo))
+
+    def join_all():
+        for tb, p, i, v in blocks:
+            K._check(K.library().kg_tiles_to_csr(ctx.handle, K.ctypes.byref(tb), p, i, v))
+
+    join_all()
+    torch.cuda.synchronize()
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    join_all()
+    e.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(e)
+    same_entries = bool(torch.equal(out_idx, d_idx.view(torch.int32)) and
+                        torch.equal(out_val, counts))
+    same_rows = True
+    for b in range(n_cb):
+        r = min(c, n - b * c)
+        want = indptr[b * c:b * c + r + 1] - indptr[b * c]
+        same_rows &= bool(torch.equal(out_ptr[b * (c + 1):b * (c + 1) + r + 1], want))
+    shard_bytes = 4 * n_gb * (c + 1) * n_cb
+    moved = 8 * nnz + 8 * nnz + 8 * (n + n_cb) + shard_bytes
+    del t_idx, t_val, out_idx, out_val, shards, counts
+    torch.cuda.empty_cache()
+    return {"workload": (f"{n:,} cells x {genes:,} genes raw counts ({nnz:,} stored) in "
+                         f"{c:,} x {gs:,} tiles: {n_cb} cell blocks of {n_gb} gene blocks"),
+            "ms": ms, "ms_per_block": ms / n_cb,
+            "gb_per_s": moved / (ms / 1e3) / 1e9,
+            "algorithmic": ("8 nnz in + 8 nnz out + 8 (rows + 1) + the indptr shards per pass; "
+                            "one host wait a block for the checks' verdict (tile_offsets "
+                            "from host memory)"),
+            "rows_equal": same_rows, "entries_equal": same_entries}
 
 
 def connectivities_timing(args, ctx, graph) -> dict:
@@ -671,6 +758,10 @@ def main() -> int:
                 extra["hvg_moments"] = hvg_timing(args, ctx, x, d_indptr, d_idx)
             except Exception as e:  # a side measurement never costs the main line
                 extra["hvg_moments"] = {"error": f"{type(e).__name__}: {e}"}
+            try:
+                extra["tile_join"] = tiles_timing(args, ctx, x, d_indptr, d_idx)
+            except Exception as e:  # a side measurement never costs the main line
+                extra["tile_join"] = {"error": f"{type(e).__name__}: {e}"}
         for name, fn, on in (("learned_vs_exact", learned_vs_exact, args.learned_cells),
                              ("batching", batching, args.batch_samples)):
             if not on:

@@ -43,7 +43,8 @@ typedef enum kg_status {
   KG_ERR_OOM = 3,       /* device memory exhausted (KY-E505, "lower memory_limit") */
   KG_CANCELLED = 4,     /* the cancel flag was set (kyto: KY-E503) */
   KG_ERR_TIMEOUT = 5,   /* a bounded wait on the device ran out (KY-E505) */
-  KG_ERR_STATE = 6      /* calls out of order, e.g. results before run (KY-E505) */
+  KG_ERR_STATE = 6,     /* calls out of order, e.g. results before run (KY-E505) */
+  KG_ERR_CORRUPT = 7    /* a tiled layer breaks the store format (kyto: KY-E107) */
 } kg_status;
 
 /* Value type of a CSR block: kyto's CellValues::{U32, F32}
@@ -188,6 +189,46 @@ KG_API kg_status kg_pca_push_block_async(kg_pca* pca, const uint64_t* indptr,
                                          const uint32_t* indices, const void* values,
                                          kg_dtype dtype, uint64_t n_rows, const uint64_t* cells);
 
+/* One cell block of a tiled sparse layer as kyto's store holds it (docs/format.md
+ * 4.1-4.3): tile (b, g) covers cells [b C, b C + rows) and genes [g G, g G + width(g)),
+ * width(g) = min(G, n_genes - g G); its entries are a CSR of local gene indices. The
+ * arrays are those kyto-store's reader decodes from the layer's shards (zstd inner
+ * chunks), host (page-locked or not) or device memory. */
+typedef struct kg_tile_block {
+  uint64_t block;               /* cell block number b */
+  uint32_t rows;                /* rows(b): C, or fewer in the last cell block */
+  uint32_t cell_block_size;     /* C */
+  uint64_t gene_block_size;     /* G */
+  uint64_t n_genes;             /* the layer's genes; n_gene_blocks = ceil(n_genes / G) */
+  const uint32_t* indptr;       /* the block's indptr shard, n_gene_blocks x (C + 1) */
+  const uint64_t* tile_offsets; /* the layer's tile_offsets[b n_gene_blocks ..
+                                   (b + 1) n_gene_blocks], n_gene_blocks + 1 values */
+  const uint32_t* indices;      /* the block's entries: the layer's indices from
+                                   tile_offsets[b n_gene_blocks] on (local gene indices) */
+  const void* data;             /* the same entries' values */
+  kg_dtype dtype;
+  uint32_t reserved;
+} kg_tile_block;
+
+/* Join one cell block's tiles into CSR rows with global gene indices, on the device,
+ * after kyto's checks of every tile (indptr starts at 0, ends at the tile's nnz, never
+ * decreases and is flat over padding rows; each row's local indices strictly increase
+ * below the block width). Replaces decode_cell_block and its checks
+ * (crates/kyto-store/src/tile_decode.rs:74-196); the first problem, in kyto's order (tile,
+ * then check, then row), returns KG_ERR_CORRUPT with kyto's wording, and no entry is
+ * read through an indptr that failed its check. Outputs (host or device): indptr
+ * rows + 1 values from 0; indices and values tile_offsets[last] - tile_offsets[0]
+ * entries, each row's genes in increasing order. */
+KG_API kg_status kg_tiles_to_csr(kg_ctx* ctx, const kg_tile_block* block, uint64_t* indptr,
+                                 uint32_t* indices, void* values);
+
+/* kg_pca_push_block of one tiled cell block: the tiles are joined on the device
+ * (kg_tiles_to_csr, into the session's scratch) and pushed as they are, each row's
+ * table position b C + r as its cell (Omega's seed input). Replaces the host row
+ * rebuild of crates/kyto-exec/src/pca/gpu.rs:73-115 for a tiled store: no CSR is built
+ * on the host. Returns once the block is held on the device. */
+KG_API kg_status kg_pca_push_tiles(kg_pca* pca, const kg_tile_block* block);
+
 /* Run all passes on the device (pass 0 sketch, 9 Krylov products, the embedding pass)
  * with the FP64 orthonormalisation and Rayleigh-Ritz steps between them. Replaces
  * the folds of pca/gpu.rs:149-219 and PcaAccumulator::end_pass (pca.rs:699-801). */
@@ -223,6 +264,25 @@ typedef struct kg_pca_stats {
 } kg_pca_stats;
 
 KG_API kg_status kg_pca_run_stats(const kg_pca* pca, kg_pca_stats* out);
+
+/* A PCA result kept on the device and handed over as a DLPack tensor (DLPack's C ABI,
+ * kDLCUDA on the session's device, kDLFloat 32, row-major, no strides): which =
+ * KG_RESULT_EMBEDDING (n_cells x k) or KG_RESULT_LOADINGS (n_genes x k). The tensor owns
+ * a device copy (cudaMalloc) that outlives the session; its deleter frees it (cudaFree,
+ * which waits for queued work, so a consumer may drop it from any thread at any time).
+ * Hand it to a consumer (torch.from_dlpack, CuPy, JAX) or give it back with
+ * kg_dlpack_free. Replaces the host copy of kyto's embedding for a device consumer
+ * (Implementation Plan.md:144, kDLCUDA export). */
+#define KG_RESULT_EMBEDDING 0
+#define KG_RESULT_LOADINGS 1
+struct DLManagedTensor;
+KG_API kg_status kg_pca_result_dlpack(kg_pca* pca, int32_t which, struct DLManagedTensor** out);
+
+/* Calls a DLPack tensor's deleter (for a tensor no consumer took). */
+KG_API void kg_dlpack_free(struct DLManagedTensor* tensor);
+
+/* DLPack tensors this library handed out and whose deleter has not run yet. */
+KG_API kg_status kg_diag_dlpack_live(int64_t* count);
 
 KG_API void kg_pca_free(kg_pca* pca);
 

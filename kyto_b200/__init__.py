@@ -20,7 +20,8 @@ import numpy as np
 _HERE = Path(__file__).resolve().parent
 LIB_PATH = _HERE / "libkyto_gpu.so"
 
-KG_OK, KG_ERR_INVALID, KG_ERR_DEVICE, KG_ERR_OOM, KG_CANCELLED, KG_ERR_TIMEOUT, KG_ERR_STATE = range(7)
+(KG_OK, KG_ERR_INVALID, KG_ERR_DEVICE, KG_ERR_OOM, KG_CANCELLED, KG_ERR_TIMEOUT, KG_ERR_STATE,
+ KG_ERR_CORRUPT) = range(8)
 KG_U32, KG_F32 = 0, 1
 KG_LEARNED_RANDOM_INIT = 1
 NO_GENE = 0xFFFFFFFF
@@ -33,6 +34,7 @@ KYTO_CODE = {
     KG_CANCELLED: "KY-E503",
     KG_ERR_TIMEOUT: "KY-E505",
     KG_ERR_STATE: "KY-E505",
+    KG_ERR_CORRUPT: "KY-E107",
 }
 
 # Every entry point of include/kyto_gpu.h.
@@ -46,6 +48,8 @@ EXPORTS = (
     "kg_pca_run_stats", "kg_diag_omega", "kg_diag_pool_usage", "kg_diag_fail_allocations",
     "kg_tune_lookup", "kg_tune_store",
     "kg_set_wait_limit", "kg_diag_spmm", "kg_pca_push_block_async",
+    "kg_tiles_to_csr", "kg_pca_push_tiles", "kg_pca_result_dlpack", "kg_dlpack_free",
+    "kg_diag_dlpack_live",
 )
 
 
@@ -56,6 +60,24 @@ class KytoError(RuntimeError):
         self.status = status
         self.code = KYTO_CODE.get(status, "KY-E505")
         super().__init__(f"{self.code}: {message}")
+
+
+class TileBlock(ctypes.Structure):
+    """kg_tile_block: one cell block of a tiled sparse layer (kyto's store format)."""
+
+    _fields_ = [
+        ("block", ctypes.c_uint64),
+        ("rows", ctypes.c_uint32),
+        ("cell_block_size", ctypes.c_uint32),
+        ("gene_block_size", ctypes.c_uint64),
+        ("n_genes", ctypes.c_uint64),
+        ("indptr", ctypes.c_void_p),
+        ("tile_offsets", ctypes.c_void_p),
+        ("indices", ctypes.c_void_p),
+        ("data", ctypes.c_void_p),
+        ("dtype", ctypes.c_int),
+        ("reserved", ctypes.c_uint32),
+    ]
 
 
 class _PcaParams(ctypes.Structure):
@@ -182,6 +204,10 @@ def library() -> ctypes.CDLL:
             "kg_pca_begin": [P, ctypes.POINTER(_PcaParams), ctypes.POINTER(P)],
             "kg_pca_push_block": [P, P, P, P, ctypes.c_int, U64, P],
             "kg_pca_push_block_async": [P, P, P, P, ctypes.c_int, U64, P],
+            "kg_tiles_to_csr": [P, ctypes.POINTER(TileBlock), P, P, P],
+            "kg_pca_push_tiles": [P, ctypes.POINTER(TileBlock)],
+            "kg_pca_result_dlpack": [P, I32, ctypes.POINTER(P)],
+            "kg_diag_dlpack_live": [ctypes.POINTER(ctypes.c_int64)],
             "kg_pca_run": [P],
             "kg_pca_results": [P, P, P, P, P, P],
             "kg_pca_info": [P, P, P, P],
@@ -215,6 +241,8 @@ def library() -> ctypes.CDLL:
         lib.kg_close.restype = None
         lib.kg_pca_free.argtypes = [P]
         lib.kg_pca_free.restype = None
+        lib.kg_dlpack_free.argtypes = [P]
+        lib.kg_dlpack_free.restype = None
         lib.kg_last_error.restype = ctypes.c_size_t
         _lib = lib
     return _lib
@@ -482,6 +510,26 @@ class PcaSession:
         if not wait:
             self._held = getattr(self, "_held", []) + [indptr, indices, values, cells]
 
+    def push_tiles(self, block: int, cell_block_size: int, gene_block_size: int, n_cells: int,
+                   shard, tile_offsets, indices, data) -> None:
+        """Push cell block ``block`` of a tiled layer (kg_pca_push_tiles): the tiles are
+        joined into rows on the device after kyto's checks; arguments as
+        ``tiles_to_csr``. Returns once the block is held on the device."""
+        tb, keep = _tile_block(block, cell_block_size, gene_block_size, n_cells, self.n_genes,
+                               shard, tile_offsets, indices, data)
+        _check(library().kg_pca_push_tiles(self._h, ctypes.byref(tb)))
+        del keep
+
+    def result_dlpack(self, which: str = "embedding") -> "DeviceResult":
+        """A PCA result kept on the device (kg_pca_result_dlpack) for a DLPack consumer:
+        ``torch.from_dlpack(result)`` (or CuPy / JAX) takes it without a host copy. The
+        result owns a device copy that outlives the session; one consumer may take it,
+        else ``close()`` (or collection) gives it back."""
+        code = {"embedding": 0, "loadings": 1}[which]
+        out = ctypes.c_void_p()
+        _check(library().kg_pca_result_dlpack(self._h, code, ctypes.byref(out)))
+        return DeviceResult(out.value)
+
     def run(self) -> None:
         try:
             _check(library().kg_pca_run(self._h))
@@ -723,3 +771,97 @@ def learned_gradients(params: np.ndarray, x: np.ndarray, labels: np.ndarray, hid
         ctx.handle, din, hidden, parts, _ptr(np.ascontiguousarray(params, dtype=np.float32)),
         _ptr(x), rows, _ptr(labels), labels.shape[1], _ptr(grads), _ptr(loss), _ptr(logits)))
     return grads, loss, logits
+
+
+def _tile_block(block, cell_block_size, gene_block_size, n_cells, n_genes, shard, tile_offsets,
+                indices, data):
+    """A TileBlock for cell block ``block`` from the layer's arrays (the block's slices are
+    taken here), and the arrays it points into (kept alive by the caller)."""
+    c, g = int(cell_block_size), int(gene_block_size)
+    n_gb = -(-int(n_genes) // g)
+    rows = min(c, int(n_cells) - int(block) * c)
+    to = tile_offsets[int(block) * n_gb:(int(block) + 1) * n_gb + 1]
+    if isinstance(to, np.ndarray):
+        to = np.ascontiguousarray(to, dtype=np.uint64)
+    lo, hi = int(to[0]), int(to[-1])
+    if hi < lo or hi > len(indices) or len(data) != len(indices):
+        raise KytoError(KG_ERR_CORRUPT, f"the layer is corrupt: tile_offsets of cell block "
+                                        f"{int(block)} end at {hi} but indices and data hold "
+                                        f"{len(indices)} and {len(data)} entries")
+    idx = indices[lo:hi] if hi > lo else indices
+    val = data[lo:hi] if hi > lo else data
+    if isinstance(shard, np.ndarray):
+        shard = np.ascontiguousarray(shard, dtype=np.uint32)
+    if isinstance(idx, np.ndarray):
+        idx = np.ascontiguousarray(idx, dtype=np.uint32)
+    tb = TileBlock(int(block), rows, c, g, int(n_genes), _ptr(shard).value if _ptr(shard) else None,
+                   _ptr(to).value, _ptr(idx).value if len(idx) else None,
+                   _ptr(val).value if len(val) else None, _dtype_code(data), 0)
+    return tb, (shard, to, idx, val)
+
+
+def tiles_to_csr(block: int, cell_block_size: int, gene_block_size: int, n_cells: int,
+                 n_genes: int, shard, tile_offsets, indices, data, ctx: Context | None = None):
+    """Cell block ``block`` of a tiled layer joined into CSR rows on the device
+    (kg_tiles_to_csr; kyto-store's decode_cell_block with its checks). ``shard``: the
+    block's indptr shard (n_gene_blocks x (C + 1)); ``tile_offsets``, ``indices`` and
+    ``data``: the whole layer's arrays (numpy, or torch tensors on the device). Returns
+    (indptr u64 from 0, global gene indices u32, values) as numpy arrays; a corrupt tile
+    raises KytoError with kyto's code KY-E107."""
+    ctx = ctx or default_context()
+    tb, keep = _tile_block(block, cell_block_size, gene_block_size, n_cells, n_genes, shard,
+                           tile_offsets, indices, data)
+    nnz = int(keep[1][-1]) - int(keep[1][0])
+    out_ptr = np.empty(tb.rows + 1, dtype=np.uint64)
+    out_idx = np.empty(nnz, dtype=np.uint32)
+    vdt = np.float32 if tb.dtype == KG_F32 else np.uint32
+    out_val = np.empty(nnz, dtype=vdt)
+    _check(library().kg_tiles_to_csr(ctx.handle, ctypes.byref(tb), _ptr(out_ptr), _ptr(out_idx),
+                                     _ptr(out_val)))
+    return out_ptr, out_idx, out_val
+
+
+_capsule_new = ctypes.pythonapi.PyCapsule_New
+_capsule_new.restype = ctypes.py_object
+_capsule_new.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_void_p]
+
+
+class DeviceResult:
+    """A DLPack tensor the library handed out (a DLManagedTensor owning a device copy),
+    exported once through the DLPack protocol (``__dlpack__``: a "dltensor" capsule the
+    consumer takes over, its deleter run when the consumer drops the tensor). Until
+    then ``close()`` (or collection) runs the deleter here."""
+
+    def __init__(self, managed: int):
+        self._m = managed
+        # DLTensor.device.device_id: after the data pointer and the device type.
+        self._device = ctypes.c_int32.from_address(managed + 12).value
+
+    def __dlpack_device__(self):
+        return (2, self._device)  # kDLCUDA
+
+    def __dlpack__(self, stream=None, max_version=None, dl_device=None, copy=None):
+        # The copy is complete when the library returns it, so any consumer stream may
+        # read it at once; the legacy capsule is what this producer offers.
+        if self._m is None:
+            raise BufferError("this result was already exported or closed")
+        m, self._m = self._m, None
+        return _capsule_new(m, b"dltensor", None)
+
+    def close(self) -> None:
+        m, self._m = self._m, None
+        if m:
+            library().kg_dlpack_free(m)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def dlpack_live() -> int:
+    """DLPack tensors handed out by the library whose deleter has not run yet."""
+    n = ctypes.c_int64()
+    _check(library().kg_diag_dlpack_live(ctypes.byref(n)))
+    return int(n.value)

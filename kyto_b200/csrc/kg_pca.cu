@@ -26,6 +26,7 @@
 #include "kg_maps.cuh"
 #include "kg_spmm.cuh"
 #include "kg_spmm_tc.cuh"
+#include "kg_tiles.cuh"
 
 namespace kg {
 
@@ -1861,6 +1862,25 @@ kg_status kg_pca_push_block_async(kg_pca* pca, const uint64_t* indptr, const uin
   });
 }
 
+kg_status kg_pca_push_tiles(kg_pca* pca, const kg_tile_block* block) {
+  return guarded([&] {
+    if (!pca || !block) fail(KG_ERR_INVALID, "kg_pca_push_tiles: NULL argument");
+    use_device(pca->ctx);
+    if (pca->ran) fail(KG_ERR_STATE, "kg_pca_push_tiles after kg_pca_run");
+    cudaStream_t s = pca->stream;
+    const TileShape sh = tile_shape(block, s);
+    const uint64_t rows = block->rows;
+    DeviceBuffer<uint64_t> indptr(rows + 1, s), cells(rows, s);
+    DeviceBuffer<uint32_t> indices(sh.nnz, s), values(sh.nnz, s);
+    join_tiles(pca->ctx, s, block, sh, indptr.ptr, indices.ptr, values.ptr);
+    // The rows' table positions b C + r (docs/format.md 4.1).
+    iota64_kernel<<<blocks_for(rows, 256), 256, 0, s>>>(
+        cells.ptr, rows, block->block * (uint64_t)block->cell_block_size);
+    KG_LAUNCH_CHECK();
+    pca->push(indptr.ptr, indices.ptr, values.ptr, block->dtype, rows, cells.ptr, false);
+  });
+}
+
 kg_status kg_pca_run(kg_pca* pca) {
   return guarded([&] {
     if (!pca) fail(KG_ERR_INVALID, "kg_pca_run: NULL argument");
@@ -2015,6 +2035,112 @@ kg_status kg_pca_info(const kg_pca* pca, uint64_t* n_cells, uint32_t* n_pca_gene
     if (n_cells) *n_cells = pca->n_cells;
     if (n_pca_genes) *n_pca_genes = pca->n_genes;
     if (passes_run) *passes_run = pca->passes_run;
+  });
+}
+
+}  // extern "C"
+
+// DLPack's C ABI (the open DLPack standard, dlpack.h v0.8): the layouts a consumer reads,
+// with the standard's names and field order (a consumer checks nothing but these bytes).
+struct DLDevice {
+  int32_t device_type;  // kDLCUDA = 2
+  int32_t device_id;
+};
+struct DLDataType {
+  uint8_t code;  // kDLFloat = 2
+  uint8_t bits;
+  uint16_t lanes;
+};
+struct DLTensor {
+  void* data;
+  DLDevice device;
+  int32_t ndim;
+  DLDataType dtype;
+  int64_t* shape;
+  int64_t* strides;
+  uint64_t byte_offset;
+};
+struct DLManagedTensor {
+  DLTensor dl_tensor;
+  void* manager_ctx;
+  void (*deleter)(DLManagedTensor* self);
+};
+
+namespace {
+
+// One exported result: the managed tensor, its shape and the device its copy lives on.
+struct DlpackExport {
+  DLManagedTensor managed{};
+  int64_t shape[2] = {0, 0};
+  int device = 0;
+};
+
+std::atomic<int64_t> g_dlpack_live{0};
+
+void dlpack_deleter(DLManagedTensor* t) {
+  auto* e = static_cast<DlpackExport*>(t->manager_ctx);
+  int prev = 0;
+  const bool had = cudaGetDevice(&prev) == cudaSuccess;
+  cudaSetDevice(e->device);
+  if (t->dl_tensor.data) cudaFree(t->dl_tensor.data);
+  if (had) cudaSetDevice(prev);
+  delete e;
+  g_dlpack_live.fetch_sub(1);
+}
+
+}  // namespace
+
+extern "C" {
+
+kg_status kg_pca_result_dlpack(kg_pca* pca, int32_t which, DLManagedTensor** out) {
+  return guarded([&] {
+    if (!pca || !out) fail(KG_ERR_INVALID, "kg_pca_result_dlpack: NULL argument");
+    if (which != KG_RESULT_EMBEDDING && which != KG_RESULT_LOADINGS)
+      fail(KG_ERR_INVALID, "kg_pca_result_dlpack: which must be KG_RESULT_EMBEDDING or "
+                           "KG_RESULT_LOADINGS");
+    if (!pca->ran) fail(KG_ERR_STATE, "kg_pca_result_dlpack before kg_pca_run");
+    use_device(pca->ctx);
+    const DeviceBuffer<float>& src = which == KG_RESULT_EMBEDDING ? pca->embedding : pca->loadings;
+    auto e = std::make_unique<DlpackExport>();
+    e->device = pca->ctx->device;
+    e->shape[0] = (int64_t)(src.count / pca->k);
+    e->shape[1] = (int64_t)pca->k;
+    void* copy = nullptr;
+    if (src.bytes()) KG_CUDA(cudaMalloc(&copy, src.bytes()));
+    struct Guard {
+      void* p;
+      ~Guard() {
+        if (p) cudaFree(p);
+      }
+    } guard{copy};
+    if (src.bytes())
+      KG_CUDA(cudaMemcpyAsync(copy, src.ptr, src.bytes(), cudaMemcpyDeviceToDevice, pca->stream));
+    wait_stream(pca->ctx, pca->stream);
+    DLTensor& t = e->managed.dl_tensor;
+    t.data = copy;
+    t.device = {2, e->device};
+    t.ndim = 2;
+    t.dtype = {2, 32, 1};
+    t.shape = e->shape;
+    t.strides = nullptr;
+    t.byte_offset = 0;
+    e->managed.manager_ctx = e.get();
+    e->managed.deleter = dlpack_deleter;
+    guard.p = nullptr;
+    *out = &e->managed;
+    e.release();
+    g_dlpack_live.fetch_add(1);
+  });
+}
+
+void kg_dlpack_free(DLManagedTensor* tensor) {
+  if (tensor && tensor->deleter) tensor->deleter(tensor);
+}
+
+kg_status kg_diag_dlpack_live(int64_t* count) {
+  return guarded([&] {
+    if (!count) fail(KG_ERR_INVALID, "kg_diag_dlpack_live: NULL argument");
+    *count = g_dlpack_live.load();
   });
 }
 

@@ -87,3 +87,44 @@ def test_push_beside_a_search(ctx, cells):
     assert np.array_equal(got.embedding.view(np.uint32), ref.embedding.view(np.uint32))
     assert np.array_equal(beside.indices, alone.indices)
     assert np.array_equal(beside.distances.view(np.uint32), alone.distances.view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_pca_results_exported_through_dlpack():
+    """kg_pca_result_dlpack: the embedding and loadings reach torch as kDLCUDA tensors with
+    the results' bits, outlive the session, and are freed by their deleter once torch
+    drops them; a result nobody took is given back by close()."""
+    import gc
+
+    import torch
+
+    ctx = K.Context(0)
+    x = synthetic.counts_csr(3000, 800, 80, 5, 40, seed=2, device="cpu")
+    sess = K.PcaSession(15, 800, seed=0, target_sum=1e4, log1p=True, ctx=ctx)
+    sess.push(x.indptr, x.indices, x.values)
+    sess.run()
+    res = sess.results()
+    live = K.dlpack_live()
+    emb = torch.from_dlpack(sess.result_dlpack("embedding"))
+    load = torch.from_dlpack(sess.result_dlpack("loadings"))
+    assert K.dlpack_live() == live + 2
+    unused = sess.result_dlpack("embedding")
+    assert unused.__dlpack_device__() == (2, 0)
+    assert K.dlpack_live() == live + 3
+    unused.close()
+    assert K.dlpack_live() == live + 2
+    with pytest.raises(BufferError):
+        unused.__dlpack__()
+    sess.close()
+    assert emb.is_cuda and emb.dtype == torch.float32 and tuple(emb.shape) == (3000, 15)
+    assert emb.device.index == 0
+    assert np.array_equal(emb.cpu().numpy().view(np.uint32), res.embedding.view(np.uint32))
+    assert np.array_equal(load.cpu().numpy().view(np.uint32), res.loadings.view(np.uint32))
+    # A device consumer uses it in place: the row norms on the GPU.
+    assert torch.allclose((emb * emb).sum(1).cpu(),
+                          torch.from_numpy((res.embedding.astype(np.float64) ** 2).sum(1)).float(),
+                          rtol=1e-5, atol=1e-6)
+    del emb, load
+    gc.collect()
+    torch.cuda.synchronize()
+    assert K.dlpack_live() == live
