@@ -608,6 +608,33 @@ def batching(n_samples: int, ctx) -> dict:
     }
 
 
+def replica_barrier(dist, cuda: bool) -> None:
+    """Every rank's queued device work done (cuda), then every rank at the same point."""
+    if cuda:
+        import torch
+
+        torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+
+
+def replica_max(dist, v: float, device: str) -> float:
+    """The largest of the ranks' values (the timing rule: a step takes as long as its
+    slowest rank); ``v`` itself with one rank."""
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job(world: int, cells: int, ms: float) -> float:
+    """cells/s of the whole job: every rank searched its own ``cells`` (weak scaling)."""
+    return world * cells / (ms / 1e3)
+
+
 def main() -> int:
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -639,16 +666,10 @@ def main() -> int:
                torch.empty(n * k, dtype=torch.float32, device="cuda"))
 
     def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
+        replica_barrier(dist, cuda=True)
 
     def max_over_ranks(v: float) -> float:
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replica_max(dist, v, device="cuda")
 
     for _ in range(args.warmup):
         run_step(args, ctx, d_indptr, d_idx, d_vals, out_dev, host=False)
@@ -678,7 +699,7 @@ def main() -> int:
     clk = clocks.stop()
     launches = K.kernel_launches() - launches0
     ms = max_over_ranks(start.elapsed_time(stop) / args.steps)
-    value = world * n / (ms / 1e3)
+    value = whole_job(world, n, ms)
 
     e2e = None
     if not args.no_e2e:
@@ -699,7 +720,7 @@ def main() -> int:
         ems = max_over_ranks(e0.elapsed_time(e1) / args.steps)
         h2d = x.indptr.nbytes + x.indices.nbytes + vals.nbytes
         d2h = sum(t.numel() * t.element_size() for t in out_host)
-        e2e = {"value": world * n / (ems / 1e3), "unit": "cells/s", "ms_per_step": ems,
+        e2e = {"value": whole_job(world, n, ems), "unit": "cells/s", "ms_per_step": ems,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
     pk = peaks()
