@@ -414,7 +414,7 @@ def cpu_baseline_and_parity(args, x, vals, res, graph, precision=None) -> tuple[
     workload, and the device results checked against it.
 
     - PCA: the oracle's whole PCA of the same 1M cells (all 11 passes), timed; its singular
-      values and loadings judge the device PCA (``res``) of the timed configuration.
+      values and loadings check the device PCA (``res``) of the timed configuration.
     - kNN: kyto's exact search prepared once over the device embedding (timed), then the
       queries of ``spread_rows`` (timed); the 1M search is estimated as setup + per-query
       time x n. The same queries' rows of the device graph (``graph``, searched on the same

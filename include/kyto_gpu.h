@@ -312,7 +312,7 @@ KG_API kg_status kg_knn_exact(kg_ctx* ctx, const float* embedding, uint64_t n_ro
                        uint64_t* indptr, uint32_t* indices, float* distances,
                        kg_knn_stats* stats);
 
-/* Exact kNN of a batch of samples in one search (the north star's batching form): sample
+/* Exact kNN of a batch of samples in one search (the batching form): sample
  * s is rows [sample_rows[s], sample_rows[s + 1]) of `embedding` (sample_rows: host array
  * of n_samples + 1 offsets from 0 to n_rows); each row gets the n_neighbors - 1 nearest
  * rows of its own sample, exactly as kg_knn_exact on that sample alone. One filter launch
@@ -381,7 +381,7 @@ KG_API kg_status kg_connectivities(kg_ctx* ctx, const uint64_t* indptr, const ui
 
 /* ------------------------------------------------------- learned-partition kNN ---- */
 
-/* No counterpart in kyto: the north star's learned form. A BF16 MLP (n_components ->
+/* No counterpart in kyto: the learned-partition form of the search. A BF16 MLP (n_components ->
  * hidden -> hidden -> n_parts, ReLU) is trained on the device on the exact kNN graph of
  * train_cells evenly strided rows (it starts as the k-means parts' nearest-centre
  * classifier; targets: the parts of a row and of its n_neighbors - 1 neighbours;

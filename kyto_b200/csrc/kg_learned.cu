@@ -2,7 +2,7 @@
 // sample of the rows proposes, for every row, the partitions to search; the search is
 // the exact kNN's tensor-core filter and exact re-rank restricted to those partitions'
 // points, and every row whose proposal is not confident enough is searched against
-// every row. kyto has no learned partitioner: this is the north star's learned form.
+// every row. kyto has no learned partitioner: this form is this library's own.
 //
 //   1. sample: m evenly strided rows; their exact graph (the exact search itself);
 //   2. partitions: k-means of the sample into P parts (kg_cluster.cuh);
