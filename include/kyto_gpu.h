@@ -44,7 +44,8 @@ typedef enum kg_status {
   KG_CANCELLED = 4,     /* the cancel flag was set (kyto: KY-E503) */
   KG_ERR_TIMEOUT = 5,   /* a bounded wait on the device ran out (KY-E505) */
   KG_ERR_STATE = 6,     /* calls out of order, e.g. results before run (KY-E505) */
-  KG_ERR_CORRUPT = 7    /* a tiled layer breaks the store format (kyto: KY-E107) */
+  KG_ERR_CORRUPT = 7,   /* a tiled layer breaks the store format (kyto: KY-E107) */
+  KG_ERR_STORE = 8      /* a stored shard or chunk cannot be read (kyto: KY-E110) */
 } kg_status;
 
 /* Value type of a CSR block: kyto's CellValues::{U32, F32}
@@ -221,6 +222,29 @@ typedef struct kg_tile_block {
  * entries, each row's genes in increasing order. */
 KG_API kg_status kg_tiles_to_csr(kg_ctx* ctx, const kg_tile_block* block, uint64_t* indptr,
                                  uint32_t* indices, void* values);
+
+/* Elements [first, first + count) of one shard of a sharded array of kyto's tiled
+ * layers (indptr, indices or data: Zarr v3 sharding_indexed, inner chunks
+ * [bytes(little), zstd], index [bytes(little), crc32c] at the shard's end; docs/format.md
+ * 4.4), decoded on the host into `out` (elem_bytes 4 or 8; a page-locked buffer lets the
+ * tile join's copies run at the link's rate). shard: the shard file's bytes;
+ * chunks_per_shard and chunk_elems: the array's shard and inner chunk shapes (an indptr
+ * shard: n_gene_blocks chunks of C + 1; indices and data: S / K chunks of K); first: from
+ * the shard's first element. A chunk the range covers whole decodes straight into `out`;
+ * a chunk that is not stored reads as zeros. A short shard, an index whose CRC-32C does
+ * not match, a chunk outside the shard or one that does not decode to its full shape
+ * returns KG_ERR_STORE (KY-E110). Replaces the read of a tile's arrays through kyto's
+ * Zarr crate (crates/kyto-store/src/tile_reader.rs:304-383, read_subset :444-452).
+ * Host code: needs no device. */
+KG_API kg_status kg_shard_read(const uint8_t* shard, uint64_t shard_bytes,
+                               uint64_t chunks_per_shard, uint64_t chunk_elems,
+                               uint32_t elem_bytes, uint64_t first, uint64_t count, void* out);
+
+/* One unsharded chunk ([bytes(little), zstd]: tile_offsets' chunks, docs/format.md 4.4)
+ * decoded into `out` (elems elements of elem_bytes 4 or 8). KG_ERR_STORE if it does not
+ * decode to exactly that. Host code: needs no device. */
+KG_API kg_status kg_chunk_read(const uint8_t* chunk, uint64_t chunk_bytes, uint64_t elems,
+                               uint32_t elem_bytes, void* out);
 
 /* kg_pca_push_block of one tiled cell block: the tiles are joined on the device
  * (kg_tiles_to_csr, into the session's scratch) and pushed as they are, each row's

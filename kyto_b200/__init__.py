@@ -21,7 +21,7 @@ _HERE = Path(__file__).resolve().parent
 LIB_PATH = _HERE / "libkyto_gpu.so"
 
 (KG_OK, KG_ERR_INVALID, KG_ERR_DEVICE, KG_ERR_OOM, KG_CANCELLED, KG_ERR_TIMEOUT, KG_ERR_STATE,
- KG_ERR_CORRUPT) = range(8)
+ KG_ERR_CORRUPT, KG_ERR_STORE) = range(9)
 KG_U32, KG_F32 = 0, 1
 KG_LEARNED_RANDOM_INIT = 1
 NO_GENE = 0xFFFFFFFF
@@ -35,6 +35,7 @@ KYTO_CODE = {
     KG_ERR_TIMEOUT: "KY-E505",
     KG_ERR_STATE: "KY-E505",
     KG_ERR_CORRUPT: "KY-E107",
+    KG_ERR_STORE: "KY-E110",
 }
 
 # Every entry point of include/kyto_gpu.h.
@@ -49,7 +50,7 @@ EXPORTS = (
     "kg_tune_lookup", "kg_tune_store",
     "kg_set_wait_limit", "kg_diag_spmm", "kg_pca_push_block_async",
     "kg_tiles_to_csr", "kg_pca_push_tiles", "kg_pca_result_dlpack", "kg_dlpack_free",
-    "kg_diag_dlpack_live",
+    "kg_diag_dlpack_live", "kg_shard_read", "kg_chunk_read",
 )
 
 
@@ -208,6 +209,8 @@ def library() -> ctypes.CDLL:
             "kg_pca_push_tiles": [P, ctypes.POINTER(TileBlock)],
             "kg_pca_result_dlpack": [P, I32, ctypes.POINTER(P)],
             "kg_diag_dlpack_live": [ctypes.POINTER(ctypes.c_int64)],
+            "kg_shard_read": [P, U64, U64, U64, U32, U64, U64, P],
+            "kg_chunk_read": [P, U64, U64, U32, P],
             "kg_pca_run": [P],
             "kg_pca_results": [P, P, P, P, P, P],
             "kg_pca_info": [P, P, P, P],
@@ -798,6 +801,53 @@ def _tile_block(block, cell_block_size, gene_block_size, n_cells, n_genes, shard
                    _ptr(to).value, _ptr(idx).value if len(idx) else None,
                    _ptr(val).value if len(val) else None, _dtype_code(data), 0)
     return tb, (shard, to, idx, val)
+
+
+def _bytes_ptr(b):
+    """A bytes-like object's data pointer (bytes, bytearray, numpy u8) and the object to
+    keep alive while it is used."""
+    a = np.frombuffer(b, dtype=np.uint8) if isinstance(b, (bytes, bytearray, memoryview)) else b
+    return _ptr(a), a
+
+
+def shard_read(shard, chunks_per_shard: int, chunk_elems: int, dtype, first: int, count: int,
+               out=None) -> np.ndarray:
+    """Elements [first, first + count) of one shard of a tiled layer's sharded array
+    (kg_shard_read), decoded on the host into ``out`` (a new array if None; a page-locked
+    torch tensor works too). A shard that cannot be read raises KytoError KY-E110."""
+    dtype = np.dtype(dtype)
+    if out is None:
+        out = np.empty(int(count), dtype=dtype)
+    p, keep = _bytes_ptr(shard)
+    _check(library().kg_shard_read(p, len(keep), int(chunks_per_shard), int(chunk_elems),
+                                   dtype.itemsize, int(first), int(count), _ptr(out)))
+    return out
+
+
+def read_sharded(shards, chunk_elems: int, shard_elems: int, dtype, first: int, count: int,
+                 out=None) -> np.ndarray:
+    """Elements [first, first + count) of a sharded array given as its shards' bytes in
+    order (each read with ``shard_read`` into its part of ``out``)."""
+    dtype = np.dtype(dtype)
+    if out is None:
+        out = np.empty(int(count), dtype=dtype)
+    e, end = int(first), int(first) + int(count)
+    while e < end:
+        s = e // shard_elems
+        stop = min(end, (s + 1) * shard_elems)
+        shard_read(shards[s], shard_elems // chunk_elems, chunk_elems, dtype, e - s * shard_elems,
+                   stop - e, out[e - first:stop - first])
+        e = stop
+    return out
+
+
+def chunk_read(chunk, elems: int, dtype) -> np.ndarray:
+    """One unsharded chunk (tile_offsets') decoded on the host (kg_chunk_read)."""
+    dtype = np.dtype(dtype)
+    out = np.empty(int(elems), dtype=dtype)
+    p, keep = _bytes_ptr(chunk)
+    _check(library().kg_chunk_read(p, len(keep), int(elems), dtype.itemsize, _ptr(out)))
+    return out
 
 
 def tiles_to_csr(block: int, cell_block_size: int, gene_block_size: int, n_cells: int,
