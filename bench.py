@@ -24,6 +24,9 @@ On one GPU the line also carries the metric's second half and the batching form:
 - ``tile_join``: the benchmark's raw counts cut into the store's default tiles and every
   cell block joined back into CSR rows on the device (kyto's tile checks included),
   checked bit for bit against the counts;
+- ``store_path``: 200,000 of those cells as a tiled layer's zstd shards, every cell block
+  decoded on the host into page-locked buffers and joined on the device, checked against
+  the counts;
 - ``parity.precision_form``: the precision form's search (n_neighbors 30, bf16
   distances, exact re-rank) on the timed 1M embedding, 4,096 rows checked against the
   oracle.
@@ -336,6 +339,158 @@ def tiles_timing(args, ctx, x, d_indptr, d_idx, cell_block=4096, gene_block=1024
                             "one host wait a block for the checks' verdict (tile_offsets "
                             "from host memory)"),
             "rows_equal": same_rows, "entries_equal": same_entries}
+
+
+def _crc32c(data: bytes) -> int:
+    """CRC-32C (Castagnoli, reflected 0x82F63B78): the shard index's checksum."""
+    c = 0xFFFFFFFF
+    for byte in data:
+        c ^= byte
+        for _ in range(8):
+            c = (c >> 1) ^ 0x82F63B78 if c & 1 else c >> 1
+    return c ^ 0xFFFFFFFF
+
+
+def write_shards(values: np.ndarray, inner: int, per_shard: int) -> list[bytes]:
+    """A 1-D array as the store writes a sharded array (docs/format.md 4.4): shards of
+    ``per_shard`` inner chunks of ``inner`` elements, each chunk one zstd frame (none for
+    a chunk of zeros), then the index of (offset, nbytes) little-endian u64 pairs and its
+    CRC-32C. The bench's synthetic store input."""
+    import pyarrow as pa
+
+    values = np.ascontiguousarray(values)
+    shards = []
+    step = inner * per_shard
+    for s0 in range(0, max(len(values), 1), step):
+        body, index = [], []
+        at = 0
+        for c in range(per_shard):
+            chunk = np.zeros(inner, dtype=values.dtype)
+            part = values[s0 + c * inner:s0 + (c + 1) * inner]
+            chunk[:len(part)] = part
+            if not chunk.any():
+                index.append((2**64 - 1, 2**64 - 1))
+                continue
+            frame = pa.compress(chunk.tobytes(), codec="zstd", asbytes=True)
+            index.append((at, len(frame)))
+            body.append(frame)
+            at += len(frame)
+        ib = np.array(index, dtype="<u8").tobytes()
+        shards.append(b"".join(body) + ib + _crc32c(ib).to_bytes(4, "little"))
+    return shards
+
+
+def tiled_store(indptr, indices, values, n_genes: int, cell_block=4096, gene_block=1024,
+                inner=65536, per_shard=64) -> dict:
+    """A CSR (sorted rows) as a tiled layer's shards (docs/format.md 4.1-4.4): an indptr
+    shard per cell block (one inner chunk a tile), the entries' local gene indices and
+    values in sharded arrays, tile_offsets on the host (as a reader holds them)."""
+    indptr = np.asarray(indptr, dtype=np.int64)
+    n = len(indptr) - 1
+    c, gs = cell_block, gene_block
+    n_gb, n_cb = -(-n_genes // gs), -(-n // c)
+    rows = np.repeat(np.arange(n, dtype=np.int64), np.diff(indptr))
+    gb = np.asarray(indices, dtype=np.int64) // gs
+    tile = (rows // c) * n_gb + gb
+    # A stable sort by tile keeps rows, then genes, in order (16-bit keys sort by radix).
+    key = tile.astype(np.int16) if n_cb * n_gb < (1 << 15) else tile
+    order = np.argsort(key, kind="stable")
+    del key
+    local = (np.asarray(indices, dtype=np.int64) - gb * gs).astype(np.uint32)[order]
+    vals = np.asarray(values)[order]
+    per_row = np.bincount(tile * c + rows % c, minlength=n_cb * n_gb * c).reshape(n_cb, n_gb, c)
+    offsets = np.zeros(n_cb * n_gb + 1, dtype=np.uint64)
+    offsets[1:] = np.cumsum(per_row.sum(axis=2).ravel())
+    ptr_shards = []
+    for b in range(n_cb):
+        sh = np.zeros((n_gb, c + 1), dtype=np.uint32)
+        sh[:, 1:] = np.cumsum(per_row[b], axis=1)
+        ptr_shards.append(write_shards(sh.ravel(), c + 1, n_gb)[0])
+    return {"n_cells": n, "n_genes": n_genes, "cell_block": c, "gene_block": gs,
+            "n_gb": n_gb, "n_cb": n_cb, "inner": inner, "per_shard": per_shard,
+            "offsets": offsets, "indptr_shards": ptr_shards,
+            "indices_shards": write_shards(local, inner, per_shard),
+            "values_shards": write_shards(vals, inner, per_shard)}
+
+
+def read_cell_block(store: dict, b: int, shard_out, idx_out, val_out) -> tuple[int, int]:
+    """Cell block ``b`` decoded on the host into the given (page-locked) buffers, as a
+    block stream reads it: its indptr shard whole, its entries' range across the entry
+    shards (kg_shard_read). Returns the range (first entry, entries)."""
+    import kyto_b200 as K
+
+    n_gb, c = store["n_gb"], store["cell_block"]
+    K.shard_read(store["indptr_shards"][b], n_gb, c + 1, np.uint32, 0, n_gb * (c + 1),
+                 shard_out[:n_gb * (c + 1)])
+    lo, hi = int(store["offsets"][b * n_gb]), int(store["offsets"][(b + 1) * n_gb])
+    step = store["inner"] * store["per_shard"]
+    K.read_sharded(store["indices_shards"], store["inner"], step, np.uint32, lo, hi - lo,
+                   idx_out[:hi - lo])
+    K.read_sharded(store["values_shards"], store["inner"], step, np.uint32, lo, hi - lo,
+                   val_out[:hi - lo])
+    return lo, hi - lo
+
+
+def store_path_timing(args, ctx, x, d_indptr, d_idx, cells=200_000) -> dict:
+    """kyto's store path, from the shards' bytes to the rows on the device: the first
+    ``cells`` cells of the benchmark's raw counts as a tiled layer's shards (the store's
+    default 4,096 x 1,024 tiles, 64K-element zstd inner chunks), then every cell block
+    decoded on the host into page-locked buffers (kg_shard_read, all host threads) and
+    joined on the device with kyto's checks (kg_tiles_to_csr). Host wall clock over all
+    blocks after one warm-up pass; the joined rows must equal the counts' CSR."""
+    import torch
+
+    import kyto_b200 as K
+
+    n = min(cells, args.cells)
+    nnz = int(x.indptr[n])
+    store = tiled_store(x.indptr[:n + 1], x.indices[:nnz], x.values[:nnz], args.genes)
+    n_gb, c = store["n_gb"], store["cell_block"]
+    most = int(max(store["offsets"][(b + 1) * n_gb] - store["offsets"][b * n_gb]
+                   for b in range(store["n_cb"])))
+    pin = lambda m: torch.empty(max(m, 1), dtype=torch.int32).pin_memory()  # noqa: E731
+    h_shard, h_idx, h_val = pin(n_gb * (c + 1)), pin(most), pin(most)
+    s_np, i_np, v_np = (t.numpy().view(np.uint32) for t in (h_shard, h_idx, h_val))
+    out_ptr = torch.empty(store["n_cb"] * (c + 1), dtype=torch.int64, device="cuda")
+    out_idx = torch.empty(nnz, dtype=torch.int32, device="cuda")
+    out_val = torch.empty(nnz, dtype=torch.int32, device="cuda")
+    offsets = store["offsets"]
+
+    def one_pass() -> tuple[float, float]:
+        decode = join = 0.0
+        for b in range(store["n_cb"]):
+            t0 = time.perf_counter()
+            lo, m = read_cell_block(store, b, s_np, i_np, v_np)
+            t1 = time.perf_counter()
+            tb = K.TileBlock(b, min(c, n - b * c), c, store["gene_block"], args.genes,
+                             h_shard.data_ptr(), offsets.ctypes.data + 8 * b * n_gb,
+                             h_idx.data_ptr(), h_val.data_ptr(), K.KG_U32, 0)
+            K._check(K.library().kg_tiles_to_csr(
+                ctx.handle, K.ctypes.byref(tb), out_ptr.data_ptr() + 8 * b * (c + 1),
+                out_idx.data_ptr() + 4 * lo, out_val.data_ptr() + 4 * lo))
+            decode += t1 - t0
+            join += time.perf_counter() - t1
+        return decode, join
+
+    one_pass()
+    t0 = time.perf_counter()
+    decode, join = one_pass()
+    wall = time.perf_counter() - t0
+    counts = torch.from_numpy(x.values[:nnz].view(np.int32)).cuda()
+    same = bool(torch.equal(out_idx, d_idx[:nnz].view(torch.int32)) and torch.equal(out_val, counts))
+    indptr = d_indptr[:n + 1].to(torch.int64)
+    for b in range(store["n_cb"]):
+        r = min(c, n - b * c)
+        same &= bool(torch.equal(out_ptr[b * (c + 1):b * (c + 1) + r + 1],
+                                 indptr[b * c:b * c + r + 1] - indptr[b * c]))
+    stored = sum(len(s) for k in ("indptr_shards", "indices_shards", "values_shards")
+                 for s in store[k])
+    return {"workload": (f"{n:,} cells x {args.genes:,} genes raw counts ({nnz:,} stored) as "
+                         f"a tiled layer's shards ({stored / 1e6:.0f} MB of zstd frames): "
+                         f"{store['n_cb']} cell blocks of 4,096 x 1,024 tiles"),
+            "ms": 1e3 * wall, "decode_ms": 1e3 * decode, "join_ms": 1e3 * join,
+            "cells_per_s": n / wall, "decoded_gb_per_s": 8 * nnz / decode / 1e9,
+            "host_threads": os.cpu_count(), "rows_equal_csr": same}
 
 
 def connectivities_timing(args, ctx, graph) -> dict:
@@ -783,6 +938,10 @@ def main() -> int:
                 extra["tile_join"] = tiles_timing(args, ctx, x, d_indptr, d_idx)
             except Exception as e:  # a side measurement never costs the main line
                 extra["tile_join"] = {"error": f"{type(e).__name__}: {e}"}
+            try:
+                extra["store_path"] = store_path_timing(args, ctx, x, d_indptr, d_idx)
+            except Exception as e:  # a side measurement never costs the main line
+                extra["store_path"] = {"error": f"{type(e).__name__}: {e}"}
         for name, fn, on in (("learned_vs_exact", learned_vs_exact, args.learned_cells),
                              ("batching", batching, args.batch_samples)):
             if not on:

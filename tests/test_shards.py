@@ -146,3 +146,40 @@ def test_threaded_decode_reports_the_lowest_damaged_chunk():
         assert e.value.code == "KY-E110" and "inner chunk 5" in str(e.value), str(e.value)
     good = S.write_shards(v, k, len(v))[0]
     assert np.array_equal(K.shard_read(good, n_chunks, k, np.uint32, 0, len(v)), v)
+
+
+def test_bench_store_writer_and_block_reader_give_the_rows():
+    """bench.py's store leg on the host: its tiled-layer writer (the store's layout) and
+    its block reader (kg_shard_read into the buffers the join reads) give, through the
+    oracle's join, the rows of the CSR it wrote."""
+    import bench
+
+    rng = np.random.default_rng(5)
+    n_cells, n_genes = 9000, 2000
+    counts = rng.poisson(60, n_cells).clip(0, n_genes)
+    indptr = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint64)
+    indices = np.concatenate([np.sort(rng.choice(n_genes, x, replace=False)) for x in counts]
+                             ).astype(np.uint32)
+    values = rng.integers(1, 50, len(indices)).astype(np.uint32)
+    store = bench.tiled_store(indptr, indices, values, n_genes, inner=4096, per_shard=8)
+    grid = T.TileGrid(n_cells, n_genes, 4096, 1024)
+    n_gb, c = store["n_gb"], 4096
+    shard = np.zeros(n_gb * (c + 1), np.uint32)
+    idx = np.zeros(len(indices), np.uint32)
+    val = np.zeros(len(indices), np.uint32)
+    joined = []
+    for b in range(store["n_cb"]):
+        lo, m = bench.read_cell_block(store, b, shard, idx, val)
+        # read_cell_block wrote the entries at the front of the buffers; the oracle's
+        # join wants them at the layer's offsets.
+        layer_idx = np.zeros(len(indices), np.uint32)
+        layer_val = np.zeros(len(indices), np.uint32)
+        layer_idx[lo:lo + m], layer_val[lo:lo + m] = idx[:m], val[:m]
+        joined.append(T.decode_cell_block(grid, b, shard, store["offsets"], layer_idx,
+                                          layer_val))
+    assert np.array_equal(np.concatenate([j[1] for j in joined]), indices)
+    assert np.array_equal(np.concatenate([j[2] for j in joined]), values)
+    ends = np.cumsum([len(j[1]) for j in joined])
+    starts = np.concatenate([[0], ends[:-1]])
+    ptr = np.concatenate([[0]] + [j[0][1:] + s for j, s in zip(joined, starts)])
+    assert np.array_equal(ptr.astype(np.uint64), indptr)
