@@ -858,9 +858,9 @@ def tiles_to_csr(block: int, cell_block_size: int, gene_block_size: int, n_cells
     ``data``: the whole layer's arrays (numpy, or torch tensors on the device). Returns
     (indptr u64 from 0, global gene indices u32, values) as numpy arrays; a corrupt tile
     raises KytoError with kyto's code KY-E107."""
-    ctx = ctx or default_context()
     tb, keep = _tile_block(block, cell_block_size, gene_block_size, n_cells, n_genes, shard,
                            tile_offsets, indices, data)
+    ctx = ctx or default_context()
     nnz = int(keep[1][-1]) - int(keep[1][0])
     out_ptr = np.empty(tb.rows + 1, dtype=np.uint64)
     out_idx = np.empty(nnz, dtype=np.uint32)

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cstring>
+#include <new>
 #include <string>
 #include <thread>
 #include <vector>
@@ -185,12 +186,25 @@ kg_status kg_shard_read(const uint8_t* shard, uint64_t shard_bytes, uint64_t chu
       while (!stop.load(std::memory_order_relaxed)) {
         const uint64_t c = next.fetch_add(1);
         if (c > c_last) break;
+        // Nothing may leave a worker: an exception escaping a thread ends the process.
+        Error err;
+        bool failed = true;
         try {
           one(c, scratch);
+          failed = false;
         } catch (const Error& e) {
+          err = e;
+        } catch (const std::bad_alloc&) {
+          err = Error{KG_ERR_OOM, "host memory exhausted while decoding inner chunk " +
+                                      std::to_string(c)};
+        } catch (...) {
+          err = Error{KG_ERR_STORE, "could not read the shard: inner chunk " +
+                                        std::to_string(c) + ": an unknown error"};
+        }
+        if (failed) {
           if (c < bad[t]) {
             bad[t] = c;
-            errors[t] = e;
+            errors[t] = err;
           }
           stop.store(true);
         }

@@ -116,6 +116,17 @@ def test_oracle_fast_encoder_equals_the_loop():
             assert np.array_equal(a, b)
 
 
+def test_entries_shorter_than_tile_offsets_are_refused_on_the_host():
+    """The binding refuses a block whose tile_offsets run past the entries it was given
+    (kyto's check_tile_offsets wording, KY-E107) before any device work."""
+    import kyto_b200 as K
+
+    with pytest.raises(K.KytoError) as e:
+        K.tiles_to_csr(0, 2, 2, 3, 5, np.array(GOOD0, np.uint32), OFFSETS, INDICES[:2],
+                       DATA[:2])
+    assert e.value.code == "KY-E107" and "hold 2 and 2 entries" in str(e.value)
+
+
 # ---------------------------------------------------------------- device ----------------
 
 @pytest.fixture(scope="module")
