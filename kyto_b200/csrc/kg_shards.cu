@@ -211,7 +211,15 @@ kg_status kg_shard_read(const uint8_t* shard, uint64_t shard_bytes, uint64_t chu
       }
     };
     std::vector<std::thread> pool;
-    for (unsigned t = 1; t < threads; ++t) pool.emplace_back(work, t);
+    for (unsigned t = 1; t < threads; ++t) {
+      // A thread that cannot be started leaves its chunks to the others (the calling
+      // thread takes part in the hand-out too), never a joinable thread behind a throw.
+      try {
+        pool.emplace_back(work, t);
+      } catch (...) {
+        break;
+      }
+    }
     work(0);
     for (auto& th : pool) th.join();
     unsigned worst = 0;
