@@ -183,3 +183,15 @@ def test_bench_store_writer_and_block_reader_give_the_rows():
     starts = np.concatenate([[0], ends[:-1]])
     ptr = np.concatenate([[0]] + [j[0][1:] + s for j, s in zip(joined, starts)])
     assert np.array_equal(ptr.astype(np.uint64), indptr)
+
+
+def test_bench_shard_writer_writes_the_oracles_bytes():
+    """bench.py keeps its own copy of the shard writer (its device legs use no oracle);
+    it writes the same bytes as the oracle's restatement of the layout."""
+    import bench
+
+    rng = np.random.default_rng(9)
+    v = rng.integers(0, 5, 70_000).astype(np.uint32)
+    v[10_000:30_000] = 0
+    assert bench.write_shards(v, 4096, 4) == S.write_shards(v, 4096, 4 * 4096)
+    assert bench._crc32c(b"123456789") == 0xE3069283
